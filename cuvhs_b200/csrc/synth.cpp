@@ -1,0 +1,399 @@
+// Seeded synthetic NTSC VHS RF generator.
+//
+// Produces an 8-bit RF capture of the kind cuVHS decodes: an FM luma carrier
+// (sync tip 3.4 MHz, white 4.4 MHz, on the IRE map of src/format/video_format.cpp:113-116
+// of the reference) carrying NTSC timing (hsync 4.7 us, EQ 2.3 us, broad pulses
+// with 4.7 us serrations, burst 5.3-7.8 us), pre-emphasised with the same
+// high-shelf biquad the decoder inverts (src/pipeline/fm_demod.cu:310-314), plus
+// a colour-under chroma signal at 40 fH with the VHS +/-90 degree per-line
+// rotation that src/pipeline/chroma_decode.cu:143-148 undoes.  Noise, a bounded
+// per-line timebase random walk, amplitude-collapse dropouts, a head-switch
+// time jump and slow speed drift are all seeded and deterministic: the same
+// parameters give byte-identical output on any machine and thread count.
+#include "cuvhs_synth.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kLineRate = 15734.264;
+constexpr double kFsc = 3579545.0;
+constexpr double kChromaUnder = (525.0 * (30.0 / 1.001)) * 40.0;
+constexpr double kHzIre = 1e6 / 140.0;
+constexpr double kIre0 = 4.4e6 - kHzIre * 100.0;
+
+// SplitMix64: counter-based stream so every block of samples has its own
+// reproducible generator.
+struct SplitMix {
+  uint64_t s;
+  explicit SplitMix(uint64_t seed) : s(seed) {}
+  uint64_t next() {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  }
+  double uniform() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
+  double gauss() {
+    double u1 = uniform();
+    double u2 = uniform();
+    if (u1 < 1e-300) u1 = 1e-300;
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * kPi * u2);
+  }
+};
+
+uint64_t mix_seed(uint64_t a, uint64_t b) {
+  SplitMix m(a * 0x632BE59BD9B4E019ull + b + 0x8CB92BA72F3D8DD7ull);
+  m.next();
+  return m.next();
+}
+
+double smoothstep01(double x) {
+  if (x <= 0.0) return 0.0;
+  if (x >= 1.0) return 1.0;
+  return 0.5 - 0.5 * std::cos(kPi * x);
+}
+
+// A level that is `inside` on [a, b) and `outside` elsewhere, with raised-cosine
+// edges `edge` wide centred on a and b.
+double window_level(double t, double a, double b, double edge) {
+  double up = smoothstep01((t - (a - 0.5 * edge)) / edge);
+  double down = smoothstep01((t - (b - 0.5 * edge)) / edge);
+  return up - down;
+}
+
+struct Bar {
+  double ire;   // luma level
+  double u, v;  // chroma components in IRE
+};
+
+// 75% colour bars: white, yellow, cyan, green, magenta, red, blue.
+void make_bars(Bar bars[7]) {
+  const double rgb[7][3] = {{1, 1, 1}, {1, 1, 0}, {0, 1, 1}, {0, 1, 0},
+                            {1, 0, 1}, {1, 0, 0}, {0, 0, 1}};
+  for (int i = 0; i < 7; i++) {
+    double r = 0.75 * rgb[i][0], g = 0.75 * rgb[i][1], b = 0.75 * rgb[i][2];
+    double y = 0.299 * r + 0.587 * g + 0.114 * b;
+    bars[i].ire = 7.5 + 92.5 * y;
+    bars[i].u = 92.5 * 0.492 * (b - y);
+    bars[i].v = 92.5 * 0.877 * (r - y);
+  }
+}
+
+struct LineGeom {
+  int field_line;   // line index within its field (0-based), from the field's first EQ pulse
+  int frame_half;   // half-line index at the line start within the 1050 half-line frame
+  int field_index;  // running field counter (for moving content and track alternation)
+};
+
+// Composite luma (IRE) and chroma components (u, v in IRE) at program time
+// `tau` (samples) measured from the start of frame-aligned line `lam`.
+struct Content {
+  double spl;      // nominal samples per line
+  double fs;
+  Bar bars[7];
+  int n_frame_lines;
+  double us;       // samples per microsecond
+
+  void eval(long long lam, double u, double* ire, double* cu, double* cv) const {
+    // Frame-relative line and half-line.
+    long long fl = lam % 525;
+    if (fl < 0) fl += 525;
+    double half = spl * 0.5;
+    int hidx = (int)(2 * fl + (u >= half ? 1 : 0));
+    double v = (u >= half) ? u - half : u;
+    double t_us = u / us;
+    double tv_us = v / us;
+    long long frame = (lam >= 0 ? lam : lam - 524) / 525;
+    // Field-relative line numbering (field 1 starts at frame line 0, field 2 at
+    // half-line 525, i.e. mid line 262).
+    bool field2 = (hidx >= 525);
+    double field_line_d = field2 ? (hidx - 525) * 0.5 : hidx * 0.5;
+    long long field_index = frame * 2 + (field2 ? 1 : 0);
+
+    const double edge = 0.2;  // us, sync edge width
+    double level = 0.0;       // blanking
+    double cu_ = 0.0, cv_ = 0.0;
+    int rel = field2 ? hidx - 525 : hidx;  // half-lines since the field's first EQ
+    bool vert = rel >= 0 && rel < 18;
+    if (vert) {
+      bool broad = rel >= 6 && rel < 12;
+      double w = broad ? (31.777 - 4.7) : 2.3;
+      level = -40.0 * window_level(tv_us, 0.0, w, edge);
+      // The half-line slot before the first EQ (second half of the previous
+      // line) is handled by the previous line's eval; nothing else here.
+    } else {
+      // Full line with hsync at its start (only even half-lines start lines;
+      // odd half-lines are second halves of normal lines).
+      double sync = window_level(t_us, 0.0, 4.7, edge);
+      // Guard the very start of the field-2 vertical interval: the second half
+      // of frame line 262 belongs to the EQ train (handled above).
+      level = -40.0 * sync;
+      // Colour burst on lines after the vertical interval.
+      int fline = (int)field_line_d;
+      if (fline >= 9) {
+        double bw = window_level(t_us, 5.3, 7.8, 0.3);
+        cu_ += -20.0 * bw;
+      }
+      if (fline >= 20 && fline < 262) {
+        double a0 = 9.4, a1 = 62.4;
+        double act = window_level(t_us, a0, a1, 0.25);
+        double x = (t_us - a0) / (a1 - a0);
+        double yl = 7.5, uu = 0.0, vv = 0.0;
+        if (fline < 170) {
+          // bars with raised-cosine transitions
+          double pos = x * 7.0;
+          int bi = (int)std::floor(pos);
+          bi = std::max(0, std::min(6, bi));
+          double frac = pos - std::floor(pos);
+          const Bar& b0 = bars[bi];
+          const Bar& b1 = bars[std::min(6, bi + 1)];
+          const Bar& bm = bars[std::max(0, bi - 1)];
+          // blend near edges over +-0.03 of a bar width
+          double wr = smoothstep01((frac - 0.97) / 0.06);
+          double wl = smoothstep01((0.03 - frac) / 0.06);
+          yl = b0.ire * (1.0 - wr - wl) + b1.ire * wr + bm.ire * wl;
+          uu = b0.u * (1.0 - wr - wl) + b1.u * wr + bm.u * wl;
+          vv = b0.v * (1.0 - wr - wl) + b1.v * wr + bm.v * wl;
+        } else if (fline < 200) {
+          yl = 7.5 + 45.0 * (1.0 + std::sin(2.0 * kPi * (2.0 * x)));
+        } else {
+          // moving triangle ramp
+          double ph = x + 0.013 * (double)field_index;
+          ph -= std::floor(ph);
+          double tri = ph < 0.5 ? 2.0 * ph : 2.0 - 2.0 * ph;
+          yl = 7.5 + 92.5 * tri;
+        }
+        level += act * yl;
+        cu_ += act * uu;
+        cv_ += act * vv;
+      }
+    }
+    *ire = level;
+    *cu = cu_;
+    *cv = cv_;
+  }
+};
+
+void shelf_high(double f0, double dbgain, double fs, double q, double b[3], double a[3]) {
+  double A = std::pow(10.0, dbgain / 40.0);
+  double w0 = 2.0 * kPi * f0 / fs;
+  double alpha = std::sin(w0) / (2.0 * q);
+  double c = std::cos(w0);
+  double sa = std::sqrt(A);
+  b[0] = A * ((A + 1) + (A - 1) * c + 2 * sa * alpha);
+  b[1] = -2 * A * ((A - 1) + (A + 1) * c);
+  b[2] = A * ((A + 1) + (A - 1) * c - 2 * sa * alpha);
+  a[0] = (A + 1) - (A - 1) * c + 2 * sa * alpha;
+  a[1] = 2 * ((A - 1) - (A + 1) * c);
+  a[2] = (A + 1) - (A - 1) * c - 2 * sa * alpha;
+}
+
+template <typename F>
+void parallel_for(size_t n, int threads, F fn) {
+  if (threads <= 1 || n < 2) {
+    fn(0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  size_t per = (n + threads - 1) / threads;
+  for (int t = 0; t < threads; t++) {
+    size_t a = (size_t)t * per, b = std::min(n, a + per);
+    if (a >= b) break;
+    pool.emplace_back([=] { fn(a, b); });
+  }
+  for (auto& th : pool) th.join();
+}
+
+}  // namespace
+
+extern "C" void cuvhs_synth_default_params(cuvhs_synth_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->sample_rate_hz = 28e6;
+  p->n_fields = 40;
+  p->seed = 1;
+  p->snr_db = 40.0;
+  p->jitter_bound = 0.5;
+  p->jitter_step = 0.15;
+  p->dropout_line_rate = 0.0;
+  p->dropout_min = 5;
+  p->dropout_max = 200;
+  p->headswitch_min = 0;
+  p->headswitch_max = 0;
+  p->speed_drift = 0.0;
+  p->start_line = -1.0;
+  p->tail_lines = 40;
+  p->chroma_level = 0.2;
+  p->carrier_offset_hz = 0.0;
+  p->deviation_scale = 1.0;
+  p->first_track = 0;
+  p->threads = 0;
+}
+
+extern "C" long long cuvhs_synth_length(const cuvhs_synth_params* p) {
+  double spl = p->sample_rate_hz / kLineRate;
+  double lines = p->n_fields * 262.5 + (double)p->tail_lines;
+  double lead = p->start_line >= 0 ? 0.0 : 0.0;
+  (void)lead;
+  return (long long)std::floor(lines * spl);
+}
+
+extern "C" int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long long n_out) {
+  if (!p || !out || n_out <= 0) return -1;
+  if (!(p->sample_rate_hz > 4e6)) return -2;
+  const double fs = p->sample_rate_hz;
+  const double spl = fs / kLineRate;
+  const size_t n = (size_t)n_out;
+  int threads = p->threads > 0 ? p->threads : (int)std::max(1u, std::thread::hardware_concurrency());
+
+  SplitMix master(mix_seed(p->seed, 0x5EED));
+  // Start position: seeded phase within the first frame, so the file starts mid-field.
+  double start_line = p->start_line >= 0 ? p->start_line : 20.0 + 480.0 * master.uniform();
+  long long lam0 = (long long)std::floor(start_line);
+  double u0 = (start_line - (double)lam0) * spl;
+
+  // ---- line-start table r[k] (RF sample position where program line lam0+k starts)
+  size_t n_lines = (size_t)std::ceil((double)n / (spl * 0.95)) + 8;
+  std::vector<double> r(n_lines + 1);
+  {
+    SplitMix jr(mix_seed(p->seed, 0x717));
+    double delta = 0.0, prev_delta = 0.0;
+    r[0] = -u0;
+    for (size_t k = 1; k <= n_lines; k++) {
+      long long lam = lam0 + (long long)k;
+      double step = jr.gauss() * p->jitter_step;
+      delta += step;
+      if (p->jitter_bound > 0) {
+        if (delta > p->jitter_bound) delta = 2 * p->jitter_bound - delta;
+        if (delta < -p->jitter_bound) delta = -2 * p->jitter_bound - delta;
+        delta = std::max(-p->jitter_bound, std::min(p->jitter_bound, delta));
+      } else {
+        delta = 0.0;
+      }
+      double speed = 1.0;
+      if (p->speed_drift != 0.0) {
+        speed = 1.0 + p->speed_drift * std::sin(2.0 * kPi * (double)lam / 21000.0);
+      }
+      double len = spl * speed + (delta - prev_delta);
+      prev_delta = delta;
+      // head switch: a time jump 6 lines before each field's vertical interval
+      long long fl = lam % 525;
+      if (p->headswitch_max > 0 && (fl == 519 || fl == 256)) {
+        int span = std::max(0, p->headswitch_max - p->headswitch_min);
+        int jump = p->headswitch_min + (int)(jr.uniform() * (span + 1));
+        len += (double)jump;
+      }
+      r[k] = r[k - 1] + len;
+    }
+  }
+
+  // ---- dropouts: per-line seeded events, stored as RF sample spans
+  struct Span { double a, b; };
+  std::vector<Span> drops;
+  if (p->dropout_line_rate > 0) {
+    SplitMix dr(mix_seed(p->seed, 0xD0D0));
+    for (size_t k = 0; k < n_lines; k++) {
+      if (dr.uniform() < p->dropout_line_rate) {
+        int span = std::max(0, p->dropout_max - p->dropout_min);
+        int len = p->dropout_min + (int)(dr.uniform() * (span + 1));
+        double pos = r[k] + dr.uniform() * (r[k + 1] - r[k]);
+        drops.push_back({pos, pos + len});
+      }
+    }
+  }
+
+  Content content;
+  content.spl = spl;
+  content.fs = fs;
+  content.us = fs * 1e-6;
+  make_bars(content.bars);
+
+  // ---- pass 1 (parallel): program-time content per RF sample
+  std::vector<float> ire(n), chroma(n);
+  parallel_for(n, threads, [&](size_t a, size_t b) {
+    size_t k = (size_t)(std::upper_bound(r.begin(), r.end(), (double)a) - r.begin());
+    if (k > 0) k--;
+    for (size_t i = a; i < b; i++) {
+      while (k + 1 < r.size() && r[k + 1] <= (double)i) k++;
+      double len = r[k + 1] - r[k];
+      double u = ((double)i - r[k]) * (spl / len);
+      long long lam = lam0 + (long long)k;
+      double y, cu, cv;
+      content.eval(lam, u, &y, &cu, &cv);
+      ire[i] = (float)y;
+      // colour-under: rotation by +/-90 degrees per line, alternating by field track
+      long long fl = lam % 525;
+      bool field2 = (2 * fl + (u >= spl * 0.5 ? 1 : 0)) >= 525;
+      long long field_index = (lam / 525) * 2 + (field2 ? 1 : 0);
+      long long field_line = field2 ? fl - 262 : fl;
+      int track = (int)((field_index + p->first_track) & 1);
+      int rot = track ? 1 : 3;
+      int q = (int)(((field_line * rot) % 4 + 4) % 4);
+      double theta = 2.0 * kPi * std::fmod(kChromaUnder * (double)i / fs, 1.0) + q * (kPi * 0.5);
+      chroma[i] = (float)(cu * std::sin(theta) + cv * std::cos(theta));
+    }
+  });
+
+  // ---- pass 2 (sequential): pre-emphasis IIR on the IRE signal, then FM phase
+  double b[3], a[3];
+  shelf_high(273755.82, 13.9794, fs, 0.462088186, b, a);
+  for (int i = 0; i < 3; i++) { b[i] /= a[0]; }
+  a[1] /= a[0];
+  a[2] /= a[0];
+  a[0] = 1.0;
+  {
+    double x1 = ire[0], x2 = ire[0];
+    double y1 = ire[0], y2 = ire[0];  // DC gain is exactly 1
+    double phase = 0.0;
+    const double dev = p->deviation_scale * kHzIre;
+    const double fc = kIre0 + p->carrier_offset_hz;
+    for (size_t i = 0; i < n; i++) {
+      double x0 = ire[i];
+      double y0 = b[0] * x0 + b[1] * x1 + b[2] * x2 - a[1] * y1 - a[2] * y2;
+      x2 = x1; x1 = x0; y2 = y1; y1 = y0;
+      double f = fc + dev * y0;
+      phase += 2.0 * kPi * f / fs;
+      if (phase > 2.0 * kPi) phase -= 2.0 * kPi * std::floor(phase / (2.0 * kPi));
+      ire[i] = (float)phase;  // reuse the buffer for the carrier phase
+    }
+  }
+
+  // ---- pass 3 (parallel): RF = luma carrier + colour-under, dropouts, noise, u8
+  const double amp_l = 1.0;
+  const double amp_c = p->chroma_level / 40.0;  // chroma components are in IRE (burst 20)
+  const double sig_rms = amp_l / std::sqrt(2.0);
+  const double sigma = sig_rms / std::pow(10.0, p->snr_db / 20.0);
+  const double peak = amp_l + 2.5 * p->chroma_level;
+  const size_t kBlock = 65536;
+  size_t n_blocks = (n + kBlock - 1) / kBlock;
+  parallel_for(n_blocks, threads, [&](size_t ba, size_t bb) {
+    size_t di = 0;
+    for (size_t blk = ba; blk < bb; blk++) {
+      SplitMix nr(mix_seed(p->seed, 0xA0000000ull + blk));
+      size_t i0 = blk * kBlock, i1 = std::min(n, i0 + kBlock);
+      if (!drops.empty()) {
+        di = (size_t)(std::upper_bound(drops.begin(), drops.end(), (double)i0,
+                                       [](double v, const Span& s) { return v < s.b; }) - drops.begin());
+      }
+      for (size_t i = i0; i < i1; i++) {
+        double rf = amp_l * std::cos((double)ire[i]) + amp_c * (double)chroma[i];
+        if (!drops.empty()) {
+          while (di < drops.size() && drops[di].b <= (double)i) di++;
+          if (di < drops.size() && drops[di].a <= (double)i && (double)i < drops[di].b) rf *= 0.03;
+        }
+        rf += sigma * nr.gauss();
+        double q = std::nearbyint(128.0 + 100.0 * rf / peak);
+        if (q < 0) q = 0;
+        if (q > 255) q = 255;
+        out[i] = (uint8_t)q;
+      }
+    }
+  });
+  return 0;
+}

@@ -1,0 +1,45 @@
+/* Seeded synthetic NTSC VHS RF test-signal generator (part of libcuvhs).
+ *
+ * No counterpart in the reference, which ships no test signal: it stands in for
+ * the private tape captures the reference was developed on.  The parameters
+ * follow the workload descriptions used to measure this decoder (sample rate,
+ * field count, SNR, timebase jitter, dropouts, head switch, speed drift, and the
+ * FM carrier/deviation perturbations used for parameter calibration).
+ */
+#ifndef CUVHS_SYNTH_H
+#define CUVHS_SYNTH_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cuvhs_synth_params {
+  double sample_rate_hz;     /* capture rate, e.g. 28e6 */
+  int n_fields;              /* fields of program material */
+  int tail_lines;            /* extra lines appended after the last field */
+  uint64_t seed;
+  double snr_db;             /* RF SNR of the luma carrier against white noise */
+  double jitter_bound;       /* per-line timebase random walk bound, samples */
+  double jitter_step;        /* random walk step std-dev per line, samples */
+  double dropout_line_rate;  /* probability that a line carries a dropout */
+  int dropout_min, dropout_max;        /* dropout length range, samples */
+  int headswitch_min, headswitch_max;  /* head-switch time jump range, samples (0 = off) */
+  double speed_drift;        /* relative slow tape-speed drift amplitude */
+  double start_line;         /* program line at sample 0; <0 picks a seeded start */
+  double chroma_level;       /* colour-under amplitude relative to the luma carrier */
+  double carrier_offset_hz;  /* FM carrier offset */
+  double deviation_scale;    /* FM deviation scale (1 = nominal) */
+  int first_track;           /* head track of the first field (0/1) */
+  int threads;               /* 0 = all host cores */
+} cuvhs_synth_params;
+
+void cuvhs_synth_default_params(cuvhs_synth_params* p);
+/* Number of u8 samples the parameters describe. */
+long long cuvhs_synth_length(const cuvhs_synth_params* p);
+/* Fill out[0..n) with the capture; returns 0 on success. */
+int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long long n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

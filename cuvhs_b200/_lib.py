@@ -1,0 +1,286 @@
+"""ctypes binding of libcuvhs (include/cuvhs.h).
+
+The decoder itself is native: CUDA kernels for sm_100a behind a C ABI, with
+C++ host orchestration.  This module only loads that library and moves numpy
+buffers across the boundary.  There is no Python fallback: importing fails if
+the built library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libcuvhs.so")
+CLI_PATH = os.path.join(_HERE, "bin", "cuvhs")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"libcuvhs.so not found at {LIB_PATH}; build it with `make -C cuvhs_b200/csrc` "
+        "(or __graft_entry__.build())")
+
+lib = ctypes.CDLL(LIB_PATH)
+
+FIELD_W, FIELD_H = 910, 263
+FIELD_PIXELS = FIELD_W * FIELD_H
+MAX_DROPOUTS_PER_FIELD = 512
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "I/O error",
+          5: "capacity exceeded", 6: "unsupported", 7: "output exists"}
+
+
+class CuvhsError(RuntimeError):
+    def __init__(self, status, message=""):
+        super().__init__(f"cuvhs: {STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("system", ctypes.c_int), ("sample_rate_mhz", ctypes.c_double), ("device", ctypes.c_int),
+                ("batch_fields", ctypes.c_int), ("stream_mode", ctypes.c_int)]
+
+
+class FieldInfo(ctypes.Structure):
+    _fields_ = [("file_loc", ctypes.c_uint64), ("is_first_field", ctypes.c_int32),
+                ("field_phase_id", ctypes.c_int32), ("dropout_count", ctypes.c_int32),
+                ("dropout_offset", ctypes.c_int32)]
+
+
+class Output(ctypes.Structure):
+    _fields_ = [("luma", ctypes.c_void_p), ("chroma", ctypes.c_void_p), ("fields", ctypes.c_void_p),
+                ("dropout_line", ctypes.c_void_p), ("dropout_startx", ctypes.c_void_p),
+                ("dropout_endx", ctypes.c_void_p), ("max_fields", ctypes.c_size_t),
+                ("max_dropouts", ctypes.c_size_t), ("fields_out", ctypes.c_size_t),
+                ("dropouts_out", ctypes.c_size_t), ("next_raw_offset", ctypes.c_uint64)]
+
+
+class SynthParams(ctypes.Structure):
+    _fields_ = [("sample_rate_hz", ctypes.c_double), ("n_fields", ctypes.c_int), ("tail_lines", ctypes.c_int),
+                ("seed", ctypes.c_uint64), ("snr_db", ctypes.c_double), ("jitter_bound", ctypes.c_double),
+                ("jitter_step", ctypes.c_double), ("dropout_line_rate", ctypes.c_double),
+                ("dropout_min", ctypes.c_int), ("dropout_max", ctypes.c_int), ("headswitch_min", ctypes.c_int),
+                ("headswitch_max", ctypes.c_int), ("speed_drift", ctypes.c_double),
+                ("start_line", ctypes.c_double), ("chroma_level", ctypes.c_double),
+                ("carrier_offset_hz", ctypes.c_double), ("deviation_scale", ctypes.c_double),
+                ("first_track", ctypes.c_int), ("threads", ctypes.c_int)]
+
+
+_vp = ctypes.c_void_p
+lib.cuvhs_default_config.argtypes = [ctypes.POINTER(Config)]
+lib.cuvhs_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(_vp)]
+lib.cuvhs_create.restype = ctypes.c_int
+lib.cuvhs_destroy.argtypes = [_vp]
+lib.cuvhs_last_error.argtypes = [_vp]
+lib.cuvhs_last_error.restype = ctypes.c_char_p
+lib.cuvhs_status_string.argtypes = [ctypes.c_int]
+lib.cuvhs_status_string.restype = ctypes.c_char_p
+lib.cuvhs_batch_fields.argtypes = [_vp]
+lib.cuvhs_samples_per_field.argtypes = [_vp]
+lib.cuvhs_samples_per_field.restype = ctypes.c_size_t
+lib.cuvhs_tile_stride.argtypes = [_vp]
+lib.cuvhs_tile_stride.restype = ctypes.c_size_t
+lib.cuvhs_reset.argtypes = [_vp]
+lib.cuvhs_set_debug.argtypes = [_vp, ctypes.c_int]
+lib.cuvhs_decode_chunk.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(Output)]
+lib.cuvhs_decode_chunk.restype = ctypes.c_int
+lib.cuvhs_decode_chunk_device.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_uint64)]
+lib.cuvhs_decode_chunk_device.restype = ctypes.c_int
+lib.cuvhs_device_outputs.argtypes = [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]
+lib.cuvhs_device_outputs.restype = ctypes.c_int
+lib.cuvhs_decode_capture.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.POINTER(Output)]
+lib.cuvhs_decode_capture.restype = ctypes.c_int
+lib.cuvhs_json.argtypes = [_vp, ctypes.POINTER(Output), ctypes.c_char_p, ctypes.c_longlong]
+lib.cuvhs_json.restype = ctypes.c_longlong
+lib.cuvhs_decode_file.argtypes = [ctypes.POINTER(Config), ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]
+lib.cuvhs_decode_file.restype = ctypes.c_int
+lib.cuvhs_debug_array.argtypes = [_vp, ctypes.c_char_p, _vp, ctypes.c_longlong]
+lib.cuvhs_debug_array.restype = ctypes.c_longlong
+lib.cuvhs_synth_default_params.argtypes = [ctypes.POINTER(SynthParams)]
+lib.cuvhs_synth_length.argtypes = [ctypes.POINTER(SynthParams)]
+lib.cuvhs_synth_length.restype = ctypes.c_longlong
+lib.cuvhs_synth_ntsc.argtypes = [ctypes.POINTER(SynthParams), _vp, ctypes.c_longlong]
+lib.cuvhs_synth_ntsc.restype = ctypes.c_int
+
+# every symbol include/cuvhs.h and include/cuvhs_synth.h declare
+EXPORTED = [
+    "cuvhs_default_config", "cuvhs_create", "cuvhs_destroy", "cuvhs_last_error", "cuvhs_status_string",
+    "cuvhs_batch_fields", "cuvhs_samples_per_field", "cuvhs_tile_stride", "cuvhs_reset", "cuvhs_decode_chunk",
+    "cuvhs_decode_chunk_device", "cuvhs_device_outputs", "cuvhs_decode_capture", "cuvhs_json",
+    "cuvhs_decode_file", "cuvhs_set_debug", "cuvhs_debug_array", "cuvhs_synth_default_params",
+    "cuvhs_synth_length", "cuvhs_synth_ntsc",
+]
+
+
+def synth_params(**kw) -> SynthParams:
+    p = SynthParams()
+    lib.cuvhs_synth_default_params(ctypes.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def synth_capture(**kw) -> np.ndarray:
+    """Seeded synthetic NTSC VHS RF capture (u8)."""
+    p = synth_params(**kw)
+    n = lib.cuvhs_synth_length(ctypes.byref(p))
+    buf = np.empty(n, np.uint8)
+    rc = lib.cuvhs_synth_ntsc(ctypes.byref(p), buf.ctypes.data, ctypes.c_longlong(n))
+    if rc != 0:
+        raise CuvhsError(1, f"synthesizer returned {rc}")
+    return buf
+
+
+@dataclass
+class DecodeResult:
+    luma: np.ndarray          # [fields, 263, 910] u16
+    chroma: np.ndarray        # [fields, 263, 910] u16
+    file_loc: np.ndarray      # [fields] u64
+    is_first_field: np.ndarray
+    field_phase_id: np.ndarray
+    dropouts: list = field(default_factory=list)  # per field: (line, startx, endx) int32 arrays
+    json: str = ""
+
+    @property
+    def n_fields(self):
+        return self.luma.shape[0]
+
+
+class Decoder:
+    """One libcuvhs context (device memory and stream, carried decode state)."""
+
+    def __init__(self, sample_rate_mhz=28.0, device=0, batch_fields=0, stream_mode=False, debug=False):
+        cfg = Config()
+        lib.cuvhs_default_config(ctypes.byref(cfg))
+        cfg.sample_rate_mhz = float(sample_rate_mhz)
+        cfg.device = int(device)
+        cfg.batch_fields = int(batch_fields)
+        cfg.stream_mode = 1 if stream_mode else 0
+        h = _vp()
+        st = lib.cuvhs_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st != 0:
+            raise CuvhsError(st, "cuvhs_create failed")
+        self._h = h
+        if debug:
+            lib.cuvhs_set_debug(self._h, 1)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.cuvhs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def batch_fields(self):
+        return lib.cuvhs_batch_fields(self._h)
+
+    @property
+    def samples_per_field(self):
+        return lib.cuvhs_samples_per_field(self._h)
+
+    @property
+    def tile_stride(self):
+        return lib.cuvhs_tile_stride(self._h)
+
+    def reset(self):
+        lib.cuvhs_reset(self._h)
+
+    def _check(self, st):
+        if st != 0:
+            raise CuvhsError(st, lib.cuvhs_last_error(self._h).decode())
+
+    def _alloc_output(self, max_fields):
+        bufs = {
+            "luma": np.empty((max_fields, FIELD_H, FIELD_W), np.uint16),
+            "chroma": np.empty((max_fields, FIELD_H, FIELD_W), np.uint16),
+            "fields": (FieldInfo * max_fields)(),
+            "dl": np.empty(max_fields * MAX_DROPOUTS_PER_FIELD, np.int32),
+            "ds": np.empty(max_fields * MAX_DROPOUTS_PER_FIELD, np.int32),
+            "de": np.empty(max_fields * MAX_DROPOUTS_PER_FIELD, np.int32),
+        }
+        out = Output()
+        out.luma = bufs["luma"].ctypes.data
+        out.chroma = bufs["chroma"].ctypes.data
+        out.fields = ctypes.addressof(bufs["fields"])
+        out.dropout_line = bufs["dl"].ctypes.data
+        out.dropout_startx = bufs["ds"].ctypes.data
+        out.dropout_endx = bufs["de"].ctypes.data
+        out.max_fields = max_fields
+        out.max_dropouts = max_fields * MAX_DROPOUTS_PER_FIELD
+        return out, bufs
+
+    def _result(self, out, bufs):
+        n = out.fields_out
+        fi = bufs["fields"]
+        dropouts = []
+        for i in range(n):
+            o, c = fi[i].dropout_offset, fi[i].dropout_count
+            dropouts.append((bufs["dl"][o:o + c].copy(), bufs["ds"][o:o + c].copy(), bufs["de"][o:o + c].copy()))
+        jl = lib.cuvhs_json(self._h, ctypes.byref(out), None, 0)
+        jb = ctypes.create_string_buffer(int(jl) + 1)
+        lib.cuvhs_json(self._h, ctypes.byref(out), jb, jl + 1)
+        return DecodeResult(
+            luma=bufs["luma"][:n], chroma=bufs["chroma"][:n],
+            file_loc=np.array([fi[i].file_loc for i in range(n)], np.uint64),
+            is_first_field=np.array([fi[i].is_first_field for i in range(n)], np.int32),
+            field_phase_id=np.array([fi[i].field_phase_id for i in range(n)], np.int32),
+            dropouts=dropouts, json=jb.value.decode())
+
+    def decode_capture(self, samples: np.ndarray) -> DecodeResult:
+        samples = np.ascontiguousarray(samples, dtype=np.uint8)
+        max_fields = samples.size // self.samples_per_field + 2
+        out, bufs = self._alloc_output(max_fields)
+        self._check(lib.cuvhs_decode_capture(self._h, samples.ctypes.data, samples.size, ctypes.byref(out)))
+        return self._result(out, bufs)
+
+    def decode_chunk(self, samples: np.ndarray, raw_offset: int, num_fields: int):
+        """One reference-style chunk; `samples` starts at capture sample raw_offset."""
+        samples = np.ascontiguousarray(samples, dtype=np.uint8)
+        out, bufs = self._alloc_output(num_fields)
+        self._check(lib.cuvhs_decode_chunk(self._h, samples.ctypes.data, samples.size, raw_offset, num_fields,
+                                           ctypes.byref(out)))
+        return self._result(out, bufs), int(out.next_raw_offset)
+
+    def decode_chunk_device(self, d_ptr: int, n_avail: int, raw_offset: int, num_fields: int):
+        fo = ctypes.c_int(0)
+        nxt = ctypes.c_uint64(0)
+        self._check(lib.cuvhs_decode_chunk_device(self._h, _vp(d_ptr), n_avail, raw_offset, num_fields,
+                                                  ctypes.byref(fo), ctypes.byref(nxt)))
+        return fo.value, nxt.value
+
+    _DTYPES = {"field_offsets": np.int64, "linelocs_coarse": np.float64, "linelocs": np.float64,
+               "demod": np.float32, "video": np.float32, "sync": np.float32, "envelope": np.float32,
+               "chroma_prefilt": np.float32}
+
+    def debug_array(self, name: str) -> np.ndarray:
+        n = lib.cuvhs_debug_array(self._h, name.encode(), None, 0)
+        if n < 0:
+            raise KeyError(name)
+        a = np.empty(n, self._DTYPES.get(name, np.int32))
+        if n:
+            lib.cuvhs_debug_array(self._h, name.encode(), a.ctypes.data, n)
+        return a
+
+
+def decode_file(in_path, out_base, sample_rate_mhz=28.0, device=0, overwrite=True, batch_fields=0):
+    cfg = Config()
+    lib.cuvhs_default_config(ctypes.byref(cfg))
+    cfg.sample_rate_mhz = float(sample_rate_mhz)
+    cfg.device = int(device)
+    cfg.batch_fields = int(batch_fields)
+    st = lib.cuvhs_decode_file(ctypes.byref(cfg), str(in_path).encode(), str(out_base).encode(), 1 if overwrite else 0)
+    if st != 0:
+        raise CuvhsError(st, "cuvhs_decode_file failed")

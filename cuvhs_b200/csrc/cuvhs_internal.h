@@ -1,0 +1,185 @@
+// Internal interfaces of libcuvhs: NTSC format constants, the filter design
+// that turns the reference's frequency responses into short time-domain
+// kernels for shared-memory overlap-save, the device kernels' launchers and
+// the host-side line-location logic.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace cuvhs {
+
+constexpr int kOverlap = 2048;        // overlap-save history of every demod tile
+constexpr int kFieldMarginLines = 20;  // extra lines per tile beyond one field
+constexpr int kMaxPulses = 800;        // pulses kept per field
+constexpr int kMaxDropouts = 512;      // TBC dropout entries per field
+constexpr int kMaxRfDropouts = 128;    // RF-domain dropout spans per field
+constexpr int kLineFFT = 1024;         // chroma per-line transform
+constexpr int kBurstLen = 36;          // burst window width in output samples (76..111)
+enum PulseType { kHsync = 0, kEq1 = 1, kVsync = 2, kEq2 = 3 };
+
+// NTSC constants derived from the capture rate
+// (reference: src/format/video_format.cpp:23-104).
+struct Format {
+  double fs_hz = 0;
+  int lines_per_frame = 525;
+  int output_line_len = 910;
+  int output_field_lines = 263;
+  int field_lines_first = 263, field_lines_second = 262;
+  int num_eq_pulses = 6;
+  int active_line_start = 10;
+  double line_rate = 15734.264;
+  double fsc = 3579545.0;
+  double chroma_under = 0;
+  double hz_ire = 0, ire0 = 0, vsync_ire = -40.0;
+  double pulse_threshold_hz = 0;
+  double output_zero = 1024.0, output_scale = 0;
+  double output_rate = 0;
+  double burst_abs_ref = 4416.0, burst_start_us = 5.3, burst_end_us = 7.8;
+  int samples_per_line = 0, samples_per_field = 0;
+  int spp = 0;  // tile stride: samples_per_field + 20 lines
+  double hsync_width = 0, eq_pulse_width = 0, vsync_width = 0;
+  int burst_start = 0, burst_end = 0;  // in output samples
+  void init(double mhz);
+};
+
+// Filter kernels for the three overlap-save stages.  Every stage reproduces a
+// circular convolution over one reference tile (length `tile`), evaluated
+// block by block: a block of N samples yields N - (neg + pos) outputs.
+struct Design {
+  int tile = 0;     // demod tile length: 7-smooth >= spp + 2048
+  int bins = 0;     // tile/2 + 1
+  // K1a: u8 -> analytic signal (RF band-pass x Hilbert weighting)
+  static constexpr int kNa = 4096;
+  int a_neg = 0, a_pos = 0, a_out = 0;
+  std::vector<float2> ga;       // block spectrum of the truncated analytic kernel / kNa
+  double a_tail = 0;            // relative l2 energy outside the kept support
+  float rot_re = 1, rot_im = 0;  // e^{-i d0}: nominal carrier phase step removed before atan2
+  double d0 = 0;                 // nominal phase step (rad/sample) at ire0
+  float demod_scale = 0;         // fs / 2pi
+  float demod_offset = 0;        // d0 * fs/2pi - ire0 (Hz)
+  // K1b: demod -> video (real part) + sync (imag part)
+  static constexpr int kNb = 8192;
+  int b_neg = 0, b_pos = 0, b_out = 0;
+  std::vector<float2> gb;
+  double b_tail = 0;
+  float corr_video = 0, corr_sync = 0;
+  // chroma colour-under pre-band-pass (zero-padded tile of length ctile)
+  static constexpr int kNc = 16384;
+  int ctile = 0;
+  int c_half = 0, c_out = 0;  // kernel half-width, outputs per half block
+  std::vector<float> gc;       // real block spectrum / kNc
+  double c_tail = 0;
+  // twiddle tables W_N^m
+  std::vector<float2> tw_a, tw_b, tw_c, tw_line;
+  // chroma per-line constants
+  double het_scale = 0;
+  int fsc_bin = 0, bw_bins = 0;
+  void build(const Format& fmt);
+};
+
+// ---------------------------------------------------------------- kernels
+struct DemodArgs {
+  const uint8_t* raw;  // chunk samples, values past the read are 128
+  long long total;     // T * spp (clamp bound of the tile gathers)
+  int tiles, spp, tile;
+  const float2* ga;
+  const float2* gb;
+  const float2* tw_a;
+  const float2* tw_b;
+  int a_pos, a_out, b_pos, b_out;
+  float rot_re, rot_im, d0, demod_scale, demod_offset;
+  float corr_video, corr_sync;
+  float* dem;      // [T*spp] demod - ire0 (Hz)
+  float* env;      // [T*spp] |analytic|
+  double* env_part;  // [T * env_blocks] per-block envelope sums
+  int env_blocks;    // blocks per tile of the K1a grid
+  float* video;    // [T*spp] video - ire0
+  float* sync;     // [T*spp] sync - ire0
+};
+void launch_k1a(const DemodArgs& a, cudaStream_t st);
+void launch_k1b(const DemodArgs& a, cudaStream_t st);
+
+// Threshold edges of the sync signal: falling (x<=thr, prev>thr or start) and
+// rising (x>thr, prev<=thr).  Unordered; the host sorts.
+void launch_edges(const float* sync, long long total, float thr_rel, unsigned* fall, unsigned* rise,
+                  int* counts, int cap, cudaStream_t st);
+
+struct LineArgs {
+  const float* video;
+  const float* sync;
+  double* ll;  // [P*525]
+  int fields;
+  long long total;  // P * spp
+  int lines_per_frame, active_line_start;
+  float thr_rel;
+  double one_us, hsync_width, right_edge_offset;
+  // luma resample
+  uint16_t* luma;  // [P*263*910]
+  int out_w, out_h;
+  float luma_gain, luma_offset;  // u16 = video_rel * gain + offset
+};
+void launch_hsync_refine(const LineArgs& a, cudaStream_t st);
+void launch_luma(const LineArgs& a, cudaStream_t st);
+
+struct ChromaArgs {
+  const uint8_t* raw;
+  float* pre;  // [P*spp]
+  int fields, spp, ctile, c_half, c_out;
+  const float* gc;
+  const float2* tw_c;
+  const float2* tw_line;
+  const double* ll;
+  long long total;  // P * spp
+  const int* track;  // per field
+  double het_scale;
+  int fsc_bin, bw_bins, burst_start;
+  int out_w, out_h, lines_per_frame;
+  float burst_abs_ref;
+  uint16_t* chroma;  // [P*263*910]
+  float* burst;      // [P*263*kBurstLen] band-passed burst window (scaled)
+  double* metric;    // per field burst cancellation metric
+};
+void launch_chroma_prefilter(const ChromaArgs& a, cudaStream_t st);
+// Lines [field0*263, (field0+nfields)*263) of the chunk.
+void launch_chroma_lines(const ChromaArgs& a, int field0, int nfields, bool write_output, cudaStream_t st);
+void launch_burst_metric(const ChromaArgs& a, int field0, int nfields, cudaStream_t st);
+
+struct DropoutArgs {
+  const float* env;
+  const double* env_part;
+  int env_blocks;
+  const double* ll;
+  int fields, spp, lines_per_frame, active_line_start, out_w, out_h;
+  uint16_t* luma;
+  uint16_t* chroma;
+  int* do_count;
+  int* do_lines;
+  int* do_starts;
+  int* do_ends;
+};
+void launch_dropouts(const DropoutArgs& a, cudaStream_t st);
+
+// ---------------------------------------------------------------- host line locations
+// Per-field pulse validation, mean line length, vertical-blanking anchor and
+// line-location snapping (reference: src/pipeline/pipeline.cu:410-893), with
+// the state carried from field to field (pipeline.h:92-97).
+struct LineLocState {
+  int prev_first_field = -1;
+  int prev_progressive_field = -1;
+  long long prev_first_hsync_readloc = -1;
+  double prev_first_hsync_loc = -1.0;
+  double prev_first_hsync_diff = -1.0;
+};
+struct FieldLines {
+  std::vector<int> starts, lengths, types;  // validated pulses
+  std::vector<double> locs;                 // lines_per_frame line starts
+  int is_first = -1;
+};
+void locate_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
+                  long long field_readloc, LineLocState& st, FieldLines& out);
+
+}  // namespace cuvhs

@@ -1,0 +1,186 @@
+// Colour-under chroma kernels (reference K6, src/pipeline/chroma_decode.cu:526-1002).
+//
+//  * prefilter: the reference band-passes each zero-padded tile (60 kHz - 1.2 MHz,
+//    |Butterworth order 4|^2) with one FP64 FFT pair per field in a serial loop
+//    (chroma_decode.cu:596-633).  Here: overlap-save over the same circular
+//    zero-padded tile, 16384-point shared-memory transforms; the kernel is real,
+//    so two output blocks ride in the real and imaginary parts of one transform.
+//  * lines: Catmull-Rom resample of the prefiltered signal on the line grid,
+//    times the heterodyne carrier with the per-line track rotation
+//    (chroma_decode.cu:75-157), 1024-point transform, keep bins fsc +/- 500 kHz
+//    (chroma_decode.cu:163-182), inverse, then burst RMS -> ACC gain -> u16
+//    (chroma_decode.cu:188-231).  One warp transforms two lines at once.
+//  * metric: adjacent-line burst cancellation per field (chroma_decode.cu:242-296).
+#include <cuda_runtime.h>
+
+#include "cuvhs_internal.h"
+#include "smem_fft.cuh"
+
+namespace cuvhs {
+namespace {
+
+constexpr int kThreadsC = 512;
+constexpr int kLineWarps = 4;
+
+__global__ void __launch_bounds__(kThreadsC) prefilter_kernel(ChromaArgs a) {
+  constexpr int N = Design::kNc;
+  extern __shared__ float2 sm[];
+  const int f = blockIdx.y;
+  const int i0 = blockIdx.x * 2 * a.c_out;  // first output of the real half
+  const uint8_t* tile = a.raw + (size_t)f * a.spp;
+  for (int t = threadIdx.x; t < N; t += kThreadsC) {
+    int q0 = (i0 - a.c_half + t) % a.ctile;
+    if (q0 < 0) q0 += a.ctile;
+    int q1 = q0 + a.c_out;
+    if (q1 >= a.ctile) q1 -= a.ctile;
+    const float v0 = q0 < a.spp ? ((float)tile[q0] - 128.0f) * 256.0f : 0.0f;
+    const float v1 = q1 < a.spp ? ((float)tile[q1] - 128.0f) * 256.0f : 0.0f;
+    sm[pidx(t)] = make_float2(v0, v1);
+  }
+  __syncthreads();
+  smem_fft<N, kThreadsC, false>(sm, a.tw_c);
+  for (int k = threadIdx.x; k < N; k += kThreadsC) {
+    const float g = __ldg(&a.gc[k]);
+    const float2 x = sm[pidx(k)];
+    sm[pidx(k)] = make_float2(x.x * g, x.y * g);
+  }
+  __syncthreads();
+  smem_fft<N, kThreadsC, true>(sm, a.tw_c);
+  float* out = a.pre + (size_t)f * a.spp;
+  for (int i = threadIdx.x; i < a.c_out; i += kThreadsC) {
+    const float2 v = sm[pidx(a.c_half + i)];
+    const int p0 = i0 + i, p1 = i0 + a.c_out + i;
+    if (p0 < a.spp) out[p0] = v.x;
+    if (p1 < a.spp) out[p1] = v.y;
+  }
+}
+
+// Heterodyned, resampled chroma sample of chunk line gl at column c.
+__device__ __forceinline__ float het_sample(const ChromaArgs& a, int gl, int c) {
+  const int field = gl / a.out_h, row = gl % a.out_h;
+  if (row + 1 >= a.lines_per_frame) return 0.0f;
+  const double a0 = a.ll[(size_t)field * a.lines_per_frame + row];
+  const double a1 = a.ll[(size_t)field * a.lines_per_frame + row + 1];
+  const double coord = a0 + ((double)c / (double)a.out_w) * (a1 - a0);
+  const int ci = (int)coord;
+  if (ci < 1 || (long long)ci + 2 >= a.total) return 0.0f;
+  const float x = (float)(coord - (double)ci);
+  const float p0 = __ldg(&a.pre[ci - 1]), p1 = __ldg(&a.pre[ci]);
+  const float p2 = __ldg(&a.pre[ci + 1]), p3 = __ldg(&a.pre[ci + 2]);
+  const float c1 = p2 - p0;
+  const float c2 = 2.0f * p0 - 5.0f * p1 + 4.0f * p2 - p3;
+  const float c3 = 3.0f * (p1 - p2) + p3 - p0;
+  const float v = p1 + 0.5f * x * (c1 + x * (c2 + x * c3));
+  // carrier phase in FP64 turns, reduced before the FP32 cosine
+  const int rot = a.track[field] ? 1 : 3;
+  const int lp = (row * rot) & 3;
+  const double u = a.het_scale * (double)(row * a.out_w + c);
+  const float fr = (float)(u - floor(u));
+  const float het = -cospif(2.0f * fr + 0.5f * (float)lp);
+  return v * het;
+}
+
+__global__ void __launch_bounds__(32 * kLineWarps) lines_kernel(ChromaArgs a, int line0, int nlines, int write_output) {
+  __shared__ float2 sm_all[kLineWarps][fft_pad(kLineFFT)];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* sm = sm_all[warp];
+  const int pair = blockIdx.x * kLineWarps + warp;
+  const int la = 2 * pair, lb = la + 1;  // relative to line0
+  if (la >= nlines) return;               // whole warp leaves together
+  const bool has_b = lb < nlines;
+  for (int c = lane; c < kLineFFT; c += 32) {
+    float va = 0.0f, vb = 0.0f;
+    if (c < a.out_w) {
+      va = het_sample(a, line0 + la, c);
+      if (has_b) vb = het_sample(a, line0 + lb, c);
+    }
+    sm[pidx(c)] = make_float2(va, vb);
+  }
+  __syncwarp();
+  smem_fft<kLineFFT, 32, false>(sm, a.tw_line);
+  const int lo = a.fsc_bin - a.bw_bins, hi = a.fsc_bin + a.bw_bins;
+  const float scale = 1.0f / (float)kLineFFT;
+  for (int k = lane; k < kLineFFT; k += 32) {
+    const int kk = k <= kLineFFT / 2 ? k : kLineFFT - k;
+    const float m = (kk >= lo && kk <= hi) ? scale : 0.0f;
+    const float2 x = sm[pidx(k)];
+    sm[pidx(k)] = make_float2(x.x * m, x.y * m);
+  }
+  __syncwarp();
+  smem_fft<kLineFFT, 32, true>(sm, a.tw_line);
+  // burst RMS per line -> ACC gain
+  float ssa = 0.0f, ssb = 0.0f;
+  for (int i = lane; i < kBurstLen; i += 32) {
+    const float2 v = sm[pidx(a.burst_start + i)];
+    ssa += v.x * v.x;
+    ssb += v.y * v.y;
+    a.burst[(size_t)(line0 + la) * kBurstLen + i] = v.x;
+    if (has_b) a.burst[(size_t)(line0 + lb) * kBurstLen + i] = v.y;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    ssa += __shfl_xor_sync(0xffffffffu, ssa, off);
+    ssb += __shfl_xor_sync(0xffffffffu, ssb, off);
+  }
+  if (!write_output) return;
+  const float rms_a = sqrtf(ssa / (float)kBurstLen), rms_b = sqrtf(ssb / (float)kBurstLen);
+  const float acc_a = rms_a > 1.0f ? a.burst_abs_ref / rms_a : 0.0f;
+  const float acc_b = rms_b > 1.0f ? a.burst_abs_ref / rms_b : 0.0f;
+  uint16_t* oa = a.chroma + (size_t)(line0 + la) * a.out_w;
+  uint16_t* ob = a.chroma + (size_t)(line0 + lb) * a.out_w;
+  for (int c = lane; c < a.out_w; c += 32) {
+    const float2 v = sm[pidx(c)];
+    const float xa = fminf(fmaxf(v.x * acc_a + 32768.0f, 0.0f), 65535.0f);
+    oa[c] = (uint16_t)(xa + 0.5f);
+    if (has_b) {
+      const float xb = fminf(fmaxf(v.y * acc_b + 32768.0f, 0.0f), 65535.0f);
+      ob[c] = (uint16_t)(xb + 0.5f);
+    }
+  }
+}
+
+// One warp per field: mean over line pairs (16+2p, 17+2p), p < 115, of the
+// mean |a + b| over the burst window.
+__global__ void metric_kernel(ChromaArgs a, int field0, int nfields) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= nfields) return;
+  const int f = field0 + warp;
+  const int skip = 16;
+  const int npairs = (a.out_h - 2 * skip - 1) / 2;
+  double acc = 0.0;
+  for (int p = lane; p < npairs; p += 32) {
+    const int line = f * a.out_h + skip + 2 * p;
+    const float* x = a.burst + (size_t)line * kBurstLen;
+    const float* y = x + kBurstLen;
+    double s = 0.0;
+    for (int i = 0; i < kBurstLen; i++) s += fabs((double)x[i] + (double)y[i]);
+    acc += s / kBurstLen;
+  }
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if (lane == 0) a.metric[f] = npairs > 0 ? acc / npairs : 1e9;
+}
+
+}  // namespace
+
+void launch_chroma_prefilter(const ChromaArgs& a, cudaStream_t st) {
+  const size_t smem = sizeof(float2) * fft_pad(Design::kNc);
+  cudaFuncSetAttribute(prefilter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dim3 grid((a.spp + 2 * a.c_out - 1) / (2 * a.c_out), a.fields);
+  prefilter_kernel<<<grid, kThreadsC, smem, st>>>(a);
+}
+
+void launch_chroma_lines(const ChromaArgs& a, int field0, int nfields, bool write_output, cudaStream_t st) {
+  const int nlines = nfields * a.out_h;
+  if (nlines <= 0) return;
+  const int pairs = (nlines + 1) / 2;
+  lines_kernel<<<(pairs + kLineWarps - 1) / kLineWarps, 32 * kLineWarps, 0, st>>>(a, field0 * a.out_h, nlines,
+                                                                                  write_output ? 1 : 0);
+}
+
+void launch_burst_metric(const ChromaArgs& a, int field0, int nfields, cudaStream_t st) {
+  if (nfields <= 0) return;
+  const int threads = 128;
+  const int blocks = (nfields * 32 + threads - 1) / threads;
+  metric_kernel<<<blocks, threads, 0, st>>>(a, field0, nfields);
+}
+
+}  // namespace cuvhs

@@ -1,0 +1,598 @@
+// Chunk decode orchestration (host side of libcuvhs).
+//
+// Mirrors the reference's per-chunk flow (src/pipeline/pipeline.cu:1525-2624):
+// demod the chunk's tiles, find VSYNC candidates and cluster them into field
+// windows, find each window's sync pulses, derive line locations, refine them,
+// resample luma and chroma, detect dropouts, then assign field parity.  The
+// sample-rate work runs in the kernels; the per-field pulse logic (a few
+// hundred pulses per field) and the chroma track decisions run here on the
+// host, exactly as the reference does them.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cuvhs.h"
+#include "cuvhs_internal.h"
+#include "pipeline.h"
+
+namespace cuvhs {
+
+namespace {
+
+template <typename T>
+T* dalloc(size_t n, std::string& err, bool& ok) {
+  if (!ok) return nullptr;
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    ok = false;
+    err = std::string("cudaMalloc failed: ") + cudaGetErrorString(e);
+    cudaGetLastError();
+    return nullptr;
+  }
+  return static_cast<T*>(p);
+}
+
+template <typename T>
+void upload(T* d, const std::vector<T>& h, cudaStream_t st) {
+  if (!h.empty()) cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+constexpr int kPhaseCycle[8] = {3, 2, 1, 4, 3, 2, 1, 4};
+
+// NTSC field phase table keyed by (first field, burst quadrant), no phase
+// delta known (src/pipeline/chroma_decode.cu:337-377: the decoder always looks
+// up the first field of a run with delta -1).
+int phase_id_for(int is_first, int quadrant) {
+  static const int first_q[4] = {3, 1, 3, 1};   // quadrant -> id for first fields
+  static const int second_q[4] = {4, 2, 4, 2};  // quadrant -> id for second fields
+  if (quadrant < 0 || quadrant > 3) return 1;
+  return is_first ? first_q[quadrant] : second_q[quadrant];
+}
+
+}  // namespace
+
+Context::~Context() { release(); }
+
+void Context::release() {
+  if (device >= 0) cudaSetDevice(device);
+  for (void* p : allocations) cudaFree(p);
+  allocations.clear();
+  if (stream) cudaStreamDestroy(stream);
+  stream = nullptr;
+}
+
+bool Context::init(const cuvhs_config& c) {
+  cfg = c;
+  if (c.system != 0) {
+    err = "only NTSC is supported";
+    status = CUVHS_ERR_UNSUPPORTED;
+    return false;
+  }
+  if (!(c.sample_rate_mhz >= 8.0 && c.sample_rate_mhz <= 100.0)) {
+    err = "sample rate out of range (8-100 MHz)";
+    status = CUVHS_ERR_INVALID_ARGUMENT;
+    return false;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    err = "no CUDA device";
+    status = CUVHS_ERR_CUDA;
+    return false;
+  }
+  device = c.device;
+  if (device < 0) {
+    size_t best = 0;
+    for (int i = 0; i < ndev; i++) {
+      cudaDeviceProp p;
+      cudaGetDeviceProperties(&p, i);
+      if (p.totalGlobalMem > best) {
+        best = p.totalGlobalMem;
+        device = i;
+      }
+    }
+  }
+  if (device >= ndev) {
+    err = "GPU " + std::to_string(device) + " not found";
+    status = CUVHS_ERR_INVALID_ARGUMENT;
+    return false;
+  }
+  cudaSetDevice(device);
+  fmt.init(c.sample_rate_mhz);
+  des.build(fmt);
+  spp = fmt.spp;
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const size_t per_field = (size_t)spp * (1 + 4 * 5) + (size_t)263 * 910 * 4 + 263 * kBurstLen * 4 + 65536;
+  int b = c.batch_fields;
+  if (b <= 0) {
+    b = (int)std::min<size_t>((size_t)(free_b * 0.5) / per_field, 2048);
+    if (b < 1) b = 1;
+  }
+  if (c.stream_mode && b > 64) b = 64;
+  // 32-bit sample indices inside a chunk
+  const int cap_fields = (int)std::min<long long>(INT_MAX / 2 / (long long)spp, 1 << 20);
+  if (b > cap_fields) b = cap_fields;
+  batch = b;
+  if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) {
+    err = "cudaStreamCreate failed";
+    status = CUVHS_ERR_CUDA;
+    return false;
+  }
+  bool ok = true;
+  const size_t S = (size_t)batch * spp;
+  auto A = [&](auto* tag, size_t n) {
+    using T = std::remove_pointer_t<decltype(tag)>;
+    T* p = dalloc<T>(n, err, ok);
+    if (p) allocations.push_back(p);
+    return p;
+  };
+  env_blocks = (spp + des.a_out - 1) / des.a_out;
+  d_raw = A((uint8_t*)nullptr, S + 64);
+  d_dem = A((float*)nullptr, S);
+  d_env = A((float*)nullptr, S);
+  d_video = A((float*)nullptr, S);
+  d_sync = A((float*)nullptr, S);
+  d_env_part = A((double*)nullptr, (size_t)batch * env_blocks);
+  edge_cap = (int)std::min<size_t>(S / 4 + 4096, (size_t)INT_MAX / 2);
+  d_fall = A((unsigned*)nullptr, edge_cap);
+  d_rise = A((unsigned*)nullptr, edge_cap);
+  d_counts = A((int*)nullptr, 4);
+  d_ll = A((double*)nullptr, (size_t)batch * fmt.lines_per_frame);
+  const size_t F = (size_t)fmt.output_line_len * fmt.output_field_lines;
+  d_luma = A((uint16_t*)nullptr, (size_t)batch * F);
+  d_chroma = A((uint16_t*)nullptr, (size_t)batch * F);
+  d_burst = A((float*)nullptr, (size_t)batch * fmt.output_field_lines * kBurstLen);
+  d_metric = A((double*)nullptr, batch);
+  d_track = A((int*)nullptr, batch);
+  d_do_count = A((int*)nullptr, batch);
+  d_do_lines = A((int*)nullptr, (size_t)batch * kMaxDropouts);
+  d_do_starts = A((int*)nullptr, (size_t)batch * kMaxDropouts);
+  d_do_ends = A((int*)nullptr, (size_t)batch * kMaxDropouts);
+  d_ga = A((float2*)nullptr, des.ga.size());
+  d_gb = A((float2*)nullptr, des.gb.size());
+  d_gc = A((float*)nullptr, des.gc.size());
+  d_twa = A((float2*)nullptr, des.tw_a.size());
+  d_twb = A((float2*)nullptr, des.tw_b.size());
+  d_twc = A((float2*)nullptr, des.tw_c.size());
+  d_twl = A((float2*)nullptr, des.tw_line.size());
+  if (!ok) {
+    status = CUVHS_ERR_OUT_OF_MEMORY;
+    release();
+    return false;
+  }
+  upload(d_ga, des.ga, stream);
+  upload(d_gb, des.gb, stream);
+  upload(d_gc, des.gc, stream);
+  upload(d_twa, des.tw_a, stream);
+  upload(d_twb, des.tw_b, stream);
+  upload(d_twc, des.tw_c, stream);
+  upload(d_twl, des.tw_line, stream);
+  if (cudaStreamSynchronize(stream) != cudaSuccess) {
+    err = std::string("upload failed: ") + cudaGetErrorString(cudaGetLastError());
+    status = CUVHS_ERR_CUDA;
+    return false;
+  }
+  return true;
+}
+
+bool Context::check_cuda(const char* where) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    err = std::string(where) + ": " + cudaGetErrorString(e);
+    status = CUVHS_ERR_CUDA;
+    return false;
+  }
+  return true;
+}
+
+bool Context::sync(const char* where) {
+  cudaError_t e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) {
+    err = std::string(where) + ": " + cudaGetErrorString(e);
+    status = CUVHS_ERR_CUDA;
+    return false;
+  }
+  return check_cuda(where);
+}
+
+void Context::reset_state() {
+  lls = LineLocState();
+  chroma_valid = false;
+  chroma_track = 0;
+  chroma_threshold = 0.0;
+  chroma_cycle_start = 0;
+  last_parity = true;
+}
+
+// Host burst-cancellation metric over one field's burst windows (lines 16..245
+// in pairs), as the track detector measures it (chroma_decode.cu:383-411).
+static double host_burst_metric(const float* b, int H) {
+  const int skip = 16;
+  double total = 0.0;
+  int count = 0;
+  for (int line = skip; line < H - skip - 1; line += 2) {
+    const float* x = b + (size_t)line * kBurstLen;
+    const float* y = x + kBurstLen;
+    double s = 0.0;
+    for (int i = 0; i < kBurstLen; i++) s += std::fabs((double)x[i] + (double)y[i]);
+    total += s / kBurstLen;
+    count++;
+  }
+  return count > 0 ? total / count : 1e9;
+}
+
+// Burst phase in degrees by I/Q product detection over lines 16..246
+// (chroma_decode.cu:415-450).
+static double host_burst_phase(const float* b, int H, const Format& fmt) {
+  const int skip = 16;
+  const double PI = 3.14159265358979323846;
+  double It = 0.0, Qt = 0.0;
+  for (int line = skip; line < H - skip; line++) {
+    const float* x = b + (size_t)line * kBurstLen;
+    double I = 0.0, Q = 0.0;
+    for (int i = 0; i < kBurstLen; i++) {
+      const double v = x[i];
+      const double t = 2.0 * PI * fmt.fsc / fmt.output_rate * (double)(fmt.burst_start + i);
+      I += v * std::cos(t);
+      Q += v * std::sin(t);
+    }
+    const double m = std::sqrt(I * I + Q * Q);
+    if (m > 0.0) {
+      It += I / m;
+      Qt += Q / m;
+    }
+  }
+  return std::fmod(std::atan2(Qt, It) * 180.0 / PI + 360.0, 360.0);
+}
+
+// Decode one chunk.  `src` is host memory unless `src_on_device`.
+bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avail, uint64_t raw_offset,
+                           int num_fields, ChunkResult& res) {
+  res = ChunkResult();
+  if (num_fields < 1 || num_fields > batch) {
+    err = "num_fields must be in [1, batch_fields]";
+    status = CUVHS_ERR_INVALID_ARGUMENT;
+    return false;
+  }
+  cudaSetDevice(device);
+  const size_t spf = (size_t)fmt.samples_per_field;
+  const size_t total_samples = (size_t)num_fields * spp;
+  const size_t n_read = std::min(total_samples, n_avail);
+  if (n_read < spf) return true;  // no field: end of capture
+  // ---- input: the chunk window, the rest set to the u8 mid level (0.0 after conversion)
+  cudaMemcpyAsync(d_raw, src, n_read, src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream);
+  if (n_read < total_samples) cudaMemsetAsync(d_raw + n_read, 128, total_samples - n_read, stream);
+  const int T = (int)std::min(n_read / spf, (size_t)num_fields);
+  // ---- K1: FM demod over T tiles
+  DemodArgs da;
+  da.raw = d_raw;
+  da.total = (long long)T * spp;
+  da.tiles = T;
+  da.spp = spp;
+  da.tile = des.tile;
+  da.ga = d_ga;
+  da.gb = d_gb;
+  da.tw_a = d_twa;
+  da.tw_b = d_twb;
+  da.a_pos = des.a_pos;
+  da.a_out = des.a_out;
+  da.b_pos = des.b_pos;
+  da.b_out = des.b_out;
+  da.rot_re = des.rot_re;
+  da.rot_im = des.rot_im;
+  da.d0 = (float)des.d0;
+  da.demod_scale = des.demod_scale;
+  da.demod_offset = des.demod_offset;
+  da.corr_video = des.corr_video;
+  da.corr_sync = des.corr_sync;
+  da.dem = d_dem;
+  da.env = d_env;
+  da.env_part = d_env_part;
+  da.env_blocks = env_blocks;
+  da.video = d_video;
+  da.sync = d_sync;
+  launch_k1a(da, stream);
+  launch_k1b(da, stream);
+  if (!check_cuda("demod")) return false;
+  // ---- sync edges over the demodulated range
+  const float thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
+  cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), stream);
+  const long long total_chunk = (long long)T * spp;
+  launch_edges(d_sync, total_chunk, thr_rel, d_fall, d_rise, d_counts, edge_cap, stream);
+  int counts[4] = {0, 0, 0, 0};
+  cudaMemcpyAsync(counts, d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  if (!sync("edges")) return false;
+  if (counts[0] > edge_cap || counts[1] > edge_cap) {
+    err = "sync edge list overflow";
+    status = CUVHS_ERR_CAPACITY;
+    return false;
+  }
+  h_fall.resize(counts[0]);
+  h_rise.resize(counts[1]);
+  if (counts[0]) cudaMemcpyAsync(h_fall.data(), d_fall, counts[0] * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
+  if (counts[1]) cudaMemcpyAsync(h_rise.data(), d_rise, counts[1] * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
+  if (!sync("edge lists")) return false;
+  std::sort(h_fall.begin(), h_fall.end());
+  std::sort(h_rise.begin(), h_rise.end());
+  // runs [start, end): end = first rising edge after start, or the range end
+  run_start.resize(h_fall.size());
+  run_end.resize(h_fall.size());
+  {
+    size_t r = 0;
+    for (size_t i = 0; i < h_fall.size(); i++) {
+      while (r < h_rise.size() && h_rise[r] <= h_fall[i]) r++;
+      run_start[i] = (long long)h_fall[i];
+      run_end[i] = r < h_rise.size() ? (long long)h_rise[r] : total_chunk;
+    }
+  }
+  // ---- VSYNC candidates and field windows (vsync_discover.cu:58-72, pipeline.cu:1567-1651)
+  const int minw = (int)(20.0e-6 * fmt.fs_hz), maxw = (int)(35.0e-6 * fmt.fs_hz);
+  std::vector<int> cand;
+  for (size_t i = 0; i < run_start.size(); i++) {
+    const long long w = run_end[i] - run_start[i];
+    if (w >= minw && w <= maxw) cand.push_back((int)run_start[i]);
+  }
+  std::vector<size_t> offs;
+  for (int pos : cand) {
+    if (offs.empty() || ((size_t)pos - offs.back() > (size_t)(fmt.samples_per_field / 2))) {
+      const size_t safe = (pos > 5 * fmt.samples_per_line) ? (size_t)(pos - 5 * fmt.samples_per_line) : 0;
+      offs.push_back(safe);
+    }
+  }
+  if (offs.empty())
+    for (int i = 0; i < T; i++) offs.push_back((size_t)i * spf);
+  int P = (int)offs.size();
+  if (P > num_fields) {
+    P = num_fields;
+    offs.resize(P);
+  }
+  size_t actual_spf = spf;
+  if (offs.size() >= 2) actual_spf = (offs.back() - offs.front()) / (offs.size() - 1);
+  const size_t predicted = offs.back() + actual_spf, margin = 10 * (size_t)fmt.samples_per_line;
+  res.next_raw_offset = predicted > margin ? raw_offset + predicted - margin : raw_offset + predicted;
+  // ---- per-field pulses and line locations (sync_pulses.cu:10-58, pipeline.cu:1717-1778)
+  const int LPF = fmt.lines_per_frame;
+  h_ll.assign((size_t)P * LPF, 0.0);
+  h_is_first.assign(P, -1);
+  if (debug) {
+    dbg_k2c.assign(P, 0);
+    dbg_k2s.assign((size_t)P * kMaxPulses, 0);
+    dbg_k2l.assign((size_t)P * kMaxPulses, 0);
+    dbg_k2bc.assign(P, 0);
+    dbg_k2bs.assign((size_t)P * kMaxPulses, 0);
+    dbg_k2bl.assign((size_t)P * kMaxPulses, 0);
+    dbg_k2bt.assign((size_t)P * kMaxPulses, kHsync);
+  }
+  std::vector<int> ps, pl;
+  FieldLines fl;
+  for (int f = 0; f < P; f++) {
+    ps.clear();
+    pl.clear();
+    const long long off = (long long)offs[f];
+    const long long lim = off + spp - 1;  // last sample index the field's scan reaches
+    size_t i = std::lower_bound(run_start.begin(), run_start.end(), off + 1) - run_start.begin();
+    for (; i < run_start.size() && run_start[i] <= lim; i++) {
+      if (run_end[i] > lim) break;  // still open when the scan ends
+      if ((int)ps.size() < kMaxPulses) {
+        ps.push_back((int)run_start[i]);
+        pl.push_back((int)(run_end[i] - run_start[i]));
+      }
+    }
+    locate_lines(fmt, ps.data(), pl.data(), (int)ps.size(), (long long)(raw_offset + offs[f]), lls, fl);
+    std::copy(fl.locs.begin(), fl.locs.end(), h_ll.begin() + (size_t)f * LPF);
+    h_is_first[f] = fl.is_first;
+    if (debug) {
+      dbg_k2c[f] = (int)ps.size();
+      std::copy(ps.begin(), ps.end(), dbg_k2s.begin() + (size_t)f * kMaxPulses);
+      std::copy(pl.begin(), pl.end(), dbg_k2l.begin() + (size_t)f * kMaxPulses);
+      dbg_k2bc[f] = (int)fl.starts.size();
+      std::copy(fl.starts.begin(), fl.starts.end(), dbg_k2bs.begin() + (size_t)f * kMaxPulses);
+      std::copy(fl.lengths.begin(), fl.lengths.end(), dbg_k2bl.begin() + (size_t)f * kMaxPulses);
+      std::copy(fl.types.begin(), fl.types.end(), dbg_k2bt.begin() + (size_t)f * kMaxPulses);
+    }
+  }
+  if (debug) {
+    dbg_vsync = cand;
+    dbg_offs.assign(offs.begin(), offs.end());
+    dbg_ll_coarse = h_ll;
+    dbg_meta = {T, P, spp};
+  }
+  cudaMemcpyAsync(d_ll, h_ll.data(), h_ll.size() * sizeof(double), cudaMemcpyHostToDevice, stream);
+  // ---- K4 hsync refinement, K5 luma
+  LineArgs la;
+  la.video = d_video;
+  la.sync = d_sync;
+  la.ll = d_ll;
+  la.fields = P;
+  la.total = (long long)P * spp;
+  la.lines_per_frame = LPF;
+  la.active_line_start = fmt.active_line_start;
+  la.thr_rel = thr_rel;
+  la.one_us = 1.0e-6 * fmt.fs_hz;
+  la.hsync_width = fmt.hsync_width;
+  la.right_edge_offset = 2.25 * ((fmt.fs_hz / 1.0e6) / 40.0);
+  la.luma = d_luma;
+  la.out_w = fmt.output_line_len;
+  la.out_h = fmt.output_field_lines;
+  la.luma_gain = (float)(fmt.output_scale / fmt.hz_ire);
+  la.luma_offset = (float)(-fmt.vsync_ire * fmt.output_scale + fmt.output_zero);
+  launch_hsync_refine(la, stream);
+  launch_luma(la, stream);
+  if (!check_cuda("lines")) return false;
+  // ---- K6 chroma
+  ChromaArgs ca;
+  ca.raw = d_raw;
+  ca.pre = d_dem;  // the raw demod is no longer needed
+  ca.fields = P;
+  ca.spp = spp;
+  ca.ctile = des.ctile;
+  ca.c_half = des.c_half;
+  ca.c_out = des.c_out;
+  ca.gc = d_gc;
+  ca.tw_c = d_twc;
+  ca.tw_line = d_twl;
+  ca.ll = d_ll;
+  ca.total = (long long)P * spp;
+  ca.track = d_track;
+  ca.het_scale = des.het_scale;
+  ca.fsc_bin = des.fsc_bin;
+  ca.bw_bins = des.bw_bins;
+  ca.burst_start = fmt.burst_start;
+  ca.out_w = fmt.output_line_len;
+  ca.out_h = fmt.output_field_lines;
+  ca.lines_per_frame = LPF;
+  ca.burst_abs_ref = (float)fmt.burst_abs_ref;
+  ca.chroma = d_chroma;
+  ca.burst = d_burst;
+  ca.metric = d_metric;
+  if (debug) {
+    dbg_demod.resize(std::min<size_t>((size_t)T * spp, (size_t)debug_tiles * spp));
+    cudaMemcpyAsync(dbg_demod.data(), d_dem, dbg_demod.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
+  }
+  launch_chroma_prefilter(ca, stream);
+  if (!check_cuda("chroma prefilter")) return false;
+  const int H = fmt.output_field_lines;
+  h_track.assign(P, 0);
+  int det_track, cycle_start;
+  double thr;
+  if (chroma_valid) {
+    det_track = chroma_track;
+    thr = chroma_threshold;
+    cycle_start = chroma_cycle_start;
+  } else {
+    // track and burst phase from field 0 (chroma_decode.cu:684-743)
+    std::vector<float> b0((size_t)H * kBurstLen);
+    double metric[2];
+    for (int t = 0; t < 2; t++) {
+      h_track[0] = t;
+      cudaMemcpyAsync(d_track, h_track.data(), sizeof(int), cudaMemcpyHostToDevice, stream);
+      launch_chroma_lines(ca, 0, 1, false, stream);
+      cudaMemcpyAsync(b0.data(), d_burst, b0.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
+      if (!sync("chroma track detect")) return false;
+      metric[t] = host_burst_metric(b0.data(), H);
+    }
+    det_track = (metric[1] < metric[0]) ? 1 : 0;
+    thr = metric[det_track] * 4.0;
+    h_track[0] = det_track;
+    cudaMemcpyAsync(d_track, h_track.data(), sizeof(int), cudaMemcpyHostToDevice, stream);
+    launch_chroma_lines(ca, 0, 1, false, stream);
+    cudaMemcpyAsync(b0.data(), d_burst, b0.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
+    if (!sync("chroma burst phase")) return false;
+    const double ph = host_burst_phase(b0.data(), H, fmt);
+    const int quadrant = ((int)(ph / 90.0 + 0.5)) % 4;
+    const int pid = phase_id_for(1, quadrant);
+    cycle_start = 0;
+    for (int i = 0; i < 8; i += 2)
+      if (kPhaseCycle[i] == pid) {
+        cycle_start = i;
+        break;
+      }
+  }
+  int cur = det_track;
+  h_phase.assign(P, 0);
+  for (int f = 0; f < P; f++) {
+    h_track[f] = (f & 1) ? (1 - cur) : cur;
+    h_phase[f] = kPhaseCycle[(cycle_start + f) % 8];
+  }
+  // chunks of 15 fields with track-flip retries (chroma_decode.cu:782-981)
+  const int fpc = std::max(1, std::min((4096 / H), P));
+  std::vector<double> metrics(P);
+  for (int f0 = 0; f0 < P; f0 += fpc) {
+    const int nf = std::min(fpc, P - f0);
+    int retries = 3;
+    bool ok = false;
+    while (!ok && retries-- > 0) {
+      cudaMemcpyAsync(d_track + f0, h_track.data() + f0, nf * sizeof(int), cudaMemcpyHostToDevice, stream);
+      launch_chroma_lines(ca, f0, nf, true, stream);
+      launch_burst_metric(ca, f0, nf, stream);
+      cudaMemcpyAsync(metrics.data() + f0, d_metric + f0, nf * sizeof(double), cudaMemcpyDeviceToHost, stream);
+      if (!sync("chroma lines")) return false;
+      int first_bad = INT_MAX;
+      for (int f = 0; f < nf; f++)
+        if (metrics[f0 + f] > thr) {
+          first_bad = f;
+          break;
+        }
+      if (first_bad == INT_MAX) {
+        ok = true;
+      } else {
+        cur = 1 - cur;
+        for (int ff = f0 + first_bad; ff < P; ff++) h_track[ff] = (ff & 1) ? (1 - cur) : cur;
+      }
+    }
+  }
+  chroma_valid = true;
+  chroma_track = (P & 1) ? (1 - cur) : cur;
+  chroma_threshold = thr;
+  chroma_cycle_start = (cycle_start + P) % 8;
+  // ---- K7 dropouts + concealment
+  DropoutArgs dd;
+  dd.env = d_env;
+  dd.env_part = d_env_part;
+  dd.env_blocks = env_blocks;
+  dd.ll = d_ll;
+  dd.fields = P;
+  dd.spp = spp;
+  dd.lines_per_frame = LPF;
+  dd.active_line_start = fmt.active_line_start;
+  dd.out_w = fmt.output_line_len;
+  dd.out_h = H;
+  dd.luma = d_luma;
+  dd.chroma = d_chroma;
+  dd.do_count = d_do_count;
+  dd.do_lines = d_do_lines;
+  dd.do_starts = d_do_starts;
+  dd.do_ends = d_do_ends;
+  launch_dropouts(dd, stream);
+  if (!check_cuda("dropouts")) return false;
+  // ---- small results back
+  h_do_count.resize(P);
+  cudaMemcpyAsync(h_do_count.data(), d_do_count, P * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  h_do_lines.resize((size_t)P * kMaxDropouts);
+  h_do_starts.resize((size_t)P * kMaxDropouts);
+  h_do_ends.resize((size_t)P * kMaxDropouts);
+  cudaMemcpyAsync(h_do_lines.data(), d_do_lines, h_do_lines.size() * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(h_do_starts.data(), d_do_starts, h_do_starts.size() * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(h_do_ends.data(), d_do_ends, h_do_ends.size() * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  if (debug) {
+    dbg_ll.resize(h_ll.size());
+    cudaMemcpyAsync(dbg_ll.data(), d_ll, h_ll.size() * sizeof(double), cudaMemcpyDeviceToHost, stream);
+    const size_t nt = std::min<size_t>((size_t)T * spp, (size_t)debug_tiles * spp);
+    dbg_video.resize(nt);
+    dbg_sync.resize(nt);
+    dbg_env.resize(nt);
+    dbg_pre.resize(std::min<size_t>((size_t)P * spp, nt));
+    cudaMemcpyAsync(dbg_video.data(), d_video, nt * sizeof(float), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(dbg_sync.data(), d_sync, nt * sizeof(float), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(dbg_env.data(), d_env, nt * sizeof(float), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(dbg_pre.data(), d_dem, dbg_pre.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
+  }
+  if (!sync("dropouts")) return false;
+  // ---- field metadata: parity alternation (pipeline.cu:2575-2610)
+  res.fields = P;
+  res.field_info.resize(P);
+  for (int i = 0; i < P; i++) {
+    cuvhs_field_info& fi = res.field_info[i];
+    fi.file_loc = raw_offset + offs[i];
+    bool first;
+    if (h_is_first[i] >= 0 && (h_is_first[i] == 1) != last_parity) first = (h_is_first[i] == 1);
+    else first = !last_parity;
+    last_parity = first;
+    fi.is_first_field = first ? 1 : 0;
+    fi.field_phase_id = h_phase[i] > 0 ? h_phase[i] : 0;
+    fi.dropout_count = std::max(0, std::min(h_do_count[i], kMaxDropouts));
+    fi.dropout_offset = 0;
+  }
+  if (debug) dbg_is_first = h_is_first;
+  return true;
+}
+
+}  // namespace cuvhs

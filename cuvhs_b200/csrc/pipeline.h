@@ -1,0 +1,86 @@
+// Decoder context: device buffers (allocated once), one CUDA stream, the
+// state carried from chunk to chunk, and host copies of the last chunk's
+// intermediates for inspection.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/cuvhs.h"
+#include "cuvhs_internal.h"
+
+namespace cuvhs {
+
+struct ChunkResult {
+  int fields = 0;
+  uint64_t next_raw_offset = 0;
+  std::vector<cuvhs_field_info> field_info;
+};
+
+struct Context {
+  cuvhs_config cfg{};
+  Format fmt;
+  Design des;
+  int device = -1;
+  int batch = 0;
+  int spp = 0;
+  int env_blocks = 0;
+  int edge_cap = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  cuvhs_status status = CUVHS_OK;
+  std::vector<void*> allocations;
+
+  uint8_t* d_raw = nullptr;
+  float *d_dem = nullptr, *d_env = nullptr, *d_video = nullptr, *d_sync = nullptr;
+  double* d_env_part = nullptr;
+  unsigned *d_fall = nullptr, *d_rise = nullptr;
+  int* d_counts = nullptr;
+  double* d_ll = nullptr;
+  uint16_t *d_luma = nullptr, *d_chroma = nullptr;
+  float* d_burst = nullptr;
+  double* d_metric = nullptr;
+  int* d_track = nullptr;
+  int *d_do_count = nullptr, *d_do_lines = nullptr, *d_do_starts = nullptr, *d_do_ends = nullptr;
+  float2 *d_ga = nullptr, *d_gb = nullptr, *d_twa = nullptr, *d_twb = nullptr, *d_twc = nullptr, *d_twl = nullptr;
+  float* d_gc = nullptr;
+
+  // carried state
+  LineLocState lls;
+  bool chroma_valid = false;
+  int chroma_track = 0;
+  double chroma_threshold = 0.0;
+  int chroma_cycle_start = 0;
+  bool last_parity = true;
+
+  // host scratch (kept to avoid reallocation)
+  std::vector<unsigned> h_fall, h_rise;
+  std::vector<long long> run_start, run_end;
+  std::vector<double> h_ll;
+  std::vector<int> h_is_first, h_track, h_phase;
+  std::vector<int> h_do_count, h_do_lines, h_do_starts, h_do_ends;
+
+  // last-chunk intermediates (debug)
+  bool debug = false;
+  int debug_tiles = 2;
+  std::vector<int> dbg_meta, dbg_vsync, dbg_k2c, dbg_k2s, dbg_k2l, dbg_k2bc, dbg_k2bs, dbg_k2bl, dbg_k2bt, dbg_is_first;
+  std::vector<long long> dbg_offs;
+  std::vector<double> dbg_ll_coarse, dbg_ll;
+  std::vector<float> dbg_demod, dbg_video, dbg_sync, dbg_env, dbg_pre;
+
+  ~Context();
+  bool init(const cuvhs_config& c);
+  void release();
+  void reset_state();
+  bool check_cuda(const char* where);
+  bool sync(const char* where);
+  bool decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avail, uint64_t raw_offset, int num_fields,
+                    ChunkResult& res);
+};
+
+// .tbc.json text (reference format, src/io/tbc_writer.cpp:89-175).
+std::string tbc_json(const Format& fmt, const cuvhs_field_info* fields, size_t n, const int32_t* dl,
+                     const int32_t* ds, const int32_t* de);
+
+}  // namespace cuvhs

@@ -1,0 +1,184 @@
+// Shared-memory FP32 complex FFT for one CTA (sm_100a).
+//
+// Stockham auto-sort, radix-16 passes (plus one radix-2/4/8 pass for sizes that
+// are not a power of 16).  Each thread holds its butterflies' inputs in
+// registers, so one padded buffer serves as both source and destination of a
+// pass (read all -> barrier -> write all -> barrier).  Index i lives at i + i/16
+// so the stride-16 writes of the first pass do not collide on banks.
+// Twiddles come from a table W_N^m, m in [0, N), computed in FP64 on the host
+// and rounded once to FP32.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace cuvhs {
+
+__host__ __device__ constexpr int fft_pad(int n) { return n + (n >> 4); }
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
+
+template <bool INV>
+__device__ __forceinline__ float2 cmul_tw(float2 a, float2 w) {
+  // a * w (forward) or a * conj(w) (inverse)
+  if (INV) return make_float2(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y);
+  return make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+}
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// multiply by -i (forward) / +i (inverse)
+template <bool INV>
+__device__ __forceinline__ float2 mul_mi(float2 a) {
+  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// e^{-+2 pi i m / 16} constants
+struct Root16 {
+  static constexpr float c[16] = {1.0f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f,
+                                  0.0f, -0.38268343236508977f, -0.70710678118654752f, -0.92387953251128674f,
+                                  -1.0f, -0.92387953251128674f, -0.70710678118654752f, -0.38268343236508977f,
+                                  0.0f, 0.38268343236508977f, 0.70710678118654752f, 0.92387953251128674f};
+  static constexpr float s[16] = {0.0f, 0.38268343236508977f, 0.70710678118654752f, 0.92387953251128674f,
+                                  1.0f, 0.92387953251128674f, 0.70710678118654752f, 0.38268343236508977f,
+                                  0.0f, -0.38268343236508977f, -0.70710678118654752f, -0.92387953251128674f,
+                                  -1.0f, -0.92387953251128674f, -0.70710678118654752f, -0.38268343236508977f};
+};
+
+// v * W_R^m with R | 16 (m in units of 1/R turn)
+template <int R, int M, bool INV>
+__device__ __forceinline__ float2 rot(float2 v) {
+  constexpr int m16 = (M * (16 / R)) & 15;
+  if (m16 == 0) return v;
+  if (m16 == 4) return mul_mi<INV>(v);
+  if (m16 == 8) return make_float2(-v.x, -v.y);
+  if (m16 == 12) return mul_mi<!INV>(v);
+  const float c = Root16::c[m16];
+  const float s = INV ? Root16::s[m16] : -Root16::s[m16];
+  return make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft2(float2& a, float2& b) {
+  float2 t = a;
+  a = cadd(t, b);
+  b = csub(t, b);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2& a3) {
+  float2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = mul_mi<INV>(csub(a1, a3));
+  a0 = cadd(t0, t2);
+  a2 = csub(t0, t2);
+  a1 = cadd(t1, t3);
+  a3 = csub(t1, t3);
+}
+
+// In-register DFT of size R in natural order.
+template <int R, bool INV>
+__device__ __forceinline__ void dft(float2* v) {
+  if constexpr (R == 2) {
+    dft2<INV>(v[0], v[1]);
+  } else if constexpr (R == 4) {
+    dft4<INV>(v[0], v[1], v[2], v[3]);
+  } else if constexpr (R == 8) {
+    // 8 = 4 (n1) x 2 (n2): x[2 n1 + n2]
+    dft4<INV>(v[0], v[2], v[4], v[6]);
+    dft4<INV>(v[1], v[3], v[5], v[7]);
+    v[3] = rot<8, 1, INV>(v[3]);
+    v[5] = rot<8, 2, INV>(v[5]);
+    v[7] = rot<8, 3, INV>(v[7]);
+    float2 o[8];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) {
+      float2 a = v[2 * k1], b = v[2 * k1 + 1];
+      o[k1] = cadd(a, b);
+      o[k1 + 4] = csub(a, b);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = o[i];
+  } else if constexpr (R == 16) {
+    // 16 = 4 (n1) x 4 (n2): x[4 n1 + n2]; A[n2][k1] in v[4 k1 + n2]
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) dft4<INV>(v[n2], v[4 + n2], v[8 + n2], v[12 + n2]);
+    v[4 + 1] = rot<16, 1, INV>(v[4 + 1]);
+    v[4 + 2] = rot<16, 2, INV>(v[4 + 2]);
+    v[4 + 3] = rot<16, 3, INV>(v[4 + 3]);
+    v[8 + 1] = rot<16, 2, INV>(v[8 + 1]);
+    v[8 + 2] = rot<16, 4, INV>(v[8 + 2]);
+    v[8 + 3] = rot<16, 6, INV>(v[8 + 3]);
+    v[12 + 1] = rot<16, 3, INV>(v[12 + 1]);
+    v[12 + 2] = rot<16, 6, INV>(v[12 + 2]);
+    v[12 + 3] = rot<16, 9, INV>(v[12 + 3]);
+    float2 o[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) {
+      float2 a0 = v[4 * k1], a1 = v[4 * k1 + 1], a2 = v[4 * k1 + 2], a3 = v[4 * k1 + 3];
+      dft4<INV>(a0, a1, a2, a3);
+      o[k1] = a0;
+      o[k1 + 4] = a1;
+      o[k1 + 8] = a2;
+      o[k1 + 12] = a3;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = o[i];
+  }
+}
+
+template <int THREADS>
+__device__ __forceinline__ void fft_sync() {
+  if constexpr (THREADS == 32) __syncwarp();
+  else __syncthreads();
+}
+
+// One Stockham pass of radix R on an N-point padded buffer, current span NS.
+template <int N, int THREADS, int R, int NS, bool INV>
+__device__ __forceinline__ void fft_pass(float2* s, const float2* __restrict__ tw) {
+  constexpr int NB = N / R;
+  constexpr int PER = (NB + THREADS - 1) / THREADS;
+  // A 32-thread transform belongs to one warp (several may share a CTA).
+  const int tid = (THREADS == 32) ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
+  float2 v[PER][R];
+#pragma unroll
+  for (int p = 0; p < PER; p++) {
+    const int j = tid + p * THREADS;
+    if ((NB % THREADS) == 0 || j < NB) {
+#pragma unroll
+      for (int r = 0; r < R; r++) v[p][r] = s[pidx(j + r * NB)];
+      if constexpr (NS > 1) {
+        const int k = j & (NS - 1);
+        constexpr int STEP = N / (NS * R);
+#pragma unroll
+        for (int r = 1; r < R; r++) v[p][r] = cmul_tw<INV>(v[p][r], __ldg(&tw[r * k * STEP]));
+      }
+      dft<R, INV>(v[p]);
+    }
+  }
+  fft_sync<THREADS>();
+#pragma unroll
+  for (int p = 0; p < PER; p++) {
+    const int j = tid + p * THREADS;
+    if ((NB % THREADS) == 0 || j < NB) {
+      const int k = j & (NS - 1);
+      const int base = (j / NS) * NS * R + k;
+#pragma unroll
+      for (int r = 0; r < R; r++) s[pidx(base + r * NS)] = v[p][r];
+    }
+  }
+  fft_sync<THREADS>();
+}
+
+// Full N-point transform (N a power of two, 64 <= N <= 65536), natural order
+// in and out, unnormalised.  Caller must synchronise (CTA, or warp for
+// THREADS == 32) after filling s.
+template <int N, int THREADS, bool INV, int NS = 1>
+__device__ __forceinline__ void smem_fft(float2* s, const float2* __restrict__ tw) {
+  if constexpr (NS * 16 <= N) {
+    fft_pass<N, THREADS, 16, NS, INV>(s, tw);
+    smem_fft<N, THREADS, INV, NS * 16>(s, tw);
+  } else if constexpr (NS < N) {
+    constexpr int R = N / NS;  // 2, 4 or 8
+    static_assert(R == 2 || R == 4 || R == 8, "N must be a power of two");
+    fft_pass<N, THREADS, R, NS, INV>(s, tw);
+  }
+}
+
+}  // namespace cuvhs

@@ -1,0 +1,28 @@
+"""Named synthetic workloads (seeded synthetic NTSC VHS RF captures).
+
+They stand in for real tape captures: the reference was developed on private
+captures, so every measurement and parity case here runs on seeded synthetic
+signals with the stated sizes and impairments.
+"""
+from ._lib import synth_capture
+
+WORKLOADS = {
+    # 6 fields at 28 MHz, clean (small parity case)
+    "small28": dict(sample_rate_hz=28e6, n_fields=6, seed=7, snr_db=40, jitter_bound=0.5),
+    # 8 fields at 28 MHz with 1% dropout lines, head switch, 36 dB
+    "dropouts28": dict(sample_rate_hz=28e6, n_fields=8, seed=11, snr_db=36, jitter_bound=1.0,
+                       dropout_line_rate=0.01, headswitch_min=3, headswitch_max=8),
+    # plain decode: 40 fields at 28 MHz, 40 dB, +/-0.5 sample jitter, no dropouts
+    "plain40_28": dict(sample_rate_hz=28e6, n_fields=40, seed=1001, snr_db=40, jitter_bound=0.5),
+    # harder signal: 600 fields at 40 MHz, 32 dB, +/-2 jitter, 0.1% dropouts, head switch 3-8
+    "hard600_40": dict(sample_rate_hz=40e6, n_fields=600, seed=2001, snr_db=32, jitter_bound=2.0,
+                       dropout_line_rate=0.001, headswitch_min=3, headswitch_max=8),
+    # 35.8 MHz rate coverage
+    "small358": dict(sample_rate_hz=35.8e6, n_fields=6, seed=31, snr_db=38, jitter_bound=1.0),
+}
+
+
+def make_workload(name, **overrides):
+    kw = dict(WORKLOADS[name])
+    kw.update(overrides)
+    return synth_capture(**kw)

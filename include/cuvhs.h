@@ -1,0 +1,137 @@
+/* libcuvhs: B200 (sm_100a) VHS RF decoder, C ABI.
+ *
+ * Drop-in for the decode path of hunterschuler/cuVHS: u8 NTSC VHS RF capture in,
+ * 910x263 u16 luma and chroma TBC fields plus .tbc.json field/line/dropout
+ * metadata out.  Every entry point returns a cuvhs_status; no C++ types or
+ * exceptions cross the boundary.  A context owns one CUDA stream and all of its
+ * device memory, allocated once in cuvhs_create.  Contexts are independent;
+ * one context is not safe to use from two threads at once.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   cuvhs_create / cuvhs_destroy      Pipeline::Pipeline + allocate_buffers +
+ *                                     FMDemodState::init (src/pipeline/pipeline.h:28-33,
+ *                                     src/pipeline/pipeline.cu:1383-1475,
+ *                                     src/pipeline/fm_demod.cu:273-374)
+ *   cuvhs_decode_chunk                Pipeline::process_chunk (src/pipeline/pipeline.cu:1525-2624)
+ *   cuvhs_decode_capture              Pipeline::run chunk loop (src/pipeline/pipeline.cu:2626-2713)
+ *   cuvhs_decode_file                 main + RawReader + TBCWriter (src/main.cpp:97-165,
+ *                                     src/io/raw_reader.cpp:128-151, src/io/tbc_writer.cpp:10-175)
+ *   cuvhs_json                        TBCWriter::write_json (src/io/tbc_writer.cpp:89-175)
+ *   cuvhs_debug_array                 the stage outputs the reference keeps in device
+ *                                     buffers (d_pulse_*, d_linelocs, d_is_first_field,
+ *                                     d_do_*; src/pipeline/pipeline.h:52-87)
+ */
+#ifndef CUVHS_H
+#define CUVHS_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUVHS_FIELD_WIDTH 910
+#define CUVHS_FIELD_HEIGHT 263
+#define CUVHS_MAX_DROPOUTS_PER_FIELD 512
+
+typedef enum cuvhs_status {
+  CUVHS_OK = 0,
+  CUVHS_ERR_INVALID_ARGUMENT = 1,
+  CUVHS_ERR_CUDA = 2,
+  CUVHS_ERR_OUT_OF_MEMORY = 3,
+  CUVHS_ERR_IO = 4,
+  CUVHS_ERR_CAPACITY = 5,    /* an internal fixed-size list overflowed */
+  CUVHS_ERR_UNSUPPORTED = 6, /* e.g. PAL, which this build does not decode */
+  CUVHS_ERR_EXISTS = 7       /* output exists and overwrite was not requested */
+} cuvhs_status;
+
+typedef struct cuvhs_ctx cuvhs_ctx;
+
+typedef struct cuvhs_config {
+  int system;             /* 0 = NTSC (--system NTSC) */
+  double sample_rate_mhz; /* -f, capture rate */
+  int device;             /* --gpu: CUDA device id, -1 = the one with most memory */
+  int batch_fields;       /* fields per chunk; 0 = derive from free device memory */
+  int stream_mode;        /* non-zero caps the chunk at 64 fields (pipe input) */
+} cuvhs_config;
+
+/* Per-field metadata, one .tbc.json "fields" entry. */
+typedef struct cuvhs_field_info {
+  uint64_t file_loc;      /* capture sample where the field's window starts */
+  int32_t is_first_field;
+  int32_t field_phase_id; /* 1..4, 0 = unset */
+  int32_t dropout_count;
+  int32_t dropout_offset; /* first entry in the dropout arrays */
+} cuvhs_field_info;
+
+/* Caller-owned host output buffers. */
+typedef struct cuvhs_output {
+  uint16_t* luma;          /* [max_fields][263][910] */
+  uint16_t* chroma;        /* [max_fields][263][910] */
+  cuvhs_field_info* fields; /* [max_fields] */
+  int32_t* dropout_line;   /* [max_dropouts] */
+  int32_t* dropout_startx;
+  int32_t* dropout_endx;
+  size_t max_fields;
+  size_t max_dropouts;
+  /* filled in by the decoder */
+  size_t fields_out;
+  size_t dropouts_out;
+  uint64_t next_raw_offset; /* chunk calls: where the next chunk starts */
+} cuvhs_output;
+
+void cuvhs_default_config(cuvhs_config* cfg);
+cuvhs_status cuvhs_create(const cuvhs_config* cfg, cuvhs_ctx** out);
+void cuvhs_destroy(cuvhs_ctx* ctx);
+const char* cuvhs_last_error(const cuvhs_ctx* ctx);
+const char* cuvhs_status_string(cuvhs_status s);
+
+int cuvhs_batch_fields(const cuvhs_ctx* ctx);
+size_t cuvhs_samples_per_field(const cuvhs_ctx* ctx); /* samples_per_line * 263 */
+size_t cuvhs_tile_stride(const cuvhs_ctx* ctx);       /* samples per chunk field slot (+20 lines) */
+/* Forget carried state (field parity, line-location and chroma track state). */
+void cuvhs_reset(cuvhs_ctx* ctx);
+
+/* One chunk of at most batch_fields fields starting at capture sample raw_offset.
+ * `samples` points at that sample in host memory, n_avail samples remain from
+ * there.  Appends to `out` (fields_out, dropouts_out grow) and sets
+ * out->next_raw_offset.  A chunk that yields no field leaves fields_out unchanged. */
+cuvhs_status cuvhs_decode_chunk(cuvhs_ctx* ctx, const uint8_t* samples, size_t n_avail, uint64_t raw_offset,
+                                int num_fields, cuvhs_output* out);
+
+/* The same chunk decode on samples already in device memory; the luma/chroma
+ * TBC and dropout results stay on the device (read them with
+ * cuvhs_device_outputs).  *fields_out = fields decoded. */
+cuvhs_status cuvhs_decode_chunk_device(cuvhs_ctx* ctx, const uint8_t* d_samples, size_t n_avail,
+                                       uint64_t raw_offset, int num_fields, int* fields_out,
+                                       uint64_t* next_raw_offset);
+/* Device pointers to the last chunk's luma and chroma fields. */
+cuvhs_status cuvhs_device_outputs(const cuvhs_ctx* ctx, const uint16_t** d_luma, const uint16_t** d_chroma);
+
+/* A whole capture in host memory, chunk by chunk as the reference's run loop. */
+cuvhs_status cuvhs_decode_capture(cuvhs_ctx* ctx, const uint8_t* samples, size_t n, cuvhs_output* out);
+
+/* .tbc.json text for `out`'s fields; returns the length (excluding NUL) and
+ * writes at most cap bytes including the NUL. */
+long long cuvhs_json(const cuvhs_ctx* ctx, const cuvhs_output* out, char* dst, long long cap);
+
+/* The CLI path: decode a u8 capture file (or "-" for stdin) to
+ * <out_base>.tbc, <out_base>_chroma.tbc and <out_base>.tbc.json. */
+cuvhs_status cuvhs_decode_file(const cuvhs_config* cfg, const char* in_path, const char* out_base,
+                               int overwrite);
+
+/* Keep host copies of the last chunk's intermediates (costs copies). */
+void cuvhs_set_debug(cuvhs_ctx* ctx, int on);
+/* Copy an intermediate of the last chunk into dst (cap elements; dst NULL
+ * queries the count).  int32: "meta"(raw_offset lo/hi words excluded: tiles,
+ * fields, spp), "vsync_candidates", "k2_pulse_count", "k2_pulse_starts",
+ * "k2_pulse_lengths", "k2b_pulse_count", "k2b_pulse_starts", "k2b_pulse_lengths",
+ * "k2b_pulse_types", "is_first", "do_count", "do_lines", "do_starts", "do_ends";
+ * int64: "field_offsets"; float64: "linelocs_coarse", "linelocs"; float32 (Hz
+ * relative to the 0 IRE carrier, or raw units): "demod", "video", "sync",
+ * "envelope", "chroma_prefilt".  Returns -1 for an unknown name. */
+long long cuvhs_debug_array(const cuvhs_ctx* ctx, const char* name, void* dst, long long cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 VHS decoder.
+
+Workload (one "step"): decode the plain 28 MHz capture -- 40 NTSC fields of
+seeded synthetic VHS SP RF (u8, 40 dB SNR, +/-0.5 sample timebase jitter, no
+dropouts; the reference's own captures are private, so a seeded synthetic
+signal with those properties stands in) -- through the same chunk loop the
+reference's Pipeline::run uses.
+
+  value      fields/s of the device-resident decode (u8 capture already in HBM,
+             luma/chroma TBC and metadata produced in HBM), L2 flushed between
+             steps with a 256 MiB write, CUDA events on the decoder's stream
+  e2e        the same metric through the C ABI from pinned host memory:
+             host->device copy of the capture and device->host copy of the luma
+             and chroma fields are inside every timed step
+  roofline   the dominant kernel's algorithmic bytes per launch / its average
+             event-timed launch duration, against the measured HBM copy peak
+  cpu_baseline  the FP64 oracle port on the host cores (bounded sample)
+
+--impl reference runs the reference decoder compiled from its own sources
+(oracle/_ref/ref_harness, its Pipeline chunk loop timed from after buffer
+allocation, as the reference times itself) on the same GPU.
+With torchrun and --gpus N every rank decodes its own replica (weak scaling);
+rank 0 reports total fields / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "NTSC fields/s at 28 MHz u8 and % of HBM roofline vs reference, at ≤1 LSB luma"
+WORKLOAD = "plain40_28"
+WORKLOAD_DESC = ("plain decode: 40 NTSC fields of seeded synthetic VHS SP RF at 28 MHz u8 "
+                 "(colour bars + moving luma ramp, 40 dB SNR, +/-0.5 sample jitter, no dropouts)")
+
+# Algorithmic HBM bytes per field of each stage: N samples per field
+# (fs / 59.94), F = 910 x 263 output pixels.
+def stage_bytes_per_field(stage, fs_hz):
+    N = fs_hz / 59.94
+    F = 910 * 263
+    return {
+        "k1a_demod": 9 * N,                # u8 in, FP32 demod + envelope out
+        "k1b_video_sync": 12 * N,          # FP32 demod in, FP32 video + sync out
+        "sync_edges": 4 * N,               # FP32 sync scan
+        "hsync_refine": 515 * 13e-6 * fs_hz * 4,
+        "luma_resample": 4 * N + 2 * F,
+        "chroma_prefilter": 5 * N,         # u8 in, FP32 out
+        "chroma_lines": 4 * N + 2 * F,
+        "burst_metric": 0.0,
+        "dropouts": 4 * N,
+    }[stage]
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from a committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{WORKLOAD}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, n in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def run_reference(args, rank):
+    """Reference arm: the reference's own decoder built from its sources."""
+    if rank != 0:
+        return 0
+    from cuvhs_b200 import make_workload, WORKLOADS
+    from oracle.oracle import REF_HARNESS
+    if not os.path.exists(REF_HARNESS):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built "
+                          "(the reference is built from its sources by __graft_entry__.build())"}))
+        return 0
+    mhz = WORKLOADS[WORKLOAD]["sample_rate_hz"] / 1e6
+    x = make_workload(WORKLOAD)
+    d = tempfile.mkdtemp(prefix="cuvhs_ref_", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    inp = os.path.join(d, "in.u8")
+    x.tofile(inp)
+    runs = []
+    for i in range(args.warmup + args.steps):
+        out = subprocess.run([REF_HARNESS, "-f", str(mhz), "--time", inp, os.path.join(d, "out")],
+                             capture_output=True, text=True)
+        if out.returncode != 0:
+            print(json.dumps({"impl": "reference", "unavailable": f"reference harness exited {out.returncode}"}))
+            return 0
+        runs.append(json.loads(out.stdout.strip().splitlines()[-1]))
+    timed = runs[args.warmup:]
+    fields = sum(r["fields"] for r in timed)
+    secs = sum(r["seconds"] for r in timed)
+    value = fields / secs
+    for fn in os.listdir(d):
+        os.unlink(os.path.join(d, fn))
+    os.rmdir(d)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "fields/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * secs / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC, "fields_per_step": timed[0]["fields"],
+                   "reference_batch_fields": timed[0]["batch_size"],
+                   "timing": "reference Pipeline chunk loop after buffer allocation (file in /dev/shm, "
+                             "TBC/JSON written to /dev/shm)"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "fields/s", "cores": 1, "kind": "reference",
+                         "sample": f"{WORKLOAD}, reference CUDA build on GPU 0, {args.steps} runs"},
+        "e2e": {"value": round(value, 3), "unit": "fields/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def cpu_baseline():
+    """FP64 oracle port on all host cores, bounded sample (6 fields)."""
+    try:
+        from oracle.oracle import Oracle
+        from cuvhs_b200 import make_workload
+        x = make_workload("small28")
+        cores = os.cpu_count() or 1
+        o = Oracle(28.0, threads=cores)
+        t = time.perf_counter()
+        n = o.decode(x)
+        dt = time.perf_counter() - t
+        return {"value": round(n / dt, 3), "unit": "fields/s", "cores": cores, "kind": "port",
+                "sample": f"{n} fields at 28 MHz (small28 synthetic capture), FP64 oracle, {dt:.1f} s"}
+    except Exception as e:  # the baseline is reported, never required
+        return {"value": None, "unit": "fields/s", "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    import cuvhs_b200 as cv
+    from cuvhs_b200._lib import Output, FieldInfo, lib
+    import ctypes
+
+    mhz = cv.WORKLOADS[WORKLOAD]["sample_rate_hz"] / 1e6
+    x = cv.make_workload(WORKLOAD)
+    n = x.size
+    dec = cv.Decoder(mhz, device=local, batch_fields=0)
+    spf = dec.samples_per_field
+    stream = torch.cuda.ExternalStream(dec.stream, device=local)
+    d_in = torch.from_numpy(x).to(f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+
+    def device_step():
+        raw = 0
+        fields = 0
+        while raw < n:
+            rem = (n - raw) // spf
+            if rem <= 0:
+                break
+            nf = min(dec.batch_fields, rem)
+            got, nxt = dec.decode_chunk_device(d_in.data_ptr() + raw, n - raw, raw, nf)
+            if got == 0:
+                break
+            fields += got
+            raw = nxt
+        return fields
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident decode
+    for _ in range(args.warmup):
+        device_step()
+    torch.cuda.synchronize()
+    dec.set_timing(True)
+    dec.reset_stage_times()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    total_fields = 0
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        for _ in range(args.steps):
+            flush.fill_(1)
+            total_fields += device_step()
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    stage = dec.stage_times()
+    launches = dec.launch_count
+    dec.set_timing(False)
+
+    # ---- end to end through the C ABI from pinned host memory
+    h_in = torch.from_numpy(x).pin_memory()
+    max_fields = n // spf + 2
+    F = 910 * 263
+    h_luma = torch.empty(max_fields * F, dtype=torch.int16).pin_memory()
+    h_chroma = torch.empty(max_fields * F, dtype=torch.int16).pin_memory()
+    finfo = (FieldInfo * max_fields)()
+    dl = np.empty(max_fields * 512, np.int32)
+    ds = np.empty_like(dl)
+    de = np.empty_like(dl)
+    out = Output()
+    out.luma = h_luma.data_ptr()
+    out.chroma = h_chroma.data_ptr()
+    out.fields = ctypes.addressof(finfo)
+    out.dropout_line, out.dropout_startx, out.dropout_endx = dl.ctypes.data, ds.ctypes.data, de.ctypes.data
+    out.max_fields = max_fields
+    out.max_dropouts = dl.size
+
+    def e2e_step():
+        out.fields_out = 0
+        out.dropouts_out = 0
+        st = lib.cuvhs_decode_capture(dec._h, h_in.data_ptr(), n, ctypes.byref(out))
+        if st != 0:
+            raise RuntimeError(lib.cuvhs_last_error(dec._h).decode())
+        return out.fields_out
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_fields = 0
+    for _ in range(args.steps):
+        e2e_fields += e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    barrier()
+    fields_per_step = total_fields // args.steps
+
+    # ---- reduce over ranks (max time)
+    t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max, e2e_max = float(t[0]), float(t[1])
+    value = total_fields * world / (ms_max / 1000.0)
+    e2e_value = e2e_fields * world / e2e_max
+
+    if rank == 0:
+        peak, peak_kind = read_peaks()
+        dom = max(stage, key=lambda k: stage[k][0])
+        dom_ms, dom_launches = stage[dom]
+        avg_launch_s = dom_ms / 1000.0 / max(1, dom_launches)
+        fields_per_launch = fields_per_step * args.steps / max(1, dom_launches)
+        alg_bytes = stage_bytes_per_field(dom, mhz * 1e6) * fields_per_launch
+        achieved = alg_bytes / avg_launch_s / 1e9
+        traffic = profiled_traffic(dom)
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "fields/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD_DESC, "fields_per_step": fields_per_step, "sample_rate_mhz": mhz,
+                       "batch_fields": dec.batch_fields, "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "e2e": {"value": round(e2e_value, 2), "unit": "fields/s", "h2d_bytes_per_step": int(n),
+                    "d2h_bytes_per_step": int(fields_per_step * F * 2 * 2)},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "traffic": traffic,
+                         "alg_bytes_per_launch": round(alg_bytes), "avg_launch_ms": round(avg_launch_s * 1e3, 4)},
+            "stages_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in stage.items()},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line))
+    dec.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

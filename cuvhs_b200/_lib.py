@@ -99,6 +99,17 @@ lib.cuvhs_decode_file.argtypes = [ctypes.POINTER(Config), ctypes.c_char_p, ctype
 lib.cuvhs_decode_file.restype = ctypes.c_int
 lib.cuvhs_debug_array.argtypes = [_vp, ctypes.c_char_p, _vp, ctypes.c_longlong]
 lib.cuvhs_debug_array.restype = ctypes.c_longlong
+lib.cuvhs_stream.argtypes = [_vp]
+lib.cuvhs_stream.restype = _vp
+lib.cuvhs_set_timing.argtypes = [_vp, ctypes.c_int]
+lib.cuvhs_stage_count.restype = ctypes.c_int
+lib.cuvhs_stage_name.argtypes = [ctypes.c_int]
+lib.cuvhs_stage_name.restype = ctypes.c_char_p
+lib.cuvhs_stage_times.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
+lib.cuvhs_stage_times.restype = ctypes.c_int
+lib.cuvhs_reset_stage_times.argtypes = [_vp]
+lib.cuvhs_launch_count.argtypes = [_vp]
+lib.cuvhs_launch_count.restype = ctypes.c_longlong
 lib.cuvhs_synth_default_params.argtypes = [ctypes.POINTER(SynthParams)]
 lib.cuvhs_synth_length.argtypes = [ctypes.POINTER(SynthParams)]
 lib.cuvhs_synth_length.restype = ctypes.c_longlong
@@ -110,7 +121,8 @@ EXPORTED = [
     "cuvhs_default_config", "cuvhs_create", "cuvhs_destroy", "cuvhs_last_error", "cuvhs_status_string",
     "cuvhs_batch_fields", "cuvhs_samples_per_field", "cuvhs_tile_stride", "cuvhs_reset", "cuvhs_decode_chunk",
     "cuvhs_decode_chunk_device", "cuvhs_device_outputs", "cuvhs_decode_capture", "cuvhs_json",
-    "cuvhs_decode_file", "cuvhs_set_debug", "cuvhs_debug_array", "cuvhs_synth_default_params",
+    "cuvhs_decode_file", "cuvhs_set_debug", "cuvhs_debug_array", "cuvhs_stream", "cuvhs_set_timing",
+    "cuvhs_stage_count", "cuvhs_stage_name", "cuvhs_stage_times", "cuvhs_reset_stage_times", "cuvhs_launch_count", "cuvhs_synth_default_params",
     "cuvhs_synth_length", "cuvhs_synth_ntsc",
 ]
 
@@ -264,6 +276,27 @@ class Decoder:
     _DTYPES = {"field_offsets": np.int64, "linelocs_coarse": np.float64, "linelocs": np.float64,
                "demod": np.float32, "video": np.float32, "sync": np.float32, "envelope": np.float32,
                "chroma_prefilt": np.float32}
+
+    @property
+    def stream(self) -> int:
+        return lib.cuvhs_stream(self._h) or 0
+
+    def set_timing(self, on=True):
+        lib.cuvhs_set_timing(self._h, 1 if on else 0)
+
+    def reset_stage_times(self):
+        lib.cuvhs_reset_stage_times(self._h)
+
+    def stage_times(self) -> dict:
+        n = lib.cuvhs_stage_count()
+        ms = (ctypes.c_double * n)()
+        la = (ctypes.c_longlong * n)()
+        lib.cuvhs_stage_times(self._h, ms, la, n)
+        return {lib.cuvhs_stage_name(i).decode(): (ms[i], la[i]) for i in range(n)}
+
+    @property
+    def launch_count(self) -> int:
+        return lib.cuvhs_launch_count(self._h)
 
     def debug_array(self, name: str) -> np.ndarray:
         n = lib.cuvhs_debug_array(self._h, name.encode(), None, 0)

@@ -188,6 +188,37 @@ long long cuvhs_json(const cuvhs_ctx* ctx, const cuvhs_output* out, char* dst, l
   return (long long)s.size();
 }
 
+void* cuvhs_stream(const cuvhs_ctx* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
+
+void cuvhs_set_timing(cuvhs_ctx* ctx, int on) {
+  if (ctx) ctx->c.timing = on != 0;
+}
+
+int cuvhs_stage_count(void) { return cuvhs::kNumStages; }
+
+const char* cuvhs_stage_name(int i) { return (i >= 0 && i < cuvhs::kNumStages) ? cuvhs::kStageNames[i] : ""; }
+
+int cuvhs_stage_times(const cuvhs_ctx* ctx, double* ms, long long* launches, int cap) {
+  if (!ctx) return 0;
+  const int n = std::min(cap, (int)cuvhs::kNumStages);
+  for (int i = 0; i < n; i++) {
+    if (ms) ms[i] = ctx->c.stage_ms[i];
+    if (launches) launches[i] = ctx->c.stage_launches[i];
+  }
+  return cuvhs::kNumStages;
+}
+
+void cuvhs_reset_stage_times(cuvhs_ctx* ctx) {
+  if (!ctx) return;
+  for (int i = 0; i < cuvhs::kNumStages; i++) {
+    ctx->c.stage_ms[i] = 0.0;
+    ctx->c.stage_launches[i] = 0;
+  }
+  ctx->c.launches = 0;
+}
+
+long long cuvhs_launch_count(const cuvhs_ctx* ctx) { return ctx ? ctx->c.launches : 0; }
+
 long long cuvhs_debug_array(const cuvhs_ctx* ctx, const char* name, void* dst, long long cap) {
   if (!ctx || !name) return -1;
   const Context& c = ctx->c;

@@ -58,10 +58,54 @@ int phase_id_for(int is_first, int quadrant) {
 
 }  // namespace
 
+const char* const kStageNames[kNumStages] = {"k1a_demod",      "k1b_video_sync", "sync_edges",
+                                             "hsync_refine",   "luma_resample",  "chroma_prefilter",
+                                             "chroma_lines",   "burst_metric",   "dropouts"};
+
 Context::~Context() { release(); }
+
+cudaEvent_t Context::next_event() {
+  if (pool_used == event_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    event_pool.push_back(e);
+  }
+  return event_pool[pool_used++];
+}
+
+void Context::begin_stage(int stage, cudaEvent_t& a) {
+  (void)stage;
+  a = nullptr;
+  if (!timing) return;
+  a = next_event();
+  cudaEventRecord(a, stream);
+}
+
+void Context::end_stage(int stage, cudaEvent_t a) {
+  stage_launches[stage]++;
+  launches++;
+  if (!timing || !a) return;
+  cudaEvent_t b = next_event();
+  cudaEventRecord(b, stream);
+  marks.push_back({stage, a, b});
+}
+
+// Called after a stream synchronisation: every recorded pair has completed.
+void Context::collect_stage_times() {
+  for (const Mark& m : marks) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, m.a, m.b) == cudaSuccess) stage_ms[m.stage] += ms;
+  }
+  marks.clear();
+  pool_used = 0;
+}
 
 void Context::release() {
   if (device >= 0) cudaSetDevice(device);
+  for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+  event_pool.clear();
+  marks.clear();
+  pool_used = 0;
   for (void* p : allocations) cudaFree(p);
   allocations.clear();
   if (stream) cudaStreamDestroy(stream);
@@ -200,6 +244,7 @@ bool Context::sync(const char* where) {
     status = CUVHS_ERR_CUDA;
     return false;
   }
+  collect_stage_times();
   return check_cuda(where);
 }
 
@@ -299,14 +344,29 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   da.env_blocks = env_blocks;
   da.video = d_video;
   da.sync = d_sync;
-  launch_k1a(da, stream);
-  launch_k1b(da, stream);
+  {
+    cudaEvent_t ev_;
+    begin_stage(kStageK1a, ev_);
+    launch_k1a(da, stream);
+    end_stage(kStageK1a, ev_);
+  }
+  {
+    cudaEvent_t ev_;
+    begin_stage(kStageK1b, ev_);
+    launch_k1b(da, stream);
+    end_stage(kStageK1b, ev_);
+  }
   if (!check_cuda("demod")) return false;
   // ---- sync edges over the demodulated range
   const float thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
   cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), stream);
   const long long total_chunk = (long long)T * spp;
-  launch_edges(d_sync, total_chunk, thr_rel, d_fall, d_rise, d_counts, edge_cap, stream);
+  {
+    cudaEvent_t ev_;
+    begin_stage(kStageEdges, ev_);
+    launch_edges(d_sync, total_chunk, thr_rel, d_fall, d_rise, d_counts, edge_cap, stream);
+    end_stage(kStageEdges, ev_);
+  }
   int counts[4] = {0, 0, 0, 0};
   cudaMemcpyAsync(counts, d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream);
   if (!sync("edges")) return false;
@@ -424,8 +484,18 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   la.out_h = fmt.output_field_lines;
   la.luma_gain = (float)(fmt.output_scale / fmt.hz_ire);
   la.luma_offset = (float)(-fmt.vsync_ire * fmt.output_scale + fmt.output_zero);
-  launch_hsync_refine(la, stream);
-  launch_luma(la, stream);
+  {
+    cudaEvent_t ev_;
+    begin_stage(kStageHsync, ev_);
+    launch_hsync_refine(la, stream);
+    end_stage(kStageHsync, ev_);
+  }
+  {
+    cudaEvent_t ev_;
+    begin_stage(kStageLuma, ev_);
+    launch_luma(la, stream);
+    end_stage(kStageLuma, ev_);
+  }
   if (!check_cuda("lines")) return false;
   // ---- K6 chroma
   ChromaArgs ca;
@@ -457,7 +527,12 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     dbg_demod.resize(std::min<size_t>((size_t)T * spp, (size_t)debug_tiles * spp));
     cudaMemcpyAsync(dbg_demod.data(), d_dem, dbg_demod.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
   }
-  launch_chroma_prefilter(ca, stream);
+  {
+    cudaEvent_t ev_;
+    begin_stage(kStageChromaPre, ev_);
+    launch_chroma_prefilter(ca, stream);
+    end_stage(kStageChromaPre, ev_);
+  }
   if (!check_cuda("chroma prefilter")) return false;
   const int H = fmt.output_field_lines;
   h_track.assign(P, 0);
@@ -474,7 +549,12 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     for (int t = 0; t < 2; t++) {
       h_track[0] = t;
       cudaMemcpyAsync(d_track, h_track.data(), sizeof(int), cudaMemcpyHostToDevice, stream);
-      launch_chroma_lines(ca, 0, 1, false, stream);
+      {
+        cudaEvent_t ev_;
+        begin_stage(kStageChromaLines, ev_);
+        launch_chroma_lines(ca, 0, 1, false, stream);
+        end_stage(kStageChromaLines, ev_);
+      }
       cudaMemcpyAsync(b0.data(), d_burst, b0.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
       if (!sync("chroma track detect")) return false;
       metric[t] = host_burst_metric(b0.data(), H);
@@ -483,7 +563,12 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     thr = metric[det_track] * 4.0;
     h_track[0] = det_track;
     cudaMemcpyAsync(d_track, h_track.data(), sizeof(int), cudaMemcpyHostToDevice, stream);
-    launch_chroma_lines(ca, 0, 1, false, stream);
+    {
+      cudaEvent_t ev_;
+      begin_stage(kStageChromaLines, ev_);
+      launch_chroma_lines(ca, 0, 1, false, stream);
+      end_stage(kStageChromaLines, ev_);
+    }
     cudaMemcpyAsync(b0.data(), d_burst, b0.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
     if (!sync("chroma burst phase")) return false;
     const double ph = host_burst_phase(b0.data(), H, fmt);
@@ -511,8 +596,15 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     bool ok = false;
     while (!ok && retries-- > 0) {
       cudaMemcpyAsync(d_track + f0, h_track.data() + f0, nf * sizeof(int), cudaMemcpyHostToDevice, stream);
-      launch_chroma_lines(ca, f0, nf, true, stream);
-      launch_burst_metric(ca, f0, nf, stream);
+      {
+        cudaEvent_t ev_;
+        begin_stage(kStageChromaLines, ev_);
+        launch_chroma_lines(ca, f0, nf, true, stream);
+        end_stage(kStageChromaLines, ev_);
+        begin_stage(kStageBurstMetric, ev_);
+        launch_burst_metric(ca, f0, nf, stream);
+        end_stage(kStageBurstMetric, ev_);
+      }
       cudaMemcpyAsync(metrics.data() + f0, d_metric + f0, nf * sizeof(double), cudaMemcpyDeviceToHost, stream);
       if (!sync("chroma lines")) return false;
       int first_bad = INT_MAX;
@@ -551,7 +643,12 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   dd.do_lines = d_do_lines;
   dd.do_starts = d_do_starts;
   dd.do_ends = d_do_ends;
-  launch_dropouts(dd, stream);
+  {
+    cudaEvent_t ev_;
+    begin_stage(kStageDropouts, ev_);
+    launch_dropouts(dd, stream);
+    end_stage(kStageDropouts, ev_);
+  }
   if (!check_cuda("dropouts")) return false;
   // ---- small results back
   h_do_count.resize(P);

@@ -18,6 +18,20 @@ struct ChunkResult {
   std::vector<cuvhs_field_info> field_info;
 };
 
+enum Stage {
+  kStageK1a = 0,
+  kStageK1b,
+  kStageEdges,
+  kStageHsync,
+  kStageLuma,
+  kStageChromaPre,
+  kStageChromaLines,
+  kStageBurstMetric,
+  kStageDropouts,
+  kNumStages
+};
+extern const char* const kStageNames[kNumStages];
+
 struct Context {
   cuvhs_config cfg{};
   Format fmt;
@@ -68,6 +82,23 @@ struct Context {
   std::vector<long long> dbg_offs;
   std::vector<double> dbg_ll_coarse, dbg_ll;
   std::vector<float> dbg_demod, dbg_video, dbg_sync, dbg_env, dbg_pre;
+
+  // per-stage device time (CUDA events on the decode stream) and launch count
+  bool timing = false;
+  double stage_ms[kNumStages] = {};
+  long long stage_launches[kNumStages] = {};
+  long long launches = 0;
+  struct Mark {
+    int stage;
+    cudaEvent_t a, b;
+  };
+  std::vector<Mark> marks;
+  std::vector<cudaEvent_t> event_pool;
+  size_t pool_used = 0;
+  cudaEvent_t next_event();
+  void begin_stage(int stage, cudaEvent_t& a);
+  void end_stage(int stage, cudaEvent_t a);
+  void collect_stage_times();
 
   ~Context();
   bool init(const cuvhs_config& c);

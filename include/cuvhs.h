@@ -119,6 +119,23 @@ long long cuvhs_json(const cuvhs_ctx* ctx, const cuvhs_output* out, char* dst, l
 cuvhs_status cuvhs_decode_file(const cuvhs_config* cfg, const char* in_path, const char* out_base,
                                int overwrite);
 
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events against the decoder. */
+void* cuvhs_stream(const cuvhs_ctx* ctx);
+
+/* Per-stage device time: with timing on, every kernel launch is bracketed by
+ * CUDA events on the decode stream and its duration accumulated per stage.
+ * cuvhs_stage_times fills up to cap entries (ms, launches) and returns the
+ * number of stages.  No counterpart in the reference, which has no
+ * per-stage timers. */
+void cuvhs_set_timing(cuvhs_ctx* ctx, int on);
+int cuvhs_stage_count(void);
+const char* cuvhs_stage_name(int i);
+int cuvhs_stage_times(const cuvhs_ctx* ctx, double* ms, long long* launches, int cap);
+void cuvhs_reset_stage_times(cuvhs_ctx* ctx);
+/* Kernel launches issued since the last cuvhs_reset_stage_times. */
+long long cuvhs_launch_count(const cuvhs_ctx* ctx);
+
 /* Keep host copies of the last chunk's intermediates (costs copies). */
 void cuvhs_set_debug(cuvhs_ctx* ctx, int on);
 /* Copy an intermediate of the last chunk into dst (cap elements; dst NULL

@@ -1,0 +1,117 @@
+#!/usr/bin/env python
+"""Golden fixtures from the reference decoder's own outputs.
+
+  run  OUTDIR [names]   on a GPU box with oracle/_ref/ref_harness built (the
+                        reference compiled from its sources by oracle/Makefile):
+                        synthesize each workload, run the reference's chunk loop
+                        through the harness and dump its intermediates and
+                        outputs to OUTDIR/<name>/
+  pack DUMPDIR NAME     pack one dump into tests/golden/NAME.npz (+ NAME.tbc.json)
+
+The fixtures pin the FP64 oracle (tests/test_oracle_golden.py) and the GPU
+decoder (tests/test_gpu_parity.py) to the reference's behaviour on the same
+seeded inputs.  The reference decodes its batch in one chunk; its batch size on
+a 180 GB B200 is recorded in the fixture.
+"""
+import hashlib
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+NAMES = ["small28", "dropouts28", "plain40_28"]
+FIELD = 910 * 263
+DTYPES = {"i32": np.int32, "i64": np.int64, "f32": np.float32, "f64": np.float64}
+
+
+def load_dump(d):
+    out = {}
+    for line in open(os.path.join(d, "manifest.txt")):
+        name, dt, _ = line.split()
+        out[name] = np.fromfile(os.path.join(d, name + ".bin"), DTYPES[dt])
+    return out
+
+
+def run(outdir, names):
+    import cuvhs_b200 as cv
+    from oracle.oracle import REF_HARNESS
+    for name in names:
+        x = cv.make_workload(name)
+        mhz = cv.WORKLOADS[name]["sample_rate_hz"] / 1e6
+        d = os.path.join(outdir, name)
+        os.makedirs(d, exist_ok=True)
+        inp = os.path.join(d, "in.u8")
+        x.tofile(inp)
+        with open(os.path.join(d, "input.md5"), "w") as f:
+            f.write(hashlib.md5(x.tobytes()).hexdigest())
+        subprocess.check_call([REF_HARNESS, "-f", str(mhz), "--dump", d, "--dump-tiles", "1", inp,
+                               os.path.join(d, "out")], stdout=open(os.path.join(d, "harness.json"), "w"),
+                              stderr=open(os.path.join(d, "harness.err"), "w"))
+        os.unlink(inp)
+
+
+def pack(dumpdir, name):
+    import cuvhs_b200 as cv
+    x = cv.make_workload(name)
+    ref = load_dump(dumpdir)
+    meta = ref["c0_meta"]
+    P = int(meta[1])
+    json_path = os.path.join(dumpdir, "out.tbc.json")
+    if not os.path.exists(json_path):
+        json_path = [os.path.join(dumpdir, f) for f in os.listdir(dumpdir) if f.endswith(".tbc.json")][0]
+    text = open(json_path).read()
+    with open(os.path.join(HERE, name + ".tbc.json"), "w") as f:
+        f.write(text)
+    arrs = {"input_md5": np.array(hashlib.md5(x.tobytes()).hexdigest()), "n_input": np.array(x.size),
+            "sample_rate_mhz": np.array(cv.WORKLOADS[name]["sample_rate_hz"] / 1e6), "meta": meta}
+    for key in ["field_offsets", "is_first", "do_count"]:
+        arrs[key] = ref["c0_" + key]
+    arrs["vsync_candidates"] = np.sort(ref["c0_vsync_candidates"])
+    for pre in ["k2", "k2b"]:
+        cnt = ref[f"c0_{pre}_pulse_count"]
+        arrs[f"{pre}_count"] = cnt
+        for part in (["starts", "lengths"] + (["types"] if pre == "k2b" else [])):
+            a = ref[f"c0_{pre}_pulse_{part}"].reshape(P, 800)
+            arrs[f"{pre}_{part}"] = np.concatenate([a[f, :min(800, cnt[f])] for f in range(P)])
+    dcnt = ref["c0_do_count"]
+    for part in ["lines", "starts", "ends"]:
+        a = ref[f"c0_do_{part}"].reshape(P, 512)
+        arrs[f"do_{part}"] = np.concatenate([a[f, :dcnt[f]] for f in range(P)])
+    arrs["linelocs_coarse"] = ref["c0_linelocs_coarse"].reshape(P, 525)
+    arrs["linelocs"] = ref["c0_linelocs"].reshape(P, 525)
+    arrs["chroma_state"] = ref["c0_chroma_state"]
+    arrs["k2b_state"] = ref["c0_k2b_state"]
+    # per-field digests of the TBC output and a sample of rows of field 0
+    tbc = {}
+    for suf, key in ((".tbc", "luma"), ("_chroma.tbc", "chroma")):
+        path = os.path.join(dumpdir, "out" + suf)
+        if os.path.exists(path):
+            a = np.fromfile(path, np.uint16).reshape(-1, 263, 910)
+        else:  # packed run: full first fields in fields_*.npy, digests in hash files
+            a = None
+        if a is not None:
+            arrs[f"{key}_md5"] = np.array([hashlib.md5(f.tobytes()).hexdigest() for f in a])
+            arrs[f"{key}_rows_f0"] = a[0, ::16]
+        else:
+            hs = [l.split()[1] for l in open(os.path.join(dumpdir, "hash" + suf + ".txt"))]
+            arrs[f"{key}_md5"] = np.array(hs)
+            fl = np.load(os.path.join(dumpdir, "fields" + suf.replace(".", "_") + ".npy")).reshape(-1, 263, 910)
+            arrs[f"{key}_rows_f0"] = fl[0, ::16]
+        tbc[key] = True
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrs)
+    print("packed", name, "fields", P)
+
+
+if __name__ == "__main__":
+    if len(sys.argv) >= 3 and sys.argv[1] == "run":
+        run(sys.argv[2], sys.argv[3].split(",") if len(sys.argv) > 3 else NAMES)
+    elif len(sys.argv) == 4 and sys.argv[1] == "pack":
+        pack(sys.argv[2], sys.argv[3])
+    else:
+        print(__doc__)
+        sys.exit(2)

@@ -1,0 +1,180 @@
+"""GPU decoder (through the C ABI) against the FP64 oracle and the reference.
+
+Bar: on every field whose analysis window lies inside the capture, field
+metadata (.tbc.json entries: file location, field order, phase ID, dropouts),
+sync pulses before and after validation and coarse line locations are
+bit-exact; refined line locations agree within 0.01 sample; luma and chroma
+agree within 1 LSB on at least 99.9% of samples."""
+import json
+
+import numpy as np
+import pytest
+
+import cuvhs_b200 as cv
+from conftest import GOLDEN, golden, inside_fields, json_fields, oracle_decode, workload
+
+LSB_FRACTION = 1e-3
+POS_TOL = 0.01
+
+
+def decode(name, batch_fields=0):
+    x = workload(name)
+    mhz = cv.WORKLOADS[name]["sample_rate_hz"] / 1e6
+    with cv.Decoder(mhz, batch_fields=batch_fields, debug=True) as d:
+        r = d.decode_capture(x)
+        dbg = {k: d.debug_array(k) for k in ("field_offsets", "k2_pulse_count", "k2_pulse_starts",
+                                             "k2_pulse_lengths", "k2b_pulse_count", "k2b_pulse_starts",
+                                             "k2b_pulse_lengths", "k2b_pulse_types", "linelocs_coarse",
+                                             "linelocs", "is_first")}
+    return x, mhz, r, dbg
+
+
+def assert_tbc_close(a, b, what):
+    d = np.abs(a.astype(np.int32) - b.astype(np.int32))
+    frac = float((d > 1).mean())
+    assert frac <= LSB_FRACTION, (what, frac, int(d.max()))
+    return frac, int(d.max())
+
+
+def compare_to_oracle(name, r, dbg, x, mhz, o, chunk_last_only=False):
+    assert r.n_fields == o.n_fields
+    ofields = json_fields(o.json)
+    mfields = json_fields(r.json)
+    assert [f["fileLoc"] for f in mfields] == [f["fileLoc"] for f in ofields]
+    inside = inside_fields([f["fileLoc"] for f in mfields], x.size, mhz)
+    assert len(inside) >= r.n_fields - 1
+    for i in inside:
+        assert mfields[i] == ofields[i], i
+    for i in inside:
+        assert_tbc_close(r.luma[i], o.luma[i], ("luma", i))
+        assert_tbc_close(r.chroma[i], o.chroma[i], ("chroma", i))
+    return inside
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["small28", "dropouts28", "plain40_28", "small358"])
+def test_decoder_matches_oracle(name):
+    x, mhz, r, dbg = decode(name)
+    o = oracle_decode(name)
+    inside = compare_to_oracle(name, r, dbg, x, mhz, o)
+    P = len(o.array(0, "field_offsets"))
+    assert o.n_chunks == 1
+    assert np.array_equal(dbg["field_offsets"], o.array(0, "field_offsets"))
+    for pre in ("k2", "k2b"):
+        cm, co = dbg[f"{pre}_pulse_count"], o.array(0, f"{pre}_pulse_count")
+        for part in ["starts", "lengths"] + (["types"] if pre == "k2b" else []):
+            a = dbg[f"{pre}_pulse_{part}"].reshape(P, 800)
+            b = o.array(0, f"{pre}_pulse_{part}").reshape(P, 800)
+            for f in inside:
+                assert cm[f] == co[f], (pre, f)
+                assert np.array_equal(a[f, :cm[f]], b[f, :co[f]]), (pre, part, f)
+    llc = dbg["linelocs_coarse"].reshape(P, 525)
+    ll = dbg["linelocs"].reshape(P, 525)
+    for f in inside:
+        assert np.array_equal(llc[f, :264], o.array(0, "linelocs_coarse").reshape(P, 525)[f, :264])
+        assert np.abs(ll[f, :264] - o.array(0, "linelocs").reshape(P, 525)[f, :264]).max() <= POS_TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["small28", "dropouts28", "plain40_28"])
+def test_decoder_matches_reference_fixture(name):
+    g = golden(name)
+    x, mhz, r, dbg = decode(name)
+    gfields = json_fields(g["json_text"])
+    mfields = json_fields(r.json)
+    assert len(mfields) == len(gfields)
+    inside = inside_fields([f["fileLoc"] for f in gfields], x.size, mhz)
+    for i in inside:
+        assert mfields[i] == gfields[i], i
+    assert np.array_equal(dbg["field_offsets"], g["field_offsets"])
+    P = len(g["field_offsets"])
+    off = np.concatenate([[0], np.cumsum(g["k2_count"])])
+    starts = dbg["k2_pulse_starts"].reshape(P, 800)
+    for f in inside:
+        assert np.array_equal(starts[f, :g["k2_count"][f]], g["k2_starts"][off[f]:off[f + 1]]), f
+        assert np.abs(dbg["linelocs"].reshape(P, 525)[f, :264] - g["linelocs"][f, :264]).max() <= POS_TOL
+    d = np.abs(r.luma[0, ::16].astype(np.int32) - g["luma_rows_f0"].astype(np.int32))
+    assert (d > 1).mean() <= LSB_FRACTION
+
+
+@pytest.mark.gpu
+def test_hard600_40_matches_reference_json():
+    """600 fields at 40 MHz, 32 dB, +/-2 jitter, 0.1% dropouts, head switch:
+    every field inside the capture has the reference's exact metadata."""
+    with open(f"{GOLDEN}/hard600_40.tbc.json") as f:
+        gtext = f.read()
+    x = workload("hard600_40")
+    with cv.Decoder(40.0) as d:
+        r = d.decode_capture(x)
+    gfields = json_fields(gtext)
+    mfields = json_fields(r.json)
+    assert len(mfields) == len(gfields) == 599
+    inside = inside_fields([f["fileLoc"] for f in gfields], x.size, 40.0)
+    assert len(inside) >= 598
+    bad = [i for i in inside if mfields[i] != gfields[i]]
+    assert not bad, (bad[:5], [mfields[i] for i in bad[:2]], [gfields[i] for i in bad[:2]])
+    assert sum(len(f["dropOuts"]["fieldLine"]) for f in mfields) >= 1
+
+
+@pytest.mark.gpu
+def test_multi_chunk_matches_oracle_with_same_chunking():
+    """Chunks of 8 fields: chunk restarts, carried line-location, chroma-track
+    and parity state must follow the reference's chunk loop."""
+    name = "plain40_28"
+    x, mhz, r, dbg = decode(name, batch_fields=8)
+    from oracle.oracle import Oracle
+    o = Oracle(mhz, batch_fields=8)
+    o.decode(x)
+    assert o.n_chunks > 3
+    compare_to_oracle(name, r, dbg, x, mhz, o)
+
+
+@pytest.mark.gpu
+def test_decode_is_deterministic_and_chunk_api_matches_capture_api():
+    x = workload("dropouts28")
+    with cv.Decoder(28.0) as d:
+        a = d.decode_capture(x)
+        d.reset()
+        b = d.decode_capture(x)
+        d.reset()
+        c, nxt = d.decode_chunk(x, 0, min(d.batch_fields, x.size // d.samples_per_field))
+    assert np.array_equal(a.luma, b.luma) and np.array_equal(a.chroma, b.chroma) and a.json == b.json
+    assert np.array_equal(a.luma[:c.n_fields], c.luma)
+    assert nxt > 0
+
+
+@pytest.mark.gpu
+def test_cli_end_to_end(tmp_path):
+    import subprocess
+    name = "plain40_28"
+    x = workload(name)
+    inp = tmp_path / "cap.u8"
+    x.tofile(inp)
+    base = tmp_path / "out"
+    p = subprocess.run([cv.CLI_PATH, "-f", "28", "--overwrite", str(inp), str(base)], capture_output=True,
+                       text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    assert "Done." in p.stderr
+    g = golden(name)
+    assert (tmp_path / "out.tbc.json").read_text() == g["json_text"]
+    luma = np.fromfile(tmp_path / "out.tbc", np.uint16).reshape(-1, 263, 910)
+    chroma = np.fromfile(tmp_path / "out_chroma.tbc", np.uint16).reshape(-1, 263, 910)
+    with cv.Decoder(28.0) as d:
+        r = d.decode_capture(x)
+    assert np.array_equal(luma, r.luma) and np.array_equal(chroma, r.chroma)
+    # a second run without --overwrite refuses
+    p2 = subprocess.run([cv.CLI_PATH, "-f", "28", str(inp), str(base)], capture_output=True, text=True, timeout=60)
+    assert p2.returncode == 1 and "Output exists" in p2.stderr
+
+
+@pytest.mark.gpu
+def test_short_and_empty_captures():
+    with cv.Decoder(28.0) as d:
+        r = d.decode_capture(np.full(1000, 128, np.uint8))
+        assert r.n_fields == 0
+        x = workload("small28")[: d.samples_per_field - 1]
+        assert d.decode_capture(x).n_fields == 0
+        # exactly one field of samples: one chunk, zero-filled to the tile stride
+        x1 = workload("small28")[: d.samples_per_field + 5000]
+        r1 = d.decode_capture(x1)
+        assert r1.n_fields <= 1

@@ -1,0 +1,106 @@
+"""Host-side checks that need no GPU: the C ABI exports, the synthesizer, the
+CLI's argument handling and its failure paths."""
+import ctypes
+import hashlib
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, has_gpu
+
+import cuvhs_b200 as cv
+
+
+def declared_functions():
+    names = []
+    for h in ("cuvhs.h", "cuvhs_synth.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"\b(cuvhs_[a-z0-9_]+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert len(names) >= 20
+    lib = ctypes.CDLL(cv.LIB_PATH)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(cv.EXPORTED) == names
+
+
+def test_synthesizer_is_seeded_and_thread_independent():
+    a = cv.make_workload("small28")
+    assert hashlib.md5(a.tobytes()).hexdigest() == "d0de38e166bc329e2c86f18cdce4e8b3"
+    b = cv.make_workload("small28", threads=1)
+    assert np.array_equal(a, b)
+    c = cv.make_workload("small28", seed=8)
+    assert not np.array_equal(a, c)
+
+
+def test_synthesizer_spectrum():
+    x = cv.make_workload("small28")[: 1 << 20].astype(np.float64) - 128
+    X = np.abs(np.fft.rfft(x * np.hanning(x.size))) ** 2
+    f = np.fft.rfftfreq(x.size, 1 / 28e6)
+    carrier = X[(f > 3.3e6) & (f < 4.5e6)].sum()
+    under = X[(f > 0.5e6) & (f < 0.8e6)].sum()
+    assert carrier > 20 * X[(f > 8e6)].sum()
+    assert under > 0.005 * carrier
+
+
+def run_cli(*args):
+    return subprocess.run([cv.CLI_PATH, *args], capture_output=True, text=True, timeout=60)
+
+
+def test_cli_usage_errors(tmp_path):
+    assert run_cli().returncode == 1
+    assert run_cli("--bogus", "a", "b").returncode == 1
+    r = run_cli("a", "b", "c")
+    assert r.returncode == 1 and "Too many arguments" in r.stderr
+    assert run_cli("--system", "SECAM", "a", "b").returncode == 1
+    assert run_cli("--format", "f32", "a", "b").returncode == 1
+    assert run_cli("-h").returncode == 0
+
+
+def test_cli_refuses_existing_outputs(tmp_path):
+    inp = tmp_path / "in.u8"
+    inp.write_bytes(bytes(1000))
+    base = tmp_path / "out"
+    (tmp_path / "out.tbc").write_bytes(b"")
+    r = run_cli("-f", "28", str(inp), str(base))
+    assert r.returncode == 1
+    assert "Output exists" in r.stderr
+
+
+def test_cli_rejects_unsupported_modes(tmp_path):
+    inp = tmp_path / "in.u16"
+    inp.write_bytes(bytes(1000))
+    assert run_cli("--overwrite", str(inp), str(tmp_path / "o")).returncode == 1
+    assert run_cli("--overwrite", "--system", "PAL", str(tmp_path / "x.u8"), str(tmp_path / "o")).returncode == 1
+
+
+def test_cli_missing_input_fails(tmp_path):
+    r = run_cli("--overwrite", str(tmp_path / "nope.u8"), str(tmp_path / "o"))
+    assert r.returncode == 1
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device error path")
+def test_create_without_device_reports_error():
+    with pytest.raises(cv.CuvhsError) as e:
+        cv.Decoder(28.0)
+    assert e.value.status == 2
+
+
+def test_invalid_config_rejected():
+    cfg = cv._lib.Config()
+    cv.lib.cuvhs_default_config(ctypes.byref(cfg))
+    cfg.system = 1  # PAL
+    h = ctypes.c_void_p()
+    assert cv.lib.cuvhs_create(ctypes.byref(cfg), ctypes.byref(h)) == 6
+    cfg.system = 0
+    cfg.sample_rate_mhz = 1.0
+    assert cv.lib.cuvhs_create(ctypes.byref(cfg), ctypes.byref(h)) == 1
+    assert cv.lib.cuvhs_create(None, ctypes.byref(h)) == 1

@@ -1,0 +1,51 @@
+"""The FP64 oracle against the reference decoder's own B200 outputs.
+
+Fixtures (tests/golden/, made by tests/golden/make_golden.py from the
+reference compiled from its sources) hold the reference's .tbc.json, per-field
+digests of its luma/chroma TBC, its sync pulses before and after validation,
+line locations, field parity and dropouts for seeded synthetic captures."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import golden, inside_fields, json_fields, oracle_decode, workload
+
+CASES = ["small28", "dropouts28", "plain40_28"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_matches_reference(name):
+    g = golden(name)
+    x = workload(name)
+    assert hashlib.md5(x.tobytes()).hexdigest() == str(g["input_md5"])
+    o = oracle_decode(name)
+    mhz = float(g["sample_rate_mhz"])
+    # identical .tbc.json text: fields, parity, phase IDs, file locations, dropouts
+    assert o.json == g["json_text"]
+    locs = [f["fileLoc"] for f in json_fields(g["json_text"])]
+    inside = inside_fields(locs, x.size, mhz)
+    assert len(inside) >= len(locs) - 1
+    # luma and chroma bit-identical on every field inside the capture
+    for i in inside:
+        assert hashlib.md5(o.luma[i].tobytes()).hexdigest() == str(g["luma_md5"][i]), i
+        assert hashlib.md5(o.chroma[i].tobytes()).hexdigest() == str(g["chroma_md5"][i]), i
+    assert np.array_equal(o.luma[0, ::16], g["luma_rows_f0"])
+    # integer intermediates
+    assert np.array_equal(o.array(0, "field_offsets"), g["field_offsets"])
+    assert np.array_equal(o.array(0, "is_first"), g["is_first"])
+    assert np.array_equal(o.array(0, "do_count"), g["do_count"])
+    P = len(g["field_offsets"])
+    for pre in ("k2", "k2b"):
+        cnt = o.array(0, f"{pre}_pulse_count")
+        off = np.concatenate([[0], np.cumsum(g[f"{pre}_count"])])
+        for f in inside:
+            assert cnt[f] == g[f"{pre}_count"][f], (pre, f)
+            for part in ["starts", "lengths"] + (["types"] if pre == "k2b" else []):
+                mine = o.array(0, f"{pre}_pulse_{part}").reshape(P, 800)[f, :cnt[f]]
+                assert np.array_equal(mine, g[f"{pre}_{part}"][off[f]:off[f + 1]]), (pre, part, f)
+    ll = o.array(0, "linelocs").reshape(P, 525)
+    llc = o.array(0, "linelocs_coarse").reshape(P, 525)
+    for f in inside:
+        assert np.array_equal(llc[f, :264], g["linelocs_coarse"][f, :264])
+        assert np.abs(ll[f, :264] - g["linelocs"][f, :264]).max() < 1e-6

@@ -110,6 +110,8 @@ lib.cuvhs_stage_times.restype = ctypes.c_int
 lib.cuvhs_reset_stage_times.argtypes = [_vp]
 lib.cuvhs_launch_count.argtypes = [_vp]
 lib.cuvhs_launch_count.restype = ctypes.c_longlong
+lib.cuvhs_dropouts_noalloc.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+lib.cuvhs_dropouts_noalloc.restype = ctypes.c_int
 lib.cuvhs_synth_default_params.argtypes = [ctypes.POINTER(SynthParams)]
 lib.cuvhs_synth_length.argtypes = [ctypes.POINTER(SynthParams)]
 lib.cuvhs_synth_length.restype = ctypes.c_longlong
@@ -122,7 +124,7 @@ EXPORTED = [
     "cuvhs_batch_fields", "cuvhs_samples_per_field", "cuvhs_tile_stride", "cuvhs_reset", "cuvhs_decode_chunk",
     "cuvhs_decode_chunk_device", "cuvhs_device_outputs", "cuvhs_decode_capture", "cuvhs_json",
     "cuvhs_decode_file", "cuvhs_set_debug", "cuvhs_debug_array", "cuvhs_stream", "cuvhs_set_timing",
-    "cuvhs_stage_count", "cuvhs_stage_name", "cuvhs_stage_times", "cuvhs_reset_stage_times", "cuvhs_launch_count", "cuvhs_synth_default_params",
+    "cuvhs_stage_count", "cuvhs_stage_name", "cuvhs_stage_times", "cuvhs_reset_stage_times", "cuvhs_launch_count", "cuvhs_dropouts_noalloc", "cuvhs_synth_default_params",
     "cuvhs_synth_length", "cuvhs_synth_ntsc",
 ]
 

@@ -148,6 +148,31 @@ void cuvhs_set_debug(cuvhs_ctx* ctx, int on);
  * "envelope", "chroma_prefilt".  Returns -1 for an unknown name. */
 long long cuvhs_debug_array(const cuvhs_ctx* ctx, const char* name, void* dst, long long cap);
 
+/* Dropout detection and concealment on caller-owned device buffers, allocating
+ * no device memory.  No counterpart in the reference (its dropout stage
+ * allocates a temporary on every call).  For callers that cannot call
+ * cudaMalloc: code running while its stream is captured into a CUDA graph,
+ * real-time capture loops that must not block in the allocator, and hosts
+ * whose device memory belongs to another allocator.
+ *   d_envelope  [fields * tile_stride] f32 RF envelope; field f's slot starts
+ *               at f * tile_stride (the decoder's layout, see cuvhs_tile_stride)
+ *   d_linelocs  [fields * 525] f64 line starts in the same sample units
+ *   d_luma, d_chroma  [fields][263][910] u16 TBC fields, concealed in place
+ *   d_count [fields], d_lines/d_startx/d_endx [fields * 512]  outputs
+ *   stream      a cudaStream_t (NULL = default stream); the call is asynchronous
+ * The only scratch is a fixed device array of CUVHS_NOALLOC_MAX_PARTIALS
+ * doubles (256 KiB, one per envelope block of 4096 samples), shared by all
+ * calls on a device and held by every GPU that loads the library until the
+ * process exits: calls that overlap on the GPU race on it.  Sizes needing more
+ * partial sums (fields * ceil(tile_stride / 4096) > the maximum: about 266
+ * fields at 28 MHz, 186 at 40 MHz) return CUVHS_ERR_CAPACITY.  The first call
+ * on each device looks up the array's device address; make that first call
+ * before any stream capture. */
+#define CUVHS_NOALLOC_MAX_PARTIALS 32768
+cuvhs_status cuvhs_dropouts_noalloc(const float* d_envelope, const double* d_linelocs, int fields, int tile_stride,
+                                    uint16_t* d_luma, uint16_t* d_chroma, int32_t* d_count, int32_t* d_lines,
+                                    int32_t* d_startx, int32_t* d_endx, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -86,19 +86,22 @@ def profiled_traffic(kernel):
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
 
-    def __init__(self, index):
+    def __init__(self, index, interval_ms=200):
         self.index = index
+        self.interval_ms = interval_ms
         self.proc = None
         self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
 
     def start(self):
+        if self.interval_ms <= 0:
+            return
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -195,6 +198,21 @@ def cpu_baseline():
         return {"value": None, "unit": "fields/s", "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
 
 
+def profile_case():
+    """A single decode of the workload (small device footprint) for ncu."""
+    import torch
+    import cuvhs_b200 as cv
+    x = cv.make_workload(WORKLOAD)
+    mhz = cv.WORKLOADS[WORKLOAD]["sample_rate_hz"] / 1e6
+    with cv.Decoder(mhz, batch_fields=48) as d:
+        din = torch.from_numpy(x).cuda()
+        torch.cuda.synchronize()
+        got, _ = d.decode_chunk_device(din.data_ptr(), x.size, 0, min(48, x.size // d.samples_per_field))
+        torch.cuda.synchronize()
+    print(f"profile case: {got} fields")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -202,8 +220,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--clock-interval-ms", type=int, default=200,
+                    help="nvidia-smi sampling period during the timed region (0 = off)")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="one device-resident decode of the workload with a 48-field allocation, "
+                         "for kernel profilers; prints nothing else")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.profile_case:
+        return profile_case()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -257,7 +282,7 @@ def main():
     torch.cuda.synchronize()
     dec.set_timing(True)
     dec.reset_stage_times()
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(local, args.clock_interval_ms)
     clocks.start()
     barrier()
     torch.cuda.synchronize()
@@ -327,7 +352,8 @@ def main():
 
     if rank == 0:
         peak, peak_kind = read_peaks()
-        dom = max(stage, key=lambda k: stage[k][0])
+        kernels = {k: v for k, v in stage.items() if not k.startswith("host_")}
+        dom = max(kernels, key=lambda k: kernels[k][0])
         dom_ms, dom_launches = stage[dom]
         avg_launch_s = dom_ms / 1000.0 / max(1, dom_launches)
         fields_per_launch = fields_per_step * args.steps / max(1, dom_launches)

@@ -52,9 +52,9 @@ cuvhs_status append_chunk(Context& c, const ChunkResult& r, cuvhs_output* out) {
     fi.dropout_offset = (int32_t)out->dropouts_out;
     for (int d = 0; d < fi.dropout_count; d++) {
       const size_t k = (size_t)i * cuvhs::kMaxDropouts + d;
-      if (out->dropout_line) out->dropout_line[out->dropouts_out] = c.h_do_lines[k];
-      if (out->dropout_startx) out->dropout_startx[out->dropouts_out] = c.h_do_starts[k];
-      if (out->dropout_endx) out->dropout_endx[out->dropouts_out] = c.h_do_ends[k];
+      if (out->dropout_line) out->dropout_line[out->dropouts_out] = c.hp_do_lines[k];
+      if (out->dropout_startx) out->dropout_startx[out->dropouts_out] = c.hp_do_starts[k];
+      if (out->dropout_endx) out->dropout_endx[out->dropouts_out] = c.hp_do_ends[k];
       out->dropouts_out++;
     }
     if (out->fields) out->fields[out->fields_out] = fi;
@@ -68,6 +68,12 @@ template <typename T>
 long long copy_out(const std::vector<T>& v, void* dst, long long cap) {
   if (dst && cap > 0) std::memcpy(dst, v.data(), sizeof(T) * (size_t)std::min<long long>(cap, (long long)v.size()));
   return (long long)v.size();
+}
+
+template <typename T>
+long long copy_ptr(const T* p, size_t n, void* dst, long long cap) {
+  if (dst && cap > 0 && p) std::memcpy(dst, p, sizeof(T) * (size_t)std::min<long long>(cap, (long long)n));
+  return (long long)n;
 }
 
 }  // namespace
@@ -234,10 +240,11 @@ long long cuvhs_debug_array(const cuvhs_ctx* ctx, const char* name, void* dst, l
   if (s == "k2b_pulse_lengths") return copy_out(c.dbg_k2bl, dst, cap);
   if (s == "k2b_pulse_types") return copy_out(c.dbg_k2bt, dst, cap);
   if (s == "is_first") return copy_out(c.dbg_is_first, dst, cap);
-  if (s == "do_count") return copy_out(c.h_do_count, dst, cap);
-  if (s == "do_lines") return copy_out(c.h_do_lines, dst, cap);
-  if (s == "do_starts") return copy_out(c.h_do_starts, dst, cap);
-  if (s == "do_ends") return copy_out(c.h_do_ends, dst, cap);
+  const size_t P = (size_t)c.last_fields;
+  if (s == "do_count") return copy_ptr(c.hp_do_count, P, dst, cap);
+  if (s == "do_lines") return copy_ptr(c.hp_do_lines, P * cuvhs::kMaxDropouts, dst, cap);
+  if (s == "do_starts") return copy_ptr(c.hp_do_starts, P * cuvhs::kMaxDropouts, dst, cap);
+  if (s == "do_ends") return copy_ptr(c.hp_do_ends, P * cuvhs::kMaxDropouts, dst, cap);
   if (s == "linelocs_coarse") return copy_out(c.dbg_ll_coarse, dst, cap);
   if (s == "linelocs") return copy_out(c.dbg_ll, dst, cap);
   if (s == "demod") return copy_out(c.dbg_demod, dst, cap);

@@ -103,10 +103,12 @@ struct DemodArgs {
 void launch_k1a(const DemodArgs& a, cudaStream_t st);
 void launch_k1b(const DemodArgs& a, cudaStream_t st);
 
-// Threshold edges of the sync signal: falling (x<=thr, prev>thr or start) and
-// rising (x>thr, prev<=thr).  Unordered; the host sorts.
+// Threshold edges of the sync signal in sample order: falling (x<=thr after
+// x>thr, or at 0) and rising (x>thr after x<=thr).  counts[0..1] = totals;
+// blk is scratch of edge_blocks(total) entries.
+int edge_blocks(long long total);
 void launch_edges(const float* sync, long long total, float thr_rel, unsigned* fall, unsigned* rise,
-                  int* counts, int cap, cudaStream_t st);
+                  int* counts, int cap, int2* blk, cudaStream_t st);
 
 struct LineArgs {
   const float* video;

@@ -116,11 +116,17 @@ double place_kernel(const std::vector<cd>& k, int neg, int pos, int N, std::vect
   return total > 0 ? std::max(0.0, total - kept) / total : 0.0;
 }
 
+// Per-pass twiddles of the shared-memory FFT (smem_fft.cuh): pass NS >= 16 of
+// radix R holds W_{NS*R}^{r*k} at (NS - 16) + (r - 1) * NS + k.
 std::vector<float2> twiddles(int n) {
-  std::vector<float2> t(n);
-  for (int m = 0; m < n; m++) {
-    const double a = -2.0 * kPi * (double)m / (double)n;
-    t[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+  std::vector<float2> t;
+  for (int ns = 16; ns < n; ns *= 16) {
+    const int R = ns * 16 <= n ? 16 : n / ns;
+    for (int r = 1; r < R; r++)
+      for (int k = 0; k < ns; k++) {
+        const double a = -2.0 * kPi * (double)r * (double)k / (double)(ns * R);
+        t.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+      }
   }
   return t;
 }
@@ -208,7 +214,7 @@ void Design::build(const Format& fmt) {
     std::vector<cd> hv = host_dft(FV, +1), hs = host_dft(FS, +1);
     std::vector<cd> c(tile);
     for (int n = 0; n < tile; n++) c[n] = cd(hv[n].real(), hs[n].real());
-    b_neg = b_pos = 1536;
+    b_neg = b_pos = 1024;
     b_out = kNb - b_neg - b_pos;
     std::vector<cd> blk;
     b_tail = place_kernel(c, b_neg, b_pos, kNb, blk);

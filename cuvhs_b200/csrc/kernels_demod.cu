@@ -111,37 +111,136 @@ __global__ void __launch_bounds__(kThreadsB) k1b_kernel(DemodArgs a) {
   }
 }
 
-// Threshold edges.  Positions are chunk-relative sample indices.
-__global__ void edges_kernel(const float* __restrict__ x, long long total, float thr, unsigned* __restrict__ fall,
-                             unsigned* __restrict__ rise, int* __restrict__ counts, int cap) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  bool f_edge = false, r_edge = false;
-  if (i < total) {
-    const float v = __ldg(&x[i]);
-    const bool in = v <= thr;
-    const bool prev_in = i > 0 ? (__ldg(&x[i - 1]) <= thr) : false;
-    f_edge = in && (i == 0 || !prev_in);
-    r_edge = !in && i > 0 && prev_in;
+// Threshold edges in sample order.  Each thread owns 16 consecutive samples
+// (one 64-byte line), a CTA 4096; counts per CTA, one scan, then an ordered
+// write, so the host receives sorted falling and rising edge positions.
+constexpr int kEdgeThreads = 256;
+constexpr int kEdgePer = 16;
+constexpr int kEdgeSeg = kEdgeThreads * kEdgePer;
+
+__device__ __forceinline__ void edge_masks(const float* __restrict__ x, long long total, float thr, long long i0,
+                                           unsigned& fm, unsigned& rm) {
+  fm = 0;
+  rm = 0;
+  if (i0 >= total) return;
+  float v[kEdgePer];
+  if (i0 + kEdgePer <= total) {
+    const float4* p = reinterpret_cast<const float4*>(x + i0);
+#pragma unroll
+    for (int q = 0; q < kEdgePer / 4; q++) {
+      const float4 t = __ldg(p + q);
+      v[4 * q] = t.x;
+      v[4 * q + 1] = t.y;
+      v[4 * q + 2] = t.z;
+      v[4 * q + 3] = t.w;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < kEdgePer; j++) v[j] = (i0 + j < total) ? __ldg(&x[i0 + j]) : 0.0f;
   }
-  // warp-aggregated appends
-  const unsigned mf = __ballot_sync(0xffffffffu, f_edge);
-  const unsigned mr = __ballot_sync(0xffffffffu, r_edge);
-  const int lane = threadIdx.x & 31;
-  int bf = 0, br = 0;
-  if (lane == 0) {
-    if (mf) bf = atomicAdd(&counts[0], __popc(mf));
-    if (mr) br = atomicAdd(&counts[1], __popc(mr));
+  bool prev_in = i0 > 0 ? (__ldg(&x[i0 - 1]) <= thr) : false;
+#pragma unroll
+  for (int j = 0; j < kEdgePer; j++) {
+    if (i0 + j >= total) break;
+    const bool in = v[j] <= thr;
+    if (in && (i0 + j == 0 || !prev_in)) fm |= 1u << j;
+    if (!in && i0 + j > 0 && prev_in) rm |= 1u << j;
+    prev_in = in;
   }
-  bf = __shfl_sync(0xffffffffu, bf, 0);
-  br = __shfl_sync(0xffffffffu, br, 0);
-  const unsigned below = (1u << lane) - 1u;
-  if (f_edge) {
-    const int k = bf + __popc(mf & below);
-    if (k < cap) fall[k] = (unsigned)i;
+}
+
+// Block-wide exclusive scan of two counters; returns the block totals.
+__device__ __forceinline__ int2 block_scan2(int a, int b, int& pa, int& pb) {
+  __shared__ int2 warp_tot[kEdgeThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int sa = a, sb = b;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int ta = __shfl_up_sync(0xffffffffu, sa, off), tb = __shfl_up_sync(0xffffffffu, sb, off);
+    if (lane >= off) {
+      sa += ta;
+      sb += tb;
+    }
   }
-  if (r_edge) {
-    const int k = br + __popc(mr & below);
-    if (k < cap) rise[k] = (unsigned)i;
+  if (lane == 31) warp_tot[warp] = make_int2(sa, sb);
+  __syncthreads();
+  int ba = 0, bb = 0, ta = 0, tb = 0;
+  for (int w = 0; w < kEdgeThreads / 32; w++) {
+    if (w < warp) {
+      ba += warp_tot[w].x;
+      bb += warp_tot[w].y;
+    }
+    ta += warp_tot[w].x;
+    tb += warp_tot[w].y;
+  }
+  pa = ba + sa - a;
+  pb = bb + sb - b;
+  return make_int2(ta, tb);
+}
+
+__global__ void __launch_bounds__(kEdgeThreads) edge_count_kernel(const float* __restrict__ x, long long total,
+                                                                  float thr, int2* __restrict__ blk) {
+  const long long i0 = (long long)blockIdx.x * kEdgeSeg + (long long)threadIdx.x * kEdgePer;
+  unsigned fm, rm;
+  edge_masks(x, total, thr, i0, fm, rm);
+  int pa, pb;
+  const int2 t = block_scan2(__popc(fm), __popc(rm), pa, pb);
+  if (threadIdx.x == 0) blk[blockIdx.x] = t;
+}
+
+// One CTA: exclusive scan of the per-CTA counts, totals to counts[0..1].
+__global__ void __launch_bounds__(1024) edge_scan_kernel(int2* __restrict__ blk, int nblk, int* __restrict__ counts) {
+  __shared__ int2 part[1024];
+  __shared__ int2 carry;
+  if (threadIdx.x == 0) carry = make_int2(0, 0);
+  __syncthreads();
+  for (int base = 0; base < nblk; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int2 v = i < nblk ? blk[i] : make_int2(0, 0);
+    part[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+      int2 t = make_int2(0, 0);
+      if (threadIdx.x >= off) t = part[threadIdx.x - off];
+      __syncthreads();
+      part[threadIdx.x].x += t.x;
+      part[threadIdx.x].y += t.y;
+      __syncthreads();
+    }
+    const int2 inc = part[threadIdx.x];
+    const int2 c = carry;
+    if (i < nblk) blk[i] = make_int2(c.x + inc.x - v.x, c.y + inc.y - v.y);
+    __syncthreads();
+    if (threadIdx.x == 1023) carry = make_int2(c.x + inc.x, c.y + inc.y);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    counts[0] = carry.x;
+    counts[1] = carry.y;
+  }
+}
+
+__global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(const float* __restrict__ x, long long total,
+                                                                  float thr, const int2* __restrict__ blk,
+                                                                  unsigned* __restrict__ fall,
+                                                                  unsigned* __restrict__ rise, int cap) {
+  const long long i0 = (long long)blockIdx.x * kEdgeSeg + (long long)threadIdx.x * kEdgePer;
+  unsigned fm, rm;
+  edge_masks(x, total, thr, i0, fm, rm);
+  int pa, pb;
+  block_scan2(__popc(fm), __popc(rm), pa, pb);
+  int kf = blk[blockIdx.x].x + pa, kr = blk[blockIdx.x].y + pb;
+  while (fm) {
+    const int j = __ffs(fm) - 1;
+    fm &= fm - 1;
+    if (kf < cap) fall[kf] = (unsigned)(i0 + j);
+    kf++;
+  }
+  while (rm) {
+    const int j = __ffs(rm) - 1;
+    rm &= rm - 1;
+    if (kr < cap) rise[kr] = (unsigned)(i0 + j);
+    kr++;
   }
 }
 
@@ -164,11 +263,15 @@ void launch_k1b(const DemodArgs& a, cudaStream_t st) {
   k1b_kernel<<<grid, kThreadsB, smem, st>>>(a);
 }
 
+int edge_blocks(long long total) { return (int)((total + kEdgeSeg - 1) / kEdgeSeg); }
+
 void launch_edges(const float* sync, long long total, float thr_rel, unsigned* fall, unsigned* rise, int* counts,
-                  int cap, cudaStream_t st) {
-  const int threads = 256;
-  const long long blocks = (total + threads - 1) / threads;
-  edges_kernel<<<(unsigned)blocks, threads, 0, st>>>(sync, total, thr_rel, fall, rise, counts, cap);
+                  int cap, int2* blk, cudaStream_t st) {
+  const int nblk = edge_blocks(total);
+  if (nblk <= 0) return;
+  edge_count_kernel<<<nblk, kEdgeThreads, 0, st>>>(sync, total, thr_rel, blk);
+  edge_scan_kernel<<<1, 1024, 0, st>>>(blk, nblk, counts);
+  edge_write_kernel<<<nblk, kEdgeThreads, 0, st>>>(sync, total, thr_rel, blk, fall, rise, cap);
 }
 
 }  // namespace cuvhs

@@ -164,13 +164,15 @@ std::vector<Valid> validate(const int* starts, const int* lengths, int n, const 
       out.push_back({kHsync, cur, good});
       i++;
     } else if (i > 2 && within((double)cur.len, w.e_lo, w.e_hi) && !out.empty() && out.back().type == kHsync) {
-      std::vector<Valid> seq = out;
-      const bool done = blanking_sequence(raw, (size_t)(i - 2), w, fmt.num_eq_pulses, fmt.samples_per_line, seq);
-      if (done && seq.size() > out.size()) {
-        out = seq;
+      // The recogniser extends the list in place; an unfinished attempt is
+      // rolled back (the reference runs it on a copy and keeps it on success).
+      const size_t before = out.size();
+      const bool done = blanking_sequence(raw, (size_t)(i - 2), w, fmt.num_eq_pulses, fmt.samples_per_line, out);
+      if (done && out.size() > before) {
         // the reference measures the advance after replacing the list, so it is one
         i = std::min(i + 1, n);
       } else {
+        out.resize(before);
         i++;
       }
     } else {
@@ -370,7 +372,16 @@ void snap_lines(const std::vector<Valid>& v, double ref_pos, double ref_line, do
   std::vector<double> ps;
   ps.reserve(v.size());
   for (const Valid& p : v) ps.push_back((double)p.p.start);
-  std::sort(ps.begin(), ps.end());
+  // nearly sorted already (the recogniser revisits two pulses): insertion sort
+  for (size_t a = 1; a < ps.size(); a++) {
+    const double v = ps[a];
+    size_t b = a;
+    while (b > 0 && ps[b - 1] > v) {
+      ps[b] = ps[b - 1];
+      b--;
+    }
+    ps[b] = v;
+  }
   const double max_dist = mll / 1.5;
   size_t cur = 0;
   for (int line = 0; line < nlines; line++) {

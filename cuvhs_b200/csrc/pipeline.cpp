@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -60,7 +61,13 @@ int phase_id_for(int is_first, int quadrant) {
 
 const char* const kStageNames[kNumStages] = {"k1a_demod",      "k1b_video_sync", "sync_edges",
                                              "hsync_refine",   "luma_resample",  "chroma_prefilter",
-                                             "chroma_lines",   "burst_metric",   "dropouts"};
+                                             "chroma_lines",   "burst_metric",   "dropouts",
+                                             "host_edges_wait", "host_lines",     "host_chroma_wait",
+                                             "host_final_wait"};
+
+double Context::host_clock() const {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 Context::~Context() { release(); }
 
@@ -108,6 +115,10 @@ void Context::release() {
   pool_used = 0;
   for (void* p : allocations) cudaFree(p);
   allocations.clear();
+  for (void* p : host_allocations) cudaFreeHost(p);
+  host_allocations.clear();
+  if (ev_host) cudaEventDestroy(ev_host);
+  ev_host = nullptr;
   if (stream) cudaStreamDestroy(stream);
   stream = nullptr;
 }
@@ -189,6 +200,7 @@ bool Context::init(const cuvhs_config& c) {
   d_fall = A((unsigned*)nullptr, edge_cap);
   d_rise = A((unsigned*)nullptr, edge_cap);
   d_counts = A((int*)nullptr, 4);
+  d_edge_blk = A((int2*)nullptr, (size_t)edge_blocks((long long)batch * spp) + 1);
   d_ll = A((double*)nullptr, (size_t)batch * fmt.lines_per_frame);
   const size_t F = (size_t)fmt.output_line_len * fmt.output_field_lines;
   d_luma = A((uint16_t*)nullptr, (size_t)batch * F);
@@ -210,6 +222,45 @@ bool Context::init(const cuvhs_config& c) {
   if (!ok) {
     status = CUVHS_ERR_OUT_OF_MEMORY;
     release();
+    return false;
+  }
+  // pinned host staging for the per-chunk round trips
+  auto H = [&](auto* tag, size_t n) {
+    using T = std::remove_pointer_t<decltype(tag)>;
+    void* p = nullptr;
+    if (!ok) return (T*)nullptr;
+    if (cudaHostAlloc(&p, std::max<size_t>(n, 1) * sizeof(T), cudaHostAllocDefault) != cudaSuccess) {
+      ok = false;
+      err = "cudaHostAlloc failed";
+      cudaGetLastError();
+      return (T*)nullptr;
+    }
+    host_allocations.push_back(p);
+    return static_cast<T*>(p);
+  };
+  const size_t guess = (size_t)std::min(edge_cap, batch * kEdgeGuessPerField);
+  hp_counts = H((int*)nullptr, 4);
+  hp_fall = H((unsigned*)nullptr, guess);
+  hp_rise = H((unsigned*)nullptr, guess);
+  hp_ll = H((double*)nullptr, (size_t)batch * fmt.lines_per_frame);
+  hp_track = H((int*)nullptr, batch);
+  hp_trial = H((int*)nullptr, 2);
+  hp_burst = H((float*)nullptr, (size_t)2 * fmt.output_field_lines * kBurstLen);
+  hp_metric = H((double*)nullptr, batch);
+  hp_do_count = H((int*)nullptr, batch);
+  hp_do_lines = H((int*)nullptr, (size_t)batch * kMaxDropouts);
+  hp_do_starts = H((int*)nullptr, (size_t)batch * kMaxDropouts);
+  hp_do_ends = H((int*)nullptr, (size_t)batch * kMaxDropouts);
+  if (!ok) {
+    status = CUVHS_ERR_OUT_OF_MEMORY;
+    release();
+    return false;
+  }
+  hp_trial[0] = 0;
+  hp_trial[1] = 1;
+  if (cudaEventCreateWithFlags(&ev_host, cudaEventDisableTiming) != cudaSuccess) {
+    err = "cudaEventCreate failed";
+    status = CUVHS_ERR_CUDA;
     return false;
   }
   upload(d_ga, des.ga, stream);
@@ -245,6 +296,18 @@ bool Context::sync(const char* where) {
     return false;
   }
   collect_stage_times();
+  return check_cuda(where);
+}
+
+// Wait for the work recorded before ev_host (the host reads results it
+// copied); later work on the stream keeps running.
+bool Context::wait_host_event(const char* where) {
+  cudaError_t e = cudaEventSynchronize(ev_host);
+  if (e != cudaSuccess) {
+    err = std::string(where) + ": " + cudaGetErrorString(e);
+    status = CUVHS_ERR_CUDA;
+    return false;
+  }
   return check_cuda(where);
 }
 
@@ -357,31 +420,88 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     end_stage(kStageK1b, ev_);
   }
   if (!check_cuda("demod")) return false;
-  // ---- sync edges over the demodulated range
+  // ---- sync edges over the demodulated range.  One copy brings back the
+  // counts and a speculative prefix of both edge lists; a second copy is
+  // needed only when a list is longer than the prefix.
   const float thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
   cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), stream);
   const long long total_chunk = (long long)T * spp;
   {
     cudaEvent_t ev_;
     begin_stage(kStageEdges, ev_);
-    launch_edges(d_sync, total_chunk, thr_rel, d_fall, d_rise, d_counts, edge_cap, stream);
+    launch_edges(d_sync, total_chunk, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, stream);
     end_stage(kStageEdges, ev_);
   }
-  int counts[4] = {0, 0, 0, 0};
-  cudaMemcpyAsync(counts, d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream);
-  if (!sync("edges")) return false;
-  if (counts[0] > edge_cap || counts[1] > edge_cap) {
+  const int guess = std::min(edge_cap, T * kEdgeGuessPerField);
+  cudaMemcpyAsync(hp_counts, d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(hp_fall, d_fall, (size_t)guess * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(hp_rise, d_rise, (size_t)guess * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
+  cudaEventRecord(ev_host, stream);
+  // ---- the colour-under pre-band-pass needs only the raw samples: it runs on
+  // the GPU while the host turns edges into field windows and line locations.
+  // It covers all T demodulated slots; the detected fields are a prefix.
+  const int LPF = fmt.lines_per_frame;
+  const int H = fmt.output_field_lines;
+  ChromaArgs ca;
+  ca.raw = d_raw;
+  ca.pre = d_dem;  // the raw demod is no longer needed after K1b
+  ca.fields = T;
+  ca.spp = spp;
+  ca.ctile = des.ctile;
+  ca.c_half = des.c_half;
+  ca.c_out = des.c_out;
+  ca.gc = d_gc;
+  ca.tw_c = d_twc;
+  ca.tw_line = d_twl;
+  ca.ll = d_ll;
+  ca.total = 0;
+  ca.track = d_track;
+  ca.het_scale = des.het_scale;
+  ca.fsc_bin = des.fsc_bin;
+  ca.bw_bins = des.bw_bins;
+  ca.burst_start = fmt.burst_start;
+  ca.out_w = fmt.output_line_len;
+  ca.out_h = H;
+  ca.lines_per_frame = LPF;
+  ca.burst_abs_ref = (float)fmt.burst_abs_ref;
+  ca.chroma = d_chroma;
+  ca.burst = d_burst;
+  ca.metric = d_metric;
+  if (debug) {
+    dbg_demod.resize(std::min<size_t>((size_t)T * spp, (size_t)debug_tiles * spp));
+    cudaMemcpyAsync(dbg_demod.data(), d_dem, dbg_demod.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
+  }
+  {
+    cudaEvent_t ev_;
+    begin_stage(kStageChromaPre, ev_);
+    launch_chroma_prefilter(ca, stream);
+    end_stage(kStageChromaPre, ev_);
+  }
+  if (!check_cuda("chroma prefilter")) return false;
+  double t_host = host_clock();
+  if (!wait_host_event("edges")) return false;
+  host_phase(kHostEdgesWait, t_host);
+  t_host = host_clock();
+  const int nfall = hp_counts[0], nrise = hp_counts[1];
+  if (nfall > edge_cap || nrise > edge_cap) {
     err = "sync edge list overflow";
     status = CUVHS_ERR_CAPACITY;
     return false;
   }
-  h_fall.resize(counts[0]);
-  h_rise.resize(counts[1]);
-  if (counts[0]) cudaMemcpyAsync(h_fall.data(), d_fall, counts[0] * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
-  if (counts[1]) cudaMemcpyAsync(h_rise.data(), d_rise, counts[1] * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
-  if (!sync("edge lists")) return false;
-  std::sort(h_fall.begin(), h_fall.end());
-  std::sort(h_rise.begin(), h_rise.end());
+  h_fall.assign(hp_fall, hp_fall + std::min(nfall, guess));
+  h_rise.assign(hp_rise, hp_rise + std::min(nrise, guess));
+  if (nfall > guess || nrise > guess) {
+    h_fall.resize(nfall);
+    h_rise.resize(nrise);
+    if (nfall > guess)
+      cudaMemcpyAsync(h_fall.data() + guess, d_fall + guess, (size_t)(nfall - guess) * sizeof(unsigned),
+                      cudaMemcpyDeviceToHost, stream);
+    if (nrise > guess)
+      cudaMemcpyAsync(h_rise.data() + guess, d_rise + guess, (size_t)(nrise - guess) * sizeof(unsigned),
+                      cudaMemcpyDeviceToHost, stream);
+    if (!sync("edge lists")) return false;
+  }
+  // both lists arrive in sample order
   // runs [start, end): end = first rising edge after start, or the range end
   run_start.resize(h_fall.size());
   run_end.resize(h_fall.size());
@@ -419,8 +539,6 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   const size_t predicted = offs.back() + actual_spf, margin = 10 * (size_t)fmt.samples_per_line;
   res.next_raw_offset = predicted > margin ? raw_offset + predicted - margin : raw_offset + predicted;
   // ---- per-field pulses and line locations (sync_pulses.cu:10-58, pipeline.cu:1717-1778)
-  const int LPF = fmt.lines_per_frame;
-  h_ll.assign((size_t)P * LPF, 0.0);
   h_is_first.assign(P, -1);
   if (debug) {
     dbg_k2c.assign(P, 0);
@@ -447,7 +565,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
       }
     }
     locate_lines(fmt, ps.data(), pl.data(), (int)ps.size(), (long long)(raw_offset + offs[f]), lls, fl);
-    std::copy(fl.locs.begin(), fl.locs.end(), h_ll.begin() + (size_t)f * LPF);
+    std::copy(fl.locs.begin(), fl.locs.end(), hp_ll + (size_t)f * LPF);
     h_is_first[f] = fl.is_first;
     if (debug) {
       dbg_k2c[f] = (int)ps.size();
@@ -462,10 +580,11 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   if (debug) {
     dbg_vsync = cand;
     dbg_offs.assign(offs.begin(), offs.end());
-    dbg_ll_coarse = h_ll;
+    dbg_ll_coarse.assign(hp_ll, hp_ll + (size_t)P * LPF);
     dbg_meta = {T, P, spp};
   }
-  cudaMemcpyAsync(d_ll, h_ll.data(), h_ll.size() * sizeof(double), cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(d_ll, hp_ll, (size_t)P * LPF * sizeof(double), cudaMemcpyHostToDevice, stream);
+  host_phase(kHostLines, t_host);
   // ---- K4 hsync refinement, K5 luma
   LineArgs la;
   la.video = d_video;
@@ -481,7 +600,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   la.right_edge_offset = 2.25 * ((fmt.fs_hz / 1.0e6) / 40.0);
   la.luma = d_luma;
   la.out_w = fmt.output_line_len;
-  la.out_h = fmt.output_field_lines;
+  la.out_h = H;
   la.luma_gain = (float)(fmt.output_scale / fmt.hz_ire);
   la.luma_offset = (float)(-fmt.vsync_ire * fmt.output_scale + fmt.output_zero);
   {
@@ -497,45 +616,21 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     end_stage(kStageLuma, ev_);
   }
   if (!check_cuda("lines")) return false;
-  // ---- K6 chroma
-  ChromaArgs ca;
-  ca.raw = d_raw;
-  ca.pre = d_dem;  // the raw demod is no longer needed
+  // ---- K6 chroma on the P detected fields
   ca.fields = P;
-  ca.spp = spp;
-  ca.ctile = des.ctile;
-  ca.c_half = des.c_half;
-  ca.c_out = des.c_out;
-  ca.gc = d_gc;
-  ca.tw_c = d_twc;
-  ca.tw_line = d_twl;
-  ca.ll = d_ll;
   ca.total = (long long)P * spp;
-  ca.track = d_track;
-  ca.het_scale = des.het_scale;
-  ca.fsc_bin = des.fsc_bin;
-  ca.bw_bins = des.bw_bins;
-  ca.burst_start = fmt.burst_start;
-  ca.out_w = fmt.output_line_len;
-  ca.out_h = fmt.output_field_lines;
-  ca.lines_per_frame = LPF;
-  ca.burst_abs_ref = (float)fmt.burst_abs_ref;
-  ca.chroma = d_chroma;
-  ca.burst = d_burst;
-  ca.metric = d_metric;
-  if (debug) {
-    dbg_demod.resize(std::min<size_t>((size_t)T * spp, (size_t)debug_tiles * spp));
-    cudaMemcpyAsync(dbg_demod.data(), d_dem, dbg_demod.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
-  }
-  {
+  auto chroma_pass = [&](int f0, int nf, bool write) {
     cudaEvent_t ev_;
-    begin_stage(kStageChromaPre, ev_);
-    launch_chroma_prefilter(ca, stream);
-    end_stage(kStageChromaPre, ev_);
-  }
-  if (!check_cuda("chroma prefilter")) return false;
-  const int H = fmt.output_field_lines;
-  h_track.assign(P, 0);
+    begin_stage(kStageChromaLines, ev_);
+    launch_chroma_lines(ca, f0, nf, write, stream);
+    end_stage(kStageChromaLines, ev_);
+    if (write) {
+      begin_stage(kStageBurstMetric, ev_);
+      launch_burst_metric(ca, f0, nf, stream);
+      end_stage(kStageBurstMetric, ev_);
+      cudaMemcpyAsync(hp_metric + f0, d_metric + f0, nf * sizeof(double), cudaMemcpyDeviceToHost, stream);
+    }
+  };
   int det_track, cycle_start;
   double thr;
   if (chroma_valid) {
@@ -543,35 +638,23 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     thr = chroma_threshold;
     cycle_start = chroma_cycle_start;
   } else {
-    // track and burst phase from field 0 (chroma_decode.cu:684-743)
-    std::vector<float> b0((size_t)H * kBurstLen);
-    double metric[2];
+    // Track and burst phase from field 0 (chroma_decode.cu:684-743): both
+    // trial tracks in one round trip; the detected track's burst windows are
+    // the ones the phase measurement reads.
+    const size_t nb = (size_t)H * kBurstLen;
     for (int t = 0; t < 2; t++) {
-      h_track[0] = t;
-      cudaMemcpyAsync(d_track, h_track.data(), sizeof(int), cudaMemcpyHostToDevice, stream);
-      {
-        cudaEvent_t ev_;
-        begin_stage(kStageChromaLines, ev_);
-        launch_chroma_lines(ca, 0, 1, false, stream);
-        end_stage(kStageChromaLines, ev_);
-      }
-      cudaMemcpyAsync(b0.data(), d_burst, b0.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
-      if (!sync("chroma track detect")) return false;
-      metric[t] = host_burst_metric(b0.data(), H);
+      cudaMemcpyAsync(d_track, hp_trial + t, sizeof(int), cudaMemcpyHostToDevice, stream);
+      chroma_pass(0, 1, false);
+      cudaMemcpyAsync(hp_burst + t * nb, d_burst, nb * sizeof(float), cudaMemcpyDeviceToHost, stream);
     }
-    det_track = (metric[1] < metric[0]) ? 1 : 0;
-    thr = metric[det_track] * 4.0;
-    h_track[0] = det_track;
-    cudaMemcpyAsync(d_track, h_track.data(), sizeof(int), cudaMemcpyHostToDevice, stream);
-    {
-      cudaEvent_t ev_;
-      begin_stage(kStageChromaLines, ev_);
-      launch_chroma_lines(ca, 0, 1, false, stream);
-      end_stage(kStageChromaLines, ev_);
-    }
-    cudaMemcpyAsync(b0.data(), d_burst, b0.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
-    if (!sync("chroma burst phase")) return false;
-    const double ph = host_burst_phase(b0.data(), H, fmt);
+    cudaEventRecord(ev_host, stream);
+    t_host = host_clock();
+    if (!wait_host_event("chroma track detect")) return false;
+    host_phase(kHostChromaWait, t_host);
+    const double m0 = host_burst_metric(hp_burst, H), m1 = host_burst_metric(hp_burst + nb, H);
+    det_track = (m1 < m0) ? 1 : 0;
+    thr = (det_track ? m1 : m0) * 4.0;
+    const double ph = host_burst_phase(hp_burst + det_track * nb, H, fmt);
     const int quadrant = ((int)(ph / 90.0 + 0.5)) % 4;
     const int pid = phase_id_for(1, quadrant);
     cycle_start = 0;
@@ -584,32 +667,39 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   int cur = det_track;
   h_phase.assign(P, 0);
   for (int f = 0; f < P; f++) {
-    h_track[f] = (f & 1) ? (1 - cur) : cur;
+    hp_track[f] = (f & 1) ? (1 - cur) : cur;
     h_phase[f] = kPhaseCycle[(cycle_start + f) % 8];
   }
-  // chunks of 15 fields with track-flip retries (chroma_decode.cu:782-981)
+  // Every field's chroma depends only on its own track, so all fields are
+  // computed in one pass with the initial assignment; the reference's
+  // 15-field chunks with up to three flip-and-retry passes each
+  // (chroma_decode.cu:782-981) are then replayed on the host, recomputing
+  // only fields whose track a flip changed.
+  computed_track.assign(hp_track, hp_track + P);
+  cudaMemcpyAsync(d_track, hp_track, P * sizeof(int), cudaMemcpyHostToDevice, stream);
+  chroma_pass(0, P, true);
+  cudaEventRecord(ev_host, stream);
+  t_host = host_clock();
+  if (!wait_host_event("chroma lines")) return false;
+  host_phase(kHostChromaWait, t_host);
   const int fpc = std::max(1, std::min((4096 / H), P));
-  std::vector<double> metrics(P);
   for (int f0 = 0; f0 < P; f0 += fpc) {
     const int nf = std::min(fpc, P - f0);
     int retries = 3;
     bool ok = false;
     while (!ok && retries-- > 0) {
-      cudaMemcpyAsync(d_track + f0, h_track.data() + f0, nf * sizeof(int), cudaMemcpyHostToDevice, stream);
-      {
-        cudaEvent_t ev_;
-        begin_stage(kStageChromaLines, ev_);
-        launch_chroma_lines(ca, f0, nf, true, stream);
-        end_stage(kStageChromaLines, ev_);
-        begin_stage(kStageBurstMetric, ev_);
-        launch_burst_metric(ca, f0, nf, stream);
-        end_stage(kStageBurstMetric, ev_);
+      bool stale = false;
+      for (int f = f0; f < f0 + nf; f++) stale = stale || computed_track[f] != hp_track[f];
+      if (stale) {
+        cudaMemcpyAsync(d_track + f0, hp_track + f0, nf * sizeof(int), cudaMemcpyHostToDevice, stream);
+        chroma_pass(f0, nf, true);
+        cudaEventRecord(ev_host, stream);
+        if (!wait_host_event("chroma retry")) return false;
+        for (int f = f0; f < f0 + nf; f++) computed_track[f] = hp_track[f];
       }
-      cudaMemcpyAsync(metrics.data() + f0, d_metric + f0, nf * sizeof(double), cudaMemcpyDeviceToHost, stream);
-      if (!sync("chroma lines")) return false;
       int first_bad = INT_MAX;
       for (int f = 0; f < nf; f++)
-        if (metrics[f0 + f] > thr) {
+        if (hp_metric[f0 + f] > thr) {
           first_bad = f;
           break;
         }
@@ -617,7 +707,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
         ok = true;
       } else {
         cur = 1 - cur;
-        for (int ff = f0 + first_bad; ff < P; ff++) h_track[ff] = (ff & 1) ? (1 - cur) : cur;
+        for (int ff = f0 + first_bad; ff < P; ff++) hp_track[ff] = (ff & 1) ? (1 - cur) : cur;
       }
     }
   }
@@ -651,17 +741,14 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   }
   if (!check_cuda("dropouts")) return false;
   // ---- small results back
-  h_do_count.resize(P);
-  cudaMemcpyAsync(h_do_count.data(), d_do_count, P * sizeof(int), cudaMemcpyDeviceToHost, stream);
-  h_do_lines.resize((size_t)P * kMaxDropouts);
-  h_do_starts.resize((size_t)P * kMaxDropouts);
-  h_do_ends.resize((size_t)P * kMaxDropouts);
-  cudaMemcpyAsync(h_do_lines.data(), d_do_lines, h_do_lines.size() * sizeof(int), cudaMemcpyDeviceToHost, stream);
-  cudaMemcpyAsync(h_do_starts.data(), d_do_starts, h_do_starts.size() * sizeof(int), cudaMemcpyDeviceToHost, stream);
-  cudaMemcpyAsync(h_do_ends.data(), d_do_ends, h_do_ends.size() * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(hp_do_count, d_do_count, P * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  const size_t ndo = (size_t)P * kMaxDropouts;
+  cudaMemcpyAsync(hp_do_lines, d_do_lines, ndo * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(hp_do_starts, d_do_starts, ndo * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(hp_do_ends, d_do_ends, ndo * sizeof(int), cudaMemcpyDeviceToHost, stream);
   if (debug) {
-    dbg_ll.resize(h_ll.size());
-    cudaMemcpyAsync(dbg_ll.data(), d_ll, h_ll.size() * sizeof(double), cudaMemcpyDeviceToHost, stream);
+    dbg_ll.resize((size_t)P * LPF);
+    cudaMemcpyAsync(dbg_ll.data(), d_ll, dbg_ll.size() * sizeof(double), cudaMemcpyDeviceToHost, stream);
     const size_t nt = std::min<size_t>((size_t)T * spp, (size_t)debug_tiles * spp);
     dbg_video.resize(nt);
     dbg_sync.resize(nt);
@@ -672,7 +759,10 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     cudaMemcpyAsync(dbg_env.data(), d_env, nt * sizeof(float), cudaMemcpyDeviceToHost, stream);
     cudaMemcpyAsync(dbg_pre.data(), d_dem, dbg_pre.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
   }
+  t_host = host_clock();
   if (!sync("dropouts")) return false;
+  host_phase(kHostFinalWait, t_host);
+  last_fields = P;
   // ---- field metadata: parity alternation (pipeline.cu:2575-2610)
   res.fields = P;
   res.field_info.resize(P);
@@ -685,7 +775,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     last_parity = first;
     fi.is_first_field = first ? 1 : 0;
     fi.field_phase_id = h_phase[i] > 0 ? h_phase[i] : 0;
-    fi.dropout_count = std::max(0, std::min(h_do_count[i], kMaxDropouts));
+    fi.dropout_count = std::max(0, std::min(hp_do_count[i], kMaxDropouts));
     fi.dropout_offset = 0;
   }
   if (debug) dbg_is_first = h_is_first;

@@ -28,8 +28,14 @@ enum Stage {
   kStageChromaLines,
   kStageBurstMetric,
   kStageDropouts,
+  // host phases (wall time on the calling thread)
+  kHostEdgesWait,
+  kHostLines,
+  kHostChromaWait,
+  kHostFinalWait,
   kNumStages
 };
+constexpr int kFirstHostStage = kHostEdgesWait;
 extern const char* const kStageNames[kNumStages];
 
 struct Context {
@@ -45,12 +51,17 @@ struct Context {
   std::string err;
   cuvhs_status status = CUVHS_OK;
   std::vector<void*> allocations;
+  std::vector<void*> host_allocations;
+  cudaEvent_t ev_host = nullptr;
+  int last_fields = 0;
+  static constexpr int kEdgeGuessPerField = 2048;  // edges per field copied speculatively
 
   uint8_t* d_raw = nullptr;
   float *d_dem = nullptr, *d_env = nullptr, *d_video = nullptr, *d_sync = nullptr;
   double* d_env_part = nullptr;
   unsigned *d_fall = nullptr, *d_rise = nullptr;
   int* d_counts = nullptr;
+  int2* d_edge_blk = nullptr;
   double* d_ll = nullptr;
   uint16_t *d_luma = nullptr, *d_chroma = nullptr;
   float* d_burst = nullptr;
@@ -71,9 +82,15 @@ struct Context {
   // host scratch (kept to avoid reallocation)
   std::vector<unsigned> h_fall, h_rise;
   std::vector<long long> run_start, run_end;
-  std::vector<double> h_ll;
-  std::vector<int> h_is_first, h_track, h_phase;
-  std::vector<int> h_do_count, h_do_lines, h_do_starts, h_do_ends;
+  std::vector<int> h_is_first, h_phase, computed_track;
+  // pinned staging
+  int* hp_counts = nullptr;
+  unsigned *hp_fall = nullptr, *hp_rise = nullptr;
+  double* hp_ll = nullptr;
+  int *hp_track = nullptr, *hp_trial = nullptr;
+  float* hp_burst = nullptr;
+  double* hp_metric = nullptr;
+  int *hp_do_count = nullptr, *hp_do_lines = nullptr, *hp_do_starts = nullptr, *hp_do_ends = nullptr;
 
   // last-chunk intermediates (debug)
   bool debug = false;
@@ -99,6 +116,10 @@ struct Context {
   void begin_stage(int stage, cudaEvent_t& a);
   void end_stage(int stage, cudaEvent_t a);
   void collect_stage_times();
+  double host_clock() const;
+  void host_phase(int stage, double t0) {
+    if (timing) stage_ms[stage] += host_clock() - t0;
+  }
 
   ~Context();
   bool init(const cuvhs_config& c);
@@ -106,6 +127,7 @@ struct Context {
   void reset_state();
   bool check_cuda(const char* where);
   bool sync(const char* where);
+  bool wait_host_event(const char* where);
   bool decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avail, uint64_t raw_offset, int num_fields,
                     ChunkResult& res);
 };

@@ -5,14 +5,25 @@
 // registers, so one padded buffer serves as both source and destination of a
 // pass (read all -> barrier -> write all -> barrier).  Index i lives at i + i/16
 // so the stride-16 writes of the first pass do not collide on banks.
-// Twiddles come from a table W_N^m, m in [0, N), computed in FP64 on the host
-// and rounded once to FP32.
+// Twiddles come from a per-pass table computed in FP64 on the host and
+// rounded once to FP32: pass NS (>= 16) stores W_{NS*R}^{r*k} at
+// (NS - 16) + (r - 1) * NS + k, so a warp's twiddle loads (consecutive k) are
+// contiguous.  fft_twiddle_count(N) entries in all.
 #pragma once
 #include <cuda_runtime.h>
 
 namespace cuvhs {
 
 __host__ __device__ constexpr int fft_pad(int n) { return n + (n >> 4); }
+
+// Radix of the pass that starts at span NS in an N-point transform.
+__host__ __device__ constexpr int fft_radix(int N, int NS) { return NS * 16 <= N ? 16 : N / NS; }
+// Entries of the per-pass twiddle table of an N-point transform.
+__host__ __device__ constexpr int fft_twiddle_count(int N) {
+  int n = 0;
+  for (int ns = 16; ns < N; ns *= 16) n += (fft_radix(N, ns) - 1) * ns;
+  return n;
+}
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
 
 template <bool INV>
@@ -145,9 +156,9 @@ __device__ __forceinline__ void fft_pass(float2* s, const float2* __restrict__ t
       for (int r = 0; r < R; r++) v[p][r] = s[pidx(j + r * NB)];
       if constexpr (NS > 1) {
         const int k = j & (NS - 1);
-        constexpr int STEP = N / (NS * R);
+        const float2* twp = tw + (NS - 16) + k;
 #pragma unroll
-        for (int r = 1; r < R; r++) v[p][r] = cmul_tw<INV>(v[p][r], __ldg(&tw[r * k * STEP]));
+        for (int r = 1; r < R; r++) v[p][r] = cmul_tw<INV>(v[p][r], __ldg(&twp[(r - 1) * NS]));
       }
       dft<R, INV>(v[p]);
     }

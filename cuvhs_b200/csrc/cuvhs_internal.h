@@ -90,6 +90,11 @@ struct DemodArgs {
   const float2* gb;
   const float2* tw_a;
   const float2* tw_b;
+  // The inverse transforms read their own copies of the twiddle tables, so the
+  // compiler cannot merge the two transforms' twiddle loads and keep them all
+  // live at once.
+  const float2* tw_a_inv;
+  const float2* tw_b_inv;
   int a_pos, a_out, b_pos, b_out;
   float rot_re, rot_im, d0, demod_scale, demod_offset;
   float corr_video, corr_sync;
@@ -134,6 +139,8 @@ struct ChromaArgs {
   const float* gc;
   const float2* tw_c;
   const float2* tw_line;
+  const float2* tw_c_inv;
+  const float2* tw_line_inv;
   const double* ll;
   long long total;  // P * spp
   const int* track;  // per field

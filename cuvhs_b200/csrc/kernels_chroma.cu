@@ -14,44 +14,50 @@
 #include <cuda_runtime.h>
 
 #include "cuvhs_internal.h"
-#include "smem_fft.cuh"
+#include "reg_fft.cuh"
 
 namespace cuvhs {
 namespace {
 
-constexpr int kThreadsC = 512;
+constexpr int kThreadsC = Design::kNc / 16;
 constexpr int kLineWarps = 4;
 
-__global__ void __launch_bounds__(kThreadsC) prefilter_kernel(ChromaArgs a) {
-  constexpr int N = Design::kNc;
+// Two adjacent output blocks ride in the real and imaginary parts of one
+// transform (the kernel is real).  Thread t holds block samples t + T*q.
+__global__ void __launch_bounds__(kThreadsC, 1) prefilter_kernel(ChromaArgs a) {
+  constexpr int N = Design::kNc, T = kThreadsC;
   extern __shared__ float2 sm[];
+  const int t = threadIdx.x;
   const int f = blockIdx.y;
   const int i0 = blockIdx.x * 2 * a.c_out;  // first output of the real half
   const uint8_t* tile = a.raw + (size_t)f * a.spp;
-  for (int t = threadIdx.x; t < N; t += kThreadsC) {
-    int q0 = (i0 - a.c_half + t) % a.ctile;
+  float2 v[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    int q0 = (i0 - a.c_half + t + T * q) % a.ctile;
     if (q0 < 0) q0 += a.ctile;
     int q1 = q0 + a.c_out;
     if (q1 >= a.ctile) q1 -= a.ctile;
-    const float v0 = q0 < a.spp ? ((float)tile[q0] - 128.0f) * 256.0f : 0.0f;
-    const float v1 = q1 < a.spp ? ((float)tile[q1] - 128.0f) * 256.0f : 0.0f;
-    sm[pidx(t)] = make_float2(v0, v1);
+    const float v0 = q0 < a.spp ? ((float)__ldg(&tile[q0]) - 128.0f) * 256.0f : 0.0f;
+    const float v1 = q1 < a.spp ? ((float)__ldg(&tile[q1]) - 128.0f) * 256.0f : 0.0f;
+    v[q] = make_float2(v0, v1);
   }
-  __syncthreads();
-  smem_fft<N, kThreadsC, false>(sm, a.tw_c);
-  for (int k = threadIdx.x; k < N; k += kThreadsC) {
-    const float g = __ldg(&a.gc[k]);
-    const float2 x = sm[pidx(k)];
-    sm[pidx(k)] = make_float2(x.x * g, x.y * g);
+  RegFFT<N>::run<false>(v, sm, a.tw_c, t);
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const float g = __ldg(&a.gc[t + T * q]);
+    v[q] = make_float2(v[q].x * g, v[q].y * g);
   }
-  __syncthreads();
-  smem_fft<N, kThreadsC, true>(sm, a.tw_c);
+  RegFFT<N>::run<true>(v, sm, a.tw_c_inv, t);
   float* out = a.pre + (size_t)f * a.spp;
-  for (int i = threadIdx.x; i < a.c_out; i += kThreadsC) {
-    const float2 v = sm[pidx(a.c_half + i)];
-    const int p0 = i0 + i, p1 = i0 + a.c_out + i;
-    if (p0 < a.spp) out[p0] = v.x;
-    if (p1 < a.spp) out[p1] = v.y;
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int i = t + T * q - a.c_half;
+    if (i >= 0 && i < a.c_out) {
+      const int p0 = i0 + i, p1 = i0 + a.c_out + i;
+      if (p0 < a.spp) out[p0] = v[q].x;
+      if (p1 < a.spp) out[p1] = v[q].y;
+    }
   }
 }
 
@@ -107,7 +113,7 @@ __global__ void __launch_bounds__(32 * kLineWarps) lines_kernel(ChromaArgs a, in
     sm[pidx(k)] = make_float2(x.x * m, x.y * m);
   }
   __syncwarp();
-  smem_fft<kLineFFT, 32, true>(sm, a.tw_line);
+  smem_fft<kLineFFT, 32, true>(sm, a.tw_line_inv);
   // burst RMS per line -> ACC gain
   float ssa = 0.0f, ssb = 0.0f;
   for (int i = lane; i < kBurstLen; i += 32) {

@@ -12,102 +12,124 @@
 #include <cuda_runtime.h>
 
 #include "cuvhs_internal.h"
-#include "smem_fft.cuh"
+#include "reg_fft.cuh"
 
 namespace cuvhs {
 namespace {
 
-constexpr int kThreadsA = 256;
-constexpr int kThreadsB = 512;
+constexpr int kThreadsA = Design::kNa / 16;
+constexpr int kThreadsB = Design::kNb / 16;
 
 __device__ __forceinline__ int wrap_tile(int q, int tile) {
   return q < 0 ? q + tile : (q >= tile ? q - tile : q);
 }
-__device__ __forceinline__ long long clamp_ll(long long p, long long total) {
-  return p < 0 ? 0 : (p >= total ? total - 1 : p);
-}
 
 // K1a: u8 -> analytic signal -> phase step (FP32 Hz, relative to ire0) + envelope.
-__global__ void __launch_bounds__(kThreadsA) k1a_kernel(DemodArgs a) {
-  constexpr int N = Design::kNa;
+// Thread t holds block samples t + 256*q throughout (RegFFT layout).
+__global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(DemodArgs a) {
+  constexpr int N = Design::kNa, T = kThreadsA;
   extern __shared__ float2 sm[];
-  __shared__ double red[kThreadsA / 32];
+  __shared__ float2 warp_last[T / 32][16];
+  __shared__ double red[T / 32];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int f = blockIdx.y;
-  const int j0 = kOverlap + blockIdx.x * a.a_out;       // first demod output (tile position)
-  const long long tile0 = (long long)f * a.spp - kOverlap;  // chunk position of tile position 0
-  const int base = j0 - 1 - a.a_pos;                    // tile position of block sample 0
-  for (int t = threadIdx.x; t < N; t += kThreadsA) {
-    const int q = wrap_tile(base + t, a.tile);
-    const long long p = clamp_ll(tile0 + q, a.total);
-    const float v = ((float)a.raw[p] - 128.0f) * 256.0f;
-    sm[pidx(t)] = make_float2(v, 0.0f);
+  const int j0 = kOverlap + blockIdx.x * a.a_out;  // first demod output (tile position)
+  // chunk positions fit in 32 bits (the batch is capped so T * spp < 2^31)
+  const int tile0 = f * a.spp - kOverlap;          // chunk position of tile position 0
+  const int last = (int)a.total - 1;
+  const int base = j0 - 1 - a.a_pos;               // tile position of block sample 0
+  float2 v[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int p = min(max(tile0 + wrap_tile(base + t + T * q, a.tile), 0), last);
+    v[q] = make_float2(((float)__ldg(&a.raw[p]) - 128.0f) * 256.0f, 0.0f);
+  }
+  RegFFT<N>::run<false>(v, sm, a.tw_a, t);
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const float2 g = __ldg(&a.ga[t + T * q]);
+    v[q] = make_float2(v[q].x * g.x - v[q].y * g.y, v[q].x * g.y + v[q].y * g.x);
+  }
+  RegFFT<N>::run<true>(v, sm, a.tw_a_inv, t);
+  // the previous sample of t + T*q is held by thread t-1 (same q), or for t = 0
+  // by thread T-1 at q-1
+  if (lane == 31) {
+#pragma unroll
+    for (int q = 0; q < 16; q++) warp_last[warp][q] = v[q];
   }
   __syncthreads();
-  smem_fft<N, kThreadsA, false>(sm, a.tw_a);
-  for (int k = threadIdx.x; k < N; k += kThreadsA) {
-    const float2 x = sm[pidx(k)], g = __ldg(&a.ga[k]);
-    sm[pidx(k)] = make_float2(x.x * g.x - x.y * g.y, x.x * g.y + x.y * g.x);
-  }
-  __syncthreads();
-  smem_fft<N, kThreadsA, true>(sm, a.tw_a);
   const int nout = min(a.a_out, kOverlap + a.spp - j0);
-  const size_t o0 = (size_t)f * a.spp + (size_t)(j0 - kOverlap);
+  float* dem_out = a.dem + (f * a.spp + (j0 - kOverlap));
+  float* env_out = a.env + (f * a.spp + (j0 - kOverlap));
   double esum = 0.0;
-  for (int i = threadIdx.x; i < nout; i += kThreadsA) {
-    const int t = a.a_pos + 1 + i;
-    const float2 z = sm[pidx(t)], zp = sm[pidx(t - 1)];
-    // z * conj(zp) rotated by the nominal step, so atan2 sees a small angle
-    const float re0 = z.x * zp.x + z.y * zp.y;
-    const float im0 = z.y * zp.x - z.x * zp.y;
-    const float re = re0 * a.rot_re - im0 * a.rot_im;
-    const float im = re0 * a.rot_im + im0 * a.rot_re;
-    float r = atan2f(im, re);
-    // keep the un-rotated step in (-pi, pi] as the reference's wrap does
-    if (r + a.d0 > 3.14159265358979f) r -= 6.28318530717959f;
-    a.dem[o0 + i] = r * a.demod_scale + a.demod_offset;
-    const float e = sqrtf(z.x * z.x + z.y * z.y);
-    a.env[o0 + i] = e;
-    esum += (double)e;
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    float2 zp;
+    zp.x = __shfl_up_sync(0xffffffffu, v[q].x, 1);
+    zp.y = __shfl_up_sync(0xffffffffu, v[q].y, 1);
+    if (lane == 0) zp = warp > 0 ? warp_last[warp - 1][q] : (q > 0 ? warp_last[T / 32 - 1][q - 1] : v[q]);
+    const int i = t + T * q - (a.a_pos + 1);
+    if (i >= 0 && i < nout) {
+      const float2 z = v[q];
+      // z * conj(zp) rotated by the nominal step, so atan2 sees a small angle
+      const float re0 = z.x * zp.x + z.y * zp.y;
+      const float im0 = z.y * zp.x - z.x * zp.y;
+      const float re = re0 * a.rot_re - im0 * a.rot_im;
+      const float im = re0 * a.rot_im + im0 * a.rot_re;
+      float r = atan2f(im, re);
+      // keep the un-rotated step in (-pi, pi] as the reference's wrap does
+      if (r + a.d0 > 3.14159265358979f) r -= 6.28318530717959f;
+      dem_out[i] = r * a.demod_scale + a.demod_offset;
+      const float e = sqrtf(z.x * z.x + z.y * z.y);
+      env_out[i] = e;
+      esum += (double)e;
+    }
   }
   // Deterministic per-CTA envelope partial sums (the dropout stage needs the
   // tile mean).
   for (int off = 16; off > 0; off >>= 1) esum += __shfl_down_sync(0xffffffffu, esum, off);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = esum;
+  if (lane == 0) red[warp] = esum;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < kThreadsA / 32; w++) s += red[w];
-    a.env_part[(size_t)f * a.env_blocks + blockIdx.x] = s;
+  if (t == 0) {
+    double sacc = 0.0;
+    for (int w = 0; w < T / 32; w++) sacc += red[w];
+    a.env_part[(size_t)f * a.env_blocks + blockIdx.x] = sacc;
   }
 }
 
 // K1b: demod -> video (real part) and sync (imag part) in one complex transform.
-__global__ void __launch_bounds__(kThreadsB) k1b_kernel(DemodArgs a) {
-  constexpr int N = Design::kNb;
+__global__ void __launch_bounds__(kThreadsB, 1) k1b_kernel(DemodArgs a) {
+  constexpr int N = Design::kNb, T = kThreadsB;
   extern __shared__ float2 sm[];
+  const int t = threadIdx.x;
   const int f = blockIdx.y;
   const int j0 = kOverlap + blockIdx.x * a.b_out;
-  const long long tile0 = (long long)f * a.spp - kOverlap;
+  const int tile0 = f * a.spp - kOverlap;
+  const int last = (int)a.total - 1;
   const int base = j0 - a.b_pos;
-  for (int t = threadIdx.x; t < N; t += kThreadsB) {
-    const int q = wrap_tile(base + t, a.tile);
-    const long long p = clamp_ll(tile0 + q, a.total);
-    sm[pidx(t)] = make_float2(__ldg(&a.dem[p]), 0.0f);
+  float2 v[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int p = min(max(tile0 + wrap_tile(base + t + T * q, a.tile), 0), last);
+    v[q] = make_float2(__ldg(&a.dem[p]), 0.0f);
   }
-  __syncthreads();
-  smem_fft<N, kThreadsB, false>(sm, a.tw_b);
-  for (int k = threadIdx.x; k < N; k += kThreadsB) {
-    const float2 x = sm[pidx(k)], g = __ldg(&a.gb[k]);
-    sm[pidx(k)] = make_float2(x.x * g.x - x.y * g.y, x.x * g.y + x.y * g.x);
+  RegFFT<N>::run<false>(v, sm, a.tw_b, t);
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const float2 g = __ldg(&a.gb[t + T * q]);
+    v[q] = make_float2(v[q].x * g.x - v[q].y * g.y, v[q].x * g.y + v[q].y * g.x);
   }
-  __syncthreads();
-  smem_fft<N, kThreadsB, true>(sm, a.tw_b);
+  RegFFT<N>::run<true>(v, sm, a.tw_b_inv, t);
   const int nout = min(a.b_out, kOverlap + a.spp - j0);
-  const size_t o0 = (size_t)f * a.spp + (size_t)(j0 - kOverlap);
-  for (int i = threadIdx.x; i < nout; i += kThreadsB) {
-    const float2 v = sm[pidx(a.b_pos + i)];
-    a.video[o0 + i] = v.x + a.corr_video;
-    a.sync[o0 + i] = v.y + a.corr_sync;
+  float* video_out = a.video + (f * a.spp + (j0 - kOverlap));
+  float* sync_out = a.sync + (f * a.spp + (j0 - kOverlap));
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int i = t + T * q - a.b_pos;
+    if (i >= 0 && i < nout) {
+      video_out[i] = v[q].x + a.corr_video;
+      sync_out[i] = v[q].y + a.corr_sync;
+    }
   }
 }
 

@@ -219,6 +219,10 @@ bool Context::init(const cuvhs_config& c) {
   d_twb = A((float2*)nullptr, des.tw_b.size());
   d_twc = A((float2*)nullptr, des.tw_c.size());
   d_twl = A((float2*)nullptr, des.tw_line.size());
+  d_twa_inv = A((float2*)nullptr, des.tw_a.size());
+  d_twb_inv = A((float2*)nullptr, des.tw_b.size());
+  d_twc_inv = A((float2*)nullptr, des.tw_c.size());
+  d_twl_inv = A((float2*)nullptr, des.tw_line.size());
   if (!ok) {
     status = CUVHS_ERR_OUT_OF_MEMORY;
     release();
@@ -270,6 +274,10 @@ bool Context::init(const cuvhs_config& c) {
   upload(d_twb, des.tw_b, stream);
   upload(d_twc, des.tw_c, stream);
   upload(d_twl, des.tw_line, stream);
+  upload(d_twa_inv, des.tw_a, stream);
+  upload(d_twb_inv, des.tw_b, stream);
+  upload(d_twc_inv, des.tw_c, stream);
+  upload(d_twl_inv, des.tw_line, stream);
   if (cudaStreamSynchronize(stream) != cudaSuccess) {
     err = std::string("upload failed: ") + cudaGetErrorString(cudaGetLastError());
     status = CUVHS_ERR_CUDA;
@@ -390,6 +398,8 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   da.gb = d_gb;
   da.tw_a = d_twa;
   da.tw_b = d_twb;
+  da.tw_a_inv = d_twa_inv;
+  da.tw_b_inv = d_twb_inv;
   da.a_pos = des.a_pos;
   da.a_out = des.a_out;
   da.b_pos = des.b_pos;
@@ -453,6 +463,8 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   ca.gc = d_gc;
   ca.tw_c = d_twc;
   ca.tw_line = d_twl;
+  ca.tw_c_inv = d_twc_inv;
+  ca.tw_line_inv = d_twl_inv;
   ca.ll = d_ll;
   ca.total = 0;
   ca.track = d_track;

@@ -1,0 +1,85 @@
+// Register-resident block FFT for one CTA of T = N/16 threads (sm_100a).
+//
+// Thread t owns elements t + T*q, q = 0..15, of an N-point transform, both on
+// entry (natural-order input) and on exit (natural-order output): Stockham
+// passes of radix 16 (and one final radix 2/4/8 when N is not a power of 16)
+// exchange data through a padded shared buffer between passes, but the first
+// pass reads its inputs from registers and the last pass leaves its outputs in
+// registers.  Since the output layout equals the input layout, a forward
+// transform, a per-bin multiply and an inverse transform chain without any
+// shared-memory round trip at the seams, and inputs/outputs move between HBM
+// and registers with coalesced accesses (consecutive threads, consecutive
+// elements).  Twiddles: the per-pass table of smem_fft.cuh (coalesced loads).
+#pragma once
+#include "smem_fft.cuh"
+
+namespace cuvhs {
+
+template <int N>
+struct RegFFT {
+  static constexpr int T = N / 16;
+
+  // One pass of radix R at span NS (> 1).  v holds the 16 values this thread
+  // reads; LAST leaves the results in v in the t + T*q layout.
+  template <int NS, bool INV, bool LAST>
+  __device__ __forceinline__ static void pass(float2 (&v)[16], float2* s, const float2* __restrict__ tw, int t) {
+    constexpr int R = fft_radix(N, NS);
+    constexpr int B = 16 / R;  // butterflies per thread
+    float2 w[B][R];
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      const int j = t + T * b;
+#pragma unroll
+      for (int r = 0; r < R; r++) w[b][r] = s[pidx(j + r * (N / R))];
+    }
+    __syncthreads();  // every read done before this pass (or the caller) overwrites
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      const int j = t + T * b;
+      const int k = j & (NS - 1);
+      const float2* twp = tw + (NS - 16) + k;
+#pragma unroll
+      for (int r = 1; r < R; r++) w[b][r] = cmul_tw<INV>(w[b][r], __ldg(&twp[(r - 1) * NS]));
+      dft<R, INV>(w[b]);
+    }
+    if constexpr (LAST) {
+#pragma unroll
+      for (int b = 0; b < B; b++)
+#pragma unroll
+        for (int r = 0; r < R; r++) v[b + B * r] = w[b][dft_slot<R>(r)];
+    } else {
+#pragma unroll
+      for (int b = 0; b < B; b++) {
+        const int j = t + T * b;
+        const int k = j & (NS - 1);
+        const int base = (j / NS) * NS * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) s[pidx(base + r * NS)] = w[b][dft_slot<R>(r)];
+      }
+      __syncthreads();
+    }
+  }
+
+  template <int NS, bool INV>
+  __device__ __forceinline__ static void rest(float2 (&v)[16], float2* s, const float2* __restrict__ tw, int t) {
+    constexpr int R = fft_radix(N, NS);
+    constexpr bool LAST = NS * R >= N;
+    pass<NS, INV, LAST>(v, s, tw, t);
+    if constexpr (!LAST) rest<NS * R, INV>(v, s, tw, t);
+  }
+
+  // Transform v in place.  The buffer s (fft_pad(N) float2) may be in use by
+  // the caller until this call: the first write waits on a barrier.
+  template <bool INV>
+  __device__ __forceinline__ static void run(float2 (&v)[16], float2* s, const float2* __restrict__ tw, int t) {
+    static_assert(N >= 256 && (N & (N - 1)) == 0, "power of two >= 256");
+    dft<16, INV>(v);  // pass NS = 1: inputs t + T*r are exactly this thread's
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 16; r++) s[pidx(16 * t + r)] = v[dft_slot<16>(r)];
+    __syncthreads();
+    rest<16, INV>(v, s, tw, t);
+  }
+};
+
+}  // namespace cuvhs

@@ -83,7 +83,13 @@ __device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2&
   a3 = csub(t1, t3);
 }
 
-// In-register DFT of size R in natural order.
+// In-register DFT of size R, in place.  Output bin r ends up in v[dft_slot<R>(r)]
+// (a compile-time permutation, free once the loops are unrolled).
+template <int R>
+__host__ __device__ constexpr int dft_slot(int r) {
+  return R == 16 ? 4 * (r & 3) + (r >> 2) : (R == 8 ? 2 * (r & 3) + (r >> 2) : r);
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void dft(float2* v) {
   if constexpr (R == 2) {
@@ -91,23 +97,17 @@ __device__ __forceinline__ void dft(float2* v) {
   } else if constexpr (R == 4) {
     dft4<INV>(v[0], v[1], v[2], v[3]);
   } else if constexpr (R == 8) {
-    // 8 = 4 (n1) x 2 (n2): x[2 n1 + n2]
+    // 8 = 4 (n1) x 2 (n2): x[2 n1 + n2]; bin k1 + 4 k2 lands in v[2 k1 + k2]
     dft4<INV>(v[0], v[2], v[4], v[6]);
     dft4<INV>(v[1], v[3], v[5], v[7]);
     v[3] = rot<8, 1, INV>(v[3]);
     v[5] = rot<8, 2, INV>(v[5]);
     v[7] = rot<8, 3, INV>(v[7]);
-    float2 o[8];
 #pragma unroll
-    for (int k1 = 0; k1 < 4; k1++) {
-      float2 a = v[2 * k1], b = v[2 * k1 + 1];
-      o[k1] = cadd(a, b);
-      o[k1 + 4] = csub(a, b);
-    }
-#pragma unroll
-    for (int i = 0; i < 8; i++) v[i] = o[i];
+    for (int k1 = 0; k1 < 4; k1++) dft2<INV>(v[2 * k1], v[2 * k1 + 1]);
   } else if constexpr (R == 16) {
-    // 16 = 4 (n1) x 4 (n2): x[4 n1 + n2]; A[n2][k1] in v[4 k1 + n2]
+    // 16 = 4 (n1) x 4 (n2): x[4 n1 + n2]; A[n2][k1] in v[4 k1 + n2];
+    // bin k1 + 4 k2 lands in v[4 k1 + k2]
 #pragma unroll
     for (int n2 = 0; n2 < 4; n2++) dft4<INV>(v[n2], v[4 + n2], v[8 + n2], v[12 + n2]);
     v[4 + 1] = rot<16, 1, INV>(v[4 + 1]);
@@ -119,18 +119,8 @@ __device__ __forceinline__ void dft(float2* v) {
     v[12 + 1] = rot<16, 3, INV>(v[12 + 1]);
     v[12 + 2] = rot<16, 6, INV>(v[12 + 2]);
     v[12 + 3] = rot<16, 9, INV>(v[12 + 3]);
-    float2 o[16];
 #pragma unroll
-    for (int k1 = 0; k1 < 4; k1++) {
-      float2 a0 = v[4 * k1], a1 = v[4 * k1 + 1], a2 = v[4 * k1 + 2], a3 = v[4 * k1 + 3];
-      dft4<INV>(a0, a1, a2, a3);
-      o[k1] = a0;
-      o[k1 + 4] = a1;
-      o[k1 + 8] = a2;
-      o[k1 + 12] = a3;
-    }
-#pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = o[i];
+    for (int k1 = 0; k1 < 4; k1++) dft4<INV>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
   }
 }
 
@@ -171,7 +161,7 @@ __device__ __forceinline__ void fft_pass(float2* s, const float2* __restrict__ t
       const int k = j & (NS - 1);
       const int base = (j / NS) * NS * R + k;
 #pragma unroll
-      for (int r = 0; r < R; r++) s[pidx(base + r * NS)] = v[p][r];
+      for (int r = 0; r < R; r++) s[pidx(base + r * NS)] = v[p][dft_slot<R>(r)];
     }
   }
   fft_sync<THREADS>();

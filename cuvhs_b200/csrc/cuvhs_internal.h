@@ -5,9 +5,14 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <condition_variable>
 #include <cstddef>
 #include <cstdint>
+#include <functional>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace cuvhs {
@@ -169,8 +174,13 @@ struct DropoutArgs {
   int* do_lines;
   int* do_starts;
   int* do_ends;
+  unsigned char* cls = nullptr;  // two-pass form: [fields * dropout_class_bytes_per_field()]
 };
+// Fused form: one CTA per field, no scratch beyond env_part.
 void launch_dropouts(const DropoutArgs& a, cudaStream_t st);
+// Two-pass form: wide class kernel over every field, then a per-field scan.
+size_t dropout_class_bytes_per_field();
+void launch_dropouts_two_pass(const DropoutArgs& a, cudaStream_t st);
 
 // ---------------------------------------------------------------- host line locations
 // Per-field pulse validation, mean line length, vertical-blanking anchor and
@@ -183,12 +193,61 @@ struct LineLocState {
   double prev_first_hsync_loc = -1.0;
   double prev_first_hsync_diff = -1.0;
 };
+struct SyncPulse {
+  int start, len;
+};
+struct ValidPulse {
+  int type;
+  SyncPulse p;
+  bool good;
+};
+// The part of a field's line location that needs no carried state: pulse
+// validation and the mean line length.  Fields can be prepared in parallel.
+struct LinePrep {
+  std::vector<ValidPulse> v;
+  double mll = 0.0;
+  int n_raw = 0;
+  double raw0 = 0.0;  // first raw pulse start, the fallback grid origin
+};
 struct FieldLines {
   std::vector<int> starts, lengths, types;  // validated pulses
   std::vector<double> locs;                 // lines_per_frame line starts
   int is_first = -1;
 };
+void prepare_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
+                   LinePrep& out);
+// The stateful part, in field order: vertical-blanking anchor, field order,
+// line snapping, carried-state update.
+void finish_lines(const Format& fmt, const LinePrep& prep, long long field_readloc, LineLocState& st,
+                  FieldLines& out);
 void locate_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
                   long long field_readloc, LineLocState& st, FieldLines& out);
+
+// Fixed pool of host threads for per-field work; run(n, fn) calls fn(i) for
+// i < n across the pool and the caller, and returns when all are done.
+class WorkPool {
+ public:
+  explicit WorkPool(int threads);
+  ~WorkPool();
+  template <typename F>
+  void run(int n, F&& fn) {
+    std::function<void(int)> f(std::forward<F>(fn));
+    run_impl(n, f);
+  }
+  int size() const { return (int)threads_.size() + 1; }
+
+ private:
+  void run_impl(int n, std::function<void(int)>& fn);
+  void worker();
+  std::vector<std::thread> threads_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_cv_;
+  std::function<void(int)>* job_ = nullptr;
+  int n_ = 0;
+  std::atomic<int> next_{0};
+  int active_ = 0;
+  unsigned long long generation_ = 0;
+  bool stop_ = false;
+};
 
 }  // namespace cuvhs

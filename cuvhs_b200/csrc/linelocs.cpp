@@ -12,14 +12,6 @@
 namespace cuvhs {
 namespace {
 
-struct Pulse {
-  int start, len;
-};
-struct Valid {
-  int type;
-  Pulse p;
-  bool good;
-};
 
 struct Windows {  // adaptive pulse-width classes (pipeline.cu:450-477)
   double h_lo, h_hi, e_lo, e_hi, v_lo, v_hi;
@@ -74,14 +66,14 @@ Windows width_windows(const int* lengths, int n, const Format& fmt) {
 
 // Vertical-blanking sequence recogniser over at most 26 pulses from `first`
 // (pipeline.cu:519-609).  Appends to `seq`; true when the sequence closed.
-bool blanking_sequence(const std::vector<Pulse>& raw, size_t first, const Windows& w, int eq_pulses, int line_len,
-                       std::vector<Valid>& seq) {
+bool blanking_sequence(const std::vector<SyncPulse>& raw, size_t first, const Windows& w, int eq_pulses, int line_len,
+                       std::vector<ValidPulse>& seq) {
   bool done = false;
   const double half = eq_pulses / 2.0;
   int vsync_at = -1;
   double hold_until = 0.0, pending = -1.0;
   for (size_t i = first; i < raw.size() && i < first + 26; i++) {
-    const Pulse& p = raw[i];
+    const SyncPulse& p = raw[i];
     const double len = (double)p.len;
     const int cur = seq.empty() ? -1 : seq.back().type;
     int type = -1;
@@ -149,15 +141,15 @@ bool blanking_sequence(const std::vector<Pulse>& raw, size_t first, const Window
 }
 
 // Pulse validation (pipeline.cu:611-648).
-std::vector<Valid> validate(const int* starts, const int* lengths, int n, const Format& fmt) {
-  std::vector<Valid> out;
+std::vector<ValidPulse> validate(const int* starts, const int* lengths, int n, const Format& fmt) {
+  std::vector<ValidPulse> out;
   if (n <= 0) return out;
   const Windows w = width_windows(lengths, n, fmt);
-  std::vector<Pulse> raw((size_t)n);
+  std::vector<SyncPulse> raw((size_t)n);
   for (int i = 0; i < n; i++) raw[i] = {starts[i], lengths[i]};
   int i = 0;
   while (i < n) {
-    const Pulse cur = raw[i];
+    const SyncPulse cur = raw[i];
     if (within((double)cur.len, w.h_lo, w.h_hi)) {
       const bool good =
           !out.empty() && spacing_ok(out.back().type, kHsync, cur.start - out.back().p.start, fmt.samples_per_line);
@@ -183,7 +175,7 @@ std::vector<Valid> validate(const int* starts, const int* lengths, int n, const 
 }
 
 // Mean line length from the longest HSYNC run (pipeline.cu:479-517).
-double mean_line(const std::vector<Valid>& v, double nominal) {
+double mean_line(const std::vector<ValidPulse>& v, double nominal) {
   int best_start = -1, best_len = -1, run_start = -1, run_len = 0;
   for (int i = 0; i < (int)v.size(); i++) {
     if (v[i].type != kHsync) {
@@ -227,7 +219,7 @@ struct Anchor {
 };
 
 // Vertical-blanking anchor and field order (pipeline.cu:650-855).
-Anchor anchor_field(const std::vector<Valid>& v, double mll, const Format& fmt, int prev_first, double prev_off_lines,
+Anchor anchor_field(const std::vector<ValidPulse>& v, double mll, const Format& fmt, int prev_first, double prev_off_lines,
                     double prev_loc, double prev_diff, int confidence) {
   Anchor out;
   if (v.empty() || mll <= 0.0) return out;
@@ -342,7 +334,7 @@ Anchor anchor_field(const std::vector<Valid>& v, double mll, const Format& fmt, 
   if (!used_prediction) prev_diff = (loc - predicted) / mll;
   double hoff = 0.0;
   int hcnt = 0;
-  for (const Valid& p : v) {
+  for (const ValidPulse& p : v) {
     if (p.type != kHsync || !p.good) continue;
     const double line = ((double)p.p.start - loc) / mll + hsync_line;
     const int rl = (int)std::llround(line);
@@ -366,12 +358,12 @@ Anchor anchor_field(const std::vector<Valid>& v, double mll, const Format& fmt, 
 }
 
 // Nominal line grid snapped to the nearest pulse (pipeline.cu:857-893).
-void snap_lines(const std::vector<Valid>& v, double ref_pos, double ref_line, double mll, int nlines,
+void snap_lines(const std::vector<ValidPulse>& v, double ref_pos, double ref_line, double mll, int nlines,
                 std::vector<double>& locs) {
   locs.assign((size_t)nlines, 0.0);
   std::vector<double> ps;
   ps.reserve(v.size());
-  for (const Valid& p : v) ps.push_back((double)p.p.start);
+  for (const ValidPulse& p : v) ps.push_back((double)p.p.start);
   // nearly sorted already (the recogniser revisits two pulses): insertion sort
   for (size_t a = 1; a < ps.size(); a++) {
     const double v = ps[a];
@@ -410,28 +402,33 @@ void snap_lines(const std::vector<Valid>& v, double ref_pos, double ref_line, do
 
 }  // namespace
 
-void locate_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
-                  long long field_readloc, LineLocState& st, FieldLines& out) {
+void prepare_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
+                   LinePrep& out) {
   const int n = std::max(0, std::min(count, kMaxPulses));
-  std::vector<Valid> v = validate(pulse_starts, pulse_lengths, n, fmt);
-  const double mll = mean_line(v, (double)fmt.samples_per_line);
+  out.v = validate(pulse_starts, pulse_lengths, n, fmt);
+  out.mll = mean_line(out.v, (double)fmt.samples_per_line);
+  out.n_raw = n;
+  out.raw0 = n > 0 ? (double)pulse_starts[0] : 0.0;
+}
+
+void finish_lines(const Format& fmt, const LinePrep& prep, long long field_readloc, LineLocState& st,
+                  FieldLines& out) {
+  const std::vector<ValidPulse>& v = prep.v;
+  const double mll = prep.mll;
   double prev_off = 0.0;
   if (st.prev_first_hsync_readloc != -1 && mll > 0.0)
     prev_off = ((double)st.prev_first_hsync_readloc - (double)field_readloc) / mll;
   const Anchor an = anchor_field(v, mll, fmt, st.prev_first_field, prev_off, st.prev_first_hsync_loc,
                                  st.prev_first_hsync_diff, 75);
   const int kept = std::min((int)v.size(), kMaxPulses);
-  out.starts.assign(kMaxPulses, 0);
-  out.lengths.assign(kMaxPulses, 0);
-  out.types.assign(kMaxPulses, kHsync);
+  out.starts.resize(kept);
+  out.lengths.resize(kept);
+  out.types.resize(kept);
   for (int i = 0; i < kept; i++) {
     out.starts[i] = v[i].p.start;
     out.lengths[i] = v[i].p.len;
     out.types[i] = v[i].type;
   }
-  out.starts.resize(kept);
-  out.lengths.resize(kept);
-  out.types.resize(kept);
   if (an.valid) {
     snap_lines(v, an.first_hsync_loc, an.first_hsync_line, mll, fmt.lines_per_frame, out.locs);
     out.is_first = an.first_field;
@@ -442,10 +439,16 @@ void locate_lines(const Format& fmt, const int* pulse_starts, const int* pulse_l
     st.prev_first_hsync_diff = an.hsync_diff;
   } else {
     out.locs.assign((size_t)fmt.lines_per_frame, 0.0);
-    const double ref = n > 0 ? (double)pulse_starts[0] : 0.0;
-    for (int line = 0; line < fmt.lines_per_frame; line++) out.locs[line] = ref + mll * (double)line;
+    for (int line = 0; line < fmt.lines_per_frame; line++) out.locs[line] = prep.raw0 + mll * (double)line;
     out.is_first = st.prev_first_field >= 0 ? (1 - st.prev_first_field) : 1;
   }
+}
+
+void locate_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
+                  long long field_readloc, LineLocState& st, FieldLines& out) {
+  LinePrep prep;
+  prepare_lines(fmt, pulse_starts, pulse_lengths, count, prep);
+  finish_lines(fmt, prep, field_readloc, st, out);
 }
 
 }  // namespace cuvhs

@@ -88,9 +88,9 @@ void Context::begin_stage(int stage, cudaEvent_t& a) {
   cudaEventRecord(a, stream);
 }
 
-void Context::end_stage(int stage, cudaEvent_t a) {
-  stage_launches[stage]++;
-  launches++;
+void Context::end_stage(int stage, cudaEvent_t a, int kernels) {
+  stage_launches[stage] += kernels;
+  launches += kernels;
   if (!timing || !a) return;
   cudaEvent_t b = next_event();
   cudaEventRecord(b, stream);
@@ -165,7 +165,8 @@ bool Context::init(const cuvhs_config& c) {
   spp = fmt.spp;
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
-  const size_t per_field = (size_t)spp * (1 + 4 * 5) + (size_t)263 * 910 * 4 + 263 * kBurstLen * 4 + 65536;
+  const size_t per_field = (size_t)spp * (1 + 4 * 5) + (size_t)263 * 910 * 4 + 263 * kBurstLen * 4 + 65536 +
+                           dropout_class_bytes_per_field();
   int b = c.batch_fields;
   if (b <= 0) {
     b = (int)std::min<size_t>((size_t)(free_b * 0.5) / per_field, 2048);
@@ -176,6 +177,10 @@ bool Context::init(const cuvhs_config& c) {
   const int cap_fields = (int)std::min<long long>(INT_MAX / 2 / (long long)spp, 1 << 20);
   if (b > cap_fields) b = cap_fields;
   batch = b;
+  {
+    const int hw = (int)std::thread::hardware_concurrency();
+    pool.reset(new WorkPool(std::max(0, std::min(hw - 1, 15))));
+  }
   if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) {
     err = "cudaStreamCreate failed";
     status = CUVHS_ERR_CUDA;
@@ -212,6 +217,7 @@ bool Context::init(const cuvhs_config& c) {
   d_do_lines = A((int*)nullptr, (size_t)batch * kMaxDropouts);
   d_do_starts = A((int*)nullptr, (size_t)batch * kMaxDropouts);
   d_do_ends = A((int*)nullptr, (size_t)batch * kMaxDropouts);
+  d_do_cls = A((unsigned char*)nullptr, (size_t)batch * dropout_class_bytes_per_field());
   d_ga = A((float2*)nullptr, des.ga.size());
   d_gb = A((float2*)nullptr, des.gb.size());
   d_gc = A((float*)nullptr, des.gc.size());
@@ -440,7 +446,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     cudaEvent_t ev_;
     begin_stage(kStageEdges, ev_);
     launch_edges(d_sync, total_chunk, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, stream);
-    end_stage(kStageEdges, ev_);
+    end_stage(kStageEdges, ev_, 3);
   }
   const int guess = std::min(edge_cap, T * kEdgeGuessPerField);
   cudaMemcpyAsync(hp_counts, d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream);
@@ -561,9 +567,10 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     dbg_k2bl.assign((size_t)P * kMaxPulses, 0);
     dbg_k2bt.assign((size_t)P * kMaxPulses, kHsync);
   }
-  std::vector<int> ps, pl;
-  FieldLines fl;
-  for (int f = 0; f < P; f++) {
+  // stateless per-field part (pulses, validation, mean line) on the host pool
+  if ((int)preps.size() < P) preps.resize(P);
+  pool->run(P, [&](int f) {
+    thread_local std::vector<int> ps, pl;
     ps.clear();
     pl.clear();
     const long long off = (long long)offs[f];
@@ -576,13 +583,20 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
         pl.push_back((int)(run_end[i] - run_start[i]));
       }
     }
-    locate_lines(fmt, ps.data(), pl.data(), (int)ps.size(), (long long)(raw_offset + offs[f]), lls, fl);
-    std::copy(fl.locs.begin(), fl.locs.end(), hp_ll + (size_t)f * LPF);
-    h_is_first[f] = fl.is_first;
+    prepare_lines(fmt, ps.data(), pl.data(), (int)ps.size(), preps[f]);
     if (debug) {
       dbg_k2c[f] = (int)ps.size();
       std::copy(ps.begin(), ps.end(), dbg_k2s.begin() + (size_t)f * kMaxPulses);
       std::copy(pl.begin(), pl.end(), dbg_k2l.begin() + (size_t)f * kMaxPulses);
+    }
+  });
+  // stateful part in field order
+  FieldLines fl;
+  for (int f = 0; f < P; f++) {
+    finish_lines(fmt, preps[f], (long long)(raw_offset + offs[f]), lls, fl);
+    std::copy(fl.locs.begin(), fl.locs.end(), hp_ll + (size_t)f * LPF);
+    h_is_first[f] = fl.is_first;
+    if (debug) {
       dbg_k2bc[f] = (int)fl.starts.size();
       std::copy(fl.starts.begin(), fl.starts.end(), dbg_k2bs.begin() + (size_t)f * kMaxPulses);
       std::copy(fl.lengths.begin(), fl.lengths.end(), dbg_k2bl.begin() + (size_t)f * kMaxPulses);
@@ -745,11 +759,12 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   dd.do_lines = d_do_lines;
   dd.do_starts = d_do_starts;
   dd.do_ends = d_do_ends;
+  dd.cls = d_do_cls;
   {
     cudaEvent_t ev_;
     begin_stage(kStageDropouts, ev_);
-    launch_dropouts(dd, stream);
-    end_stage(kStageDropouts, ev_);
+    launch_dropouts_two_pass(dd, stream);
+    end_stage(kStageDropouts, ev_, 2);
   }
   if (!check_cuda("dropouts")) return false;
   // ---- small results back

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -68,6 +69,7 @@ struct Context {
   double* d_metric = nullptr;
   int* d_track = nullptr;
   int *d_do_count = nullptr, *d_do_lines = nullptr, *d_do_starts = nullptr, *d_do_ends = nullptr;
+  unsigned char* d_do_cls = nullptr;
   float2 *d_ga = nullptr, *d_gb = nullptr, *d_twa = nullptr, *d_twb = nullptr, *d_twc = nullptr, *d_twl = nullptr;
   float2 *d_twa_inv = nullptr, *d_twb_inv = nullptr, *d_twc_inv = nullptr, *d_twl_inv = nullptr;
   float* d_gc = nullptr;
@@ -84,6 +86,8 @@ struct Context {
   std::vector<unsigned> h_fall, h_rise;
   std::vector<long long> run_start, run_end;
   std::vector<int> h_is_first, h_phase, computed_track;
+  std::vector<LinePrep> preps;
+  std::unique_ptr<WorkPool> pool;
   // pinned staging
   int* hp_counts = nullptr;
   unsigned *hp_fall = nullptr, *hp_rise = nullptr;
@@ -115,7 +119,7 @@ struct Context {
   size_t pool_used = 0;
   cudaEvent_t next_event();
   void begin_stage(int stage, cudaEvent_t& a);
-  void end_stage(int stage, cudaEvent_t a);
+  void end_stage(int stage, cudaEvent_t a, int kernels = 1);
   void collect_stage_times();
   double host_clock() const;
   void host_phase(int stage, double t0) {

@@ -133,6 +133,7 @@ struct LineArgs {
   uint16_t* luma;  // [P*263*910]
   int out_w, out_h;
   float luma_gain, luma_offset;  // u16 = video_rel * gain + offset
+  const double* col_frac;        // [out_w]: (double)col / (double)out_w
 };
 void launch_hsync_refine(const LineArgs& a, cudaStream_t st);
 void launch_luma(const LineArgs& a, cudaStream_t st);
@@ -156,6 +157,7 @@ struct ChromaArgs {
   uint16_t* chroma;  // [P*263*910]
   float* burst;      // [P*263*kBurstLen] band-passed burst window (scaled)
   double* metric;    // per field burst cancellation metric
+  const double* col_frac;  // [out_w]: (double)col / (double)out_w
 };
 void launch_chroma_prefilter(const ChromaArgs& a, cudaStream_t st);
 // Lines [field0*263, (field0+nfields)*263) of the chunk.

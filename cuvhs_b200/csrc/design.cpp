@@ -12,6 +12,7 @@
 // re-transformed to the block size of a shared-memory overlap-save kernel.
 // The GPU then evaluates the same circular tile convolution block by block in
 // one HBM pass per stage instead of 500k-point transforms.
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -116,6 +117,15 @@ double place_kernel(const std::vector<cd>& k, int neg, int pos, int N, std::vect
   return total > 0 ? std::max(0.0, total - kept) / total : 0.0;
 }
 
+// Kernel half-support for sample rate fs: the filters are specified in Hz, so
+// their time responses stretch in proportion to fs.  per_mhz samples per MHz
+// keep every dropped tap below ~5e-9 of the kernel's peak (below FP32
+// resolution) at 28, 35.8 and 40 MHz; rounded up to a multiple of quantum.
+int half_support(double fs_hz, double per_mhz, int quantum, int cap) {
+  const int n = (int)std::ceil(fs_hz * 1e-6 * per_mhz / quantum) * quantum;
+  return std::min(n, cap);
+}
+
 // Per-pass twiddles of the shared-memory FFT (smem_fft.cuh): pass NS >= 16 of
 // radix R holds W_{NS*R}^{r*k} at (NS - 16) + (r - 1) * NS + k.
 std::vector<float2> twiddles(int n) {
@@ -168,8 +178,7 @@ void Design::build(const Format& fmt) {
       H[k] = bw_bandpass(w, wbl, wbh, 8) * bw_lowpass(w, wl, 8) * bw_highpass(w, wh, 8) * hil;
     }
     std::vector<cd> g = host_dft(H, +1);  // unnormalised inverse, as the reference's C2C
-    a_neg = 768;
-    a_pos = 768;
+    a_neg = a_pos = half_support(fs, 13.7, 64, 1024);
     a_out = kNa - a_neg - a_pos - 1;
     std::vector<cd> blk;
     a_tail = place_kernel(g, a_neg, a_pos, kNa, blk);
@@ -214,7 +223,7 @@ void Design::build(const Format& fmt) {
     std::vector<cd> hv = host_dft(FV, +1), hs = host_dft(FS, +1);
     std::vector<cd> c(tile);
     for (int n = 0; n < tile; n++) c[n] = cd(hv[n].real(), hs[n].real());
-    b_neg = b_pos = 1024;
+    b_neg = b_pos = half_support(fs, 25.6, 64, 2048);
     b_out = kNb - b_neg - b_pos;
     std::vector<cd> blk;
     b_tail = place_kernel(c, b_neg, b_pos, kNb, blk);
@@ -241,7 +250,7 @@ void Design::build(const Format& fmt) {
     for (int k = rb; k < ctile; k++) H[k] = std::conj(H[ctile - k]);
     std::vector<cd> h = host_dft(H, +1);
     for (auto& v : h) v = cd(v.real(), 0.0);
-    c_half = 4096;
+    c_half = half_support(fs, 102.0, 1024, 6144);
     c_out = kNc - 2 * c_half;
     std::vector<cd> blk;
     c_tail = place_kernel(h, c_half, c_half, kNc, blk);

@@ -67,7 +67,7 @@ __device__ __forceinline__ float het_sample(const ChromaArgs& a, int gl, int c) 
   if (row + 1 >= a.lines_per_frame) return 0.0f;
   const double a0 = a.ll[(size_t)field * a.lines_per_frame + row];
   const double a1 = a.ll[(size_t)field * a.lines_per_frame + row + 1];
-  const double coord = a0 + ((double)c / (double)a.out_w) * (a1 - a0);
+  const double coord = a0 + __ldg(&a.col_frac[c]) * (a1 - a0);
   const int ci = (int)coord;
   if (ci < 1 || (long long)ci + 2 >= a.total) return 0.0f;
   const float x = (float)(coord - (double)ci);

@@ -12,56 +12,101 @@
 namespace cuvhs {
 namespace {
 
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kHsyncWarps = 4;   // lines per 128-thread CTA
+constexpr int kLumaThreads = 128;
+
+__device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(kFull, v, src); }
+
 // First sample pair (i-1, i) in [start, start+count) with prev >= target > cur;
-// returns the linearly interpolated crossing or -1.
-__device__ double falling_cross(const float* __restrict__ s, int start, int count, double target, long long total) {
+// returns the linearly interpolated crossing or -1.  The warp tests 32 pairs
+// per step and takes the lowest hit, so the result is the sequential scan's.
+__device__ double falling_cross(const float* __restrict__ s, int start, int count, double target, long long total,
+                                int lane) {
   if (start < 0 || (long long)start + count > total || count < 2) return -1.0;
-  for (int i = start + 1; i < start + count; i++) {
-    const double p = s[i - 1], q = s[i];
-    if (p >= target && q < target) {
-      const double a = p - target, b = q - target;
-      const double fr = (a - b != 0.0) ? (a / (a - b)) : 0.0;
-      return (double)(i - 1) + fr;
+  for (int base = start + 1; base < start + count; base += 32) {
+    const int i = base + lane;
+    double p = 0.0, q = 0.0;
+    bool hit = false;
+    if (i < start + count) {
+      p = s[i - 1];
+      q = s[i];
+      hit = p >= target && q < target;
+    }
+    const unsigned m = __ballot_sync(kFull, hit);
+    if (m) {
+      const int src = __ffs(m) - 1;
+      double r = 0.0;
+      if (lane == src) {
+        const double a = p - target, b = q - target;
+        const double fr = (a - b != 0.0) ? (a / (a - b)) : 0.0;
+        r = (double)(i - 1) + fr;
+      }
+      return shfl_d(r, src);
     }
   }
   return -1.0;
 }
 
-__device__ double rising_cross(const float* __restrict__ s, int start, int count, double target, long long total) {
+__device__ double rising_cross(const float* __restrict__ s, int start, int count, double target, long long total,
+                               int lane) {
   if (start < 0 || (long long)start + count > total || count < 2) return -1.0;
   if ((double)s[start] > target) return -1.0;
-  for (int i = start + 1; i < start + count; i++) {
-    const double p = s[i - 1], q = s[i];
-    if (p < target && q >= target) {
-      const double a = target - p, b = target - q;
-      const double fr = (a + b != 0.0) ? (a / (a - b)) : 0.0;
-      return (double)(i - 1) + fr;
+  for (int base = start + 1; base < start + count; base += 32) {
+    const int i = base + lane;
+    double p = 0.0, q = 0.0;
+    bool hit = false;
+    if (i < start + count) {
+      p = s[i - 1];
+      q = s[i];
+      hit = p < target && q >= target;
+    }
+    const unsigned m = __ballot_sync(kFull, hit);
+    if (m) {
+      const int src = __ffs(m) - 1;
+      double r = 0.0;
+      if (lane == src) {
+        const double a = target - p, b = target - q;
+        const double fr = (a + b != 0.0) ? (a / (a - b)) : 0.0;
+        r = (double)(i - 1) + fr;
+      }
+      return shfl_d(r, src);
     }
   }
   return -1.0;
 }
 
-// Order statistic n/2 of the window (the upper median for even n), n <= 64.
-__device__ double window_median(const float* __restrict__ s, int start, int count, long long total) {
+// Order statistic n/2 of the window (the upper median for even n), n <= 64:
+// lane l ranks samples l and l+32 against the whole window; the sample with
+// (#smaller <= n/2 < #smaller-or-equal) is the order statistic, whichever
+// duplicate supplies it.
+__device__ double window_median(const float* __restrict__ s, int start, int count, long long total, int lane) {
   if (start < 0 || (long long)start + count > total || count <= 0) return 0.0;
   const int n = min(count, 64);
-  float buf[64];
-  for (int i = 0; i < n; i++) buf[i] = s[start + i];
   const int mid = n / 2;
-  for (int i = 0; i <= mid; i++) {
-    int m = i;
-    for (int j = i + 1; j < n; j++)
-      if (buf[j] < buf[m]) m = j;
-    const float t = buf[i];
-    buf[i] = buf[m];
-    buf[m] = t;
+  const float x0 = lane < n ? s[start + lane] : 0.0f;
+  const float x1 = lane + 32 < n ? s[start + lane + 32] : 0.0f;
+  int lt0 = 0, le0 = 0, lt1 = 0, le1 = 0;
+  for (int j = 0; j < n; j++) {
+    const float y = __shfl_sync(kFull, j < 32 ? x0 : x1, j & 31);
+    lt0 += y < x0;
+    le0 += y <= x0;
+    lt1 += y < x1;
+    le1 += y <= x1;
   }
-  return (double)buf[mid];
+  const bool h0 = lane < n && lt0 <= mid && mid < le0;
+  const bool h1 = lane + 32 < n && lt1 <= mid && mid < le1;
+  const unsigned m0 = __ballot_sync(kFull, h0), m1 = __ballot_sync(kFull, h1);
+  const float v = m0 ? __shfl_sync(kFull, x0, __ffs(m0) - 1) : __shfl_sync(kFull, x1, __ffs(m1) - 1);
+  return (double)v;
 }
 
-__global__ void hsync_kernel(LineArgs a) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= a.fields * a.lines_per_frame) return;
+// One warp per line location (lines from the first active line to the end of
+// the frame table).
+__global__ void __launch_bounds__(32 * kHsyncWarps) hsync_kernel(LineArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int idx = blockIdx.x * kHsyncWarps + (threadIdx.x >> 5);
+  if (idx >= a.fields * a.lines_per_frame) return;  // whole warp
   const int line = idx % a.lines_per_frame;
   if (line < a.active_line_start) return;
   const float* s = a.sync;
@@ -70,28 +115,28 @@ __global__ void hsync_kernel(LineArgs a) {
   const double orig = a.ll[idx];
   const int ou = (int)(us + 0.5);
   // leading (falling) edge
-  const double zc = falling_cross(s, (int)(orig - ou), ou * 2, thr, a.total);
+  const double zc = falling_cross(s, (int)(orig - ou), ou * 2, thr, a.total, lane);
   double left = -1.0;
   if (zc >= 0.0) {
     const int zi = (int)(zc + 0.5);
-    const double sync_lv = window_median(s, zi + (int)(1.0 * us), (int)(1.5 * us), a.total);
-    const double porch_lv = window_median(s, zi + (int)(8.0 * us), (int)(1.0 * us), a.total);
+    const double sync_lv = window_median(s, zi + (int)(1.0 * us), (int)(1.5 * us), a.total, lane);
+    const double porch_lv = window_median(s, zi + (int)(8.0 * us), (int)(1.0 * us), a.total, lane);
     if (porch_lv > sync_lv) {
       const double mid = (sync_lv + porch_lv) / 2.0;
-      const double zc2 = falling_cross(s, (int)(orig - ou * 2), (int)(us * 4), mid, a.total);
+      const double zc2 = falling_cross(s, (int)(orig - ou * 2), (int)(us * 4), mid, a.total, lane);
       if (zc2 >= 0.0 && fabs(zc2 - zc) <= us * 0.5) left = zc2;
     }
   }
   // trailing (rising) edge
   double right = -1.0;
-  const double rx = rising_cross(s, (int)(orig + hw - us), (int)(hw * 2), thr, a.total);
+  const double rx = rising_cross(s, (int)(orig + hw - us), (int)(hw * 2), thr, a.total, lane);
   if (rx >= 0.0) {
     const int zfi = (int)(rx - hw + 0.5);
-    const double rs = window_median(s, zfi + (int)(1.0 * us), (int)(1.5 * us), a.total);
-    const double rp = window_median(s, zfi + (int)(hw + 1.0 * us), (int)(1.0 * us), a.total);
+    const double rs = window_median(s, zfi + (int)(1.0 * us), (int)(1.5 * us), a.total, lane);
+    const double rp = window_median(s, zfi + (int)(hw + 1.0 * us), (int)(1.0 * us), a.total, lane);
     if (rp > rs) {
       const double rmid = (rs + rp) / 2.0;
-      const double zc2r = rising_cross(s, (int)(orig + hw - us), (int)(hw * 2), rmid, a.total);
+      const double zc2r = rising_cross(s, (int)(orig + hw - us), (int)(hw * 2), rmid, a.total, lane);
       if (zc2r >= 0.0 && fabs(zc2r - rx) <= us * 0.5) {
         const double cand = rx - hw + a.right_edge_offset;
         const double ref = (left >= 0.0) ? left : orig;
@@ -99,28 +144,32 @@ __global__ void hsync_kernel(LineArgs a) {
       }
     }
   }
-  if (right >= 0.0) a.ll[idx] = right;
-  else if (left >= 0.0) a.ll[idx] = left;
+  if (lane == 0) {
+    if (right >= 0.0) a.ll[idx] = right;
+    else if (left >= 0.0) a.ll[idx] = left;
+  }
 }
 
-__global__ void luma_kernel(LineArgs a) {
+// One CTA per output row: the row's two line starts are read once, the column
+// fractions col/W come from a table (the same FP64 quotient), and consecutive
+// threads write consecutive pixels.
+__global__ void __launch_bounds__(kLumaThreads) luma_kernel(LineArgs a) {
   const int W = a.out_w, H = a.out_h;
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long long)a.fields * H * W) return;
-  const int field = (int)(idx / (H * W));
-  const int rem = (int)(idx % (H * W));
-  const int row = rem / W, col = rem % W;
-  uint16_t out;
+  const int grow = blockIdx.x;  // field * H + row
+  const int field = grow / H, row = grow % H;
+  uint16_t* out = a.luma + (size_t)grow * W;
   if (row + 1 >= a.lines_per_frame) {
-    out = 1024;
-  } else {
-    const double a0 = a.ll[(size_t)field * a.lines_per_frame + row];
-    const double a1 = a.ll[(size_t)field * a.lines_per_frame + row + 1];
-    const double coord = a0 + ((double)col / (double)W) * (a1 - a0);
+    for (int col = threadIdx.x; col < W; col += kLumaThreads) out[col] = 1024;
+    return;
+  }
+  const double a0 = a.ll[(size_t)field * a.lines_per_frame + row];
+  const double a1 = a.ll[(size_t)field * a.lines_per_frame + row + 1];
+  const double span = a1 - a0;
+  for (int col = threadIdx.x; col < W; col += kLumaThreads) {
+    const double coord = a0 + __ldg(&a.col_frac[col]) * span;
     const int ci = (int)coord;
-    if (ci < 1 || (long long)ci + 2 >= a.total) {
-      out = 1024;
-    } else {
+    uint16_t o = 1024;
+    if (ci >= 1 && (long long)ci + 2 < a.total) {
       const float x = (float)(coord - (double)ci);
       const float p0 = __ldg(&a.video[ci - 1]), p1 = __ldg(&a.video[ci]);
       const float p2 = __ldg(&a.video[ci + 1]), p3 = __ldg(&a.video[ci + 2]);
@@ -130,10 +179,10 @@ __global__ void luma_kernel(LineArgs a) {
       const float hz = p1 + 0.5f * x * (c1 + x * (c2 + x * c3));
       float v = hz * a.luma_gain + a.luma_offset;
       v = fminf(fmaxf(v, 0.0f), 65535.0f);
-      out = (uint16_t)(v + 0.5f);
+      o = (uint16_t)(v + 0.5f);
     }
+    out[col] = o;
   }
-  a.luma[idx] = out;
 }
 
 }  // namespace
@@ -141,13 +190,13 @@ __global__ void luma_kernel(LineArgs a) {
 void launch_hsync_refine(const LineArgs& a, cudaStream_t st) {
   const int n = a.fields * a.lines_per_frame;
   if (n <= 0) return;
-  hsync_kernel<<<(n + 127) / 128, 128, 0, st>>>(a);
+  hsync_kernel<<<(n + kHsyncWarps - 1) / kHsyncWarps, 32 * kHsyncWarps, 0, st>>>(a);
 }
 
 void launch_luma(const LineArgs& a, cudaStream_t st) {
-  const long long n = (long long)a.fields * a.out_h * a.out_w;
-  if (n <= 0) return;
-  luma_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a);
+  const int rows = a.fields * a.out_h;
+  if (rows <= 0) return;
+  luma_kernel<<<rows, kLumaThreads, 0, st>>>(a);
 }
 
 }  // namespace cuvhs

@@ -284,6 +284,10 @@ bool Context::init(const cuvhs_config& c) {
   upload(d_twb_inv, des.tw_b, stream);
   upload(d_twc_inv, des.tw_c, stream);
   upload(d_twl_inv, des.tw_line, stream);
+  std::vector<double> col_frac(fmt.output_line_len);
+  for (int c = 0; c < fmt.output_line_len; c++) col_frac[c] = (double)c / (double)fmt.output_line_len;
+  d_col_frac = A((double*)nullptr, col_frac.size());
+  upload(d_col_frac, col_frac, stream);
   if (cudaStreamSynchronize(stream) != cudaSuccess) {
     err = std::string("upload failed: ") + cudaGetErrorString(cudaGetLastError());
     status = CUVHS_ERR_CUDA;
@@ -485,6 +489,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   ca.chroma = d_chroma;
   ca.burst = d_burst;
   ca.metric = d_metric;
+  ca.col_frac = d_col_frac;
   if (debug) {
     dbg_demod.resize(std::min<size_t>((size_t)T * spp, (size_t)debug_tiles * spp));
     cudaMemcpyAsync(dbg_demod.data(), d_dem, dbg_demod.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
@@ -629,6 +634,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   la.out_h = H;
   la.luma_gain = (float)(fmt.output_scale / fmt.hz_ire);
   la.luma_offset = (float)(-fmt.vsync_ire * fmt.output_scale + fmt.output_zero);
+  la.col_frac = d_col_frac;
   {
     cudaEvent_t ev_;
     begin_stage(kStageHsync, ev_);

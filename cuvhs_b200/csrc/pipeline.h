@@ -70,6 +70,7 @@ struct Context {
   int* d_track = nullptr;
   int *d_do_count = nullptr, *d_do_lines = nullptr, *d_do_starts = nullptr, *d_do_ends = nullptr;
   unsigned char* d_do_cls = nullptr;
+  double* d_col_frac = nullptr;
   float2 *d_ga = nullptr, *d_gb = nullptr, *d_twa = nullptr, *d_twb = nullptr, *d_twc = nullptr, *d_twl = nullptr;
   float2 *d_twa_inv = nullptr, *d_twb_inv = nullptr, *d_twc_inv = nullptr, *d_twl_inv = nullptr;
   float* d_gc = nullptr;

@@ -216,10 +216,19 @@ class Decoder:
         if st != 0:
             raise CuvhsError(st, lib.cuvhs_last_error(self._h).decode())
 
-    def _alloc_output(self, max_fields):
+    def _alloc_output(self, max_fields, pinned=False):
+        if pinned:
+            import torch
+            planes = [torch.empty((max_fields, FIELD_H, FIELD_W), dtype=torch.int16).pin_memory() for _ in range(2)]
+            luma, chroma = (p.numpy().view(np.uint16) for p in planes)
+        else:
+            planes = []
+            luma = np.empty((max_fields, FIELD_H, FIELD_W), np.uint16)
+            chroma = np.empty((max_fields, FIELD_H, FIELD_W), np.uint16)
         bufs = {
-            "luma": np.empty((max_fields, FIELD_H, FIELD_W), np.uint16),
-            "chroma": np.empty((max_fields, FIELD_H, FIELD_W), np.uint16),
+            "planes": planes,
+            "luma": luma,
+            "chroma": chroma,
             "fields": (FieldInfo * max_fields)(),
             "dl": np.empty(max_fields * MAX_DROPOUTS_PER_FIELD, np.int32),
             "ds": np.empty(max_fields * MAX_DROPOUTS_PER_FIELD, np.int32),
@@ -246,18 +255,29 @@ class Decoder:
         jl = lib.cuvhs_json(self._h, ctypes.byref(out), None, 0)
         jb = ctypes.create_string_buffer(int(jl) + 1)
         lib.cuvhs_json(self._h, ctypes.byref(out), jb, jl + 1)
+        own = (lambda a: a.copy()) if bufs["planes"] else (lambda a: a)  # pinned staging is not kept
         return DecodeResult(
-            luma=bufs["luma"][:n], chroma=bufs["chroma"][:n],
+            luma=own(bufs["luma"][:n]), chroma=own(bufs["chroma"][:n]),
             file_loc=np.array([fi[i].file_loc for i in range(n)], np.uint64),
             is_first_field=np.array([fi[i].is_first_field for i in range(n)], np.int32),
             field_phase_id=np.array([fi[i].field_phase_id for i in range(n)], np.int32),
             dropouts=dropouts, json=jb.value.decode())
 
-    def decode_capture(self, samples: np.ndarray) -> DecodeResult:
+    def decode_capture(self, samples: np.ndarray, pinned: bool = False) -> DecodeResult:
+        """Decode a whole capture.  pinned=True stages the input and the output
+        planes in page-locked memory, which lets the library overlap the
+        host<->device copies with the decode."""
         samples = np.ascontiguousarray(samples, dtype=np.uint8)
         max_fields = samples.size // self.samples_per_field + 2
-        out, bufs = self._alloc_output(max_fields)
-        self._check(lib.cuvhs_decode_capture(self._h, samples.ctypes.data, samples.size, ctypes.byref(out)))
+        out, bufs = self._alloc_output(max_fields, pinned)
+        if pinned:
+            import torch
+            pin = torch.from_numpy(samples).pin_memory()
+            bufs["input"] = pin
+            src = pin.data_ptr()
+        else:
+            src = samples.ctypes.data
+        self._check(lib.cuvhs_decode_capture(self._h, src, samples.size, ctypes.byref(out)))
         return self._result(out, bufs)
 
     def decode_chunk(self, samples: np.ndarray, raw_offset: int, num_fields: int):

@@ -38,7 +38,7 @@ cuvhs_status append_chunk(Context& c, const ChunkResult& r, cuvhs_output* out) {
   for (int i = 0; i < r.fields; i++) need += (size_t)r.field_info[i].dropout_count;
   if (out->dropouts_out + need > out->max_dropouts && need > 0)
     return fail(c, CUVHS_ERR_CAPACITY, "output dropout buffer too small");
-  if (r.fields > 0) {
+  if (r.fields > 0 && !r.outputs_copied) {
     if (out->luma)
       cudaMemcpyAsync(out->luma + out->fields_out * F, c.d_luma, (size_t)r.fields * F * sizeof(uint16_t),
                       cudaMemcpyDeviceToHost, c.stream);
@@ -62,6 +62,34 @@ cuvhs_status append_chunk(Context& c, const ChunkResult& r, cuvhs_output* out) {
   }
   out->next_raw_offset = r.next_raw_offset;
   return CUVHS_OK;
+}
+
+bool page_locked(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
+// Decode one chunk into `out`.  When the caller's planes are page-locked and
+// have room for every field the chunk can produce, the decoder copies each
+// plane there as soon as it is final (overlapping the rest of the decode);
+// otherwise the planes are copied after the decode.
+cuvhs_status decode_into(Context& c, const uint8_t* src, size_t n_avail, uint64_t raw_offset, int num_fields,
+                         cuvhs_output* out) {
+  const size_t F = (size_t)c.fmt.output_line_len * c.fmt.output_field_lines;
+  uint16_t *dl = nullptr, *dc = nullptr;
+  if (out->fields_out + (size_t)num_fields <= out->max_fields) {
+    if (page_locked(out->luma)) dl = out->luma + out->fields_out * F;
+    if (page_locked(out->chroma)) dc = out->chroma + out->fields_out * F;
+    if ((out->luma && !dl) || (out->chroma && !dc)) dl = dc = nullptr;  // both or neither
+  }
+  ChunkResult r;
+  if (!c.decode_chunk(src, false, n_avail, raw_offset, num_fields, r, dl, dc)) return c.status;
+  return append_chunk(c, r, out);
 }
 
 template <typename T>
@@ -136,9 +164,7 @@ cuvhs_status cuvhs_decode_chunk(cuvhs_ctx* ctx, const uint8_t* samples, size_t n
   if (!ctx || !samples || !out) return CUVHS_ERR_INVALID_ARGUMENT;
   Context& c = ctx->c;
   c.status = CUVHS_OK;
-  ChunkResult r;
-  if (!c.decode_chunk(samples, false, n_avail, raw_offset, num_fields, r)) return c.status;
-  return append_chunk(c, r, out);
+  return decode_into(c, samples, n_avail, raw_offset, num_fields, out);
 }
 
 cuvhs_status cuvhs_decode_chunk_device(cuvhs_ctx* ctx, const uint8_t* d_samples, size_t n_avail,
@@ -172,12 +198,15 @@ cuvhs_status cuvhs_decode_capture(cuvhs_ctx* ctx, const uint8_t* samples, size_t
     const int remaining_fields = (int)((n - raw_offset) / spf);
     if (remaining_fields <= 0) break;
     const int nf = std::min(c.batch, remaining_fields);
-    ChunkResult r;
-    if (!c.decode_chunk(samples + raw_offset, false, n - raw_offset, raw_offset, nf, r)) return c.status;
-    if (r.fields == 0) break;
-    cuvhs_status s = append_chunk(c, r, out);
+    const size_t before = out->fields_out;
+    const uint64_t prev_next = out->next_raw_offset;
+    cuvhs_status s = decode_into(c, samples + raw_offset, n - raw_offset, raw_offset, nf, out);
     if (s != CUVHS_OK) return s;
-    raw_offset = r.next_raw_offset;
+    if (out->fields_out == before) {
+      out->next_raw_offset = prev_next;
+      break;
+    }
+    raw_offset = out->next_raw_offset;
   }
   return CUVHS_OK;
 }

@@ -110,7 +110,8 @@ struct DemodArgs {
   float* video;    // [T*spp] video - ire0
   float* sync;     // [T*spp] sync - ire0
 };
-void launch_k1a(const DemodArgs& a, cudaStream_t st);
+// K1a over tiles [f0, f0 + nf).
+void launch_k1a(const DemodArgs& a, int f0, int nf, cudaStream_t st);
 void launch_k1b(const DemodArgs& a, cudaStream_t st);
 
 // Threshold edges of the sync signal in sample order: falling (x<=thr after
@@ -180,9 +181,12 @@ struct DropoutArgs {
 };
 // Fused form: one CTA per field, no scratch beyond env_part.
 void launch_dropouts(const DropoutArgs& a, cudaStream_t st);
-// Two-pass form: wide class kernel over every field, then a per-field scan.
+// Two-pass form: wide class kernel over every field, then a per-field scan
+// that maps the entries and conceals the luma; chroma concealment follows
+// once the chroma planes are final.
 size_t dropout_class_bytes_per_field();
 void launch_dropouts_two_pass(const DropoutArgs& a, cudaStream_t st);
+void launch_dropout_conceal_chroma(const DropoutArgs& a, cudaStream_t st);
 
 // ---------------------------------------------------------------- host line locations
 // Per-field pulse validation, mean line length, vertical-blanking anchor and
@@ -203,25 +207,48 @@ struct ValidPulse {
   SyncPulse p;
   bool good;
 };
+constexpr int kAnchorConfidence = 75;  // pattern vote (percent) that fixes the field order
+// Vertical-blanking pulses of one field and their half-line pattern.
+struct BlankingScan {
+  int vb_pulse[8];
+  double order_len[4];
+  double agree = 0.0, seen = 0.0;
+};
+// First-hsync anchor of one field for a given field order.
+struct AnchorFit {
+  int cnt = 0;                 // estimates combined (0: no anchor)
+  bool used_prediction = false;
+  double loc_round = 0.0;      // estimate before the hsync refinement
+  double loc = 0.0;            // first-hsync location
+  double hsync_line = 0.0;
+};
 // The part of a field's line location that needs no carried state: pulse
-// validation and the mean line length.  Fields can be prepared in parallel.
+// validation, the mean line length, the blanking scan and, when the field
+// order follows from the field's own pattern, the anchor and snapped grid.
+// Fields can be prepared in parallel.
 struct LinePrep {
   std::vector<ValidPulse> v;
   double mll = 0.0;
   int n_raw = 0;
   double raw0 = 0.0;  // first raw pulse start, the fallback grid origin
+  BlankingScan scan;
+  int spec_first = -1;  // field order of the precomputed anchor, -1 if none
+  AnchorFit spec;
 };
 struct FieldLines {
   std::vector<int> starts, lengths, types;  // validated pulses
   std::vector<double> locs;                 // lines_per_frame line starts
   int is_first = -1;
 };
-void prepare_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
-                   LinePrep& out);
-// The stateful part, in field order: vertical-blanking anchor, field order,
-// line snapping, carried-state update.
-void finish_lines(const Format& fmt, const LinePrep& prep, long long field_readloc, LineLocState& st,
-                  FieldLines& out);
+// spec_locs (lines_per_frame, may be null) receives the precomputed grid.
+void prepare_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count, LinePrep& out,
+                   double* spec_locs);
+// The stateful part, in field order: field order, vertical-blanking anchor,
+// line snapping, carried-state update.  locs (lines_per_frame) must hold what
+// prepare_lines wrote to spec_locs; it receives the field's line starts.
+// pulses (optional) receives the validated pulses.
+void finish_lines(const Format& fmt, const LinePrep& prep, long long field_readloc, LineLocState& st, double* locs,
+                  FieldLines* pulses, int* is_first);
 void locate_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
                   long long field_readloc, LineLocState& st, FieldLines& out);
 

@@ -26,13 +26,13 @@ __device__ __forceinline__ int wrap_tile(int q, int tile) {
 
 // K1a: u8 -> analytic signal -> phase step (FP32 Hz, relative to ire0) + envelope.
 // Thread t holds block samples t + 256*q throughout (RegFFT layout).
-__global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(DemodArgs a) {
+__global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(DemodArgs a, int f_begin) {
   constexpr int N = Design::kNa, T = kThreadsA;
   extern __shared__ float2 sm[];
   __shared__ float2 warp_last[T / 32][16];
   __shared__ double red[T / 32];
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const int f = blockIdx.y;
+  const int f = f_begin + blockIdx.y;
   const int j0 = kOverlap + blockIdx.x * a.a_out;  // first demod output (tile position)
   // chunk positions fit in 32 bits (the batch is capped so T * spp < 2^31)
   const int tile0 = f * a.spp - kOverlap;          // chunk position of tile position 0
@@ -268,10 +268,11 @@ __global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(const float* _
 
 }  // namespace
 
-void launch_k1a(const DemodArgs& a, cudaStream_t st) {
+void launch_k1a(const DemodArgs& a, int f0, int nf, cudaStream_t st) {
+  if (nf <= 0) return;
   const size_t smem = sizeof(float2) * fft_pad(Design::kNa);
-  dim3 grid((a.spp + a.a_out - 1) / a.a_out, a.tiles);
-  k1a_kernel<<<grid, kThreadsA, smem, st>>>(a);
+  dim3 grid((a.spp + a.a_out - 1) / a.a_out, nf);
+  k1a_kernel<<<grid, kThreadsA, smem, st>>>(a, f0);
 }
 
 void launch_k1b(const DemodArgs& a, cudaStream_t st) {

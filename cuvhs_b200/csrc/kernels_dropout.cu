@@ -15,8 +15,10 @@
 //  * two-pass (the decoder): a wide class kernel (one thread per block, every
 //    field at once, the envelope staged through shared memory with coalesced
 //    loads) writes one class byte per block, and a per-field kernel reads the
-//    bytes back from L2 and scans, maps and conceals.  The envelope read -- the
-//    stage's HBM traffic -- runs on every SM.
+//    bytes back from L2, scans, maps and conceals the luma.  The envelope read
+//    -- the stage's HBM traffic -- runs on every SM.  Luma is final once the
+//    luma resampler has run, so it is concealed (and can leave the device)
+//    while chroma is still being decoded; chroma is concealed afterwards.
 //  * fused (cuvhs_dropouts_noalloc): one CTA per field does everything, with
 //    the classes in shared memory, so it needs no scratch beyond the partials.
 #include <cuda_runtime.h>
@@ -108,8 +110,9 @@ __device__ int map_events(const DropoutArgs& a, int f, const int* events, int ne
 }
 
 // Step 5 (one warp): conceal from the line above (below for line 0), groups of
-// 32 entries, every load of a column step before its stores.
-__device__ void conceal(const DropoutArgs& a, int f, int n, int lane) {
+// 32 entries, every load of a column step before its stores.  Planes are
+// independent, so luma and chroma may be concealed in separate passes.
+__device__ void conceal(const DropoutArgs& a, int f, int n, int lane, bool luma, bool chroma) {
   const int H = a.out_h, W = a.out_w;
   const int* ol = a.do_lines + (size_t)f * kMaxDropouts;
   const int* os = a.do_starts + (size_t)f * kMaxDropouts;
@@ -129,9 +132,11 @@ __device__ void conceal(const DropoutArgs& a, int f, int n, int lane) {
     for (int it = 0; it < maxspan; it++) {
       const bool act = it < span;
       uint16_t vl = 0, vc = 0;
-      if (act) { vl = lf[src * W + sx + it]; vc = cf[src * W + sx + it]; }
+      if (act && luma) vl = lf[src * W + sx + it];
+      if (act && chroma) vc = cf[src * W + sx + it];
       __syncwarp();
-      if (act) { lf[line * W + sx + it] = vl; cf[line * W + sx + it] = vc; }
+      if (act && luma) lf[line * W + sx + it] = vl;
+      if (act && chroma) cf[line * W + sx + it] = vc;
       __syncwarp();
     }
   }
@@ -210,7 +215,7 @@ __global__ void __launch_bounds__(kThreadsD) dropout_kernel(DropoutArgs a) {
   __syncthreads();
   if (tid == 0) n_entries = map_events(a, f, events, min(n_events, kMaxEvents), s0, s1, rf_s, rf_e);
   __syncthreads();
-  if (tid < 32) conceal(a, f, n_entries, tid);
+  if (tid < 32) conceal(a, f, n_entries, tid, true, true);
 }
 
 // --------------------------------------------------------------- two-pass form
@@ -298,7 +303,8 @@ __device__ __forceinline__ int block_excl_last(int v, int* wsh) {
 }
 
 // One CTA per field: class bytes back from L2 into shared memory, then the
-// hysteresis scan, event list, mapping and concealment.
+// hysteresis scan, event list, mapping and luma concealment (chroma is
+// concealed by dropout_chroma_kernel once the chroma planes are final).
 __global__ void __launch_bounds__(kThreadsScan) dropout_scan_kernel(DropoutArgs a) {
   extern __shared__ uint4 cls4[];  // [kMaxBlocks / 16]
   __shared__ int wsh[32];
@@ -339,7 +345,15 @@ __global__ void __launch_bounds__(kThreadsScan) dropout_scan_kernel(DropoutArgs 
   __syncthreads();
   if (tid == 0) n_entries = map_events(a, f, events, min(n_events, kMaxEvents), s0, s1, rf_s, rf_e);
   __syncthreads();
-  if (tid < 32) conceal(a, f, n_entries, tid);
+  if (tid < 32) conceal(a, f, n_entries, tid, true, false);
+}
+
+// One warp per field: chroma concealment from the entries the scan kernel wrote.
+__global__ void dropout_chroma_kernel(DropoutArgs a) {
+  const int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (f >= a.fields) return;  // whole warp
+  const int n = min(max(a.do_count[f], 0), kMaxDropouts);
+  conceal(a, f, n, threadIdx.x & 31, false, true);
 }
 
 }  // namespace
@@ -360,6 +374,12 @@ void launch_dropouts_two_pass(const DropoutArgs& a, cudaStream_t st) {
   const size_t smem = kMaxBlocks;
   cudaFuncSetAttribute(dropout_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dropout_scan_kernel<<<a.fields, kThreadsScan, smem, st>>>(a);
+}
+
+void launch_dropout_conceal_chroma(const DropoutArgs& a, cudaStream_t st) {
+  if (a.fields <= 0) return;
+  const int threads = 128;
+  dropout_chroma_kernel<<<(a.fields * 32 + threads - 1) / threads, threads, 0, st>>>(a);
 }
 
 }  // namespace cuvhs

@@ -211,65 +211,96 @@ double mean_line(const std::vector<ValidPulse>& v, double nominal) {
   return cnt == 0 ? nominal : sum / (double)cnt;
 }
 
-struct Anchor {
-  bool valid = false;
-  double first_hsync_loc = 0.0, first_hsync_line = 0.0;
-  int first_field = -1, progressive_field = 0;
-  double hsync_diff = -1.0;
-};
+// Vertical-blanking anchor and field order (pipeline.cu:650-855), in three
+// parts so that everything but a few scalar decisions can run before the
+// carried state is known:
+//   scan_blanking  the blanking pulses and the half-line pattern (no state);
+//   decide_first   field order from the pattern and the previous field;
+//   fit_anchor     first-hsync location for a given field order (state only
+//                  through prev_loc, and the prediction when nothing fits).
 
-// Vertical-blanking anchor and field order (pipeline.cu:650-855).
-Anchor anchor_field(const std::vector<ValidPulse>& v, double mll, const Format& fmt, int prev_first, double prev_off_lines,
-                    double prev_loc, double prev_diff, int confidence) {
-  Anchor out;
-  if (v.empty() || mll <= 0.0) return out;
-  const int lines[2] = {fmt.field_lines_first, fmt.field_lines_second};
-  const double tol_lines = 0.5;
-  double order_len[4] = {-1, -1, -1, -1};
-  int vb_pulse[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+// Vertical-blanking pulse positions and pattern agreement of one field.
+BlankingScan scan_blanking(const std::vector<ValidPulse>& v, double mll, const Format& fmt) {
+  BlankingScan s;
+  for (int i = 0; i < 8; i++) s.vb_pulse[i] = -1;
+  for (int i = 0; i < 4; i++) s.order_len[i] = -1;
+  s.agree = s.seen = 0.0;
+  if (v.empty() || mll <= 0.0) return s;
+  const int lines0 = fmt.field_lines_first;
   int prev = -1, grp = 0, fgrp = 0;
   for (int i = 0; i < (int)v.size(); i++) {
     if (prev != -1 && v[i].good) {
-      if (grp == 0 && v[i].p.start > v[0].p.start + lines[0] * mll) {
+      if (grp == 0 && v[i].p.start > v[0].p.start + lines0 * mll) {
         grp = 4;
         fgrp = 2;
       }
       const int pt = v[prev].type, t = v[i].type;
       if (pt == kHsync && t > kHsync) {
-        vb_pulse[0 + grp] = v[i].p.start;
-        order_len[0 + fgrp] = half_line_round((v[i].p.start - v[prev].p.start) / mll);
+        s.vb_pulse[0 + grp] = v[i].p.start;
+        s.order_len[0 + fgrp] = half_line_round((v[i].p.start - v[prev].p.start) / mll);
       } else if (pt == kEq1 && t == kVsync) {
-        vb_pulse[1 + grp] = v[i].p.start;
+        s.vb_pulse[1 + grp] = v[i].p.start;
       } else if (pt == kVsync && t == kEq2) {
-        vb_pulse[2 + grp] = v[i].p.start;
+        s.vb_pulse[2 + grp] = v[i].p.start;
       } else if (pt > kHsync && t == kHsync) {
-        vb_pulse[3 + grp] = v[prev].p.start;
-        order_len[1 + fgrp] = half_line_round((v[i].p.start - v[prev].p.start) / mll);
+        s.vb_pulse[3 + grp] = v[prev].p.start;
+        s.order_len[1 + fgrp] = half_line_round((v[i].p.start - v[prev].p.start) / mll);
       }
     }
     prev = i;
   }
-  double first_pat[4] = {1, 0.5, 0.5, 1};
-  double second_pat[4] = {0.5, 1, 1, 0.5};
-  double agree = 0.0, seen = 0.0;
+  static const double first_pat[4] = {1, 0.5, 0.5, 1};
+  static const double second_pat[4] = {0.5, 1, 1, 0.5};
   for (int i = 0; i < 4; i++) {
-    if (order_len[i] == first_pat[i]) {
-      agree += 1.0;
-      seen += 1.0;
+    if (s.order_len[i] == first_pat[i]) {
+      s.agree += 1.0;
+      s.seen += 1.0;
     }
-    if (order_len[i] == second_pat[i]) seen += 1.0;
+    if (s.order_len[i] == second_pat[i]) s.seen += 1.0;
   }
+  return s;
+}
+
+// Field order: the pattern's vote when it reaches `confidence`, else the
+// opposite of the previous field (the pattern alone for the first field).
+bool decide_first(const BlankingScan& s, int prev_first, double prev_loc, int confidence) {
   bool first;
-  if (prev_first == -1) first = seen == 0.0 || std::round(agree / std::max(1.0, seen)) == 1.0;
+  if (prev_first == -1) first = s.seen == 0.0 || std::round(s.agree / std::max(1.0, s.seen)) == 1.0;
   else first = !prev_first;
-  if (seen > 0.0) {
+  if (s.seen > 0.0) {
     if (prev_loc < 0.0) confidence = std::min(confidence, 50);
-    const double weight = seen / 4.0;
-    const int c_first = (int)std::llround((agree / seen) * weight * 100.0);
-    const int c_second = (int)std::llround(((seen - agree) / seen) * weight * 100.0);
+    const double weight = s.seen / 4.0;
+    const int c_first = (int)std::llround((s.agree / s.seen) * weight * 100.0);
+    const int c_second = (int)std::llround(((s.seen - s.agree) / s.seen) * weight * 100.0);
     if (c_first >= confidence && c_first > c_second) first = true;
     else if (c_second >= confidence && c_second > c_first) first = false;
   }
+  return first;
+}
+
+// The field order the pattern fixes on its own at `confidence` whatever the
+// carried state is (a vote that clears `confidence` also clears the lower
+// threshold used after an invalid field), or -1.
+int pattern_first(const BlankingScan& s, int confidence) {
+  if (s.seen <= 0.0) return -1;
+  const double weight = s.seen / 4.0;
+  const int c_first = (int)std::llround((s.agree / s.seen) * weight * 100.0);
+  const int c_second = (int)std::llround(((s.seen - s.agree) / s.seen) * weight * 100.0);
+  if (c_first >= confidence && c_first > c_second) return 1;
+  if (c_second >= confidence && c_second > c_first) return 0;
+  return -1;
+}
+
+// First-hsync location for field order `first`.  loc_round is the estimate
+// before the hsync refinement (the carried hsync_diff is taken from it).
+AnchorFit fit_anchor(const BlankingScan& s, const std::vector<ValidPulse>& v, double mll, const Format& fmt,
+                     bool first, double prev_off_lines, double prev_loc, double prev_diff) {
+  AnchorFit out;
+  if (v.empty() || mll <= 0.0) return out;
+  const int lines[2] = {fmt.field_lines_first, fmt.field_lines_second};
+  const double tol_lines = 0.5;
+  static const double first_pat[4] = {1, 0.5, 0.5, 1};
+  static const double second_pat[4] = {0.5, 1, 1, 0.5};
   const double section = fmt.num_eq_pulses / 2.0;
   const double cur_lines = first ? lines[0] : lines[1];
   const double prev_lines = first ? lines[1] : lines[0];
@@ -285,7 +316,7 @@ Anchor anchor_field(const std::vector<ValidPulse>& v, double mll, const Format& 
   vb_line[6] = vb_line[5] + section;
   vb_line[7] = vb_line[6] + section - 0.5;
   auto pair_estimate = [&](int i1, int i2, double& loc, int& cnt, double& off) {
-    const int p1 = vb_pulse[i1], p2 = vb_pulse[i2];
+    const int p1 = s.vb_pulse[i1], p2 = s.vb_pulse[i2];
     if (p1 == -1 || p2 == -1 || mll == 0.0) return;
     const double actual = ((double)p1 - (double)p2) / mll;
     const double expect = vb_line[i1] - vb_line[i2];
@@ -320,18 +351,18 @@ Anchor anchor_field(const std::vector<ValidPulse>& v, double mll, const Format& 
     off = b_off;
   }
   const int predicted = (int)std::llround((prev_off_lines + prev_lines + prev_loc / mll) * mll);
-  bool used_prediction = false;
   if (cnt == 0 && prev_loc > 0.0) {
     double p = (prev_diff <= 0.5 && prev_diff >= -0.5) ? predicted + mll * prev_diff : (double)predicted;
     if (p <= 0.0) p = (double)v.front().p.start;
     loc += p;
     cnt += 1;
-    used_prediction = true;
+    out.used_prediction = true;
   }
+  out.cnt = cnt;
   if (cnt <= 0) return out;
   off /= cnt;
   loc = std::round((loc + off) / cnt);
-  if (!used_prediction) prev_diff = (loc - predicted) / mll;
+  out.loc_round = loc;
   double hoff = 0.0;
   int hcnt = 0;
   for (const ValidPulse& p : v) {
@@ -348,20 +379,25 @@ Anchor anchor_field(const std::vector<ValidPulse>& v, double mll, const Format& 
     hoff /= hcnt;
     loc -= hoff;
   }
-  out.valid = true;
-  out.first_hsync_loc = loc;
-  out.first_hsync_line = hsync_line;
-  out.first_field = first ? 1 : 0;
-  out.progressive_field = 0;
-  out.hsync_diff = prev_diff;
+  out.loc = loc;
+  out.hsync_line = hsync_line;
   return out;
+}
+
+// The carried hsync_diff after a fit that used no prediction.
+double hsync_diff_after(const AnchorFit& f, const Format& fmt, bool first, double mll, double prev_off_lines,
+                        double prev_loc) {
+  const int lines[2] = {fmt.field_lines_first, fmt.field_lines_second};
+  const double prev_lines = first ? lines[1] : lines[0];
+  const int predicted = (int)std::llround((prev_off_lines + prev_lines + prev_loc / mll) * mll);
+  return (f.loc_round - predicted) / mll;
 }
 
 // Nominal line grid snapped to the nearest pulse (pipeline.cu:857-893).
 void snap_lines(const std::vector<ValidPulse>& v, double ref_pos, double ref_line, double mll, int nlines,
-                std::vector<double>& locs) {
-  locs.assign((size_t)nlines, 0.0);
-  std::vector<double> ps;
+                double* locs) {
+  thread_local std::vector<double> ps;
+  ps.clear();
   ps.reserve(v.size());
   for (const ValidPulse& p : v) ps.push_back((double)p.p.start);
   // nearly sorted already (the recogniser revisits two pulses): insertion sort
@@ -402,53 +438,80 @@ void snap_lines(const std::vector<ValidPulse>& v, double ref_pos, double ref_lin
 
 }  // namespace
 
-void prepare_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
-                   LinePrep& out) {
+void prepare_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count, LinePrep& out,
+                   double* spec_locs) {
   const int n = std::max(0, std::min(count, kMaxPulses));
   out.v = validate(pulse_starts, pulse_lengths, n, fmt);
   out.mll = mean_line(out.v, (double)fmt.samples_per_line);
   out.n_raw = n;
   out.raw0 = n > 0 ? (double)pulse_starts[0] : 0.0;
+  out.scan = scan_blanking(out.v, out.mll, fmt);
+  out.spec_first = -1;
+  out.spec = AnchorFit();
+  if (!spec_locs) return;
+  // Ahead of the carried state: when the pattern fixes the field order and
+  // the blanking pulses fit, the anchor and the snapped grid equal what the
+  // in-order pass computes for any previous field with prev_loc > 0.
+  const int pf = pattern_first(out.scan, kAnchorConfidence);
+  if (pf < 0) return;
+  const AnchorFit f = fit_anchor(out.scan, out.v, out.mll, fmt, pf == 1, 0.0, 1.0, 0.0);
+  if (f.cnt <= 0 || f.used_prediction) return;
+  snap_lines(out.v, f.loc, f.hsync_line, out.mll, fmt.lines_per_frame, spec_locs);
+  out.spec_first = pf;
+  out.spec = f;
 }
 
-void finish_lines(const Format& fmt, const LinePrep& prep, long long field_readloc, LineLocState& st,
-                  FieldLines& out) {
+void finish_lines(const Format& fmt, const LinePrep& prep, long long field_readloc, LineLocState& st, double* locs,
+                  FieldLines* pulses, int* is_first) {
   const std::vector<ValidPulse>& v = prep.v;
   const double mll = prep.mll;
   double prev_off = 0.0;
   if (st.prev_first_hsync_readloc != -1 && mll > 0.0)
     prev_off = ((double)st.prev_first_hsync_readloc - (double)field_readloc) / mll;
-  const Anchor an = anchor_field(v, mll, fmt, st.prev_first_field, prev_off, st.prev_first_hsync_loc,
-                                 st.prev_first_hsync_diff, 75);
-  const int kept = std::min((int)v.size(), kMaxPulses);
-  out.starts.resize(kept);
-  out.lengths.resize(kept);
-  out.types.resize(kept);
-  for (int i = 0; i < kept; i++) {
-    out.starts[i] = v[i].p.start;
-    out.lengths[i] = v[i].p.len;
-    out.types[i] = v[i].type;
+  if (pulses) {
+    const int kept = std::min((int)v.size(), kMaxPulses);
+    pulses->starts.resize(kept);
+    pulses->lengths.resize(kept);
+    pulses->types.resize(kept);
+    for (int i = 0; i < kept; i++) {
+      pulses->starts[i] = v[i].p.start;
+      pulses->lengths[i] = v[i].p.len;
+      pulses->types[i] = v[i].type;
+    }
   }
-  if (an.valid) {
-    snap_lines(v, an.first_hsync_loc, an.first_hsync_line, mll, fmt.lines_per_frame, out.locs);
-    out.is_first = an.first_field;
-    st.prev_first_field = an.first_field;
-    st.prev_progressive_field = an.progressive_field;
+  const double prev_loc = st.prev_first_hsync_loc;
+  bool valid = !v.empty() && mll > 0.0;
+  bool first = false;
+  AnchorFit f;
+  if (valid) {
+    first = decide_first(prep.scan, st.prev_first_field, prev_loc, kAnchorConfidence);
+    if (prep.spec_first == (first ? 1 : 0) && prev_loc > 0.0) {
+      f = prep.spec;  // locs already hold the snapped grid
+    } else {
+      f = fit_anchor(prep.scan, v, mll, fmt, first, prev_off, prev_loc, st.prev_first_hsync_diff);
+      if (f.cnt > 0) snap_lines(v, f.loc, f.hsync_line, mll, fmt.lines_per_frame, locs);
+    }
+    valid = f.cnt > 0;
+  }
+  if (valid) {
+    *is_first = first ? 1 : 0;
+    st.prev_first_field = first ? 1 : 0;
+    st.prev_progressive_field = 0;
     st.prev_first_hsync_readloc = field_readloc;
-    st.prev_first_hsync_loc = an.first_hsync_loc;
-    st.prev_first_hsync_diff = an.hsync_diff;
+    st.prev_first_hsync_loc = f.loc;
+    if (!f.used_prediction) st.prev_first_hsync_diff = hsync_diff_after(f, fmt, first, mll, prev_off, prev_loc);
   } else {
-    out.locs.assign((size_t)fmt.lines_per_frame, 0.0);
-    for (int line = 0; line < fmt.lines_per_frame; line++) out.locs[line] = prep.raw0 + mll * (double)line;
-    out.is_first = st.prev_first_field >= 0 ? (1 - st.prev_first_field) : 1;
+    for (int line = 0; line < fmt.lines_per_frame; line++) locs[line] = prep.raw0 + mll * (double)line;
+    *is_first = st.prev_first_field >= 0 ? (1 - st.prev_first_field) : 1;
   }
 }
 
 void locate_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
                   long long field_readloc, LineLocState& st, FieldLines& out) {
   LinePrep prep;
-  prepare_lines(fmt, pulse_starts, pulse_lengths, count, prep);
-  finish_lines(fmt, prep, field_readloc, st, out);
+  prepare_lines(fmt, pulse_starts, pulse_lengths, count, prep, nullptr);
+  out.locs.assign((size_t)fmt.lines_per_frame, 0.0);
+  finish_lines(fmt, prep, field_readloc, st, out.locs.data(), &out, &out.is_first);
 }
 
 }  // namespace cuvhs

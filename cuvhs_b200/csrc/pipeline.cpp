@@ -62,8 +62,8 @@ int phase_id_for(int is_first, int quadrant) {
 const char* const kStageNames[kNumStages] = {"k1a_demod",      "k1b_video_sync", "sync_edges",
                                              "hsync_refine",   "luma_resample",  "chroma_prefilter",
                                              "chroma_lines",   "burst_metric",   "dropouts",
-                                             "host_edges_wait", "host_lines",     "host_chroma_wait",
-                                             "host_final_wait"};
+                                             "host_edges_wait", "host_runs",      "host_prepare",
+                                             "host_lines",     "host_chroma_wait", "host_final_wait"};
 
 double Context::host_clock() const {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -119,6 +119,16 @@ void Context::release() {
   host_allocations.clear();
   if (ev_host) cudaEventDestroy(ev_host);
   ev_host = nullptr;
+  for (cudaEvent_t& e : ev_piece) {
+    if (e) cudaEventDestroy(e);
+    e = nullptr;
+  }
+  if (ev_luma) cudaEventDestroy(ev_luma);
+  ev_luma = nullptr;
+  if (ev_edges) cudaEventDestroy(ev_edges);
+  ev_edges = nullptr;
+  if (xstream) cudaStreamDestroy(xstream);
+  xstream = nullptr;
   if (stream) cudaStreamDestroy(stream);
   stream = nullptr;
 }
@@ -181,7 +191,8 @@ bool Context::init(const cuvhs_config& c) {
     const int hw = (int)std::thread::hardware_concurrency();
     pool.reset(new WorkPool(std::max(0, std::min(hw - 1, 15))));
   }
-  if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&xstream, cudaStreamNonBlocking) != cudaSuccess) {
     err = "cudaStreamCreate failed";
     status = CUVHS_ERR_CUDA;
     return false;
@@ -211,7 +222,6 @@ bool Context::init(const cuvhs_config& c) {
   d_luma = A((uint16_t*)nullptr, (size_t)batch * F);
   d_chroma = A((uint16_t*)nullptr, (size_t)batch * F);
   d_burst = A((float*)nullptr, (size_t)batch * fmt.output_field_lines * kBurstLen);
-  d_metric = A((double*)nullptr, batch);
   d_track = A((int*)nullptr, batch);
   d_do_count = A((int*)nullptr, batch);
   d_do_lines = A((int*)nullptr, (size_t)batch * kMaxDropouts);
@@ -256,7 +266,18 @@ bool Context::init(const cuvhs_config& c) {
   hp_track = H((int*)nullptr, batch);
   hp_trial = H((int*)nullptr, 2);
   hp_burst = H((float*)nullptr, (size_t)2 * fmt.output_field_lines * kBurstLen);
-  hp_metric = H((double*)nullptr, batch);
+  {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, std::max(batch, 1) * sizeof(double), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer((void**)&dp_metric, p, 0) != cudaSuccess) {
+      if (p) cudaFreeHost(p);
+      err = "cudaHostAlloc (mapped) failed";
+      ok = false;
+    } else {
+      host_allocations.push_back(p);
+      hp_metric = static_cast<double*>(p);
+    }
+  }
   hp_do_count = H((int*)nullptr, batch);
   hp_do_lines = H((int*)nullptr, (size_t)batch * kMaxDropouts);
   hp_do_starts = H((int*)nullptr, (size_t)batch * kMaxDropouts);
@@ -268,7 +289,11 @@ bool Context::init(const cuvhs_config& c) {
   }
   hp_trial[0] = 0;
   hp_trial[1] = 1;
-  if (cudaEventCreateWithFlags(&ev_host, cudaEventDisableTiming) != cudaSuccess) {
+  bool ev_ok = cudaEventCreateWithFlags(&ev_host, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev_luma, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev_edges, cudaEventDisableTiming) == cudaSuccess;
+  for (cudaEvent_t& e : ev_piece) ev_ok = ev_ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+  if (!ev_ok) {
     err = "cudaEventCreate failed";
     status = CUVHS_ERR_CUDA;
     return false;
@@ -308,6 +333,7 @@ bool Context::check_cuda(const char* where) {
 
 bool Context::sync(const char* where) {
   cudaError_t e = cudaStreamSynchronize(stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(xstream);
   if (e != cudaSuccess) {
     err = std::string(where) + ": " + cudaGetErrorString(e);
     status = CUVHS_ERR_CUDA;
@@ -381,8 +407,14 @@ static double host_burst_phase(const float* b, int H, const Format& fmt) {
 
 // Decode one chunk.  `src` is host memory unless `src_on_device`.
 bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avail, uint64_t raw_offset,
-                           int num_fields, ChunkResult& res) {
+                           int num_fields, ChunkResult& res, uint16_t* dst_luma, uint16_t* dst_chroma) {
   res = ChunkResult();
+  // whatever path leaves this function, no copy into caller memory or pinned
+  // staging is still in flight on the copy stream afterwards
+  struct CopyStreamDrain {
+    cudaStream_t s;
+    ~CopyStreamDrain() { cudaStreamSynchronize(s); }
+  } drain{xstream};
   if (num_fields < 1 || num_fields > batch) {
     err = "num_fields must be in [1, batch_fields]";
     status = CUVHS_ERR_INVALID_ARGUMENT;
@@ -393,9 +425,6 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   const size_t total_samples = (size_t)num_fields * spp;
   const size_t n_read = std::min(total_samples, n_avail);
   if (n_read < spf) return true;  // no field: end of capture
-  // ---- input: the chunk window, the rest set to the u8 mid level (0.0 after conversion)
-  cudaMemcpyAsync(d_raw, src, n_read, src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream);
-  if (n_read < total_samples) cudaMemsetAsync(d_raw + n_read, 128, total_samples - n_read, stream);
   const int T = (int)std::min(n_read / spf, (size_t)num_fields);
   // ---- K1: FM demod over T tiles
   DemodArgs da;
@@ -427,11 +456,44 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   da.env_blocks = env_blocks;
   da.video = d_video;
   da.sync = d_sync;
+  // ---- input: the chunk window, the rest set to the u8 mid level (0.0 after
+  // conversion).  Host input arrives in pieces on the copy stream; K1a of
+  // tiles [fa, fb) reads chunk samples up to (fb-1)*spp - kOverlap + tile, so
+  // it starts as soon as the piece reaching that far has landed.
   {
     cudaEvent_t ev_;
     begin_stage(kStageK1a, ev_);
-    launch_k1a(da, stream);
-    end_stage(kStageK1a, ev_);
+    if (src_on_device) {
+      // a full window is read in place; a short one is padded in d_raw
+      if (n_read < total_samples) {
+        cudaMemcpyAsync(d_raw, src, n_read, cudaMemcpyDeviceToDevice, stream);
+        cudaMemsetAsync(d_raw + n_read, 128, total_samples - n_read, stream);
+      } else {
+        da.raw = src;
+      }
+      launch_k1a(da, 0, T, stream);
+      end_stage(kStageK1a, ev_);
+    } else {
+      const int pieces = std::min(kInputPieces, T);
+      size_t have = 0;
+      for (int i = 0; i < pieces; i++) {
+        const int fa = (int)((long long)T * i / pieces), fb = (int)((long long)T * (i + 1) / pieces);
+        size_t need = (size_t)(fb - 1) * spp + (size_t)des.tile - kOverlap;
+        if (i == pieces - 1 || need > total_samples) need = total_samples;
+        if (need > have) {
+          const size_t c_end = std::min(need, n_read);
+          if (c_end > have)
+            cudaMemcpyAsync(d_raw + have, src + have, c_end - have, cudaMemcpyHostToDevice, xstream);
+          const size_t m_beg = std::max(have, n_read);
+          if (need > m_beg) cudaMemsetAsync(d_raw + m_beg, 128, need - m_beg, xstream);
+          have = need;
+        }
+        cudaEventRecord(ev_piece[i], xstream);
+        cudaStreamWaitEvent(stream, ev_piece[i], 0);
+        launch_k1a(da, fa, fb - fa, stream);
+      }
+      end_stage(kStageK1a, ev_, pieces);
+    }
   }
   {
     cudaEvent_t ev_;
@@ -452,18 +514,22 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     launch_edges(d_sync, total_chunk, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, stream);
     end_stage(kStageEdges, ev_, 3);
   }
+  // the copies run on the copy stream, so the pre-band-pass below starts
+  // right after the edge kernels
   const int guess = std::min(edge_cap, T * kEdgeGuessPerField);
-  cudaMemcpyAsync(hp_counts, d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream);
-  cudaMemcpyAsync(hp_fall, d_fall, (size_t)guess * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
-  cudaMemcpyAsync(hp_rise, d_rise, (size_t)guess * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
-  cudaEventRecord(ev_host, stream);
+  cudaEventRecord(ev_edges, stream);
+  cudaStreamWaitEvent(xstream, ev_edges, 0);
+  cudaMemcpyAsync(hp_counts, d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, xstream);
+  cudaMemcpyAsync(hp_fall, d_fall, (size_t)guess * sizeof(unsigned), cudaMemcpyDeviceToHost, xstream);
+  cudaMemcpyAsync(hp_rise, d_rise, (size_t)guess * sizeof(unsigned), cudaMemcpyDeviceToHost, xstream);
+  cudaEventRecord(ev_host, xstream);
   // ---- the colour-under pre-band-pass needs only the raw samples: it runs on
   // the GPU while the host turns edges into field windows and line locations.
   // It covers all T demodulated slots; the detected fields are a prefix.
   const int LPF = fmt.lines_per_frame;
   const int H = fmt.output_field_lines;
   ChromaArgs ca;
-  ca.raw = d_raw;
+  ca.raw = da.raw;
   ca.pre = d_dem;  // the raw demod is no longer needed after K1b
   ca.fields = T;
   ca.spp = spp;
@@ -488,7 +554,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   ca.burst_abs_ref = (float)fmt.burst_abs_ref;
   ca.chroma = d_chroma;
   ca.burst = d_burst;
-  ca.metric = d_metric;
+  ca.metric = dp_metric;
   ca.col_frac = d_col_frac;
   if (debug) {
     dbg_demod.resize(std::min<size_t>((size_t)T * spp, (size_t)debug_tiles * spp));
@@ -572,6 +638,8 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     dbg_k2bl.assign((size_t)P * kMaxPulses, 0);
     dbg_k2bt.assign((size_t)P * kMaxPulses, kHsync);
   }
+  host_phase(kHostRuns, t_host);
+  t_host = host_clock();
   // stateless per-field part (pulses, validation, mean line) on the host pool
   if ((int)preps.size() < P) preps.resize(P);
   pool->run(P, [&](int f) {
@@ -588,19 +656,22 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
         pl.push_back((int)(run_end[i] - run_start[i]));
       }
     }
-    prepare_lines(fmt, ps.data(), pl.data(), (int)ps.size(), preps[f]);
+    prepare_lines(fmt, ps.data(), pl.data(), (int)ps.size(), preps[f], hp_ll + (size_t)f * LPF);
     if (debug) {
       dbg_k2c[f] = (int)ps.size();
       std::copy(ps.begin(), ps.end(), dbg_k2s.begin() + (size_t)f * kMaxPulses);
       std::copy(pl.begin(), pl.end(), dbg_k2l.begin() + (size_t)f * kMaxPulses);
     }
   });
+  host_phase(kHostPrepare, t_host);
+  t_host = host_clock();
   // stateful part in field order
   FieldLines fl;
   for (int f = 0; f < P; f++) {
-    finish_lines(fmt, preps[f], (long long)(raw_offset + offs[f]), lls, fl);
-    std::copy(fl.locs.begin(), fl.locs.end(), hp_ll + (size_t)f * LPF);
-    h_is_first[f] = fl.is_first;
+    int first = -1;
+    finish_lines(fmt, preps[f], (long long)(raw_offset + offs[f]), lls, hp_ll + (size_t)f * LPF,
+                 debug ? &fl : nullptr, &first);
+    h_is_first[f] = first;
     if (debug) {
       dbg_k2bc[f] = (int)fl.starts.size();
       std::copy(fl.starts.begin(), fl.starts.end(), dbg_k2bs.begin() + (size_t)f * kMaxPulses);
@@ -648,6 +719,45 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     end_stage(kStageLuma, ev_);
   }
   if (!check_cuda("lines")) return false;
+  // ---- K7 dropouts: detection, mapping and luma concealment (luma is final
+  // now, so it leaves the device on the copy stream while chroma decodes)
+  DropoutArgs dd;
+  dd.env = d_env;
+  dd.env_part = d_env_part;
+  dd.env_blocks = env_blocks;
+  dd.ll = d_ll;
+  dd.fields = P;
+  dd.spp = spp;
+  dd.lines_per_frame = LPF;
+  dd.active_line_start = fmt.active_line_start;
+  dd.out_w = fmt.output_line_len;
+  dd.out_h = H;
+  dd.luma = d_luma;
+  dd.chroma = d_chroma;
+  dd.do_count = d_do_count;
+  dd.do_lines = d_do_lines;
+  dd.do_starts = d_do_starts;
+  dd.do_ends = d_do_ends;
+  dd.cls = d_do_cls;
+  {
+    cudaEvent_t ev_;
+    begin_stage(kStageDropouts, ev_);
+    launch_dropouts_two_pass(dd, stream);
+    end_stage(kStageDropouts, ev_, 2);
+  }
+  if (!check_cuda("dropouts")) return false;
+  // the copy stream takes the finished luma and the dropout lists (read by the
+  // host after the final synchronisation)
+  const size_t F = (size_t)fmt.output_line_len * H;
+  cudaEventRecord(ev_luma, stream);
+  cudaStreamWaitEvent(xstream, ev_luma, 0);
+  if (dst_luma)
+    cudaMemcpyAsync(dst_luma, d_luma, (size_t)P * F * sizeof(uint16_t), cudaMemcpyDeviceToHost, xstream);
+  cudaMemcpyAsync(hp_do_count, d_do_count, P * sizeof(int), cudaMemcpyDeviceToHost, xstream);
+  const size_t ndo = (size_t)P * kMaxDropouts;
+  cudaMemcpyAsync(hp_do_lines, d_do_lines, ndo * sizeof(int), cudaMemcpyDeviceToHost, xstream);
+  cudaMemcpyAsync(hp_do_starts, d_do_starts, ndo * sizeof(int), cudaMemcpyDeviceToHost, xstream);
+  cudaMemcpyAsync(hp_do_ends, d_do_ends, ndo * sizeof(int), cudaMemcpyDeviceToHost, xstream);
   // ---- K6 chroma on the P detected fields
   ca.fields = P;
   ca.total = (long long)P * spp;
@@ -658,9 +768,8 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     end_stage(kStageChromaLines, ev_);
     if (write) {
       begin_stage(kStageBurstMetric, ev_);
-      launch_burst_metric(ca, f0, nf, stream);
+      launch_burst_metric(ca, f0, nf, stream);  // writes hp_metric through its mapping
       end_stage(kStageBurstMetric, ev_);
-      cudaMemcpyAsync(hp_metric + f0, d_metric + f0, nf * sizeof(double), cudaMemcpyDeviceToHost, stream);
     }
   };
   int det_track, cycle_start;
@@ -747,38 +856,16 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   chroma_track = (P & 1) ? (1 - cur) : cur;
   chroma_threshold = thr;
   chroma_cycle_start = (cycle_start + P) % 8;
-  // ---- K7 dropouts + concealment
-  DropoutArgs dd;
-  dd.env = d_env;
-  dd.env_part = d_env_part;
-  dd.env_blocks = env_blocks;
-  dd.ll = d_ll;
-  dd.fields = P;
-  dd.spp = spp;
-  dd.lines_per_frame = LPF;
-  dd.active_line_start = fmt.active_line_start;
-  dd.out_w = fmt.output_line_len;
-  dd.out_h = H;
-  dd.luma = d_luma;
-  dd.chroma = d_chroma;
-  dd.do_count = d_do_count;
-  dd.do_lines = d_do_lines;
-  dd.do_starts = d_do_starts;
-  dd.do_ends = d_do_ends;
-  dd.cls = d_do_cls;
+  // ---- chroma is final: conceal it and send both planes' remaining copies
   {
     cudaEvent_t ev_;
     begin_stage(kStageDropouts, ev_);
-    launch_dropouts_two_pass(dd, stream);
-    end_stage(kStageDropouts, ev_, 2);
+    launch_dropout_conceal_chroma(dd, stream);
+    end_stage(kStageDropouts, ev_);
   }
-  if (!check_cuda("dropouts")) return false;
-  // ---- small results back
-  cudaMemcpyAsync(hp_do_count, d_do_count, P * sizeof(int), cudaMemcpyDeviceToHost, stream);
-  const size_t ndo = (size_t)P * kMaxDropouts;
-  cudaMemcpyAsync(hp_do_lines, d_do_lines, ndo * sizeof(int), cudaMemcpyDeviceToHost, stream);
-  cudaMemcpyAsync(hp_do_starts, d_do_starts, ndo * sizeof(int), cudaMemcpyDeviceToHost, stream);
-  cudaMemcpyAsync(hp_do_ends, d_do_ends, ndo * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  if (!check_cuda("chroma concealment")) return false;
+  if (dst_chroma)
+    cudaMemcpyAsync(dst_chroma, d_chroma, (size_t)P * F * sizeof(uint16_t), cudaMemcpyDeviceToHost, stream);
   if (debug) {
     dbg_ll.resize((size_t)P * LPF);
     cudaMemcpyAsync(dbg_ll.data(), d_ll, dbg_ll.size() * sizeof(double), cudaMemcpyDeviceToHost, stream);
@@ -796,6 +883,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   if (!sync("dropouts")) return false;
   host_phase(kHostFinalWait, t_host);
   last_fields = P;
+  res.outputs_copied = dst_luma != nullptr || dst_chroma != nullptr;
   // ---- field metadata: parity alternation (pipeline.cu:2575-2610)
   res.fields = P;
   res.field_info.resize(P);

@@ -16,6 +16,7 @@ namespace cuvhs {
 struct ChunkResult {
   int fields = 0;
   uint64_t next_raw_offset = 0;
+  bool outputs_copied = false;  // luma/chroma already in the caller's host buffers
   std::vector<cuvhs_field_info> field_info;
 };
 
@@ -31,7 +32,9 @@ enum Stage {
   kStageDropouts,
   // host phases (wall time on the calling thread)
   kHostEdgesWait,
-  kHostLines,
+  kHostRuns,      // edge lists -> pulse runs, VSYNC candidates, field windows
+  kHostPrepare,   // per-field pulse validation on the host pool
+  kHostLines,     // stateful line locations in field order + upload
   kHostChromaWait,
   kHostFinalWait,
   kNumStages
@@ -49,6 +52,13 @@ struct Context {
   int env_blocks = 0;
   int edge_cap = 0;
   cudaStream_t stream = nullptr;
+  // Copy stream: host input arrives in pieces (K1a starts on each piece as it
+  // lands) and the finished luma leaves while chroma is still being decoded.
+  cudaStream_t xstream = nullptr;
+  static constexpr int kInputPieces = 4;
+  cudaEvent_t ev_piece[kInputPieces] = {};
+  cudaEvent_t ev_luma = nullptr;
+  cudaEvent_t ev_edges = nullptr;
   std::string err;
   cuvhs_status status = CUVHS_OK;
   std::vector<void*> allocations;
@@ -66,7 +76,6 @@ struct Context {
   double* d_ll = nullptr;
   uint16_t *d_luma = nullptr, *d_chroma = nullptr;
   float* d_burst = nullptr;
-  double* d_metric = nullptr;
   int* d_track = nullptr;
   int *d_do_count = nullptr, *d_do_lines = nullptr, *d_do_starts = nullptr, *d_do_ends = nullptr;
   unsigned char* d_do_cls = nullptr;
@@ -95,7 +104,8 @@ struct Context {
   double* hp_ll = nullptr;
   int *hp_track = nullptr, *hp_trial = nullptr;
   float* hp_burst = nullptr;
-  double* hp_metric = nullptr;
+  double* hp_metric = nullptr;  // mapped: the metric kernel writes it directly
+  double* dp_metric = nullptr;  // device alias of hp_metric
   int *hp_do_count = nullptr, *hp_do_lines = nullptr, *hp_do_starts = nullptr, *hp_do_ends = nullptr;
 
   // last-chunk intermediates (debug)
@@ -134,8 +144,11 @@ struct Context {
   bool check_cuda(const char* where);
   bool sync(const char* where);
   bool wait_host_event(const char* where);
+  // dst_luma / dst_chroma: optional page-locked host destinations for the
+  // chunk's fields (num_fields fields of room each); when given, the planes
+  // are copied there as soon as each is final and res.outputs_copied is set.
   bool decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avail, uint64_t raw_offset, int num_fields,
-                    ChunkResult& res);
+                    ChunkResult& res, uint16_t* dst_luma = nullptr, uint16_t* dst_chroma = nullptr);
 };
 
 // .tbc.json text (reference format, src/io/tbc_writer.cpp:89-175).

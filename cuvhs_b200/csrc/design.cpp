@@ -184,7 +184,9 @@ void Design::build(const Format& fmt) {
     a_tail = place_kernel(g, a_neg, a_pos, kNa, blk);
     std::vector<cd> G = host_dft(blk, -1);
     ga.resize(kNa);
-    for (int k = 0; k < kNa; k++) ga[k] = make_float2((float)(G[k].real() / kNa), (float)(G[k].imag() / kNa));
+    // halved: the paired-block kernel separates two spectra as (U +/- conj(U'))
+    for (int k = 0; k < kNa; k++)
+      ga[k] = make_float2((float)(G[k].real() / kNa) * 0.5f, (float)(G[k].imag() / kNa) * 0.5f);
     demod_scale = (float)(fs / (2.0 * kPi));
     d0 = fmt.ire0 * 2.0 * kPi / fs;
     const float d0f = (float)d0;
@@ -229,7 +231,8 @@ void Design::build(const Format& fmt) {
     b_tail = place_kernel(c, b_neg, b_pos, kNb, blk);
     std::vector<cd> G = host_dft(blk, -1);
     gb.resize(kNb);
-    for (int k = 0; k < kNb; k++) gb[k] = make_float2((float)(G[k].real() / kNb), (float)(G[k].imag() / kNb));
+    for (int k = 0; k < kNb; k++)  // halved, as ga
+      gb[k] = make_float2((float)(G[k].real() / kNb) * 0.5f, (float)(G[k].imag() / kNb) * 0.5f);
     // Output relative to ire0: the constant ire0 passes with the filters' DC gain.
     corr_video = (float)(fmt.ire0 * (FV[0].real() * tile - 1.0));
     corr_sync = (float)(fmt.ire0 * (FS[0].real() * tile - 1.0));

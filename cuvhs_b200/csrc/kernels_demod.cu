@@ -3,11 +3,11 @@
 // src/pipeline/vsync_discover.cu:5-45 and src/pipeline/sync_pulses.cu:10-58).
 //
 // Each tile f of the reference covers chunk samples [f*spp - 2048, f*spp - 2048 + tile)
-// (clamped to the chunk) and is filtered circularly.  A CTA here computes a
-// contiguous run of one tile's outputs with one shared-memory FFT pair: gather
-// the tile window (mod tile, clamped) into shared memory, forward FFT, multiply
-// by the block spectrum of the truncated kernel, inverse FFT, emit the valid
-// middle.  HBM traffic is the stage interface only: K1a reads u8 and writes the
+// (clamped to the chunk) and is filtered circularly.  A CTA here computes two
+// adjacent runs of one tile's outputs: gather both block windows (mod tile,
+// clamped) as the real and imaginary parts of one input, forward FFT,
+// separate and multiply by the block spectrum of the truncated kernel,
+// inverse FFT per block, emit the valid middles.  HBM traffic is the stage interface only: K1a reads u8 and writes the
 // FP32 demod and envelope; K1b reads the demod and writes video and sync.
 #include <cuda_runtime.h>
 
@@ -24,38 +24,62 @@ __device__ __forceinline__ int wrap_tile(int q, int tile) {
   return q < 0 ? q + tile : (q >= tile ? q - tile : q);
 }
 
-// K1a: u8 -> analytic signal -> phase step (FP32 Hz, relative to ire0) + envelope.
-// Thread t holds block samples t + 256*q throughout (RegFFT layout).
-__global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(DemodArgs a, int f_begin) {
-  constexpr int N = Design::kNa, T = kThreadsA;
-  extern __shared__ float2 sm[];
-  __shared__ float2 warp_last[T / 32][16];
-  __shared__ double red[T / 32];
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const int f = f_begin + blockIdx.y;
-  const int j0 = kOverlap + blockIdx.x * a.a_out;  // first demod output (tile position)
-  // chunk positions fit in 32 bits (the batch is capped so T * spp < 2^31)
-  const int tile0 = f * a.spp - kOverlap;          // chunk position of tile position 0
-  const int last = (int)a.total - 1;
-  const int base = j0 - 1 - a.a_pos;               // tile position of block sample 0
-  float2 v[16];
+// Both demod stages filter a real signal with a complex kernel g, so one CTA
+// takes two adjacent blocks x1, x2 of a tile in one forward transform of
+// u = x1 + i*x2.  With m = -k mod N, X1[k] = (U[k] + conj(U[m]))/2 and
+// X2[k] = (U[k] - conj(U[m]))/2i, so Z1 = X1*g and Z2 = X2*g follow from U and
+// its mirror (g is stored halved); each is inverted on its own.  Three
+// transforms serve two blocks instead of four.  ONE_SIDED (the analytic-signal
+// kernel of K1a, whose tile response is zero at negative frequencies) skips
+// bins k >= N/2: they are not formed and enter the inverse as zeros, which
+// also prunes the inverse's first pass.
+//
+// On return v holds Z1 (RegFFT layout) and sA holds Z2 in natural order; sB
+// is free once the caller's next barrier has passed.
+template <int N, bool ONE_SIDED>
+__device__ __forceinline__ void pair_spectra(float2 (&v)[16], float2* sA, float2* sB, const float2* __restrict__ g,
+                                             const float2* __restrict__ tw, int t) {
+  constexpr int T = N / 16;
+  RegFFT<N>::template run<false>(v, sA, tw, t);
+#pragma unroll
+  for (int q = 0; q < 16; q++) sB[pidx(t + T * q)] = v[q];
+  __syncthreads();
 #pragma unroll
   for (int q = 0; q < 16; q++) {
-    const int p = min(max(tile0 + wrap_tile(base + t + T * q, a.tile), 0), last);
-    v[q] = make_float2(((float)__ldg(&a.raw[p]) - 128.0f) * 256.0f, 0.0f);
+    if (ONE_SIDED && q >= 8) {
+      v[q] = make_float2(0.0f, 0.0f);  // k >= N/2: the kernel passes no negative frequencies
+      continue;
+    }
+    const int k = t + T * q;
+    const float2 um = sB[pidx((N - k) & (N - 1))];
+    const float2 u = v[q];
+    const float2 gg = __ldg(&g[k]);
+    const float2 x1 = make_float2(u.x + um.x, u.y - um.y);
+    const float2 x2 = make_float2(u.y + um.y, um.x - u.x);
+    v[q] = make_float2(x1.x * gg.x - x1.y * gg.y, x1.x * gg.y + x1.y * gg.x);
+    sA[pidx(k)] = make_float2(x2.x * gg.x - x2.y * gg.y, x2.x * gg.y + x2.y * gg.x);
   }
-  RegFFT<N>::run<false>(v, sm, a.tw_a, t);
+}
+
+// Z2 back from sA into the RegFFT layout (slots q >= 8 are zero when ONE_SIDED).
+template <int N, bool ONE_SIDED>
+__device__ __forceinline__ void load_second(float2 (&v)[16], const float2* sA, int t) {
+  constexpr int T = N / 16;
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
-    const float2 g = __ldg(&a.ga[t + T * q]);
-    v[q] = make_float2(v[q].x * g.x - v[q].y * g.y, v[q].x * g.y + v[q].y * g.x);
-  }
-  RegFFT<N>::run<true>(v, sm, a.tw_a_inv, t);
-  // the previous sample of t + T*q is held by thread t-1 (same q), or for t = 0
-  // by thread T-1 at q-1
+  for (int q = 0; q < 16; q++) v[q] = (ONE_SIDED && q >= 8) ? make_float2(0.0f, 0.0f) : sA[pidx(t + T * q)];
+}
+
+// K1a output stage for one block: phase step (FP32 Hz, relative to ire0) and
+// envelope of outputs [j0, j0 + nout) of tile f, and the block's envelope sum.
+// z (thread t, slot q) is block sample t + T*q; its predecessor is held by
+// thread t-1 (same q), or for t = 0 by thread T-1 at q-1.
+template <int T>
+__device__ __forceinline__ void k1a_emit(const DemodArgs& a, const float2 (&z)[16], int f, int j0, int block,
+                                         float2 (*warp_last)[16], double* red, int t) {
+  const int lane = t & 31, warp = t >> 5;
   if (lane == 31) {
 #pragma unroll
-    for (int q = 0; q < 16; q++) warp_last[warp][q] = v[q];
+    for (int q = 0; q < 16; q++) warp_last[warp][q] = z[q];
   }
   __syncthreads();
   const int nout = min(a.a_out, kOverlap + a.spp - j0);
@@ -65,61 +89,86 @@ __global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(DemodArgs a, int f_be
 #pragma unroll
   for (int q = 0; q < 16; q++) {
     float2 zp;
-    zp.x = __shfl_up_sync(0xffffffffu, v[q].x, 1);
-    zp.y = __shfl_up_sync(0xffffffffu, v[q].y, 1);
-    if (lane == 0) zp = warp > 0 ? warp_last[warp - 1][q] : (q > 0 ? warp_last[T / 32 - 1][q - 1] : v[q]);
+    zp.x = __shfl_up_sync(0xffffffffu, z[q].x, 1);
+    zp.y = __shfl_up_sync(0xffffffffu, z[q].y, 1);
+    if (lane == 0) zp = warp > 0 ? warp_last[warp - 1][q] : (q > 0 ? warp_last[T / 32 - 1][q - 1] : z[q]);
     const int i = t + T * q - (a.a_pos + 1);
     if (i >= 0 && i < nout) {
-      const float2 z = v[q];
+      const float2 zz = z[q];
       // z * conj(zp) rotated by the nominal step, so atan2 sees a small angle
-      const float re0 = z.x * zp.x + z.y * zp.y;
-      const float im0 = z.y * zp.x - z.x * zp.y;
+      const float re0 = zz.x * zp.x + zz.y * zp.y;
+      const float im0 = zz.y * zp.x - zz.x * zp.y;
       const float re = re0 * a.rot_re - im0 * a.rot_im;
       const float im = re0 * a.rot_im + im0 * a.rot_re;
       float r = atan2f(im, re);
       // keep the un-rotated step in (-pi, pi] as the reference's wrap does
       if (r + a.d0 > 3.14159265358979f) r -= 6.28318530717959f;
       dem_out[i] = r * a.demod_scale + a.demod_offset;
-      const float e = sqrtf(z.x * z.x + z.y * z.y);
+      const float e = sqrtf(zz.x * zz.x + zz.y * zz.y);
       env_out[i] = e;
       esum += (double)e;
     }
   }
-  // Deterministic per-CTA envelope partial sums (the dropout stage needs the
-  // tile mean).
+  // Deterministic per-block envelope partial sums (the dropout stage needs
+  // the tile mean).
   for (int off = 16; off > 0; off >>= 1) esum += __shfl_down_sync(0xffffffffu, esum, off);
   if (lane == 0) red[warp] = esum;
   __syncthreads();
   if (t == 0) {
     double sacc = 0.0;
     for (int w = 0; w < T / 32; w++) sacc += red[w];
-    a.env_part[(size_t)f * a.env_blocks + blockIdx.x] = sacc;
+    a.env_part[(size_t)f * a.env_blocks + block] = sacc;
   }
 }
 
-// K1b: demod -> video (real part) and sync (imag part) in one complex transform.
-__global__ void __launch_bounds__(kThreadsB, 1) k1b_kernel(DemodArgs a) {
-  constexpr int N = Design::kNb, T = kThreadsB;
+// K1a: u8 -> analytic signal -> phase step + envelope, blocks 2x and 2x+1 of
+// the tile (the second may lie past the tile's end).
+__global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(DemodArgs a, int f_begin) {
+  constexpr int N = Design::kNa, T = kThreadsA;
   extern __shared__ float2 sm[];
+  float2* sA = sm;
+  float2* sB = sm + fft_pad(N);
+  __shared__ float2 warp_last[T / 32][16];
+  __shared__ double red[T / 32];
   const int t = threadIdx.x;
-  const int f = blockIdx.y;
-  const int j0 = kOverlap + blockIdx.x * a.b_out;
-  const int tile0 = f * a.spp - kOverlap;
+  const int f = f_begin + blockIdx.y;
+  const int blk0 = 2 * blockIdx.x;
+  const int j0 = kOverlap + blk0 * a.a_out;  // first demod output of block 0 (tile position)
+  // chunk positions fit in 32 bits (the batch is capped so T * spp < 2^31)
+  const int tile0 = f * a.spp - kOverlap;    // chunk position of tile position 0
   const int last = (int)a.total - 1;
-  const int base = j0 - a.b_pos;
+  const int base = j0 - 1 - a.a_pos;         // tile position of block-0 sample 0
   float2 v[16];
+  // Interior windows (no wrap inside the tile, no clamp at the chunk ends)
+  // take the direct addresses; the CTA-uniform test keeps the loop branch-free.
+  const int span = a.a_out + N;  // tile positions [base, base + span) are read
+  if (base >= 0 && base + span <= a.tile && tile0 + base >= 0 && tile0 + base + span - 1 <= last) {
+    const uint8_t* src = a.raw + (tile0 + base + t);
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
-    const int p = min(max(tile0 + wrap_tile(base + t + T * q, a.tile), 0), last);
-    v[q] = make_float2(__ldg(&a.dem[p]), 0.0f);
-  }
-  RegFFT<N>::run<false>(v, sm, a.tw_b, t);
+    for (int q = 0; q < 16; q++)
+      v[q] = make_float2(((float)__ldg(&src[T * q]) - 128.0f) * 256.0f,
+                         ((float)__ldg(&src[T * q + a.a_out]) - 128.0f) * 256.0f);
+  } else {
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
-    const float2 g = __ldg(&a.gb[t + T * q]);
-    v[q] = make_float2(v[q].x * g.x - v[q].y * g.y, v[q].x * g.y + v[q].y * g.x);
+    for (int q = 0; q < 16; q++) {
+      const int q0 = base + t + T * q;
+      const int p0 = min(max(tile0 + wrap_tile(q0, a.tile), 0), last);
+      const int p1 = min(max(tile0 + wrap_tile(q0 + a.a_out, a.tile), 0), last);
+      v[q] = make_float2(((float)__ldg(&a.raw[p0]) - 128.0f) * 256.0f, ((float)__ldg(&a.raw[p1]) - 128.0f) * 256.0f);
+    }
   }
-  RegFFT<N>::run<true>(v, sm, a.tw_b_inv, t);
+  pair_spectra<N, true>(v, sA, sB, a.ga, a.tw_a, t);
+  RegFFT<N>::run<true>(v, sB, a.tw_a_inv, t);
+  k1a_emit<T>(a, v, f, j0, blk0, warp_last, red, t);
+  if (blk0 + 1 >= a.env_blocks) return;  // whole CTA
+  load_second<N, true>(v, sA, t);
+  RegFFT<N>::run<true>(v, sA, a.tw_a_inv, t);
+  k1a_emit<T>(a, v, f, j0 + a.a_out, blk0 + 1, warp_last, red, t);
+}
+
+// K1b output stage: video (real part) and sync (imaginary part) of one block.
+template <int T>
+__device__ __forceinline__ void k1b_emit(const DemodArgs& a, const float2 (&z)[16], int f, int j0, int t) {
   const int nout = min(a.b_out, kOverlap + a.spp - j0);
   float* video_out = a.video + (f * a.spp + (j0 - kOverlap));
   float* sync_out = a.sync + (f * a.spp + (j0 - kOverlap));
@@ -127,10 +176,40 @@ __global__ void __launch_bounds__(kThreadsB, 1) k1b_kernel(DemodArgs a) {
   for (int q = 0; q < 16; q++) {
     const int i = t + T * q - a.b_pos;
     if (i >= 0 && i < nout) {
-      video_out[i] = v[q].x + a.corr_video;
-      sync_out[i] = v[q].y + a.corr_sync;
+      video_out[i] = z[q].x + a.corr_video;
+      sync_out[i] = z[q].y + a.corr_sync;
     }
   }
+}
+
+// K1b: demod -> video + sync, blocks 2x and 2x+1 of the tile.
+__global__ void __launch_bounds__(kThreadsB, 1) k1b_kernel(DemodArgs a) {
+  constexpr int N = Design::kNb, T = kThreadsB;
+  extern __shared__ float2 sm[];
+  float2* sA = sm;
+  float2* sB = sm + fft_pad(N);
+  const int t = threadIdx.x;
+  const int f = blockIdx.y;
+  const int blk0 = 2 * blockIdx.x;
+  const int j0 = kOverlap + blk0 * a.b_out;
+  const int tile0 = f * a.spp - kOverlap;
+  const int last = (int)a.total - 1;
+  const int base = j0 - a.b_pos;
+  float2 v[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int q0 = base + t + T * q;
+    const int p0 = min(max(tile0 + wrap_tile(q0, a.tile), 0), last);
+    const int p1 = min(max(tile0 + wrap_tile(q0 + a.b_out, a.tile), 0), last);
+    v[q] = make_float2(__ldg(&a.dem[p0]), __ldg(&a.dem[p1]));
+  }
+  pair_spectra<N, false>(v, sA, sB, a.gb, a.tw_b, t);
+  RegFFT<N>::run<true>(v, sB, a.tw_b_inv, t);
+  k1b_emit<T>(a, v, f, j0, t);
+  if (kOverlap + (blk0 + 1) * a.b_out >= kOverlap + a.spp) return;  // whole CTA
+  load_second<N, false>(v, sA, t);
+  RegFFT<N>::run<true>(v, sA, a.tw_b_inv, t);
+  k1b_emit<T>(a, v, f, j0 + a.b_out, t);
 }
 
 // Threshold edges in sample order.  Each thread owns 16 consecutive samples
@@ -270,19 +349,18 @@ __global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(const float* _
 
 void launch_k1a(const DemodArgs& a, int f0, int nf, cudaStream_t st) {
   if (nf <= 0) return;
-  const size_t smem = sizeof(float2) * fft_pad(Design::kNa);
-  dim3 grid((a.spp + a.a_out - 1) / a.a_out, nf);
+  const size_t smem = 2 * sizeof(float2) * fft_pad(Design::kNa);
+  cudaFuncSetAttribute(k1a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int blocks = (a.spp + a.a_out - 1) / a.a_out;  // = env_blocks
+  dim3 grid((blocks + 1) / 2, nf);
   k1a_kernel<<<grid, kThreadsA, smem, st>>>(a, f0);
 }
 
 void launch_k1b(const DemodArgs& a, cudaStream_t st) {
-  const size_t smem = sizeof(float2) * fft_pad(Design::kNb);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k1b_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
-  dim3 grid((a.spp + a.b_out - 1) / a.b_out, a.tiles);
+  const size_t smem = 2 * sizeof(float2) * fft_pad(Design::kNb);
+  cudaFuncSetAttribute(k1b_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int blocks = (a.spp + a.b_out - 1) / a.b_out;
+  dim3 grid((blocks + 1) / 2, a.tiles);
   k1b_kernel<<<grid, kThreadsB, smem, st>>>(a);
 }
 

@@ -57,6 +57,15 @@ class Output(ctypes.Structure):
                 ("dropouts_out", ctypes.c_size_t), ("next_raw_offset", ctypes.c_uint64)]
 
 
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("lanes", ctypes.c_int), ("max_fields", ctypes.c_int)]
+
+
+class BatchItem(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_void_p), ("n", ctypes.c_size_t), ("sample_rate_mhz", ctypes.c_double),
+                ("out", ctypes.POINTER(Output)), ("status", ctypes.c_int)]
+
+
 class SynthParams(ctypes.Structure):
     _fields_ = [("sample_rate_hz", ctypes.c_double), ("n_fields", ctypes.c_int), ("tail_lines", ctypes.c_int),
                 ("seed", ctypes.c_uint64), ("snr_db", ctypes.c_double), ("jitter_bound", ctypes.c_double),
@@ -112,6 +121,17 @@ lib.cuvhs_launch_count.argtypes = [_vp]
 lib.cuvhs_launch_count.restype = ctypes.c_longlong
 lib.cuvhs_dropouts_noalloc.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
 lib.cuvhs_dropouts_noalloc.restype = ctypes.c_int
+lib.cuvhs_batch_create.argtypes = [ctypes.POINTER(BatchConfig), ctypes.POINTER(_vp)]
+lib.cuvhs_batch_create.restype = ctypes.c_int
+lib.cuvhs_batch_destroy.argtypes = [_vp]
+lib.cuvhs_batch_lanes.argtypes = [_vp]
+lib.cuvhs_batch_lanes.restype = ctypes.c_int
+lib.cuvhs_batch_decode.argtypes = [_vp, ctypes.POINTER(BatchItem), ctypes.c_int]
+lib.cuvhs_batch_decode.restype = ctypes.c_int
+lib.cuvhs_batch_last_error.argtypes = [_vp]
+lib.cuvhs_batch_last_error.restype = ctypes.c_char_p
+lib.cuvhs_batch_json.argtypes = [ctypes.POINTER(BatchItem), ctypes.c_char_p, ctypes.c_longlong]
+lib.cuvhs_batch_json.restype = ctypes.c_longlong
 lib.cuvhs_synth_default_params.argtypes = [ctypes.POINTER(SynthParams)]
 lib.cuvhs_synth_length.argtypes = [ctypes.POINTER(SynthParams)]
 lib.cuvhs_synth_length.restype = ctypes.c_longlong
@@ -124,7 +144,9 @@ EXPORTED = [
     "cuvhs_batch_fields", "cuvhs_samples_per_field", "cuvhs_tile_stride", "cuvhs_reset", "cuvhs_decode_chunk",
     "cuvhs_decode_chunk_device", "cuvhs_device_outputs", "cuvhs_decode_capture", "cuvhs_json",
     "cuvhs_decode_file", "cuvhs_set_debug", "cuvhs_debug_array", "cuvhs_stream", "cuvhs_set_timing",
-    "cuvhs_stage_count", "cuvhs_stage_name", "cuvhs_stage_times", "cuvhs_reset_stage_times", "cuvhs_launch_count", "cuvhs_dropouts_noalloc", "cuvhs_synth_default_params",
+    "cuvhs_stage_count", "cuvhs_stage_name", "cuvhs_stage_times", "cuvhs_reset_stage_times", "cuvhs_launch_count",
+    "cuvhs_dropouts_noalloc", "cuvhs_batch_create", "cuvhs_batch_destroy", "cuvhs_batch_lanes",
+    "cuvhs_batch_decode", "cuvhs_batch_last_error", "cuvhs_batch_json", "cuvhs_synth_default_params",
     "cuvhs_synth_length", "cuvhs_synth_ntsc",
 ]
 
@@ -163,6 +185,54 @@ class DecodeResult:
     @property
     def n_fields(self):
         return self.luma.shape[0]
+
+
+def alloc_output(max_fields, pinned=False):
+    """Host output buffers for max_fields fields (page-locked when pinned)."""
+    if pinned:
+        import torch
+        planes = [torch.empty((max_fields, FIELD_H, FIELD_W), dtype=torch.int16).pin_memory() for _ in range(2)]
+        luma, chroma = (p.numpy().view(np.uint16) for p in planes)
+    else:
+        planes = []
+        luma = np.empty((max_fields, FIELD_H, FIELD_W), np.uint16)
+        chroma = np.empty((max_fields, FIELD_H, FIELD_W), np.uint16)
+    bufs = {
+        "planes": planes,
+        "luma": luma,
+        "chroma": chroma,
+        "fields": (FieldInfo * max_fields)(),
+        "dl": np.empty(max_fields * MAX_DROPOUTS_PER_FIELD, np.int32),
+        "ds": np.empty(max_fields * MAX_DROPOUTS_PER_FIELD, np.int32),
+        "de": np.empty(max_fields * MAX_DROPOUTS_PER_FIELD, np.int32),
+    }
+    out = Output()
+    out.luma = bufs["luma"].ctypes.data
+    out.chroma = bufs["chroma"].ctypes.data
+    out.fields = ctypes.addressof(bufs["fields"])
+    out.dropout_line = bufs["dl"].ctypes.data
+    out.dropout_startx = bufs["ds"].ctypes.data
+    out.dropout_endx = bufs["de"].ctypes.data
+    out.max_fields = max_fields
+    out.max_dropouts = max_fields * MAX_DROPOUTS_PER_FIELD
+    return out, bufs
+
+
+def collect_result(out, bufs, json_text):
+    """DecodeResult from a filled cuvhs_output (json_text() gives the .tbc.json)."""
+    n = out.fields_out
+    fi = bufs["fields"]
+    dropouts = []
+    for i in range(n):
+        o, c = fi[i].dropout_offset, fi[i].dropout_count
+        dropouts.append((bufs["dl"][o:o + c].copy(), bufs["ds"][o:o + c].copy(), bufs["de"][o:o + c].copy()))
+    own = (lambda a: a.copy()) if bufs["planes"] else (lambda a: a)  # pinned staging is not kept
+    return DecodeResult(
+        luma=own(bufs["luma"][:n]), chroma=own(bufs["chroma"][:n]),
+        file_loc=np.array([fi[i].file_loc for i in range(n)], np.uint64),
+        is_first_field=np.array([fi[i].is_first_field for i in range(n)], np.int32),
+        field_phase_id=np.array([fi[i].field_phase_id for i in range(n)], np.int32),
+        dropouts=dropouts, json=json_text())
 
 
 class Decoder:
@@ -217,51 +287,15 @@ class Decoder:
             raise CuvhsError(st, lib.cuvhs_last_error(self._h).decode())
 
     def _alloc_output(self, max_fields, pinned=False):
-        if pinned:
-            import torch
-            planes = [torch.empty((max_fields, FIELD_H, FIELD_W), dtype=torch.int16).pin_memory() for _ in range(2)]
-            luma, chroma = (p.numpy().view(np.uint16) for p in planes)
-        else:
-            planes = []
-            luma = np.empty((max_fields, FIELD_H, FIELD_W), np.uint16)
-            chroma = np.empty((max_fields, FIELD_H, FIELD_W), np.uint16)
-        bufs = {
-            "planes": planes,
-            "luma": luma,
-            "chroma": chroma,
-            "fields": (FieldInfo * max_fields)(),
-            "dl": np.empty(max_fields * MAX_DROPOUTS_PER_FIELD, np.int32),
-            "ds": np.empty(max_fields * MAX_DROPOUTS_PER_FIELD, np.int32),
-            "de": np.empty(max_fields * MAX_DROPOUTS_PER_FIELD, np.int32),
-        }
-        out = Output()
-        out.luma = bufs["luma"].ctypes.data
-        out.chroma = bufs["chroma"].ctypes.data
-        out.fields = ctypes.addressof(bufs["fields"])
-        out.dropout_line = bufs["dl"].ctypes.data
-        out.dropout_startx = bufs["ds"].ctypes.data
-        out.dropout_endx = bufs["de"].ctypes.data
-        out.max_fields = max_fields
-        out.max_dropouts = max_fields * MAX_DROPOUTS_PER_FIELD
-        return out, bufs
+        return alloc_output(max_fields, pinned)
 
     def _result(self, out, bufs):
-        n = out.fields_out
-        fi = bufs["fields"]
-        dropouts = []
-        for i in range(n):
-            o, c = fi[i].dropout_offset, fi[i].dropout_count
-            dropouts.append((bufs["dl"][o:o + c].copy(), bufs["ds"][o:o + c].copy(), bufs["de"][o:o + c].copy()))
-        jl = lib.cuvhs_json(self._h, ctypes.byref(out), None, 0)
-        jb = ctypes.create_string_buffer(int(jl) + 1)
-        lib.cuvhs_json(self._h, ctypes.byref(out), jb, jl + 1)
-        own = (lambda a: a.copy()) if bufs["planes"] else (lambda a: a)  # pinned staging is not kept
-        return DecodeResult(
-            luma=own(bufs["luma"][:n]), chroma=own(bufs["chroma"][:n]),
-            file_loc=np.array([fi[i].file_loc for i in range(n)], np.uint64),
-            is_first_field=np.array([fi[i].is_first_field for i in range(n)], np.int32),
-            field_phase_id=np.array([fi[i].field_phase_id for i in range(n)], np.int32),
-            dropouts=dropouts, json=jb.value.decode())
+        def json_text():
+            jl = lib.cuvhs_json(self._h, ctypes.byref(out), None, 0)
+            jb = ctypes.create_string_buffer(int(jl) + 1)
+            lib.cuvhs_json(self._h, ctypes.byref(out), jb, jl + 1)
+            return jb.value.decode()
+        return collect_result(out, bufs, json_text)
 
     def decode_capture(self, samples: np.ndarray, pinned: bool = False) -> DecodeResult:
         """Decode a whole capture.  pinned=True stages the input and the output
@@ -328,6 +362,84 @@ class Decoder:
         if n:
             lib.cuvhs_debug_array(self._h, name.encode(), a.ctypes.data, n)
         return a
+
+
+class Batch:
+    """cuvhs_batch: many independent captures (mixed rates) decoded concurrently."""
+
+    def __init__(self, lanes=0, max_fields=0, device=0):
+        cfg = BatchConfig(int(device), int(lanes), int(max_fields))
+        h = _vp()
+        st = lib.cuvhs_batch_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st != 0:
+            raise CuvhsError(st, "cuvhs_batch_create failed")
+        self._h = h
+
+    @property
+    def lanes(self):
+        return lib.cuvhs_batch_lanes(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.cuvhs_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def prepare(self, captures, pinned=False):
+        """Items and buffers for [(samples u8, sample_rate_mhz), ...]; pinned
+        stages inputs and output planes in page-locked memory."""
+        items = (BatchItem * len(captures))()
+        keep = []
+        for i, (x, mhz) in enumerate(captures):
+            x = np.ascontiguousarray(x, dtype=np.uint8)
+            spf = int(round(mhz * 1e6 / (525 * 30 / 1.001))) * 263
+            out, bufs = alloc_output(x.size // spf + 2, pinned)
+            if pinned:
+                import torch
+                t = torch.from_numpy(x).pin_memory()
+                bufs["input"] = t
+                items[i].samples = t.data_ptr()
+            else:
+                bufs["input"] = x
+                items[i].samples = x.ctypes.data
+            items[i].n = x.size
+            items[i].sample_rate_mhz = float(mhz)
+            bufs["out"] = out
+            items[i].out = ctypes.pointer(out)
+            keep.append(bufs)
+        return items, keep
+
+    def run(self, items):
+        st = lib.cuvhs_batch_decode(self._h, items, len(items))
+        if st != 0:
+            raise CuvhsError(st, lib.cuvhs_batch_last_error(self._h).decode())
+
+    def results(self, items, keep):
+        res = []
+        for i, bufs in enumerate(keep):
+            it = items[i]
+
+            def json_text(it=it):
+                jl = lib.cuvhs_batch_json(ctypes.byref(it), None, 0)
+                jb = ctypes.create_string_buffer(int(jl) + 1)
+                lib.cuvhs_batch_json(ctypes.byref(it), jb, jl + 1)
+                return jb.value.decode()
+            res.append(collect_result(bufs["out"], bufs, json_text))
+        return res
+
+    def decode(self, captures, pinned=False):
+        """Decode [(samples, sample_rate_mhz), ...]; one DecodeResult per capture."""
+        items, keep = self.prepare(captures, pinned)
+        self.run(items)
+        return self.results(items, keep)
 
 
 def decode_file(in_path, out_base, sample_rate_mhz=28.0, device=0, overwrite=True, batch_fields=0):

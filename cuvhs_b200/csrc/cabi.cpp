@@ -106,6 +106,25 @@ long long copy_ptr(const T* p, size_t n, void* dst, long long cap) {
 
 }  // namespace
 
+namespace cuvhs {
+
+cuvhs_status create_context(const cuvhs_config& cfg, int pool_threads, cuvhs_ctx** out) {
+  *out = nullptr;
+  cuvhs_ctx* h = new (std::nothrow) cuvhs_ctx();
+  if (!h) return CUVHS_ERR_OUT_OF_MEMORY;
+  h->c.pool_threads = pool_threads;
+  if (!h->c.init(cfg)) {
+    cuvhs_status s = h->c.status != CUVHS_OK ? h->c.status : CUVHS_ERR_CUDA;
+    fprintf(stderr, "cuvhs_create: %s\n", h->c.err.c_str());
+    delete h;
+    return s;
+  }
+  *out = h;
+  return CUVHS_OK;
+}
+
+}  // namespace cuvhs
+
 extern "C" {
 
 void cuvhs_default_config(cuvhs_config* cfg) {
@@ -133,17 +152,7 @@ const char* cuvhs_status_string(cuvhs_status s) {
 
 cuvhs_status cuvhs_create(const cuvhs_config* cfg, cuvhs_ctx** out) {
   if (!cfg || !out) return CUVHS_ERR_INVALID_ARGUMENT;
-  *out = nullptr;
-  cuvhs_ctx* h = new (std::nothrow) cuvhs_ctx();
-  if (!h) return CUVHS_ERR_OUT_OF_MEMORY;
-  if (!h->c.init(*cfg)) {
-    cuvhs_status s = h->c.status != CUVHS_OK ? h->c.status : CUVHS_ERR_CUDA;
-    fprintf(stderr, "cuvhs_create: %s\n", h->c.err.c_str());
-    delete h;
-    return s;
-  }
-  *out = h;
-  return CUVHS_OK;
+  return cuvhs::create_context(*cfg, -1, out);
 }
 
 void cuvhs_destroy(cuvhs_ctx* ctx) { delete ctx; }

@@ -84,6 +84,9 @@ struct Design {
   double het_scale = 0;
   int fsc_bin = 0, bw_bins = 0;
   void build(const Format& fmt);
+  // build() once per sample rate per process; later calls copy the result
+  // (thread-safe).  Contexts of one rate then share the FP64 design work.
+  void build_cached(const Format& fmt);
 };
 
 // ---------------------------------------------------------------- kernels

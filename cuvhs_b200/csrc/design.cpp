@@ -16,6 +16,8 @@
 #include <cmath>
 #include <complex>
 #include <cstdio>
+#include <map>
+#include <mutex>
 
 #include "cuvhs_internal.h"
 #include "host_fft.h"
@@ -270,6 +272,23 @@ void Design::build(const Format& fmt) {
   fsc_bin = (int)(fmt.fsc / fmt.output_rate * kLineFFT + 0.5);
   bw_bins = (int)(500000.0 / fmt.output_rate * kLineFFT + 0.5);
   if (bw_bins < 10) bw_bins = 10;
+}
+
+}  // namespace cuvhs
+
+namespace cuvhs {
+
+void Design::build_cached(const Format& fmt) {
+  static std::mutex mu;
+  static std::map<double, Design> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(fmt.fs_hz);
+  if (it == cache.end()) {
+    Design d;
+    d.build(fmt);
+    it = cache.emplace(fmt.fs_hz, std::move(d)).first;
+  }
+  *this = it->second;
 }
 
 }  // namespace cuvhs

@@ -171,7 +171,7 @@ bool Context::init(const cuvhs_config& c) {
   }
   cudaSetDevice(device);
   fmt.init(c.sample_rate_mhz);
-  des.build(fmt);
+  des.build_cached(fmt);
   spp = fmt.spp;
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
@@ -189,7 +189,8 @@ bool Context::init(const cuvhs_config& c) {
   batch = b;
   {
     const int hw = (int)std::thread::hardware_concurrency();
-    pool.reset(new WorkPool(std::max(0, std::min(hw - 1, 15))));
+    const int n = pool_threads >= 0 ? pool_threads : std::min(hw - 1, 15);
+    pool.reset(new WorkPool(std::max(0, n)));
   }
   if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&xstream, cudaStreamNonBlocking) != cudaSuccess) {

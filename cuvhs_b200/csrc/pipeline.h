@@ -51,6 +51,7 @@ struct Context {
   int spp = 0;
   int env_blocks = 0;
   int edge_cap = 0;
+  int pool_threads = -1;  // host line-location helpers; -1 = min(cores - 1, 15)
   cudaStream_t stream = nullptr;
   // Copy stream: host input arrives in pieces (K1a starts on each piece as it
   // lands) and the finished luma leaves while chroma is still being decoded.

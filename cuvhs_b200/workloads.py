@@ -26,3 +26,29 @@ def make_workload(name, **overrides):
     kw = dict(WORKLOADS[name])
     kw.update(overrides)
     return synth_capture(**kw)
+
+
+BATCH_RATES = (28.0, 35.8, 40.0)
+
+
+def batch_specs(count=64, min_fields=2, max_fields=240, seed=3000):
+    """Per-capture synthesis parameters of a mixed batch: lengths uniform in
+    [min_fields, max_fields], rates from 28 / 35.8 / 40 MHz, SNR 30-45 dB,
+    jitter bound 0.5-2 samples, dropout-line rate 0-0.5%; capture i is seeded
+    seed + i."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(count):
+        mhz = float(BATCH_RATES[int(rng.integers(0, len(BATCH_RATES)))])
+        specs.append(dict(sample_rate_hz=mhz * 1e6, n_fields=int(rng.integers(min_fields, max_fields + 1)),
+                          seed=seed + i, snr_db=float(rng.uniform(30, 45)),
+                          jitter_bound=float(rng.uniform(0.5, 2.0)),
+                          dropout_line_rate=float(rng.uniform(0.0, 0.005))))
+    return specs
+
+
+def make_batch_workload(count=64, min_fields=2, max_fields=240, seed=3000):
+    """[(capture u8, sample_rate_mhz), ...] for batch_specs(...)."""
+    return [(synth_capture(**kw), kw["sample_rate_hz"] / 1e6)
+            for kw in batch_specs(count, min_fields, max_fields, seed)]

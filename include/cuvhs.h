@@ -20,6 +20,10 @@
  *   cuvhs_debug_array                 the stage outputs the reference keeps in device
  *                                     buffers (d_pulse_*, d_linelocs, d_is_first_field,
  *                                     d_do_*; src/pipeline/pipeline.h:52-87)
+ *   cuvhs_batch_*                     no counterpart: the reference decodes one capture per
+ *                                     process (src/main.cpp:97-165); a batch decodes many
+ *                                     captures of mixed sample rates concurrently, each
+ *                                     exactly as a single-capture decode would
  */
 #ifndef CUVHS_H
 #define CUVHS_H
@@ -172,6 +176,43 @@ long long cuvhs_debug_array(const cuvhs_ctx* ctx, const char* name, void* dst, l
 cuvhs_status cuvhs_dropouts_noalloc(const float* d_envelope, const double* d_linelocs, int fields, int tile_stride,
                                     uint16_t* d_luma, uint16_t* d_chroma, int32_t* d_count, int32_t* d_lines,
                                     int32_t* d_startx, int32_t* d_endx, void* stream);
+
+/* ---------------------------------------------------------------- batches
+ * Many independent captures (mixed sample rates and lengths) decoded
+ * concurrently on one GPU.  `lanes` host threads each drive their own decoder
+ * contexts (one per sample rate seen, created on first use and kept), so the
+ * GPU overlaps the kernels and copies of several captures while their host
+ * decisions run in parallel.  Every capture is decoded from a fresh state
+ * exactly as cuvhs_decode_capture on a new context with a chunk of
+ * max_fields fields would decode it: outputs do not depend on the lane count
+ * or on the order of the items. */
+typedef struct cuvhs_batch cuvhs_batch;
+
+typedef struct cuvhs_batch_config {
+  int device;     /* CUDA device id, -1 = the one with most memory */
+  int lanes;      /* concurrent decoders; 0 = choose (min(4, cores / 2), at least 1) */
+  int max_fields; /* chunk size of each lane's contexts; 0 = 256 (one chunk per capture
+                     of up to 256 fields, as a single-capture decode with the default
+                     chunk size) */
+} cuvhs_batch_config;
+
+typedef struct cuvhs_batch_item {
+  const uint8_t* samples;  /* host capture (page-locked memory lets copies overlap) */
+  size_t n;                /* samples */
+  double sample_rate_mhz;
+  cuvhs_output* out;       /* caller-owned, as for cuvhs_decode_capture */
+  cuvhs_status status;     /* filled in per item */
+} cuvhs_batch_item;
+
+cuvhs_status cuvhs_batch_create(const cuvhs_batch_config* cfg, cuvhs_batch** out);
+void cuvhs_batch_destroy(cuvhs_batch* b);
+int cuvhs_batch_lanes(const cuvhs_batch* b);
+/* Decode all items; returns CUVHS_OK when every item's status is CUVHS_OK,
+ * else the first failing item's status (cuvhs_batch_last_error has its message). */
+cuvhs_status cuvhs_batch_decode(cuvhs_batch* b, cuvhs_batch_item* items, int n_items);
+const char* cuvhs_batch_last_error(const cuvhs_batch* b);
+/* .tbc.json text of one decoded item (as cuvhs_json for a single capture). */
+long long cuvhs_batch_json(const cuvhs_batch_item* item, char* dst, long long cap);
 
 #ifdef __cplusplus
 }

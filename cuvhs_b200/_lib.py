@@ -187,6 +187,12 @@ class DecodeResult:
         return self.luma.shape[0]
 
 
+def max_fields_for(n_samples, samples_per_field):
+    """Output room for a capture: its nominal field count plus 1% (tape running
+    fast packs more fields into the same samples) and a few fields."""
+    return int(n_samples / samples_per_field * 1.01) + 4
+
+
 def alloc_output(max_fields, pinned=False):
     """Host output buffers for max_fields fields (page-locked when pinned)."""
     if pinned:
@@ -302,7 +308,7 @@ class Decoder:
         planes in page-locked memory, which lets the library overlap the
         host<->device copies with the decode."""
         samples = np.ascontiguousarray(samples, dtype=np.uint8)
-        max_fields = samples.size // self.samples_per_field + 2
+        max_fields = max_fields_for(samples.size, self.samples_per_field)
         out, bufs = self._alloc_output(max_fields, pinned)
         if pinned:
             import torch
@@ -401,7 +407,7 @@ class Batch:
         for i, (x, mhz) in enumerate(captures):
             x = np.ascontiguousarray(x, dtype=np.uint8)
             spf = int(round(mhz * 1e6 / (525 * 30 / 1.001))) * 263
-            out, bufs = alloc_output(x.size // spf + 2, pinned)
+            out, bufs = alloc_output(max_fields_for(x.size, spf), pinned)
             if pinned:
                 import torch
                 t = torch.from_numpy(x).pin_memory()

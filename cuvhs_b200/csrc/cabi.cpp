@@ -79,16 +79,24 @@ bool page_locked(const void* p) {
 // plane there as soon as it is final (overlapping the rest of the decode);
 // otherwise the planes are copied after the decode.
 cuvhs_status decode_into(Context& c, const uint8_t* src, size_t n_avail, uint64_t raw_offset, int num_fields,
-                         cuvhs_output* out) {
+                         cuvhs_output* out, const uint8_t* cap_base = nullptr, size_t cap_n = 0) {
   const size_t F = (size_t)c.fmt.output_line_len * c.fmt.output_field_lines;
   uint16_t *dl = nullptr, *dc = nullptr;
-  if (out->fields_out + (size_t)num_fields <= out->max_fields) {
+  // a chunk yields at most min(num_fields, n_avail / samples_per_field) fields
+  const size_t most = std::min<size_t>((size_t)std::max(num_fields, 0), n_avail / (size_t)c.fmt.samples_per_field);
+  if (out->fields_out + most <= out->max_fields) {
     if (page_locked(out->luma)) dl = out->luma + out->fields_out * F;
     if (page_locked(out->chroma)) dc = out->chroma + out->fields_out * F;
     if ((out->luma && !dl) || (out->chroma && !dc)) dl = dc = nullptr;  // both or neither
   }
   ChunkResult r;
-  if (!c.decode_chunk(src, false, n_avail, raw_offset, num_fields, r, dl, dc)) return c.status;
+  // a chunk of a whole page-locked capture prefetches the next chunk's window
+  // and, with page-locked planes, defers its plane copies (the capture loop
+  // drains them)
+  if (cap_base && !page_locked(cap_base)) cap_base = nullptr;
+  const bool defer = cap_base != nullptr && (dl || dc);
+  if (!c.decode_chunk(src, false, n_avail, raw_offset, num_fields, r, dl, dc, cap_base, cap_n, defer))
+    return c.status;
   return append_chunk(c, r, out);
 }
 
@@ -209,14 +217,18 @@ cuvhs_status cuvhs_decode_capture(cuvhs_ctx* ctx, const uint8_t* samples, size_t
     const int nf = std::min(c.batch, remaining_fields);
     const size_t before = out->fields_out;
     const uint64_t prev_next = out->next_raw_offset;
-    cuvhs_status s = decode_into(c, samples + raw_offset, n - raw_offset, raw_offset, nf, out);
-    if (s != CUVHS_OK) return s;
+    cuvhs_status s = decode_into(c, samples + raw_offset, n - raw_offset, raw_offset, nf, out, samples, n);
+    if (s != CUVHS_OK) {
+      c.drain_copies();
+      return s;
+    }
     if (out->fields_out == before) {
       out->next_raw_offset = prev_next;
       break;
     }
     raw_offset = out->next_raw_offset;
   }
+  if (!c.drain_copies()) return c.status;
   return CUVHS_OK;
 }
 

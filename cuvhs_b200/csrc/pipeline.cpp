@@ -127,6 +127,13 @@ void Context::release() {
   ev_luma = nullptr;
   if (ev_edges) cudaEventDestroy(ev_edges);
   ev_edges = nullptr;
+  for (cudaEvent_t* e : {&ev_prefetch, &ev_small, &ev_chroma, &ev_out_done[0], &ev_out_done[1]}) {
+    if (*e) cudaEventDestroy(*e);
+    *e = nullptr;
+  }
+  if (hstream) cudaStreamDestroy(hstream);
+  hstream = nullptr;
+  pf = Prefetch();
   if (xstream) cudaStreamDestroy(xstream);
   xstream = nullptr;
   if (stream) cudaStreamDestroy(stream);
@@ -175,7 +182,7 @@ bool Context::init(const cuvhs_config& c) {
   spp = fmt.spp;
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
-  const size_t per_field = (size_t)spp * (1 + 4 * 5) + (size_t)263 * 910 * 4 + 263 * kBurstLen * 4 + 65536 +
+  const size_t per_field = (size_t)spp * (2 + 4 * 5) + (size_t)263 * 910 * 8 + 263 * kBurstLen * 4 + 65536 +
                            dropout_class_bytes_per_field();
   int b = c.batch_fields;
   if (b <= 0) {
@@ -193,7 +200,8 @@ bool Context::init(const cuvhs_config& c) {
     pool.reset(new WorkPool(std::max(0, n)));
   }
   if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&xstream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&xstream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&hstream, cudaStreamNonBlocking) != cudaSuccess) {
     err = "cudaStreamCreate failed";
     status = CUVHS_ERR_CUDA;
     return false;
@@ -207,7 +215,9 @@ bool Context::init(const cuvhs_config& c) {
     return p;
   };
   env_blocks = (spp + des.a_out - 1) / des.a_out;
-  d_raw = A((uint8_t*)nullptr, S + 64);
+  d_raw_set[0] = A((uint8_t*)nullptr, S + 64);
+  d_raw_set[1] = A((uint8_t*)nullptr, S + 64);
+  d_raw = d_raw_set[0];
   d_dem = A((float*)nullptr, S);
   d_env = A((float*)nullptr, S);
   d_video = A((float*)nullptr, S);
@@ -220,8 +230,12 @@ bool Context::init(const cuvhs_config& c) {
   d_edge_blk = A((int2*)nullptr, (size_t)edge_blocks((long long)batch * spp) + 1);
   d_ll = A((double*)nullptr, (size_t)batch * fmt.lines_per_frame);
   const size_t F = (size_t)fmt.output_line_len * fmt.output_field_lines;
-  d_luma = A((uint16_t*)nullptr, (size_t)batch * F);
-  d_chroma = A((uint16_t*)nullptr, (size_t)batch * F);
+  for (int k = 0; k < 2; k++) {
+    d_luma_set[k] = A((uint16_t*)nullptr, (size_t)batch * F);
+    d_chroma_set[k] = A((uint16_t*)nullptr, (size_t)batch * F);
+  }
+  d_luma = d_luma_set[0];
+  d_chroma = d_chroma_set[0];
   d_burst = A((float*)nullptr, (size_t)batch * fmt.output_field_lines * kBurstLen);
   d_track = A((int*)nullptr, batch);
   d_do_count = A((int*)nullptr, batch);
@@ -293,6 +307,8 @@ bool Context::init(const cuvhs_config& c) {
   bool ev_ok = cudaEventCreateWithFlags(&ev_host, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_luma, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_edges, cudaEventDisableTiming) == cudaSuccess;
+  for (cudaEvent_t* e : {&ev_prefetch, &ev_small, &ev_chroma, &ev_out_done[0], &ev_out_done[1]})
+    ev_ok = ev_ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t& e : ev_piece) ev_ok = ev_ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
   if (!ev_ok) {
     err = "cudaEventCreate failed";
@@ -335,6 +351,7 @@ bool Context::check_cuda(const char* where) {
 bool Context::sync(const char* where) {
   cudaError_t e = cudaStreamSynchronize(stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(xstream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(hstream);
   if (e != cudaSuccess) {
     err = std::string(where) + ": " + cudaGetErrorString(e);
     status = CUVHS_ERR_CUDA;
@@ -346,6 +363,19 @@ bool Context::sync(const char* where) {
 
 // Wait for the work recorded before ev_host (the host reads results it
 // copied); later work on the stream keeps running.
+bool Context::drain_copies() {
+  cudaError_t e = cudaStreamSynchronize(xstream);
+  const cudaError_t e2 = cudaStreamSynchronize(hstream);
+  pf.valid = false;
+  if (e == cudaSuccess) e = e2;
+  if (e != cudaSuccess) {
+    err = std::string("output copies: ") + cudaGetErrorString(e);
+    status = CUVHS_ERR_CUDA;
+    return false;
+  }
+  return true;
+}
+
 bool Context::wait_host_event(const char* where) {
   cudaError_t e = cudaEventSynchronize(ev_host);
   if (e != cudaSuccess) {
@@ -408,14 +438,21 @@ static double host_burst_phase(const float* b, int H, const Format& fmt) {
 
 // Decode one chunk.  `src` is host memory unless `src_on_device`.
 bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avail, uint64_t raw_offset,
-                           int num_fields, ChunkResult& res, uint16_t* dst_luma, uint16_t* dst_chroma) {
+                           int num_fields, ChunkResult& res, uint16_t* dst_luma, uint16_t* dst_chroma,
+                           const uint8_t* cap_base, size_t cap_n, bool defer) {
   res = ChunkResult();
-  // whatever path leaves this function, no copy into caller memory or pinned
-  // staging is still in flight on the copy stream afterwards
-  struct CopyStreamDrain {
-    cudaStream_t s;
-    ~CopyStreamDrain() { cudaStreamSynchronize(s); }
-  } drain{xstream};
+  // Unless the caller defers them and the chunk succeeded, no copy into
+  // caller memory or pinned staging is still in flight when this returns.
+  struct CopyDrain {
+    Context* c;
+    bool keep = false;
+    ~CopyDrain() {
+      if (keep) return;
+      cudaStreamSynchronize(c->xstream);
+      cudaStreamSynchronize(c->hstream);
+      c->pf.valid = false;
+    }
+  } drain{this};
   if (num_fields < 1 || num_fields > batch) {
     err = "num_fields must be in [1, batch_fields]";
     status = CUVHS_ERR_INVALID_ARGUMENT;
@@ -427,6 +464,19 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   const size_t n_read = std::min(total_samples, n_avail);
   if (n_read < spf) return true;  // no field: end of capture
   const int T = (int)std::min(n_read / spf, (size_t)num_fields);
+  // ---- buffer sets: planes alternate between two sets when they are copied
+  // out asynchronously; the input window may already be on the device
+  const bool pipelined = dst_luma != nullptr || dst_chroma != nullptr;
+  const int oset = pipelined ? out_set : 0;
+  d_luma = d_luma_set[oset];
+  d_chroma = d_chroma_set[oset];
+  cudaStreamWaitEvent(stream, ev_out_done[oset], 0);  // an earlier chunk's copies out of this set
+  const bool prefetched = !src_on_device && pf.valid && pf.raw_offset == raw_offset && pf.n_read == n_read &&
+                          pf.total == total_samples;
+  const int rset = prefetched ? pf.set : raw_set;
+  pf.valid = false;
+  d_raw = d_raw_set[rset];
+  raw_set = rset;
   // ---- K1: FM demod over T tiles
   DemodArgs da;
   da.raw = d_raw;
@@ -474,6 +524,10 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
       }
       launch_k1a(da, 0, T, stream);
       end_stage(kStageK1a, ev_);
+    } else if (prefetched) {
+      cudaStreamWaitEvent(stream, ev_prefetch, 0);
+      launch_k1a(da, 0, T, stream);
+      end_stage(kStageK1a, ev_);
     } else {
       const int pieces = std::min(kInputPieces, T);
       size_t have = 0;
@@ -484,12 +538,12 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
         if (need > have) {
           const size_t c_end = std::min(need, n_read);
           if (c_end > have)
-            cudaMemcpyAsync(d_raw + have, src + have, c_end - have, cudaMemcpyHostToDevice, xstream);
+            cudaMemcpyAsync(d_raw + have, src + have, c_end - have, cudaMemcpyHostToDevice, hstream);
           const size_t m_beg = std::max(have, n_read);
-          if (need > m_beg) cudaMemsetAsync(d_raw + m_beg, 128, need - m_beg, xstream);
+          if (need > m_beg) cudaMemsetAsync(d_raw + m_beg, 128, need - m_beg, hstream);
           have = need;
         }
-        cudaEventRecord(ev_piece[i], xstream);
+        cudaEventRecord(ev_piece[i], hstream);
         cudaStreamWaitEvent(stream, ev_piece[i], 0);
         launch_k1a(da, fa, fb - fa, stream);
       }
@@ -628,6 +682,28 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   if (offs.size() >= 2) actual_spf = (offs.back() - offs.front()) / (offs.size() - 1);
   const size_t predicted = offs.back() + actual_spf, margin = 10 * (size_t)fmt.samples_per_line;
   res.next_raw_offset = predicted > margin ? raw_offset + predicted - margin : raw_offset + predicted;
+  // ---- the next chunk of a host capture starts at next_raw_offset: copy its
+  // window into the other raw buffer now (the chunk loop's arithmetic, so the
+  // next call finds it); the previous chunk that read that buffer has ended.
+  if (cap_base && !src_on_device && res.next_raw_offset < cap_n) {
+    const uint64_t nxt = res.next_raw_offset;
+    const size_t rem_fields = (size_t)(cap_n - nxt) / spf;
+    if (rem_fields > 0) {
+      const int nf = (int)std::min<size_t>((size_t)batch, rem_fields);
+      const size_t tot = (size_t)nf * spp, nr = std::min(tot, (size_t)(cap_n - nxt));
+      if (nr >= spf) {
+        const int ps = 1 - rset;
+        cudaMemcpyAsync(d_raw_set[ps], cap_base + nxt, nr, cudaMemcpyHostToDevice, hstream);
+        if (nr < tot) cudaMemsetAsync(d_raw_set[ps] + nr, 128, tot - nr, hstream);
+        cudaEventRecord(ev_prefetch, hstream);
+        pf.valid = true;
+        pf.raw_offset = nxt;
+        pf.n_read = nr;
+        pf.total = tot;
+        pf.set = ps;
+      }
+    }
+  }
   // ---- per-field pulses and line locations (sync_pulses.cu:10-58, pipeline.cu:1717-1778)
   h_is_first.assign(P, -1);
   if (debug) {
@@ -752,13 +828,14 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   const size_t F = (size_t)fmt.output_line_len * H;
   cudaEventRecord(ev_luma, stream);
   cudaStreamWaitEvent(xstream, ev_luma, 0);
-  if (dst_luma)
-    cudaMemcpyAsync(dst_luma, d_luma, (size_t)P * F * sizeof(uint16_t), cudaMemcpyDeviceToHost, xstream);
   cudaMemcpyAsync(hp_do_count, d_do_count, P * sizeof(int), cudaMemcpyDeviceToHost, xstream);
   const size_t ndo = (size_t)P * kMaxDropouts;
   cudaMemcpyAsync(hp_do_lines, d_do_lines, ndo * sizeof(int), cudaMemcpyDeviceToHost, xstream);
   cudaMemcpyAsync(hp_do_starts, d_do_starts, ndo * sizeof(int), cudaMemcpyDeviceToHost, xstream);
   cudaMemcpyAsync(hp_do_ends, d_do_ends, ndo * sizeof(int), cudaMemcpyDeviceToHost, xstream);
+  cudaEventRecord(ev_small, xstream);
+  if (dst_luma)
+    cudaMemcpyAsync(dst_luma, d_luma, (size_t)P * F * sizeof(uint16_t), cudaMemcpyDeviceToHost, xstream);
   // ---- K6 chroma on the P detected fields
   ca.fields = P;
   ca.total = (long long)P * spp;
@@ -865,8 +942,11 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     end_stage(kStageDropouts, ev_);
   }
   if (!check_cuda("chroma concealment")) return false;
+  cudaEventRecord(ev_chroma, stream);
+  cudaStreamWaitEvent(xstream, ev_chroma, 0);
   if (dst_chroma)
-    cudaMemcpyAsync(dst_chroma, d_chroma, (size_t)P * F * sizeof(uint16_t), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(dst_chroma, d_chroma, (size_t)P * F * sizeof(uint16_t), cudaMemcpyDeviceToHost, xstream);
+  cudaEventRecord(ev_out_done[oset], xstream);
   if (debug) {
     dbg_ll.resize((size_t)P * LPF);
     cudaMemcpyAsync(dbg_ll.data(), d_ll, dbg_ll.size() * sizeof(double), cudaMemcpyDeviceToHost, stream);
@@ -881,8 +961,21 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     cudaMemcpyAsync(dbg_pre.data(), d_dem, dbg_pre.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
   }
   t_host = host_clock();
-  if (!sync("dropouts")) return false;
+  {
+    // the decode stream and the dropout lists; the plane copies may continue
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev_small);
+    if (e != cudaSuccess) {
+      err = std::string("decode: ") + cudaGetErrorString(e);
+      status = CUVHS_ERR_CUDA;
+      return false;
+    }
+    collect_stage_times();
+    if (!check_cuda("decode")) return false;
+  }
   host_phase(kHostFinalWait, t_host);
+  if (pipelined) out_set = 1 - oset;
+  drain.keep = defer;
   last_fields = P;
   res.outputs_copied = dst_luma != nullptr || dst_chroma != nullptr;
   // ---- field metadata: parity alternation (pipeline.cu:2575-2610)

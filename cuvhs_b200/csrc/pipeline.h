@@ -60,6 +60,23 @@ struct Context {
   cudaEvent_t ev_piece[kInputPieces] = {};
   cudaEvent_t ev_luma = nullptr;
   cudaEvent_t ev_edges = nullptr;
+  // Cross-chunk pipelining of a capture held in host memory: while a chunk
+  // decodes, the next chunk's window is copied into the other raw buffer on
+  // the prefetch stream, and with page-locked destinations a chunk's planes
+  // leave from one of two output sets while the next chunk already runs.
+  cudaStream_t hstream = nullptr;  // host->device input copies
+  uint8_t* d_raw_set[2] = {};
+  uint16_t* d_luma_set[2] = {};
+  uint16_t* d_chroma_set[2] = {};
+  int raw_set = 0, out_set = 0;
+  cudaEvent_t ev_prefetch = nullptr, ev_small = nullptr, ev_chroma = nullptr;
+  cudaEvent_t ev_out_done[2] = {};
+  struct Prefetch {
+    bool valid = false;
+    uint64_t raw_offset = 0;
+    size_t n_read = 0, total = 0;
+    int set = 0;
+  } pf;
   std::string err;
   cuvhs_status status = CUVHS_OK;
   std::vector<void*> allocations;
@@ -148,8 +165,14 @@ struct Context {
   // dst_luma / dst_chroma: optional page-locked host destinations for the
   // chunk's fields (num_fields fields of room each); when given, the planes
   // are copied there as soon as each is final and res.outputs_copied is set.
+  // cap_base / cap_n: the whole host capture `src` lies in (src = cap_base +
+  // raw_offset); when given, the next chunk's window is prefetched.  defer:
+  // return before the plane copies end (drain_copies() waits for them).
   bool decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avail, uint64_t raw_offset, int num_fields,
-                    ChunkResult& res, uint16_t* dst_luma = nullptr, uint16_t* dst_chroma = nullptr);
+                    ChunkResult& res, uint16_t* dst_luma = nullptr, uint16_t* dst_chroma = nullptr,
+                    const uint8_t* cap_base = nullptr, size_t cap_n = 0, bool defer = false);
+  // Waits for deferred plane copies and input prefetches; returns false on a CUDA error.
+  bool drain_copies();
 };
 
 // .tbc.json text (reference format, src/io/tbc_writer.cpp:89-175).

@@ -161,6 +161,26 @@ def test_pinned_buffers_give_identical_output(name, batch):
 
 
 @pytest.mark.gpu
+def test_field_locations_past_32_bits():
+    """A chunk whose first sample is capture sample 5*2^32 + 12345 (a long
+    stream): field locations are that offset plus the chunk-relative ones,
+    everything else is unchanged."""
+    x = workload("small28")
+    off = 5 * 2**32 + 12345
+    with cv.Decoder(28.0) as d:
+        nf = min(d.batch_fields, x.size // d.samples_per_field)
+        a, na = d.decode_chunk(x, 0, nf)
+        d.reset()
+        b, nb = d.decode_chunk(x, off, nf)
+    assert a.n_fields == b.n_fields > 0
+    assert np.array_equal(b.file_loc - np.uint64(off), a.file_loc)
+    assert nb == na + off
+    assert np.array_equal(a.luma, b.luma) and np.array_equal(a.chroma, b.chroma)
+    assert np.array_equal(a.is_first_field, b.is_first_field)
+    assert [json.loads(b.json)["fields"][i]["fileLoc"] for i in range(b.n_fields)] == [int(v) for v in b.file_loc]
+
+
+@pytest.mark.gpu
 def test_cli_end_to_end(tmp_path):
     import subprocess
     name = "plain40_28"

@@ -66,6 +66,11 @@ class BatchItem(ctypes.Structure):
                 ("out", ctypes.POINTER(Output)), ("status", ctypes.c_int)]
 
 
+class AdjointParams(ctypes.Structure):
+    _fields_ = [("deemph", ctypes.c_double * 4), ("carrier_hz", ctypes.c_double), ("deviation", ctypes.c_double),
+                ("line_offset", ctypes.c_void_p), ("chroma_phase", ctypes.c_void_p)]
+
+
 class SynthParams(ctypes.Structure):
     _fields_ = [("sample_rate_hz", ctypes.c_double), ("n_fields", ctypes.c_int), ("tail_lines", ctypes.c_int),
                 ("seed", ctypes.c_uint64), ("snr_db", ctypes.c_double), ("jitter_bound", ctypes.c_double),
@@ -74,7 +79,9 @@ class SynthParams(ctypes.Structure):
                 ("headswitch_max", ctypes.c_int), ("speed_drift", ctypes.c_double),
                 ("start_line", ctypes.c_double), ("chroma_level", ctypes.c_double),
                 ("carrier_offset_hz", ctypes.c_double), ("deviation_scale", ctypes.c_double),
-                ("first_track", ctypes.c_int), ("threads", ctypes.c_int)]
+                ("first_track", ctypes.c_int), ("threads", ctypes.c_int),
+                ("preemph_perturb", ctypes.c_double * 3), ("line_offset_bound", ctypes.c_double),
+                ("chroma_phase_bound", ctypes.c_double)]
 
 
 _vp = ctypes.c_void_p
@@ -132,11 +139,30 @@ lib.cuvhs_batch_last_error.argtypes = [_vp]
 lib.cuvhs_batch_last_error.restype = ctypes.c_char_p
 lib.cuvhs_batch_json.argtypes = [ctypes.POINTER(BatchItem), ctypes.c_char_p, ctypes.c_longlong]
 lib.cuvhs_batch_json.restype = ctypes.c_longlong
+lib.cuvhs_adjoint_create.argtypes = [ctypes.POINTER(Config), _vp, ctypes.c_size_t, ctypes.c_int, ctypes.POINTER(_vp)]
+lib.cuvhs_adjoint_create.restype = ctypes.c_int
+lib.cuvhs_adjoint_destroy.argtypes = [_vp]
+lib.cuvhs_adjoint_fields.argtypes = [_vp]
+lib.cuvhs_adjoint_fields.restype = ctypes.c_int
+lib.cuvhs_adjoint_default_params.argtypes = [_vp, ctypes.POINTER(AdjointParams)]
+lib.cuvhs_adjoint_default_params.restype = ctypes.c_int
+lib.cuvhs_adjoint_set_target.argtypes = [_vp, _vp, _vp]
+lib.cuvhs_adjoint_set_target.restype = ctypes.c_int
+lib.cuvhs_adjoint_fwd.argtypes = [_vp, ctypes.POINTER(AdjointParams), ctypes.POINTER(ctypes.c_double), _vp, _vp]
+lib.cuvhs_adjoint_fwd.restype = ctypes.c_int
+lib.cuvhs_adjoint_bwd.argtypes = [_vp, ctypes.POINTER(AdjointParams), ctypes.POINTER(ctypes.c_double),
+                                  ctypes.POINTER(AdjointParams)]
+lib.cuvhs_adjoint_bwd.restype = ctypes.c_int
+lib.cuvhs_adjoint_array.argtypes = [_vp, ctypes.c_char_p, _vp, ctypes.c_longlong]
+lib.cuvhs_adjoint_array.restype = ctypes.c_longlong
 lib.cuvhs_synth_default_params.argtypes = [ctypes.POINTER(SynthParams)]
 lib.cuvhs_synth_length.argtypes = [ctypes.POINTER(SynthParams)]
 lib.cuvhs_synth_length.restype = ctypes.c_longlong
 lib.cuvhs_synth_ntsc.argtypes = [ctypes.POINTER(SynthParams), _vp, ctypes.c_longlong]
 lib.cuvhs_synth_ntsc.restype = ctypes.c_int
+lib.cuvhs_synth_lines.argtypes = [ctypes.POINTER(SynthParams), ctypes.c_longlong, _vp, _vp, _vp, ctypes.c_longlong]
+lib.cuvhs_synth_lines.restype = ctypes.c_longlong
+lib.cuvhs_synth_preemphasis.argtypes = [ctypes.POINTER(SynthParams), _vp, _vp]
 
 # every symbol include/cuvhs.h and include/cuvhs_synth.h declare
 EXPORTED = [
@@ -146,8 +172,10 @@ EXPORTED = [
     "cuvhs_decode_file", "cuvhs_set_debug", "cuvhs_debug_array", "cuvhs_stream", "cuvhs_set_timing",
     "cuvhs_stage_count", "cuvhs_stage_name", "cuvhs_stage_times", "cuvhs_reset_stage_times", "cuvhs_launch_count",
     "cuvhs_dropouts_noalloc", "cuvhs_batch_create", "cuvhs_batch_destroy", "cuvhs_batch_lanes",
-    "cuvhs_batch_decode", "cuvhs_batch_last_error", "cuvhs_batch_json", "cuvhs_synth_default_params",
-    "cuvhs_synth_length", "cuvhs_synth_ntsc",
+    "cuvhs_batch_decode", "cuvhs_batch_last_error", "cuvhs_batch_json", "cuvhs_adjoint_create",
+    "cuvhs_adjoint_destroy", "cuvhs_adjoint_fields", "cuvhs_adjoint_default_params", "cuvhs_adjoint_set_target",
+    "cuvhs_adjoint_fwd", "cuvhs_adjoint_bwd", "cuvhs_adjoint_array", "cuvhs_synth_default_params",
+    "cuvhs_synth_length", "cuvhs_synth_ntsc", "cuvhs_synth_lines", "cuvhs_synth_preemphasis",
 ]
 
 
@@ -157,8 +185,30 @@ def synth_params(**kw) -> SynthParams:
     for k, v in kw.items():
         if not hasattr(p, k):
             raise KeyError(k)
+        if k == "preemph_perturb":
+            v = (ctypes.c_double * 3)(*v)
         setattr(p, k, v)
     return p
+
+
+def synth_lines(**kw):
+    """Program-line table of a synthetic capture: (start sample, picture
+    delay in samples, colour-under phase offset in radians) per line."""
+    p = synth_params(**kw)
+    n = lib.cuvhs_synth_length(ctypes.byref(p))
+    m = lib.cuvhs_synth_lines(ctypes.byref(p), n, None, None, None, 0)
+    st, off, ph = (np.empty(m, np.float64) for _ in range(3))
+    lib.cuvhs_synth_lines(ctypes.byref(p), n, st.ctypes.data, off.ctypes.data, ph.ctypes.data, m)
+    return st, off, ph
+
+
+def synth_preemphasis(**kw):
+    """(b, a) of the capture's pre-emphasis biquad, a[0] = 1."""
+    p = synth_params(**kw)
+    b = np.empty(3, np.float64)
+    a = np.empty(3, np.float64)
+    lib.cuvhs_synth_preemphasis(ctypes.byref(p), b.ctypes.data, a.ctypes.data)
+    return b, a
 
 
 def synth_capture(**kw) -> np.ndarray:

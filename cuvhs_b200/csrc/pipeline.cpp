@@ -436,6 +436,39 @@ static double host_burst_phase(const float* b, int H, const Format& fmt) {
   return std::fmod(std::atan2(Qt, It) * 180.0 / PI + 360.0, 360.0);
 }
 
+DemodArgs Context::demod_args(int T) const {
+  DemodArgs da;
+  da.raw = d_raw;
+  da.total = (long long)T * spp;
+  da.tiles = T;
+  da.spp = spp;
+  da.tile = des.tile;
+  da.ga = d_ga;
+  da.gb = d_gb;
+  da.tw_a = d_twa;
+  da.tw_b = d_twb;
+  da.tw_a_inv = d_twa_inv;
+  da.tw_b_inv = d_twb_inv;
+  da.a_pos = des.a_pos;
+  da.a_out = des.a_out;
+  da.b_pos = des.b_pos;
+  da.b_out = des.b_out;
+  da.rot_re = des.rot_re;
+  da.rot_im = des.rot_im;
+  da.d0 = (float)des.d0;
+  da.demod_scale = des.demod_scale;
+  da.demod_offset = des.demod_offset;
+  da.corr_video = des.corr_video;
+  da.corr_sync = des.corr_sync;
+  da.dem = d_dem;
+  da.env = d_env;
+  da.env_part = d_env_part;
+  da.env_blocks = env_blocks;
+  da.video = d_video;
+  da.sync = d_sync;
+  return da;
+}
+
 // Decode one chunk.  `src` is host memory unless `src_on_device`.
 bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avail, uint64_t raw_offset,
                            int num_fields, ChunkResult& res, uint16_t* dst_luma, uint16_t* dst_chroma,
@@ -478,35 +511,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   d_raw = d_raw_set[rset];
   raw_set = rset;
   // ---- K1: FM demod over T tiles
-  DemodArgs da;
-  da.raw = d_raw;
-  da.total = (long long)T * spp;
-  da.tiles = T;
-  da.spp = spp;
-  da.tile = des.tile;
-  da.ga = d_ga;
-  da.gb = d_gb;
-  da.tw_a = d_twa;
-  da.tw_b = d_twb;
-  da.tw_a_inv = d_twa_inv;
-  da.tw_b_inv = d_twb_inv;
-  da.a_pos = des.a_pos;
-  da.a_out = des.a_out;
-  da.b_pos = des.b_pos;
-  da.b_out = des.b_out;
-  da.rot_re = des.rot_re;
-  da.rot_im = des.rot_im;
-  da.d0 = (float)des.d0;
-  da.demod_scale = des.demod_scale;
-  da.demod_offset = des.demod_offset;
-  da.corr_video = des.corr_video;
-  da.corr_sync = des.corr_sync;
-  da.dem = d_dem;
-  da.env = d_env;
-  da.env_part = d_env_part;
-  da.env_blocks = env_blocks;
-  da.video = d_video;
-  da.sync = d_sync;
+  DemodArgs da = demod_args(T);
   // ---- input: the chunk window, the rest set to the u8 mid level (0.0 after
   // conversion).  Host input arrives in pieces on the copy stream; K1a of
   // tiles [fa, fb) reads chunk samples up to (fb-1)*spp - kOverlap + tile, so

@@ -173,6 +173,8 @@ struct Context {
                     const uint8_t* cap_base = nullptr, size_t cap_n = 0, bool defer = false);
   // Waits for deferred plane copies and input prefetches; returns false on a CUDA error.
   bool drain_copies();
+  // K1 arguments over T tiles of the current raw buffer into the context's buffers.
+  DemodArgs demod_args(int T) const;
 };
 
 // .tbc.json text (reference format, src/io/tbc_writer.cpp:89-175).

@@ -101,7 +101,8 @@ struct Content {
   int n_frame_lines;
   double us;       // samples per microsecond
 
-  void eval(long long lam, double u, double* ire, double* cu, double* cv) const {
+  // du: delay of the picture and burst against the line's sync, samples
+  void eval(long long lam, double u, double du, double* ire, double* cu, double* cv) const {
     // Frame-relative line and half-line.
     long long fl = lam % 525;
     if (fl < 0) fl += 525;
@@ -109,6 +110,7 @@ struct Content {
     int hidx = (int)(2 * fl + (u >= half ? 1 : 0));
     double v = (u >= half) ? u - half : u;
     double t_us = u / us;
+    double tp_us = (u - du) / us;  // picture and burst time
     double tv_us = v / us;
     long long frame = (lam >= 0 ? lam : lam - 524) / 525;
     // Field-relative line numbering (field 1 starts at frame line 0, field 2 at
@@ -138,13 +140,13 @@ struct Content {
       // Colour burst on lines after the vertical interval.
       int fline = (int)field_line_d;
       if (fline >= 9) {
-        double bw = window_level(t_us, 5.3, 7.8, 0.3);
+        double bw = window_level(tp_us, 5.3, 7.8, 0.3);
         cu_ += -20.0 * bw;
       }
       if (fline >= 20 && fline < 262) {
         double a0 = 9.4, a1 = 62.4;
-        double act = window_level(t_us, a0, a1, 0.25);
-        double x = (t_us - a0) / (a1 - a0);
+        double act = window_level(tp_us, a0, a1, 0.25);
+        double x = (tp_us - a0) / (a1 - a0);
         double yl = 7.5, uu = 0.0, vv = 0.0;
         if (fline < 170) {
           // bars with raised-cosine transitions
@@ -193,6 +195,78 @@ void shelf_high(double f0, double dbgain, double fs, double q, double b[3], doub
   a[0] = (A + 1) - (A - 1) * c + 2 * sa * alpha;
   a[1] = 2 * ((A - 1) - (A + 1) * c);
   a[2] = (A + 1) - (A - 1) * c - 2 * sa * alpha;
+}
+
+// Seeded per-program-line perturbations, independent of threads and ranges.
+double line_uniform(uint64_t seed, uint64_t salt, long long lam) {
+  SplitMix m(mix_seed(seed ^ salt, (uint64_t)lam));
+  return 2.0 * m.uniform() - 1.0;
+}
+double line_offset(const cuvhs_synth_params* p, long long lam) {
+  return p->line_offset_bound > 0 ? p->line_offset_bound * line_uniform(p->seed, 0x11F5E7ull, lam) : 0.0;
+}
+double line_phase(const cuvhs_synth_params* p, long long lam) {
+  return p->chroma_phase_bound > 0 ? p->chroma_phase_bound * line_uniform(p->seed, 0xC4A5Eull, lam) : 0.0;
+}
+
+// The pre-emphasis shelf (the one the decoder inverts), its design parameters
+// optionally perturbed, normalised to a0 = 1.
+void preemphasis(const cuvhs_synth_params* p, double b[3], double a[3]) {
+  shelf_high(273755.82 * (1.0 + p->preemph_perturb[0]), 13.9794 * (1.0 + p->preemph_perturb[1]),
+             p->sample_rate_hz, 0.462088186 * (1.0 + p->preemph_perturb[2]), b, a);
+  for (int i = 0; i < 3; i++) b[i] /= a[0];
+  a[1] /= a[0];
+  a[2] /= a[0];
+  a[0] = 1.0;
+}
+
+// Line-start table: r[k] is the RF sample where program line lam0 + k starts
+// (seeded start phase, per-line timebase random walk, speed drift, head
+// switch jumps).
+void line_table(const cuvhs_synth_params* p, size_t n, long long& lam0_out, std::vector<double>& r) {
+  const double fs = p->sample_rate_hz;
+  const double spl = fs / kLineRate;
+  SplitMix master(mix_seed(p->seed, 0x5EED));
+  // Start position: seeded phase within the first frame, so the file starts mid-field.
+  double start_line = p->start_line >= 0 ? p->start_line : 20.0 + 480.0 * master.uniform();
+  long long lam0 = (long long)std::floor(start_line);
+  double u0 = (start_line - (double)lam0) * spl;
+
+  size_t n_lines = (size_t)std::ceil((double)n / (spl * 0.95)) + 8;
+  r.assign(n_lines + 1, 0.0);
+  {
+    SplitMix jr(mix_seed(p->seed, 0x717));
+    double delta = 0.0, prev_delta = 0.0;
+    r[0] = -u0;
+    for (size_t k = 1; k <= n_lines; k++) {
+      long long lam = lam0 + (long long)k;
+      double step = jr.gauss() * p->jitter_step;
+      delta += step;
+      if (p->jitter_bound > 0) {
+        if (delta > p->jitter_bound) delta = 2 * p->jitter_bound - delta;
+        if (delta < -p->jitter_bound) delta = -2 * p->jitter_bound - delta;
+        delta = std::max(-p->jitter_bound, std::min(p->jitter_bound, delta));
+      } else {
+        delta = 0.0;
+      }
+      double speed = 1.0;
+      if (p->speed_drift != 0.0) {
+        speed = 1.0 + p->speed_drift * std::sin(2.0 * kPi * (double)lam / 21000.0);
+      }
+      double len = spl * speed + (delta - prev_delta);
+      prev_delta = delta;
+      // head switch: a time jump 6 lines before each field's vertical interval
+      long long fl = lam % 525;
+      if (p->headswitch_max > 0 && (fl == 519 || fl == 256)) {
+        int span = std::max(0, p->headswitch_max - p->headswitch_min);
+        int jump = p->headswitch_min + (int)(jr.uniform() * (span + 1));
+        len += (double)jump;
+      }
+      r[k] = r[k - 1] + len;
+    }
+  }
+
+  lam0_out = lam0;
 }
 
 template <typename F>
@@ -252,46 +326,10 @@ extern "C" int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long 
   const size_t n = (size_t)n_out;
   int threads = p->threads > 0 ? p->threads : (int)std::max(1u, std::thread::hardware_concurrency());
 
-  SplitMix master(mix_seed(p->seed, 0x5EED));
-  // Start position: seeded phase within the first frame, so the file starts mid-field.
-  double start_line = p->start_line >= 0 ? p->start_line : 20.0 + 480.0 * master.uniform();
-  long long lam0 = (long long)std::floor(start_line);
-  double u0 = (start_line - (double)lam0) * spl;
-
-  // ---- line-start table r[k] (RF sample position where program line lam0+k starts)
-  size_t n_lines = (size_t)std::ceil((double)n / (spl * 0.95)) + 8;
-  std::vector<double> r(n_lines + 1);
-  {
-    SplitMix jr(mix_seed(p->seed, 0x717));
-    double delta = 0.0, prev_delta = 0.0;
-    r[0] = -u0;
-    for (size_t k = 1; k <= n_lines; k++) {
-      long long lam = lam0 + (long long)k;
-      double step = jr.gauss() * p->jitter_step;
-      delta += step;
-      if (p->jitter_bound > 0) {
-        if (delta > p->jitter_bound) delta = 2 * p->jitter_bound - delta;
-        if (delta < -p->jitter_bound) delta = -2 * p->jitter_bound - delta;
-        delta = std::max(-p->jitter_bound, std::min(p->jitter_bound, delta));
-      } else {
-        delta = 0.0;
-      }
-      double speed = 1.0;
-      if (p->speed_drift != 0.0) {
-        speed = 1.0 + p->speed_drift * std::sin(2.0 * kPi * (double)lam / 21000.0);
-      }
-      double len = spl * speed + (delta - prev_delta);
-      prev_delta = delta;
-      // head switch: a time jump 6 lines before each field's vertical interval
-      long long fl = lam % 525;
-      if (p->headswitch_max > 0 && (fl == 519 || fl == 256)) {
-        int span = std::max(0, p->headswitch_max - p->headswitch_min);
-        int jump = p->headswitch_min + (int)(jr.uniform() * (span + 1));
-        len += (double)jump;
-      }
-      r[k] = r[k - 1] + len;
-    }
-  }
+  long long lam0 = 0;
+  std::vector<double> r;
+  line_table(p, n, lam0, r);
+  const size_t n_lines = r.size() - 1;
 
   // ---- dropouts: per-line seeded events, stored as RF sample spans
   struct Span { double a, b; };
@@ -325,7 +363,11 @@ extern "C" int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long 
       double u = ((double)i - r[k]) * (spl / len);
       long long lam = lam0 + (long long)k;
       double y, cu, cv;
-      content.eval(lam, u, &y, &cu, &cv);
+      // picture timebase: the delay runs linearly from this line's offset at
+      // its start to the next line's at its end
+      const double d0 = line_offset(p, lam), d1 = line_offset(p, lam + 1);
+      const double du = d0 + (u / spl) * (d1 - d0);
+      content.eval(lam, u, du, &y, &cu, &cv);
       ire[i] = (float)y;
       // colour-under: rotation by +/-90 degrees per line, alternating by field track
       long long fl = lam % 525;
@@ -335,21 +377,19 @@ extern "C" int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long 
       int track = (int)((field_index + p->first_track) & 1);
       int rot = track ? 1 : 3;
       int q = (int)(((field_line * rot) % 4 + 4) % 4);
-      double theta = 2.0 * kPi * std::fmod(kChromaUnder * (double)i / fs, 1.0) + q * (kPi * 0.5);
+      // the picture delay moves the colour-under carrier with the picture
+      double theta = 2.0 * kPi * std::fmod(kChromaUnder * ((double)i - du) / fs, 1.0) + q * (kPi * 0.5) +
+                     line_phase(p, lam);
       chroma[i] = (float)(cu * std::sin(theta) + cv * std::cos(theta));
     }
   });
 
   // ---- pass 2 (sequential): pre-emphasis IIR on the IRE signal, then FM phase
   double b[3], a[3];
-  shelf_high(273755.82, 13.9794, fs, 0.462088186, b, a);
-  for (int i = 0; i < 3; i++) { b[i] /= a[0]; }
-  a[1] /= a[0];
-  a[2] /= a[0];
-  a[0] = 1.0;
+  preemphasis(p, b, a);
   {
     double x1 = ire[0], x2 = ire[0];
-    double y1 = ire[0], y2 = ire[0];  // DC gain is exactly 1
+    double y1 = ire[0], y2 = ire[0];  // the shelf's DC gain is 1
     double phase = 0.0;
     const double dev = p->deviation_scale * kHzIre;
     const double fc = kIre0 + p->carrier_offset_hz;
@@ -397,3 +437,20 @@ extern "C" int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long 
   });
   return 0;
 }
+
+extern "C" long long cuvhs_synth_lines(const cuvhs_synth_params* p, long long n, double* start, double* offset,
+                                       double* phase, long long cap) {
+  if (!p || n <= 0 || !(p->sample_rate_hz > 4e6)) return -1;
+  long long lam0 = 0;
+  std::vector<double> r;
+  line_table(p, (size_t)n, lam0, r);
+  const long long m = (long long)r.size() - 1;
+  for (long long k = 0; k < std::min(m, cap); k++) {
+    if (start) start[k] = r[(size_t)k];
+    if (offset) offset[k] = line_offset(p, lam0 + k);
+    if (phase) phase[k] = line_phase(p, lam0 + k);
+  }
+  return m;
+}
+
+extern "C" void cuvhs_synth_preemphasis(const cuvhs_synth_params* p, double b[3], double a[3]) { preemphasis(p, b, a); }

@@ -20,6 +20,9 @@
  *   cuvhs_debug_array                 the stage outputs the reference keeps in device
  *                                     buffers (d_pulse_*, d_linelocs, d_is_first_field,
  *                                     d_do_*; src/pipeline/pipeline.h:52-87)
+ *   cuvhs_adjoint_*                   no counterpart: the reference has no gradients; a
+ *                                     differentiable decode model with adjoint kernels for
+ *                                     tape parameter calibration
  *   cuvhs_batch_*                     no counterpart: the reference decodes one capture per
  *                                     process (src/main.cpp:97-165); a batch decodes many
  *                                     captures of mixed sample rates concurrently, each
@@ -213,6 +216,62 @@ cuvhs_status cuvhs_batch_decode(cuvhs_batch* b, cuvhs_batch_item* items, int n_i
 const char* cuvhs_batch_last_error(const cuvhs_batch* b);
 /* .tbc.json text of one decoded item (as cuvhs_json for a single capture). */
 long long cuvhs_batch_json(const cuvhs_batch_item* item, char* dst, long long cap);
+
+/* ------------------------------------------------------------- calibration
+ * A differentiable decode model and its adjoint, for calibrating a tape's
+ * decode parameters against a known test pattern.  No counterpart in the
+ * reference, which has no gradients.  cuvhs_adjoint_create decodes the
+ * capture's first `fields` fields with the normal decoder and keeps, on the
+ * device, what the parameter-dependent part of the decode starts from: the
+ * FM demod, the colour-under pre-band-pass, the refined line locations and
+ * the chroma tracks.  The model then redoes, for parameters
+ *   de-emphasis  H(z) = (n0 + n1 z^-1 + n2 z^-2) / (1 + m1 z^-1 + m2 z^-2),
+ *                n0 = 1 + m1 + m2 - n1 - n2 (unit DC gain), times the
+ *                decoder's 3 MHz super-Gaussian video low-pass,
+ *   carrier_hz   FM carrier offset removed from the video,
+ *   deviation    FM deviation scale,
+ *   line_offset  per-line start offsets (samples) added to the line locations,
+ *   chroma_phase per-line colour-under phase offsets (radians),
+ * the video filter, the Catmull-Rom luma and chroma resampling, the
+ * heterodyne, the 1024-point chroma line band-pass and the burst-driven ACC
+ * gain (FP32 samples, FP64 positions), and
+ *   L = mean (Y - Y*)^2 + mean (C - C*)^2
+ * over lines 10..261, columns 80..893 (back porch with the burst, and the
+ * active picture) of every field, in TBC units, against target planes.  cuvhs_adjoint_bwd returns dL/d every
+ * parameter through hand-written adjoint kernels, recomputing the forward
+ * quantities it needs instead of storing them. */
+typedef struct cuvhs_adjoint cuvhs_adjoint;
+
+#define CUVHS_ADJOINT_ROWS 264 /* line_offset entries per field (rows 0..263) */
+
+typedef struct cuvhs_adjoint_params {
+  double deemph[4];      /* n1, n2, m1, m2 */
+  double carrier_hz;
+  double deviation;
+  double* line_offset;   /* [fields * CUVHS_ADJOINT_ROWS] */
+  double* chroma_phase;  /* [fields * CUVHS_FIELD_HEIGHT] */
+} cuvhs_adjoint_params;
+
+cuvhs_status cuvhs_adjoint_create(const cuvhs_config* cfg, const uint8_t* samples, size_t n, int fields,
+                                  cuvhs_adjoint** out);
+void cuvhs_adjoint_destroy(cuvhs_adjoint* a);
+int cuvhs_adjoint_fields(const cuvhs_adjoint* a); /* fields the model covers (<= requested) */
+/* Nominal parameters (the decoder's own de-emphasis, no offsets); the caller
+ * provides the per-line arrays, which are zeroed. */
+cuvhs_status cuvhs_adjoint_default_params(const cuvhs_adjoint* a, cuvhs_adjoint_params* p);
+/* Target planes [fields][263][910] in TBC units. */
+cuvhs_status cuvhs_adjoint_set_target(cuvhs_adjoint* a, const float* luma, const float* chroma);
+/* Forward: the loss (needs a target) and, optionally, the model's planes. */
+cuvhs_status cuvhs_adjoint_fwd(cuvhs_adjoint* a, const cuvhs_adjoint_params* p, double* loss, float* luma,
+                               float* chroma);
+/* Backward: the loss and dL/dparameters into grad (whose arrays the caller provides). */
+cuvhs_status cuvhs_adjoint_bwd(cuvhs_adjoint* a, const cuvhs_adjoint_params* p, double* loss,
+                               cuvhs_adjoint_params* grad);
+/* Model inputs and state for inspection: "linelocs" (f64, fields*525),
+ * "gains" (f32, fields*263, the ACC gains of the last pass), "tracks" (i32,
+ * fields), "demod" and "pre" (f32, fields*tile_stride).  Returns the element
+ * count; copies at most cap. */
+long long cuvhs_adjoint_array(const cuvhs_adjoint* a, const char* name, void* dst, long long cap);
 
 #ifdef __cplusplus
 }

@@ -31,6 +31,13 @@ typedef struct cuvhs_synth_params {
   double deviation_scale;    /* FM deviation scale (1 = nominal) */
   int first_track;           /* head track of the first field (0/1) */
   int threads;               /* 0 = all host cores */
+  /* calibration perturbations (all 0 = the nominal tape) */
+  double preemph_perturb[3]; /* relative changes of the pre-emphasis shelf's corner frequency, gain (dB)
+                                and Q; the 2-pole filter stays stable */
+  double line_offset_bound;  /* per-line delay of the picture and burst against the sync at the line's
+                                start, uniform in +/- bound samples; within a line the delay runs
+                                linearly to the next line's */
+  double chroma_phase_bound; /* per-line colour-under phase offset, uniform in +/- bound radians */
 } cuvhs_synth_params;
 
 void cuvhs_synth_default_params(cuvhs_synth_params* p);
@@ -38,6 +45,14 @@ void cuvhs_synth_default_params(cuvhs_synth_params* p);
 long long cuvhs_synth_length(const cuvhs_synth_params* p);
 /* Fill out[0..n) with the capture; returns 0 on success. */
 int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long long n);
+/* The program-line table of the capture: for up to cap lines, the RF sample
+ * where each line starts, its picture delay at the line start (samples) and
+ * its colour-under phase offset (radians).  Returns the number of lines. */
+long long cuvhs_synth_lines(const cuvhs_synth_params* p, long long n, double* start, double* offset, double* phase,
+                            long long cap);
+/* The pre-emphasis biquad the parameters use, normalised to a0 = 1:
+ * b[0..2], a[0..2]. */
+void cuvhs_synth_preemphasis(const cuvhs_synth_params* p, double b[3], double a[3]);
 
 #ifdef __cplusplus
 }

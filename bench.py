@@ -371,6 +371,76 @@ def run_stream(args, rank, world, local):
     return 0
 
 
+def run_adjoint(args, rank, world, local):
+    """Adjoint calibration: 8 fields at 28 MHz u8 synthesized from the seeded
+    test pattern twice -- nominally (the target, decoded by the model at the
+    nominal parameters) and with a perturbed pre-emphasis shelf (+10% corner,
+    -10% gain, +10% Q), +30 kHz carrier, +3% deviation, per-line picture delays
+    up to 1.5 samples and per-line chroma phases up to 20 degrees.  A step is
+    one forward + backward pass (loss and full gradient) on the device; the
+    line also reports a 200-step calibration and a central-difference check of
+    the global parameters.  Under torchrun every rank runs its own replica."""
+    import torch
+    torch.cuda.set_device(local)
+    import cuvhs_b200 as cv
+    from cuvhs_b200.calibrate import Adjoint, calibrate, shelf_deemph
+    base = dict(sample_rate_hz=28e6, n_fields=10, seed=404, snr_db=40, jitter_bound=0.5)
+    pert = dict(base, carrier_offset_hz=30e3, deviation_scale=1.03, preemph_perturb=(0.1, -0.1, 0.1),
+                line_offset_bound=1.5, chroma_phase_bound=np.deg2rad(20))
+    clean = Adjoint(cv.synth_capture(**base), 28.0, fields=8, device=local)
+    p0 = clean.default_params()
+    yt, ct = clean.planes(p0)
+    adj = Adjoint(cv.synth_capture(**pert), 28.0, fields=8, device=local)
+    adj.set_target(yt, ct)
+    for _ in range(args.warmup):
+        adj.grad(p0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        adj.grad(p0)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / args.steps
+    loss, g = adj.grad(p0)
+
+    def fd(setter, h):
+        a = p0.copy()
+        setter(a, h)
+        b = p0.copy()
+        setter(b, -h)
+        return (adj.loss(a) - adj.loss(b)) / (2 * h)
+    rel = []
+    for j, h in enumerate((1e-3, 1e-3, 1e-6, 1e-6)):
+        def st(p, d, j=j):
+            p.deemph[j] += d
+        rel.append(abs(g.deemph[j] - fd(st, h)) / abs(fd(st, h)))
+    f_c = fd(lambda p, d: setattr(p, "carrier_hz", p.carrier_hz + d), 1.0)
+    f_d = fd(lambda p, d: setattr(p, "deviation", p.deviation + d), 1e-3)
+    rel += [abs(g.carrier_hz - f_c) / abs(f_c), abs(g.deviation - f_d) / abs(f_d)]
+    t1 = time.perf_counter()
+    pc, shelf, hist = calibrate(adj, p0, steps=200)
+    t_cal = time.perf_counter() - t1
+    if rank == 0:
+        print(json.dumps({
+            "metric": "adjoint gradient evaluations/s (forward + backward), 8 NTSC fields at 28 MHz u8",
+            "value": round(1.0 / dt, 2), "unit": "gradients/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "8 fields at 28 MHz u8, perturbed pre-emphasis/carrier/deviation/"
+                                   "line offsets/chroma phase against the nominal tape",
+                       "parameters": 6 + adj.fields * (264 + 263)},
+            "gradient_check": {"max_rel_err_vs_central_differences": float(max(rel)),
+                               "params": "n1 n2 m1 m2 carrier deviation"},
+            "calibration": {"steps": 200, "seconds": round(t_cal, 2), "loss_start": round(hist[0], 1),
+                            "loss_end": round(hist[-1], 1), "carrier_hz": round(pc.carrier_hz, 1),
+                            "carrier_true": 30e3, "deviation": round(pc.deviation, 5), "deviation_true": 1.03,
+                            "shelf_scales": [round(float(v), 4) for v in shelf],
+                            "shelf_true": [1.1, 0.9, 1.1]},
+        }))
+    adj.close()
+    clean.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -383,9 +453,10 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="one device-resident decode of the workload with a 48-field allocation, "
                          "for kernel profilers; prints nothing else")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "batched64", "stream40"],
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "batched64", "stream40", "adjoint8"],
                     help="batched64: the 64-capture mixed batch through cuvhs_batch_decode; "
-                         "stream40: one long 40 MHz capture streamed from pinned memory")
+                         "stream40: one long 40 MHz capture streamed from pinned memory; "
+                         "adjoint8: forward+backward passes of the calibration model")
     ap.add_argument("--stream-fields", type=int, default=6000, help="stream40: fields in the capture")
     ap.add_argument("--lanes", type=int, default=0, help="batched64: concurrent decoders (0 = library default)")
     args = ap.parse_args()
@@ -402,6 +473,8 @@ def main():
         return run_batched(args, rank, world, local)
     if args.workload == "stream40":
         return run_stream(args, rank, world, local)
+    if args.workload == "adjoint8":
+        return run_adjoint(args, rank, world, local)
 
     import torch
     import torch.distributed as dist

@@ -2,10 +2,11 @@
 // cuvhs_adjoint_*).  The device kernels are in adjoint.cu.
 //
 // The video filter's block spectrum and its four parameter derivatives are
-// built here in FP64 for every call: the response R = H(z) S(f) on the
-// 8192-point block grid goes to the time domain, is truncated to the same
-// +/-b_pos support the decoder's K1b uses and comes back, so the forward
-// filter and its derivatives are the same linear map of the response.
+// built here in FP64 for every call, directly on the 8192-point block grid:
+// the response R = H(z) S(f) there is the spectrum of the filter's time
+// kernel wrapped to 8192 samples, whose taps beyond the +/-b_pos support of
+// the overlap-save blocks (the support the decoder's K1b uses) are below
+// ~5e-9 of the peak, so the blocks see the filter itself.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -19,7 +20,6 @@
 
 #include "../../include/cuvhs.h"
 #include "adjoint.h"
-#include "host_fft.h"
 #include "pipeline.h"
 
 namespace cuvhs {
@@ -105,21 +105,13 @@ struct cuvhs_adjoint {
       dR[2][k] = (1.0 / den - H * z1 / den) * S;  // n0 moves with m1
       dR[3][k] = (1.0 / den - H * z2 / den) * S;
     }
-    const int bp = c().des.b_pos;
-    auto to_block = [&](const std::vector<cd>& resp, float2* out) {
-      std::vector<cd> h = cuvhs::host_dft(resp, +1);  // time kernel x N
-      std::vector<cd> blk(kN, cd(0.0, 0.0));
-      for (int m = -bp; m <= bp; m++) {
-        const int i = (m % kN + kN) % kN;
-        blk[i] = cd(h[i].real() / kN, 0.0);  // real kernel
-      }
-      std::vector<cd> G = cuvhs::host_dft(blk, -1);
-      for (int k = 0; k < kN; k++) out[k] = make_float2((float)(G[k].real() / kN), (float)(G[k].imag() / kN));
-    };
     h_gv.resize(kN);
     h_dg.resize((size_t)4 * kN);
-    to_block(R, h_gv.data());
-    for (int j = 0; j < 4; j++) to_block(dR[j], h_dg.data() + (size_t)j * kN);
+    for (int k = 0; k < kN; k++) {
+      h_gv[k] = make_float2((float)(R[k].real() / kN), (float)(R[k].imag() / kN));
+      for (int j = 0; j < 4; j++)
+        h_dg[(size_t)j * kN + k] = make_float2((float)(dR[j][k].real() / kN), (float)(dR[j][k].imag() / kN));
+    }
   }
 
   void upload_params(const cuvhs_adjoint_params* p, bool derivs) {

@@ -1,8 +1,8 @@
 """FP64 restatement of the calibration decode model (test infrastructure).
 
 The checker for the library's adjoint kernels (cuvhs_adjoint_*): the same
-model -- de-emphasis and video low-pass on the block grid truncated to the
-decoder's support, Catmull-Rom luma, heterodyned and band-passed chroma with
+model -- de-emphasis and video low-pass (here as a linear convolution with the
+filter's taps within the decoder's +/-b_pos support), Catmull-Rom luma, heterodyned and band-passed chroma with
 the burst-driven ACC gain, mean squared error over lines 10..261, columns
 80..893 -- evaluated in FP64 with numpy on the fixed inputs the GPU model
 holds (demod, pre-band-pass, line locations, tracks), so that FP64 central

@@ -39,6 +39,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "NTSC fields/s at 28 MHz u8 and % of HBM roofline vs reference, at ≤1 LSB luma"
 WORKLOAD = "plain40_28"
+HARD_DESC = ("harder signal: 600 NTSC fields of seeded synthetic VHS SP RF at 40 MHz u8 (32 dB SNR, "
+             "+/-2 sample jitter, dropouts of 5-200 samples on 0.1% of lines, head switch of 3-8 samples)")
 WORKLOAD_DESC = ("plain decode: 40 NTSC fields of seeded synthetic VHS SP RF at 28 MHz u8 "
                  "(colour bars + moving luma ramp, 40 dB SNR, +/-0.5 sample jitter, no dropouts)")
 
@@ -453,14 +455,18 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="one device-resident decode of the workload with a 48-field allocation, "
                          "for kernel profilers; prints nothing else")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, "batched64", "stream40", "adjoint8"],
-                    help="batched64: the 64-capture mixed batch through cuvhs_batch_decode; "
+    ap.add_argument("--workload", default="plain40_28",
+                    choices=["plain40_28", "hard600_40", "batched64", "stream40", "adjoint8"],
+                    help="hard600_40: the 600-field 40 MHz capture through the same measurement; "
+                         "batched64: the 64-capture mixed batch through cuvhs_batch_decode; "
                          "stream40: one long 40 MHz capture streamed from pinned memory; "
                          "adjoint8: forward+backward passes of the calibration model")
     ap.add_argument("--stream-fields", type=int, default=6000, help="stream40: fields in the capture")
     ap.add_argument("--lanes", type=int, default=0, help="batched64: concurrent decoders (0 = library default)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload == "hard600_40":
+        globals().update(WORKLOAD="hard600_40", WORKLOAD_DESC=HARD_DESC)
     if args.profile_case:
         return profile_case()
 

@@ -158,12 +158,17 @@ __global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(DemodArgs a, int f_be
     }
   }
   pair_spectra<N, true>(v, sA, sB, a.ga, a.tw_a, t);
-  RegFFT<N>::run<true>(v, sB, a.tw_a_inv, t);
-  k1a_emit<T>(a, v, f, j0, blk0, warp_last, red, t);
-  if (blk0 + 1 >= a.env_blocks) return;  // whole CTA
-  load_second<N, true>(v, sA, t);
-  RegFFT<N>::run<true>(v, sA, a.tw_a_inv, t);
-  k1a_emit<T>(a, v, f, j0 + a.a_out, blk0 + 1, warp_last, red, t);
+  // one copy of the inverse transform and output stage serves both blocks
+  // (a rolled loop keeps the kernel body small for the instruction cache)
+#pragma unroll 1
+  for (int b = 0; b < 2; b++) {
+    if (b == 1) {
+      if (blk0 + 1 >= a.env_blocks) return;  // whole CTA
+      load_second<N, true>(v, sA, t);
+    }
+    RegFFT<N>::run<true>(v, b == 0 ? sB : sA, a.tw_a_inv, t);
+    k1a_emit<T>(a, v, f, j0 + b * a.a_out, blk0 + b, warp_last, red, t);
+  }
 }
 
 // K1b output stage: video (real part) and sync (imaginary part) of one block.

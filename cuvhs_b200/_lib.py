@@ -40,7 +40,8 @@ class CuvhsError(RuntimeError):
 
 class Config(ctypes.Structure):
     _fields_ = [("system", ctypes.c_int), ("sample_rate_mhz", ctypes.c_double), ("device", ctypes.c_int),
-                ("batch_fields", ctypes.c_int), ("stream_mode", ctypes.c_int)]
+                ("batch_fields", ctypes.c_int), ("stream_mode", ctypes.c_int), ("input_format", ctypes.c_int),
+                ("dc_correct", ctypes.c_int)]
 
 
 class FieldInfo(ctypes.Structure):
@@ -294,13 +295,18 @@ def collect_result(out, bufs, json_text):
 class Decoder:
     """One libcuvhs context (device memory and stream, carried decode state)."""
 
-    def __init__(self, sample_rate_mhz=28.0, device=0, batch_fields=0, stream_mode=False, debug=False):
+    FORMATS = {"u8": (0, np.uint8), "s16": (1, np.int16), "u16": (2, np.uint16)}
+
+    def __init__(self, sample_rate_mhz=28.0, device=0, batch_fields=0, stream_mode=False, debug=False,
+                 input_format="u8", dc_correct=False):
         cfg = Config()
         lib.cuvhs_default_config(ctypes.byref(cfg))
         cfg.sample_rate_mhz = float(sample_rate_mhz)
         cfg.device = int(device)
         cfg.batch_fields = int(batch_fields)
         cfg.stream_mode = 1 if stream_mode else 0
+        cfg.input_format, self._dtype = self.FORMATS[input_format]
+        cfg.dc_correct = 1 if dc_correct else 0
         h = _vp()
         st = lib.cuvhs_create(ctypes.byref(cfg), ctypes.byref(h))
         if st != 0:
@@ -357,7 +363,7 @@ class Decoder:
         """Decode a whole capture.  pinned=True stages the input and the output
         planes in page-locked memory, which lets the library overlap the
         host<->device copies with the decode."""
-        samples = np.ascontiguousarray(samples, dtype=np.uint8)
+        samples = np.ascontiguousarray(samples, dtype=self._dtype)
         max_fields = max_fields_for(samples.size, self.samples_per_field)
         out, bufs = self._alloc_output(max_fields, pinned)
         if pinned:
@@ -372,7 +378,7 @@ class Decoder:
 
     def decode_chunk(self, samples: np.ndarray, raw_offset: int, num_fields: int):
         """One reference-style chunk; `samples` starts at capture sample raw_offset."""
-        samples = np.ascontiguousarray(samples, dtype=np.uint8)
+        samples = np.ascontiguousarray(samples, dtype=self._dtype)
         out, bufs = self._alloc_output(num_fields)
         self._check(lib.cuvhs_decode_chunk(self._h, samples.ctypes.data, samples.size, raw_offset, num_fields,
                                            ctypes.byref(out)))
@@ -498,12 +504,15 @@ class Batch:
         return self.results(items, keep)
 
 
-def decode_file(in_path, out_base, sample_rate_mhz=28.0, device=0, overwrite=True, batch_fields=0):
+def decode_file(in_path, out_base, sample_rate_mhz=28.0, device=0, overwrite=True, batch_fields=0,
+                input_format="u8", dc_correct=False):
     cfg = Config()
     lib.cuvhs_default_config(ctypes.byref(cfg))
     cfg.sample_rate_mhz = float(sample_rate_mhz)
     cfg.device = int(device)
     cfg.batch_fields = int(batch_fields)
+    cfg.input_format = Decoder.FORMATS[input_format][0]
+    cfg.dc_correct = 1 if dc_correct else 0
     st = lib.cuvhs_decode_file(ctypes.byref(cfg), str(in_path).encode(), str(out_base).encode(), 1 if overwrite else 0)
     if st != 0:
         raise CuvhsError(st, "cuvhs_decode_file failed")

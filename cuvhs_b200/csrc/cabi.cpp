@@ -142,6 +142,8 @@ void cuvhs_default_config(cuvhs_config* cfg) {
   cfg->device = 0;
   cfg->batch_fields = 0;
   cfg->stream_mode = 0;
+  cfg->input_format = 0;
+  cfg->dc_correct = 0;
 }
 
 const char* cuvhs_status_string(cuvhs_status s) {
@@ -217,7 +219,7 @@ cuvhs_status cuvhs_decode_capture(cuvhs_ctx* ctx, const uint8_t* samples, size_t
     const int nf = std::min(c.batch, remaining_fields);
     const size_t before = out->fields_out;
     const uint64_t prev_next = out->next_raw_offset;
-    cuvhs_status s = decode_into(c, samples + raw_offset, n - raw_offset, raw_offset, nf, out, samples, n);
+    cuvhs_status s = decode_into(c, samples + raw_offset * c.bps, n - raw_offset, raw_offset, nf, out, samples, n);
     if (s != CUVHS_OK) {
       c.drain_copies();
       return s;
@@ -338,7 +340,7 @@ cuvhs_status cuvhs_decode_file(const cuvhs_config* cfg, const char* in_path, con
       return CUVHS_ERR_IO;
     }
     if (S_ISFIFO(st.st_mode) || S_ISCHR(st.st_mode)) streaming = true;
-    else file_size = (size_t)st.st_size;
+    else file_size = (size_t)st.st_size / (cfg->input_format == 0 ? 1 : 2);  // samples
   }
   cuvhs_config c2 = *cfg;
   if (streaming) c2.stream_mode = 1;
@@ -360,17 +362,19 @@ cuvhs_status cuvhs_decode_file(const cuvhs_config* cfg, const char* in_path, con
   }
   const size_t spf = (size_t)c.fmt.samples_per_field, spp = (size_t)c.spp;
   const size_t F = (size_t)c.fmt.output_line_len * c.fmt.output_field_lines;
+  const size_t bps = (size_t)c.bps;  // bytes per sample; offsets and counts below are in samples
   std::vector<uint16_t> luma((size_t)c.batch * F), chroma((size_t)c.batch * F);
   std::vector<int32_t> dl, ds, de;
   std::vector<cuvhs_field_info> all;
   std::vector<int32_t> all_dl, all_ds, all_de;
   std::vector<uint8_t> buf;
-  // stream mode keeps bytes from buf_origin on, reading forward as needed
+  // stream mode keeps the samples from buf_origin on, reading forward as needed
   uint64_t buf_origin = 0;
   bool eof = false;
+  auto buffered = [&]() { return (uint64_t)(buf.size() / bps); };
   auto fill_stream = [&](uint64_t upto) {
-    while (!eof && buf_origin + buf.size() < upto) {
-      const size_t want = (size_t)(upto - (buf_origin + buf.size()));
+    while (!eof && buf_origin + buffered() < upto) {
+      const size_t want = (size_t)(upto - (buf_origin + buffered())) * bps;
       const size_t old = buf.size();
       buf.resize(old + want);
       size_t got = 0;
@@ -414,26 +418,26 @@ cuvhs_status cuvhs_decode_file(const cuvhs_config* cfg, const char* in_path, con
     size_t n_avail = 0;
     const uint8_t* src = nullptr;
     if (!streaming) {
-      const size_t n = std::min(want, file_size - (size_t)raw_offset);
+      const size_t n = std::min(want, file_size - (size_t)raw_offset) * bps;
       buf.resize(n);
       size_t got = 0;
       while (got < n) {
-        ssize_t r = pread(fd, buf.data() + got, n - got, (off_t)(raw_offset + got));
+        ssize_t r = pread(fd, buf.data() + got, n - got, (off_t)(raw_offset * bps + got));
         if (r > 0) got += (size_t)r;
         else if (r < 0 && errno == EINTR) continue;
         else break;
       }
-      n_avail = got;
+      n_avail = got / bps;
       src = buf.data();
     } else {
       if (raw_offset > buf_origin) {
-        const size_t drop = std::min((size_t)(raw_offset - buf_origin), buf.size());
-        buf.erase(buf.begin(), buf.begin() + drop);
+        const size_t drop = std::min((size_t)(raw_offset - buf_origin), (size_t)buffered());
+        buf.erase(buf.begin(), buf.begin() + drop * bps);
         buf_origin += drop;
       }
       fill_stream(raw_offset + want);
-      n_avail = buf_origin + buf.size() > raw_offset ? (size_t)(buf_origin + buf.size() - raw_offset) : 0;
-      src = buf.data() + (raw_offset - buf_origin);
+      n_avail = buf_origin + buffered() > raw_offset ? (size_t)(buf_origin + buffered() - raw_offset) : 0;
+      src = buf.data() + (raw_offset - buf_origin) * bps;
     }
     if (n_avail < spf) break;
     cuvhs_output out;

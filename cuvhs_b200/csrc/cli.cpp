@@ -21,7 +21,7 @@ void usage(const char* prog) {
           "Usage: %s [options] <input_file> <output_base>\n"
           "\n"
           "Arguments:\n"
-          "  input_file       Raw RF capture (.u8, .raw), or - for stdin\n"
+          "  input_file       Raw RF capture (.u8, .s16, .u16, .raw), or - for stdin\n"
           "  output_base      Output prefix (creates .tbc, _chroma.tbc, .tbc.json)\n"
           "\n"
           "Options:\n"
@@ -95,10 +95,12 @@ int main(int argc, char** argv) {
     const std::string ext = dot == std::string::npos ? in : in.substr(dot + 1);
     format = (ext == "s16") ? "s16" : (ext == "u16") ? "u16" : "u8";
   }
-  if (pal || format != "u8" || dc_correct) {
-    fprintf(stderr, "This build decodes NTSC u8 captures without DC correction only\n");
+  if (pal) {
+    fprintf(stderr, "This build decodes NTSC captures only\n");
     return 1;
   }
+  cfg.input_format = format == "s16" ? 1 : (format == "u16" ? 2 : 0);
+  cfg.dc_correct = dc_correct ? 1 : 0;
   cuvhs_status s = cuvhs_decode_file(&cfg, in.c_str(), out.c_str(), overwrite ? 1 : 0);
   if (s != CUVHS_OK) {
     fprintf(stderr, "Pipeline failed: %s\n", cuvhs_status_string(s));

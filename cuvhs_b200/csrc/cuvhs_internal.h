@@ -91,7 +91,10 @@ struct Design {
 
 // ---------------------------------------------------------------- kernels
 struct DemodArgs {
-  const uint8_t* raw;  // chunk samples, values past the read are 128
+  const uint8_t* raw;  // chunk samples in the input format (raw_input.cuh)
+  int in_fmt;          // InputFormat
+  int n_read;          // samples read; chunk positions past them are 0
+  const float* dc;     // device scalar subtracted from every sample read, or null
   long long total;     // T * spp (clamp bound of the tile gathers)
   int tiles, spp, tile;
   const float2* ga;
@@ -115,6 +118,10 @@ struct DemodArgs {
 };
 // K1a over tiles [f0, f0 + nf).
 void launch_k1a(const DemodArgs& a, int f0, int nf, cudaStream_t st);
+// DC correction: *dc = mean of the n converted samples of raw (exact integer
+// sum, one FP64 division, as the reference's FP64 loop), as FP32.
+// sum is scratch for one unsigned long long.
+void launch_dc_mean(const uint8_t* raw, int n, int in_fmt, unsigned long long* sum, float* dc, cudaStream_t st);
 void launch_k1b(const DemodArgs& a, cudaStream_t st);
 
 // Threshold edges of the sync signal in sample order: falling (x<=thr after
@@ -143,7 +150,9 @@ void launch_hsync_refine(const LineArgs& a, cudaStream_t st);
 void launch_luma(const LineArgs& a, cudaStream_t st);
 
 struct ChromaArgs {
-  const uint8_t* raw;
+  const uint8_t* raw;  // as DemodArgs
+  int in_fmt, n_read;
+  const float* dc;
   float* pre;  // [P*spp]
   int fields, spp, ctile, c_half, c_out;
   const float* gc;

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "cuvhs_internal.h"
+#include "raw_input.cuh"
 #include "reg_fft.cuh"
 
 namespace cuvhs {
@@ -24,13 +25,15 @@ constexpr int kLineWarps = 4;
 
 // Two adjacent output blocks ride in the real and imaginary parts of one
 // transform (the kernel is real).  Thread t holds block samples t + T*q.
+template <int FMT>
 __global__ void __launch_bounds__(kThreadsC, 1) prefilter_kernel(ChromaArgs a) {
   constexpr int N = Design::kNc, T = kThreadsC;
   extern __shared__ float2 sm[];
   const int t = threadIdx.x;
   const int f = blockIdx.y;
   const int i0 = blockIdx.x * 2 * a.c_out;  // first output of the real half
-  const uint8_t* tile = a.raw + (size_t)f * a.spp;
+  const int tile = f * a.spp;               // chunk position of the tile
+  const float dc = a.dc ? *a.dc : 0.0f;
   float2 v[16];
 #pragma unroll
   for (int q = 0; q < 16; q++) {
@@ -38,8 +41,8 @@ __global__ void __launch_bounds__(kThreadsC, 1) prefilter_kernel(ChromaArgs a) {
     if (q0 < 0) q0 += a.ctile;
     int q1 = q0 + a.c_out;
     if (q1 >= a.ctile) q1 -= a.ctile;
-    const float v0 = q0 < a.spp ? ((float)__ldg(&tile[q0]) - 128.0f) * 256.0f : 0.0f;
-    const float v1 = q1 < a.spp ? ((float)__ldg(&tile[q1]) - 128.0f) * 256.0f : 0.0f;
+    const float v0 = q0 < a.spp ? raw_sample<FMT>(a.raw, tile + q0, a.n_read, dc) : 0.0f;
+    const float v1 = q1 < a.spp ? raw_sample<FMT>(a.raw, tile + q1, a.n_read, dc) : 0.0f;
     v[q] = make_float2(v0, v1);
   }
   RegFFT<N>::run<false>(v, sm, a.tw_c, t);
@@ -169,9 +172,14 @@ __global__ void metric_kernel(ChromaArgs a, int field0, int nfields) {
 
 void launch_chroma_prefilter(const ChromaArgs& a, cudaStream_t st) {
   const size_t smem = sizeof(float2) * fft_pad(Design::kNc);
-  cudaFuncSetAttribute(prefilter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 grid((a.spp + 2 * a.c_out - 1) / (2 * a.c_out), a.fields);
-  prefilter_kernel<<<grid, kThreadsC, smem, st>>>(a);
+  auto go = [&](auto kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kernel<<<grid, kThreadsC, smem, st>>>(a);
+  };
+  if (a.in_fmt == kInS16) go(prefilter_kernel<kInS16>);
+  else if (a.in_fmt == kInU16) go(prefilter_kernel<kInU16>);
+  else go(prefilter_kernel<kInU8>);
 }
 
 void launch_chroma_lines(const ChromaArgs& a, int field0, int nfields, bool write_output, cudaStream_t st) {

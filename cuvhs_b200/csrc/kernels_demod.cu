@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include "cuvhs_internal.h"
+#include "raw_input.cuh"
 #include "reg_fft.cuh"
 
 namespace cuvhs {
@@ -123,6 +124,7 @@ __device__ __forceinline__ void k1a_emit(const DemodArgs& a, const float2 (&z)[1
 
 // K1a: u8 -> analytic signal -> phase step + envelope, blocks 2x and 2x+1 of
 // the tile (the second may lie past the tile's end).
+template <int FMT>
 __global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(DemodArgs a, int f_begin) {
   constexpr int N = Design::kNa, T = kThreadsA;
   extern __shared__ float2 sm[];
@@ -142,19 +144,20 @@ __global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(DemodArgs a, int f_be
   // Interior windows (no wrap inside the tile, no clamp at the chunk ends)
   // take the direct addresses; the CTA-uniform test keeps the loop branch-free.
   const int span = a.a_out + N;  // tile positions [base, base + span) are read
-  if (base >= 0 && base + span <= a.tile && tile0 + base >= 0 && tile0 + base + span - 1 <= last) {
-    const uint8_t* src = a.raw + (tile0 + base + t);
+  const float dc = a.dc ? *a.dc : 0.0f;
+  if (base >= 0 && base + span <= a.tile && tile0 + base >= 0 && tile0 + base + span - 1 <= last &&
+      tile0 + base + span <= a.n_read) {
+    const int p = tile0 + base + t;
 #pragma unroll
     for (int q = 0; q < 16; q++)
-      v[q] = make_float2(((float)__ldg(&src[T * q]) - 128.0f) * 256.0f,
-                         ((float)__ldg(&src[T * q + a.a_out]) - 128.0f) * 256.0f);
+      v[q] = make_float2(raw_convert<FMT>(a.raw, p + T * q) - dc, raw_convert<FMT>(a.raw, p + T * q + a.a_out) - dc);
   } else {
 #pragma unroll
     for (int q = 0; q < 16; q++) {
       const int q0 = base + t + T * q;
       const int p0 = min(max(tile0 + wrap_tile(q0, a.tile), 0), last);
       const int p1 = min(max(tile0 + wrap_tile(q0 + a.a_out, a.tile), 0), last);
-      v[q] = make_float2(((float)__ldg(&a.raw[p0]) - 128.0f) * 256.0f, ((float)__ldg(&a.raw[p1]) - 128.0f) * 256.0f);
+      v[q] = make_float2(raw_sample<FMT>(a.raw, p0, a.n_read, dc), raw_sample<FMT>(a.raw, p1, a.n_read, dc));
     }
   }
   pair_spectra<N, true>(v, sA, sB, a.ga, a.tw_a, t);
@@ -355,10 +358,52 @@ __global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(const float* _
 void launch_k1a(const DemodArgs& a, int f0, int nf, cudaStream_t st) {
   if (nf <= 0) return;
   const size_t smem = 2 * sizeof(float2) * fft_pad(Design::kNa);
-  cudaFuncSetAttribute(k1a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int blocks = (a.spp + a.a_out - 1) / a.a_out;  // = env_blocks
   dim3 grid((blocks + 1) / 2, nf);
-  k1a_kernel<<<grid, kThreadsA, smem, st>>>(a, f0);
+  auto go = [&](auto kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kernel<<<grid, kThreadsA, smem, st>>>(a, f0);
+  };
+  if (a.in_fmt == kInS16) go(k1a_kernel<kInS16>);
+  else if (a.in_fmt == kInU16) go(k1a_kernel<kInU16>);
+  else go(k1a_kernel<kInU8>);
+}
+
+namespace {
+
+// Sum of the converted samples as a 64-bit integer (every converted value is
+// an integer, so the sum is exact and order-free).
+template <int FMT>
+__global__ void dc_sum_kernel(const uint8_t* raw, int n, unsigned long long* sum) {
+  __shared__ long long part[8];
+  long long acc = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    acc += (long long)raw_convert<FMT>(raw, i);
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += part[w];
+    atomicAdd(sum, (unsigned long long)s);
+  }
+}
+
+__global__ void dc_mean_kernel(const unsigned long long* sum, int n, float* dc) {
+  *dc = (float)((double)(long long)*sum / (double)n);
+}
+
+}  // namespace
+
+void launch_dc_mean(const uint8_t* raw, int n, int in_fmt, unsigned long long* sum, float* dc, cudaStream_t st) {
+  cudaMemsetAsync(sum, 0, sizeof(unsigned long long), st);
+  const int threads = 256, blocks = 148 * 8;
+  if (n > 0) {
+    if (in_fmt == kInS16) dc_sum_kernel<kInS16><<<blocks, threads, 0, st>>>(raw, n, sum);
+    else if (in_fmt == kInU16) dc_sum_kernel<kInU16><<<blocks, threads, 0, st>>>(raw, n, sum);
+    else dc_sum_kernel<kInU8><<<blocks, threads, 0, st>>>(raw, n, sum);
+  }
+  dc_mean_kernel<<<1, 1, 0, st>>>(sum, n > 0 ? n : 1, dc);
 }
 
 void launch_k1b(const DemodArgs& a, cudaStream_t st) {

@@ -177,12 +177,20 @@ bool Context::init(const cuvhs_config& c) {
     return false;
   }
   cudaSetDevice(device);
+  if (c.input_format < 0 || c.input_format > 2) {
+    err = "input_format must be 0 (u8), 1 (s16) or 2 (u16)";
+    status = CUVHS_ERR_INVALID_ARGUMENT;
+    return false;
+  }
+  in_fmt = c.input_format;
+  bps = in_fmt == 0 ? 1 : 2;
+  dc_correct = c.dc_correct != 0;
   fmt.init(c.sample_rate_mhz);
   des.build_cached(fmt);
   spp = fmt.spp;
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
-  const size_t per_field = (size_t)spp * (2 + 4 * 5) + (size_t)263 * 910 * 8 + 263 * kBurstLen * 4 + 65536 +
+  const size_t per_field = (size_t)spp * (2 * bps + 4 * 5) + (size_t)263 * 910 * 8 + 263 * kBurstLen * 4 + 65536 +
                            dropout_class_bytes_per_field();
   int b = c.batch_fields;
   if (b <= 0) {
@@ -215,8 +223,10 @@ bool Context::init(const cuvhs_config& c) {
     return p;
   };
   env_blocks = (spp + des.a_out - 1) / des.a_out;
-  d_raw_set[0] = A((uint8_t*)nullptr, S + 64);
-  d_raw_set[1] = A((uint8_t*)nullptr, S + 64);
+  d_raw_set[0] = A((uint8_t*)nullptr, S * bps + 64);
+  d_raw_set[1] = A((uint8_t*)nullptr, S * bps + 64);
+  d_dc = A((float*)nullptr, 1);
+  d_dcsum = A((unsigned long long*)nullptr, 1);
   d_raw = d_raw_set[0];
   d_dem = A((float*)nullptr, S);
   d_env = A((float*)nullptr, S);
@@ -439,6 +449,9 @@ static double host_burst_phase(const float* b, int H, const Format& fmt) {
 DemodArgs Context::demod_args(int T) const {
   DemodArgs da;
   da.raw = d_raw;
+  da.in_fmt = in_fmt;
+  da.n_read = cur_n_read;
+  da.dc = dc_correct ? d_dc : nullptr;
   da.total = (long long)T * spp;
   da.tiles = T;
   da.spp = spp;
@@ -510,50 +523,49 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   pf.valid = false;
   d_raw = d_raw_set[rset];
   raw_set = rset;
+  cur_n_read = (int)n_read;
   // ---- K1: FM demod over T tiles
   DemodArgs da = demod_args(T);
-  // ---- input: the chunk window, the rest set to the u8 mid level (0.0 after
-  // conversion).  Host input arrives in pieces on the copy stream; K1a of
-  // tiles [fa, fb) reads chunk samples up to (fb-1)*spp - kOverlap + tile, so
-  // it starts as soon as the piece reaching that far has landed.
+  // ---- input: the chunk window (bps bytes per sample); positions past the
+  // samples read count as 0 in every kernel, the reference's zero fill.  Host
+  // input arrives in pieces on the copy stream; K1a of tiles [fa, fb) reads
+  // chunk samples up to (fb-1)*spp - kOverlap + tile, so it starts as soon as
+  // the piece reaching that far has landed.  With DC correction the chunk
+  // mean is needed first, so K1a waits for the whole window.
   {
     cudaEvent_t ev_;
     begin_stage(kStageK1a, ev_);
+    int kernels = 1;
     if (src_on_device) {
-      // a full window is read in place; a short one is padded in d_raw
-      if (n_read < total_samples) {
-        cudaMemcpyAsync(d_raw, src, n_read, cudaMemcpyDeviceToDevice, stream);
-        cudaMemsetAsync(d_raw + n_read, 128, total_samples - n_read, stream);
-      } else {
-        da.raw = src;
-      }
+      // a full window is read in place; a short one is copied
+      if (n_read < total_samples) cudaMemcpyAsync(d_raw, src, n_read * bps, cudaMemcpyDeviceToDevice, stream);
+      else da.raw = src;
+      if (dc_correct) launch_dc_mean(da.raw, (int)n_read, in_fmt, d_dcsum, d_dc, stream);
       launch_k1a(da, 0, T, stream);
-      end_stage(kStageK1a, ev_);
     } else if (prefetched) {
       cudaStreamWaitEvent(stream, ev_prefetch, 0);
+      if (dc_correct) launch_dc_mean(da.raw, (int)n_read, in_fmt, d_dcsum, d_dc, stream);
       launch_k1a(da, 0, T, stream);
-      end_stage(kStageK1a, ev_);
     } else {
-      const int pieces = std::min(kInputPieces, T);
+      const int pieces = dc_correct ? 1 : std::min(kInputPieces, T);
       size_t have = 0;
       for (int i = 0; i < pieces; i++) {
         const int fa = (int)((long long)T * i / pieces), fb = (int)((long long)T * (i + 1) / pieces);
         size_t need = (size_t)(fb - 1) * spp + (size_t)des.tile - kOverlap;
-        if (i == pieces - 1 || need > total_samples) need = total_samples;
+        if (i == pieces - 1 || need > n_read) need = n_read;
         if (need > have) {
-          const size_t c_end = std::min(need, n_read);
-          if (c_end > have)
-            cudaMemcpyAsync(d_raw + have, src + have, c_end - have, cudaMemcpyHostToDevice, hstream);
-          const size_t m_beg = std::max(have, n_read);
-          if (need > m_beg) cudaMemsetAsync(d_raw + m_beg, 128, need - m_beg, hstream);
+          cudaMemcpyAsync(d_raw + have * bps, src + have * bps, (need - have) * bps, cudaMemcpyHostToDevice,
+                          hstream);
           have = need;
         }
         cudaEventRecord(ev_piece[i], hstream);
         cudaStreamWaitEvent(stream, ev_piece[i], 0);
+        if (dc_correct) launch_dc_mean(da.raw, (int)n_read, in_fmt, d_dcsum, d_dc, stream);
         launch_k1a(da, fa, fb - fa, stream);
       }
-      end_stage(kStageK1a, ev_, pieces);
+      kernels = pieces;
     }
+    end_stage(kStageK1a, ev_, kernels + (dc_correct ? 2 : 0));
   }
   {
     cudaEvent_t ev_;
@@ -590,6 +602,9 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   const int H = fmt.output_field_lines;
   ChromaArgs ca;
   ca.raw = da.raw;
+  ca.in_fmt = in_fmt;
+  ca.n_read = (int)n_read;
+  ca.dc = da.dc;
   ca.pre = d_dem;  // the raw demod is no longer needed after K1b
   ca.fields = T;
   ca.spp = spp;
@@ -698,8 +713,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
       const size_t tot = (size_t)nf * spp, nr = std::min(tot, (size_t)(cap_n - nxt));
       if (nr >= spf) {
         const int ps = 1 - rset;
-        cudaMemcpyAsync(d_raw_set[ps], cap_base + nxt, nr, cudaMemcpyHostToDevice, hstream);
-        if (nr < tot) cudaMemsetAsync(d_raw_set[ps] + nr, 128, tot - nr, hstream);
+        cudaMemcpyAsync(d_raw_set[ps], cap_base + nxt * bps, nr * bps, cudaMemcpyHostToDevice, hstream);
         cudaEventRecord(ev_prefetch, hstream);
         pf.valid = true;
         pf.raw_offset = nxt;

@@ -52,6 +52,12 @@ struct Context {
   int env_blocks = 0;
   int edge_cap = 0;
   int pool_threads = -1;  // host line-location helpers; -1 = min(cores - 1, 15)
+  int in_fmt = 0;         // InputFormat of the capture samples
+  int bps = 1;            // bytes per capture sample
+  bool dc_correct = false;
+  int cur_n_read = 0;     // samples read into the current chunk window
+  float* d_dc = nullptr;  // chunk DC mean (DC correction)
+  unsigned long long* d_dcsum = nullptr;
   cudaStream_t stream = nullptr;
   // Copy stream: host input arrives in pieces (K1a starts on each piece as it
   // lands) and the finished luma leaves while chroma is still being decoded.

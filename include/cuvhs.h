@@ -59,6 +59,8 @@ typedef struct cuvhs_config {
   int device;             /* --gpu: CUDA device id, -1 = the one with most memory */
   int batch_fields;       /* fields per chunk; 0 = derive from free device memory */
   int stream_mode;        /* non-zero caps the chunk at 64 fields (pipe input) */
+  int input_format;       /* --format: 0 = u8, 1 = s16, 2 = u16 (src/io/raw_reader.cpp:71-91) */
+  int dc_correct;         /* --dc-correct: subtract each chunk's mean sample (raw_reader.cpp:93-99) */
 } cuvhs_config;
 
 /* Per-field metadata, one .tbc.json "fields" entry. */
@@ -114,7 +116,9 @@ cuvhs_status cuvhs_decode_chunk_device(cuvhs_ctx* ctx, const uint8_t* d_samples,
 /* Device pointers to the last chunk's luma and chroma fields. */
 cuvhs_status cuvhs_device_outputs(const cuvhs_ctx* ctx, const uint16_t** d_luma, const uint16_t** d_chroma);
 
-/* A whole capture in host memory, chunk by chunk as the reference's run loop. */
+/* A whole capture in host memory, chunk by chunk as the reference's run loop.
+ * For every decode call, `samples` holds samples of the configured input
+ * format (1 byte each for u8, 2 for s16/u16) and sizes count samples. */
 cuvhs_status cuvhs_decode_capture(cuvhs_ctx* ctx, const uint8_t* samples, size_t n, cuvhs_output* out);
 
 /* .tbc.json text for `out`'s fields; returns the length (excluding NUL) and

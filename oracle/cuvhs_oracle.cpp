@@ -235,6 +235,8 @@ struct oracle_ctx {
   int batch;
   int threads;
   bool keep_signals = false;
+  int in_fmt = 0;         // 0 u8, 1 s16, 2 u16
+  bool dc_correct = false;
   oracle::DemodFilters filt;
   int spp;
   // carried state (pipeline.h:92-97, chroma_decode.h:9-15, pipeline.cu:2575)
@@ -1219,8 +1221,22 @@ int process_chunk(oracle_ctx* c, const uint8_t* data, size_t n, size_t raw_offse
   const size_t total_samples = (size_t)num_fields * spp;
   size_t n_read = raw_offset < n ? std::min(total_samples, n - raw_offset) : 0;
   if (n_read < spf) return 0;
+  // RawReader::convert (src/io/raw_reader.cpp:71-99): per-format conversion,
+  // then the mean of the samples read subtracted; the zero fill past them is
+  // applied after (pipeline.cu:1539-1541)
   std::vector<double> raw(total_samples, 0.0);
-  for (size_t i = 0; i < n_read; i++) raw[i] = ((double)data[raw_offset + i] - 128.0) * 256.0;
+  for (size_t i = 0; i < n_read; i++) {
+    const size_t k = raw_offset + i;
+    if (c->in_fmt == 1) raw[i] = (double)reinterpret_cast<const int16_t*>(data)[k];
+    else if (c->in_fmt == 2) raw[i] = (double)reinterpret_cast<const uint16_t*>(data)[k] - 32768.0;
+    else raw[i] = ((double)data[k] - 128.0) * 256.0;
+  }
+  if (c->dc_correct && n_read > 0) {
+    double sum = 0.0;
+    for (size_t i = 0; i < n_read; i++) sum += raw[i];
+    const double mean = sum / (double)n_read;
+    for (size_t i = 0; i < n_read; i++) raw[i] -= mean;
+  }
   int T = (int)(n_read / spf);
   if (T > num_fields) T = num_fields;
   if (T == 0) return 0;
@@ -1359,6 +1375,10 @@ oracle_ctx* oracle_create(double mhz, int batch_fields, int threads) {
 
 void oracle_destroy(oracle_ctx* c) { delete c; }
 void oracle_keep_signals(oracle_ctx* c, int keep) { c->keep_signals = keep != 0; }
+void oracle_set_input(oracle_ctx* c, int format, int dc_correct) {
+  c->in_fmt = format;
+  c->dc_correct = dc_correct != 0;
+}
 
 int oracle_decode(oracle_ctx* c, const uint8_t* data, size_t n) {
   c->luma.clear();

@@ -51,6 +51,10 @@ long long oracle_chunk_array(const oracle_ctx* c, int k, const char* name, void*
 /* Keep the per-chunk FP64 sample arrays (demod, demod05, envelope,
  * chroma_prefilt) of chunk 0 for inspection (memory heavy). */
 void oracle_keep_signals(oracle_ctx* c, int keep);
+/* Capture sample format (0 u8, 1 s16, 2 u16; oracle_decode's data then holds
+ * 1 or 2 bytes per sample and n counts samples) and DC correction, as the
+ * reference's --format and --dc-correct. */
+void oracle_set_input(oracle_ctx* c, int format, int dc_correct);
 
 #ifdef __cplusplus
 }

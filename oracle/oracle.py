@@ -49,6 +49,7 @@ def _load():
         L.oracle_chunk_array.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p,
                                          ctypes.c_longlong]
         L.oracle_keep_signals.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_set_input.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.oracle_destroy.argtypes = [ctypes.c_void_p]
         _lib = L
     return _lib
@@ -58,11 +59,16 @@ class Oracle:
     """One oracle decoder.  batch_fields is the reference's chunk size (its
     VRAM-derived batch; 3282 on a 180 GB B200 at 28 MHz)."""
 
-    def __init__(self, sample_rate_mhz=28.0, batch_fields=3282, threads=0, keep_signals=False):
+    FORMATS = {"u8": (0, np.uint8), "s16": (1, np.int16), "u16": (2, np.uint16)}
+
+    def __init__(self, sample_rate_mhz=28.0, batch_fields=3282, threads=0, keep_signals=False, input_format="u8",
+                 dc_correct=False):
         L = _load()
         self._h = L.oracle_create(float(sample_rate_mhz), int(batch_fields), int(threads))
         if keep_signals:
             L.oracle_keep_signals(self._h, 1)
+        fmt, self._dtype = self.FORMATS[input_format]
+        L.oracle_set_input(self._h, fmt, 1 if dc_correct else 0)
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
@@ -71,7 +77,7 @@ class Oracle:
 
     def decode(self, samples):
         L = _load()
-        samples = np.ascontiguousarray(samples, np.uint8)
+        samples = np.ascontiguousarray(samples, self._dtype)
         n = L.oracle_decode(self._h, samples.ctypes.data, samples.size)
         self.n_fields = n
         P = ctypes.POINTER(ctypes.c_uint16)

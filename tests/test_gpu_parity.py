@@ -160,6 +160,47 @@ def test_pinned_buffers_give_identical_output(name, batch):
     assert a.json == b.json
 
 
+def _as_format(x, fmt, dc=0):
+    """The u8 capture x as s16 / u16 samples of the same converted values
+    ((x - 128) * 256), plus a constant DC offset."""
+    v = (x.astype(np.int32) - 128) * 256 + dc
+    if fmt == "s16":
+        return np.clip(v, -32768, 32767).astype(np.int16)
+    return np.clip(v + 32768, 0, 65535).astype(np.uint16)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fmt", ["s16", "u16"])
+def test_16_bit_inputs_decode_as_the_u8_capture(fmt):
+    """s16 and u16 samples carrying the u8 capture's converted values decode
+    to the same bytes (conversion of src/io/raw_reader.cpp:71-91), in one
+    chunk and in chunks of 4 fields."""
+    x = workload("small28")
+    y = _as_format(x, fmt)
+    for batch in (0, 4):
+        with cv.Decoder(28.0, batch_fields=batch) as d:
+            a = d.decode_capture(x)
+        with cv.Decoder(28.0, batch_fields=batch, input_format=fmt) as d:
+            b = d.decode_capture(y)
+        assert b.n_fields == a.n_fields > 0
+        assert np.array_equal(a.luma, b.luma) and np.array_equal(a.chroma, b.chroma) and a.json == b.json
+
+
+@pytest.mark.gpu
+def test_dc_correction_matches_oracle():
+    """--dc-correct on an s16 capture with a DC offset of 2500 (the chunk mean
+    of the samples read is subtracted before the zero fill,
+    src/io/raw_reader.cpp:93-99): against the oracle with the same option."""
+    x = workload("small28")
+    y = _as_format(x, "s16", dc=2500)
+    with cv.Decoder(28.0, input_format="s16", dc_correct=True) as d:
+        r = d.decode_capture(y)
+    from oracle.oracle import Oracle
+    o = Oracle(28.0, input_format="s16", dc_correct=True)
+    o.decode(y)
+    compare_to_oracle("small28", r, None, x, 28.0, o)
+
+
 @pytest.mark.gpu
 def test_field_locations_past_32_bits():
     """A chunk whose first sample is capture sample 5*2^32 + 12345 (a long
@@ -202,6 +243,18 @@ def test_cli_end_to_end(tmp_path):
     # a second run without --overwrite refuses
     p2 = subprocess.run([cv.CLI_PATH, "-f", "28", str(inp), str(base)], capture_output=True, text=True, timeout=60)
     assert p2.returncode == 1 and "Output exists" in p2.stderr
+    # the same capture as .s16 (format from the extension) and as raw u16 named
+    # with --format, read in 2-byte samples from the file, give the same files
+    for ext, fmt, extra in (("s16", "s16", []), ("bin", "u16", ["--format", "u16"])):
+        f16 = tmp_path / f"cap16.{ext}"
+        _as_format(x, fmt).tofile(f16)
+        b16 = tmp_path / f"out_{fmt}"
+        p3 = subprocess.run([cv.CLI_PATH, "-f", "28", "--overwrite"] + extra + [str(f16), str(b16)],
+                            capture_output=True, text=True, timeout=300)
+        assert p3.returncode == 0, p3.stderr
+        assert (tmp_path / f"out_{fmt}.tbc.json").read_text() == g["json_text"]
+        assert (tmp_path / f"out_{fmt}.tbc").read_bytes() == (tmp_path / "out.tbc").read_bytes()
+        assert (tmp_path / f"out_{fmt}_chroma.tbc").read_bytes() == (tmp_path / "out_chroma.tbc").read_bytes()
 
 
 @pytest.mark.gpu

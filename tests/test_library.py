@@ -76,10 +76,28 @@ def test_cli_refuses_existing_outputs(tmp_path):
 
 
 def test_cli_rejects_unsupported_modes(tmp_path):
-    inp = tmp_path / "in.u16"
-    inp.write_bytes(bytes(1000))
-    assert run_cli("--overwrite", str(inp), str(tmp_path / "o")).returncode == 1
-    assert run_cli("--overwrite", "--system", "PAL", str(tmp_path / "x.u8"), str(tmp_path / "o")).returncode == 1
+    r = run_cli("--overwrite", "--system", "PAL", str(tmp_path / "x.u8"), str(tmp_path / "o"))
+    assert r.returncode == 1 and "NTSC" in r.stderr
+
+
+def test_oracle_16_bit_inputs_and_dc_correction():
+    """The oracle's --format / --dc-correct restatement (src/io/raw_reader.cpp:71-99):
+    s16 and u16 samples of the u8 capture's converted values decode to the same
+    bytes; DC correction removes an added constant offset up to FP64 rounding."""
+    from oracle.oracle import Oracle
+    x = cv.make_workload("small28")
+    v = (x.astype(np.int32) - 128) * 256
+    outs = []
+    for fmt, y, dc in (("u8", x, False), ("s16", v.astype(np.int16), False),
+                       ("u16", (v + 32768).astype(np.uint16), False),
+                       ("s16", np.clip(v + 2500, -32768, 32767).astype(np.int16), True)):
+        o = Oracle(28.0, input_format=fmt, dc_correct=dc)
+        o.decode(y)
+        outs.append(o)
+    for o in outs[1:3]:
+        assert o.json == outs[0].json
+        assert np.array_equal(o.luma, outs[0].luma) and np.array_equal(o.chroma, outs[0].chroma)
+    assert outs[3].n_fields == outs[0].n_fields
 
 
 def test_cli_missing_input_fails(tmp_path):

@@ -35,15 +35,26 @@ __global__ void __launch_bounds__(kThreadsC, 1) prefilter_kernel(ChromaArgs a) {
   const int tile = f * a.spp;               // chunk position of the tile
   const float dc = a.dc ? *a.dc : 0.0f;
   float2 v[16];
+  const int base = i0 - a.c_half;  // tile position of block sample 0 (before the wrap)
+  if (base >= 0 && base + N + a.c_out <= a.spp && tile + base + N + a.c_out <= a.n_read) {
+    // interior: no wrap, inside the tile's samples and the samples read
+    const int p = tile + base + t;
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
-    int q0 = (i0 - a.c_half + t + T * q) % a.ctile;
-    if (q0 < 0) q0 += a.ctile;
-    int q1 = q0 + a.c_out;
-    if (q1 >= a.ctile) q1 -= a.ctile;
-    const float v0 = q0 < a.spp ? raw_sample<FMT>(a.raw, tile + q0, a.n_read, dc) : 0.0f;
-    const float v1 = q1 < a.spp ? raw_sample<FMT>(a.raw, tile + q1, a.n_read, dc) : 0.0f;
-    v[q] = make_float2(v0, v1);
+    for (int q = 0; q < 16; q++)
+      v[q] = make_float2(raw_convert<FMT>(a.raw, p + T * q) - dc, raw_convert<FMT>(a.raw, p + T * q + a.c_out) - dc);
+  } else {
+    // the zero-padded tile wraps at most once (ctile > N + c_out)
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      int q0 = base + t + T * q;
+      if (q0 < 0) q0 += a.ctile;
+      else if (q0 >= a.ctile) q0 -= a.ctile;
+      int q1 = q0 + a.c_out;
+      if (q1 >= a.ctile) q1 -= a.ctile;
+      const float v0 = q0 < a.spp ? raw_sample<FMT>(a.raw, tile + q0, a.n_read, dc) : 0.0f;
+      const float v1 = q1 < a.spp ? raw_sample<FMT>(a.raw, tile + q1, a.n_read, dc) : 0.0f;
+      v[q] = make_float2(v0, v1);
+    }
   }
   RegFFT<N>::run<false>(v, sm, a.tw_c, t);
 #pragma unroll

@@ -164,6 +164,28 @@ lib.cuvhs_synth_ntsc.restype = ctypes.c_int
 lib.cuvhs_synth_lines.argtypes = [ctypes.POINTER(SynthParams), ctypes.c_longlong, _vp, _vp, _vp, ctypes.c_longlong]
 lib.cuvhs_synth_lines.restype = ctypes.c_longlong
 lib.cuvhs_synth_preemphasis.argtypes = [ctypes.POINTER(SynthParams), _vp, _vp]
+lib.cuvhs_decode_chunk_async.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int,
+                                         ctypes.POINTER(Output)]
+lib.cuvhs_decode_chunk_async.restype = ctypes.c_int
+lib.cuvhs_flush.argtypes = [_vp]
+lib.cuvhs_flush.restype = ctypes.c_int
+lib.cuvhs_ire0_hz.argtypes = [_vp]
+lib.cuvhs_ire0_hz.restype = ctypes.c_double
+lib.cuvhs_stage_fm_demod.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.c_int, _vp, _vp, _vp]
+lib.cuvhs_stage_fm_demod.restype = ctypes.c_int
+lib.cuvhs_stage_discover_vsyncs.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int64)]
+lib.cuvhs_stage_discover_vsyncs.restype = ctypes.c_int
+lib.cuvhs_stage_sync_pulses.argtypes = [_vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, _vp]
+lib.cuvhs_stage_sync_pulses.restype = ctypes.c_int
+lib.cuvhs_stage_line_locations.argtypes = [_vp, ctypes.c_uint64, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]
+lib.cuvhs_stage_line_locations.restype = ctypes.c_int
+lib.cuvhs_stage_hsync_refine.argtypes = [_vp, _vp, ctypes.c_int, _vp, ctypes.c_int]
+lib.cuvhs_stage_hsync_refine.restype = ctypes.c_int
+lib.cuvhs_stage_tbc_resample.argtypes = [_vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp]
+lib.cuvhs_stage_tbc_resample.restype = ctypes.c_int
+lib.cuvhs_stage_chroma_decode.argtypes = [_vp, _vp, ctypes.c_size_t, _vp, ctypes.c_int, _vp, _vp]
+lib.cuvhs_stage_chroma_decode.restype = ctypes.c_int
 
 # every symbol include/cuvhs.h and include/cuvhs_synth.h declare
 EXPORTED = [
@@ -177,6 +199,9 @@ EXPORTED = [
     "cuvhs_adjoint_destroy", "cuvhs_adjoint_fields", "cuvhs_adjoint_default_params", "cuvhs_adjoint_set_target",
     "cuvhs_adjoint_fwd", "cuvhs_adjoint_bwd", "cuvhs_adjoint_array", "cuvhs_synth_default_params",
     "cuvhs_synth_length", "cuvhs_synth_ntsc", "cuvhs_synth_lines", "cuvhs_synth_preemphasis",
+    "cuvhs_decode_chunk_async", "cuvhs_flush", "cuvhs_ire0_hz", "cuvhs_stage_fm_demod",
+    "cuvhs_stage_discover_vsyncs", "cuvhs_stage_sync_pulses", "cuvhs_stage_line_locations",
+    "cuvhs_stage_hsync_refine", "cuvhs_stage_tbc_resample", "cuvhs_stage_chroma_decode",
 ]
 
 
@@ -383,6 +408,29 @@ class Decoder:
         self._check(lib.cuvhs_decode_chunk(self._h, samples.ctypes.data, samples.size, raw_offset, num_fields,
                                            ctypes.byref(out)))
         return self._result(out, bufs), int(out.next_raw_offset)
+
+    def decode_chunks_async(self, samples: np.ndarray, num_fields: int = 0) -> DecodeResult:
+        """A capture chunk by chunk through cuvhs_decode_chunk_async into
+        page-locked planes (each chunk's plane copies overlap the next chunk's
+        decode), completed by cuvhs_flush."""
+        samples = np.ascontiguousarray(samples, dtype=self._dtype)
+        nf = num_fields or self.batch_fields
+        spf = self.samples_per_field
+        out, bufs = self._alloc_output(max_fields_for(samples.size, spf), pinned=True)
+        raw = 0
+        while raw < samples.size and (samples.size - raw) // spf > 0:
+            before = out.fields_out
+            n = min(nf, (samples.size - raw) // spf)
+            st = lib.cuvhs_decode_chunk_async(self._h, samples[raw:].ctypes.data, samples.size - raw, raw, n,
+                                              ctypes.byref(out))
+            if st != 0:
+                lib.cuvhs_flush(self._h)
+                self._check(st)
+            if out.fields_out == before:
+                break
+            raw = int(out.next_raw_offset)
+        self._check(lib.cuvhs_flush(self._h))
+        return self._result(out, bufs)
 
     def decode_chunk_device(self, d_ptr: int, n_avail: int, raw_offset: int, num_fields: int):
         fo = ctypes.c_int(0)

@@ -26,10 +26,6 @@ namespace cuvhs {
 cuvhs_status create_context(const cuvhs_config& cfg, int pool_threads, cuvhs_ctx** out);
 }  // namespace cuvhs
 
-struct cuvhs_ctx {
-  cuvhs::Context c;
-};
-
 namespace {
 
 using cd = std::complex<double>;

@@ -14,10 +14,6 @@
 #include "../../include/cuvhs.h"
 #include "pipeline.h"
 
-struct cuvhs_ctx {
-  cuvhs::Context c;
-};
-
 namespace {
 
 using cuvhs::ChunkResult;
@@ -79,7 +75,8 @@ bool page_locked(const void* p) {
 // plane there as soon as it is final (overlapping the rest of the decode);
 // otherwise the planes are copied after the decode.
 cuvhs_status decode_into(Context& c, const uint8_t* src, size_t n_avail, uint64_t raw_offset, int num_fields,
-                         cuvhs_output* out, const uint8_t* cap_base = nullptr, size_t cap_n = 0) {
+                         cuvhs_output* out, const uint8_t* cap_base = nullptr, size_t cap_n = 0,
+                         bool async = false) {
   const size_t F = (size_t)c.fmt.output_line_len * c.fmt.output_field_lines;
   uint16_t *dl = nullptr, *dc = nullptr;
   // a chunk yields at most min(num_fields, n_avail / samples_per_field) fields
@@ -92,9 +89,9 @@ cuvhs_status decode_into(Context& c, const uint8_t* src, size_t n_avail, uint64_
   ChunkResult r;
   // a chunk of a whole page-locked capture prefetches the next chunk's window
   // and, with page-locked planes, defers its plane copies (the capture loop
-  // drains them)
+  // drains them); so does an asynchronous chunk call (cuvhs_flush drains them)
   if (cap_base && !page_locked(cap_base)) cap_base = nullptr;
-  const bool defer = cap_base != nullptr && (dl || dc);
+  const bool defer = (cap_base != nullptr || async) && (dl || dc);
   if (!c.decode_chunk(src, false, n_avail, raw_offset, num_fields, r, dl, dc, cap_base, cap_n, defer))
     return c.status;
   return append_chunk(c, r, out);
@@ -184,6 +181,23 @@ cuvhs_status cuvhs_decode_chunk(cuvhs_ctx* ctx, const uint8_t* samples, size_t n
   Context& c = ctx->c;
   c.status = CUVHS_OK;
   return decode_into(c, samples, n_avail, raw_offset, num_fields, out);
+}
+
+cuvhs_status cuvhs_decode_chunk_async(cuvhs_ctx* ctx, const uint8_t* samples, size_t n_avail, uint64_t raw_offset,
+                                      int num_fields, cuvhs_output* out) {
+  if (!ctx || !samples || !out) return CUVHS_ERR_INVALID_ARGUMENT;
+  Context& c = ctx->c;
+  c.status = CUVHS_OK;
+  return decode_into(c, samples, n_avail, raw_offset, num_fields, out, nullptr, 0, true);
+}
+
+cuvhs_status cuvhs_flush(cuvhs_ctx* ctx) {
+  if (!ctx) return CUVHS_ERR_INVALID_ARGUMENT;
+  Context& c = ctx->c;
+  c.status = CUVHS_OK;
+  cudaSetDevice(c.device);
+  if (!c.drain_copies()) return c.status;
+  return CUVHS_OK;
 }
 
 cuvhs_status cuvhs_decode_chunk_device(cuvhs_ctx* ctx, const uint8_t* d_samples, size_t n_avail,

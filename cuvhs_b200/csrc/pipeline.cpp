@@ -482,6 +482,275 @@ DemodArgs Context::demod_args(int T) const {
   return da;
 }
 
+ChromaArgs Context::chroma_args(const uint8_t* raw, int n_read, const float* dc, int T) const {
+  ChromaArgs ca;
+  ca.raw = raw;
+  ca.in_fmt = in_fmt;
+  ca.n_read = n_read;
+  ca.dc = dc;
+  ca.pre = d_dem;  // the raw demod is no longer needed after K1b
+  ca.fields = T;
+  ca.spp = spp;
+  ca.ctile = des.ctile;
+  ca.c_half = des.c_half;
+  ca.c_out = des.c_out;
+  ca.gc = d_gc;
+  ca.tw_c = d_twc;
+  ca.tw_line = d_twl;
+  ca.tw_c_inv = d_twc_inv;
+  ca.tw_line_inv = d_twl_inv;
+  ca.ll = d_ll;
+  ca.total = 0;
+  ca.track = d_track;
+  ca.het_scale = des.het_scale;
+  ca.fsc_bin = des.fsc_bin;
+  ca.bw_bins = des.bw_bins;
+  ca.burst_start = fmt.burst_start;
+  ca.out_w = fmt.output_line_len;
+  ca.out_h = fmt.output_field_lines;
+  ca.lines_per_frame = fmt.lines_per_frame;
+  ca.burst_abs_ref = (float)fmt.burst_abs_ref;
+  ca.chroma = d_chroma;
+  ca.burst = d_burst;
+  ca.metric = dp_metric;
+  ca.col_frac = d_col_frac;
+  return ca;
+}
+
+LineArgs Context::line_args(int P) const {
+  LineArgs la;
+  la.video = d_video;
+  la.sync = d_sync;
+  la.ll = d_ll;
+  la.fields = P;
+  la.total = (long long)P * spp;
+  la.lines_per_frame = fmt.lines_per_frame;
+  la.active_line_start = fmt.active_line_start;
+  la.thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
+  la.one_us = 1.0e-6 * fmt.fs_hz;
+  la.hsync_width = fmt.hsync_width;
+  la.right_edge_offset = 2.25 * ((fmt.fs_hz / 1.0e6) / 40.0);
+  la.luma = d_luma;
+  la.out_w = fmt.output_line_len;
+  la.out_h = fmt.output_field_lines;
+  la.luma_gain = (float)(fmt.output_scale / fmt.hz_ire);
+  la.luma_offset = (float)(-fmt.vsync_ire * fmt.output_scale + fmt.output_zero);
+  la.col_frac = d_col_frac;
+  return la;
+}
+
+DropoutArgs Context::dropout_args(int P) const {
+  DropoutArgs dd;
+  dd.env = d_env;
+  dd.env_part = d_env_part;
+  dd.env_blocks = env_blocks;
+  dd.ll = d_ll;
+  dd.fields = P;
+  dd.spp = spp;
+  dd.lines_per_frame = fmt.lines_per_frame;
+  dd.active_line_start = fmt.active_line_start;
+  dd.out_w = fmt.output_line_len;
+  dd.out_h = fmt.output_field_lines;
+  dd.luma = d_luma;
+  dd.chroma = d_chroma;
+  dd.do_count = d_do_count;
+  dd.do_lines = d_do_lines;
+  dd.do_starts = d_do_starts;
+  dd.do_ends = d_do_ends;
+  dd.cls = d_do_cls;
+  return dd;
+}
+
+bool Context::read_edges(const float* sync, long long total) {
+  const float thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
+  cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), stream);
+  {
+    cudaEvent_t ev_;
+    begin_stage(kStageEdges, ev_);
+    launch_edges(sync, total, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, stream);
+    end_stage(kStageEdges, ev_, 3);
+  }
+  cudaMemcpyAsync(hp_counts, d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream);
+  if (!this->sync("sync edges")) return false;
+  const int nfall = hp_counts[0], nrise = hp_counts[1];
+  if (nfall > edge_cap || nrise > edge_cap) {
+    err = "sync edge list overflow";
+    status = CUVHS_ERR_CAPACITY;
+    return false;
+  }
+  h_fall.resize(nfall);
+  h_rise.resize(nrise);
+  if (nfall) cudaMemcpyAsync(h_fall.data(), d_fall, (size_t)nfall * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
+  if (nrise) cudaMemcpyAsync(h_rise.data(), d_rise, (size_t)nrise * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
+  return this->sync("sync edge lists");
+}
+
+// Sync threshold runs [start, end) from the falling and rising edge lists
+// (both in sample order): end = the first rising edge after start, or the
+// range end.
+void edge_runs(const std::vector<unsigned>& fall, const std::vector<unsigned>& rise, long long total,
+               std::vector<long long>& run_start, std::vector<long long>& run_end) {
+  run_start.resize(fall.size());
+  run_end.resize(fall.size());
+  size_t r = 0;
+  for (size_t i = 0; i < fall.size(); i++) {
+    while (r < rise.size() && rise[r] <= fall[i]) r++;
+    run_start[i] = (long long)fall[i];
+    run_end[i] = r < rise.size() ? (long long)rise[r] : total;
+  }
+}
+
+// VSYNC candidates (runs of 20-35 us, vsync_discover.cu:58-72) and the field
+// windows clustered from them (pipeline.cu:1567-1651).
+void field_windows(const Format& fmt, const std::vector<long long>& run_start, const std::vector<long long>& run_end,
+                   int T, int num_fields, FieldWindows& w) {
+  const size_t spf = (size_t)fmt.samples_per_field;
+  const int minw = (int)(20.0e-6 * fmt.fs_hz), maxw = (int)(35.0e-6 * fmt.fs_hz);
+  w.cand.clear();
+  for (size_t i = 0; i < run_start.size(); i++) {
+    const long long wd = run_end[i] - run_start[i];
+    if (wd >= minw && wd <= maxw) w.cand.push_back((int)run_start[i]);
+  }
+  w.offs.clear();
+  for (int pos : w.cand) {
+    if (w.offs.empty() || ((size_t)pos - w.offs.back() > (size_t)(fmt.samples_per_field / 2))) {
+      const size_t safe = (pos > 5 * fmt.samples_per_line) ? (size_t)(pos - 5 * fmt.samples_per_line) : 0;
+      w.offs.push_back(safe);
+    }
+  }
+  if (w.offs.empty())
+    for (int i = 0; i < T; i++) w.offs.push_back((size_t)i * spf);
+  if ((int)w.offs.size() > num_fields) w.offs.resize(num_fields);
+  size_t actual_spf = spf;
+  if (w.offs.size() >= 2) actual_spf = (w.offs.back() - w.offs.front()) / (w.offs.size() - 1);
+  const size_t predicted = w.offs.back() + actual_spf, margin = 10 * (size_t)fmt.samples_per_line;
+  w.next_rel = predicted > margin ? predicted - margin : predicted;
+}
+
+// Pulses of the field window starting at chunk sample off (sync_pulses.cu:10-58):
+// runs that start after off and end within the spp-sample scan, at most
+// kMaxPulses.
+void window_pulses(const std::vector<long long>& run_start, const std::vector<long long>& run_end, long long off,
+                   int spp, std::vector<int>& ps, std::vector<int>& pl) {
+  ps.clear();
+  pl.clear();
+  const long long lim = off + spp - 1;  // last sample index the field's scan reaches
+  size_t i = std::lower_bound(run_start.begin(), run_start.end(), off + 1) - run_start.begin();
+  for (; i < run_start.size() && run_start[i] <= lim; i++) {
+    if (run_end[i] > lim) break;  // still open when the scan ends
+    if ((int)ps.size() < kMaxPulses) {
+      ps.push_back((int)run_start[i]);
+      pl.push_back((int)(run_end[i] - run_start[i]));
+    }
+  }
+}
+
+// Chroma of fields [0, P) with the track and phase decisions of
+// chroma_decode.cu:640-1001: on the first chunk the track and burst phase come
+// from two trial passes over field 0; then every field is computed with the
+// alternating track assignment and the reference's per-15-field flip-and-retry
+// passes are replayed on the host.  Sets h_phase and the carried chroma state.
+bool Context::chroma_fields(ChromaArgs& ca, int P) {
+  const int H = fmt.output_field_lines;
+  double t_host = 0.0;
+  auto chroma_pass = [&](int f0, int nf, bool write) {
+    cudaEvent_t ev_;
+    begin_stage(kStageChromaLines, ev_);
+    launch_chroma_lines(ca, f0, nf, write, stream);
+    end_stage(kStageChromaLines, ev_);
+    if (write) {
+      begin_stage(kStageBurstMetric, ev_);
+      launch_burst_metric(ca, f0, nf, stream);  // writes hp_metric through its mapping
+      end_stage(kStageBurstMetric, ev_);
+    }
+  };
+  int det_track, cycle_start;
+  double thr;
+  if (chroma_valid) {
+    det_track = chroma_track;
+    thr = chroma_threshold;
+    cycle_start = chroma_cycle_start;
+  } else {
+    // Track and burst phase from field 0 (chroma_decode.cu:684-743): both
+    // trial tracks in one round trip; the detected track's burst windows are
+    // the ones the phase measurement reads.
+    const size_t nb = (size_t)H * kBurstLen;
+    for (int t = 0; t < 2; t++) {
+      cudaMemcpyAsync(d_track, hp_trial + t, sizeof(int), cudaMemcpyHostToDevice, stream);
+      chroma_pass(0, 1, false);
+      cudaMemcpyAsync(hp_burst + t * nb, d_burst, nb * sizeof(float), cudaMemcpyDeviceToHost, stream);
+    }
+    cudaEventRecord(ev_host, stream);
+    t_host = host_clock();
+    if (!wait_host_event("chroma track detect")) return false;
+    host_phase(kHostChromaWait, t_host);
+    const double m0 = host_burst_metric(hp_burst, H), m1 = host_burst_metric(hp_burst + nb, H);
+    det_track = (m1 < m0) ? 1 : 0;
+    thr = (det_track ? m1 : m0) * 4.0;
+    const double ph = host_burst_phase(hp_burst + det_track * nb, H, fmt);
+    const int quadrant = ((int)(ph / 90.0 + 0.5)) % 4;
+    const int pid = phase_id_for(1, quadrant);
+    cycle_start = 0;
+    for (int i = 0; i < 8; i += 2)
+      if (kPhaseCycle[i] == pid) {
+        cycle_start = i;
+        break;
+      }
+  }
+  int cur = det_track;
+  h_phase.assign(P, 0);
+  for (int f = 0; f < P; f++) {
+    hp_track[f] = (f & 1) ? (1 - cur) : cur;
+    h_phase[f] = kPhaseCycle[(cycle_start + f) % 8];
+  }
+  // Every field's chroma depends only on its own track, so all fields are
+  // computed in one pass with the initial assignment; the reference's
+  // 15-field chunks with up to three flip-and-retry passes each
+  // (chroma_decode.cu:782-981) are then replayed on the host, recomputing
+  // only fields whose track a flip changed.
+  computed_track.assign(hp_track, hp_track + P);
+  cudaMemcpyAsync(d_track, hp_track, P * sizeof(int), cudaMemcpyHostToDevice, stream);
+  chroma_pass(0, P, true);
+  cudaEventRecord(ev_host, stream);
+  t_host = host_clock();
+  if (!wait_host_event("chroma lines")) return false;
+  host_phase(kHostChromaWait, t_host);
+  const int fpc = std::max(1, std::min((4096 / H), P));
+  for (int f0 = 0; f0 < P; f0 += fpc) {
+    const int nf = std::min(fpc, P - f0);
+    int retries = 3;
+    bool ok = false;
+    while (!ok && retries-- > 0) {
+      bool stale = false;
+      for (int f = f0; f < f0 + nf; f++) stale = stale || computed_track[f] != hp_track[f];
+      if (stale) {
+        cudaMemcpyAsync(d_track + f0, hp_track + f0, nf * sizeof(int), cudaMemcpyHostToDevice, stream);
+        chroma_pass(f0, nf, true);
+        cudaEventRecord(ev_host, stream);
+        if (!wait_host_event("chroma retry")) return false;
+        for (int f = f0; f < f0 + nf; f++) computed_track[f] = hp_track[f];
+      }
+      int first_bad = INT_MAX;
+      for (int f = 0; f < nf; f++)
+        if (hp_metric[f0 + f] > thr) {
+          first_bad = f;
+          break;
+        }
+      if (first_bad == INT_MAX) {
+        ok = true;
+      } else {
+        cur = 1 - cur;
+        for (int ff = f0 + first_bad; ff < P; ff++) hp_track[ff] = (ff & 1) ? (1 - cur) : cur;
+      }
+    }
+  }
+  chroma_valid = true;
+  chroma_track = (P & 1) ? (1 - cur) : cur;
+  chroma_threshold = thr;
+  chroma_cycle_start = (cycle_start + P) % 8;
+  return true;
+}
+
 // Decode one chunk.  `src` is host memory unless `src_on_device`.
 bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avail, uint64_t raw_offset,
                            int num_fields, ChunkResult& res, uint16_t* dst_luma, uint16_t* dst_chroma,
@@ -600,37 +869,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   // It covers all T demodulated slots; the detected fields are a prefix.
   const int LPF = fmt.lines_per_frame;
   const int H = fmt.output_field_lines;
-  ChromaArgs ca;
-  ca.raw = da.raw;
-  ca.in_fmt = in_fmt;
-  ca.n_read = (int)n_read;
-  ca.dc = da.dc;
-  ca.pre = d_dem;  // the raw demod is no longer needed after K1b
-  ca.fields = T;
-  ca.spp = spp;
-  ca.ctile = des.ctile;
-  ca.c_half = des.c_half;
-  ca.c_out = des.c_out;
-  ca.gc = d_gc;
-  ca.tw_c = d_twc;
-  ca.tw_line = d_twl;
-  ca.tw_c_inv = d_twc_inv;
-  ca.tw_line_inv = d_twl_inv;
-  ca.ll = d_ll;
-  ca.total = 0;
-  ca.track = d_track;
-  ca.het_scale = des.het_scale;
-  ca.fsc_bin = des.fsc_bin;
-  ca.bw_bins = des.bw_bins;
-  ca.burst_start = fmt.burst_start;
-  ca.out_w = fmt.output_line_len;
-  ca.out_h = H;
-  ca.lines_per_frame = LPF;
-  ca.burst_abs_ref = (float)fmt.burst_abs_ref;
-  ca.chroma = d_chroma;
-  ca.burst = d_burst;
-  ca.metric = dp_metric;
-  ca.col_frac = d_col_frac;
+  ChromaArgs ca = chroma_args(da.raw, (int)n_read, da.dc, T);
   if (debug) {
     dbg_demod.resize(std::min<size_t>((size_t)T * spp, (size_t)debug_tiles * spp));
     cudaMemcpyAsync(dbg_demod.data(), d_dem, dbg_demod.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
@@ -666,42 +905,12 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     if (!sync("edge lists")) return false;
   }
   // both lists arrive in sample order
-  // runs [start, end): end = first rising edge after start, or the range end
-  run_start.resize(h_fall.size());
-  run_end.resize(h_fall.size());
-  {
-    size_t r = 0;
-    for (size_t i = 0; i < h_fall.size(); i++) {
-      while (r < h_rise.size() && h_rise[r] <= h_fall[i]) r++;
-      run_start[i] = (long long)h_fall[i];
-      run_end[i] = r < h_rise.size() ? (long long)h_rise[r] : total_chunk;
-    }
-  }
+  edge_runs(h_fall, h_rise, total_chunk, run_start, run_end);
   // ---- VSYNC candidates and field windows (vsync_discover.cu:58-72, pipeline.cu:1567-1651)
-  const int minw = (int)(20.0e-6 * fmt.fs_hz), maxw = (int)(35.0e-6 * fmt.fs_hz);
-  std::vector<int> cand;
-  for (size_t i = 0; i < run_start.size(); i++) {
-    const long long w = run_end[i] - run_start[i];
-    if (w >= minw && w <= maxw) cand.push_back((int)run_start[i]);
-  }
-  std::vector<size_t> offs;
-  for (int pos : cand) {
-    if (offs.empty() || ((size_t)pos - offs.back() > (size_t)(fmt.samples_per_field / 2))) {
-      const size_t safe = (pos > 5 * fmt.samples_per_line) ? (size_t)(pos - 5 * fmt.samples_per_line) : 0;
-      offs.push_back(safe);
-    }
-  }
-  if (offs.empty())
-    for (int i = 0; i < T; i++) offs.push_back((size_t)i * spf);
-  int P = (int)offs.size();
-  if (P > num_fields) {
-    P = num_fields;
-    offs.resize(P);
-  }
-  size_t actual_spf = spf;
-  if (offs.size() >= 2) actual_spf = (offs.back() - offs.front()) / (offs.size() - 1);
-  const size_t predicted = offs.back() + actual_spf, margin = 10 * (size_t)fmt.samples_per_line;
-  res.next_raw_offset = predicted > margin ? raw_offset + predicted - margin : raw_offset + predicted;
+  field_windows(fmt, run_start, run_end, T, num_fields, win);
+  const std::vector<size_t>& offs = win.offs;
+  const int P = (int)offs.size();
+  res.next_raw_offset = raw_offset + win.next_rel;
   // ---- the next chunk of a host capture starts at next_raw_offset: copy its
   // window into the other raw buffer now (the chunk loop's arithmetic, so the
   // next call finds it); the previous chunk that read that buffer has ended.
@@ -740,18 +949,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   if ((int)preps.size() < P) preps.resize(P);
   pool->run(P, [&](int f) {
     thread_local std::vector<int> ps, pl;
-    ps.clear();
-    pl.clear();
-    const long long off = (long long)offs[f];
-    const long long lim = off + spp - 1;  // last sample index the field's scan reaches
-    size_t i = std::lower_bound(run_start.begin(), run_start.end(), off + 1) - run_start.begin();
-    for (; i < run_start.size() && run_start[i] <= lim; i++) {
-      if (run_end[i] > lim) break;  // still open when the scan ends
-      if ((int)ps.size() < kMaxPulses) {
-        ps.push_back((int)run_start[i]);
-        pl.push_back((int)(run_end[i] - run_start[i]));
-      }
-    }
+    window_pulses(run_start, run_end, (long long)offs[f], spp, ps, pl);
     prepare_lines(fmt, ps.data(), pl.data(), (int)ps.size(), preps[f], hp_ll + (size_t)f * LPF);
     if (debug) {
       dbg_k2c[f] = (int)ps.size();
@@ -776,7 +974,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     }
   }
   if (debug) {
-    dbg_vsync = cand;
+    dbg_vsync = win.cand;
     dbg_offs.assign(offs.begin(), offs.end());
     dbg_ll_coarse.assign(hp_ll, hp_ll + (size_t)P * LPF);
     dbg_meta = {T, P, spp};
@@ -784,24 +982,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   cudaMemcpyAsync(d_ll, hp_ll, (size_t)P * LPF * sizeof(double), cudaMemcpyHostToDevice, stream);
   host_phase(kHostLines, t_host);
   // ---- K4 hsync refinement, K5 luma
-  LineArgs la;
-  la.video = d_video;
-  la.sync = d_sync;
-  la.ll = d_ll;
-  la.fields = P;
-  la.total = (long long)P * spp;
-  la.lines_per_frame = LPF;
-  la.active_line_start = fmt.active_line_start;
-  la.thr_rel = thr_rel;
-  la.one_us = 1.0e-6 * fmt.fs_hz;
-  la.hsync_width = fmt.hsync_width;
-  la.right_edge_offset = 2.25 * ((fmt.fs_hz / 1.0e6) / 40.0);
-  la.luma = d_luma;
-  la.out_w = fmt.output_line_len;
-  la.out_h = H;
-  la.luma_gain = (float)(fmt.output_scale / fmt.hz_ire);
-  la.luma_offset = (float)(-fmt.vsync_ire * fmt.output_scale + fmt.output_zero);
-  la.col_frac = d_col_frac;
+  LineArgs la = line_args(P);
   {
     cudaEvent_t ev_;
     begin_stage(kStageHsync, ev_);
@@ -817,24 +998,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   if (!check_cuda("lines")) return false;
   // ---- K7 dropouts: detection, mapping and luma concealment (luma is final
   // now, so it leaves the device on the copy stream while chroma decodes)
-  DropoutArgs dd;
-  dd.env = d_env;
-  dd.env_part = d_env_part;
-  dd.env_blocks = env_blocks;
-  dd.ll = d_ll;
-  dd.fields = P;
-  dd.spp = spp;
-  dd.lines_per_frame = LPF;
-  dd.active_line_start = fmt.active_line_start;
-  dd.out_w = fmt.output_line_len;
-  dd.out_h = H;
-  dd.luma = d_luma;
-  dd.chroma = d_chroma;
-  dd.do_count = d_do_count;
-  dd.do_lines = d_do_lines;
-  dd.do_starts = d_do_starts;
-  dd.do_ends = d_do_ends;
-  dd.cls = d_do_cls;
+  DropoutArgs dd = dropout_args(P);
   {
     cudaEvent_t ev_;
     begin_stage(kStageDropouts, ev_);
@@ -858,101 +1022,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   // ---- K6 chroma on the P detected fields
   ca.fields = P;
   ca.total = (long long)P * spp;
-  auto chroma_pass = [&](int f0, int nf, bool write) {
-    cudaEvent_t ev_;
-    begin_stage(kStageChromaLines, ev_);
-    launch_chroma_lines(ca, f0, nf, write, stream);
-    end_stage(kStageChromaLines, ev_);
-    if (write) {
-      begin_stage(kStageBurstMetric, ev_);
-      launch_burst_metric(ca, f0, nf, stream);  // writes hp_metric through its mapping
-      end_stage(kStageBurstMetric, ev_);
-    }
-  };
-  int det_track, cycle_start;
-  double thr;
-  if (chroma_valid) {
-    det_track = chroma_track;
-    thr = chroma_threshold;
-    cycle_start = chroma_cycle_start;
-  } else {
-    // Track and burst phase from field 0 (chroma_decode.cu:684-743): both
-    // trial tracks in one round trip; the detected track's burst windows are
-    // the ones the phase measurement reads.
-    const size_t nb = (size_t)H * kBurstLen;
-    for (int t = 0; t < 2; t++) {
-      cudaMemcpyAsync(d_track, hp_trial + t, sizeof(int), cudaMemcpyHostToDevice, stream);
-      chroma_pass(0, 1, false);
-      cudaMemcpyAsync(hp_burst + t * nb, d_burst, nb * sizeof(float), cudaMemcpyDeviceToHost, stream);
-    }
-    cudaEventRecord(ev_host, stream);
-    t_host = host_clock();
-    if (!wait_host_event("chroma track detect")) return false;
-    host_phase(kHostChromaWait, t_host);
-    const double m0 = host_burst_metric(hp_burst, H), m1 = host_burst_metric(hp_burst + nb, H);
-    det_track = (m1 < m0) ? 1 : 0;
-    thr = (det_track ? m1 : m0) * 4.0;
-    const double ph = host_burst_phase(hp_burst + det_track * nb, H, fmt);
-    const int quadrant = ((int)(ph / 90.0 + 0.5)) % 4;
-    const int pid = phase_id_for(1, quadrant);
-    cycle_start = 0;
-    for (int i = 0; i < 8; i += 2)
-      if (kPhaseCycle[i] == pid) {
-        cycle_start = i;
-        break;
-      }
-  }
-  int cur = det_track;
-  h_phase.assign(P, 0);
-  for (int f = 0; f < P; f++) {
-    hp_track[f] = (f & 1) ? (1 - cur) : cur;
-    h_phase[f] = kPhaseCycle[(cycle_start + f) % 8];
-  }
-  // Every field's chroma depends only on its own track, so all fields are
-  // computed in one pass with the initial assignment; the reference's
-  // 15-field chunks with up to three flip-and-retry passes each
-  // (chroma_decode.cu:782-981) are then replayed on the host, recomputing
-  // only fields whose track a flip changed.
-  computed_track.assign(hp_track, hp_track + P);
-  cudaMemcpyAsync(d_track, hp_track, P * sizeof(int), cudaMemcpyHostToDevice, stream);
-  chroma_pass(0, P, true);
-  cudaEventRecord(ev_host, stream);
-  t_host = host_clock();
-  if (!wait_host_event("chroma lines")) return false;
-  host_phase(kHostChromaWait, t_host);
-  const int fpc = std::max(1, std::min((4096 / H), P));
-  for (int f0 = 0; f0 < P; f0 += fpc) {
-    const int nf = std::min(fpc, P - f0);
-    int retries = 3;
-    bool ok = false;
-    while (!ok && retries-- > 0) {
-      bool stale = false;
-      for (int f = f0; f < f0 + nf; f++) stale = stale || computed_track[f] != hp_track[f];
-      if (stale) {
-        cudaMemcpyAsync(d_track + f0, hp_track + f0, nf * sizeof(int), cudaMemcpyHostToDevice, stream);
-        chroma_pass(f0, nf, true);
-        cudaEventRecord(ev_host, stream);
-        if (!wait_host_event("chroma retry")) return false;
-        for (int f = f0; f < f0 + nf; f++) computed_track[f] = hp_track[f];
-      }
-      int first_bad = INT_MAX;
-      for (int f = 0; f < nf; f++)
-        if (hp_metric[f0 + f] > thr) {
-          first_bad = f;
-          break;
-        }
-      if (first_bad == INT_MAX) {
-        ok = true;
-      } else {
-        cur = 1 - cur;
-        for (int ff = f0 + first_bad; ff < P; ff++) hp_track[ff] = (ff & 1) ? (1 - cur) : cur;
-      }
-    }
-  }
-  chroma_valid = true;
-  chroma_track = (P & 1) ? (1 - cur) : cur;
-  chroma_threshold = thr;
-  chroma_cycle_start = (cycle_start + P) % 8;
+  if (!chroma_fields(ca, P)) return false;
   // ---- chroma is final: conceal it and send both planes' remaining copies
   {
     cudaEvent_t ev_;

@@ -42,6 +42,20 @@ enum Stage {
 constexpr int kFirstHostStage = kHostEdgesWait;
 extern const char* const kStageNames[kNumStages];
 
+// VSYNC candidates, field windows and the predicted start of the next chunk
+// (relative to this chunk's first sample) from one chunk's sync runs.
+struct FieldWindows {
+  std::vector<int> cand;
+  std::vector<size_t> offs;
+  size_t next_rel = 0;
+};
+void edge_runs(const std::vector<unsigned>& fall, const std::vector<unsigned>& rise, long long total,
+               std::vector<long long>& run_start, std::vector<long long>& run_end);
+void field_windows(const Format& fmt, const std::vector<long long>& run_start, const std::vector<long long>& run_end,
+                   int T, int num_fields, FieldWindows& w);
+void window_pulses(const std::vector<long long>& run_start, const std::vector<long long>& run_end, long long off,
+                   int spp, std::vector<int>& ps, std::vector<int>& pl);
+
 struct Context {
   cuvhs_config cfg{};
   Format fmt;
@@ -119,6 +133,7 @@ struct Context {
   // host scratch (kept to avoid reallocation)
   std::vector<unsigned> h_fall, h_rise;
   std::vector<long long> run_start, run_end;
+  FieldWindows win;
   std::vector<int> h_is_first, h_phase, computed_track;
   std::vector<LinePrep> preps;
   std::unique_ptr<WorkPool> pool;
@@ -181,6 +196,16 @@ struct Context {
   bool drain_copies();
   // K1 arguments over T tiles of the current raw buffer into the context's buffers.
   DemodArgs demod_args(int T) const;
+  // Kernel arguments on the context's buffers: chroma over T tiles of `raw`,
+  // lines and dropouts over P fields.
+  ChromaArgs chroma_args(const uint8_t* raw, int n_read, const float* dc, int T) const;
+  LineArgs line_args(int P) const;
+  DropoutArgs dropout_args(int P) const;
+  // Chroma lines of fields [0, P) of ca (pre-band-passed already) with the
+  // track/phase decisions and the carried chroma state; sets h_phase.
+  bool chroma_fields(ChromaArgs& ca, int P);
+  // Sync edges of `sync` over [0, total) into h_fall / h_rise (synchronous).
+  bool read_edges(const float* sync, long long total);
 };
 
 // .tbc.json text (reference format, src/io/tbc_writer.cpp:89-175).
@@ -188,3 +213,8 @@ std::string tbc_json(const Format& fmt, const cuvhs_field_info* fields, size_t n
                      const int32_t* ds, const int32_t* de);
 
 }  // namespace cuvhs
+
+// The C ABI's opaque context handle.
+struct cuvhs_ctx {
+  cuvhs::Context c;
+};

@@ -17,6 +17,14 @@
  *   cuvhs_decode_file                 main + RawReader + TBCWriter (src/main.cpp:97-165,
  *                                     src/io/raw_reader.cpp:128-151, src/io/tbc_writer.cpp:10-175)
  *   cuvhs_json                        TBCWriter::write_json (src/io/tbc_writer.cpp:89-175)
+ *   cuvhs_stage_*                     the stage functions fm_demod, discover_vsyncs,
+ *                                     sync_pulses, hsync_refine, tbc_resample,
+ *                                     chroma_decode and the K2b host line locations
+ *                                     (src/pipeline/{fm_demod,vsync_discover,...}.h;
+ *                                     pipeline.cu:1557-2548)
+ *   cuvhs_decode_chunk_async,         no counterpart (the reference's calls are
+ *   cuvhs_flush                       synchronous): chunk decode whose plane copies
+ *                                     overlap the next chunk, and the wait for them
  *   cuvhs_debug_array                 the stage outputs the reference keeps in device
  *                                     buffers (d_pulse_*, d_linelocs, d_is_first_field,
  *                                     d_do_*; src/pipeline/pipeline.h:52-87)
@@ -107,6 +115,20 @@ void cuvhs_reset(cuvhs_ctx* ctx);
 cuvhs_status cuvhs_decode_chunk(cuvhs_ctx* ctx, const uint8_t* samples, size_t n_avail, uint64_t raw_offset,
                                 int num_fields, cuvhs_output* out);
 
+/* cuvhs_decode_chunk without waiting for the output planes: when out's luma
+ * and chroma are page-locked host memory with room for the chunk, the call
+ * returns once the field metadata and dropout lists are in `out`, while the
+ * planes are still being copied there, so the next chunk's decode overlaps
+ * them.  The planes are complete after cuvhs_flush.  With pageable planes it
+ * is cuvhs_decode_chunk. */
+cuvhs_status cuvhs_decode_chunk_async(cuvhs_ctx* ctx, const uint8_t* samples, size_t n_avail, uint64_t raw_offset,
+                                      int num_fields, cuvhs_output* out);
+/* Waits for everything the context still has in flight (plane copies of
+ * cuvhs_decode_chunk_async, input prefetches); afterwards every result that a
+ * call reported is in the caller's memory.  Returns the first CUDA error of
+ * that work.  The reference's calls are synchronous and need no flush. */
+cuvhs_status cuvhs_flush(cuvhs_ctx* ctx);
+
 /* The same chunk decode on samples already in device memory; the luma/chroma
  * TBC and dropout results stay on the device (read them with
  * cuvhs_device_outputs).  *fields_out = fields decoded. */
@@ -158,6 +180,76 @@ void cuvhs_set_debug(cuvhs_ctx* ctx, int on);
  * relative to the 0 IRE carrier, or raw units): "demod", "video", "sync",
  * "envelope", "chroma_prefilt".  Returns -1 for an unknown name. */
 long long cuvhs_debug_array(const cuvhs_ctx* ctx, const char* name, void* dst, long long cap);
+
+/* ---------------------------------------------------------------- stages
+ * One stage of the decode at a time on caller-owned buffers, for parity tests
+ * of single stages and for callers that compose their own pipeline.  Each
+ * entry point is the counterpart of one stage function of the reference's
+ * Pipeline::process_chunk (src/pipeline/pipeline.cu:1557-2548), runs the same
+ * kernels and host code as cuvhs_decode_chunk on the context's stream and
+ * scratch, shares its carried state (line-location history, chroma track and
+ * phase cycle) and returns when its results are complete.
+ *   A chunk is `tiles` field slots of cuvhs_tile_stride samples (tiles and
+ * n_fields at most cuvhs_batch_fields); chunk positions count samples from
+ * the chunk's first sample.  d_ arguments are device memory, the rest host
+ * memory.  Signals are FP32: video and sync in Hz relative to the 0 IRE
+ * frequency (cuvhs_ire0_hz), the envelope as |analytic signal| in the
+ * reference's scale.  Line locations are FP64 chunk positions, 525 per field.
+ * The dropout stage (dropout_detect, src/pipeline/dropout_detect.h:22-32) is
+ * cuvhs_dropouts_noalloc below. */
+#define CUVHS_MAX_PULSES_PER_FIELD 800
+#define CUVHS_LINES_PER_FRAME 525
+double cuvhs_ire0_hz(const cuvhs_ctx* ctx);
+
+/* fm_demod (src/pipeline/fm_demod.h:46-53): d_raw holds n_read samples of the
+ * configured input format (positions past n_read count as 0, the reference's
+ * zero fill); d_video, d_sync, d_envelope [tiles * tile_stride]. */
+cuvhs_status cuvhs_stage_fm_demod(cuvhs_ctx* ctx, const void* d_raw, size_t n_read, int tiles, float* d_video,
+                                  float* d_sync, float* d_envelope);
+
+/* discover_vsyncs (src/pipeline/vsync_discover.h:6-11) and the clustering of
+ * its candidates (src/pipeline/pipeline.cu:1567-1651): the field windows'
+ * starts (field_offsets, room for max_fields), their count, and where the
+ * next chunk starts (next_offset, may be NULL), all chunk positions.  Pass
+ * the chunk's requested field count as max_fields, as the reference caps it
+ * (pipeline.cu:1622-1624): a window can start past the last demodulated tile,
+ * so n_fields may exceed tiles by one. */
+cuvhs_status cuvhs_stage_discover_vsyncs(cuvhs_ctx* ctx, const float* d_sync, int tiles, int max_fields,
+                                         int64_t* field_offsets, int* n_fields, int64_t* next_offset);
+
+/* sync_pulses (src/pipeline/sync_pulses.h:20-27) with per-field offsets:
+ * starts/lengths [n_fields * CUVHS_MAX_PULSES_PER_FIELD], counts [n_fields]. */
+cuvhs_status cuvhs_stage_sync_pulses(cuvhs_ctx* ctx, const float* d_sync, int tiles, const int64_t* field_offsets,
+                                     int n_fields, int32_t* starts, int32_t* lengths, int32_t* counts);
+
+/* The host line locations that follow sync_pulses (src/pipeline/pipeline.cu:1717-1778):
+ * pulse validation, field order, blanking anchor and the snapped line grid,
+ * field by field with the field-order state carried across fields and calls.
+ * raw_offset is the capture sample of the chunk's first sample.  linelocs
+ * [n_fields * 525]; is_first_field [n_fields] (may be NULL) = 1, 0, or -1. */
+cuvhs_status cuvhs_stage_line_locations(cuvhs_ctx* ctx, uint64_t raw_offset, const int64_t* field_offsets,
+                                        int n_fields, const int32_t* starts, const int32_t* lengths,
+                                        const int32_t* counts, double* linelocs, int32_t* is_first_field);
+
+/* hsync_refine (src/pipeline/hsync_refine.h:18-22): refines d_linelocs
+ * [n_fields * 525] in place.  d_sync holds `tiles` slots; the refinement
+ * reads min(n_fields, tiles) * tile_stride samples of it (the reference's
+ * total_demod_samples = n_fields * tile_stride when the buffer covers them). */
+cuvhs_status cuvhs_stage_hsync_refine(cuvhs_ctx* ctx, const float* d_sync, int tiles, double* d_linelocs,
+                                      int n_fields);
+
+/* tbc_resample (src/pipeline/tbc_resample.h:16-27): d_luma [n_fields][263][910];
+ * d_video holds `tiles` slots, read as hsync_refine reads d_sync. */
+cuvhs_status cuvhs_stage_tbc_resample(cuvhs_ctx* ctx, const float* d_video, int tiles, const double* d_linelocs,
+                                      int n_fields, uint16_t* d_luma);
+
+/* chroma_decode (src/pipeline/chroma_decode.h:38-46): the colour-under chroma
+ * of n_fields fields from the raw chunk (n_read samples of the configured
+ * format) into d_chroma [n_fields][263][910]; field_phase_ids [n_fields] (may
+ * be NULL) receives the NTSC field phase IDs.  The first call after create or
+ * cuvhs_reset detects the track and phase cycle; later calls carry them. */
+cuvhs_status cuvhs_stage_chroma_decode(cuvhs_ctx* ctx, const void* d_raw, size_t n_read, const double* d_linelocs,
+                                       int n_fields, uint16_t* d_chroma, int32_t* field_phase_ids);
 
 /* Dropout detection and concealment on caller-owned device buffers, allocating
  * no device memory.  No counterpart in the reference (its dropout stage

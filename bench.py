@@ -95,9 +95,10 @@ def profiled_traffic(kernel):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons, sampled every interval_ms from
+    the first sample (start() waits for it) until stop()."""
 
-    def __init__(self, index, interval_ms=200):
+    def __init__(self, index, interval_ms=25):
         self.index = index
         self.interval_ms = interval_ms
         self.proc = None
@@ -116,6 +117,13 @@ class ClockSampler:
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi needs a moment to start: time nothing before its first row
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.01)
 
     def stop(self):
         if self.proc is None:
@@ -450,7 +458,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--clock-interval-ms", type=int, default=200,
+    ap.add_argument("--clock-interval-ms", type=int, default=25,
                     help="nvidia-smi sampling period during the timed region (0 = off)")
     ap.add_argument("--profile-case", action="store_true",
                     help="one device-resident decode of the workload with a 48-field allocation, "
@@ -543,7 +551,6 @@ def main():
         ev1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     stage = dec.stage_times()
     launches = dec.launch_count
@@ -585,6 +592,7 @@ def main():
         e2e_fields += e2e_step()
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
+    clk = clocks.stop()  # the samples span both timed regions
     barrier()
     fields_per_step = total_fields // args.steps
 

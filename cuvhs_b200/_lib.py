@@ -82,7 +82,7 @@ class SynthParams(ctypes.Structure):
                 ("carrier_offset_hz", ctypes.c_double), ("deviation_scale", ctypes.c_double),
                 ("first_track", ctypes.c_int), ("threads", ctypes.c_int),
                 ("preemph_perturb", ctypes.c_double * 3), ("line_offset_bound", ctypes.c_double),
-                ("chroma_phase_bound", ctypes.c_double)]
+                ("chroma_phase_bound", ctypes.c_double), ("system", ctypes.c_int)]
 
 
 _vp = ctypes.c_void_p
@@ -164,6 +164,12 @@ lib.cuvhs_synth_ntsc.restype = ctypes.c_int
 lib.cuvhs_synth_lines.argtypes = [ctypes.POINTER(SynthParams), ctypes.c_longlong, _vp, _vp, _vp, ctypes.c_longlong]
 lib.cuvhs_synth_lines.restype = ctypes.c_longlong
 lib.cuvhs_synth_preemphasis.argtypes = [ctypes.POINTER(SynthParams), _vp, _vp]
+lib.cuvhs_field_width.argtypes = [_vp]
+lib.cuvhs_field_width.restype = ctypes.c_int
+lib.cuvhs_field_height.argtypes = [_vp]
+lib.cuvhs_field_height.restype = ctypes.c_int
+lib.cuvhs_lines_per_frame.argtypes = [_vp]
+lib.cuvhs_lines_per_frame.restype = ctypes.c_int
 lib.cuvhs_decode_chunk_async.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int,
                                          ctypes.POINTER(Output)]
 lib.cuvhs_decode_chunk_async.restype = ctypes.c_int
@@ -202,6 +208,7 @@ EXPORTED = [
     "cuvhs_decode_chunk_async", "cuvhs_flush", "cuvhs_ire0_hz", "cuvhs_stage_fm_demod",
     "cuvhs_stage_discover_vsyncs", "cuvhs_stage_sync_pulses", "cuvhs_stage_line_locations",
     "cuvhs_stage_hsync_refine", "cuvhs_stage_tbc_resample", "cuvhs_stage_chroma_decode",
+    "cuvhs_field_width", "cuvhs_field_height", "cuvhs_lines_per_frame",
 ]
 
 
@@ -250,8 +257,8 @@ def synth_capture(**kw) -> np.ndarray:
 
 @dataclass
 class DecodeResult:
-    luma: np.ndarray          # [fields, 263, 910] u16
-    chroma: np.ndarray        # [fields, 263, 910] u16
+    luma: np.ndarray          # [fields, rows, columns] u16: 263 x 910 NTSC, 313 x 1135 PAL
+    chroma: np.ndarray        # [fields, rows, columns] u16
     file_loc: np.ndarray      # [fields] u64
     is_first_field: np.ndarray
     field_phase_id: np.ndarray
@@ -269,16 +276,17 @@ def max_fields_for(n_samples, samples_per_field):
     return int(n_samples / samples_per_field * 1.01) + 4
 
 
-def alloc_output(max_fields, pinned=False):
-    """Host output buffers for max_fields fields (page-locked when pinned)."""
+def alloc_output(max_fields, pinned=False, shape=(FIELD_H, FIELD_W)):
+    """Host output buffers for max_fields fields of `shape` (rows, columns;
+    NTSC by default), page-locked when pinned."""
     if pinned:
         import torch
-        planes = [torch.empty((max_fields, FIELD_H, FIELD_W), dtype=torch.int16).pin_memory() for _ in range(2)]
+        planes = [torch.empty((max_fields,) + tuple(shape), dtype=torch.int16).pin_memory() for _ in range(2)]
         luma, chroma = (p.numpy().view(np.uint16) for p in planes)
     else:
         planes = []
-        luma = np.empty((max_fields, FIELD_H, FIELD_W), np.uint16)
-        chroma = np.empty((max_fields, FIELD_H, FIELD_W), np.uint16)
+        luma = np.empty((max_fields,) + tuple(shape), np.uint16)
+        chroma = np.empty((max_fields,) + tuple(shape), np.uint16)
     bufs = {
         "planes": planes,
         "luma": luma,
@@ -321,11 +329,13 @@ class Decoder:
     """One libcuvhs context (device memory and stream, carried decode state)."""
 
     FORMATS = {"u8": (0, np.uint8), "s16": (1, np.int16), "u16": (2, np.uint16)}
+    SYSTEMS = {"NTSC": 0, "PAL": 1}
 
     def __init__(self, sample_rate_mhz=28.0, device=0, batch_fields=0, stream_mode=False, debug=False,
-                 input_format="u8", dc_correct=False):
+                 input_format="u8", dc_correct=False, system="NTSC"):
         cfg = Config()
         lib.cuvhs_default_config(ctypes.byref(cfg))
+        cfg.system = self.SYSTEMS[system.upper()]
         cfg.sample_rate_mhz = float(sample_rate_mhz)
         cfg.device = int(device)
         cfg.batch_fields = int(batch_fields)
@@ -366,6 +376,15 @@ class Decoder:
     def tile_stride(self):
         return lib.cuvhs_tile_stride(self._h)
 
+    @property
+    def field_shape(self):
+        """(rows, columns) of an output field: (263, 910) NTSC, (313, 1135) PAL."""
+        return lib.cuvhs_field_height(self._h), lib.cuvhs_field_width(self._h)
+
+    @property
+    def lines_per_frame(self):
+        return lib.cuvhs_lines_per_frame(self._h)
+
     def reset(self):
         lib.cuvhs_reset(self._h)
 
@@ -374,7 +393,7 @@ class Decoder:
             raise CuvhsError(st, lib.cuvhs_last_error(self._h).decode())
 
     def _alloc_output(self, max_fields, pinned=False):
-        return alloc_output(max_fields, pinned)
+        return alloc_output(max_fields, pinned, self.field_shape)
 
     def _result(self, out, bufs):
         def json_text():
@@ -553,9 +572,10 @@ class Batch:
 
 
 def decode_file(in_path, out_base, sample_rate_mhz=28.0, device=0, overwrite=True, batch_fields=0,
-                input_format="u8", dc_correct=False):
+                input_format="u8", dc_correct=False, system="NTSC"):
     cfg = Config()
     lib.cuvhs_default_config(ctypes.byref(cfg))
+    cfg.system = Decoder.SYSTEMS[system.upper()]
     cfg.sample_rate_mhz = float(sample_rate_mhz)
     cfg.device = int(device)
     cfg.batch_fields = int(batch_fields)

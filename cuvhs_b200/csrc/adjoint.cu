@@ -19,6 +19,10 @@ constexpr int kN = Design::kNb;
 constexpr int kT = kN / 16;
 constexpr int kRowThreads = 128;
 constexpr int kLineWarps = 4;
+// The calibration model is NTSC: 910-sample lines in a 1024-point line
+// transform, a 36-sample burst window.
+constexpr int kLineFFT = 1024;
+constexpr int kBurstLen = 36;
 
 template <int THREADS, int K>
 __device__ __forceinline__ void block_sum(double (&v)[K], double* sh /* [THREADS/32][K] */) {

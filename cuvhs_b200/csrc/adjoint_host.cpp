@@ -137,6 +137,10 @@ cuvhs_status cuvhs_adjoint_create(const cuvhs_config* cfg, const uint8_t* sample
                                   cuvhs_adjoint** out) {
   if (!cfg || !samples || !out || fields < 1) return CUVHS_ERR_INVALID_ARGUMENT;
   *out = nullptr;
+  if (cfg->system != 0) {
+    fprintf(stderr, "cuvhs_adjoint_create: the calibration model is NTSC only\n");
+    return CUVHS_ERR_UNSUPPORTED;
+  }
   cuvhs_adjoint* a = new (std::nothrow) cuvhs_adjoint();
   if (!a) return CUVHS_ERR_OUT_OF_MEMORY;
   cuvhs_config cc = *cfg;

@@ -166,6 +166,9 @@ void cuvhs_destroy(cuvhs_ctx* ctx) { delete ctx; }
 
 const char* cuvhs_last_error(const cuvhs_ctx* ctx) { return ctx ? ctx->c.err.c_str() : "null context"; }
 int cuvhs_batch_fields(const cuvhs_ctx* ctx) { return ctx ? ctx->c.batch : 0; }
+int cuvhs_field_width(const cuvhs_ctx* ctx) { return ctx ? ctx->c.fmt.output_line_len : 0; }
+int cuvhs_field_height(const cuvhs_ctx* ctx) { return ctx ? ctx->c.fmt.output_field_lines : 0; }
+int cuvhs_lines_per_frame(const cuvhs_ctx* ctx) { return ctx ? ctx->c.fmt.lines_per_frame : 0; }
 size_t cuvhs_samples_per_field(const cuvhs_ctx* ctx) { return ctx ? (size_t)ctx->c.fmt.samples_per_field : 0; }
 size_t cuvhs_tile_stride(const cuvhs_ctx* ctx) { return ctx ? (size_t)ctx->c.spp : 0; }
 void cuvhs_reset(cuvhs_ctx* ctx) {

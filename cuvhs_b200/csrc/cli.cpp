@@ -95,10 +95,7 @@ int main(int argc, char** argv) {
     const std::string ext = dot == std::string::npos ? in : in.substr(dot + 1);
     format = (ext == "s16") ? "s16" : (ext == "u16") ? "u16" : "u8";
   }
-  if (pal) {
-    fprintf(stderr, "This build decodes NTSC captures only\n");
-    return 1;
-  }
+  cfg.system = pal ? 1 : 0;
   cfg.input_format = format == "s16" ? 1 : (format == "u16" ? 2 : 0);
   cfg.dc_correct = dc_correct ? 1 : 0;
   cuvhs_status s = cuvhs_decode_file(&cfg, in.c_str(), out.c_str(), overwrite ? 1 : 0);

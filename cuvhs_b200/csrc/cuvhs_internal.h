@@ -22,13 +22,15 @@ constexpr int kFieldMarginLines = 20;  // extra lines per tile beyond one field
 constexpr int kMaxPulses = 800;        // pulses kept per field
 constexpr int kMaxDropouts = 512;      // TBC dropout entries per field
 constexpr int kMaxRfDropouts = 128;    // RF-domain dropout spans per field
-constexpr int kLineFFT = 1024;         // chroma per-line transform
-constexpr int kBurstLen = 36;          // burst window width in output samples (76..111)
+constexpr int kMaxBurstLen = 48;       // burst window width bound, output samples (NTSC 36, PAL 40)
 enum PulseType { kHsync = 0, kEq1 = 1, kVsync = 2, kEq2 = 3 };
+enum VideoSystem { kNtsc = 0, kPal = 1 };
 
-// NTSC constants derived from the capture rate
-// (reference: src/format/video_format.cpp:23-104).
+// Format constants of the video system, derived from the capture rate
+// (reference: src/format/video_format.cpp:23-104; the members' initial
+// values are NTSC's).
 struct Format {
+  int system = kNtsc;
   double fs_hz = 0;
   int lines_per_frame = 525;
   int output_line_len = 910;
@@ -48,7 +50,10 @@ struct Format {
   int spp = 0;  // tile stride: samples_per_field + 20 lines
   double hsync_width = 0, eq_pulse_width = 0, vsync_width = 0;
   int burst_start = 0, burst_end = 0;  // in output samples
-  void init(double mhz);
+  int burst_len = 0;                   // burst_end - burst_start
+  int lines_per_field = 263;
+  int line_fft = 1024;                 // chroma per-line transform: next power of 2 >= output_line_len
+  void init(double mhz, int system = kNtsc);
 };
 
 // Filter kernels for the three overlap-save stages.  Every stage reproduces a
@@ -144,6 +149,7 @@ struct LineArgs {
   uint16_t* luma;  // [P*263*910]
   int out_w, out_h;
   float luma_gain, luma_offset;  // u16 = video_rel * gain + offset
+  uint16_t oob_value;            // pixels outside the signal: output_zero (tbc_resample.cu:91-96)
   const double* col_frac;        // [out_w]: (double)col / (double)out_w
 };
 void launch_hsync_refine(const LineArgs& a, cudaStream_t st);
@@ -164,16 +170,17 @@ struct ChromaArgs {
   long long total;  // P * spp
   const int* track;  // per field
   double het_scale;
-  int fsc_bin, bw_bins, burst_start;
+  int fsc_bin, bw_bins, burst_start, burst_len;
+  int line_fft;      // per-line transform size (1024 or 2048)
   int out_w, out_h, lines_per_frame;
   float burst_abs_ref;
-  uint16_t* chroma;  // [P*263*910]
-  float* burst;      // [P*263*kBurstLen] band-passed burst window (scaled)
+  uint16_t* chroma;  // [P*out_h*out_w]
+  float* burst;      // [P*out_h*burst_len] band-passed burst window (scaled)
   double* metric;    // per field burst cancellation metric
   const double* col_frac;  // [out_w]: (double)col / (double)out_w
 };
 void launch_chroma_prefilter(const ChromaArgs& a, cudaStream_t st);
-// Lines [field0*263, (field0+nfields)*263) of the chunk.
+// Lines [field0*out_h, (field0+nfields)*out_h) of the chunk.
 void launch_chroma_lines(const ChromaArgs& a, int field0, int nfields, bool write_output, cudaStream_t st);
 void launch_burst_metric(const ChromaArgs& a, int field0, int nfields, cudaStream_t st);
 
@@ -189,14 +196,17 @@ struct DropoutArgs {
   int* do_lines;
   int* do_starts;
   int* do_ends;
-  unsigned char* cls = nullptr;  // two-pass form: [fields * dropout_class_bytes_per_field()]
+  unsigned char* cls = nullptr;  // two-pass form: [fields * max_blocks]
+  int max_blocks = 0;            // 16-sample blocks per field slot, dropout_class_bytes_per_field(spp)
 };
 // Fused form: one CTA per field, no scratch beyond env_part.
 void launch_dropouts(const DropoutArgs& a, cudaStream_t st);
 // Two-pass form: wide class kernel over every field, then a per-field scan
 // that maps the entries and conceals the luma; chroma concealment follows
 // once the chroma planes are final.
-size_t dropout_class_bytes_per_field();
+// Class bytes per field slot of spp samples: one per 16-sample block, rounded
+// up to a multiple of 16.
+size_t dropout_class_bytes_per_field(int spp);
 void launch_dropouts_two_pass(const DropoutArgs& a, cudaStream_t st);
 void launch_dropout_conceal_chroma(const DropoutArgs& a, cudaStream_t st);
 

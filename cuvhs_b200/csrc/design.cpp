@@ -145,24 +145,64 @@ std::vector<float2> twiddles(int n) {
 
 }  // namespace
 
-void Format::init(double mhz) {
+void Format::init(double mhz, int sys) {
+  system = sys == kPal ? kPal : kNtsc;
   fs_hz = mhz * 1e6;
-  chroma_under = (525.0 * (30.0 / 1.001)) * 40.0;
-  hz_ire = 1e6 / 140.0;
-  ire0 = 4.4e6 - (hz_ire * 100.0);
-  vsync_ire = -40.0;
+  if (system == kNtsc) {
+    lines_per_frame = 525;
+    lines_per_field = 263;
+    output_line_len = 910;
+    output_field_lines = 263;
+    field_lines_first = 263;
+    field_lines_second = 262;
+    num_eq_pulses = 6;
+    active_line_start = 10;
+    line_rate = 15734.264;
+    fsc = 3579545.0;
+    chroma_under = (525.0 * (30.0 / 1.001)) * 40.0;
+    burst_abs_ref = 4416.0;
+    burst_start_us = 5.3;
+    burst_end_us = 7.8;
+    hz_ire = 1e6 / 140.0;
+    ire0 = 4.4e6 - (hz_ire * 100.0);
+    vsync_ire = -40.0;
+    output_zero = 1024.0;
+    output_scale = (51200.0 - 1024.0) / (100.0 - vsync_ire);
+    vsync_width = 27.1e-6 * fs_hz;
+  } else {
+    lines_per_frame = 625;
+    lines_per_field = 313;
+    output_line_len = 1135;
+    output_field_lines = 313;
+    field_lines_first = 312;
+    field_lines_second = 313;
+    num_eq_pulses = 5;
+    active_line_start = 8;
+    line_rate = 15625.0;
+    fsc = 4433618.75;
+    chroma_under = ((625.0 * 25.0) * 40.0) + 1953.0;
+    burst_abs_ref = 5000.0;
+    burst_start_us = 5.6;
+    burst_end_us = 7.85;
+    vsync_ire = -0.3 * (100.0 / 0.7);
+    hz_ire = 1e6 / (100.0 + (-vsync_ire));
+    ire0 = 4.8e6 - (hz_ire * 100.0);
+    output_zero = 256.0;
+    output_scale = (54016.0 - 256.0) / (100.0 - vsync_ire);
+    vsync_width = 27.3e-6 * fs_hz;
+  }
   pulse_threshold_hz = ire0 + hz_ire * (-20.0);
-  output_zero = 1024.0;
-  output_scale = (51200.0 - 1024.0) / (100.0 - vsync_ire);
   output_rate = 4.0 * fsc;
   samples_per_line = (int)std::round(fs_hz / line_rate);
-  samples_per_field = samples_per_line * 263;
+  samples_per_field = samples_per_line * lines_per_field;
   spp = samples_per_field + kFieldMarginLines * samples_per_line;
   hsync_width = 4.7e-6 * fs_hz;
   eq_pulse_width = 2.3e-6 * fs_hz;
-  vsync_width = 27.1e-6 * fs_hz;
   burst_start = (int)(burst_start_us * 1e-6 * output_rate + 0.5);
   burst_end = (int)(burst_end_us * 1e-6 * output_rate + 0.5);
+  burst_len = burst_end - burst_start;
+  line_fft = 1;
+  while (line_fft < output_line_len) line_fft <<= 1;
 }
 
 void Design::build(const Format& fmt) {
@@ -267,10 +307,10 @@ void Design::build(const Format& fmt) {
   tw_a = twiddles(kNa);
   tw_b = twiddles(kNb);
   tw_c = twiddles(kNc);
-  tw_line = twiddles(kLineFFT);
+  tw_line = twiddles(fmt.line_fft);
   het_scale = (fmt.fsc + fmt.chroma_under) / fmt.output_rate;
-  fsc_bin = (int)(fmt.fsc / fmt.output_rate * kLineFFT + 0.5);
-  bw_bins = (int)(500000.0 / fmt.output_rate * kLineFFT + 0.5);
+  fsc_bin = (int)(fmt.fsc / fmt.output_rate * fmt.line_fft + 0.5);
+  bw_bins = (int)(500000.0 / fmt.output_rate * fmt.line_fft + 0.5);
   if (bw_bins < 10) bw_bins = 10;
 }
 
@@ -280,13 +320,14 @@ namespace cuvhs {
 
 void Design::build_cached(const Format& fmt) {
   static std::mutex mu;
-  static std::map<double, Design> cache;
+  static std::map<std::pair<double, int>, Design> cache;
   std::lock_guard<std::mutex> lock(mu);
-  auto it = cache.find(fmt.fs_hz);
+  const std::pair<double, int> key(fmt.fs_hz, fmt.system);
+  auto it = cache.find(key);
   if (it == cache.end()) {
     Design d;
     d.build(fmt);
-    it = cache.emplace(fmt.fs_hz, std::move(d)).first;
+    it = cache.emplace(key, std::move(d)).first;
   }
   *this = it->second;
 }

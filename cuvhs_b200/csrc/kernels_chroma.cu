@@ -21,7 +21,10 @@ namespace cuvhs {
 namespace {
 
 constexpr int kThreadsC = Design::kNc / 16;
-constexpr int kLineWarps = 4;
+// warps per CTA of the line kernel: one line pair per warp, a padded N-point
+// buffer each (NTSC 1024, PAL 2048 points)
+template <int N>
+__host__ __device__ constexpr int line_warps() { return N <= 1024 ? 4 : 2; }
 
 // Two adjacent output blocks ride in the real and imaginary parts of one
 // transform (the kernel is real).  Thread t holds block samples t + T*q.
@@ -100,15 +103,18 @@ __device__ __forceinline__ float het_sample(const ChromaArgs& a, int gl, int c) 
   return v * het;
 }
 
-__global__ void __launch_bounds__(32 * kLineWarps) lines_kernel(ChromaArgs a, int line0, int nlines, int write_output) {
-  __shared__ float2 sm_all[kLineWarps][fft_pad(kLineFFT)];
+template <int N>
+__global__ void __launch_bounds__(32 * line_warps<N>()) lines_kernel(ChromaArgs a, int line0, int nlines,
+                                                                    int write_output) {
+  constexpr int W = line_warps<N>();
+  __shared__ float2 sm_all[W][fft_pad(N)];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float2* sm = sm_all[warp];
-  const int pair = blockIdx.x * kLineWarps + warp;
+  const int pair = blockIdx.x * W + warp;
   const int la = 2 * pair, lb = la + 1;  // relative to line0
   if (la >= nlines) return;               // whole warp leaves together
   const bool has_b = lb < nlines;
-  for (int c = lane; c < kLineFFT; c += 32) {
+  for (int c = lane; c < N; c += 32) {
     float va = 0.0f, vb = 0.0f;
     if (c < a.out_w) {
       va = het_sample(a, line0 + la, c);
@@ -117,32 +123,33 @@ __global__ void __launch_bounds__(32 * kLineWarps) lines_kernel(ChromaArgs a, in
     sm[pidx(c)] = make_float2(va, vb);
   }
   __syncwarp();
-  smem_fft<kLineFFT, 32, false>(sm, a.tw_line);
+  smem_fft<N, 32, false>(sm, a.tw_line);
   const int lo = a.fsc_bin - a.bw_bins, hi = a.fsc_bin + a.bw_bins;
-  const float scale = 1.0f / (float)kLineFFT;
-  for (int k = lane; k < kLineFFT; k += 32) {
-    const int kk = k <= kLineFFT / 2 ? k : kLineFFT - k;
+  const float scale = 1.0f / (float)N;
+  for (int k = lane; k < N; k += 32) {
+    const int kk = k <= N / 2 ? k : N - k;
     const float m = (kk >= lo && kk <= hi) ? scale : 0.0f;
     const float2 x = sm[pidx(k)];
     sm[pidx(k)] = make_float2(x.x * m, x.y * m);
   }
   __syncwarp();
-  smem_fft<kLineFFT, 32, true>(sm, a.tw_line_inv);
+  smem_fft<N, 32, true>(sm, a.tw_line_inv);
   // burst RMS per line -> ACC gain
+  const int bl = a.burst_len;
   float ssa = 0.0f, ssb = 0.0f;
-  for (int i = lane; i < kBurstLen; i += 32) {
+  for (int i = lane; i < bl; i += 32) {
     const float2 v = sm[pidx(a.burst_start + i)];
     ssa += v.x * v.x;
     ssb += v.y * v.y;
-    a.burst[(size_t)(line0 + la) * kBurstLen + i] = v.x;
-    if (has_b) a.burst[(size_t)(line0 + lb) * kBurstLen + i] = v.y;
+    a.burst[(size_t)(line0 + la) * bl + i] = v.x;
+    if (has_b) a.burst[(size_t)(line0 + lb) * bl + i] = v.y;
   }
   for (int off = 16; off > 0; off >>= 1) {
     ssa += __shfl_xor_sync(0xffffffffu, ssa, off);
     ssb += __shfl_xor_sync(0xffffffffu, ssb, off);
   }
   if (!write_output) return;
-  const float rms_a = sqrtf(ssa / (float)kBurstLen), rms_b = sqrtf(ssb / (float)kBurstLen);
+  const float rms_a = sqrtf(ssa / (float)bl), rms_b = sqrtf(ssb / (float)bl);
   const float acc_a = rms_a > 1.0f ? a.burst_abs_ref / rms_a : 0.0f;
   const float acc_b = rms_b > 1.0f ? a.burst_abs_ref / rms_b : 0.0f;
   uint16_t* oa = a.chroma + (size_t)(line0 + la) * a.out_w;
@@ -169,11 +176,11 @@ __global__ void metric_kernel(ChromaArgs a, int field0, int nfields) {
   double acc = 0.0;
   for (int p = lane; p < npairs; p += 32) {
     const int line = f * a.out_h + skip + 2 * p;
-    const float* x = a.burst + (size_t)line * kBurstLen;
-    const float* y = x + kBurstLen;
+    const float* x = a.burst + (size_t)line * a.burst_len;
+    const float* y = x + a.burst_len;
     double s = 0.0;
-    for (int i = 0; i < kBurstLen; i++) s += fabs((double)x[i] + (double)y[i]);
-    acc += s / kBurstLen;
+    for (int i = 0; i < a.burst_len; i++) s += fabs((double)x[i] + (double)y[i]);
+    acc += s / a.burst_len;
   }
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
   if (lane == 0) a.metric[f] = npairs > 0 ? acc / npairs : 1e9;
@@ -197,8 +204,11 @@ void launch_chroma_lines(const ChromaArgs& a, int field0, int nfields, bool writ
   const int nlines = nfields * a.out_h;
   if (nlines <= 0) return;
   const int pairs = (nlines + 1) / 2;
-  lines_kernel<<<(pairs + kLineWarps - 1) / kLineWarps, 32 * kLineWarps, 0, st>>>(a, field0 * a.out_h, nlines,
-                                                                                  write_output ? 1 : 0);
+  auto go = [&](auto kernel, int warps) {
+    kernel<<<(pairs + warps - 1) / warps, 32 * warps, 0, st>>>(a, field0 * a.out_h, nlines, write_output ? 1 : 0);
+  };
+  if (a.line_fft == 2048) go(lines_kernel<2048>, line_warps<2048>());
+  else go(lines_kernel<1024>, line_warps<1024>());
 }
 
 void launch_burst_metric(const ChromaArgs& a, int field0, int nfields, cudaStream_t st) {

@@ -30,7 +30,6 @@ namespace {
 
 constexpr int kThreadsD = 256;       // fused kernel and class kernel
 constexpr int kThreadsScan = 512;    // two-pass scan kernel
-constexpr int kMaxBlocks = 49152;    // 16-sample blocks per field (class bytes)
 constexpr int kMaxEvents = 2048;
 constexpr int kStage = kThreadsD * 16;  // envelope samples one class CTA stages
 
@@ -145,7 +144,7 @@ __device__ void conceal(const DropoutArgs& a, int f, int n, int lane, bool luma,
 // ------------------------------------------------------------------ fused form
 
 __global__ void __launch_bounds__(kThreadsD) dropout_kernel(DropoutArgs a) {
-  extern __shared__ unsigned char cls[];  // [kMaxBlocks]
+  extern __shared__ unsigned char cls[];  // [a.max_blocks]
   __shared__ int last_cls[kThreadsD];
   __shared__ int state_in[kThreadsD];
   __shared__ int ev_count[kThreadsD];
@@ -165,7 +164,7 @@ __global__ void __launch_bounds__(kThreadsD) dropout_kernel(DropoutArgs a) {
     if (tid == 0) a.do_count[f] = 0;
     return;
   }
-  const int nb = min((s1 - s0 + 15) / 16, kMaxBlocks);
+  const int nb = min((s1 - s0 + 15) / 16, a.max_blocks);
   const double down = down_s, up = down * 1.25;
   // 1. classify blocks
   for (int b = tid; b < nb; b += kThreadsD) {
@@ -220,7 +219,7 @@ __global__ void __launch_bounds__(kThreadsD) dropout_kernel(DropoutArgs a) {
 
 // --------------------------------------------------------------- two-pass form
 
-// grid (ceil(kMaxBlocks / kThreadsD), fields): CTA x classifies blocks
+// grid (ceil(max_blocks / kThreadsD), fields): CTA x classifies blocks
 // [x*256, x*256 + 256) of field y.  The 4096 envelope samples behind them are
 // staged with coalesced loads into rows of 17 floats (conflict-free column
 // reads), then each thread sums its row in sample order.
@@ -230,7 +229,7 @@ __global__ void __launch_bounds__(kThreadsD) dropout_class_kernel(DropoutArgs a)
   const int f = blockIdx.y, tid = threadIdx.x;
   int s0, s1;
   active_range(a, f, s0, s1);
-  const int nb = min((s1 - s0 + 15) / 16, kMaxBlocks);
+  const int nb = min((s1 - s0 + 15) / 16, a.max_blocks);
   const int b_first = blockIdx.x * kThreadsD;
   if (s1 <= s0 || b_first >= nb) return;  // whole CTA leaves together
   if (tid == 0) down_s = down_threshold(a, f);
@@ -245,7 +244,7 @@ __global__ void __launch_bounds__(kThreadsD) dropout_class_kernel(DropoutArgs a)
   double sum = 0.0;
   for (int i = 0; i < n; i++) sum += (double)stage[tid * 17 + i];
   const double down = down_s;
-  a.cls[(size_t)f * kMaxBlocks + b] = block_class(sum, n, down, down * 1.25);
+  a.cls[(size_t)f * a.max_blocks + b] = block_class(sum, n, down, down * 1.25);
 }
 
 // Block-wide exclusive scans over kThreadsScan threads (warp shuffles, then
@@ -306,7 +305,7 @@ __device__ __forceinline__ int block_excl_last(int v, int* wsh) {
 // hysteresis scan, event list, mapping and luma concealment (chroma is
 // concealed by dropout_chroma_kernel once the chroma planes are final).
 __global__ void __launch_bounds__(kThreadsScan) dropout_scan_kernel(DropoutArgs a) {
-  extern __shared__ uint4 cls4[];  // [kMaxBlocks / 16]
+  extern __shared__ uint4 cls4[];  // [a.max_blocks / 16]
   __shared__ int wsh[32];
   __shared__ int events[kMaxEvents];
   __shared__ int rf_s[kMaxRfDropouts], rf_e[kMaxRfDropouts];
@@ -319,8 +318,8 @@ __global__ void __launch_bounds__(kThreadsScan) dropout_scan_kernel(DropoutArgs 
     if (tid == 0) a.do_count[f] = 0;
     return;  // whole CTA leaves together
   }
-  const int nb = min((s1 - s0 + 15) / 16, kMaxBlocks);
-  const uint4* src = reinterpret_cast<const uint4*>(a.cls + (size_t)f * kMaxBlocks);
+  const int nb = min((s1 - s0 + 15) / 16, a.max_blocks);
+  const uint4* src = reinterpret_cast<const uint4*>(a.cls + (size_t)f * a.max_blocks);
   for (int i = tid; i < (nb + 15) / 16; i += kThreadsScan) cls4[i] = src[i];
   __syncthreads();
   const int per = (nb + kThreadsScan - 1) / kThreadsScan;
@@ -360,18 +359,18 @@ __global__ void dropout_chroma_kernel(DropoutArgs a) {
 
 void launch_dropouts(const DropoutArgs& a, cudaStream_t st) {
   if (a.fields <= 0) return;
-  const size_t smem = kMaxBlocks;
+  const size_t smem = (size_t)a.max_blocks;
   cudaFuncSetAttribute(dropout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dropout_kernel<<<a.fields, kThreadsD, smem, st>>>(a);
 }
 
-size_t dropout_class_bytes_per_field() { return kMaxBlocks; }
+size_t dropout_class_bytes_per_field(int spp) { return (size_t)(((spp + 15) / 16 + 15) / 16 * 16); }
 
 void launch_dropouts_two_pass(const DropoutArgs& a, cudaStream_t st) {
   if (a.fields <= 0) return;
-  dim3 grid((kMaxBlocks + kThreadsD - 1) / kThreadsD, a.fields);
+  dim3 grid((a.max_blocks + kThreadsD - 1) / kThreadsD, a.fields);
   dropout_class_kernel<<<grid, kThreadsD, 0, st>>>(a);
-  const size_t smem = kMaxBlocks;
+  const size_t smem = (size_t)a.max_blocks;
   cudaFuncSetAttribute(dropout_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dropout_scan_kernel<<<a.fields, kThreadsScan, smem, st>>>(a);
 }

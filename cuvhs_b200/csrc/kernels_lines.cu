@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(kLumaThreads) luma_kernel(LineArgs a) {
   const int field = grow / H, row = grow % H;
   uint16_t* out = a.luma + (size_t)grow * W;
   if (row + 1 >= a.lines_per_frame) {
-    for (int col = threadIdx.x; col < W; col += kLumaThreads) out[col] = 1024;
+    for (int col = threadIdx.x; col < W; col += kLumaThreads) out[col] = a.oob_value;
     return;
   }
   const double a0 = a.ll[(size_t)field * a.lines_per_frame + row];
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kLumaThreads) luma_kernel(LineArgs a) {
   for (int col = threadIdx.x; col < W; col += kLumaThreads) {
     const double coord = a0 + __ldg(&a.col_frac[col]) * span;
     const int ci = (int)coord;
-    uint16_t o = 1024;
+    uint16_t o = a.oob_value;
     if (ci >= 1 && (long long)ci + 2 < a.total) {
       const float x = (float)(coord - (double)ci);
       const float p0 = __ldg(&a.video[ci - 1]), p1 = __ldg(&a.video[ci]);

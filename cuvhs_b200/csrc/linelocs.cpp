@@ -19,6 +19,24 @@ struct Windows {  // adaptive pulse-width classes (pipeline.cu:450-477)
 
 bool within(double v, double lo, double hi) { return v >= lo && v <= hi; }
 
+// Spacings (lines) of the last hsync -> first EQ and last EQ -> first hsync
+// around this field's blanking interval, then around the next one, for a
+// first (or second) field of the system (pipeline.cu:704-716).
+const double* field_pattern(const Format& fmt, bool first) {
+  static const double ntsc_first[4] = {1, 0.5, 0.5, 1}, ntsc_second[4] = {0.5, 1, 1, 0.5};
+  static const double pal_first[4] = {0.5, 0.5, 1, 1}, pal_second[4] = {1, 1, 0.5, 0.5};
+  if (fmt.system == kPal) return first ? pal_first : pal_second;
+  return first ? ntsc_first : ntsc_second;
+}
+
+// Field length (lines) from the previous field's first hsync to this one's:
+// NTSC counts the previous field's lines, PAL the current one's (pipeline.cu:811).
+double predicted_field_lines(const Format& fmt, bool first) {
+  const int cur = first ? fmt.field_lines_first : fmt.field_lines_second;
+  const int prev = first ? fmt.field_lines_second : fmt.field_lines_first;
+  return fmt.system == kPal ? cur : prev;
+}
+
 // Quantise a line count to 0.5-line steps, then to 0.1 (pipeline.cu:436-438).
 double half_line_round(double lines) { return std::round(0.5 * std::round(lines / 0.5) * 10.0) / 10.0; }
 
@@ -249,8 +267,8 @@ BlankingScan scan_blanking(const std::vector<ValidPulse>& v, double mll, const F
     }
     prev = i;
   }
-  static const double first_pat[4] = {1, 0.5, 0.5, 1};
-  static const double second_pat[4] = {0.5, 1, 1, 0.5};
+  const double* first_pat = field_pattern(fmt, true);
+  const double* second_pat = field_pattern(fmt, false);
   for (int i = 0; i < 4; i++) {
     if (s.order_len[i] == first_pat[i]) {
       s.agree += 1.0;
@@ -299,12 +317,10 @@ AnchorFit fit_anchor(const BlankingScan& s, const std::vector<ValidPulse>& v, do
   if (v.empty() || mll <= 0.0) return out;
   const int lines[2] = {fmt.field_lines_first, fmt.field_lines_second};
   const double tol_lines = 0.5;
-  static const double first_pat[4] = {1, 0.5, 0.5, 1};
-  static const double second_pat[4] = {0.5, 1, 1, 0.5};
   const double section = fmt.num_eq_pulses / 2.0;
   const double cur_lines = first ? lines[0] : lines[1];
-  const double prev_lines = first ? lines[1] : lines[0];
-  const double* pat = first ? first_pat : second_pat;
+  const double pred_lines = predicted_field_lines(fmt, first);
+  const double* pat = field_pattern(fmt, first);
   double vb_line[8];
   vb_line[0] = 0.0 + pat[0];
   vb_line[1] = vb_line[0] + section;
@@ -350,7 +366,7 @@ AnchorFit fit_anchor(const BlankingScan& s, const std::vector<ValidPulse>& v, do
     cnt = b_cnt;
     off = b_off;
   }
-  const int predicted = (int)std::llround((prev_off_lines + prev_lines + prev_loc / mll) * mll);
+  const int predicted = (int)std::llround((prev_off_lines + pred_lines + prev_loc / mll) * mll);
   if (cnt == 0 && prev_loc > 0.0) {
     double p = (prev_diff <= 0.5 && prev_diff >= -0.5) ? predicted + mll * prev_diff : (double)predicted;
     if (p <= 0.0) p = (double)v.front().p.start;
@@ -387,9 +403,7 @@ AnchorFit fit_anchor(const BlankingScan& s, const std::vector<ValidPulse>& v, do
 // The carried hsync_diff after a fit that used no prediction.
 double hsync_diff_after(const AnchorFit& f, const Format& fmt, bool first, double mll, double prev_off_lines,
                         double prev_loc) {
-  const int lines[2] = {fmt.field_lines_first, fmt.field_lines_second};
-  const double prev_lines = first ? lines[1] : lines[0];
-  const int predicted = (int)std::llround((prev_off_lines + prev_lines + prev_loc / mll) * mll);
+  const int predicted = (int)std::llround((prev_off_lines + predicted_field_lines(fmt, first) + prev_loc / mll) * mll);
   return (f.loc_round - predicted) / mll;
 }
 

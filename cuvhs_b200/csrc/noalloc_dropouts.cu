@@ -64,6 +64,11 @@ extern "C" cuvhs_status cuvhs_dropouts_noalloc(const float* d_envelope, const do
       fields < 1 || tile_stride < 1)
     return CUVHS_ERR_INVALID_ARGUMENT;
   const long long per_tile = ((long long)tile_stride + kPartialSamples - 1) / kPartialSamples;
+  if (dropout_class_bytes_per_field(tile_stride) > 200 * 1024) {  // the per-field classes live in shared memory
+    fprintf(stderr, "cuvhs_dropouts_noalloc: tile_stride %d is above the %d samples one call handles\n",
+            tile_stride, 200 * 1024 * 16);
+    return CUVHS_ERR_CAPACITY;
+  }
   if ((long long)fields * per_tile > CUVHS_NOALLOC_MAX_PARTIALS) {
     fprintf(stderr,
             "cuvhs_dropouts_noalloc: %d fields of %d samples need %lld envelope partial sums; "
@@ -115,6 +120,7 @@ extern "C" cuvhs_status cuvhs_dropouts_noalloc(const float* d_envelope, const do
   a.do_lines = d_lines;
   a.do_starts = d_startx;
   a.do_ends = d_endx;
+  a.max_blocks = (int)dropout_class_bytes_per_field(tile_stride);
   launch_dropouts(a, st);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

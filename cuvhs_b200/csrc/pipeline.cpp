@@ -142,13 +142,18 @@ void Context::release() {
 
 bool Context::init(const cuvhs_config& c) {
   cfg = c;
-  if (c.system != 0) {
-    err = "only NTSC is supported";
-    status = CUVHS_ERR_UNSUPPORTED;
-    return false;
-  }
   if (!(c.sample_rate_mhz >= 8.0 && c.sample_rate_mhz <= 100.0)) {
     err = "sample rate out of range (8-100 MHz)";
+    status = CUVHS_ERR_INVALID_ARGUMENT;
+    return false;
+  }
+  if (c.system != kNtsc && c.system != kPal) {
+    err = "system must be 0 (NTSC) or 1 (PAL)";
+    status = CUVHS_ERR_INVALID_ARGUMENT;
+    return false;
+  }
+  if (c.input_format < 0 || c.input_format > 2) {
+    err = "input_format must be 0 (u8), 1 (s16) or 2 (u16)";
     status = CUVHS_ERR_INVALID_ARGUMENT;
     return false;
   }
@@ -177,21 +182,17 @@ bool Context::init(const cuvhs_config& c) {
     return false;
   }
   cudaSetDevice(device);
-  if (c.input_format < 0 || c.input_format > 2) {
-    err = "input_format must be 0 (u8), 1 (s16) or 2 (u16)";
-    status = CUVHS_ERR_INVALID_ARGUMENT;
-    return false;
-  }
   in_fmt = c.input_format;
   bps = in_fmt == 0 ? 1 : 2;
   dc_correct = c.dc_correct != 0;
-  fmt.init(c.sample_rate_mhz);
+  fmt.init(c.sample_rate_mhz, c.system);
   des.build_cached(fmt);
   spp = fmt.spp;
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
-  const size_t per_field = (size_t)spp * (2 * bps + 4 * 5) + (size_t)263 * 910 * 8 + 263 * kBurstLen * 4 + 65536 +
-                           dropout_class_bytes_per_field();
+  const size_t field_px = (size_t)fmt.output_line_len * fmt.output_field_lines;
+  const size_t per_field = (size_t)spp * (2 * bps + 4 * 5) + field_px * 8 +
+                           (size_t)fmt.output_field_lines * kMaxBurstLen * 4 + 65536 + dropout_class_bytes_per_field(spp);
   int b = c.batch_fields;
   if (b <= 0) {
     b = (int)std::min<size_t>((size_t)(free_b * 0.5) / per_field, 2048);
@@ -246,13 +247,13 @@ bool Context::init(const cuvhs_config& c) {
   }
   d_luma = d_luma_set[0];
   d_chroma = d_chroma_set[0];
-  d_burst = A((float*)nullptr, (size_t)batch * fmt.output_field_lines * kBurstLen);
+  d_burst = A((float*)nullptr, (size_t)batch * fmt.output_field_lines * fmt.burst_len);
   d_track = A((int*)nullptr, batch);
   d_do_count = A((int*)nullptr, batch);
   d_do_lines = A((int*)nullptr, (size_t)batch * kMaxDropouts);
   d_do_starts = A((int*)nullptr, (size_t)batch * kMaxDropouts);
   d_do_ends = A((int*)nullptr, (size_t)batch * kMaxDropouts);
-  d_do_cls = A((unsigned char*)nullptr, (size_t)batch * dropout_class_bytes_per_field());
+  d_do_cls = A((unsigned char*)nullptr, (size_t)batch * dropout_class_bytes_per_field(spp));
   d_ga = A((float2*)nullptr, des.ga.size());
   d_gb = A((float2*)nullptr, des.gb.size());
   d_gc = A((float*)nullptr, des.gc.size());
@@ -290,7 +291,7 @@ bool Context::init(const cuvhs_config& c) {
   hp_ll = H((double*)nullptr, (size_t)batch * fmt.lines_per_frame);
   hp_track = H((int*)nullptr, batch);
   hp_trial = H((int*)nullptr, 2);
-  hp_burst = H((float*)nullptr, (size_t)2 * fmt.output_field_lines * kBurstLen);
+  hp_burst = H((float*)nullptr, (size_t)2 * fmt.output_field_lines * fmt.burst_len);
   {
     void* p = nullptr;
     if (cudaHostAlloc(&p, std::max(batch, 1) * sizeof(double), cudaHostAllocMapped) != cudaSuccess ||
@@ -407,16 +408,16 @@ void Context::reset_state() {
 
 // Host burst-cancellation metric over one field's burst windows (lines 16..245
 // in pairs), as the track detector measures it (chroma_decode.cu:383-411).
-static double host_burst_metric(const float* b, int H) {
+static double host_burst_metric(const float* b, int H, int bl) {
   const int skip = 16;
   double total = 0.0;
   int count = 0;
   for (int line = skip; line < H - skip - 1; line += 2) {
-    const float* x = b + (size_t)line * kBurstLen;
-    const float* y = x + kBurstLen;
+    const float* x = b + (size_t)line * bl;
+    const float* y = x + bl;
     double s = 0.0;
-    for (int i = 0; i < kBurstLen; i++) s += std::fabs((double)x[i] + (double)y[i]);
-    total += s / kBurstLen;
+    for (int i = 0; i < bl; i++) s += std::fabs((double)x[i] + (double)y[i]);
+    total += s / bl;
     count++;
   }
   return count > 0 ? total / count : 1e9;
@@ -429,9 +430,9 @@ static double host_burst_phase(const float* b, int H, const Format& fmt) {
   const double PI = 3.14159265358979323846;
   double It = 0.0, Qt = 0.0;
   for (int line = skip; line < H - skip; line++) {
-    const float* x = b + (size_t)line * kBurstLen;
+    const float* x = b + (size_t)line * fmt.burst_len;
     double I = 0.0, Q = 0.0;
-    for (int i = 0; i < kBurstLen; i++) {
+    for (int i = 0; i < fmt.burst_len; i++) {
       const double v = x[i];
       const double t = 2.0 * PI * fmt.fsc / fmt.output_rate * (double)(fmt.burst_start + i);
       I += v * std::cos(t);
@@ -506,6 +507,8 @@ ChromaArgs Context::chroma_args(const uint8_t* raw, int n_read, const float* dc,
   ca.fsc_bin = des.fsc_bin;
   ca.bw_bins = des.bw_bins;
   ca.burst_start = fmt.burst_start;
+  ca.burst_len = fmt.burst_len;
+  ca.line_fft = fmt.line_fft;
   ca.out_w = fmt.output_line_len;
   ca.out_h = fmt.output_field_lines;
   ca.lines_per_frame = fmt.lines_per_frame;
@@ -536,6 +539,7 @@ LineArgs Context::line_args(int P) const {
   la.luma_gain = (float)(fmt.output_scale / fmt.hz_ire);
   la.luma_offset = (float)(-fmt.vsync_ire * fmt.output_scale + fmt.output_zero);
   la.col_frac = d_col_frac;
+  la.oob_value = (uint16_t)fmt.output_zero;
   return la;
 }
 
@@ -558,6 +562,7 @@ DropoutArgs Context::dropout_args(int P) const {
   dd.do_starts = d_do_starts;
   dd.do_ends = d_do_ends;
   dd.cls = d_do_cls;
+  dd.max_blocks = (int)dropout_class_bytes_per_field(spp);
   return dd;
 }
 
@@ -674,7 +679,7 @@ bool Context::chroma_fields(ChromaArgs& ca, int P) {
     // Track and burst phase from field 0 (chroma_decode.cu:684-743): both
     // trial tracks in one round trip; the detected track's burst windows are
     // the ones the phase measurement reads.
-    const size_t nb = (size_t)H * kBurstLen;
+    const size_t nb = (size_t)H * fmt.burst_len;
     for (int t = 0; t < 2; t++) {
       cudaMemcpyAsync(d_track, hp_trial + t, sizeof(int), cudaMemcpyHostToDevice, stream);
       chroma_pass(0, 1, false);
@@ -684,7 +689,7 @@ bool Context::chroma_fields(ChromaArgs& ca, int P) {
     t_host = host_clock();
     if (!wait_host_event("chroma track detect")) return false;
     host_phase(kHostChromaWait, t_host);
-    const double m0 = host_burst_metric(hp_burst, H), m1 = host_burst_metric(hp_burst + nb, H);
+    const double m0 = host_burst_metric(hp_burst, H, fmt.burst_len), m1 = host_burst_metric(hp_burst + nb, H, fmt.burst_len);
     det_track = (m1 < m0) ? 1 : 0;
     thr = (det_track ? m1 : m0) * 4.0;
     const double ph = host_burst_phase(hp_burst + det_track * nb, H, fmt);

@@ -1,9 +1,11 @@
-// Seeded synthetic NTSC VHS RF generator.
+// Seeded synthetic NTSC or PAL VHS RF generator.
 //
 // Produces an 8-bit RF capture of the kind cuVHS decodes: an FM luma carrier
-// (sync tip 3.4 MHz, white 4.4 MHz, on the IRE map of src/format/video_format.cpp:113-116
-// of the reference) carrying NTSC timing (hsync 4.7 us, EQ 2.3 us, broad pulses
-// with 4.7 us serrations, burst 5.3-7.8 us), pre-emphasised with the same
+// (NTSC: sync tip 3.4 MHz, white 4.4 MHz; PAL: 3.8 / 4.8 MHz; the IRE maps of
+// src/format/video_format.cpp:23-104 of the reference) carrying the system's
+// timing (hsync 4.7 us; NTSC 6 + 6 + 6 EQ / broad / EQ half-line pulses of
+// 2.3 us and a 5.3-7.8 us burst, PAL 5 + 5 + 5 of 2.35 us and a 5.6-7.85 us
+// burst; broad pulses with 4.7 us serrations), pre-emphasised with the same
 // high-shelf biquad the decoder inverts (src/pipeline/fm_demod.cu:310-314), plus
 // a colour-under chroma signal at 40 fH with the VHS +/-90 degree per-line
 // rotation that src/pipeline/chroma_decode.cu:143-148 undoes.  Noise, a bounded
@@ -22,11 +24,76 @@
 namespace {
 
 constexpr double kPi = 3.14159265358979323846;
-constexpr double kLineRate = 15734.264;
-constexpr double kFsc = 3579545.0;
-constexpr double kChromaUnder = (525.0 * (30.0 / 1.001)) * 40.0;
-constexpr double kHzIre = 1e6 / 140.0;
-constexpr double kIre0 = 4.4e6 - kHzIre * 100.0;
+
+// Timing and levels of the video system.
+struct Timing {
+  bool pal;
+  double line_rate;
+  double chroma_under;  // colour-under carrier, Hz
+  double hz_ire, ire0, sync_ire;
+  int frame_lines;      // 525 / 625: field 2 starts at half-line frame_lines
+  int eq_pulses;        // half-line pulses per EQ or broad group (6 / 5)
+  double eq_us, half_line_us;
+  double burst_a, burst_b;  // burst window, us after the line's sync
+  int burst_line;           // first field line with a burst
+  int pic_first, pic_last;  // field lines with picture
+  double pic_a, pic_b;      // picture window, us
+  int bars_end, sine_end;   // field lines of the colour bars and the sine pattern
+  int headswitch_lines[2];  // frame lines of the head-switch jumps (6 lines before each vertical interval)
+  double start_lines;       // range of the seeded start line within a frame
+};
+
+Timing timing(int system) {
+  Timing t;
+  if (system == 1) {
+    t.pal = true;
+    t.line_rate = 15625.0;
+    t.chroma_under = ((625.0 * 25.0) * 40.0) + 1953.0;
+    t.sync_ire = -0.3 * (100.0 / 0.7);
+    t.hz_ire = 1e6 / (100.0 - t.sync_ire);
+    t.ire0 = 4.8e6 - t.hz_ire * 100.0;
+    t.frame_lines = 625;
+    t.eq_pulses = 5;
+    t.eq_us = 2.35;
+    t.half_line_us = 32.0;
+    t.burst_a = 5.6;
+    t.burst_b = 7.85;
+    t.burst_line = 8;
+    t.pic_first = 23;
+    t.pic_last = 310;
+    t.pic_a = 10.5;
+    t.pic_b = 62.0;
+    t.bars_end = 200;
+    t.sine_end = 240;
+    t.headswitch_lines[0] = 619;
+    t.headswitch_lines[1] = 306;
+    t.start_lines = 580.0;
+  } else {
+    t.pal = false;
+    t.line_rate = 15734.264;
+    t.chroma_under = (525.0 * (30.0 / 1.001)) * 40.0;
+    t.hz_ire = 1e6 / 140.0;
+    t.ire0 = 4.4e6 - t.hz_ire * 100.0;
+    t.sync_ire = -40.0;
+    t.frame_lines = 525;
+    t.eq_pulses = 6;
+    t.eq_us = 2.3;
+    t.half_line_us = 31.777;
+    t.burst_a = 5.3;
+    t.burst_b = 7.8;
+    t.burst_line = 9;
+    t.pic_first = 20;
+    t.pic_last = 262;
+    t.pic_a = 9.4;
+    t.pic_b = 62.4;
+    t.bars_end = 170;
+    t.sine_end = 200;
+    t.headswitch_lines[0] = 519;
+    t.headswitch_lines[1] = 256;
+    t.start_lines = 480.0;
+  }
+  return t;
+}
 
 // SplitMix64: counter-based stream so every block of samples has its own
 // reproducible generator.
@@ -95,60 +162,67 @@ struct LineGeom {
 // Composite luma (IRE) and chroma components (u, v in IRE) at program time
 // `tau` (samples) measured from the start of frame-aligned line `lam`.
 struct Content {
+  Timing tm;
   double spl;      // nominal samples per line
   double fs;
   Bar bars[7];
-  int n_frame_lines;
   double us;       // samples per microsecond
 
   // du: delay of the picture and burst against the line's sync, samples
   void eval(long long lam, double u, double du, double* ire, double* cu, double* cv) const {
     // Frame-relative line and half-line.
-    long long fl = lam % 525;
-    if (fl < 0) fl += 525;
+    const int FL = tm.frame_lines;
+    long long fl = lam % FL;
+    if (fl < 0) fl += FL;
     double half = spl * 0.5;
     int hidx = (int)(2 * fl + (u >= half ? 1 : 0));
     double v = (u >= half) ? u - half : u;
     double t_us = u / us;
     double tp_us = (u - du) / us;  // picture and burst time
     double tv_us = v / us;
-    long long frame = (lam >= 0 ? lam : lam - 524) / 525;
+    long long frame = (lam >= 0 ? lam : lam - (FL - 1)) / FL;
     // Field-relative line numbering (field 1 starts at frame line 0, field 2 at
-    // half-line 525, i.e. mid line 262).
-    bool field2 = (hidx >= 525);
-    double field_line_d = field2 ? (hidx - 525) * 0.5 : hidx * 0.5;
+    // half-line FL, i.e. the middle of line (FL - 1) / 2).
+    bool field2 = (hidx >= FL);
+    double field_line_d = field2 ? (hidx - FL) * 0.5 : hidx * 0.5;
     long long field_index = frame * 2 + (field2 ? 1 : 0);
 
     const double edge = 0.2;  // us, sync edge width
     double level = 0.0;       // blanking
     double cu_ = 0.0, cv_ = 0.0;
-    int rel = field2 ? hidx - 525 : hidx;  // half-lines since the field's first EQ
-    bool vert = rel >= 0 && rel < 18;
+    int rel = field2 ? hidx - FL : hidx;  // half-lines since the field's first EQ
+    const int E = tm.eq_pulses;
+    bool vert = rel >= 0 && rel < 3 * E;
     if (vert) {
-      bool broad = rel >= 6 && rel < 12;
-      double w = broad ? (31.777 - 4.7) : 2.3;
-      level = -40.0 * window_level(tv_us, 0.0, w, edge);
+      bool broad = rel >= E && rel < 2 * E;
+      double w = broad ? (tm.half_line_us - 4.7) : tm.eq_us;
+      level = tm.sync_ire * window_level(tv_us, 0.0, w, edge);
       // The half-line slot before the first EQ (second half of the previous
       // line) is handled by the previous line's eval; nothing else here.
     } else {
       // Full line with hsync at its start (only even half-lines start lines;
       // odd half-lines are second halves of normal lines).
       double sync = window_level(t_us, 0.0, 4.7, edge);
-      // Guard the very start of the field-2 vertical interval: the second half
-      // of frame line 262 belongs to the EQ train (handled above).
-      level = -40.0 * sync;
-      // Colour burst on lines after the vertical interval.
+      level = tm.sync_ire * sync;
+      // Colour burst on lines after the vertical interval: NTSC at 180
+      // degrees (-U), PAL swinging +/-45 degrees about it with the V switch.
       int fline = (int)field_line_d;
-      if (fline >= 9) {
-        double bw = window_level(tp_us, 5.3, 7.8, 0.3);
-        cu_ += -20.0 * bw;
+      const double vsw = (tm.pal && (fline & 1)) ? -1.0 : 1.0;
+      if (fline >= tm.burst_line) {
+        double bw = window_level(tp_us, tm.burst_a, tm.burst_b, 0.3);
+        if (tm.pal) {
+          cu_ += -20.0 * 0.70710678118654752 * bw;
+          cv_ += vsw * 20.0 * 0.70710678118654752 * bw;
+        } else {
+          cu_ += -20.0 * bw;
+        }
       }
-      if (fline >= 20 && fline < 262) {
-        double a0 = 9.4, a1 = 62.4;
+      if (fline >= tm.pic_first && fline < tm.pic_last) {
+        double a0 = tm.pic_a, a1 = tm.pic_b;
         double act = window_level(tp_us, a0, a1, 0.25);
         double x = (tp_us - a0) / (a1 - a0);
         double yl = 7.5, uu = 0.0, vv = 0.0;
-        if (fline < 170) {
+        if (fline < tm.bars_end) {
           // bars with raised-cosine transitions
           double pos = x * 7.0;
           int bi = (int)std::floor(pos);
@@ -162,8 +236,8 @@ struct Content {
           double wl = smoothstep01((0.03 - frac) / 0.06);
           yl = b0.ire * (1.0 - wr - wl) + b1.ire * wr + bm.ire * wl;
           uu = b0.u * (1.0 - wr - wl) + b1.u * wr + bm.u * wl;
-          vv = b0.v * (1.0 - wr - wl) + b1.v * wr + bm.v * wl;
-        } else if (fline < 200) {
+          vv = vsw * (b0.v * (1.0 - wr - wl) + b1.v * wr + bm.v * wl);
+        } else if (fline < tm.sine_end) {
           yl = 7.5 + 45.0 * (1.0 + std::sin(2.0 * kPi * (2.0 * x)));
         } else {
           // moving triangle ramp
@@ -224,11 +298,12 @@ void preemphasis(const cuvhs_synth_params* p, double b[3], double a[3]) {
 // (seeded start phase, per-line timebase random walk, speed drift, head
 // switch jumps).
 void line_table(const cuvhs_synth_params* p, size_t n, long long& lam0_out, std::vector<double>& r) {
+  const Timing tm = timing(p->system);
   const double fs = p->sample_rate_hz;
-  const double spl = fs / kLineRate;
+  const double spl = fs / tm.line_rate;
   SplitMix master(mix_seed(p->seed, 0x5EED));
   // Start position: seeded phase within the first frame, so the file starts mid-field.
-  double start_line = p->start_line >= 0 ? p->start_line : 20.0 + 480.0 * master.uniform();
+  double start_line = p->start_line >= 0 ? p->start_line : 20.0 + tm.start_lines * master.uniform();
   long long lam0 = (long long)std::floor(start_line);
   double u0 = (start_line - (double)lam0) * spl;
 
@@ -256,8 +331,8 @@ void line_table(const cuvhs_synth_params* p, size_t n, long long& lam0_out, std:
       double len = spl * speed + (delta - prev_delta);
       prev_delta = delta;
       // head switch: a time jump 6 lines before each field's vertical interval
-      long long fl = lam % 525;
-      if (p->headswitch_max > 0 && (fl == 519 || fl == 256)) {
+      long long fl = lam % tm.frame_lines;
+      if (p->headswitch_max > 0 && (fl == tm.headswitch_lines[0] || fl == tm.headswitch_lines[1])) {
         int span = std::max(0, p->headswitch_max - p->headswitch_min);
         int jump = p->headswitch_min + (int)(jr.uniform() * (span + 1));
         len += (double)jump;
@@ -311,18 +386,19 @@ extern "C" void cuvhs_synth_default_params(cuvhs_synth_params* p) {
 }
 
 extern "C" long long cuvhs_synth_length(const cuvhs_synth_params* p) {
-  double spl = p->sample_rate_hz / kLineRate;
-  double lines = p->n_fields * 262.5 + (double)p->tail_lines;
-  double lead = p->start_line >= 0 ? 0.0 : 0.0;
-  (void)lead;
+  const Timing tm = timing(p->system);
+  double spl = p->sample_rate_hz / tm.line_rate;
+  double lines = p->n_fields * (tm.frame_lines * 0.5) + (double)p->tail_lines;
   return (long long)std::floor(lines * spl);
 }
 
 extern "C" int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long long n_out) {
   if (!p || !out || n_out <= 0) return -1;
   if (!(p->sample_rate_hz > 4e6)) return -2;
+  if (p->system != 0 && p->system != 1) return -3;
+  const Timing tm = timing(p->system);
   const double fs = p->sample_rate_hz;
-  const double spl = fs / kLineRate;
+  const double spl = fs / tm.line_rate;
   const size_t n = (size_t)n_out;
   int threads = p->threads > 0 ? p->threads : (int)std::max(1u, std::thread::hardware_concurrency());
 
@@ -347,6 +423,7 @@ extern "C" int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long 
   }
 
   Content content;
+  content.tm = tm;
   content.spl = spl;
   content.fs = fs;
   content.us = fs * 1e-6;
@@ -370,15 +447,16 @@ extern "C" int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long 
       content.eval(lam, u, du, &y, &cu, &cv);
       ire[i] = (float)y;
       // colour-under: rotation by +/-90 degrees per line, alternating by field track
-      long long fl = lam % 525;
-      bool field2 = (2 * fl + (u >= spl * 0.5 ? 1 : 0)) >= 525;
-      long long field_index = (lam / 525) * 2 + (field2 ? 1 : 0);
-      long long field_line = field2 ? fl - 262 : fl;
+      const int FL = tm.frame_lines;
+      long long fl = lam % FL;
+      bool field2 = (2 * fl + (u >= spl * 0.5 ? 1 : 0)) >= FL;
+      long long field_index = (lam / FL) * 2 + (field2 ? 1 : 0);
+      long long field_line = field2 ? fl - (FL - 1) / 2 : fl;
       int track = (int)((field_index + p->first_track) & 1);
       int rot = track ? 1 : 3;
       int q = (int)(((field_line * rot) % 4 + 4) % 4);
       // the picture delay moves the colour-under carrier with the picture
-      double theta = 2.0 * kPi * std::fmod(kChromaUnder * ((double)i - du) / fs, 1.0) + q * (kPi * 0.5) +
+      double theta = 2.0 * kPi * std::fmod(tm.chroma_under * ((double)i - du) / fs, 1.0) + q * (kPi * 0.5) +
                      line_phase(p, lam);
       chroma[i] = (float)(cu * std::sin(theta) + cv * std::cos(theta));
     }
@@ -391,8 +469,8 @@ extern "C" int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long 
     double x1 = ire[0], x2 = ire[0];
     double y1 = ire[0], y2 = ire[0];  // the shelf's DC gain is 1
     double phase = 0.0;
-    const double dev = p->deviation_scale * kHzIre;
-    const double fc = kIre0 + p->carrier_offset_hz;
+    const double dev = p->deviation_scale * tm.hz_ire;
+    const double fc = tm.ire0 + p->carrier_offset_hz;
     for (size_t i = 0; i < n; i++) {
       double x0 = ire[i];
       double y0 = b[0] * x0 + b[1] * x1 + b[2] * x2 - a[1] * y1 - a[2] * y2;

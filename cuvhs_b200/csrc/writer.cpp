@@ -30,8 +30,10 @@ std::string tbc_json(const Format& fmt, const cuvhs_field_info* fields, size_t n
   s.reserve(256 + n * 200);
   const double black = (0.0 - fmt.vsync_ire) * fmt.output_scale + fmt.output_zero;
   const double white = (100.0 - fmt.vsync_ire) * fmt.output_scale + fmt.output_zero;
+  const bool pal = fmt.system == kPal;
   s += "{\n  \"videoParameters\": {\n";
-  s += "    \"system\": \"NTSC\",\n    \"isSubcarrierLocked\": false,\n    \"isSourcePal\": false,\n";
+  appendf(s, "    \"system\": \"%s\",\n    \"isSubcarrierLocked\": false,\n    \"isSourcePal\": %s,\n",
+          pal ? "PAL" : "NTSC", pal ? "true" : "false");
   appendf(s, "    \"numberOfSequentialFields\": %d,\n", (int)n);
   appendf(s, "    \"black16bIre\": %.1f,\n", black);
   appendf(s, "    \"white16bIre\": %.1f,\n", white);
@@ -40,7 +42,7 @@ std::string tbc_json(const Format& fmt, const cuvhs_field_info* fields, size_t n
   appendf(s, "    \"fieldHeight\": %d,\n", fmt.output_field_lines);
   appendf(s, "    \"colourBurstStart\": %d,\n", fmt.burst_start);
   appendf(s, "    \"colourBurstEnd\": %d,\n", fmt.burst_end);
-  s += "    \"activeVideoStart\": 134,\n    \"activeVideoEnd\": 894,\n";
+  appendf(s, "    \"activeVideoStart\": %d,\n    \"activeVideoEnd\": %d,\n", pal ? 185 : 134, pal ? 1107 : 894);
   s += "    \"tapeFormat\": \"VHS\",\n    \"isMapped\": false\n  },\n  \"fields\": [\n";
   for (size_t i = 0; i < n; i++) {
     const cuvhs_field_info& f = fields[i];

@@ -9,17 +9,17 @@ order over a chunk gives exactly what Decoder's chunk decode gives.
 
 A chunk is `tiles` field slots of dec.tile_stride samples; positions are
 sample indices from the chunk's first sample.  Video and sync are FP32 Hz
-relative to the 0 IRE frequency (ire0_hz(dec)); line locations FP64, 525 per
-field; luma and chroma u16 (held in int16 tensors) [fields, 263, 910].
+relative to the 0 IRE frequency (ire0_hz(dec)); line locations FP64,
+dec.lines_per_frame per field; luma and chroma u16 (held in int16 tensors)
+[fields, *dec.field_shape].
 """
 import ctypes
 
 import numpy as np
 
-from ._lib import FIELD_H, FIELD_W, lib
+from ._lib import lib
 
 MAX_PULSES = 800
-LINES_PER_FRAME = 525
 
 
 def _p(t):
@@ -88,13 +88,13 @@ def sync_pulses(dec, sync, tiles, field_offsets):
 
 def line_locations(dec, raw_offset, field_offsets, starts, lengths, counts):
     """The host line locations after sync_pulses (src/pipeline/pipeline.cu:1717-1778):
-    (linelocs [fields, 525] float64, is_first_field [fields] int32)."""
+    (linelocs [fields, lines_per_frame] float64, is_first_field [fields] int32)."""
     offs = np.ascontiguousarray(field_offsets, np.int64)
     n = offs.size
     starts = np.ascontiguousarray(starts, np.int32).reshape(n, MAX_PULSES) if n else np.zeros((1, MAX_PULSES), np.int32)
     lengths = np.ascontiguousarray(lengths, np.int32).reshape(n, MAX_PULSES) if n else np.zeros_like(starts)
     counts = np.ascontiguousarray(counts, np.int32) if n else np.zeros(1, np.int32)
-    ll = np.zeros((max(n, 1), LINES_PER_FRAME), np.float64)
+    ll = np.zeros((max(n, 1), dec.lines_per_frame), np.float64)
     first = np.zeros(max(n, 1), np.int32)
     dec._check(lib.cuvhs_stage_line_locations(dec._h, raw_offset, _np(offs), n, _np(starts), _np(lengths),
                                               _np(counts), _np(ll), _np(first)))
@@ -103,19 +103,19 @@ def line_locations(dec, raw_offset, field_offsets, starts, lengths, counts):
 
 def hsync_refine(dec, sync, linelocs):
     """hsync_refine (src/pipeline/hsync_refine.h:18-22): refines the float64
-    CUDA tensor linelocs [fields, 525] in place."""
+    CUDA tensor linelocs [fields, lines_per_frame] in place."""
     tiles = sync.numel() // dec.tile_stride
     _ready(sync)
     dec._check(lib.cuvhs_stage_hsync_refine(dec._h, _p(sync), tiles, _p(linelocs),
-                                            linelocs.numel() // LINES_PER_FRAME))
+                                            linelocs.numel() // dec.lines_per_frame))
     return linelocs
 
 
 def tbc_resample(dec, video, linelocs):
-    """tbc_resample (src/pipeline/tbc_resample.h:16-27): luma [fields, 263, 910]."""
+    """tbc_resample (src/pipeline/tbc_resample.h:16-27): luma [fields, rows, columns]."""
     import torch
-    n = linelocs.numel() // LINES_PER_FRAME
-    luma = torch.empty((n, FIELD_H, FIELD_W), dtype=torch.int16, device=video.device)
+    n = linelocs.numel() // dec.lines_per_frame
+    luma = torch.empty((n,) + dec.field_shape, dtype=torch.int16, device=video.device)
     tiles = video.numel() // dec.tile_stride
     _ready(video)
     dec._check(lib.cuvhs_stage_tbc_resample(dec._h, _p(video), tiles, _p(linelocs), n, _p(luma)))
@@ -124,10 +124,10 @@ def tbc_resample(dec, video, linelocs):
 
 def chroma_decode(dec, raw, linelocs, n_read=None):
     """chroma_decode (src/pipeline/chroma_decode.h:38-46): (chroma [fields,
-    263, 910], field phase IDs) from the raw chunk."""
+    rows, columns], field phase IDs) from the raw chunk."""
     import torch
-    n = linelocs.numel() // LINES_PER_FRAME
-    chroma = torch.empty((n, FIELD_H, FIELD_W), dtype=torch.int16, device=raw.device)
+    n = linelocs.numel() // dec.lines_per_frame
+    chroma = torch.empty((n,) + dec.field_shape, dtype=torch.int16, device=raw.device)
     ids = np.zeros(max(n, 1), np.int32)
     n_read = raw.numel() if n_read is None else n_read
     _ready(raw)
@@ -138,9 +138,12 @@ def chroma_decode(dec, raw, linelocs, n_read=None):
 def dropout_detect(dec, envelope, linelocs, luma, chroma):
     """dropout_detect (src/pipeline/dropout_detect.h:22-32) through
     cuvhs_dropouts_noalloc on torch's current stream: conceals luma and chroma
-    in place; returns (counts, lines, startx, endx) as int32 CUDA tensors."""
+    in place; returns (counts, lines, startx, endx) as int32 CUDA tensors.
+    NTSC fields only, as cuvhs_dropouts_noalloc."""
     import torch
-    n = linelocs.numel() // LINES_PER_FRAME
+    if dec.lines_per_frame != 525:
+        raise ValueError("cuvhs_dropouts_noalloc takes NTSC fields")
+    n = linelocs.numel() // dec.lines_per_frame
     if envelope.numel() < n * dec.tile_stride:
         raise ValueError(f"the envelope covers {envelope.numel() // dec.tile_stride} field slots, "
                          f"the line locations {n} fields")

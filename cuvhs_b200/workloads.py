@@ -1,4 +1,4 @@
-"""Named synthetic workloads (seeded synthetic NTSC VHS RF captures).
+"""Named synthetic workloads (seeded synthetic NTSC and PAL VHS RF captures).
 
 They stand in for real tape captures: the reference was developed on private
 captures, so every measurement and parity case here runs on seeded synthetic
@@ -19,7 +19,18 @@ WORKLOADS = {
                        dropout_line_rate=0.001, headswitch_min=3, headswitch_max=8),
     # 35.8 MHz rate coverage
     "small358": dict(sample_rate_hz=35.8e6, n_fields=6, seed=31, snr_db=38, jitter_bound=1.0),
+    # PAL (--system PAL): 6 clean fields at 28 MHz; 8 fields at 28 MHz with dropouts and head switch
+    "small28pal": dict(sample_rate_hz=28e6, n_fields=6, seed=41, snr_db=40, jitter_bound=0.5, system=1),
+    "dropouts28pal": dict(sample_rate_hz=28e6, n_fields=8, seed=43, snr_db=36, jitter_bound=1.0,
+                          dropout_line_rate=0.01, headswitch_min=3, headswitch_max=8, system=1),
+    # PAL at 40 MHz, 20 fields
+    "pal20_40": dict(sample_rate_hz=40e6, n_fields=20, seed=47, snr_db=38, jitter_bound=1.0, system=1),
 }
+
+
+def system_of(name):
+    """The video system ("NTSC" or "PAL") of a named workload."""
+    return "PAL" if WORKLOADS[name].get("system", 0) == 1 else "NTSC"
 
 
 def make_workload(name, **overrides):

@@ -1,8 +1,8 @@
 /* libcuvhs: B200 (sm_100a) VHS RF decoder, C ABI.
  *
- * Drop-in for the decode path of hunterschuler/cuVHS: u8 NTSC VHS RF capture in,
- * 910x263 u16 luma and chroma TBC fields plus .tbc.json field/line/dropout
- * metadata out.  Every entry point returns a cuvhs_status; no C++ types or
+ * Drop-in for the decode path of hunterschuler/cuVHS: an NTSC or PAL VHS RF
+ * capture (u8, s16 or u16 samples) in, u16 luma and chroma TBC fields (910x263
+ * NTSC, 1135x313 PAL) plus .tbc.json field/line/dropout metadata out.  Every entry point returns a cuvhs_status; no C++ types or
  * exceptions cross the boundary.  A context owns one CUDA stream and all of its
  * device memory, allocated once in cuvhs_create.  Contexts are independent;
  * one context is not safe to use from two threads at once.
@@ -55,14 +55,14 @@ typedef enum cuvhs_status {
   CUVHS_ERR_OUT_OF_MEMORY = 3,
   CUVHS_ERR_IO = 4,
   CUVHS_ERR_CAPACITY = 5,    /* an internal fixed-size list overflowed */
-  CUVHS_ERR_UNSUPPORTED = 6, /* e.g. PAL, which this build does not decode */
+  CUVHS_ERR_UNSUPPORTED = 6, /* e.g. a PAL context for the NTSC-only calibration model */
   CUVHS_ERR_EXISTS = 7       /* output exists and overwrite was not requested */
 } cuvhs_status;
 
 typedef struct cuvhs_ctx cuvhs_ctx;
 
 typedef struct cuvhs_config {
-  int system;             /* 0 = NTSC (--system NTSC) */
+  int system;             /* --system: 0 = NTSC, 1 = PAL (src/format/video_format.cpp:23-104) */
   double sample_rate_mhz; /* -f, capture rate */
   int device;             /* --gpu: CUDA device id, -1 = the one with most memory */
   int batch_fields;       /* fields per chunk; 0 = derive from free device memory */
@@ -82,8 +82,8 @@ typedef struct cuvhs_field_info {
 
 /* Caller-owned host output buffers. */
 typedef struct cuvhs_output {
-  uint16_t* luma;          /* [max_fields][263][910] */
-  uint16_t* chroma;        /* [max_fields][263][910] */
+  uint16_t* luma;          /* [max_fields][field height][field width] */
+  uint16_t* chroma;        /* [max_fields][field height][field width] */
   cuvhs_field_info* fields; /* [max_fields] */
   int32_t* dropout_line;   /* [max_dropouts] */
   int32_t* dropout_startx;
@@ -103,7 +103,13 @@ const char* cuvhs_last_error(const cuvhs_ctx* ctx);
 const char* cuvhs_status_string(cuvhs_status s);
 
 int cuvhs_batch_fields(const cuvhs_ctx* ctx);
-size_t cuvhs_samples_per_field(const cuvhs_ctx* ctx); /* samples_per_line * 263 */
+/* Output field geometry of the context's system: 910 x 263 (NTSC) or
+ * 1135 x 313 (PAL) u16 samples, and line locations per field (525 / 625).
+ * CUVHS_FIELD_WIDTH / CUVHS_FIELD_HEIGHT are the NTSC values. */
+int cuvhs_field_width(const cuvhs_ctx* ctx);
+int cuvhs_field_height(const cuvhs_ctx* ctx);
+int cuvhs_lines_per_frame(const cuvhs_ctx* ctx);
+size_t cuvhs_samples_per_field(const cuvhs_ctx* ctx); /* samples_per_line * 263 (NTSC) or 313 (PAL) */
 size_t cuvhs_tile_stride(const cuvhs_ctx* ctx);       /* samples per chunk field slot (+20 lines) */
 /* Forget carried state (field parity, line-location and chroma track state). */
 void cuvhs_reset(cuvhs_ctx* ctx);
@@ -194,11 +200,13 @@ long long cuvhs_debug_array(const cuvhs_ctx* ctx, const char* name, void* dst, l
  * the chunk's first sample.  d_ arguments are device memory, the rest host
  * memory.  Signals are FP32: video and sync in Hz relative to the 0 IRE
  * frequency (cuvhs_ire0_hz), the envelope as |analytic signal| in the
- * reference's scale.  Line locations are FP64 chunk positions, 525 per field.
+ * reference's scale.  Line locations are FP64 chunk positions,
+ * cuvhs_lines_per_frame per field; TBC fields have the cuvhs_field_width x
+ * cuvhs_field_height geometry.
  * The dropout stage (dropout_detect, src/pipeline/dropout_detect.h:22-32) is
  * cuvhs_dropouts_noalloc below. */
 #define CUVHS_MAX_PULSES_PER_FIELD 800
-#define CUVHS_LINES_PER_FRAME 525
+#define CUVHS_LINES_PER_FRAME 525 /* NTSC; cuvhs_lines_per_frame gives the context's */
 double cuvhs_ire0_hz(const cuvhs_ctx* ctx);
 
 /* fm_demod (src/pipeline/fm_demod.h:46-53): d_raw holds n_read samples of the
@@ -226,33 +234,34 @@ cuvhs_status cuvhs_stage_sync_pulses(cuvhs_ctx* ctx, const float* d_sync, int ti
  * pulse validation, field order, blanking anchor and the snapped line grid,
  * field by field with the field-order state carried across fields and calls.
  * raw_offset is the capture sample of the chunk's first sample.  linelocs
- * [n_fields * 525]; is_first_field [n_fields] (may be NULL) = 1, 0, or -1. */
+ * [n_fields * lines_per_frame]; is_first_field [n_fields] (may be NULL) = 1, 0, or -1. */
 cuvhs_status cuvhs_stage_line_locations(cuvhs_ctx* ctx, uint64_t raw_offset, const int64_t* field_offsets,
                                         int n_fields, const int32_t* starts, const int32_t* lengths,
                                         const int32_t* counts, double* linelocs, int32_t* is_first_field);
 
 /* hsync_refine (src/pipeline/hsync_refine.h:18-22): refines d_linelocs
- * [n_fields * 525] in place.  d_sync holds `tiles` slots; the refinement
+ * [n_fields * lines_per_frame] in place.  d_sync holds `tiles` slots; the refinement
  * reads min(n_fields, tiles) * tile_stride samples of it (the reference's
  * total_demod_samples = n_fields * tile_stride when the buffer covers them). */
 cuvhs_status cuvhs_stage_hsync_refine(cuvhs_ctx* ctx, const float* d_sync, int tiles, double* d_linelocs,
                                       int n_fields);
 
-/* tbc_resample (src/pipeline/tbc_resample.h:16-27): d_luma [n_fields][263][910];
+/* tbc_resample (src/pipeline/tbc_resample.h:16-27): d_luma [n_fields][height][width];
  * d_video holds `tiles` slots, read as hsync_refine reads d_sync. */
 cuvhs_status cuvhs_stage_tbc_resample(cuvhs_ctx* ctx, const float* d_video, int tiles, const double* d_linelocs,
                                       int n_fields, uint16_t* d_luma);
 
 /* chroma_decode (src/pipeline/chroma_decode.h:38-46): the colour-under chroma
  * of n_fields fields from the raw chunk (n_read samples of the configured
- * format) into d_chroma [n_fields][263][910]; field_phase_ids [n_fields] (may
+ * format) into d_chroma [n_fields][height][width]; field_phase_ids [n_fields] (may
  * be NULL) receives the NTSC field phase IDs.  The first call after create or
  * cuvhs_reset detects the track and phase cycle; later calls carry them. */
 cuvhs_status cuvhs_stage_chroma_decode(cuvhs_ctx* ctx, const void* d_raw, size_t n_read, const double* d_linelocs,
                                        int n_fields, uint16_t* d_chroma, int32_t* field_phase_ids);
 
 /* Dropout detection and concealment on caller-owned device buffers, allocating
- * no device memory.  No counterpart in the reference (its dropout stage
+ * no device memory, for NTSC fields (525 line locations, 910x263 TBC fields,
+ * active lines from 10).  No counterpart in the reference (its dropout stage
  * allocates a temporary on every call).  For callers that cannot call
  * cudaMalloc: code running while its stream is captured into a CUDA graph,
  * real-time capture loops that must not block in the allocator, and hosts

@@ -1,4 +1,4 @@
-/* Seeded synthetic NTSC VHS RF test-signal generator (part of libcuvhs).
+/* Seeded synthetic NTSC / PAL VHS RF test-signal generator (part of libcuvhs).
  *
  * No counterpart in the reference, which ships no test signal: it stands in for
  * the private tape captures the reference was developed on.  The parameters
@@ -38,6 +38,7 @@ typedef struct cuvhs_synth_params {
                                 start, uniform in +/- bound samples; within a line the delay runs
                                 linearly to the next line's */
   double chroma_phase_bound; /* per-line colour-under phase offset, uniform in +/- bound radians */
+  int system;                /* 0 = NTSC, 1 = PAL (timing, IRE map, colour-under carrier, V switch) */
 } cuvhs_synth_params;
 
 void cuvhs_synth_default_params(cuvhs_synth_params* p);

@@ -52,8 +52,9 @@ void parallel_for(int n, int threads, F fn) {
 }
 
 // ---------------------------------------------------------------- format
-// NTSC branch of VideoFormat::VideoFormat (video_format.cpp:23-104).
+// VideoFormat::VideoFormat (video_format.cpp:23-104), NTSC and PAL branches.
 struct Format {
+  bool pal = false;
   double sample_rate;
   int lines_per_frame = 525, lines_per_field = 263;
   double line_rate = 15734.264;
@@ -70,21 +71,47 @@ struct Format {
   int samples_per_line, samples_per_field;
   double hsync_width, eq_pulse_width, bp_width, vsync_width;
 
-  explicit Format(double mhz) : sample_rate(mhz * 1e6) {
-    hz_ire = 1e6 / 140.0;
-    ire0 = 4.4e6 - (hz_ire * 100.0);
-    vsync_ire = -40.0;
+  explicit Format(double mhz, bool is_pal = false) : pal(is_pal), sample_rate(mhz * 1e6) {
+    if (!pal) {
+      hz_ire = 1e6 / 140.0;
+      ire0 = 4.4e6 - (hz_ire * 100.0);
+      vsync_ire = -40.0;
+    } else {
+      lines_per_frame = 625;
+      lines_per_field = 313;
+      line_rate = 15625.0;
+      fsc = 4433618.75;
+      chroma_under = ((625.0 * 25.0) * 40.0) + 1953.0;
+      burst_abs_ref = 5000.0;
+      burst_start_us = 5.6;
+      burst_end_us = 7.85;
+      output_line_len = 1135;
+      output_field_lines = 313;
+      num_eq_pulses = 5;
+      field_lines_first = 312;
+      field_lines_second = 313;
+      vsync_ire = -0.3 * (100.0 / 0.7);
+      hz_ire = 1e6 / (100.0 + (-vsync_ire));
+      ire0 = 4.8e6 - (hz_ire * 100.0);
+    }
     sync_tip_hz = ire0 + hz_ire * vsync_ire;
     pulse_threshold_hz = ire0 + hz_ire * (-20.0);
-    output_zero = 1024.0;
-    output_scale = (51200.0 - 1024.0) / (100.0 - vsync_ire);
+    if (!pal) {
+      output_zero = 1024.0;
+      output_scale = (51200.0 - 1024.0) / (100.0 - vsync_ire);
+      active_line_start = 10;
+    } else {
+      output_zero = 256.0;
+      output_scale = (54016.0 - 256.0) / (100.0 - vsync_ire);
+      active_line_start = 8;
+    }
     output_rate = 4.0 * fsc;
     samples_per_line = (int)std::round(sample_rate / line_rate);
     samples_per_field = samples_per_line * lines_per_field;
     hsync_width = 4.7e-6 * sample_rate;
     eq_pulse_width = 2.3e-6 * sample_rate;
     bp_width = 1.5e-6 * sample_rate;
-    vsync_width = 27.1e-6 * sample_rate;
+    vsync_width = (pal ? 27.3e-6 : 27.1e-6) * sample_rate;
   }
 };
 
@@ -252,7 +279,7 @@ struct oracle_ctx {
   std::vector<oracle::FieldMeta> meta;
   std::vector<oracle::ChunkRec> chunks;
   std::string json;
-  explicit oracle_ctx(double mhz) : fmt(mhz) {}
+  oracle_ctx(double mhz, bool pal) : fmt(mhz, pal) {}
 };
 
 namespace oracle {
@@ -556,6 +583,14 @@ Anchor first_hsync(const std::vector<VPulse>& vp, double mll, const Format& fmt,
     last = i;
   }
   double ffl[4] = {1, 0.5, 0.5, 1}, sfl[4] = {0.5, 1, 1, 0.5}, pfl[4] = {1, 0.5, 1, 0.5};
+  if (fmt.pal) {  // pipeline.cu:711-715
+    const double pf[4] = {0.5, 0.5, 1, 1}, ps[4] = {1, 1, 0.5, 0.5}, pp[4] = {0.5, 0.5, 0.5, 0.5};
+    for (int i = 0; i < 4; i++) {
+      ffl[i] = pf[i];
+      sfl[i] = ps[i];
+      pfl[i] = pp[i];
+    }
+  }
   double ic = 0.0, id = 0.0, pc = 0.0, pd = 0.0;
   for (int i = 0; i < 4; i++) {
     double fl = fol[i];
@@ -621,7 +656,7 @@ Anchor first_hsync(const std::vector<VPulse>& vp, double mll, const Format& fmt,
   } else if (l_cnt == 6 || (prev_loc <= 0.0 && l_cnt > f_cnt)) {
     loc = l_loc; cnt = l_cnt; off = l_off;
   }
-  double est_lines = prev_lines;  // NTSC (pipeline.cu:811)
+  double est_lines = fmt.pal ? cur_lines : prev_lines;  // pipeline.cu:811
   int est_loc = (int)std::llround((last_off_lines + est_lines + prev_loc / mll) * mll);
   bool used_est = false;
   if (cnt == 0 && prev_loc > 0.0) {
@@ -1182,14 +1217,18 @@ std::string make_json(const Format& fmt, const std::vector<FieldMeta>& meta) {
   double white = (100.0 - fmt.vsync_ire) * fmt.output_scale + fmt.output_zero;
   int bs = (int)(fmt.burst_start_us * 1e-6 * fmt.output_rate + 0.5);
   int be = (int)(fmt.burst_end_us * 1e-6 * fmt.output_rate + 0.5);
-  s += "{\n  \"videoParameters\": {\n    \"system\": \"NTSC\",\n    \"isSubcarrierLocked\": false,\n    \"isSourcePal\": false,\n";
+  s += fmt.pal ? "{\n  \"videoParameters\": {\n    \"system\": \"PAL\",\n    \"isSubcarrierLocked\": false,\n    \"isSourcePal\": true,\n"
+               : "{\n  \"videoParameters\": {\n    \"system\": \"NTSC\",\n    \"isSubcarrierLocked\": false,\n    \"isSourcePal\": false,\n";
   snprintf(buf, sizeof buf, "    \"numberOfSequentialFields\": %d,\n", (int)meta.size()); s += buf;
   snprintf(buf, sizeof buf, "    \"black16bIre\": %.1f,\n", black); s += buf;
   snprintf(buf, sizeof buf, "    \"white16bIre\": %.1f,\n", white); s += buf;
   snprintf(buf, sizeof buf, "    \"sampleRate\": %.0f,\n", fmt.output_rate); s += buf;
   snprintf(buf, sizeof buf, "    \"fieldWidth\": %d,\n    \"fieldHeight\": %d,\n", fmt.output_line_len, fmt.output_field_lines); s += buf;
   snprintf(buf, sizeof buf, "    \"colourBurstStart\": %d,\n    \"colourBurstEnd\": %d,\n", bs, be); s += buf;
-  s += "    \"activeVideoStart\": 134,\n    \"activeVideoEnd\": 894,\n    \"tapeFormat\": \"VHS\",\n    \"isMapped\": false\n  },\n";
+  snprintf(buf, sizeof buf, "    \"activeVideoStart\": %d,\n    \"activeVideoEnd\": %d,\n", fmt.pal ? 185 : 134,
+           fmt.pal ? 1107 : 894);  // tbc_writer.cpp:107-108
+  s += buf;
+  s += "    \"tapeFormat\": \"VHS\",\n    \"isMapped\": false\n  },\n";
   s += "  \"fields\": [\n";
   for (size_t i = 0; i < meta.size(); i++) {
     const FieldMeta& m = meta[i];
@@ -1364,14 +1403,22 @@ int process_chunk(oracle_ctx* c, const uint8_t* data, size_t n, size_t raw_offse
 
 extern "C" {
 
-oracle_ctx* oracle_create(double mhz, int batch_fields, int threads) {
-  oracle_ctx* c = new oracle_ctx(mhz);
+oracle_ctx* oracle_create_system(double mhz, int batch_fields, int threads, int system) {
+  oracle_ctx* c = new oracle_ctx(mhz, system == 1);
   c->batch = batch_fields > 0 ? batch_fields : 1;
   c->threads = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
   c->spp = c->fmt.samples_per_field + oracle::FIELD_MARGIN_LINES * c->fmt.samples_per_line;
   oracle::design_demod(c->fmt, c->spp, c->filt);
   return c;
 }
+
+oracle_ctx* oracle_create(double mhz, int batch_fields, int threads) {
+  return oracle_create_system(mhz, batch_fields, threads, 0);
+}
+
+int oracle_field_width(const oracle_ctx* c) { return c->fmt.output_line_len; }
+int oracle_field_height(const oracle_ctx* c) { return c->fmt.output_field_lines; }
+int oracle_lines_per_frame(const oracle_ctx* c) { return c->fmt.lines_per_frame; }
 
 void oracle_destroy(oracle_ctx* c) { delete c; }
 void oracle_keep_signals(oracle_ctx* c, int keep) { c->keep_signals = keep != 0; }

@@ -22,7 +22,13 @@ typedef struct oracle_ctx oracle_ctx;
 
 /* mhz: capture rate; batch_fields: the reference's chunk size in fields
  * (its VRAM-derived batch_size); threads: host threads (0 = all cores). */
-oracle_ctx* oracle_create(double mhz, int batch_fields, int threads);
+oracle_ctx* oracle_create(double mhz, int batch_fields, int threads); /* NTSC */
+/* system: 0 NTSC, 1 PAL (VideoFormat's two branches, video_format.cpp:23-104) */
+oracle_ctx* oracle_create_system(double mhz, int batch_fields, int threads, int system);
+/* output field geometry and line locations per field of the context's system */
+int oracle_field_width(const oracle_ctx* c);
+int oracle_field_height(const oracle_ctx* c);
+int oracle_lines_per_frame(const oracle_ctx* c);
 void oracle_destroy(oracle_ctx* c);
 
 /* Decode a whole u8 capture held in memory.  Returns number of fields. */
@@ -30,8 +36,8 @@ int oracle_decode(oracle_ctx* c, const uint8_t* data, size_t n);
 
 /* Results of the last decode. */
 int oracle_num_fields(const oracle_ctx* c);
-const uint16_t* oracle_luma(const oracle_ctx* c);    /* [fields][263][910] */
-const uint16_t* oracle_chroma(const oracle_ctx* c);  /* [fields][263][910] */
+const uint16_t* oracle_luma(const oracle_ctx* c);    /* [fields][height][width] */
+const uint16_t* oracle_chroma(const oracle_ctx* c);  /* [fields][height][width] */
 /* The .tbc.json text the reference writer would produce (NUL-terminated). */
 const char* oracle_json(const oracle_ctx* c);
 

@@ -17,7 +17,6 @@ LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_HARNESS = os.path.join(HERE, "_ref", "ref_harness")
 REF_CLI = os.path.join(HERE, "_ref", "cuvhs_ref")
 
-F = 910 * 263
 F64_ARRAYS = ("linelocs_coarse", "linelocs", "demod", "demod05", "envelope", "chroma_prefilt")
 
 _lib = None
@@ -35,6 +34,10 @@ def _load():
         L = ctypes.CDLL(LIB)
         L.oracle_create.restype = ctypes.c_void_p
         L.oracle_create.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        L.oracle_create_system.restype = ctypes.c_void_p
+        L.oracle_create_system.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        for fn in ("oracle_field_width", "oracle_field_height", "oracle_lines_per_frame"):
+            getattr(L, fn).argtypes = [ctypes.c_void_p]
         L.oracle_decode.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
         L.oracle_luma.restype = ctypes.c_void_p
         L.oracle_luma.argtypes = [ctypes.c_void_p]
@@ -62,9 +65,12 @@ class Oracle:
     FORMATS = {"u8": (0, np.uint8), "s16": (1, np.int16), "u16": (2, np.uint16)}
 
     def __init__(self, sample_rate_mhz=28.0, batch_fields=3282, threads=0, keep_signals=False, input_format="u8",
-                 dc_correct=False):
+                 dc_correct=False, system="NTSC"):
         L = _load()
-        self._h = L.oracle_create(float(sample_rate_mhz), int(batch_fields), int(threads))
+        self._h = L.oracle_create_system(float(sample_rate_mhz), int(batch_fields), int(threads),
+                                         {"NTSC": 0, "PAL": 1}[system.upper()])
+        self.field_shape = (L.oracle_field_height(self._h), L.oracle_field_width(self._h))
+        self.lines_per_frame = L.oracle_lines_per_frame(self._h)
         if keep_signals:
             L.oracle_keep_signals(self._h, 1)
         fmt, self._dtype = self.FORMATS[input_format]
@@ -81,10 +87,11 @@ class Oracle:
         n = L.oracle_decode(self._h, samples.ctypes.data, samples.size)
         self.n_fields = n
         P = ctypes.POINTER(ctypes.c_uint16)
-        self.luma = np.ctypeslib.as_array(ctypes.cast(L.oracle_luma(self._h), P), (n * F,)).reshape(n, 263, 910).copy() \
-            if n else np.zeros((0, 263, 910), np.uint16)
-        self.chroma = np.ctypeslib.as_array(ctypes.cast(L.oracle_chroma(self._h), P), (n * F,)).reshape(n, 263, 910).copy() \
-            if n else np.zeros((0, 263, 910), np.uint16)
+        H, W = self.field_shape
+        self.luma = np.ctypeslib.as_array(ctypes.cast(L.oracle_luma(self._h), P), (n * H * W,)).reshape(n, H, W).copy() \
+            if n else np.zeros((0, H, W), np.uint16)
+        self.chroma = np.ctypeslib.as_array(ctypes.cast(L.oracle_chroma(self._h), P), (n * H * W,)).reshape(n, H, W).copy() \
+            if n else np.zeros((0, H, W), np.uint16)
         self.json = L.oracle_json(self._h).decode()
         return n
 

@@ -21,6 +21,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <strings.h>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -75,12 +76,14 @@ struct Dumper {
 
 int main(int argc, char** argv) {
   double mhz = 28.0;
+  bool pal = false;
   std::string in, out, dump_dir;
   bool time_only = false;
   int dump_tiles = 2;
   int pos = 0;
   for (int i = 1; i < argc; i++) {
     if (!strcmp(argv[i], "-f") && i + 1 < argc) mhz = atof(argv[++i]);
+    else if (!strcmp(argv[i], "--system") && i + 1 < argc) pal = !strcasecmp(argv[++i], "PAL");
     else if (!strcmp(argv[i], "--dump") && i + 1 < argc) dump_dir = argv[++i];
     else if (!strcmp(argv[i], "--dump-tiles") && i + 1 < argc) dump_tiles = atoi(argv[++i]);
     else if (!strcmp(argv[i], "--time")) time_only = true;
@@ -88,13 +91,13 @@ int main(int argc, char** argv) {
     else if (pos == 1) { out = argv[i]; pos++; }
   }
   if (pos < 2) {
-    fprintf(stderr, "usage: ref_harness [-f MHz] [--dump DIR] [--dump-tiles N] [--time] in.u8 out_base\n");
+    fprintf(stderr, "usage: ref_harness [-f MHz] [--system NTSC|PAL] [--dump DIR] [--dump-tiles N] [--time] in.u8 out_base\n");
     return 2;
   }
 
   GPUDevice gpu;
   if (!gpu.init(0)) return 1;
-  VideoFormat fmt(VideoSystem::NTSC, mhz);
+  VideoFormat fmt(pal ? VideoSystem::PAL : VideoSystem::NTSC, mhz);
   RawReader reader;
   if (!reader.open(in, InputFormat::U8)) return 1;
   TBCWriter writer;

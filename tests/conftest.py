@@ -35,7 +35,7 @@ def oracle_decode(name):
     import cuvhs_b200 as cv
     from oracle.oracle import Oracle
     x = workload(name)
-    o = Oracle(cv.WORKLOADS[name]["sample_rate_hz"] / 1e6)
+    o = Oracle(cv.WORKLOADS[name]["sample_rate_hz"] / 1e6, system=cv.system_of(name))
     o.decode(x)
     return o
 
@@ -48,17 +48,18 @@ def golden(name):
     return g
 
 
-def tile_stride(mhz):
-    spl = int(round(mhz * 1e6 / 15734.264))
-    return spl * 263 + 20 * spl
+def tile_stride(mhz, system="NTSC"):
+    pal = system == "PAL"
+    spl = int(round(mhz * 1e6 / (15625.0 if pal else 15734.264)))
+    return spl * (313 if pal else 263) + 20 * spl
 
 
-def inside_fields(file_locs, n_input, mhz):
+def inside_fields(file_locs, n_input, mhz, system="NTSC"):
     """Fields whose analysis window (one tile stride from the field start) lies
     inside the capture.  Past the end the reference decodes zero-filled samples,
     whose FM phase is FP64 round-off noise, so no implementation can match
     those fields sample for sample."""
-    spp = tile_stride(mhz)
+    spp = tile_stride(mhz, system)
     return [i for i, f in enumerate(file_locs) if int(f) + spp <= n_input]
 
 

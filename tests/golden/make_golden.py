@@ -24,8 +24,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-NAMES = ["small28", "dropouts28", "plain40_28"]
-FIELD = 910 * 263
+NAMES = ["small28", "dropouts28", "plain40_28", "small28pal", "dropouts28pal"]
+GEOMETRY = {"NTSC": (525, 263, 910), "PAL": (625, 313, 1135)}  # line locations per field, field rows, columns
 DTYPES = {"i32": np.int32, "i64": np.int64, "f32": np.float32, "f64": np.float64}
 
 
@@ -49,8 +49,9 @@ def run(outdir, names):
         x.tofile(inp)
         with open(os.path.join(d, "input.md5"), "w") as f:
             f.write(hashlib.md5(x.tobytes()).hexdigest())
-        subprocess.check_call([REF_HARNESS, "-f", str(mhz), "--dump", d, "--dump-tiles", "1", inp,
-                               os.path.join(d, "out")], stdout=open(os.path.join(d, "harness.json"), "w"),
+        subprocess.check_call([REF_HARNESS, "-f", str(mhz), "--system", cv.system_of(name), "--dump", d,
+                               "--dump-tiles", "1", inp, os.path.join(d, "out")],
+                              stdout=open(os.path.join(d, "harness.json"), "w"),
                               stderr=open(os.path.join(d, "harness.err"), "w"))
         os.unlink(inp)
 
@@ -58,6 +59,7 @@ def run(outdir, names):
 def pack(dumpdir, name):
     import cuvhs_b200 as cv
     x = cv.make_workload(name)
+    lpf, rows, cols = GEOMETRY[cv.system_of(name)]
     ref = load_dump(dumpdir)
     meta = ref["c0_meta"]
     P = int(meta[1])
@@ -82,8 +84,8 @@ def pack(dumpdir, name):
     for part in ["lines", "starts", "ends"]:
         a = ref[f"c0_do_{part}"].reshape(P, 512)
         arrs[f"do_{part}"] = np.concatenate([a[f, :dcnt[f]] for f in range(P)])
-    arrs["linelocs_coarse"] = ref["c0_linelocs_coarse"].reshape(P, 525)
-    arrs["linelocs"] = ref["c0_linelocs"].reshape(P, 525)
+    arrs["linelocs_coarse"] = ref["c0_linelocs_coarse"].reshape(P, lpf)
+    arrs["linelocs"] = ref["c0_linelocs"].reshape(P, lpf)
     arrs["chroma_state"] = ref["c0_chroma_state"]
     arrs["k2b_state"] = ref["c0_k2b_state"]
     # per-field digests of the TBC output and a sample of rows of field 0
@@ -91,7 +93,7 @@ def pack(dumpdir, name):
     for suf, key in ((".tbc", "luma"), ("_chroma.tbc", "chroma")):
         path = os.path.join(dumpdir, "out" + suf)
         if os.path.exists(path):
-            a = np.fromfile(path, np.uint16).reshape(-1, 263, 910)
+            a = np.fromfile(path, np.uint16).reshape(-1, rows, cols)
         else:  # packed run: full first fields in fields_*.npy, digests in hash files
             a = None
         if a is not None:
@@ -100,7 +102,7 @@ def pack(dumpdir, name):
         else:
             hs = [l.split()[1] for l in open(os.path.join(dumpdir, "hash" + suf + ".txt"))]
             arrs[f"{key}_md5"] = np.array(hs)
-            fl = np.load(os.path.join(dumpdir, "fields" + suf.replace(".", "_") + ".npy")).reshape(-1, 263, 910)
+            fl = np.load(os.path.join(dumpdir, "fields" + suf.replace(".", "_") + ".npy")).reshape(-1, rows, cols)
             arrs[f"{key}_rows_f0"] = fl[0, ::16]
         tbc[key] = True
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrs)

@@ -20,7 +20,7 @@ POS_TOL = 0.01
 def decode(name, batch_fields=0):
     x = workload(name)
     mhz = cv.WORKLOADS[name]["sample_rate_hz"] / 1e6
-    with cv.Decoder(mhz, batch_fields=batch_fields, debug=True) as d:
+    with cv.Decoder(mhz, batch_fields=batch_fields, debug=True, system=cv.system_of(name)) as d:
         r = d.decode_capture(x)
         dbg = {k: d.debug_array(k) for k in ("field_offsets", "k2_pulse_count", "k2_pulse_starts",
                                              "k2_pulse_lengths", "k2b_pulse_count", "k2b_pulse_starts",
@@ -41,7 +41,7 @@ def compare_to_oracle(name, r, dbg, x, mhz, o, chunk_last_only=False):
     ofields = json_fields(o.json)
     mfields = json_fields(r.json)
     assert [f["fileLoc"] for f in mfields] == [f["fileLoc"] for f in ofields]
-    inside = inside_fields([f["fileLoc"] for f in mfields], x.size, mhz)
+    inside = inside_fields([f["fileLoc"] for f in mfields], x.size, mhz, cv.system_of(name))
     assert len(inside) >= r.n_fields - 1
     for i in inside:
         assert mfields[i] == ofields[i], i
@@ -52,7 +52,8 @@ def compare_to_oracle(name, r, dbg, x, mhz, o, chunk_last_only=False):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["small28", "dropouts28", "plain40_28", "small358"])
+@pytest.mark.parametrize("name", ["small28", "dropouts28", "plain40_28", "small358", "small28pal",
+                                  "dropouts28pal", "pal20_40"])
 def test_decoder_matches_oracle(name):
     x, mhz, r, dbg = decode(name)
     o = oracle_decode(name)
@@ -68,31 +69,34 @@ def test_decoder_matches_oracle(name):
             for f in inside:
                 assert cm[f] == co[f], (pre, f)
                 assert np.array_equal(a[f, :cm[f]], b[f, :co[f]]), (pre, part, f)
-    llc = dbg["linelocs_coarse"].reshape(P, 525)
-    ll = dbg["linelocs"].reshape(P, 525)
+    lpf, rows = o.lines_per_frame, o.field_shape[0] + 1  # the lines the resamplers read
+    llc = dbg["linelocs_coarse"].reshape(P, lpf)
+    ll = dbg["linelocs"].reshape(P, lpf)
     for f in inside:
-        assert np.array_equal(llc[f, :264], o.array(0, "linelocs_coarse").reshape(P, 525)[f, :264])
-        assert np.abs(ll[f, :264] - o.array(0, "linelocs").reshape(P, 525)[f, :264]).max() <= POS_TOL
+        assert np.array_equal(llc[f, :rows], o.array(0, "linelocs_coarse").reshape(P, lpf)[f, :rows])
+        assert np.abs(ll[f, :rows] - o.array(0, "linelocs").reshape(P, lpf)[f, :rows]).max() <= POS_TOL
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["small28", "dropouts28", "plain40_28"])
+@pytest.mark.parametrize("name", ["small28", "dropouts28", "plain40_28", "small28pal", "dropouts28pal"])
 def test_decoder_matches_reference_fixture(name):
     g = golden(name)
     x, mhz, r, dbg = decode(name)
     gfields = json_fields(g["json_text"])
     mfields = json_fields(r.json)
     assert len(mfields) == len(gfields)
-    inside = inside_fields([f["fileLoc"] for f in gfields], x.size, mhz)
+    inside = inside_fields([f["fileLoc"] for f in gfields], x.size, mhz, cv.system_of(name))
     for i in inside:
         assert mfields[i] == gfields[i], i
     assert np.array_equal(dbg["field_offsets"], g["field_offsets"])
     P = len(g["field_offsets"])
+    lpf = g["linelocs"].shape[1]
+    rows = r.luma.shape[1] + 1
     off = np.concatenate([[0], np.cumsum(g["k2_count"])])
     starts = dbg["k2_pulse_starts"].reshape(P, 800)
     for f in inside:
         assert np.array_equal(starts[f, :g["k2_count"][f]], g["k2_starts"][off[f]:off[f + 1]]), f
-        assert np.abs(dbg["linelocs"].reshape(P, 525)[f, :264] - g["linelocs"][f, :264]).max() <= POS_TOL
+        assert np.abs(dbg["linelocs"].reshape(P, lpf)[f, :rows] - g["linelocs"][f, :rows]).max() <= POS_TOL
     d = np.abs(r.luma[0, ::16].astype(np.int32) - g["luma_rows_f0"].astype(np.int32))
     assert (d > 1).mean() <= LSB_FRACTION
 
@@ -255,6 +259,33 @@ def test_cli_end_to_end(tmp_path):
         assert (tmp_path / f"out_{fmt}.tbc.json").read_text() == g["json_text"]
         assert (tmp_path / f"out_{fmt}.tbc").read_bytes() == (tmp_path / "out.tbc").read_bytes()
         assert (tmp_path / f"out_{fmt}_chroma.tbc").read_bytes() == (tmp_path / "out_chroma.tbc").read_bytes()
+
+
+@pytest.mark.gpu
+def test_cli_pal(tmp_path):
+    """--system PAL through the CLI: the reference's .tbc.json for the same
+    capture, and the 1135 x 313 fields the library decodes."""
+    import subprocess
+    name = "dropouts28pal"
+    x = workload(name)
+    inp = tmp_path / "cap.u8"
+    x.tofile(inp)
+    base = tmp_path / "pal"
+    p = subprocess.run([cv.CLI_PATH, "--system", "PAL", "-f", "28", "--overwrite", str(inp), str(base)],
+                       capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    g = golden(name)
+    mine = json_fields((tmp_path / "pal.tbc.json").read_text())
+    ref = json_fields(g["json_text"])
+    inside = inside_fields([f["fileLoc"] for f in ref], x.size, 28.0, "PAL")
+    assert len(mine) == len(ref) and all(mine[i] == ref[i] for i in inside)
+    head = (tmp_path / "pal.tbc.json").read_text().split('"fields"')[0]
+    assert head == g["json_text"].split('"fields"')[0]  # PAL video parameters
+    luma = np.fromfile(tmp_path / "pal.tbc", np.uint16).reshape(-1, 313, 1135)
+    with cv.Decoder(28.0, system="PAL") as d:
+        r = d.decode_capture(x)
+    assert r.luma.shape[1:] == (313, 1135)
+    assert np.array_equal(luma, r.luma)
 
 
 @pytest.mark.gpu

@@ -75,9 +75,14 @@ def test_cli_refuses_existing_outputs(tmp_path):
     assert "Output exists" in r.stderr
 
 
-def test_cli_rejects_unsupported_modes(tmp_path):
-    r = run_cli("--overwrite", "--system", "PAL", str(tmp_path / "x.u8"), str(tmp_path / "o"))
-    assert r.returncode == 1 and "NTSC" in r.stderr
+def test_cli_system_argument(tmp_path):
+    """--system takes NTSC or PAL (case-insensitive, src/main.cpp:52-56); anything
+    else is an argument error.  PAL passes parsing and fails here only on the
+    missing input file."""
+    r = run_cli("--overwrite", "--system", "SECAM", str(tmp_path / "x.u8"), str(tmp_path / "o"))
+    assert r.returncode == 1 and "Unknown system" in r.stderr
+    r = run_cli("--overwrite", "--system", "pal", str(tmp_path / "x.u8"), str(tmp_path / "o"))
+    assert r.returncode == 1 and "Unknown system" not in r.stderr and "I/O error" in r.stderr
 
 
 def test_oracle_16_bit_inputs_and_dc_correction():
@@ -115,10 +120,13 @@ def test_create_without_device_reports_error():
 def test_invalid_config_rejected():
     cfg = cv._lib.Config()
     cv.lib.cuvhs_default_config(ctypes.byref(cfg))
-    cfg.system = 1  # PAL
+    cfg.system = 2  # neither NTSC (0) nor PAL (1)
     h = ctypes.c_void_p()
-    assert cv.lib.cuvhs_create(ctypes.byref(cfg), ctypes.byref(h)) == 6
+    assert cv.lib.cuvhs_create(ctypes.byref(cfg), ctypes.byref(h)) == 1
     cfg.system = 0
+    cfg.input_format = 3
+    assert cv.lib.cuvhs_create(ctypes.byref(cfg), ctypes.byref(h)) == 1
+    cfg.input_format = 0
     cfg.sample_rate_mhz = 1.0
     assert cv.lib.cuvhs_create(ctypes.byref(cfg), ctypes.byref(h)) == 1
     assert cv.lib.cuvhs_create(None, ctypes.byref(h)) == 1

@@ -9,9 +9,10 @@ import hashlib
 import numpy as np
 import pytest
 
+import cuvhs_b200 as cv
 from conftest import golden, inside_fields, json_fields, oracle_decode, workload
 
-CASES = ["small28", "dropouts28", "plain40_28"]
+CASES = ["small28", "dropouts28", "plain40_28", "small28pal", "dropouts28pal"]
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -24,7 +25,7 @@ def test_oracle_matches_reference(name):
     # identical .tbc.json text: fields, parity, phase IDs, file locations, dropouts
     assert o.json == g["json_text"]
     locs = [f["fileLoc"] for f in json_fields(g["json_text"])]
-    inside = inside_fields(locs, x.size, mhz)
+    inside = inside_fields(locs, x.size, mhz, cv.system_of(name))
     assert len(inside) >= len(locs) - 1
     # luma and chroma bit-identical on every field inside the capture
     for i in inside:
@@ -44,8 +45,9 @@ def test_oracle_matches_reference(name):
             for part in ["starts", "lengths"] + (["types"] if pre == "k2b" else []):
                 mine = o.array(0, f"{pre}_pulse_{part}").reshape(P, 800)[f, :cnt[f]]
                 assert np.array_equal(mine, g[f"{pre}_{part}"][off[f]:off[f + 1]]), (pre, part, f)
-    ll = o.array(0, "linelocs").reshape(P, 525)
-    llc = o.array(0, "linelocs_coarse").reshape(P, 525)
+    lpf, rows = o.lines_per_frame, o.field_shape[0] + 1  # the lines the resamplers read
+    ll = o.array(0, "linelocs").reshape(P, lpf)
+    llc = o.array(0, "linelocs_coarse").reshape(P, lpf)
     for f in inside:
-        assert np.array_equal(llc[f, :264], g["linelocs_coarse"][f, :264])
-        assert np.abs(ll[f, :264] - g["linelocs"][f, :264]).max() < 1e-6
+        assert np.array_equal(llc[f, :rows], g["linelocs_coarse"][f, :rows])
+        assert np.abs(ll[f, :rows] - g["linelocs"][f, :rows]).max() < 1e-6

@@ -170,6 +170,9 @@ lib.cuvhs_field_height.argtypes = [_vp]
 lib.cuvhs_field_height.restype = ctypes.c_int
 lib.cuvhs_lines_per_frame.argtypes = [_vp]
 lib.cuvhs_lines_per_frame.restype = ctypes.c_int
+lib.cuvhs_set_timing_mask.argtypes = [_vp, ctypes.c_uint]
+lib.cuvhs_stage_timeline.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_int]
+lib.cuvhs_stage_timeline.restype = ctypes.c_int
 lib.cuvhs_decode_chunk_async.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int,
                                          ctypes.POINTER(Output)]
 lib.cuvhs_decode_chunk_async.restype = ctypes.c_int
@@ -208,7 +211,8 @@ EXPORTED = [
     "cuvhs_decode_chunk_async", "cuvhs_flush", "cuvhs_ire0_hz", "cuvhs_stage_fm_demod",
     "cuvhs_stage_discover_vsyncs", "cuvhs_stage_sync_pulses", "cuvhs_stage_line_locations",
     "cuvhs_stage_hsync_refine", "cuvhs_stage_tbc_resample", "cuvhs_stage_chroma_decode",
-    "cuvhs_field_width", "cuvhs_field_height", "cuvhs_lines_per_frame",
+    "cuvhs_field_width", "cuvhs_field_height", "cuvhs_lines_per_frame", "cuvhs_stage_timeline",
+    "cuvhs_set_timing_mask",
 ]
 
 
@@ -466,7 +470,15 @@ class Decoder:
     def stream(self) -> int:
         return lib.cuvhs_stream(self._h) or 0
 
-    def set_timing(self, on=True):
+    def set_timing(self, on=True, stages=None):
+        """Per-stage CUDA-event timing; `stages` (names) restricts the events
+        to those stages (default all)."""
+        if stages is None:
+            mask = 0xFFFFFFFF
+        else:
+            names = [lib.cuvhs_stage_name(i).decode() for i in range(lib.cuvhs_stage_count())]
+            mask = sum(1 << names.index(n) for n in stages)
+        lib.cuvhs_set_timing_mask(self._h, mask)
         lib.cuvhs_set_timing(self._h, 1 if on else 0)
 
     def reset_stage_times(self):
@@ -478,6 +490,17 @@ class Decoder:
         la = (ctypes.c_longlong * n)()
         lib.cuvhs_stage_times(self._h, ms, la, n)
         return {lib.cuvhs_stage_name(i).decode(): (ms[i], la[i]) for i in range(n)}
+
+    def stage_timeline(self):
+        """[(stage name, start ms, end ms)] of the last chunk's device stages
+        (timing on), from its first timed event."""
+        n = lib.cuvhs_stage_timeline(self._h, None, None, None, 0)
+        st = np.zeros(n, np.int32)
+        a = np.zeros(n)
+        b = np.zeros(n)
+        if n:
+            lib.cuvhs_stage_timeline(self._h, st.ctypes.data, a.ctypes.data, b.ctypes.data, n)
+        return [(lib.cuvhs_stage_name(int(k)).decode(), float(x), float(y)) for k, x, y in zip(st, a, b)]
 
     @property
     def launch_count(self) -> int:

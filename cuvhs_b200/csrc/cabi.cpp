@@ -265,6 +265,10 @@ long long cuvhs_json(const cuvhs_ctx* ctx, const cuvhs_output* out, char* dst, l
 
 void* cuvhs_stream(const cuvhs_ctx* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
 
+void cuvhs_set_timing_mask(cuvhs_ctx* ctx, unsigned mask) {
+  if (ctx) ctx->c.timing_mask = mask;
+}
+
 void cuvhs_set_timing(cuvhs_ctx* ctx, int on) {
   if (ctx) ctx->c.timing = on != 0;
 }
@@ -281,6 +285,18 @@ int cuvhs_stage_times(const cuvhs_ctx* ctx, double* ms, long long* launches, int
     if (launches) launches[i] = ctx->c.stage_launches[i];
   }
   return cuvhs::kNumStages;
+}
+
+int cuvhs_stage_timeline(const cuvhs_ctx* ctx, int* stage, double* start_ms, double* end_ms, int cap) {
+  if (!ctx) return 0;
+  const auto& t = ctx->c.timeline;
+  const int n = std::min(cap, (int)t.size());
+  for (int i = 0; i < n; i++) {
+    if (stage) stage[i] = t[i].stage;
+    if (start_ms) start_ms[i] = t[i].start;
+    if (end_ms) end_ms[i] = t[i].end;
+  }
+  return (int)t.size();
 }
 
 void cuvhs_reset_stage_times(cuvhs_ctx* ctx) {

@@ -81,11 +81,15 @@ cudaEvent_t Context::next_event() {
 }
 
 void Context::begin_stage(int stage, cudaEvent_t& a) {
-  (void)stage;
   a = nullptr;
-  if (!timing) return;
+  if (!timing || !((timing_mask >> stage) & 1u)) return;
   a = next_event();
   cudaEventRecord(a, stream);
+  if (t0_pending) {
+    ev_t0 = a;
+    t0_pending = false;
+    timeline.clear();
+  }
 }
 
 void Context::end_stage(int stage, cudaEvent_t a, int kernels) {
@@ -102,9 +106,12 @@ void Context::collect_stage_times() {
   for (const Mark& m : marks) {
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, m.a, m.b) == cudaSuccess) stage_ms[m.stage] += ms;
+    float s0 = 0.0f;
+    if (ev_t0 && cudaEventElapsedTime(&s0, ev_t0, m.a) == cudaSuccess) timeline.push_back({m.stage, s0, s0 + ms});
   }
   marks.clear();
-  pool_used = 0;
+  // events stay recorded until the chunk's timeline is complete
+  if (!ev_t0) pool_used = 0;
 }
 
 void Context::release() {
@@ -761,6 +768,12 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
                            int num_fields, ChunkResult& res, uint16_t* dst_luma, uint16_t* dst_chroma,
                            const uint8_t* cap_base, size_t cap_n, bool defer) {
   res = ChunkResult();
+  if (timing) {  // a new timeline (an earlier chunk that failed left its marks behind)
+    marks.clear();
+    pool_used = 0;
+    ev_t0 = nullptr;
+    t0_pending = true;
+  }
   // Unless the caller defers them and the chunk succeeded, no copy into
   // caller memory or pinned staging is still in flight when this returns.
   struct CopyDrain {
@@ -1065,6 +1078,8 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
       return false;
     }
     collect_stage_times();
+    ev_t0 = nullptr;  // the chunk's timeline is complete: its events may be reused
+    pool_used = 0;
     if (!check_cuda("decode")) return false;
   }
   host_phase(kHostFinalWait, t_host);

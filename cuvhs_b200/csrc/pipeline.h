@@ -157,6 +157,7 @@ struct Context {
 
   // per-stage device time (CUDA events on the decode stream) and launch count
   bool timing = false;
+  unsigned timing_mask = ~0u;  // device stages bracketed by events while timing (bit = Stage)
   double stage_ms[kNumStages] = {};
   long long stage_launches[kNumStages] = {};
   long long launches = 0;
@@ -165,6 +166,14 @@ struct Context {
     cudaEvent_t a, b;
   };
   std::vector<Mark> marks;
+  // the last chunk's device stage intervals, ms from its first timed event
+  struct Span {
+    int stage;
+    double start, end;
+  };
+  std::vector<Span> timeline;
+  cudaEvent_t ev_t0 = nullptr;  // first timed event of the current chunk
+  bool t0_pending = false;      // the next begin_stage opens a new chunk's timeline
   std::vector<cudaEvent_t> event_pool;
   size_t pool_used = 0;
   cudaEvent_t next_event();

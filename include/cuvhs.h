@@ -168,10 +168,19 @@ void* cuvhs_stream(const cuvhs_ctx* ctx);
  * number of stages.  No counterpart in the reference, which has no
  * per-stage timers. */
 void cuvhs_set_timing(cuvhs_ctx* ctx, int on);
+/* Which device stages the timing brackets with events (bit i = stage i;
+ * default all).  Each bracket costs host time on the decode's critical path,
+ * so a throughput measurement times only the stage it reports. */
+void cuvhs_set_timing_mask(cuvhs_ctx* ctx, unsigned mask);
 int cuvhs_stage_count(void);
 const char* cuvhs_stage_name(int i);
 int cuvhs_stage_times(const cuvhs_ctx* ctx, double* ms, long long* launches, int cap);
 void cuvhs_reset_stage_times(cuvhs_ctx* ctx);
+/* With timing on, the last chunk decode's device stage intervals in launch
+ * order: stage index and start / end in ms from the chunk's first timed event
+ * (so the gaps between intervals are time the GPU spent waiting on the host).
+ * Fills up to cap entries; returns the number of intervals. */
+int cuvhs_stage_timeline(const cuvhs_ctx* ctx, int* stage, double* start_ms, double* end_ms, int cap);
 /* Kernel launches issued since the last cuvhs_reset_stage_times. */
 long long cuvhs_launch_count(const cuvhs_ctx* ctx);
 

@@ -78,13 +78,38 @@ __global__ void __launch_bounds__(kThreadsC, 1) prefilter_kernel(ChromaArgs a) {
   }
 }
 
-// Heterodyned, resampled chroma sample of chunk line gl at column c.
-__device__ __forceinline__ float het_sample(const ChromaArgs& a, int gl, int c) {
+// Per-line constants of the heterodyne resampler: the line's start and length
+// (chunk samples), its first output index and the track's quarter-turn
+// carrier rotation.  ok is false for lines past the line-location table.
+struct HetLine {
+  double a0, span;
+  int ubase;  // row * out_w
+  float lpf;  // 0.5 * ((row * rot) & 3): the rotation in half turns
+  bool ok;
+};
+
+__device__ __forceinline__ HetLine het_line(const ChromaArgs& a, int gl) {
+  HetLine L;
   const int field = gl / a.out_h, row = gl % a.out_h;
-  if (row + 1 >= a.lines_per_frame) return 0.0f;
-  const double a0 = a.ll[(size_t)field * a.lines_per_frame + row];
-  const double a1 = a.ll[(size_t)field * a.lines_per_frame + row + 1];
-  const double coord = a0 + __ldg(&a.col_frac[c]) * (a1 - a0);
+  L.ok = row + 1 < a.lines_per_frame;
+  L.a0 = 0.0;
+  L.span = 0.0;
+  if (L.ok) {
+    const double a0 = a.ll[(size_t)field * a.lines_per_frame + row];
+    const double a1 = a.ll[(size_t)field * a.lines_per_frame + row + 1];
+    L.a0 = a0;
+    L.span = a1 - a0;
+  }
+  const int rot = a.track[field] ? 1 : 3;
+  L.lpf = 0.5f * (float)((row * rot) & 3);
+  L.ubase = row * a.out_w;
+  return L;
+}
+
+// Heterodyned, resampled chroma sample of line L at column c (frac = c / out_w).
+__device__ __forceinline__ float het_at(const ChromaArgs& a, const HetLine& L, double frac, int c) {
+  if (!L.ok) return 0.0f;
+  const double coord = L.a0 + frac * L.span;
   const int ci = (int)coord;
   if (ci < 1 || (long long)ci + 2 >= a.total) return 0.0f;
   const float x = (float)(coord - (double)ci);
@@ -95,16 +120,14 @@ __device__ __forceinline__ float het_sample(const ChromaArgs& a, int gl, int c) 
   const float c3 = 3.0f * (p1 - p2) + p3 - p0;
   const float v = p1 + 0.5f * x * (c1 + x * (c2 + x * c3));
   // carrier phase in FP64 turns, reduced before the FP32 cosine
-  const int rot = a.track[field] ? 1 : 3;
-  const int lp = (row * rot) & 3;
-  const double u = a.het_scale * (double)(row * a.out_w + c);
+  const double u = a.het_scale * (double)(L.ubase + c);
   const float fr = (float)(u - floor(u));
-  const float het = -cospif(2.0f * fr + 0.5f * (float)lp);
+  const float het = -cospif(2.0f * fr + L.lpf);
   return v * het;
 }
 
 template <int N>
-__global__ void __launch_bounds__(32 * line_warps<N>()) lines_kernel(ChromaArgs a, int line0, int nlines,
+__global__ void __launch_bounds__(32 * line_warps<N>(), N <= 1024 ? 4 : 1) lines_kernel(ChromaArgs a, int line0, int nlines,
                                                                     int write_output) {
   constexpr int W = line_warps<N>();
   __shared__ float2 sm_all[W][fft_pad(N)];
@@ -114,11 +137,19 @@ __global__ void __launch_bounds__(32 * line_warps<N>()) lines_kernel(ChromaArgs 
   const int la = 2 * pair, lb = la + 1;  // relative to line0
   if (la >= nlines) return;               // whole warp leaves together
   const bool has_b = lb < nlines;
+  const HetLine A = het_line(a, line0 + la);
+  HetLine B = A;
+  if (has_b) B = het_line(a, line0 + lb);
+  B.ok = B.ok && has_b;
+  // the gather is latency bound: unrolled so that several columns' loads are
+  // in flight (the FFT below sets the register budget, not this loop)
+#pragma unroll 4
   for (int c = lane; c < N; c += 32) {
     float va = 0.0f, vb = 0.0f;
     if (c < a.out_w) {
-      va = het_sample(a, line0 + la, c);
-      if (has_b) vb = het_sample(a, line0 + lb, c);
+      const double frac = __ldg(&a.col_frac[c]);
+      va = het_at(a, A, frac, c);
+      vb = het_at(a, B, frac, c);
     }
     sm[pidx(c)] = make_float2(va, vb);
   }
@@ -205,6 +236,8 @@ void launch_chroma_lines(const ChromaArgs& a, int field0, int nfields, bool writ
   if (nlines <= 0) return;
   const int pairs = (nlines + 1) / 2;
   auto go = [&](auto kernel, int warps) {
+    // the largest shared-memory carveout, so that the register limit sets the CTAs per SM
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     kernel<<<(pairs + warps - 1) / warps, 32 * warps, 0, st>>>(a, field0 * a.out_h, nlines, write_output ? 1 : 0);
   };
   if (a.line_fft == 2048) go(lines_kernel<2048>, line_warps<2048>());

@@ -41,7 +41,7 @@ class CuvhsError(RuntimeError):
 class Config(ctypes.Structure):
     _fields_ = [("system", ctypes.c_int), ("sample_rate_mhz", ctypes.c_double), ("device", ctypes.c_int),
                 ("batch_fields", ctypes.c_int), ("stream_mode", ctypes.c_int), ("input_format", ctypes.c_int),
-                ("dc_correct", ctypes.c_int)]
+                ("dc_correct", ctypes.c_int), ("single_pass_lines", ctypes.c_int)]
 
 
 class FieldInfo(ctypes.Structure):
@@ -336,10 +336,11 @@ class Decoder:
     SYSTEMS = {"NTSC": 0, "PAL": 1}
 
     def __init__(self, sample_rate_mhz=28.0, device=0, batch_fields=0, stream_mode=False, debug=False,
-                 input_format="u8", dc_correct=False, system="NTSC"):
+                 input_format="u8", dc_correct=False, system="NTSC", single_pass_lines=False):
         cfg = Config()
         lib.cuvhs_default_config(ctypes.byref(cfg))
         cfg.system = self.SYSTEMS[system.upper()]
+        cfg.single_pass_lines = 1 if single_pass_lines else 0
         cfg.sample_rate_mhz = float(sample_rate_mhz)
         cfg.device = int(device)
         cfg.batch_fields = int(batch_fields)

@@ -141,6 +141,7 @@ void cuvhs_default_config(cuvhs_config* cfg) {
   cfg->stream_mode = 0;
   cfg->input_format = 0;
   cfg->dc_correct = 0;
+  cfg->single_pass_lines = 0;
 }
 
 const char* cuvhs_status_string(cuvhs_status s) {

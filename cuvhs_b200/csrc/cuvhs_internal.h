@@ -273,6 +273,14 @@ void finish_lines(const Format& fmt, const LinePrep& prep, long long field_readl
                   FieldLines* pulses, int* is_first);
 void locate_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
                   long long field_readloc, LineLocState& st, FieldLines& out);
+// The reference's single-pass line locator (src/pipeline/line_locs.cu:62-543),
+// used when its host line location is off: lines_per_frame line starts and
+// the field parity (1 first, 0 second, -1 undetermined); no carried state.
+void single_pass_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
+                       double* locs, int* parity);
+// Its nominal width classes, which stand in the pulse-type list there
+// (line_locs.cu:18-49 with the thresholds of :551-558).
+void nominal_pulse_types(const Format& fmt, const int* pulse_lengths, int count, int* types);
 
 // Fixed pool of host threads for per-field work; run(n, fn) calls fn(i) for
 // i < n across the pool and the caller, and returns when all are done.

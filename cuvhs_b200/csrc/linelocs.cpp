@@ -529,3 +529,236 @@ void locate_lines(const Format& fmt, const int* pulse_starts, const int* pulse_l
 }
 
 }  // namespace cuvhs
+
+namespace cuvhs {
+
+// The single-pass line locator the reference runs when its host line
+// location is switched off (CUVHS_K2B_DISABLE; src/pipeline/line_locs.cu:62-543,
+// one GPU thread per field there, a host pool task here): width classes
+// adapted to the field's mean hsync width, the blanking state machine for the
+// reference pulse and the field parity, the mean line from the longest hsync
+// run, then the nominal grid snapped to the nearest hsync marker.  No state
+// is carried between fields.  Where the reference's device code evaluates
+// a + b * c, the fused multiply-add its compiler forms is written out.
+void nominal_pulse_types(const Format& fmt, const int* lengths, int count, int* types) {
+  const double tol = 0.5e-6 * fmt.fs_hz;
+  const double h_lo = fmt.hsync_width - tol, h_hi = fmt.hsync_width + tol;
+  const double e_lo = fmt.eq_pulse_width - tol, e_hi = fmt.eq_pulse_width + tol;
+  const double v_lo = fmt.vsync_width * 0.5, v_hi = fmt.vsync_width + 1.0e-6 * fmt.fs_hz;
+  for (int i = 0; i < std::min(count, kMaxPulses); i++) {
+    const double len = (double)lengths[i];
+    if (len >= v_lo && len <= v_hi) types[i] = kVsync;
+    else if (len >= h_lo && len <= h_hi) types[i] = kHsync;
+    else if (len >= e_lo && len <= e_hi) types[i] = kEq1;
+    else types[i] = kHsync;
+  }
+}
+
+void single_pass_lines(const Format& fmt, const int* starts, const int* lengths, int count, double* locs,
+                       int* parity) {
+  const int n = std::max(0, std::min(count, kMaxPulses));
+  const double tol = 0.5e-6 * fmt.fs_hz;
+  const double inl = (double)fmt.samples_per_line;
+  const double hnom = fmt.hsync_width, enom = fmt.eq_pulse_width, vnom = fmt.vsync_width;
+  // width classes shifted by the field's mean hsync width (line_locs.cu:99-135)
+  const double loose_lo = std::fma(-3.5, tol, hnom), loose_hi = std::fma(4.0, tol, hnom);
+  double hsum = 0.0;
+  int hcnt = 0;
+  for (int i = 0; i < n; i++) {
+    const double len = (double)lengths[i];
+    if (len >= loose_lo && len <= loose_hi) {
+      hsum += len;
+      hcnt++;
+    }
+  }
+  const double shift = (hcnt > 0 ? hsum / hcnt : hnom) - hnom;
+  const double h_lo = hnom + shift - tol, h_hi = hnom + shift + tol;
+  const double e_lo = enom + shift - tol, e_hi = enom + shift + tol;
+  const double v_lo = (vnom + shift) * 0.5, v_hi = std::fma(2.0, tol, vnom + shift);
+  thread_local std::vector<int> type;
+  type.assign((size_t)n, kHsync);
+  for (int i = 0; i < n; i++) {
+    const double len = (double)lengths[i];
+    if (len >= v_lo && len <= v_hi) type[i] = kVsync;
+    else if (len >= h_lo && len <= h_hi) type[i] = kHsync;
+    else if (len >= e_lo && len <= e_hi) type[i] = kEq1;
+    else type[i] = kHsync;  // unclassified widths count as hsync
+  }
+  // blanking state machine: the first hsync after the vertical interval
+  // (line_locs.cu:148-201)
+  int ref = -1, last_h = -1, first_eq = -1, last_eq2 = -1, state = -1;
+  for (int i = 0; i < n; i++) {
+    const int t = type[i];
+    if (state == -1) {
+      if (t == kHsync) {
+        state = kHsync;
+        last_h = i;
+      }
+    } else if (state == kHsync) {
+      if (t == kHsync) last_h = i;
+      else if (t == kEq1) {
+        state = kEq1;
+        first_eq = i;
+      } else if (t == kVsync) state = kVsync;
+    } else if (state == kEq1) {
+      if (t == kVsync) state = kVsync;
+      else if (t == kHsync) {
+        state = kHsync;
+        last_h = i;
+        first_eq = -1;
+      }
+    } else if (state == kVsync) {
+      if (t == kEq1) {
+        state = kEq2;
+        last_eq2 = i;
+      } else if (t == kHsync) {
+        ref = i;
+        break;
+      }
+    } else if (state == kEq2) {
+      if (t == kEq1) last_eq2 = i;
+      else if (t == kHsync) {
+        if (last_eq2 < 0) last_eq2 = i - 1;
+        ref = i;
+        break;
+      }
+    }
+  }
+  // field parity from the half-line spacing entering or leaving the interval
+  // (line_locs.cu:203-236)
+  const bool ntsc = fmt.system == kNtsc;
+  int par = -1;
+  if (ref >= 0 && last_h >= 0 && first_eq >= 0) {
+    const double lines = (double)(starts[first_eq] - starts[last_h]) / inl;
+    par = ntsc ? (lines > 0.75 ? 1 : 0) : (lines > 0.75 ? 0 : 1);
+  }
+  if (par < 0 && ref >= 0 && last_eq2 >= 0) {
+    const double lines = (double)(starts[ref] - starts[last_eq2]) / inl;
+    par = ntsc ? (lines > 0.75 ? 1 : 0) : (lines > 0.75 ? 0 : 1);
+  }
+  *parity = par;
+  // mean line length over the longest hsync run (line_locs.cu:246-284)
+  int best_s = -1, best_n = 0, cur_s = -1, cur_n = 0;
+  for (int i = 0; i < n; i++) {
+    if (type[i] == kHsync) {
+      if (cur_s == -1) {
+        cur_s = i;
+        cur_n = 1;
+      } else {
+        cur_n++;
+      }
+    } else {
+      if (cur_n > best_n) {
+        best_s = cur_s;
+        best_n = cur_n;
+      }
+      cur_s = -1;
+      cur_n = 0;
+    }
+  }
+  if (cur_n > best_n) {
+    best_s = cur_s;
+    best_n = cur_n;
+  }
+  double mll = inl;
+  if (best_n >= 2) {
+    double sum = 0.0;
+    int cnt = 0;
+    for (int i = best_s + 1; i < best_s + best_n; i++) {
+      const double sp = (double)(starts[i] - starts[i - 1]);
+      if (sp >= inl * 0.95 && sp <= inl * 1.05) {
+        sum += sp;
+        cnt++;
+      }
+    }
+    if (cnt > 0) mll = sum / cnt;
+  }
+  // reference position and line (line_locs.cu:295-337): a reference found in
+  // the second half of the list belongs to the next field's interval
+  double ref_pos, ref_line;
+  if (ref >= 0) {
+    ref_pos = (double)starts[ref];
+    ref_line = 10.0;
+    if (ref > n / 2) {
+      const double back = ref_pos - (double)fmt.samples_per_field;
+      if (back > 0.0) ref_pos = back;
+    }
+  } else {
+    ref = 0;
+    for (int i = 0; i < n; i++)
+      if (type[i] == kHsync) {
+        ref = i;
+        break;
+      }
+    ref_pos = n > 0 ? (double)starts[ref] : 0.0;
+    ref_line = 0.0;
+  }
+  // line markers: an EQ pulse followed closely by a tiny hsync fragment stands
+  // for the line, and the fragment is dropped (line_locs.cu:365-399)
+  thread_local std::vector<int> mk_s, mk_l, hs;
+  mk_s.clear();
+  mk_l.clear();
+  const double tiny = hnom * 0.75, gap = inl * 0.25;
+  for (int i = 0; i < n; i++) {
+    const bool eq = type[i] == kEq1 || type[i] == kEq2;
+    const bool surrogate = eq && i + 1 < n && type[i + 1] == kHsync && (double)lengths[i + 1] <= tiny &&
+                           (double)(starts[i + 1] - starts[i]) <= gap;
+    const bool fragment = type[i] == kHsync && (double)lengths[i] <= tiny && i > 0 &&
+                          (type[i - 1] == kEq1 || type[i - 1] == kEq2) && (double)(starts[i] - starts[i - 1]) <= gap;
+    if (surrogate || (type[i] == kHsync && !fragment)) {
+      mk_s.push_back(starts[i]);
+      mk_l.push_back(lengths[i]);
+    }
+  }
+  // one marker per line interval: the one whose width is nearest the nominal
+  // hsync (line_locs.cu:401-425)
+  hs.clear();
+  const double dup = inl * 0.75;
+  const int nm = (int)mk_s.size();
+  for (int c0 = 0; c0 < nm;) {
+    int best = c0;
+    double score = std::fabs((double)mk_l[c0] - hnom);
+    int c1 = c0 + 1;
+    while (c1 < nm && (double)(mk_s[c1] - mk_s[c0]) < dup) {
+      const double sc = std::fabs((double)mk_l[c1] - hnom);
+      if (sc < score || (sc == score && mk_s[c1] < mk_s[best])) {
+        best = c1;
+        score = sc;
+      }
+      c1++;
+    }
+    hs.push_back(mk_s[best]);
+    c0 = c1;
+  }
+  // nominal grid snapped to the nearest marker ahead of a monotonic cursor
+  // (line_locs.cu:429-470)
+  const double max_d = mll / 1.5;
+  const int nh = (int)hs.size();
+  int cur = 0;
+  for (int line = 0; line < fmt.lines_per_frame; line++) {
+    const double expected = std::fma(mll, (double)line - ref_line, ref_pos);
+    locs[line] = expected;
+    if (cur >= nh) continue;
+    double best_d = max_d;
+    int best_pos = -1;
+    for (int s = cur; s < nh; s++) {
+      const double d = std::fabs((double)hs[s] - expected);
+      if (d <= best_d) {
+        best_d = d;
+        best_pos = hs[s];
+        cur = s;
+      }
+      if (s + 1 < nh) {
+        if (std::fabs((double)hs[s + 1] - expected) > d) break;
+      } else {
+        break;
+      }
+    }
+    if (best_pos >= 0) {
+      locs[line] = (double)best_pos;
+      cur++;
+    }
+  }
+}
+
+}  // namespace cuvhs

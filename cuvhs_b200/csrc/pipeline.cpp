@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <chrono>
 #include <climits>
 #include <cmath>
@@ -768,6 +769,8 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
                            int num_fields, ChunkResult& res, uint16_t* dst_luma, uint16_t* dst_chroma,
                            const uint8_t* cap_base, size_t cap_n, bool defer) {
   res = ChunkResult();
+  // the reference reads its switch on every chunk (pipeline.cu:1694)
+  single_pass = cfg.single_pass_lines != 0 || std::getenv("CUVHS_K2B_DISABLE") != nullptr;
   if (timing) {  // a new timeline (an earlier chunk that failed left its marks behind)
     marks.clear();
     pool_used = 0;
@@ -968,18 +971,25 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   pool->run(P, [&](int f) {
     thread_local std::vector<int> ps, pl;
     window_pulses(run_start, run_end, (long long)offs[f], spp, ps, pl);
-    prepare_lines(fmt, ps.data(), pl.data(), (int)ps.size(), preps[f], hp_ll + (size_t)f * LPF);
+    if (single_pass) single_pass_lines(fmt, ps.data(), pl.data(), (int)ps.size(), hp_ll + (size_t)f * LPF, &h_is_first[f]);
+    else prepare_lines(fmt, ps.data(), pl.data(), (int)ps.size(), preps[f], hp_ll + (size_t)f * LPF);
     if (debug) {
       dbg_k2c[f] = (int)ps.size();
       std::copy(ps.begin(), ps.end(), dbg_k2s.begin() + (size_t)f * kMaxPulses);
       std::copy(pl.begin(), pl.end(), dbg_k2l.begin() + (size_t)f * kMaxPulses);
+      if (single_pass) {  // no validation: the raw pulses with their nominal classes
+        dbg_k2bc[f] = (int)ps.size();
+        std::copy(ps.begin(), ps.end(), dbg_k2bs.begin() + (size_t)f * kMaxPulses);
+        std::copy(pl.begin(), pl.end(), dbg_k2bl.begin() + (size_t)f * kMaxPulses);
+        nominal_pulse_types(fmt, pl.data(), (int)pl.size(), dbg_k2bt.data() + (size_t)f * kMaxPulses);
+      }
     }
   });
   host_phase(kHostPrepare, t_host);
   t_host = host_clock();
   // stateful part in field order
   FieldLines fl;
-  for (int f = 0; f < P; f++) {
+  for (int f = 0; f < P && !single_pass; f++) {
     int first = -1;
     finish_lines(fmt, preps[f], (long long)(raw_offset + offs[f]), lls, hp_ll + (size_t)f * LPF,
                  debug ? &fl : nullptr, &first);

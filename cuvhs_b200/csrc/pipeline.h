@@ -69,6 +69,7 @@ struct Context {
   int in_fmt = 0;         // InputFormat of the capture samples
   int bps = 1;            // bytes per capture sample
   bool dc_correct = false;
+  bool single_pass = false;  // the single-pass line locator (config or CUVHS_K2B_DISABLE, read per chunk)
   int cur_n_read = 0;     // samples read into the current chunk window
   float* d_dc = nullptr;  // chunk DC mean (DC correction)
   unsigned long long* d_dcsum = nullptr;

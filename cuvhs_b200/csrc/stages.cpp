@@ -4,6 +4,7 @@
 // They run the same kernels and host helpers as Context::decode_chunk, on the
 // context's stream and scratch, and share its carried state.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -121,11 +122,19 @@ cuvhs_status cuvhs_stage_line_locations(cuvhs_ctx* ctx, uint64_t raw_offset, con
   c.err.clear();
   if (n_fields < 0) return bad(c, "n_fields must not be negative");
   const int LPF = c.fmt.lines_per_frame;
+  const bool single = c.cfg.single_pass_lines != 0 || std::getenv("CUVHS_K2B_DISABLE") != nullptr;
   cuvhs::FieldLines fl;
   for (int f = 0; f < n_fields; f++) {
     const int n = std::max(0, std::min<int>(counts[f], cuvhs::kMaxPulses));
-    cuvhs::locate_lines(c.fmt, starts + (size_t)f * cuvhs::kMaxPulses, lengths + (size_t)f * cuvhs::kMaxPulses, n,
-                        (long long)(raw_offset + (uint64_t)field_offsets[f]), c.lls, fl);
+    const int* ps = starts + (size_t)f * cuvhs::kMaxPulses;
+    const int* pl = lengths + (size_t)f * cuvhs::kMaxPulses;
+    if (single) {  // line_locs (src/pipeline/line_locs.cu:544-593), no carried state
+      int parity = -1;
+      cuvhs::single_pass_lines(c.fmt, ps, pl, n, linelocs + (size_t)f * LPF, &parity);
+      if (is_first_field) is_first_field[f] = parity;
+      continue;
+    }
+    cuvhs::locate_lines(c.fmt, ps, pl, n, (long long)(raw_offset + (uint64_t)field_offsets[f]), c.lls, fl);
     std::copy(fl.locs.begin(), fl.locs.begin() + LPF, linelocs + (size_t)f * LPF);
     if (is_first_field) is_first_field[f] = fl.is_first;
   }

@@ -69,6 +69,9 @@ typedef struct cuvhs_config {
   int stream_mode;        /* non-zero caps the chunk at 64 fields (pipe input) */
   int input_format;       /* --format: 0 = u8, 1 = s16, 2 = u16 (src/io/raw_reader.cpp:71-91) */
   int dc_correct;         /* --dc-correct: subtract each chunk's mean sample (raw_reader.cpp:93-99) */
+  int single_pass_lines;  /* 1: the reference's single-pass line locator (src/pipeline/line_locs.cu) in
+                             place of its validated host line location, as the reference runs with the
+                             CUVHS_K2B_DISABLE environment variable set (which does the same here) */
 } cuvhs_config;
 
 /* Per-field metadata, one .tbc.json "fields" entry. */

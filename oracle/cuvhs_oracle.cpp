@@ -8,6 +8,7 @@
 #include "cuvhs_oracle.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <atomic>
 #include <climits>
 #include <cmath>
@@ -264,6 +265,7 @@ struct oracle_ctx {
   bool keep_signals = false;
   int in_fmt = 0;         // 0 u8, 1 s16, 2 u16
   bool dc_correct = false;
+  bool single_pass = false;  // K3 line locations in place of K2b (as CUVHS_K2B_DISABLE)
   oracle::DemodFilters filt;
   int spp;
   // carried state (pipeline.h:92-97, chroma_decode.h:9-15, pipeline.cu:2575)
@@ -1250,6 +1252,170 @@ std::string make_json(const Format& fmt, const std::vector<FieldMeta>& meta) {
   return s;
 }
 
+// ======================================================== K3 line locations
+// line_locs() (line_locs.cu:544-593): the device line locator the reference
+// runs instead of K2b when CUVHS_K2B_DISABLE is set.  Phase 1 writes nominal
+// width classes into the pulse-type list (k_classify_pulses, :18-49); phase 2
+// (k_compute_linelocs, :62-543) works per field from adaptive classes.  The
+// device compiler fuses a + b * c into one rounding; std::fma restates that.
+void k3_classify(const int* lens, int npc, const Format& fmt, int* types) {  // :18-49, :551-558
+  double tol = 0.5e-6 * fmt.sample_rate;
+  double hmin = fmt.hsync_width - tol, hmax = fmt.hsync_width + tol;
+  double emin = fmt.eq_pulse_width - tol, emax = fmt.eq_pulse_width + tol;
+  double vmin = fmt.vsync_width * 0.5, vmax = fmt.vsync_width + 1.0e-6 * fmt.sample_rate;
+  for (int p = 0; p < npc && p < MAX_PULSES; p++) {
+    double len = (double)lens[p];
+    int t;
+    if (len >= vmin && len <= vmax) t = PULSE_VSYNC;
+    else if (len >= hmin && len <= hmax) t = PULSE_HSYNC;
+    else if (len >= emin && len <= emax) t = PULSE_EQ1;
+    else t = PULSE_HSYNC;
+    types[p] = t;
+  }
+}
+
+void k3_linelocs(const int* starts, const int* lengths, int npc, const Format& fmt, double* locs,
+                 int* is_first) {  // :62-543
+  const double tol = 0.5e-6 * fmt.sample_rate;
+  const double inlinelen = (double)fmt.samples_per_line;
+  const double hnom = fmt.hsync_width, enom = fmt.eq_pulse_width, vnom = fmt.vsync_width;
+  double gmin = std::fma(-3.5, tol, hnom), gmax = std::fma(4.0, tol, hnom);
+  double hs = 0.0;
+  int hc = 0;
+  for (int i = 0; i < npc; i++) {
+    double len = (double)lengths[i];
+    if (len >= gmin && len <= gmax) { hs += len; hc++; }
+  }
+  double est = (hc > 0) ? (hs / hc) : hnom;
+  double off = est - hnom;
+  double ahmin = hnom + off - tol, ahmax = hnom + off + tol;
+  double aemin = enom + off - tol, aemax = enom + off + tol;
+  double avmin = (vnom + off) * 0.5, avmax = std::fma(2.0, tol, vnom + off);
+  int types[800];
+  int n = npc < 800 ? npc : 800;
+  for (int i = 0; i < n; i++) {
+    double len = (double)lengths[i];
+    if (len >= avmin && len <= avmax) types[i] = PULSE_VSYNC;
+    else if (len >= ahmin && len <= ahmax) types[i] = PULSE_HSYNC;
+    else if (len >= aemin && len <= aemax) types[i] = PULSE_EQ1;
+    else types[i] = PULSE_HSYNC;
+  }
+  int ref = -1, last_h = -1, first_eq1 = -1, last_eq2 = -1, state = -1;
+  for (int i = 0; i < n; i++) {  // :148-201
+    int t = types[i];
+    if (state == -1) {
+      if (t == PULSE_HSYNC) { state = PULSE_HSYNC; last_h = i; }
+    } else if (state == PULSE_HSYNC) {
+      if (t == PULSE_HSYNC) last_h = i;
+      else if (t == PULSE_EQ1) { state = PULSE_EQ1; first_eq1 = i; }
+      else if (t == PULSE_VSYNC) state = PULSE_VSYNC;
+    } else if (state == PULSE_EQ1) {
+      if (t == PULSE_VSYNC) state = PULSE_VSYNC;
+      else if (t == PULSE_HSYNC) { state = PULSE_HSYNC; last_h = i; first_eq1 = -1; }
+    } else if (state == PULSE_VSYNC) {
+      if (t == PULSE_EQ1) { state = PULSE_EQ2; last_eq2 = i; }
+      else if (t == PULSE_HSYNC) { ref = i; break; }
+    } else if (state == PULSE_EQ2) {
+      if (t == PULSE_EQ1) last_eq2 = i;
+      else if (t == PULSE_HSYNC) { if (last_eq2 < 0) last_eq2 = i - 1; ref = i; break; }
+    }
+  }
+  int parity = -1;  // :203-236
+  if (ref >= 0 && last_h >= 0 && first_eq1 >= 0) {
+    double el = (double)(starts[first_eq1] - starts[last_h]) / inlinelen;
+    parity = !fmt.pal ? (el > 0.75 ? 1 : 0) : (el > 0.75 ? 0 : 1);
+  }
+  if (parity < 0 && ref >= 0 && last_eq2 >= 0) {
+    double xl = (double)(starts[ref] - starts[last_eq2]) / inlinelen;
+    parity = !fmt.pal ? (xl > 0.75 ? 1 : 0) : (xl > 0.75 ? 0 : 1);
+  }
+  *is_first = parity;
+  int brs = -1, brl = 0, crs = -1, crl = 0;  // :246-284
+  for (int i = 0; i < n; i++) {
+    if (types[i] == PULSE_HSYNC) {
+      if (crs == -1) { crs = i; crl = 1; } else crl++;
+    } else {
+      if (crl > brl) { brs = crs; brl = crl; }
+      crs = -1;
+      crl = 0;
+    }
+  }
+  if (crl > brl) { brs = crs; brl = crl; }
+  double mll = inlinelen;
+  if (brl >= 2) {
+    double sum = 0.0;
+    int cnt = 0;
+    for (int i = brs + 1; i < brs + brl; i++) {
+      double sp = (double)(starts[i] - starts[i - 1]);
+      if (sp >= inlinelen * 0.95 && sp <= inlinelen * 1.05) { sum += sp; cnt++; }
+    }
+    if (cnt > 0) mll = sum / cnt;
+  }
+  double ref_pos, ref_line;  // :295-337
+  if (ref >= 0) {
+    ref_pos = (double)starts[ref];
+    ref_line = 10.0;
+    if (ref > n / 2) {
+      double corr = ref_pos - (double)fmt.samples_per_field;
+      if (corr > 0.0) ref_pos = corr;
+    }
+  } else {
+    ref = 0;
+    for (int i = 0; i < n; i++) if (types[i] == PULSE_HSYNC) { ref = i; break; }
+    ref_pos = (double)starts[ref];
+    ref_line = 0.0;
+  }
+  int ms[800], ml[800], mc = 0;  // :365-399
+  double tiny = hnom * 0.75, sgap = inlinelen * 0.25;
+  for (int i = 0; i < n && mc < 800; i++) {
+    bool sur = false;
+    if ((types[i] == PULSE_EQ1 || types[i] == PULSE_EQ2) && i + 1 < n && types[i + 1] == PULSE_HSYNC &&
+        (double)lengths[i + 1] <= tiny && (double)(starts[i + 1] - starts[i]) <= sgap)
+      sur = true;
+    bool sup = false;
+    if (types[i] == PULSE_HSYNC && (double)lengths[i] <= tiny && i > 0 &&
+        (types[i - 1] == PULSE_EQ1 || types[i - 1] == PULSE_EQ2) && (double)(starts[i] - starts[i - 1]) <= sgap)
+      sup = true;
+    if (sur || (types[i] == PULSE_HSYNC && !sup)) { ms[mc] = starts[i]; ml[mc] = lengths[i]; mc++; }
+  }
+  int hsl[800], nh = 0;  // :401-425
+  double dgap = inlinelen * 0.75;
+  int c0 = 0;
+  while (c0 < mc && nh < 800) {
+    int bi = c0;
+    double bs = std::fabs((double)ml[c0] - hnom);
+    int c1 = c0 + 1;
+    while (c1 < mc && (double)(ms[c1] - ms[c0]) < dgap) {
+      double sc = std::fabs((double)ml[c1] - hnom);
+      if (sc < bs || (sc == bs && ms[c1] < ms[bi])) { bi = c1; bs = sc; }
+      c1++;
+    }
+    hsl[nh++] = ms[bi];
+    c0 = c1;
+  }
+  double maxd = mll / 1.5;  // :429-470
+  int cur = 0;
+  for (int line = 0; line < fmt.lines_per_frame; line++) {
+    double expected = std::fma(mll, (double)line - ref_line, ref_pos);
+    locs[line] = expected;
+    if (cur >= nh) continue;
+    double bd = maxd;
+    int bp = -1, sidx = cur;
+    while (sidx < nh) {
+      double d = std::fabs((double)hsl[sidx] - expected);
+      if (d <= bd) { bd = d; bp = hsl[sidx]; cur = sidx; }
+      if (sidx + 1 < nh) {
+        double nd = std::fabs((double)hsl[sidx + 1] - expected);
+        if (nd > d) break;
+      } else {
+        break;
+      }
+      sidx++;
+    }
+    if (bp >= 0) { locs[line] = (double)bp; cur++; }
+  }
+}
+
 // ======================================================== chunk driver
 // Pipeline::process_chunk (pipeline.cu:1525-2624).
 int process_chunk(oracle_ctx* c, const uint8_t* data, size_t n, size_t raw_offset, int num_fields,
@@ -1316,7 +1482,19 @@ int process_chunk(oracle_ctx* c, const uint8_t* data, size_t n, size_t raw_offse
   rec.k2bs.assign((size_t)P * MAX_PULSES, 0);
   rec.k2bl.assign((size_t)P * MAX_PULSES, 0);
   rec.k2bt.assign((size_t)P * MAX_PULSES, PULSE_HSYNC);
-  for (int f = 0; f < P; f++) {
+  // pipeline.cu:1694: the switch is read on every chunk
+  const bool k2b_disabled = c->single_pass || std::getenv("CUVHS_K2B_DISABLE") != nullptr;
+  for (int f = 0; f < P && k2b_disabled; f++) {  // pipeline.cu:1848-1856: K3 leaves the pulses as found
+    int npc = std::max(0, std::min(rec.k2c[f], MAX_PULSES));
+    const int* ps = rec.k2s.data() + (size_t)f * MAX_PULSES;
+    const int* pl = rec.k2l.data() + (size_t)f * MAX_PULSES;
+    std::copy(ps, ps + npc, rec.k2bs.begin() + (size_t)f * MAX_PULSES);
+    std::copy(pl, pl + npc, rec.k2bl.begin() + (size_t)f * MAX_PULSES);
+    k3_classify(pl, npc, fmt, rec.k2bt.data() + (size_t)f * MAX_PULSES);
+    rec.k2bc[f] = npc;
+    k3_linelocs(ps, pl, npc, fmt, ll.data() + (size_t)f * LPF, &is_first[f]);
+  }
+  for (int f = 0; f < P && !k2b_disabled; f++) {
     int before = std::max(0, std::min(rec.k2c[f], MAX_PULSES));
     const int* ps = rec.k2s.data() + (size_t)f * MAX_PULSES;
     std::vector<VPulse> vp = refine_pulses(ps, rec.k2l.data() + (size_t)f * MAX_PULSES, before, fmt);
@@ -1422,6 +1600,8 @@ int oracle_lines_per_frame(const oracle_ctx* c) { return c->fmt.lines_per_frame;
 
 void oracle_destroy(oracle_ctx* c) { delete c; }
 void oracle_keep_signals(oracle_ctx* c, int keep) { c->keep_signals = keep != 0; }
+void oracle_set_single_pass(oracle_ctx* c, int on) { c->single_pass = on != 0; }
+
 void oracle_set_input(oracle_ctx* c, int format, int dc_correct) {
   c->in_fmt = format;
   c->dc_correct = dc_correct != 0;

@@ -61,6 +61,9 @@ void oracle_keep_signals(oracle_ctx* c, int keep);
  * 1 or 2 bytes per sample and n counts samples) and DC correction, as the
  * reference's --format and --dc-correct. */
 void oracle_set_input(oracle_ctx* c, int format, int dc_correct);
+/* The reference's K3 line locations in place of K2b, as its CUVHS_K2B_DISABLE
+ * environment switch (which the oracle also honours). */
+void oracle_set_single_pass(oracle_ctx* c, int on);
 
 #ifdef __cplusplus
 }

@@ -53,6 +53,7 @@ def _load():
                                          ctypes.c_longlong]
         L.oracle_keep_signals.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oracle_set_input.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.oracle_set_single_pass.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oracle_destroy.argtypes = [ctypes.c_void_p]
         _lib = L
     return _lib
@@ -65,7 +66,7 @@ class Oracle:
     FORMATS = {"u8": (0, np.uint8), "s16": (1, np.int16), "u16": (2, np.uint16)}
 
     def __init__(self, sample_rate_mhz=28.0, batch_fields=3282, threads=0, keep_signals=False, input_format="u8",
-                 dc_correct=False, system="NTSC"):
+                 dc_correct=False, system="NTSC", single_pass_lines=False):
         L = _load()
         self._h = L.oracle_create_system(float(sample_rate_mhz), int(batch_fields), int(threads),
                                          {"NTSC": 0, "PAL": 1}[system.upper()])
@@ -75,6 +76,7 @@ class Oracle:
             L.oracle_keep_signals(self._h, 1)
         fmt, self._dtype = self.FORMATS[input_format]
         L.oracle_set_input(self._h, fmt, 1 if dc_correct else 0)
+        L.oracle_set_single_pass(self._h, 1 if single_pass_lines else 0)
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:

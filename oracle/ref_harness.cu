@@ -77,6 +77,7 @@ struct Dumper {
 int main(int argc, char** argv) {
   double mhz = 28.0;
   bool pal = false;
+  long long reserve_mb = 0;
   std::string in, out, dump_dir;
   bool time_only = false;
   int dump_tiles = 2;
@@ -84,6 +85,7 @@ int main(int argc, char** argv) {
   for (int i = 1; i < argc; i++) {
     if (!strcmp(argv[i], "-f") && i + 1 < argc) mhz = atof(argv[++i]);
     else if (!strcmp(argv[i], "--system") && i + 1 < argc) pal = !strcasecmp(argv[++i], "PAL");
+    else if (!strcmp(argv[i], "--reserve-mb") && i + 1 < argc) reserve_mb = atoll(argv[++i]);
     else if (!strcmp(argv[i], "--dump") && i + 1 < argc) dump_dir = argv[++i];
     else if (!strcmp(argv[i], "--dump-tiles") && i + 1 < argc) dump_tiles = atoi(argv[++i]);
     else if (!strcmp(argv[i], "--time")) time_only = true;
@@ -91,7 +93,8 @@ int main(int argc, char** argv) {
     else if (pos == 1) { out = argv[i]; pos++; }
   }
   if (pos < 2) {
-    fprintf(stderr, "usage: ref_harness [-f MHz] [--system NTSC|PAL] [--dump DIR] [--dump-tiles N] [--time] in.u8 out_base\n");
+    fprintf(stderr, "usage: ref_harness [-f MHz] [--system NTSC|PAL] [--reserve-mb N] [--dump DIR] [--dump-tiles N] "
+                    "[--time] in.u8 out_base\n");
     return 2;
   }
 
@@ -103,7 +106,13 @@ int main(int argc, char** argv) {
   TBCWriter writer;
   if (!writer.open(out, fmt, true)) return 1;
   Pipeline pl(gpu, fmt, reader, writer);
+  // --reserve-mb: device memory held while the reference sizes its buffers
+  // (from the free memory) and released afterwards, for kernels that need
+  // local memory beyond what its default allocation leaves
+  void* reserve = nullptr;
+  if (reserve_mb > 0 && cudaMalloc(&reserve, (size_t)reserve_mb << 20) != cudaSuccess) return 1;
   if (!pl.allocate_buffers()) return 1;
+  if (reserve) cudaFree(reserve);
 
   Dumper dump;
   bool dumping = !dump_dir.empty() && !time_only;
@@ -124,6 +133,10 @@ int main(int argc, char** argv) {
     int fields_this_chunk = std::min(pl.batch_size, remaining_fields);
     size_t next_raw_offset = 0;
     int processed = pl.process_chunk(raw_offset, fields_this_chunk, next_raw_offset);
+    {
+      const cudaError_t e = cudaGetLastError();  // the reference does not check its launches
+      if (e != cudaSuccess) fprintf(stderr, "ref_harness: CUDA error after chunk %d: %s\n", chunk, cudaGetErrorString(e));
+    }
     if (processed == 0) break;
     if (dumping) {
       cudaDeviceSynchronize();

@@ -23,19 +23,41 @@ def has_gpu():
         return False
 
 
+# A case name is a workload name, or one with this suffix: the same workload
+# decoded with the single-pass line locator (the reference's CUVHS_K2B_DISABLE).
+SINGLE = "_singlepass"
+
+
+def base_name(name):
+    return name[:-len(SINGLE)] if name.endswith(SINGLE) else name
+
+
+def single_pass(name):
+    return name.endswith(SINGLE)
+
+
+def system(name):
+    import cuvhs_b200 as cv
+    return cv.system_of(base_name(name))
+
+
+def rate_mhz(name):
+    import cuvhs_b200 as cv
+    return cv.WORKLOADS[base_name(name)]["sample_rate_hz"] / 1e6
+
+
 @functools.lru_cache(maxsize=None)
 def workload(name):
     import cuvhs_b200 as cv
-    return cv.make_workload(name)
+    return cv.make_workload(base_name(name))
 
 
 @functools.lru_cache(maxsize=None)
 def oracle_decode(name):
-    """FP64 oracle decode of a named workload (cached per session)."""
-    import cuvhs_b200 as cv
+    """FP64 oracle decode of a named case (cached per session)."""
     from oracle.oracle import Oracle
     x = workload(name)
-    o = Oracle(cv.WORKLOADS[name]["sample_rate_hz"] / 1e6, system=cv.system_of(name))
+    o = Oracle(rate_mhz(name), system=system(name), single_pass_lines=single_pass(name))
     o.decode(x)
     return o
 

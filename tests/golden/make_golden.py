@@ -8,6 +8,10 @@
                         outputs to OUTDIR/<name>/
   pack DUMPDIR NAME     pack one dump into tests/golden/NAME.npz (+ NAME.tbc.json)
 
+A name ending in _singlepass is its workload decoded with the reference's
+CUVHS_K2B_DISABLE switch set (its single-pass line locator in place of the
+validated host line location).
+
 The fixtures pin the FP64 oracle (tests/test_oracle_golden.py) and the GPU
 decoder (tests/test_gpu_parity.py) to the reference's behaviour on the same
 seeded inputs.  The reference decodes its batch in one chunk; its batch size on
@@ -24,7 +28,21 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-NAMES = ["small28", "dropouts28", "plain40_28", "small28pal", "dropouts28pal"]
+NAMES = ["small28", "dropouts28", "plain40_28", "small28pal", "dropouts28pal", "small28_singlepass",
+         "dropouts28_singlepass", "small28pal_singlepass"]
+SINGLE = "_singlepass"
+
+
+def workload_of(name):
+    """(workload name, reference environment, extra harness arguments) of a
+    fixture name.  The single-pass line locator keeps four 800-entry arrays per
+    thread in local memory (about 4 GB over a B200's resident threads); the
+    reference's default allocation leaves 1.7 GB, its launch fails unchecked
+    and the decode carries zero line locations, so the harness holds 8 GB back
+    while the reference sizes its buffers."""
+    if name.endswith(SINGLE):
+        return name[:-len(SINGLE)], dict(os.environ, CUVHS_K2B_DISABLE="1"), ["--reserve-mb", "8192"]
+    return name, dict(os.environ), []
 GEOMETRY = {"NTSC": (525, 263, 910), "PAL": (625, 313, 1135)}  # line locations per field, field rows, columns
 DTYPES = {"i32": np.int32, "i64": np.int64, "f32": np.float32, "f64": np.float64}
 
@@ -41,16 +59,17 @@ def run(outdir, names):
     import cuvhs_b200 as cv
     from oracle.oracle import REF_HARNESS
     for name in names:
-        x = cv.make_workload(name)
-        mhz = cv.WORKLOADS[name]["sample_rate_hz"] / 1e6
+        wl, env, extra = workload_of(name)
+        x = cv.make_workload(wl)
+        mhz = cv.WORKLOADS[wl]["sample_rate_hz"] / 1e6
         d = os.path.join(outdir, name)
         os.makedirs(d, exist_ok=True)
         inp = os.path.join(d, "in.u8")
         x.tofile(inp)
         with open(os.path.join(d, "input.md5"), "w") as f:
             f.write(hashlib.md5(x.tobytes()).hexdigest())
-        subprocess.check_call([REF_HARNESS, "-f", str(mhz), "--system", cv.system_of(name), "--dump", d,
-                               "--dump-tiles", "1", inp, os.path.join(d, "out")],
+        subprocess.check_call([REF_HARNESS, "-f", str(mhz), "--system", cv.system_of(wl), "--dump", d,
+                               "--dump-tiles", "1"] + extra + [inp, os.path.join(d, "out")], env=env,
                               stdout=open(os.path.join(d, "harness.json"), "w"),
                               stderr=open(os.path.join(d, "harness.err"), "w"))
         os.unlink(inp)
@@ -58,8 +77,9 @@ def run(outdir, names):
 
 def pack(dumpdir, name):
     import cuvhs_b200 as cv
-    x = cv.make_workload(name)
-    lpf, rows, cols = GEOMETRY[cv.system_of(name)]
+    wl, _, _ = workload_of(name)
+    x = cv.make_workload(wl)
+    lpf, rows, cols = GEOMETRY[cv.system_of(wl)]
     ref = load_dump(dumpdir)
     meta = ref["c0_meta"]
     P = int(meta[1])
@@ -70,7 +90,7 @@ def pack(dumpdir, name):
     with open(os.path.join(HERE, name + ".tbc.json"), "w") as f:
         f.write(text)
     arrs = {"input_md5": np.array(hashlib.md5(x.tobytes()).hexdigest()), "n_input": np.array(x.size),
-            "sample_rate_mhz": np.array(cv.WORKLOADS[name]["sample_rate_hz"] / 1e6), "meta": meta}
+            "sample_rate_mhz": np.array(cv.WORKLOADS[wl]["sample_rate_hz"] / 1e6), "meta": meta}
     for key in ["field_offsets", "is_first", "do_count"]:
         arrs[key] = ref["c0_" + key]
     arrs["vsync_candidates"] = np.sort(ref["c0_vsync_candidates"])

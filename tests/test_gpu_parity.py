@@ -11,7 +11,8 @@ import numpy as np
 import pytest
 
 import cuvhs_b200 as cv
-from conftest import GOLDEN, golden, inside_fields, json_fields, oracle_decode, workload
+from conftest import (GOLDEN, golden, inside_fields, json_fields, oracle_decode, rate_mhz, single_pass, system,
+                      workload)
 
 LSB_FRACTION = 1e-3
 POS_TOL = 0.01
@@ -19,8 +20,9 @@ POS_TOL = 0.01
 
 def decode(name, batch_fields=0):
     x = workload(name)
-    mhz = cv.WORKLOADS[name]["sample_rate_hz"] / 1e6
-    with cv.Decoder(mhz, batch_fields=batch_fields, debug=True, system=cv.system_of(name)) as d:
+    mhz = rate_mhz(name)
+    with cv.Decoder(mhz, batch_fields=batch_fields, debug=True, system=system(name),
+                    single_pass_lines=single_pass(name)) as d:
         r = d.decode_capture(x)
         dbg = {k: d.debug_array(k) for k in ("field_offsets", "k2_pulse_count", "k2_pulse_starts",
                                              "k2_pulse_lengths", "k2b_pulse_count", "k2b_pulse_starts",
@@ -41,7 +43,7 @@ def compare_to_oracle(name, r, dbg, x, mhz, o, chunk_last_only=False):
     ofields = json_fields(o.json)
     mfields = json_fields(r.json)
     assert [f["fileLoc"] for f in mfields] == [f["fileLoc"] for f in ofields]
-    inside = inside_fields([f["fileLoc"] for f in mfields], x.size, mhz, cv.system_of(name))
+    inside = inside_fields([f["fileLoc"] for f in mfields], x.size, mhz, system(name))
     assert len(inside) >= r.n_fields - 1
     for i in inside:
         assert mfields[i] == ofields[i], i
@@ -53,7 +55,8 @@ def compare_to_oracle(name, r, dbg, x, mhz, o, chunk_last_only=False):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["small28", "dropouts28", "plain40_28", "small358", "small28pal",
-                                  "dropouts28pal", "pal20_40"])
+                                  "dropouts28pal", "pal20_40", "small28_singlepass", "dropouts28_singlepass",
+                                  "small28pal_singlepass"])
 def test_decoder_matches_oracle(name):
     x, mhz, r, dbg = decode(name)
     o = oracle_decode(name)
@@ -78,14 +81,15 @@ def test_decoder_matches_oracle(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["small28", "dropouts28", "plain40_28", "small28pal", "dropouts28pal"])
+@pytest.mark.parametrize("name", ["small28", "dropouts28", "plain40_28", "small28pal", "dropouts28pal",
+                                  "small28_singlepass", "dropouts28_singlepass", "small28pal_singlepass"])
 def test_decoder_matches_reference_fixture(name):
     g = golden(name)
     x, mhz, r, dbg = decode(name)
     gfields = json_fields(g["json_text"])
     mfields = json_fields(r.json)
     assert len(mfields) == len(gfields)
-    inside = inside_fields([f["fileLoc"] for f in gfields], x.size, mhz, cv.system_of(name))
+    inside = inside_fields([f["fileLoc"] for f in gfields], x.size, mhz, system(name))
     for i in inside:
         assert mfields[i] == gfields[i], i
     assert np.array_equal(dbg["field_offsets"], g["field_offsets"])

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import cuvhs_b200 as cv
-from conftest import inside_fields, json_fields, oracle_decode, workload
+from conftest import inside_fields, json_fields, oracle_decode, rate_mhz, single_pass, system, workload
 from cuvhs_b200 import stages
 
 POS_TOL = 0.01
@@ -51,17 +51,17 @@ def _run_stages(s, x):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["small28", "dropouts28", "small28pal"])
+@pytest.mark.parametrize("name", ["small28", "dropouts28", "small28pal", "dropouts28_singlepass"])
 def test_stages_in_order_reproduce_the_chunk_decode(name):
     x = workload(name)
-    mhz = cv.WORKLOADS[name]["sample_rate_hz"] / 1e6
-    system = cv.system_of(name)
-    with cv.Decoder(mhz, debug=True, system=system) as d:
+    mhz = rate_mhz(name)
+    opts = dict(system=system(name), single_pass_lines=single_pass(name))
+    with cv.Decoder(mhz, debug=True, **opts) as d:
         r = d.decode_capture(x)
         dbg = {k: d.debug_array(k) for k in ("field_offsets", "k2_pulse_count", "k2_pulse_starts",
                                              "k2_pulse_lengths", "linelocs_coarse", "linelocs", "is_first",
                                              "video", "sync", "envelope")}
-    with cv.Decoder(mhz, system=system) as s:
+    with cv.Decoder(mhz, **opts) as s:
         g = _run_stages(s, x)
         spp = s.tile_stride
     P = len(g["offs"])

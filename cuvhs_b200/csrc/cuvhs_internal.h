@@ -127,14 +127,18 @@ void launch_k1a(const DemodArgs& a, int f0, int nf, cudaStream_t st);
 // sum, one FP64 division, as the reference's FP64 loop), as FP32.
 // sum is scratch for one unsigned long long.
 void launch_dc_mean(const uint8_t* raw, int n, int in_fmt, unsigned long long* sum, float* dc, cudaStream_t st);
-void launch_k1b(const DemodArgs& a, cudaStream_t st);
+// K1b over tiles [f0, f0 + nf): every tile is filtered on its own, so it can
+// follow K1a tile range by tile range.
+void launch_k1b(const DemodArgs& a, int f0, int nf, cudaStream_t st);
 
 // Threshold edges of the sync signal in sample order: falling (x<=thr after
 // x>thr, or at 0) and rising (x>thr after x<=thr).  counts[0..1] = totals;
 // blk is scratch of edge_blocks(total) entries.
 int edge_blocks(long long total);
+// masks: scratch of edge_mask_words(total) words (per-thread edge bit masks)
+size_t edge_mask_words(long long total);
 void launch_edges(const float* sync, long long total, float thr_rel, unsigned* fall, unsigned* rise,
-                  int* counts, int cap, int2* blk, cudaStream_t st);
+                  int* counts, int cap, int2* blk, unsigned* masks, cudaStream_t st);
 
 struct LineArgs {
   const float* video;
@@ -208,7 +212,8 @@ void launch_dropouts(const DropoutArgs& a, cudaStream_t st);
 // up to a multiple of 16.
 size_t dropout_class_bytes_per_field(int spp);
 void launch_dropouts_two_pass(const DropoutArgs& a, cudaStream_t st);
-void launch_dropout_conceal_chroma(const DropoutArgs& a, cudaStream_t st);
+// Chroma concealment of fields [f0, f0 + nf) (their chroma lines final).
+void launch_dropout_conceal_chroma(const DropoutArgs& a, int f0, int nf, cudaStream_t st);
 
 // ---------------------------------------------------------------- host line locations
 // Per-field pulse validation, mean line length, vertical-blanking anchor and

@@ -198,7 +198,10 @@ __global__ void __launch_bounds__(32 * line_warps<N>(), N <= 1024 ? 4 : 1) lines
 
 // One warp per field: mean over line pairs (16+2p, 17+2p), p < 115, of the
 // mean |a + b| over the burst window.
+// BL: the burst window length when known at compile time (NTSC 36, PAL 40), 0 = a.burst_len.
+template <int BL>
 __global__ void metric_kernel(ChromaArgs a, int field0, int nfields) {
+  const int bl = BL > 0 ? BL : a.burst_len;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= nfields) return;
   const int f = field0 + warp;
@@ -207,11 +210,11 @@ __global__ void metric_kernel(ChromaArgs a, int field0, int nfields) {
   double acc = 0.0;
   for (int p = lane; p < npairs; p += 32) {
     const int line = f * a.out_h + skip + 2 * p;
-    const float* x = a.burst + (size_t)line * a.burst_len;
-    const float* y = x + a.burst_len;
+    const float* x = a.burst + (size_t)line * bl;
+    const float* y = x + bl;
     double s = 0.0;
-    for (int i = 0; i < a.burst_len; i++) s += fabs((double)x[i] + (double)y[i]);
-    acc += s / a.burst_len;
+    for (int i = 0; i < bl; i++) s += fabs((double)x[i] + (double)y[i]);
+    acc += s / bl;
   }
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
   if (lane == 0) a.metric[f] = npairs > 0 ? acc / npairs : 1e9;
@@ -248,7 +251,9 @@ void launch_burst_metric(const ChromaArgs& a, int field0, int nfields, cudaStrea
   if (nfields <= 0) return;
   const int threads = 128;
   const int blocks = (nfields * 32 + threads - 1) / threads;
-  metric_kernel<<<blocks, threads, 0, st>>>(a, field0, nfields);
+  if (a.burst_len == 36) metric_kernel<36><<<blocks, threads, 0, st>>>(a, field0, nfields);
+  else if (a.burst_len == 40) metric_kernel<40><<<blocks, threads, 0, st>>>(a, field0, nfields);
+  else metric_kernel<0><<<blocks, threads, 0, st>>>(a, field0, nfields);
 }
 
 }  // namespace cuvhs

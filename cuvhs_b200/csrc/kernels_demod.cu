@@ -191,13 +191,13 @@ __device__ __forceinline__ void k1b_emit(const DemodArgs& a, const float2 (&z)[1
 }
 
 // K1b: demod -> video + sync, blocks 2x and 2x+1 of the tile.
-__global__ void __launch_bounds__(kThreadsB, 1) k1b_kernel(DemodArgs a) {
+__global__ void __launch_bounds__(kThreadsB, 1) k1b_kernel(DemodArgs a, int f_begin) {
   constexpr int N = Design::kNb, T = kThreadsB;
   extern __shared__ float2 sm[];
   float2* sA = sm;
   float2* sB = sm + fft_pad(N);
   const int t = threadIdx.x;
-  const int f = blockIdx.y;
+  const int f = f_begin + blockIdx.y;
   const int blk0 = 2 * blockIdx.x;
   const int j0 = kOverlap + blk0 * a.b_out;
   const int tile0 = f * a.spp - kOverlap;
@@ -221,8 +221,10 @@ __global__ void __launch_bounds__(kThreadsB, 1) k1b_kernel(DemodArgs a) {
 }
 
 // Threshold edges in sample order.  Each thread owns 16 consecutive samples
-// (one 64-byte line), a CTA 4096; counts per CTA, one scan, then an ordered
-// write, so the host receives sorted falling and rising edge positions.
+// (one 64-byte line), a CTA 4096.  The count pass reads the signal once and
+// keeps each thread's 16-bit falling / rising masks; one scan turns the
+// per-CTA counts into offsets; the write pass reads only the masks and writes
+// the positions in order, so the host receives sorted edge lists.
 constexpr int kEdgeThreads = 256;
 constexpr int kEdgePer = 16;
 constexpr int kEdgeSeg = kEdgeThreads * kEdgePer;
@@ -288,54 +290,83 @@ __device__ __forceinline__ int2 block_scan2(int a, int b, int& pa, int& pb) {
 }
 
 __global__ void __launch_bounds__(kEdgeThreads) edge_count_kernel(const float* __restrict__ x, long long total,
-                                                                  float thr, int2* __restrict__ blk) {
+                                                                  float thr, int2* __restrict__ blk,
+                                                                  unsigned* __restrict__ masks) {
   const long long i0 = (long long)blockIdx.x * kEdgeSeg + (long long)threadIdx.x * kEdgePer;
   unsigned fm, rm;
   edge_masks(x, total, thr, i0, fm, rm);
+  masks[(size_t)blockIdx.x * kEdgeThreads + threadIdx.x] = fm | (rm << 16);
   int pa, pb;
   const int2 t = block_scan2(__popc(fm), __popc(rm), pa, pb);
   if (threadIdx.x == 0) blk[blockIdx.x] = t;
 }
 
-// One CTA: exclusive scan of the per-CTA counts, totals to counts[0..1].
-__global__ void __launch_bounds__(1024) edge_scan_kernel(int2* __restrict__ blk, int nblk, int* __restrict__ counts) {
-  __shared__ int2 part[1024];
-  __shared__ int2 carry;
-  if (threadIdx.x == 0) carry = make_int2(0, 0);
-  __syncthreads();
-  for (int base = 0; base < nblk; base += 1024) {
-    const int i = base + threadIdx.x;
-    const int2 v = i < nblk ? blk[i] : make_int2(0, 0);
-    part[threadIdx.x] = v;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-      int2 t = make_int2(0, 0);
-      if (threadIdx.x >= off) t = part[threadIdx.x - off];
-      __syncthreads();
-      part[threadIdx.x].x += t.x;
-      part[threadIdx.x].y += t.y;
-      __syncthreads();
+// One CTA: exclusive scan of the per-CTA counts in place, totals to
+// counts[0..1].  Thread t sums a contiguous run of ceil(nblk / 1024) counts,
+// the runs' totals are scanned with warp shuffles, then each thread writes its
+// run's offsets.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) edge_scan_kernel(int2* __restrict__ blk, int nblk,
+                                                                 int* __restrict__ counts) {
+  __shared__ int2 warp_tot[kScanThreads / 32];
+  const int per = (nblk + kScanThreads - 1) / kScanThreads;
+  const int b0 = min(nblk, (int)threadIdx.x * per), b1 = min(nblk, b0 + per);
+  int sa = 0, sb = 0;
+  for (int b = b0; b < b1; b++) {
+    const int2 v = blk[b];
+    sa += v.x;
+    sb += v.y;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int ia = sa, ib = sb;  // inclusive within the warp
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int ta = __shfl_up_sync(0xffffffffu, ia, off), tb = __shfl_up_sync(0xffffffffu, ib, off);
+    if (lane >= off) {
+      ia += ta;
+      ib += tb;
     }
-    const int2 inc = part[threadIdx.x];
-    const int2 c = carry;
-    if (i < nblk) blk[i] = make_int2(c.x + inc.x - v.x, c.y + inc.y - v.y);
-    __syncthreads();
-    if (threadIdx.x == 1023) carry = make_int2(c.x + inc.x, c.y + inc.y);
-    __syncthreads();
+  }
+  if (lane == 31) warp_tot[warp] = make_int2(ia, ib);
+  __syncthreads();
+  if (warp == 0) {
+    int wa = warp_tot[lane].x, wb = warp_tot[lane].y;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int ta = __shfl_up_sync(0xffffffffu, wa, off), tb = __shfl_up_sync(0xffffffffu, wb, off);
+      if (lane >= off) {
+        wa += ta;
+        wb += tb;
+      }
+    }
+    warp_tot[lane] = make_int2(wa, wb);  // inclusive over warps
+  }
+  __syncthreads();
+  int ca = ia - sa, cb = ib - sb;  // exclusive start of this thread's run
+  if (warp > 0) {
+    ca += warp_tot[warp - 1].x;
+    cb += warp_tot[warp - 1].y;
+  }
+  for (int b = b0; b < b1; b++) {
+    const int2 v = blk[b];
+    blk[b] = make_int2(ca, cb);
+    ca += v.x;
+    cb += v.y;
   }
   if (threadIdx.x == 0) {
-    counts[0] = carry.x;
-    counts[1] = carry.y;
+    counts[0] = warp_tot[kScanThreads / 32 - 1].x;
+    counts[1] = warp_tot[kScanThreads / 32 - 1].y;
   }
 }
 
-__global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(const float* __restrict__ x, long long total,
-                                                                  float thr, const int2* __restrict__ blk,
+__global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(long long total, const unsigned* __restrict__ masks,
+                                                                  const int2* __restrict__ blk,
                                                                   unsigned* __restrict__ fall,
                                                                   unsigned* __restrict__ rise, int cap) {
   const long long i0 = (long long)blockIdx.x * kEdgeSeg + (long long)threadIdx.x * kEdgePer;
-  unsigned fm, rm;
-  edge_masks(x, total, thr, i0, fm, rm);
+  const unsigned m = __ldg(&masks[(size_t)blockIdx.x * kEdgeThreads + threadIdx.x]);
+  unsigned fm = m & 0xFFFFu, rm = m >> 16;
+  (void)total;
   int pa, pb;
   block_scan2(__popc(fm), __popc(rm), pa, pb);
   int kf = blk[blockIdx.x].x + pa, kr = blk[blockIdx.x].y + pb;
@@ -406,23 +437,26 @@ void launch_dc_mean(const uint8_t* raw, int n, int in_fmt, unsigned long long* s
   dc_mean_kernel<<<1, 1, 0, st>>>(sum, n > 0 ? n : 1, dc);
 }
 
-void launch_k1b(const DemodArgs& a, cudaStream_t st) {
+void launch_k1b(const DemodArgs& a, int f0, int nf, cudaStream_t st) {
+  if (nf <= 0) return;
   const size_t smem = 2 * sizeof(float2) * fft_pad(Design::kNb);
   cudaFuncSetAttribute(k1b_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int blocks = (a.spp + a.b_out - 1) / a.b_out;
-  dim3 grid((blocks + 1) / 2, a.tiles);
-  k1b_kernel<<<grid, kThreadsB, smem, st>>>(a);
+  dim3 grid((blocks + 1) / 2, nf);
+  k1b_kernel<<<grid, kThreadsB, smem, st>>>(a, f0);
 }
 
 int edge_blocks(long long total) { return (int)((total + kEdgeSeg - 1) / kEdgeSeg); }
 
+size_t edge_mask_words(long long total) { return (size_t)edge_blocks(total) * kEdgeThreads; }
+
 void launch_edges(const float* sync, long long total, float thr_rel, unsigned* fall, unsigned* rise, int* counts,
-                  int cap, int2* blk, cudaStream_t st) {
+                  int cap, int2* blk, unsigned* masks, cudaStream_t st) {
   const int nblk = edge_blocks(total);
   if (nblk <= 0) return;
-  edge_count_kernel<<<nblk, kEdgeThreads, 0, st>>>(sync, total, thr_rel, blk);
-  edge_scan_kernel<<<1, 1024, 0, st>>>(blk, nblk, counts);
-  edge_write_kernel<<<nblk, kEdgeThreads, 0, st>>>(sync, total, thr_rel, blk, fall, rise, cap);
+  edge_count_kernel<<<nblk, kEdgeThreads, 0, st>>>(sync, total, thr_rel, blk, masks);
+  edge_scan_kernel<<<1, kScanThreads, 0, st>>>(blk, nblk, counts);
+  edge_write_kernel<<<nblk, kEdgeThreads, 0, st>>>(total, masks, blk, fall, rise, cap);
 }
 
 }  // namespace cuvhs

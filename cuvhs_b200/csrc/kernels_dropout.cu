@@ -348,9 +348,9 @@ __global__ void __launch_bounds__(kThreadsScan) dropout_scan_kernel(DropoutArgs 
 }
 
 // One warp per field: chroma concealment from the entries the scan kernel wrote.
-__global__ void dropout_chroma_kernel(DropoutArgs a) {
-  const int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (f >= a.fields) return;  // whole warp
+__global__ void dropout_chroma_kernel(DropoutArgs a, int f0, int nf) {
+  const int f = f0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (f >= f0 + nf || f >= a.fields) return;  // whole warp
   const int n = min(max(a.do_count[f], 0), kMaxDropouts);
   conceal(a, f, n, threadIdx.x & 31, false, true);
 }
@@ -375,10 +375,10 @@ void launch_dropouts_two_pass(const DropoutArgs& a, cudaStream_t st) {
   dropout_scan_kernel<<<a.fields, kThreadsScan, smem, st>>>(a);
 }
 
-void launch_dropout_conceal_chroma(const DropoutArgs& a, cudaStream_t st) {
-  if (a.fields <= 0) return;
+void launch_dropout_conceal_chroma(const DropoutArgs& a, int f0, int nf, cudaStream_t st) {
+  if (nf <= 0 || f0 < 0 || f0 >= a.fields) return;
   const int threads = 128;
-  dropout_chroma_kernel<<<(a.fields * 32 + threads - 1) / threads, threads, 0, st>>>(a);
+  dropout_chroma_kernel<<<(nf * 32 + threads - 1) / threads, threads, 0, st>>>(a, f0, nf);
 }
 
 }  // namespace cuvhs

@@ -199,7 +199,7 @@ bool Context::init(const cuvhs_config& c) {
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
   const size_t field_px = (size_t)fmt.output_line_len * fmt.output_field_lines;
-  const size_t per_field = (size_t)spp * (2 * bps + 4 * 5) + field_px * 8 +
+  const size_t per_field = (size_t)spp * (2 * bps + 4 * 5) + (size_t)spp / 4 + field_px * 8 +
                            (size_t)fmt.output_field_lines * kMaxBurstLen * 4 + 65536 + dropout_class_bytes_per_field(spp);
   int b = c.batch_fields;
   if (b <= 0) {
@@ -247,6 +247,7 @@ bool Context::init(const cuvhs_config& c) {
   d_rise = A((unsigned*)nullptr, edge_cap);
   d_counts = A((int*)nullptr, 4);
   d_edge_blk = A((int2*)nullptr, (size_t)edge_blocks((long long)batch * spp) + 1);
+  d_edge_mask = A((unsigned*)nullptr, edge_mask_words((long long)batch * spp));
   d_ll = A((double*)nullptr, (size_t)batch * fmt.lines_per_frame);
   const size_t F = (size_t)fmt.output_line_len * fmt.output_field_lines;
   for (int k = 0; k < 2; k++) {
@@ -580,7 +581,7 @@ bool Context::read_edges(const float* sync, long long total) {
   {
     cudaEvent_t ev_;
     begin_stage(kStageEdges, ev_);
-    launch_edges(sync, total, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, stream);
+    launch_edges(sync, total, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, d_edge_mask, stream);
     end_stage(kStageEdges, ev_, 3);
   }
   cudaMemcpyAsync(hp_counts, d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream);
@@ -663,9 +664,27 @@ void window_pulses(const std::vector<long long>& run_start, const std::vector<lo
 // from two trial passes over field 0; then every field is computed with the
 // alternating track assignment and the reference's per-15-field flip-and-retry
 // passes are replayed on the host.  Sets h_phase and the carried chroma state.
-bool Context::chroma_fields(ChromaArgs& ca, int P) {
+bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, uint16_t* dst_chroma) {
   const int H = fmt.output_field_lines;
+  const size_t F = (size_t)fmt.output_line_len * H;
   double t_host = 0.0;
+  // Fields [f0, f0 + nf) are decoded as the host's decision will most likely
+  // leave them: conceal and send them now; a retry pass that rewrites fields
+  // repeats this for them (concealment only ever runs on freshly decoded lines).
+  auto finish = [&](int f0, int nf) {
+    if (conceal) {
+      cudaEvent_t ev_;
+      begin_stage(kStageDropouts, ev_);
+      launch_dropout_conceal_chroma(*conceal, f0, nf, stream);
+      end_stage(kStageDropouts, ev_);
+    }
+    if (dst_chroma) {
+      cudaEventRecord(ev_chroma, stream);
+      cudaStreamWaitEvent(xstream, ev_chroma, 0);
+      cudaMemcpyAsync(dst_chroma + (size_t)f0 * F, ca.chroma + (size_t)f0 * F, (size_t)nf * F * sizeof(uint16_t),
+                      cudaMemcpyDeviceToHost, xstream);
+    }
+  };
   auto chroma_pass = [&](int f0, int nf, bool write) {
     cudaEvent_t ev_;
     begin_stage(kStageChromaLines, ev_);
@@ -725,6 +744,7 @@ bool Context::chroma_fields(ChromaArgs& ca, int P) {
   cudaMemcpyAsync(d_track, hp_track, P * sizeof(int), cudaMemcpyHostToDevice, stream);
   chroma_pass(0, P, true);
   cudaEventRecord(ev_host, stream);
+  finish(0, P);
   t_host = host_clock();
   if (!wait_host_event("chroma lines")) return false;
   host_phase(kHostChromaWait, t_host);
@@ -740,6 +760,7 @@ bool Context::chroma_fields(ChromaArgs& ca, int P) {
         cudaMemcpyAsync(d_track + f0, hp_track + f0, nf * sizeof(int), cudaMemcpyHostToDevice, stream);
         chroma_pass(f0, nf, true);
         cudaEventRecord(ev_host, stream);
+        finish(f0, nf);
         if (!wait_host_event("chroma retry")) return false;
         for (int f = f0; f < f0 + nf; f++) computed_track[f] = hp_track[f];
       }
@@ -822,46 +843,60 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   // chunk samples up to (fb-1)*spp - kOverlap + tile, so it starts as soon as
   // the piece reaching that far has landed.  With DC correction the chunk
   // mean is needed first, so K1a waits for the whole window.
-  {
+  const int dc_kernels = dc_correct ? 2 : 0;
+  auto k1a_range = [&](int f0, int nf) {
     cudaEvent_t ev_;
     begin_stage(kStageK1a, ev_);
-    int kernels = 1;
-    if (src_on_device) {
-      // a full window is read in place; a short one is copied
-      if (n_read < total_samples) cudaMemcpyAsync(d_raw, src, n_read * bps, cudaMemcpyDeviceToDevice, stream);
-      else da.raw = src;
-      if (dc_correct) launch_dc_mean(da.raw, (int)n_read, in_fmt, d_dcsum, d_dc, stream);
-      launch_k1a(da, 0, T, stream);
-    } else if (prefetched) {
-      cudaStreamWaitEvent(stream, ev_prefetch, 0);
-      if (dc_correct) launch_dc_mean(da.raw, (int)n_read, in_fmt, d_dcsum, d_dc, stream);
-      launch_k1a(da, 0, T, stream);
-    } else {
-      const int pieces = dc_correct ? 1 : std::min(kInputPieces, T);
-      size_t have = 0;
-      for (int i = 0; i < pieces; i++) {
-        const int fa = (int)((long long)T * i / pieces), fb = (int)((long long)T * (i + 1) / pieces);
-        size_t need = (size_t)(fb - 1) * spp + (size_t)des.tile - kOverlap;
-        if (i == pieces - 1 || need > n_read) need = n_read;
-        if (need > have) {
-          cudaMemcpyAsync(d_raw + have * bps, src + have * bps, (need - have) * bps, cudaMemcpyHostToDevice,
-                          hstream);
-          have = need;
-        }
-        cudaEventRecord(ev_piece[i], hstream);
-        cudaStreamWaitEvent(stream, ev_piece[i], 0);
-        if (dc_correct) launch_dc_mean(da.raw, (int)n_read, in_fmt, d_dcsum, d_dc, stream);
-        launch_k1a(da, fa, fb - fa, stream);
-      }
-      kernels = pieces;
-    }
-    end_stage(kStageK1a, ev_, kernels + (dc_correct ? 2 : 0));
-  }
-  {
+    launch_k1a(da, f0, nf, stream);
+    end_stage(kStageK1a, ev_);
+  };
+  auto k1b_range = [&](int f0, int nf) {
     cudaEvent_t ev_;
     begin_stage(kStageK1b, ev_);
-    launch_k1b(da, stream);
+    launch_k1b(da, f0, nf, stream);
     end_stage(kStageK1b, ev_);
+  };
+  auto dc_mean = [&] {
+    if (!dc_correct) return;
+    cudaEvent_t ev_;
+    begin_stage(kStageK1a, ev_);
+    launch_dc_mean(da.raw, (int)n_read, in_fmt, d_dcsum, d_dc, stream);
+    end_stage(kStageK1a, ev_, dc_kernels);
+  };
+  if (src_on_device || prefetched) {
+    // read in place (no kernel reads at or past n_read, so a short window
+    // needs no copy), or the window prefetched during the previous chunk
+    if (src_on_device) da.raw = src;
+    else cudaStreamWaitEvent(stream, ev_prefetch, 0);
+    dc_mean();
+    k1a_range(0, T);
+    k1b_range(0, T);
+  } else {
+    // host input in pieces: each tile range is demodulated (K1a) as soon as
+    // its samples have landed, and filtered (K1b) one tile behind: K1b's
+    // window for tile f reaches 2048 samples into tile f - 1 and a few hundred
+    // into tile f + 1
+    const int pieces = dc_correct ? 1 : std::min(kInputPieces, T);
+    size_t have = 0;
+    int k1b_next = 0;
+    for (int i = 0; i < pieces; i++) {
+      const int fa = (int)((long long)T * i / pieces), fb = (int)((long long)T * (i + 1) / pieces);
+      size_t need = (size_t)(fb - 1) * spp + (size_t)des.tile - kOverlap;
+      if (i == pieces - 1 || need > n_read) need = n_read;
+      if (need > have) {
+        cudaMemcpyAsync(d_raw + have * bps, src + have * bps, (need - have) * bps, cudaMemcpyHostToDevice, hstream);
+        have = need;
+      }
+      cudaEventRecord(ev_piece[i], hstream);
+      cudaStreamWaitEvent(stream, ev_piece[i], 0);
+      dc_mean();
+      k1a_range(fa, fb - fa);
+      const int ready = i == pieces - 1 ? T : fb - 1;  // tiles whose right neighbour is demodulated
+      if (ready > k1b_next) {
+        k1b_range(k1b_next, ready - k1b_next);
+        k1b_next = ready;
+      }
+    }
   }
   if (!check_cuda("demod")) return false;
   // ---- sync edges over the demodulated range.  One copy brings back the
@@ -873,7 +908,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   {
     cudaEvent_t ev_;
     begin_stage(kStageEdges, ev_);
-    launch_edges(d_sync, total_chunk, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, stream);
+    launch_edges(d_sync, total_chunk, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, d_edge_mask, stream);
     end_stage(kStageEdges, ev_, 3);
   }
   // the copies run on the copy stream, so the pre-band-pass below starts
@@ -1050,19 +1085,9 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   // ---- K6 chroma on the P detected fields
   ca.fields = P;
   ca.total = (long long)P * spp;
-  if (!chroma_fields(ca, P)) return false;
-  // ---- chroma is final: conceal it and send both planes' remaining copies
-  {
-    cudaEvent_t ev_;
-    begin_stage(kStageDropouts, ev_);
-    launch_dropout_conceal_chroma(dd, stream);
-    end_stage(kStageDropouts, ev_);
-  }
+  // the chroma is concealed and sent as it is decoded (chroma_fields)
+  if (!chroma_fields(ca, P, &dd, dst_chroma)) return false;
   if (!check_cuda("chroma concealment")) return false;
-  cudaEventRecord(ev_chroma, stream);
-  cudaStreamWaitEvent(xstream, ev_chroma, 0);
-  if (dst_chroma)
-    cudaMemcpyAsync(dst_chroma, d_chroma, (size_t)P * F * sizeof(uint16_t), cudaMemcpyDeviceToHost, xstream);
   cudaEventRecord(ev_out_done[oset], xstream);
   if (debug) {
     dbg_ll.resize((size_t)P * LPF);

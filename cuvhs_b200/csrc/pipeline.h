@@ -77,7 +77,7 @@ struct Context {
   // Copy stream: host input arrives in pieces (K1a starts on each piece as it
   // lands) and the finished luma leaves while chroma is still being decoded.
   cudaStream_t xstream = nullptr;
-  static constexpr int kInputPieces = 4;
+  static constexpr int kInputPieces = 8;
   cudaEvent_t ev_piece[kInputPieces] = {};
   cudaEvent_t ev_luma = nullptr;
   cudaEvent_t ev_edges = nullptr;
@@ -112,6 +112,7 @@ struct Context {
   unsigned *d_fall = nullptr, *d_rise = nullptr;
   int* d_counts = nullptr;
   int2* d_edge_blk = nullptr;
+  unsigned* d_edge_mask = nullptr;
   double* d_ll = nullptr;
   uint16_t *d_luma = nullptr, *d_chroma = nullptr;
   float* d_burst = nullptr;
@@ -212,8 +213,10 @@ struct Context {
   LineArgs line_args(int P) const;
   DropoutArgs dropout_args(int P) const;
   // Chroma lines of fields [0, P) of ca (pre-band-passed already) with the
-  // track/phase decisions and the carried chroma state; sets h_phase.
-  bool chroma_fields(ChromaArgs& ca, int P);
+  // track/phase decisions and the carried chroma state; sets h_phase.  With
+  // `conceal`, fields are concealed as they are decoded; with dst_chroma (page
+  // -locked host planes), sent there on the copy stream as well.
+  bool chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal = nullptr, uint16_t* dst_chroma = nullptr);
   // Sync edges of `sync` over [0, total) into h_fall / h_rise (synchronous).
   bool read_edges(const float* sync, long long total);
 };

@@ -62,7 +62,7 @@ cuvhs_status cuvhs_stage_fm_demod(cuvhs_ctx* ctx, const void* d_raw, size_t n_re
   cuvhs::launch_k1a(da, 0, tiles, c.stream);
   c.end_stage(cuvhs::kStageK1a, ev, c.dc_correct ? 3 : 1);
   c.begin_stage(cuvhs::kStageK1b, ev);
-  cuvhs::launch_k1b(da, c.stream);
+  cuvhs::launch_k1b(da, 0, tiles, c.stream);
   c.end_stage(cuvhs::kStageK1b, ev);
   if (!c.check_cuda("fm_demod") || !c.sync("fm_demod")) return c.status;
   return CUVHS_OK;

@@ -876,7 +876,10 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     // its samples have landed, and filtered (K1b) one tile behind: K1b's
     // window for tile f reaches 2048 samples into tile f - 1 and a few hundred
     // into tile f + 1
-    const int pieces = dc_correct ? 1 : std::min(kInputPieces, T);
+    // pieces of at least ~10 tiles: smaller launches leave SMs idle (a 5-tile
+    // K1a or K1b grid fills under half the GPU), which costs more than the
+    // earlier start gains
+    const int pieces = dc_correct ? 1 : std::max(1, std::min(kInputPieces, T / 10));
     size_t have = 0;
     int k1b_next = 0;
     for (int i = 0; i < pieces; i++) {

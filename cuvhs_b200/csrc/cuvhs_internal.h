@@ -299,6 +299,11 @@ class WorkPool {
     run_impl(n, f);
   }
   int size() const { return (int)threads_.size() + 1; }
+  // Wake the workers ahead of a run that is about to come: each spins (at
+  // most kSpinMs) for it instead of sleeping, so the run starts without the
+  // sleeping threads' wake-up latency.
+  void prime();
+  static constexpr int kSpinMs = 3;
 
  private:
   void run_impl(int n, std::function<void(int)>& fn);
@@ -311,7 +316,10 @@ class WorkPool {
   std::atomic<int> next_{0};
   int active_ = 0;
   unsigned long long generation_ = 0;
+  std::atomic<unsigned long long> published_{0};  // generation_, readable without the lock
+  unsigned long long prime_ = 0;
   bool stop_ = false;
+  std::atomic<bool> stopping_{false};
 };
 
 }  // namespace cuvhs

@@ -940,6 +940,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     end_stage(kStageChromaPre, ev_);
   }
   if (!check_cuda("chroma prefilter")) return false;
+  if (pool) pool->prime();  // the line-location job follows the edge lists
   double t_host = host_clock();
   if (!wait_host_event("edges")) return false;
   host_phase(kHostEdgesWait, t_host);

@@ -352,12 +352,15 @@ class Decoder:
         if st != 0:
             raise CuvhsError(st, "cuvhs_create failed")
         self._h = h
+        # held by the instance so that close() still works while the module's
+        # globals are torn down at interpreter exit
+        self._lib = lib
         if debug:
             lib.cuvhs_set_debug(self._h, 1)
 
     def close(self):
         if getattr(self, "_h", None):
-            lib.cuvhs_destroy(self._h)
+            self._lib.cuvhs_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -141,6 +141,10 @@ void Context::release() {
   }
   if (hstream) cudaStreamDestroy(hstream);
   hstream = nullptr;
+  if (ev_ll) cudaEventDestroy(ev_ll);
+  ev_ll = nullptr;
+  if (lstream) cudaStreamDestroy(lstream);
+  lstream = nullptr;
   pf = Prefetch();
   if (xstream) cudaStreamDestroy(xstream);
   xstream = nullptr;
@@ -218,7 +222,8 @@ bool Context::init(const cuvhs_config& c) {
   }
   if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&xstream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&hstream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&hstream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&lstream, cudaStreamNonBlocking) != cudaSuccess) {
     err = "cudaStreamCreate failed";
     status = CUVHS_ERR_CUDA;
     return false;
@@ -326,7 +331,8 @@ bool Context::init(const cuvhs_config& c) {
   hp_trial[1] = 1;
   bool ev_ok = cudaEventCreateWithFlags(&ev_host, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_luma, cudaEventDisableTiming) == cudaSuccess &&
-               cudaEventCreateWithFlags(&ev_edges, cudaEventDisableTiming) == cudaSuccess;
+               cudaEventCreateWithFlags(&ev_edges, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev_ll, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t* e : {&ev_prefetch, &ev_small, &ev_chroma, &ev_out_done[0], &ev_out_done[1]})
     ev_ok = ev_ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t& e : ev_piece) ev_ok = ev_ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
@@ -372,6 +378,7 @@ bool Context::sync(const char* where) {
   cudaError_t e = cudaStreamSynchronize(stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(xstream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(hstream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(lstream);
   if (e != cudaSuccess) {
     err = std::string(where) + ": " + cudaGetErrorString(e);
     status = CUVHS_ERR_CUDA;
@@ -1046,7 +1053,9 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     dbg_ll_coarse.assign(hp_ll, hp_ll + (size_t)P * LPF);
     dbg_meta = {T, P, spp};
   }
-  cudaMemcpyAsync(d_ll, hp_ll, (size_t)P * LPF * sizeof(double), cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(d_ll, hp_ll, (size_t)P * LPF * sizeof(double), cudaMemcpyHostToDevice, lstream);
+  cudaEventRecord(ev_ll, lstream);
+  cudaStreamWaitEvent(stream, ev_ll, 0);
   host_phase(kHostLines, t_host);
   // ---- K4 hsync refinement, K5 luma
   LineArgs la = line_args(P);

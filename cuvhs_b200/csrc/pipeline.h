@@ -86,6 +86,10 @@ struct Context {
   // the prefetch stream, and with page-locked destinations a chunk's planes
   // leave from one of two output sets while the next chunk already runs.
   cudaStream_t hstream = nullptr;  // host->device input copies
+  // Line-location upload: its own stream, so the copy overlaps the chroma
+  // prefilter instead of queueing behind it; hsync waits on ev_ll.
+  cudaStream_t lstream = nullptr;
+  cudaEvent_t ev_ll = nullptr;
   uint8_t* d_raw_set[2] = {};
   uint16_t* d_luma_set[2] = {};
   uint16_t* d_chroma_set[2] = {};

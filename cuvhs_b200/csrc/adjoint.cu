@@ -190,7 +190,7 @@ __device__ __forceinline__ ChromaSample chroma_sample(const AdjArgs& a, int gl, 
 // 1024-point band-pass of the two lines held in sm (real and imaginary parts).
 __device__ __forceinline__ void line_bandpass(float2* sm, const AdjArgs& a, int lane) {
   __syncwarp();
-  smem_fft<kLineFFT, 32, false>(sm, a.tw_l);
+  smem_fft<kLineFFT, 32, false>(sm, a.tw_l, lane);
   const int lo = a.fsc_bin - a.bw_bins, hi = a.fsc_bin + a.bw_bins;
   const float scale = 1.0f / (float)kLineFFT;
   for (int k = lane; k < kLineFFT; k += 32) {
@@ -200,7 +200,7 @@ __device__ __forceinline__ void line_bandpass(float2* sm, const AdjArgs& a, int 
     sm[pidx(k)] = make_float2(x.x * m, x.y * m);
   }
   __syncwarp();
-  smem_fft<kLineFFT, 32, true>(sm, a.tw_l_inv);
+  smem_fft<kLineFFT, 32, true>(sm, a.tw_l_inv, opaque_index(lane));
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

@@ -13,6 +13,7 @@
 //  * metric: adjacent-line burst cancellation per field (chroma_decode.cu:242-296).
 #include <cuda_runtime.h>
 
+#include "chain.cuh"
 #include "cuvhs_internal.h"
 #include "raw_input.cuh"
 #include "reg_fft.cuh"
@@ -20,35 +21,39 @@
 namespace cuvhs {
 namespace {
 
-constexpr int kThreadsC = Design::kNc / 16;
+// 32 elements per thread: 512 threads may hold 128 registers each, enough for
+// the 16384-point transform's 32 complex values without spilling
+constexpr int kElemsC = 16;
+constexpr int kThreadsC = Design::kNc / kElemsC;
 // warps per CTA of the line kernel: one line pair per warp, a padded N-point
 // buffer each (NTSC 1024, PAL 2048 points)
 template <int N>
 __host__ __device__ constexpr int line_warps() { return N <= 1024 ? 4 : 2; }
 
 // Two adjacent output blocks ride in the real and imaginary parts of one
-// transform (the kernel is real).  Thread t holds block samples t + T*q.
+// transform (the kernel is real).  Thread t holds block samples t + T*q, q < kElemsC.
 template <int FMT>
 __global__ void __launch_bounds__(kThreadsC, 1) prefilter_kernel(ChromaArgs a) {
-  constexpr int N = Design::kNc, T = kThreadsC;
+  chain_wait();
+  constexpr int N = Design::kNc, T = kThreadsC, E = kElemsC;
   extern __shared__ float2 sm[];
   const int t = threadIdx.x;
   const int f = blockIdx.y;
   const int i0 = blockIdx.x * 2 * a.c_out;  // first output of the real half
   const int tile = f * a.spp;               // chunk position of the tile
   const float dc = a.dc ? *a.dc : 0.0f;
-  float2 v[16];
+  float2 v[E];
   const int base = i0 - a.c_half;  // tile position of block sample 0 (before the wrap)
   if (base >= 0 && base + N + a.c_out <= a.spp && tile + base + N + a.c_out <= a.n_read) {
     // interior: no wrap, inside the tile's samples and the samples read
     const int p = tile + base + t;
 #pragma unroll
-    for (int q = 0; q < 16; q++)
+    for (int q = 0; q < E; q++)
       v[q] = make_float2(raw_convert<FMT>(a.raw, p + T * q) - dc, raw_convert<FMT>(a.raw, p + T * q + a.c_out) - dc);
   } else {
     // the zero-padded tile wraps at most once (ctile > N + c_out)
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
+    for (int q = 0; q < E; q++) {
       int q0 = base + t + T * q;
       if (q0 < 0) q0 += a.ctile;
       else if (q0 >= a.ctile) q0 -= a.ctile;
@@ -59,16 +64,16 @@ __global__ void __launch_bounds__(kThreadsC, 1) prefilter_kernel(ChromaArgs a) {
       v[q] = make_float2(v0, v1);
     }
   }
-  RegFFT<N>::run<false>(v, sm, a.tw_c, t);
+  RegFFT<N, E>::run<false>(v, sm, a.tw_c, t);
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
+  for (int q = 0; q < E; q++) {
     const float g = __ldg(&a.gc[t + T * q]);
     v[q] = make_float2(v[q].x * g, v[q].y * g);
   }
-  RegFFT<N>::run<true>(v, sm, a.tw_c_inv, t);
+  RegFFT<N, E>::run<true>(v, sm, a.tw_c_inv, opaque_index(t));
   float* out = a.pre + (size_t)f * a.spp;
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
+  for (int q = 0; q < E; q++) {
     const int i = t + T * q - a.c_half;
     if (i >= 0 && i < a.c_out) {
       const int p0 = i0 + i, p1 = i0 + a.c_out + i;
@@ -129,6 +134,7 @@ __device__ __forceinline__ float het_at(const ChromaArgs& a, const HetLine& L, d
 template <int N>
 __global__ void __launch_bounds__(32 * line_warps<N>(), N <= 1024 ? 4 : 1) lines_kernel(ChromaArgs a, int line0, int nlines,
                                                                     int write_output) {
+  chain_wait();
   constexpr int W = line_warps<N>();
   __shared__ float2 sm_all[W][fft_pad(N)];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -154,7 +160,7 @@ __global__ void __launch_bounds__(32 * line_warps<N>(), N <= 1024 ? 4 : 1) lines
     sm[pidx(c)] = make_float2(va, vb);
   }
   __syncwarp();
-  smem_fft<N, 32, false>(sm, a.tw_line);
+  smem_fft<N, 32, false>(sm, a.tw_line, lane);
   const int lo = a.fsc_bin - a.bw_bins, hi = a.fsc_bin + a.bw_bins;
   const float scale = 1.0f / (float)N;
   for (int k = lane; k < N; k += 32) {
@@ -164,7 +170,7 @@ __global__ void __launch_bounds__(32 * line_warps<N>(), N <= 1024 ? 4 : 1) lines
     sm[pidx(k)] = make_float2(x.x * m, x.y * m);
   }
   __syncwarp();
-  smem_fft<N, 32, true>(sm, a.tw_line_inv);
+  smem_fft<N, 32, true>(sm, a.tw_line_inv, opaque_index(lane));
   // burst RMS per line -> ACC gain
   const int bl = a.burst_len;
   float ssa = 0.0f, ssb = 0.0f;
@@ -201,6 +207,7 @@ __global__ void __launch_bounds__(32 * line_warps<N>(), N <= 1024 ? 4 : 1) lines
 // BL: the burst window length when known at compile time (NTSC 36, PAL 40), 0 = a.burst_len.
 template <int BL>
 __global__ void metric_kernel(ChromaArgs a, int field0, int nfields) {
+  chain_wait();
   const int bl = BL > 0 ? BL : a.burst_len;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= nfields) return;
@@ -227,7 +234,7 @@ void launch_chroma_prefilter(const ChromaArgs& a, cudaStream_t st) {
   dim3 grid((a.spp + 2 * a.c_out - 1) / (2 * a.c_out), a.fields);
   auto go = [&](auto kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kernel<<<grid, kThreadsC, smem, st>>>(a);
+    launch_chained(kernel, grid, dim3(kThreadsC), smem, st, a);
   };
   if (a.in_fmt == kInS16) go(prefilter_kernel<kInS16>);
   else if (a.in_fmt == kInU16) go(prefilter_kernel<kInU16>);
@@ -241,7 +248,8 @@ void launch_chroma_lines(const ChromaArgs& a, int field0, int nfields, bool writ
   auto go = [&](auto kernel, int warps) {
     // the largest shared-memory carveout, so that the register limit sets the CTAs per SM
     cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-    kernel<<<(pairs + warps - 1) / warps, 32 * warps, 0, st>>>(a, field0 * a.out_h, nlines, write_output ? 1 : 0);
+    launch_chained(kernel, dim3((pairs + warps - 1) / warps), dim3(32 * warps), 0, st, a, field0 * a.out_h, nlines,
+                   write_output ? 1 : 0);
   };
   if (a.line_fft == 2048) go(lines_kernel<2048>, line_warps<2048>());
   else go(lines_kernel<1024>, line_warps<1024>());
@@ -251,9 +259,10 @@ void launch_burst_metric(const ChromaArgs& a, int field0, int nfields, cudaStrea
   if (nfields <= 0) return;
   const int threads = 128;
   const int blocks = (nfields * 32 + threads - 1) / threads;
-  if (a.burst_len == 36) metric_kernel<36><<<blocks, threads, 0, st>>>(a, field0, nfields);
-  else if (a.burst_len == 40) metric_kernel<40><<<blocks, threads, 0, st>>>(a, field0, nfields);
-  else metric_kernel<0><<<blocks, threads, 0, st>>>(a, field0, nfields);
+  auto go = [&](auto kernel) { launch_chained(kernel, dim3(blocks), dim3(threads), 0, st, a, field0, nfields); };
+  if (a.burst_len == 36) go(metric_kernel<36>);
+  else if (a.burst_len == 40) go(metric_kernel<40>);
+  else go(metric_kernel<0>);
 }
 
 }  // namespace cuvhs

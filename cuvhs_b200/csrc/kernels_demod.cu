@@ -11,6 +11,7 @@
 // FP32 demod and envelope; K1b reads the demod and writes video and sync.
 #include <cuda_runtime.h>
 
+#include "chain.cuh"
 #include "cuvhs_internal.h"
 #include "raw_input.cuh"
 #include "reg_fft.cuh"
@@ -127,6 +128,7 @@ __device__ __forceinline__ void k1a_emit(const DemodArgs& a, const float2 (&z)[1
 template <int FMT>
 __global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(DemodArgs a, int f_begin) {
   constexpr int N = Design::kNa, T = kThreadsA;
+  chain_wait();
   extern __shared__ float2 sm[];
   float2* sA = sm;
   float2* sB = sm + fft_pad(N);
@@ -193,6 +195,7 @@ __device__ __forceinline__ void k1b_emit(const DemodArgs& a, const float2 (&z)[1
 // K1b: demod -> video + sync, blocks 2x and 2x+1 of the tile.
 __global__ void __launch_bounds__(kThreadsB, 1) k1b_kernel(DemodArgs a, int f_begin) {
   constexpr int N = Design::kNb, T = kThreadsB;
+  chain_wait();
   extern __shared__ float2 sm[];
   float2* sA = sm;
   float2* sB = sm + fft_pad(N);
@@ -292,6 +295,7 @@ __device__ __forceinline__ int2 block_scan2(int a, int b, int& pa, int& pb) {
 __global__ void __launch_bounds__(kEdgeThreads) edge_count_kernel(const float* __restrict__ x, long long total,
                                                                   float thr, int2* __restrict__ blk,
                                                                   unsigned* __restrict__ masks) {
+  chain_wait();
   const long long i0 = (long long)blockIdx.x * kEdgeSeg + (long long)threadIdx.x * kEdgePer;
   unsigned fm, rm;
   edge_masks(x, total, thr, i0, fm, rm);
@@ -309,6 +313,7 @@ constexpr int kScanThreads = 1024;
 __global__ void __launch_bounds__(kScanThreads) edge_scan_kernel(int2* __restrict__ blk, int nblk,
                                                                  int* __restrict__ counts) {
   __shared__ int2 warp_tot[kScanThreads / 32];
+  chain_wait();
   const int per = (nblk + kScanThreads - 1) / kScanThreads;
   const int b0 = min(nblk, (int)threadIdx.x * per), b1 = min(nblk, b0 + per);
   int sa = 0, sb = 0;
@@ -363,6 +368,7 @@ __global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(long long tota
                                                                   const int2* __restrict__ blk,
                                                                   unsigned* __restrict__ fall,
                                                                   unsigned* __restrict__ rise, int cap) {
+  chain_wait();
   const long long i0 = (long long)blockIdx.x * kEdgeSeg + (long long)threadIdx.x * kEdgePer;
   const unsigned m = __ldg(&masks[(size_t)blockIdx.x * kEdgeThreads + threadIdx.x]);
   unsigned fm = m & 0xFFFFu, rm = m >> 16;
@@ -393,7 +399,7 @@ void launch_k1a(const DemodArgs& a, int f0, int nf, cudaStream_t st) {
   dim3 grid((blocks + 1) / 2, nf);
   auto go = [&](auto kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kernel<<<grid, kThreadsA, smem, st>>>(a, f0);
+    launch_chained(kernel, grid, dim3(kThreadsA), smem, st, a, f0);
   };
   if (a.in_fmt == kInS16) go(k1a_kernel<kInS16>);
   else if (a.in_fmt == kInU16) go(k1a_kernel<kInU16>);
@@ -443,7 +449,7 @@ void launch_k1b(const DemodArgs& a, int f0, int nf, cudaStream_t st) {
   cudaFuncSetAttribute(k1b_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int blocks = (a.spp + a.b_out - 1) / a.b_out;
   dim3 grid((blocks + 1) / 2, nf);
-  k1b_kernel<<<grid, kThreadsB, smem, st>>>(a, f0);
+  launch_chained(k1b_kernel, grid, dim3(kThreadsB), smem, st, a, f0);
 }
 
 int edge_blocks(long long total) { return (int)((total + kEdgeSeg - 1) / kEdgeSeg); }
@@ -454,9 +460,10 @@ void launch_edges(const float* sync, long long total, float thr_rel, unsigned* f
                   int cap, int2* blk, unsigned* masks, cudaStream_t st) {
   const int nblk = edge_blocks(total);
   if (nblk <= 0) return;
-  edge_count_kernel<<<nblk, kEdgeThreads, 0, st>>>(sync, total, thr_rel, blk, masks);
-  edge_scan_kernel<<<1, kScanThreads, 0, st>>>(blk, nblk, counts);
-  edge_write_kernel<<<nblk, kEdgeThreads, 0, st>>>(total, masks, blk, fall, rise, cap);
+  launch_chained(edge_count_kernel, dim3(nblk), dim3(kEdgeThreads), 0, st, sync, total, thr_rel, blk, masks);
+  launch_chained(edge_scan_kernel, dim3(1), dim3(kScanThreads), 0, st, blk, nblk, counts);
+  launch_chained(edge_write_kernel, dim3(nblk), dim3(kEdgeThreads), 0, st, total, (const unsigned*)masks,
+                 (const int2*)blk, fall, rise, cap);
 }
 
 }  // namespace cuvhs

@@ -23,6 +23,7 @@
 //    the classes in shared memory, so it needs no scratch beyond the partials.
 #include <cuda_runtime.h>
 
+#include "chain.cuh"
 #include "cuvhs_internal.h"
 
 namespace cuvhs {
@@ -144,6 +145,7 @@ __device__ void conceal(const DropoutArgs& a, int f, int n, int lane, bool luma,
 // ------------------------------------------------------------------ fused form
 
 __global__ void __launch_bounds__(kThreadsD) dropout_kernel(DropoutArgs a) {
+  chain_wait();
   extern __shared__ unsigned char cls[];  // [a.max_blocks]
   __shared__ int last_cls[kThreadsD];
   __shared__ int state_in[kThreadsD];
@@ -224,6 +226,7 @@ __global__ void __launch_bounds__(kThreadsD) dropout_kernel(DropoutArgs a) {
 // staged with coalesced loads into rows of 17 floats (conflict-free column
 // reads), then each thread sums its row in sample order.
 __global__ void __launch_bounds__(kThreadsD) dropout_class_kernel(DropoutArgs a) {
+  chain_wait();
   __shared__ float stage[kThreadsD * 17];
   __shared__ double down_s;
   const int f = blockIdx.y, tid = threadIdx.x;
@@ -305,6 +308,7 @@ __device__ __forceinline__ int block_excl_last(int v, int* wsh) {
 // hysteresis scan, event list, mapping and luma concealment (chroma is
 // concealed by dropout_chroma_kernel once the chroma planes are final).
 __global__ void __launch_bounds__(kThreadsScan) dropout_scan_kernel(DropoutArgs a) {
+  chain_wait();
   extern __shared__ uint4 cls4[];  // [a.max_blocks / 16]
   __shared__ int wsh[32];
   __shared__ int events[kMaxEvents];
@@ -349,6 +353,7 @@ __global__ void __launch_bounds__(kThreadsScan) dropout_scan_kernel(DropoutArgs 
 
 // One warp per field: chroma concealment from the entries the scan kernel wrote.
 __global__ void dropout_chroma_kernel(DropoutArgs a, int f0, int nf) {
+  chain_wait();
   const int f = f0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (f >= f0 + nf || f >= a.fields) return;  // whole warp
   const int n = min(max(a.do_count[f], 0), kMaxDropouts);
@@ -361,7 +366,7 @@ void launch_dropouts(const DropoutArgs& a, cudaStream_t st) {
   if (a.fields <= 0) return;
   const size_t smem = (size_t)a.max_blocks;
   cudaFuncSetAttribute(dropout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  dropout_kernel<<<a.fields, kThreadsD, smem, st>>>(a);
+  launch_chained(dropout_kernel, dim3(a.fields), dim3(kThreadsD), smem, st, a);
 }
 
 size_t dropout_class_bytes_per_field(int spp) { return (size_t)(((spp + 15) / 16 + 15) / 16 * 16); }
@@ -369,16 +374,16 @@ size_t dropout_class_bytes_per_field(int spp) { return (size_t)(((spp + 15) / 16
 void launch_dropouts_two_pass(const DropoutArgs& a, cudaStream_t st) {
   if (a.fields <= 0) return;
   dim3 grid((a.max_blocks + kThreadsD - 1) / kThreadsD, a.fields);
-  dropout_class_kernel<<<grid, kThreadsD, 0, st>>>(a);
+  launch_chained(dropout_class_kernel, grid, dim3(kThreadsD), 0, st, a);
   const size_t smem = (size_t)a.max_blocks;
   cudaFuncSetAttribute(dropout_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  dropout_scan_kernel<<<a.fields, kThreadsScan, smem, st>>>(a);
+  launch_chained(dropout_scan_kernel, dim3(a.fields), dim3(kThreadsScan), smem, st, a);
 }
 
 void launch_dropout_conceal_chroma(const DropoutArgs& a, int f0, int nf, cudaStream_t st) {
   if (nf <= 0 || f0 < 0 || f0 >= a.fields) return;
   const int threads = 128;
-  dropout_chroma_kernel<<<(nf * 32 + threads - 1) / threads, threads, 0, st>>>(a, f0, nf);
+  launch_chained(dropout_chroma_kernel, dim3((nf * 32 + threads - 1) / threads), dim3(threads), 0, st, a, f0, nf);
 }
 
 }  // namespace cuvhs

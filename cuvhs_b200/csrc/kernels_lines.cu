@@ -7,6 +7,7 @@
 // the integer window truncations match.
 #include <cuda_runtime.h>
 
+#include "chain.cuh"
 #include "cuvhs_internal.h"
 
 namespace cuvhs {
@@ -104,6 +105,7 @@ __device__ double window_median(const float* __restrict__ s, int start, int coun
 // One warp per line location (lines from the first active line to the end of
 // the frame table).
 __global__ void __launch_bounds__(32 * kHsyncWarps) hsync_kernel(LineArgs a) {
+  chain_wait();
   const int lane = threadIdx.x & 31;
   const int idx = blockIdx.x * kHsyncWarps + (threadIdx.x >> 5);
   if (idx >= a.fields * a.lines_per_frame) return;  // whole warp
@@ -154,6 +156,7 @@ __global__ void __launch_bounds__(32 * kHsyncWarps) hsync_kernel(LineArgs a) {
 // fractions col/W come from a table (the same FP64 quotient), and consecutive
 // threads write consecutive pixels.
 __global__ void __launch_bounds__(kLumaThreads) luma_kernel(LineArgs a) {
+  chain_wait();
   const int W = a.out_w, H = a.out_h;
   const int grow = blockIdx.x;  // field * H + row
   const int field = grow / H, row = grow % H;
@@ -190,13 +193,13 @@ __global__ void __launch_bounds__(kLumaThreads) luma_kernel(LineArgs a) {
 void launch_hsync_refine(const LineArgs& a, cudaStream_t st) {
   const int n = a.fields * a.lines_per_frame;
   if (n <= 0) return;
-  hsync_kernel<<<(n + kHsyncWarps - 1) / kHsyncWarps, 32 * kHsyncWarps, 0, st>>>(a);
+  launch_chained(hsync_kernel, dim3((n + kHsyncWarps - 1) / kHsyncWarps), dim3(32 * kHsyncWarps), 0, st, a);
 }
 
 void launch_luma(const LineArgs& a, cudaStream_t st) {
   const int rows = a.fields * a.out_h;
   if (rows <= 0) return;
-  luma_kernel<<<rows, kLumaThreads, 0, st>>>(a);
+  launch_chained(luma_kernel, dim3(rows), dim3(kLumaThreads), 0, st, a);
 }
 
 }  // namespace cuvhs

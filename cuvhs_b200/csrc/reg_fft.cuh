@@ -1,6 +1,7 @@
-// Register-resident block FFT for one CTA of T = N/16 threads (sm_100a).
+// Register-resident block FFT for one CTA of T = N/E threads (sm_100a), E = 16
+// or 32 elements per thread.
 //
-// Thread t owns elements t + T*q, q = 0..15, of an N-point transform, both on
+// Thread t owns elements t + T*q, q = 0..E-1, of an N-point transform, both on
 // entry (natural-order input) and on exit (natural-order output): Stockham
 // passes of radix 16 (and one final radix 2/4/8 when N is not a power of 16)
 // exchange data through a padded shared buffer between passes, but the first
@@ -15,33 +16,33 @@
 
 namespace cuvhs {
 
-template <int N>
+template <int N, int E = 16>
 struct RegFFT {
-  static constexpr int T = N / 16;
+  static_assert(E == 16 || E == 32, "16 or 32 elements per thread");
+  static constexpr int T = N / E;
+  static constexpr int G = E / 16;  // first-pass radix-16 butterflies per thread
 
-  // One pass of radix R at span NS (> 1).  v holds the 16 values this thread
+  // One pass of radix R at span NS (> 1).  v holds the E values this thread
   // reads; LAST leaves the results in v in the t + T*q layout.
   template <int NS, bool INV, bool LAST>
-  __device__ __forceinline__ static void pass(float2 (&v)[16], float2* s, const float2* __restrict__ tw, int t) {
+  __device__ __forceinline__ static void pass(float2 (&v)[E], float2* s, const float2* __restrict__ tw, int t) {
     constexpr int R = fft_radix(N, NS);
-    constexpr int B = 16 / R;  // butterflies per thread
+    constexpr int B = E / R;  // butterflies per thread
+    // inputs are twiddled as they are read, so only the E values stay live
+    // across the barrier
     float2 w[B][R];
-#pragma unroll
-    for (int b = 0; b < B; b++) {
-      const int j = t + T * b;
-#pragma unroll
-      for (int r = 0; r < R; r++) w[b][r] = s[pidx(j + r * (N / R))];
-    }
-    __syncthreads();  // every read done before this pass (or the caller) overwrites
 #pragma unroll
     for (int b = 0; b < B; b++) {
       const int j = t + T * b;
       const int k = j & (NS - 1);
       const float2* twp = tw + (NS - 16) + k;
+      w[b][0] = s[pidx(j)];
 #pragma unroll
-      for (int r = 1; r < R; r++) w[b][r] = cmul_tw<INV>(w[b][r], __ldg(&twp[(r - 1) * NS]));
-      dft<R, INV>(w[b]);
+      for (int r = 1; r < R; r++) w[b][r] = cmul_tw<INV>(s[pidx(j + r * (N / R))], __ldg(&twp[(r - 1) * NS]));
     }
+    __syncthreads();  // every read done before this pass (or the caller) overwrites
+#pragma unroll
+    for (int b = 0; b < B; b++) dft<R, INV>(w[b]);
     if constexpr (LAST) {
 #pragma unroll
       for (int b = 0; b < B; b++)
@@ -61,7 +62,7 @@ struct RegFFT {
   }
 
   template <int NS, bool INV>
-  __device__ __forceinline__ static void rest(float2 (&v)[16], float2* s, const float2* __restrict__ tw, int t) {
+  __device__ __forceinline__ static void rest(float2 (&v)[E], float2* s, const float2* __restrict__ tw, int t) {
     constexpr int R = fft_radix(N, NS);
     constexpr bool LAST = NS * R >= N;
     pass<NS, INV, LAST>(v, s, tw, t);
@@ -71,12 +72,22 @@ struct RegFFT {
   // Transform v in place.  The buffer s (fft_pad(N) float2) may be in use by
   // the caller until this call: the first write waits on a barrier.
   template <bool INV>
-  __device__ __forceinline__ static void run(float2 (&v)[16], float2* s, const float2* __restrict__ tw, int t) {
+  __device__ __forceinline__ static void run(float2 (&v)[E], float2* s, const float2* __restrict__ tw, int t) {
     static_assert(N >= 256 && (N & (N - 1)) == 0, "power of two >= 256");
-    dft<16, INV>(v);  // pass NS = 1: inputs t + T*r are exactly this thread's
+    // pass NS = 1: butterfly t + T*g reads elements t + T*(g + G*r), all
+    // held by this thread (slots g + G*r)
+    float2 w[G][16];
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+#pragma unroll
+      for (int r = 0; r < 16; r++) w[g][r] = v[g + G * r];
+      dft<16, INV>(w[g]);
+    }
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < 16; r++) s[pidx(16 * t + r)] = v[dft_slot<16>(r)];
+    for (int g = 0; g < G; g++)
+#pragma unroll
+      for (int r = 0; r < 16; r++) s[pidx(16 * (t + T * g) + r)] = w[g][dft_slot<16>(r)];
     __syncthreads();
     rest<16, INV>(v, s, tw, t);
   }

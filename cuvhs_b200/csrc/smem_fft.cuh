@@ -16,6 +16,16 @@ namespace cuvhs {
 
 __host__ __device__ constexpr int fft_pad(int n) { return n + (n >> 4); }
 
+// The thread index as a value the compiler cannot prove equal to its source.
+// Two transforms in one kernel compute the same shared-memory and twiddle
+// offsets; given the plain index the compiler keeps the first transform's
+// offsets live until the second uses them, which spills the transforms' data.
+__device__ __forceinline__ int opaque_index(int t) {
+  int r;
+  asm volatile("mov.u32 %0, %1;" : "=r"(r) : "r"(t));
+  return r;
+}
+
 // Radix of the pass that starts at span NS in an N-point transform.
 __host__ __device__ constexpr int fft_radix(int N, int NS) { return NS * 16 <= N ? 16 : N / NS; }
 // Entries of the per-pass twiddle table of an N-point transform.
@@ -132,11 +142,9 @@ __device__ __forceinline__ void fft_sync() {
 
 // One Stockham pass of radix R on an N-point padded buffer, current span NS.
 template <int N, int THREADS, int R, int NS, bool INV>
-__device__ __forceinline__ void fft_pass(float2* s, const float2* __restrict__ tw) {
+__device__ __forceinline__ void fft_pass(float2* s, const float2* __restrict__ tw, int tid) {
   constexpr int NB = N / R;
   constexpr int PER = (NB + THREADS - 1) / THREADS;
-  // A 32-thread transform belongs to one warp (several may share a CTA).
-  const int tid = (THREADS == 32) ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
   float2 v[PER][R];
 #pragma unroll
   for (int p = 0; p < PER; p++) {
@@ -169,16 +177,17 @@ __device__ __forceinline__ void fft_pass(float2* s, const float2* __restrict__ t
 
 // Full N-point transform (N a power of two, 64 <= N <= 65536), natural order
 // in and out, unnormalised.  Caller must synchronise (CTA, or warp for
-// THREADS == 32) after filling s.
+// THREADS == 32) after filling s.  tid: this thread's index among the
+// transform's THREADS threads (the lane for a one-warp transform).
 template <int N, int THREADS, bool INV, int NS = 1>
-__device__ __forceinline__ void smem_fft(float2* s, const float2* __restrict__ tw) {
+__device__ __forceinline__ void smem_fft(float2* s, const float2* __restrict__ tw, int tid) {
   if constexpr (NS * 16 <= N) {
-    fft_pass<N, THREADS, 16, NS, INV>(s, tw);
-    smem_fft<N, THREADS, INV, NS * 16>(s, tw);
+    fft_pass<N, THREADS, 16, NS, INV>(s, tw, tid);
+    smem_fft<N, THREADS, INV, NS * 16>(s, tw, tid);
   } else if constexpr (NS < N) {
     constexpr int R = N / NS;  // 2, 4 or 8
     static_assert(R == 2 || R == 4 || R == 8, "N must be a power of two");
-    fft_pass<N, THREADS, R, NS, INV>(s, tw);
+    fft_pass<N, THREADS, R, NS, INV>(s, tw, tid);
   }
 }
 

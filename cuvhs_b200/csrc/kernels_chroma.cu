@@ -21,8 +21,9 @@
 namespace cuvhs {
 namespace {
 
-// 32 elements per thread: 512 threads may hold 128 registers each, enough for
-// the 16384-point transform's 32 complex values without spilling
+// 16 elements per thread, 1024 threads at 64 registers each (spill-free since
+// the inverse transform takes an opaque thread index); 32 elements with 512
+// threads at 128 registers is also spill-free but measured 9% slower.
 constexpr int kElemsC = 16;
 constexpr int kThreadsC = Design::kNc / kElemsC;
 // warps per CTA of the line kernel: one line pair per warp, a padded N-point

@@ -26,10 +26,26 @@ namespace {
 // threads at 128 registers is also spill-free but measured 9% slower.
 constexpr int kElemsC = 16;
 constexpr int kThreadsC = Design::kNc / kElemsC;
-// warps per CTA of the line kernel: one line pair per warp, a padded N-point
-// buffer each (NTSC 1024, PAL 2048 points)
+// Line kernel geometry: a line pair (two lines in one complex transform) per
+// group of line_tp threads with a padded N-point buffer (NTSC 1024, PAL 2048
+// points), line_pairs groups per CTA.  NTSC pairs take two warps, so each
+// thread holds one radix-16 butterfly per pass and the kernel fits 64
+// registers (32 warps per SM to cover the gathers' latency).
 template <int N>
-__host__ __device__ constexpr int line_warps() { return N <= 1024 ? 4 : 2; }
+__host__ __device__ constexpr int line_tp() { return N <= 1024 ? 64 : 32; }
+template <int N>
+__host__ __device__ constexpr int line_pairs() { return 2; }
+template <int N>
+__host__ __device__ constexpr int line_threads() { return line_tp<N>() * line_pairs<N>(); }
+template <int N>
+__host__ __device__ constexpr int line_min_ctas() { return N <= 1024 ? 8 : 1; }
+
+// Barrier of one line pair's threads.
+template <int TP>
+__device__ __forceinline__ void pair_sync() {
+  if constexpr (TP == 32) __syncwarp();
+  else asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)(threadIdx.x / TP)), "r"(TP) : "memory");
+}
 
 // Two adjacent output blocks ride in the real and imaginary parts of one
 // transform (the kernel is real).  Thread t holds block samples t + T*q, q < kElemsC.
@@ -133,16 +149,17 @@ __device__ __forceinline__ float het_at(const ChromaArgs& a, const HetLine& L, d
 }
 
 template <int N>
-__global__ void __launch_bounds__(32 * line_warps<N>(), N <= 1024 ? 4 : 1) lines_kernel(ChromaArgs a, int line0, int nlines,
-                                                                    int write_output) {
+__global__ void __launch_bounds__(line_threads<N>(), line_min_ctas<N>())
+    lines_kernel(ChromaArgs a, int line0, int nlines, int write_output) {
   chain_wait();
-  constexpr int W = line_warps<N>();
-  __shared__ float2 sm_all[W][fft_pad(N)];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2* sm = sm_all[warp];
-  const int pair = blockIdx.x * W + warp;
+  constexpr int TP = line_tp<N>(), P = line_pairs<N>();
+  __shared__ float2 sm_all[P][fft_pad(N)];
+  __shared__ float acc_sh[P][2];
+  const int g = threadIdx.x / TP, tid = threadIdx.x % TP, lane = threadIdx.x & 31;
+  float2* sm = sm_all[g];
+  const int pair = blockIdx.x * P + g;
   const int la = 2 * pair, lb = la + 1;  // relative to line0
-  if (la >= nlines) return;               // whole warp leaves together
+  if (la >= nlines) return;               // the pair's warps leave together
   const bool has_b = lb < nlines;
   const HetLine A = het_line(a, line0 + la);
   HetLine B = A;
@@ -151,7 +168,7 @@ __global__ void __launch_bounds__(32 * line_warps<N>(), N <= 1024 ? 4 : 1) lines
   // the gather is latency bound: unrolled so that several columns' loads are
   // in flight (the FFT below sets the register budget, not this loop)
 #pragma unroll 4
-  for (int c = lane; c < N; c += 32) {
+  for (int c = tid; c < N; c += TP) {
     float va = 0.0f, vb = 0.0f;
     if (c < a.out_w) {
       const double frac = __ldg(&a.col_frac[c]);
@@ -160,39 +177,46 @@ __global__ void __launch_bounds__(32 * line_warps<N>(), N <= 1024 ? 4 : 1) lines
     }
     sm[pidx(c)] = make_float2(va, vb);
   }
-  __syncwarp();
-  smem_fft<N, 32, false>(sm, a.tw_line, lane);
+  pair_sync<TP>();
+  smem_fft<N, TP, false>(sm, a.tw_line, tid);
   const int lo = a.fsc_bin - a.bw_bins, hi = a.fsc_bin + a.bw_bins;
   const float scale = 1.0f / (float)N;
-  for (int k = lane; k < N; k += 32) {
+  for (int k = tid; k < N; k += TP) {
     const int kk = k <= N / 2 ? k : N - k;
     const float m = (kk >= lo && kk <= hi) ? scale : 0.0f;
     const float2 x = sm[pidx(k)];
     sm[pidx(k)] = make_float2(x.x * m, x.y * m);
   }
-  __syncwarp();
-  smem_fft<N, 32, true>(sm, a.tw_line_inv, opaque_index(lane));
-  // burst RMS per line -> ACC gain
-  const int bl = a.burst_len;
-  float ssa = 0.0f, ssb = 0.0f;
-  for (int i = lane; i < bl; i += 32) {
-    const float2 v = sm[pidx(a.burst_start + i)];
-    ssa += v.x * v.x;
-    ssb += v.y * v.y;
-    a.burst[(size_t)(line0 + la) * bl + i] = v.x;
-    if (has_b) a.burst[(size_t)(line0 + lb) * bl + i] = v.y;
+  pair_sync<TP>();
+  smem_fft<N, TP, true>(sm, a.tw_line_inv, opaque_index(tid));
+  // burst RMS per line -> ACC gain, summed by the pair's first warp in a
+  // fixed order (lane sums i = lane, lane + 32, ..., then a butterfly)
+  if (tid < 32) {
+    const int bl = a.burst_len;
+    float ssa = 0.0f, ssb = 0.0f;
+    for (int i = lane; i < bl; i += 32) {
+      const float2 v = sm[pidx(a.burst_start + i)];
+      ssa += v.x * v.x;
+      ssb += v.y * v.y;
+      a.burst[(size_t)(line0 + la) * bl + i] = v.x;
+      if (has_b) a.burst[(size_t)(line0 + lb) * bl + i] = v.y;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      ssa += __shfl_xor_sync(0xffffffffu, ssa, off);
+      ssb += __shfl_xor_sync(0xffffffffu, ssb, off);
+    }
+    const float rms_a = sqrtf(ssa / (float)bl), rms_b = sqrtf(ssb / (float)bl);
+    if (lane == 0) {
+      acc_sh[g][0] = rms_a > 1.0f ? a.burst_abs_ref / rms_a : 0.0f;
+      acc_sh[g][1] = rms_b > 1.0f ? a.burst_abs_ref / rms_b : 0.0f;
+    }
   }
-  for (int off = 16; off > 0; off >>= 1) {
-    ssa += __shfl_xor_sync(0xffffffffu, ssa, off);
-    ssb += __shfl_xor_sync(0xffffffffu, ssb, off);
-  }
-  if (!write_output) return;
-  const float rms_a = sqrtf(ssa / (float)bl), rms_b = sqrtf(ssb / (float)bl);
-  const float acc_a = rms_a > 1.0f ? a.burst_abs_ref / rms_a : 0.0f;
-  const float acc_b = rms_b > 1.0f ? a.burst_abs_ref / rms_b : 0.0f;
+  if (!write_output) return;  // uniform over the pair: no barrier follows
+  pair_sync<TP>();
+  const float acc_a = acc_sh[g][0], acc_b = acc_sh[g][1];
   uint16_t* oa = a.chroma + (size_t)(line0 + la) * a.out_w;
   uint16_t* ob = a.chroma + (size_t)(line0 + lb) * a.out_w;
-  for (int c = lane; c < a.out_w; c += 32) {
+  for (int c = tid; c < a.out_w; c += TP) {
     const float2 v = sm[pidx(c)];
     const float xa = fminf(fmaxf(v.x * acc_a + 32768.0f, 0.0f), 65535.0f);
     oa[c] = (uint16_t)(xa + 0.5f);
@@ -246,14 +270,14 @@ void launch_chroma_lines(const ChromaArgs& a, int field0, int nfields, bool writ
   const int nlines = nfields * a.out_h;
   if (nlines <= 0) return;
   const int pairs = (nlines + 1) / 2;
-  auto go = [&](auto kernel, int warps) {
+  auto go = [&](auto kernel, int per_cta, int threads) {
     // the largest shared-memory carveout, so that the register limit sets the CTAs per SM
     cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-    launch_chained(kernel, dim3((pairs + warps - 1) / warps), dim3(32 * warps), 0, st, a, field0 * a.out_h, nlines,
+    launch_chained(kernel, dim3((pairs + per_cta - 1) / per_cta), dim3(threads), 0, st, a, field0 * a.out_h, nlines,
                    write_output ? 1 : 0);
   };
-  if (a.line_fft == 2048) go(lines_kernel<2048>, line_warps<2048>());
-  else go(lines_kernel<1024>, line_warps<1024>());
+  if (a.line_fft == 2048) go(lines_kernel<2048>, line_pairs<2048>(), line_threads<2048>());
+  else go(lines_kernel<1024>, line_pairs<1024>(), line_threads<1024>());
 }
 
 void launch_burst_metric(const ChromaArgs& a, int field0, int nfields, cudaStream_t st) {

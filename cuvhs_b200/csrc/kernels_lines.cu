@@ -77,29 +77,49 @@ __device__ double rising_cross(const float* __restrict__ s, int start, int count
   return -1.0;
 }
 
+// One compare-exchange stage of a warp bitonic sort: element e (value x) and
+// element e ^ j (lane ^ j), ascending within blocks of k elements whose
+// index bit k is clear, descending in the others.
+__device__ __forceinline__ float bitonic_stage(float x, int e, int j, int k) {
+  const float y = __shfl_xor_sync(kFull, x, j);
+  const bool keep_min = ((e & k) == 0) == ((e & j) == 0);
+  return keep_min ? fminf(x, y) : fmaxf(x, y);
+}
+
 // Order statistic n/2 of the window (the upper median for even n), n <= 64:
-// lane l ranks samples l and l+32 against the whole window; the sample with
-// (#smaller <= n/2 < #smaller-or-equal) is the order statistic, whichever
-// duplicate supplies it.
+// the window, padded with +inf, is sorted across the warp by a bitonic
+// network (32 elements, one per lane, when n <= 32; else 64, lane l holding
+// elements l and l + 32), and element n/2 is read from its lane.  Ties hold
+// equal values, so the result is the window's order statistic whichever
+// duplicate lands there.
 __device__ double window_median(const float* __restrict__ s, int start, int count, long long total, int lane) {
   if (start < 0 || (long long)start + count > total || count <= 0) return 0.0;
   const int n = min(count, 64);
   const int mid = n / 2;
-  const float x0 = lane < n ? s[start + lane] : 0.0f;
-  const float x1 = lane + 32 < n ? s[start + lane + 32] : 0.0f;
-  int lt0 = 0, le0 = 0, lt1 = 0, le1 = 0;
-  for (int j = 0; j < n; j++) {
-    const float y = __shfl_sync(kFull, j < 32 ? x0 : x1, j & 31);
-    lt0 += y < x0;
-    le0 += y <= x0;
-    lt1 += y < x1;
-    le1 += y <= x1;
+  float x0 = lane < n ? s[start + lane] : INFINITY;
+  if (n <= 32) {
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+      for (int j = k >> 1; j > 0; j >>= 1) x0 = bitonic_stage(x0, lane, j, k);
+    return (double)__shfl_sync(kFull, x0, mid);
   }
-  const bool h0 = lane < n && lt0 <= mid && mid < le0;
-  const bool h1 = lane + 32 < n && lt1 <= mid && mid < le1;
-  const unsigned m0 = __ballot_sync(kFull, h0), m1 = __ballot_sync(kFull, h1);
-  const float v = m0 ? __shfl_sync(kFull, x0, __ffs(m0) - 1) : __shfl_sync(kFull, x1, __ffs(m1) - 1);
-  return (double)v;
+  float x1 = lane + 32 < n ? s[start + lane + 32] : INFINITY;
+#pragma unroll
+  for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j == 32) {  // partners in the same lane; k = 64 sorts ascending
+        const float lo = fminf(x0, x1), hi = fmaxf(x0, x1);
+        x0 = lo;
+        x1 = hi;
+      } else {
+        x0 = bitonic_stage(x0, lane, j, k);
+        x1 = bitonic_stage(x1, lane + 32, j, k);
+      }
+    }
+  }
+  return (double)__shfl_sync(kFull, mid < 32 ? x0 : x1, mid & 31);
 }
 
 // One warp per line location (lines from the first active line to the end of

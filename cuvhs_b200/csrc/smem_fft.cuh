@@ -136,8 +136,14 @@ __device__ __forceinline__ void dft(float2* v) {
 
 template <int THREADS>
 __device__ __forceinline__ void fft_sync() {
-  if constexpr (THREADS == 32) __syncwarp();
-  else __syncthreads();
+  if constexpr (THREADS == 32) {
+    __syncwarp();
+  } else if constexpr (THREADS == 64) {
+    // two-warp transforms: threads [64 g, 64 g + 64) share barrier 1 + g
+    asm volatile("bar.sync %0, 64;" ::"r"(1 + (int)(threadIdx.x >> 6)) : "memory");
+  } else {
+    __syncthreads();
+  }
 }
 
 // One Stockham pass of radix R on an N-point padded buffer, current span NS.
@@ -176,8 +182,9 @@ __device__ __forceinline__ void fft_pass(float2* s, const float2* __restrict__ t
 }
 
 // Full N-point transform (N a power of two, 64 <= N <= 65536), natural order
-// in and out, unnormalised.  Caller must synchronise (CTA, or warp for
-// THREADS == 32) after filling s.  tid: this thread's index among the
+// in and out, unnormalised.  THREADS is 32 (one warp), 64 (two warps of a
+// CTA of up to 15 such groups, synchronised on named barriers) or the CTA.
+// Caller must synchronise the transform's threads after filling s.  tid: this thread's index among the
 // transform's THREADS threads (the lane for a one-warp transform).
 template <int N, int THREADS, bool INV, int NS = 1>
 __device__ __forceinline__ void smem_fft(float2* s, const float2* __restrict__ tw, int tid) {

@@ -227,27 +227,52 @@ __global__ void __launch_bounds__(line_threads<N>(), line_min_ctas<N>())
   }
 }
 
-// One warp per field: mean over line pairs (16+2p, 17+2p), p < 115, of the
-// mean |a + b| over the burst window.
+// One CTA per field: mean over line pairs (16+2p, 17+2p), p < (out_h - 33)/2,
+// of the mean |a + b| over the burst window.  Each thread sums one pair's
+// window in sample order (its loads all issued first), and the first warp
+// adds the pair means exactly as a warp-per-field loop would: lane l takes
+// pairs l, l + 32, ... in order, then a butterfly over the lanes.
 // BL: the burst window length when known at compile time (NTSC 36, PAL 40), 0 = a.burst_len.
+constexpr int kMetricThreads = 256;
 template <int BL>
-__global__ void metric_kernel(ChromaArgs a, int field0, int nfields) {
+__global__ void __launch_bounds__(kMetricThreads) metric_kernel(ChromaArgs a, int field0, int nfields) {
   chain_wait();
+  __shared__ double pair_mean[kMetricThreads];
   const int bl = BL > 0 ? BL : a.burst_len;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= nfields) return;
-  const int f = field0 + warp;
+  const int f = field0 + blockIdx.x;
+  if (blockIdx.x >= nfields) return;  // whole CTA
   const int skip = 16;
-  const int npairs = (a.out_h - 2 * skip - 1) / 2;
-  double acc = 0.0;
-  for (int p = lane; p < npairs; p += 32) {
+  const int npairs = min((a.out_h - 2 * skip - 1) / 2, kMetricThreads);
+  for (int p = threadIdx.x; p < npairs; p += kMetricThreads) {
     const int line = f * a.out_h + skip + 2 * p;
     const float* x = a.burst + (size_t)line * bl;
     const float* y = x + bl;
     double s = 0.0;
-    for (int i = 0; i < bl; i++) s += fabs((double)x[i] + (double)y[i]);
-    acc += s / bl;
+    if constexpr (BL > 0 && BL % 4 == 0) {
+      // rows start on 16-byte boundaries (BL floats per row)
+      float4 xv[BL / 4], yv[BL / 4];
+#pragma unroll
+      for (int q = 0; q < BL / 4; q++) {
+        xv[q] = __ldg(reinterpret_cast<const float4*>(x) + q);
+        yv[q] = __ldg(reinterpret_cast<const float4*>(y) + q);
+      }
+#pragma unroll
+      for (int q = 0; q < BL / 4; q++) {
+        s += fabs((double)xv[q].x + (double)yv[q].x);
+        s += fabs((double)xv[q].y + (double)yv[q].y);
+        s += fabs((double)xv[q].z + (double)yv[q].z);
+        s += fabs((double)xv[q].w + (double)yv[q].w);
+      }
+    } else {
+      for (int i = 0; i < bl; i++) s += fabs((double)x[i] + (double)y[i]);
+    }
+    pair_mean[p] = s / bl;
   }
+  __syncthreads();
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  double acc = 0.0;
+  for (int p = lane; p < npairs; p += 32) acc += pair_mean[p];
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
   if (lane == 0) a.metric[f] = npairs > 0 ? acc / npairs : 1e9;
 }
@@ -282,9 +307,9 @@ void launch_chroma_lines(const ChromaArgs& a, int field0, int nfields, bool writ
 
 void launch_burst_metric(const ChromaArgs& a, int field0, int nfields, cudaStream_t st) {
   if (nfields <= 0) return;
-  const int threads = 128;
-  const int blocks = (nfields * 32 + threads - 1) / threads;
-  auto go = [&](auto kernel) { launch_chained(kernel, dim3(blocks), dim3(threads), 0, st, a, field0, nfields); };
+  auto go = [&](auto kernel) {
+    launch_chained(kernel, dim3(nfields), dim3(kMetricThreads), 0, st, a, field0, nfields);
+  };
   if (a.burst_len == 36) go(metric_kernel<36>);
   else if (a.burst_len == 40) go(metric_kernel<40>);
   else go(metric_kernel<0>);

@@ -207,20 +207,30 @@ __global__ void __launch_bounds__(kThreadsB, 1) k1b_kernel(DemodArgs a, int f_be
   const int last = (int)a.total - 1;
   const int base = j0 - a.b_pos;
   float2 v[16];
+  const int span = a.b_out + N;  // tile positions [base, base + span) are read
+  if (base >= 0 && base + span <= a.tile && tile0 + base >= 0 && tile0 + base + span - 1 <= last) {
+    // interior: no wrap inside the tile, no clamp at the chunk ends
+    const float* p = a.dem + (tile0 + base + t);
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
-    const int q0 = base + t + T * q;
-    const int p0 = min(max(tile0 + wrap_tile(q0, a.tile), 0), last);
-    const int p1 = min(max(tile0 + wrap_tile(q0 + a.b_out, a.tile), 0), last);
-    v[q] = make_float2(__ldg(&a.dem[p0]), __ldg(&a.dem[p1]));
+    for (int q = 0; q < 16; q++) v[q] = make_float2(__ldg(p + T * q), __ldg(p + T * q + a.b_out));
+  } else {
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int q0 = base + t + T * q;
+      const int p0 = min(max(tile0 + wrap_tile(q0, a.tile), 0), last);
+      const int p1 = min(max(tile0 + wrap_tile(q0 + a.b_out, a.tile), 0), last);
+      v[q] = make_float2(__ldg(&a.dem[p0]), __ldg(&a.dem[p1]));
+    }
   }
   pair_spectra<N, false>(v, sA, sB, a.gb, a.tw_b, t);
-  RegFFT<N>::run<true>(v, sB, a.tw_b_inv, t);
+  // both blocks' inverses in lockstep (sB and sA as their buffers)
+  float2 v2[16];
+  __syncthreads();  // Z2 complete in sA
+  load_second<N, false>(v2, sA, t);
+  RegFFT<N>::run2<true>(v, sB, v2, sA, a.tw_b_inv, opaque_index(t));
   k1b_emit<T>(a, v, f, j0, t);
-  if (kOverlap + (blk0 + 1) * a.b_out >= kOverlap + a.spp) return;  // whole CTA
-  load_second<N, false>(v, sA, t);
-  RegFFT<N>::run<true>(v, sA, a.tw_b_inv, t);
-  k1b_emit<T>(a, v, f, j0 + a.b_out, t);
+  if (kOverlap + (blk0 + 1) * a.b_out >= kOverlap + a.spp) return;  // the second block lies past the tile
+  k1b_emit<T>(a, v2, f, j0 + a.b_out, t);
 }
 
 // Threshold edges in sample order.  Each thread owns 16 consecutive samples

@@ -129,14 +129,17 @@ __device__ __forceinline__ HetLine het_line(const ChromaArgs& a, int gl) {
 }
 
 // Heterodyned, resampled chroma sample of line L at column c (frac = c / out_w).
+// The loads do not depend on the range test (an out-of-range column reads
+// the first samples and is zeroed at the end), so an unrolled caller keeps
+// several columns' loads in flight.
 __device__ __forceinline__ float het_at(const ChromaArgs& a, const HetLine& L, double frac, int c) {
-  if (!L.ok) return 0.0f;
   const double coord = L.a0 + frac * L.span;
   const int ci = (int)coord;
-  if (ci < 1 || (long long)ci + 2 >= a.total) return 0.0f;
+  const bool ok = L.ok && ci >= 1 && (long long)ci + 2 < a.total;
+  const int cl = ok ? ci : 1;
   const float x = (float)(coord - (double)ci);
-  const float p0 = __ldg(&a.pre[ci - 1]), p1 = __ldg(&a.pre[ci]);
-  const float p2 = __ldg(&a.pre[ci + 1]), p3 = __ldg(&a.pre[ci + 2]);
+  const float p0 = __ldg(&a.pre[cl - 1]), p1 = __ldg(&a.pre[cl]);
+  const float p2 = __ldg(&a.pre[cl + 1]), p3 = __ldg(&a.pre[cl + 2]);
   const float c1 = p2 - p0;
   const float c2 = 2.0f * p0 - 5.0f * p1 + 4.0f * p2 - p3;
   const float c3 = 3.0f * (p1 - p2) + p3 - p0;
@@ -145,7 +148,7 @@ __device__ __forceinline__ float het_at(const ChromaArgs& a, const HetLine& L, d
   const double u = a.het_scale * (double)(L.ubase + c);
   const float fr = (float)(u - floor(u));
   const float het = -cospif(2.0f * fr + L.lpf);
-  return v * het;
+  return ok ? v * het : 0.0f;
 }
 
 template <int N>

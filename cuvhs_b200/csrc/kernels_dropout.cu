@@ -33,6 +33,7 @@ constexpr int kThreadsD = 256;       // fused kernel and class kernel
 constexpr int kThreadsScan = 512;    // two-pass scan kernel
 constexpr int kMaxEvents = 2048;
 constexpr int kStage = kThreadsD * 16;  // envelope samples one class CTA stages
+constexpr int kMaxEnvBlocks = 1024;     // envelope partials a class CTA holds in shared memory
 
 __device__ int find_line(const double* ll, int als, int n, double pos) {
   if (pos < ll[als] || pos >= ll[als + n]) return -1;
@@ -228,6 +229,7 @@ __global__ void __launch_bounds__(kThreadsD) dropout_kernel(DropoutArgs a) {
 __global__ void __launch_bounds__(kThreadsD) dropout_class_kernel(DropoutArgs a) {
   chain_wait();
   __shared__ float stage[kThreadsD * 17];
+  __shared__ double part[kMaxEnvBlocks];
   __shared__ double down_s;
   const int f = blockIdx.y, tid = threadIdx.x;
   int s0, s1;
@@ -235,11 +237,24 @@ __global__ void __launch_bounds__(kThreadsD) dropout_class_kernel(DropoutArgs a)
   const int nb = min((s1 - s0 + 15) / 16, a.max_blocks);
   const int b_first = blockIdx.x * kThreadsD;
   if (s1 <= s0 || b_first >= nb) return;  // whole CTA leaves together
-  if (tid == 0) down_s = down_threshold(a, f);
+  // the field's envelope partial sums, loaded in parallel with the stage
+  const bool part_in_smem = a.env_blocks <= kMaxEnvBlocks;
+  if (part_in_smem)
+    for (int b = tid; b < a.env_blocks; b += kThreadsD) part[b] = a.env_part[(size_t)f * a.env_blocks + b];
   const int x0 = s0 + b_first * 16;
   const int nx = min(kStage, s1 - x0);
   for (int i = tid; i < kStage; i += kThreadsD)
     stage[(i >> 4) * 17 + (i & 15)] = i < nx ? __ldg(&a.env[x0 + i]) : 0.0f;
+  __syncthreads();
+  if (tid == 0) {
+    // summed in partial order, as down_threshold
+    double tot = 0.0;
+    if (part_in_smem)
+      for (int b = 0; b < a.env_blocks; b++) tot += part[b];
+    else
+      for (int b = 0; b < a.env_blocks; b++) tot += a.env_part[(size_t)f * a.env_blocks + b];
+    down_s = tot / (double)a.spp * 0.18;
+  }
   __syncthreads();
   const int b = b_first + tid;
   if (b >= nb) return;

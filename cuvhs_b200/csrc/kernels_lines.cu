@@ -188,23 +188,25 @@ __global__ void __launch_bounds__(kLumaThreads) luma_kernel(LineArgs a) {
   const double a0 = a.ll[(size_t)field * a.lines_per_frame + row];
   const double a1 = a.ll[(size_t)field * a.lines_per_frame + row + 1];
   const double span = a1 - a0;
+  // The loads do not depend on the range test (an out-of-range column reads
+  // the first samples and writes the out-of-range value), so the unrolled
+  // loop keeps several columns' loads in flight.
+#pragma unroll 4
   for (int col = threadIdx.x; col < W; col += kLumaThreads) {
     const double coord = a0 + __ldg(&a.col_frac[col]) * span;
     const int ci = (int)coord;
-    uint16_t o = a.oob_value;
-    if (ci >= 1 && (long long)ci + 2 < a.total) {
-      const float x = (float)(coord - (double)ci);
-      const float p0 = __ldg(&a.video[ci - 1]), p1 = __ldg(&a.video[ci]);
-      const float p2 = __ldg(&a.video[ci + 1]), p3 = __ldg(&a.video[ci + 2]);
-      const float c1 = p2 - p0;
-      const float c2 = 2.0f * p0 - 5.0f * p1 + 4.0f * p2 - p3;
-      const float c3 = 3.0f * (p1 - p2) + p3 - p0;
-      const float hz = p1 + 0.5f * x * (c1 + x * (c2 + x * c3));
-      float v = hz * a.luma_gain + a.luma_offset;
-      v = fminf(fmaxf(v, 0.0f), 65535.0f);
-      o = (uint16_t)(v + 0.5f);
-    }
-    out[col] = o;
+    const bool ok = ci >= 1 && (long long)ci + 2 < a.total;
+    const int cl = ok ? ci : 1;
+    const float x = (float)(coord - (double)ci);
+    const float p0 = __ldg(&a.video[cl - 1]), p1 = __ldg(&a.video[cl]);
+    const float p2 = __ldg(&a.video[cl + 1]), p3 = __ldg(&a.video[cl + 2]);
+    const float c1 = p2 - p0;
+    const float c2 = 2.0f * p0 - 5.0f * p1 + 4.0f * p2 - p3;
+    const float c3 = 3.0f * (p1 - p2) + p3 - p0;
+    const float hz = p1 + 0.5f * x * (c1 + x * (c2 + x * c3));
+    float v = hz * a.luma_gain + a.luma_offset;
+    v = fminf(fmaxf(v, 0.0f), 65535.0f);
+    out[col] = ok ? (uint16_t)(v + 0.5f) : a.oob_value;
   }
 }
 

@@ -243,8 +243,13 @@ __global__ void __launch_bounds__(kThreadsD) dropout_class_kernel(DropoutArgs a)
     for (int b = tid; b < a.env_blocks; b += kThreadsD) part[b] = a.env_part[(size_t)f * a.env_blocks + b];
   const int x0 = s0 + b_first * 16;
   const int nx = min(kStage, s1 - x0);
-  for (int i = tid; i < kStage; i += kThreadsD)
-    stage[(i >> 4) * 17 + (i & 15)] = i < nx ? __ldg(&a.env[x0 + i]) : 0.0f;
+  // loads at a clamped index, so that all of a thread's loads are in flight
+  // at once; samples past the range are zeroed afterwards
+#pragma unroll
+  for (int i = tid; i < kStage; i += kThreadsD) {
+    const float e = __ldg(&a.env[x0 + min(i, nx - 1)]);
+    stage[(i >> 4) * 17 + (i & 15)] = i < nx ? e : 0.0f;
+  }
   __syncthreads();
   if (tid == 0) {
     // summed in partial order, as down_threshold

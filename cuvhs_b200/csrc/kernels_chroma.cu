@@ -34,17 +34,17 @@ constexpr int kThreadsC = Design::kNc / kElemsC;
 template <int N>
 __host__ __device__ constexpr int line_tp() { return N <= 1024 ? 64 : 32; }
 template <int N>
-__host__ __device__ constexpr int line_pairs() { return 2; }
+__host__ __device__ constexpr int line_pairs() { return 2; }  // at most 4 (the two-warp barriers)
 template <int N>
 __host__ __device__ constexpr int line_threads() { return line_tp<N>() * line_pairs<N>(); }
 template <int N>
 __host__ __device__ constexpr int line_min_ctas() { return N <= 1024 ? 8 : 1; }
 
-// Barrier of one line pair's threads.
+// Barrier of one line pair's threads (the transform's barrier).
 template <int TP>
 __device__ __forceinline__ void pair_sync() {
-  if constexpr (TP == 32) __syncwarp();
-  else asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)(threadIdx.x / TP)), "r"(TP) : "memory");
+  static_assert(TP == 32 || TP == 64, "one or two warps per line pair");
+  fft_sync<TP>();
 }
 
 // Two adjacent output blocks ride in the real and imaginary parts of one

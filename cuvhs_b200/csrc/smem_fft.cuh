@@ -139,8 +139,14 @@ __device__ __forceinline__ void fft_sync() {
   if constexpr (THREADS == 32) {
     __syncwarp();
   } else if constexpr (THREADS == 64) {
-    // two-warp transforms: threads [64 g, 64 g + 64) share barrier 1 + g
-    asm volatile("bar.sync %0, 64;" ::"r"(1 + (int)(threadIdx.x >> 6)) : "memory");
+    // two-warp transforms: threads [64 g, 64 g + 64) share barrier 1 + g.
+    // Immediate barrier ids: with a register id the compiler reserves all 16
+    // barriers per CTA, which caps residency at 4 CTAs per SM.
+    const int g = threadIdx.x >> 6;
+    if (g == 0) asm volatile("bar.sync 1, 64;" ::: "memory");
+    else if (g == 1) asm volatile("bar.sync 2, 64;" ::: "memory");
+    else if (g == 2) asm volatile("bar.sync 3, 64;" ::: "memory");
+    else asm volatile("bar.sync 4, 64;" ::: "memory");
   } else {
     __syncthreads();
   }
@@ -183,7 +189,7 @@ __device__ __forceinline__ void fft_pass(float2* s, const float2* __restrict__ t
 
 // Full N-point transform (N a power of two, 64 <= N <= 65536), natural order
 // in and out, unnormalised.  THREADS is 32 (one warp), 64 (two warps of a
-// CTA of up to 15 such groups, synchronised on named barriers) or the CTA.
+// CTA of up to 4 such groups, synchronised on named barriers) or the CTA.
 // Caller must synchronise the transform's threads after filling s.  tid: this thread's index among the
 // transform's THREADS threads (the lane for a one-warp transform).
 template <int N, int THREADS, bool INV, int NS = 1>

@@ -156,6 +156,7 @@ __global__ void __launch_bounds__(line_threads<N>(), line_min_ctas<N>())
     lines_kernel(ChromaArgs a, int line0, int nlines, int write_output) {
   chain_wait();
   constexpr int TP = line_tp<N>(), P = line_pairs<N>();
+  static_assert(TP == 32 || P <= 4, "two-warp pairs use named barriers 1..4");
   __shared__ float2 sm_all[P][fft_pad(N)];
   __shared__ float acc_sh[P][2];
   const int g = threadIdx.x / TP, tid = threadIdx.x % TP, lane = threadIdx.x & 31;

@@ -152,6 +152,25 @@ def test_decode_is_deterministic_and_chunk_api_matches_capture_api():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["dropouts28", "dropouts28pal"])
+def test_chained_launches_match_event_separated_launches(name):
+    """The decode kernels are launched as a chain (each may be scheduled
+    while its predecessor drains and waits for it on the device); with every
+    stage bracketed by timing events they run strictly one after another.
+    Both must give the same bytes."""
+    x = workload(name)
+    with cv.Decoder(rate_mhz(name), system=system(name)) as d:
+        chained = d.decode_capture(x)
+        d.reset()
+        d.set_timing(True)
+        separated = d.decode_capture(x)
+        d.set_timing(False)
+    assert np.array_equal(chained.luma, separated.luma)
+    assert np.array_equal(chained.chroma, separated.chroma)
+    assert chained.json == separated.json
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("name,batch", [("dropouts28", 0), ("plain40_28", 8)])
 def test_pinned_buffers_give_identical_output(name, batch):
     """Page-locked input and output buffers take the overlapped path (input in

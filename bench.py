@@ -157,50 +157,64 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def _workload_table():
+    """The workload parameter table, read by path: importing the package would
+    load libcuvhs into this process."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("cuvhs_workload_table",
+                                                  os.path.join(ROOT, "cuvhs_b200", "workload_table.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def run_reference(args, rank):
-    """Reference arm: the reference's own decoder built from its sources."""
+    """Reference arm: the reference's own decoder, built from its sources
+    (oracle/_ref/ref_harness: its Pipeline chunk loop, timed from after buffer
+    allocation), one process per step on the workload's input file.  The input
+    is written by the stand-alone synthesizer (cuvhs-synth), so neither this
+    process nor any child loads libcuvhs."""
     if rank != 0:
         return 0
-    from cuvhs_b200 import make_workload, WORKLOADS
-    from oracle.oracle import REF_HARNESS
-    if not os.path.exists(REF_HARNESS):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built "
-                          "(the reference is built from its sources by __graft_entry__.build())"}))
-        return 0
-    mhz = WORKLOADS[WORKLOAD]["sample_rate_hz"] / 1e6
-    x = make_workload(WORKLOAD)
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    synth = os.path.join(ROOT, "cuvhs_b200", "bin", "cuvhs-synth")
+    for path, what in ((harness, "oracle/_ref/ref_harness (the reference built from its sources by "
+                                 "__graft_entry__.build())"), (synth, "cuvhs_b200/bin/cuvhs-synth")):
+        if not os.path.exists(path):
+            print(json.dumps({"impl": "reference", "unavailable": f"{what} not built"}))
+            return 0
+    params = _workload_table().WORKLOADS[WORKLOAD]
+    mhz = params["sample_rate_hz"] / 1e6
     d = tempfile.mkdtemp(prefix="cuvhs_ref_", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
     inp = os.path.join(d, "in.u8")
-    x.tofile(inp)
-    # each reference run is a whole decode (~1 s with the process start), so
-    # the arm times at most 5 of them after one warm-up, whatever K is asked
-    n_warm, n_time = min(args.warmup, 1), max(1, min(args.steps, 5))
-    runs = []
-    for i in range(n_warm + n_time):
-        out = subprocess.run([REF_HARNESS, "-f", str(mhz), "--time", inp, os.path.join(d, "out")],
-                             capture_output=True, text=True)
-        if out.returncode != 0:
-            print(json.dumps({"impl": "reference", "unavailable": f"reference harness exited {out.returncode}"}))
-            return 0
-        runs.append(json.loads(out.stdout.strip().splitlines()[-1]))
-    timed = runs[n_warm:]
+    try:
+        subprocess.run([synth] + [f"{k}={v}" for k, v in params.items()] + [inp], check=True)
+        runs = []
+        for i in range(args.warmup + args.steps):
+            out = subprocess.run([harness, "-f", str(mhz), "--time", inp, os.path.join(d, "out")],
+                                 capture_output=True, text=True)
+            if out.returncode != 0:
+                print(json.dumps({"impl": "reference", "unavailable": f"reference harness exited {out.returncode}"}))
+                return 0
+            runs.append(json.loads(out.stdout.strip().splitlines()[-1]))
+    finally:
+        for fn in os.listdir(d):
+            os.unlink(os.path.join(d, fn))
+        os.rmdir(d)
+    timed = runs[args.warmup:]
     fields = sum(r["fields"] for r in timed)
     secs = sum(r["seconds"] for r in timed)
     value = fields / secs
-    for fn in os.listdir(d):
-        os.unlink(os.path.join(d, fn))
-    os.rmdir(d)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "fields/s", "n_gpus": 1,
-        "steps": n_time, "warmup": n_warm, "requested_steps": args.steps,
-        "ms_per_step": round(1000 * secs / n_time, 3),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * secs / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD_DESC, "fields_per_step": timed[0]["fields"],
-                   "reference_batch_fields": timed[0]["batch_size"],
-                   "timing": "reference Pipeline chunk loop after buffer allocation (file in /dev/shm, "
-                             "TBC/JSON written to /dev/shm)"},
+                   "reference_batch_fields": timed[0]["batch_size"], "chunks_per_step": timed[0]["chunks"],
+                   "timing": "one reference process per step: its Pipeline chunk loop after buffer allocation "
+                             "(input file in /dev/shm, TBC/JSON written to /dev/shm)"},
         "cpu_baseline": {"value": round(value, 3), "unit": "fields/s", "cores": 1, "kind": "reference",
-                         "sample": f"{WORKLOAD}, reference CUDA build on GPU 0, {n_time} runs"},
+                         "sample": f"{WORKLOAD}, reference CUDA build on GPU 0, {args.steps} timed runs"},
         "e2e": {"value": round(value, 3), "unit": "fields/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -208,18 +222,26 @@ def run_reference(args, rank):
 
 
 def cpu_baseline():
-    """FP64 oracle port on all host cores, bounded sample (6 fields)."""
+    """FP64 oracle port on all host cores over the benchmark's own workload,
+    bounded to its first 40 fields (the whole 40-field capture of the default
+    workload, ~10 s on 16 cores)."""
     try:
         from oracle.oracle import Oracle
-        from cuvhs_b200 import make_workload
-        x = make_workload("small28")
+        import cuvhs_b200 as cv
+        x = cv.make_workload(WORKLOAD)
+        mhz = cv.WORKLOADS[WORKLOAD]["sample_rate_hz"] / 1e6
+        spf = int(round(mhz * 1e6 / 15734.264)) * 263
+        n_fields = min(40, x.size // spf)
+        # the first n_fields fields plus one tile's margin, so each decoded
+        # field has its whole analysis window
+        x = x[:min(x.size, (n_fields + 1) * spf + 20 * (spf // 263))]
         cores = os.cpu_count() or 1
-        o = Oracle(28.0, threads=cores)
+        o = Oracle(mhz, threads=cores)
         t = time.perf_counter()
         n = o.decode(x)
         dt = time.perf_counter() - t
         return {"value": round(n / dt, 3), "unit": "fields/s", "cores": cores, "kind": "port",
-                "sample": f"{n} fields at 28 MHz (small28 synthetic capture), FP64 oracle, {dt:.1f} s"}
+                "sample": f"{WORKLOAD}: the first {n} fields, FP64 oracle on {cores} host threads, {dt:.1f} s"}
     except Exception as e:  # the baseline is reported, never required
         return {"value": None, "unit": "fields/s", "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
 

@@ -21,7 +21,8 @@ namespace cuvhs {
 __device__ __forceinline__ void chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 template <typename... P, typename... A>
-inline void launch_chained(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args) {
+inline cudaError_t launch_chained(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                                  A&&... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
@@ -32,8 +33,8 @@ inline void launch_chained(void (*kernel)(P...), dim3 grid, dim3 block, size_t s
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  // a failed launch is reported by the caller's cudaGetLastError check
-  (void)cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+  // callers that ignore the result see a failed launch in their cudaGetLastError check
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
 }
 
 }  // namespace cuvhs

@@ -94,6 +94,11 @@ struct Design {
   void build_cached(const Format& fmt);
 };
 
+// Half-support (samples each side) of the truncated K1a kernel at a capture
+// rate: a K1a block of Design::kNa samples yields kNa - 2 * h - 1 outputs,
+// the first at block position h + 1 (Design::a_pos, Design::a_out).
+int k1a_half_support(double fs_hz);
+
 // ---------------------------------------------------------------- kernels
 struct DemodArgs {
   const uint8_t* raw;  // chunk samples in the input format (raw_input.cuh)
@@ -203,8 +208,12 @@ struct DropoutArgs {
   unsigned char* cls = nullptr;  // two-pass form: [fields * max_blocks]
   int max_blocks = 0;            // 16-sample blocks per field slot, dropout_class_bytes_per_field(spp)
 };
-// Fused form: one CTA per field, no scratch beyond env_part.
-void launch_dropouts(const DropoutArgs& a, cudaStream_t st);
+// Dynamic shared memory cap of the kernels that hold one field's class bytes
+// (dropout_class_bytes_per_field(spp) must not exceed it).
+constexpr int kMaxClassBytes = 200 * 1024;
+// Fused form: one CTA per field, no scratch beyond env_part.  Returns the
+// error of the attribute set or of the launch.
+cudaError_t launch_dropouts(const DropoutArgs& a, cudaStream_t st);
 // Two-pass form: wide class kernel over every field, then a per-field scan
 // that maps the entries and conceals the luma; chroma concealment follows
 // once the chroma planes are final.

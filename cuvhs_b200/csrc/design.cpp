@@ -145,6 +145,8 @@ std::vector<float2> twiddles(int n) {
 
 }  // namespace
 
+int k1a_half_support(double fs_hz) { return half_support(fs_hz, 13.7, 64, 1024); }
+
 void Format::init(double mhz, int sys) {
   system = sys == kPal ? kPal : kNtsc;
   fs_hz = mhz * 1e6;
@@ -220,7 +222,7 @@ void Design::build(const Format& fmt) {
       H[k] = bw_bandpass(w, wbl, wbh, 8) * bw_lowpass(w, wl, 8) * bw_highpass(w, wh, 8) * hil;
     }
     std::vector<cd> g = host_dft(H, +1);  // unnormalised inverse, as the reference's C2C
-    a_neg = a_pos = half_support(fs, 13.7, 64, 1024);
+    a_neg = a_pos = k1a_half_support(fs);
     a_out = kNa - a_neg - a_pos - 1;
     std::vector<cd> blk;
     a_tail = place_kernel(g, a_neg, a_pos, kNa, blk);

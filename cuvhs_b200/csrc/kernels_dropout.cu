@@ -382,11 +382,17 @@ __global__ void dropout_chroma_kernel(DropoutArgs a, int f0, int nf) {
 
 }  // namespace
 
-void launch_dropouts(const DropoutArgs& a, cudaStream_t st) {
-  if (a.fields <= 0) return;
+// The per-field class bytes live in dynamic shared memory.  Both kernels that
+// hold them are given the same fixed cap (kMaxClassBytes, not the size one
+// call needs), so contexts of different rates on different host threads never
+// lower the cap between another thread's set and its launch.
+cudaError_t launch_dropouts(const DropoutArgs& a, cudaStream_t st) {
+  if (a.fields <= 0) return cudaSuccess;
   const size_t smem = (size_t)a.max_blocks;
-  cudaFuncSetAttribute(dropout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  launch_chained(dropout_kernel, dim3(a.fields), dim3(kThreadsD), smem, st, a);
+  if (smem > (size_t)kMaxClassBytes) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(dropout_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxClassBytes);
+  if (e != cudaSuccess) return e;
+  return launch_chained(dropout_kernel, dim3(a.fields), dim3(kThreadsD), smem, st, a);
 }
 
 size_t dropout_class_bytes_per_field(int spp) { return (size_t)(((spp + 15) / 16 + 15) / 16 * 16); }
@@ -396,7 +402,7 @@ void launch_dropouts_two_pass(const DropoutArgs& a, cudaStream_t st) {
   dim3 grid((a.max_blocks + kThreadsD - 1) / kThreadsD, a.fields);
   launch_chained(dropout_class_kernel, grid, dim3(kThreadsD), 0, st, a);
   const size_t smem = (size_t)a.max_blocks;
-  cudaFuncSetAttribute(dropout_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(dropout_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxClassBytes);
   launch_chained(dropout_scan_kernel, dim3(a.fields), dim3(kThreadsScan), smem, st, a);
 }
 

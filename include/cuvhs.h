@@ -285,13 +285,16 @@ cuvhs_status cuvhs_stage_chroma_decode(cuvhs_ctx* ctx, const void* d_raw, size_t
  *   d_count [fields], d_lines/d_startx/d_endx [fields * 512]  outputs
  *   stream      a cudaStream_t (NULL = default stream); the call is asynchronous
  * The only scratch is a fixed device array of CUVHS_NOALLOC_MAX_PARTIALS
- * doubles (256 KiB, one per envelope block of 4096 samples), shared by all
- * calls on a device and held by every GPU that loads the library until the
- * process exits: calls that overlap on the GPU race on it.  Sizes needing more
- * partial sums (fields * ceil(tile_stride / 4096) > the maximum: about 266
- * fields at 28 MHz, 186 at 40 MHz) return CUVHS_ERR_CAPACITY.  The first call
- * on each device looks up the array's device address; make that first call
- * before any stream capture. */
+ * doubles (256 KiB, one per envelope block of the decoder's demodulator:
+ * 3,327 samples at 28 MHz, 2,943 at 40 MHz), shared by all calls on a device
+ * and held by every GPU that loads the library until the process exits:
+ * calls that overlap on the GPU race on it.  Sizes needing more partial sums
+ * (about 215 fields at 28 MHz, 156 at 35.8 MHz, 133 at 40 MHz) return
+ * CUVHS_ERR_CAPACITY.  The first call on each device (and again in a new
+ * context, e.g. after cudaDeviceReset) looks up the array's device address;
+ * make that first call before any stream capture.  An error left pending by
+ * an earlier CUDA call is left pending and the call returns CUVHS_ERR_CUDA
+ * without launching anything. */
 #define CUVHS_NOALLOC_MAX_PARTIALS 32768
 cuvhs_status cuvhs_dropouts_noalloc(const float* d_envelope, const double* d_linelocs, int fields, int tile_stride,
                                     uint16_t* d_luma, uint16_t* d_chroma, int32_t* d_count, int32_t* d_lines,

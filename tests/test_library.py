@@ -130,3 +130,22 @@ def test_invalid_config_rejected():
     cfg.sample_rate_mhz = 1.0
     assert cv.lib.cuvhs_create(ctypes.byref(cfg), ctypes.byref(h)) == 1
     assert cv.lib.cuvhs_create(None, ctypes.byref(h)) == 1
+
+
+@pytest.mark.parametrize("name", ["small28", "dropouts28pal"])
+def test_synth_tool_writes_the_workload_bytes(name, tmp_path):
+    """cuvhs-synth (the synthesizer without the decoder, used where a process
+    must not load libcuvhs) writes the same bytes as make_workload."""
+    import subprocess
+    from cuvhs_b200.workload_table import WORKLOADS
+    tool = os.path.join(os.path.dirname(cv.CLI_PATH), "cuvhs-synth")
+    out = tmp_path / "in.u8"
+    subprocess.run([tool] + [f"{k}={v}" for k, v in WORKLOADS[name].items()] + [str(out)], check=True)
+    assert np.array_equal(np.fromfile(out, np.uint8), cv.make_workload(name))
+
+
+def test_synth_tool_rejects_unknown_parameters(tmp_path):
+    import subprocess
+    tool = os.path.join(os.path.dirname(cv.CLI_PATH), "cuvhs-synth")
+    r = subprocess.run([tool, "no_such_field=1", str(tmp_path / "x.u8")], capture_output=True, text=True)
+    assert r.returncode == 2 and "bad parameter" in r.stderr

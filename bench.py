@@ -62,11 +62,12 @@ def stage_bytes_per_field(stage, fs_hz):
         "chroma_lines": 4 * N + 2 * F,
         "burst_metric": 0.0,
         "dropouts": 4 * N,
+        "sync_guard": 0.0,                 # FP64 re-evaluation of a few near-threshold sync samples
     }[stage]
 
 
 STAGES = ("k1a_demod", "k1b_video_sync", "sync_edges", "hsync_refine", "luma_resample", "chroma_prefilter",
-          "chroma_lines", "burst_metric", "dropouts")
+          "chroma_lines", "burst_metric", "dropouts", "sync_guard")
 
 
 def stage_bytes_total(fs_hz):
@@ -244,6 +245,53 @@ def cpu_baseline():
                 "sample": f"{WORKLOAD}: the first {n} fields, FP64 oracle on {cores} host threads, {dt:.1f} s"}
     except Exception as e:  # the baseline is reported, never required
         return {"value": None, "unit": "fields/s", "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
+
+
+def fp64_report(name, mhz):
+    """FP32 decode against the FP64 oracle decode of the whole workload (one
+    chunk each): every field whose analysis window lies inside the capture."""
+    import cuvhs_b200 as cv
+    from oracle.oracle import Oracle
+    x = cv.make_workload(name)
+    with cv.Decoder(mhz, debug=True) as d:
+        r = d.decode_capture(x)
+        dbg = {k: d.debug_array(k) for k in ("field_offsets", "k2_pulse_count", "k2_pulse_starts",
+                                             "k2_pulse_lengths", "k2b_pulse_count", "k2b_pulse_starts",
+                                             "k2b_pulse_lengths", "k2b_pulse_types", "linelocs_coarse", "linelocs")}
+    t = time.perf_counter()
+    o = Oracle(mhz, threads=os.cpu_count() or 1)
+    o.decode(x)
+    t_oracle = time.perf_counter() - t
+    mf, of = json.loads(r.json)["fields"], json.loads(o.json)["fields"]
+    spp = int(round(mhz * 1e6 / 15734.264)) * 283
+    inside = [i for i, f in enumerate(mf) if int(f["fileLoc"]) + spp <= x.size]
+    P = len(dbg["field_offsets"])
+    lpf, rows = o.lines_per_frame, o.field_shape[0] + 1
+    pulses_exact = True
+    for pre in ("k2", "k2b"):
+        cm, co = dbg[f"{pre}_pulse_count"], o.array(0, f"{pre}_pulse_count")
+        for part in ["starts", "lengths"] + (["types"] if pre == "k2b" else []):
+            a = dbg[f"{pre}_pulse_{part}"].reshape(P, 800)
+            b = o.array(0, f"{pre}_pulse_{part}").reshape(P, 800)
+            for f in inside:
+                pulses_exact &= bool(cm[f] == co[f] and np.array_equal(a[f, :cm[f]], b[f, :co[f]]))
+    llc = dbg["linelocs_coarse"].reshape(P, lpf)[inside, :rows]
+    ll = dbg["linelocs"].reshape(P, lpf)[inside, :rows]
+    ollc = o.array(0, "linelocs_coarse").reshape(P, lpf)[inside, :rows]
+    oll = o.array(0, "linelocs").reshape(P, lpf)[inside, :rows]
+    dpos = np.abs(ll - oll)
+
+    def tbc(a, b):
+        d = np.abs(a[inside].astype(np.int32) - b[inside].astype(np.int32))
+        return {"max_lsb": int(d.max()), "frac_1lsb": round(float((d == 1).mean()), 6),
+                "frac_over_1lsb": float((d > 1).mean())}
+    return {"fields_compared": len(inside), "oracle_seconds": round(t_oracle, 1),
+            "json_fields_identical": all(mf[i] == of[i] for i in inside),
+            "field_offsets_identical": bool(np.array_equal(dbg["field_offsets"], o.array(0, "field_offsets"))),
+            "pulses_identical": pulses_exact,
+            "coarse_linelocs_identical": bool(np.array_equal(llc, ollc)),
+            "refined_position_err_samples": {"max": float(dpos.max()), "rms": float(np.sqrt((dpos ** 2).mean()))},
+            "luma": tbc(r.luma, o.luma), "chroma": tbc(r.chroma, o.chroma)}
 
 
 def profile_case():
@@ -487,6 +535,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-report", action="store_true",
+                    help="hard600_40: skip the FP32-vs-FP64-oracle error report (an oracle decode of 600 fields)")
     ap.add_argument("--clock-interval-ms", type=int, default=25,
                     help="nvidia-smi sampling period during the timed region (0 = off)")
     ap.add_argument("--profile-case", action="store_true",
@@ -684,6 +734,8 @@ def main():
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
+        if WORKLOAD == "hard600_40" and world == 1 and not args.no_fp64_report:
+            line["fp32_vs_fp64"] = fp64_report(WORKLOAD, mhz)
         print(json.dumps(line))
     dec.close()
     if world > 1:

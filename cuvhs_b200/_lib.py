@@ -41,7 +41,7 @@ class CuvhsError(RuntimeError):
 class Config(ctypes.Structure):
     _fields_ = [("system", ctypes.c_int), ("sample_rate_mhz", ctypes.c_double), ("device", ctypes.c_int),
                 ("batch_fields", ctypes.c_int), ("stream_mode", ctypes.c_int), ("input_format", ctypes.c_int),
-                ("dc_correct", ctypes.c_int), ("single_pass_lines", ctypes.c_int)]
+                ("dc_correct", ctypes.c_int), ("single_pass_lines", ctypes.c_int), ("guard_band_hz", ctypes.c_double)]
 
 
 class FieldInfo(ctypes.Structure):
@@ -56,6 +56,18 @@ class Output(ctypes.Structure):
                 ("dropout_endx", ctypes.c_void_p), ("max_fields", ctypes.c_size_t),
                 ("max_dropouts", ctypes.c_size_t), ("fields_out", ctypes.c_size_t),
                 ("dropouts_out", ctypes.c_size_t), ("next_raw_offset", ctypes.c_uint64)]
+
+
+class State(ctypes.Structure):
+    """cuvhs_state: what a decode carries from chunk to chunk."""
+    _fields_ = [("last_parity", ctypes.c_int32), ("prev_first_field", ctypes.c_int32),
+                ("prev_progressive_field", ctypes.c_int32), ("chroma_valid", ctypes.c_int32),
+                ("prev_first_hsync_readloc", ctypes.c_int64), ("prev_first_hsync_loc", ctypes.c_double),
+                ("prev_first_hsync_diff", ctypes.c_double), ("chroma_threshold", ctypes.c_double),
+                ("chroma_track", ctypes.c_int32), ("chroma_cycle_start", ctypes.c_int32)]
+
+    def as_tuple(self):
+        return tuple(getattr(self, k) for k, _ in self._fields_)
 
 
 class BatchConfig(ctypes.Structure):
@@ -180,6 +192,10 @@ lib.cuvhs_flush.argtypes = [_vp]
 lib.cuvhs_flush.restype = ctypes.c_int
 lib.cuvhs_ire0_hz.argtypes = [_vp]
 lib.cuvhs_ire0_hz.restype = ctypes.c_double
+lib.cuvhs_get_state.argtypes = [_vp, _vp]
+lib.cuvhs_set_state.argtypes = [_vp, _vp]
+lib.cuvhs_pulse_threshold_hz.argtypes = [_vp]
+lib.cuvhs_pulse_threshold_hz.restype = ctypes.c_double
 lib.cuvhs_stage_fm_demod.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.c_int, _vp, _vp, _vp]
 lib.cuvhs_stage_fm_demod.restype = ctypes.c_int
 lib.cuvhs_stage_discover_vsyncs.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_int),
@@ -208,7 +224,8 @@ EXPORTED = [
     "cuvhs_adjoint_destroy", "cuvhs_adjoint_fields", "cuvhs_adjoint_default_params", "cuvhs_adjoint_set_target",
     "cuvhs_adjoint_fwd", "cuvhs_adjoint_bwd", "cuvhs_adjoint_array", "cuvhs_synth_default_params",
     "cuvhs_synth_length", "cuvhs_synth_ntsc", "cuvhs_synth_lines", "cuvhs_synth_preemphasis",
-    "cuvhs_decode_chunk_async", "cuvhs_flush", "cuvhs_ire0_hz", "cuvhs_stage_fm_demod",
+    "cuvhs_decode_chunk_async", "cuvhs_flush", "cuvhs_ire0_hz", "cuvhs_pulse_threshold_hz", "cuvhs_get_state",
+    "cuvhs_set_state", "cuvhs_stage_fm_demod",
     "cuvhs_stage_discover_vsyncs", "cuvhs_stage_sync_pulses", "cuvhs_stage_line_locations",
     "cuvhs_stage_hsync_refine", "cuvhs_stage_tbc_resample", "cuvhs_stage_chroma_decode",
     "cuvhs_field_width", "cuvhs_field_height", "cuvhs_lines_per_frame", "cuvhs_stage_timeline",
@@ -336,9 +353,10 @@ class Decoder:
     SYSTEMS = {"NTSC": 0, "PAL": 1}
 
     def __init__(self, sample_rate_mhz=28.0, device=0, batch_fields=0, stream_mode=False, debug=False,
-                 input_format="u8", dc_correct=False, system="NTSC", single_pass_lines=False):
+                 input_format="u8", dc_correct=False, system="NTSC", single_pass_lines=False, guard_band_hz=0.0):
         cfg = Config()
         lib.cuvhs_default_config(ctypes.byref(cfg))
+        cfg.guard_band_hz = float(guard_band_hz)
         cfg.system = self.SYSTEMS[system.upper()]
         cfg.single_pass_lines = 1 if single_pass_lines else 0
         cfg.sample_rate_mhz = float(sample_rate_mhz)
@@ -395,6 +413,14 @@ class Decoder:
 
     def reset(self):
         lib.cuvhs_reset(self._h)
+
+    def get_state(self) -> "State":
+        st = State()
+        self._check(lib.cuvhs_get_state(self._h, ctypes.byref(st)))
+        return st
+
+    def set_state(self, st: "State"):
+        self._check(lib.cuvhs_set_state(self._h, ctypes.byref(st)))
 
     def _check(self, st):
         if st != 0:
@@ -467,6 +493,7 @@ class Decoder:
         return fo.value, nxt.value
 
     _DTYPES = {"field_offsets": np.int64, "linelocs_coarse": np.float64, "linelocs": np.float64,
+               "guard_positions": np.int64, "guard_values": np.float64,
                "demod": np.float32, "video": np.float32, "sync": np.float32, "envelope": np.float32,
                "chroma_prefilt": np.float32}
 

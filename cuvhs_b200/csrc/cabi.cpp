@@ -142,6 +142,7 @@ void cuvhs_default_config(cuvhs_config* cfg) {
   cfg->input_format = 0;
   cfg->dc_correct = 0;
   cfg->single_pass_lines = 0;
+  cfg->guard_band_hz = 0.0;
 }
 
 const char* cuvhs_status_string(cuvhs_status s) {
@@ -174,6 +175,42 @@ size_t cuvhs_samples_per_field(const cuvhs_ctx* ctx) { return ctx ? (size_t)ctx-
 size_t cuvhs_tile_stride(const cuvhs_ctx* ctx) { return ctx ? (size_t)ctx->c.spp : 0; }
 void cuvhs_reset(cuvhs_ctx* ctx) {
   if (ctx) ctx->c.reset_state();
+}
+
+cuvhs_status cuvhs_get_state(const cuvhs_ctx* ctx, cuvhs_state* s) {
+  if (!ctx || !s) return CUVHS_ERR_INVALID_ARGUMENT;
+  const Context& c = ctx->c;
+  *s = cuvhs_state();
+  s->last_parity = c.last_parity ? 1 : 0;
+  s->prev_first_field = c.lls.prev_first_field;
+  s->prev_progressive_field = c.lls.prev_progressive_field;
+  s->prev_first_hsync_readloc = c.lls.prev_first_hsync_readloc;
+  s->prev_first_hsync_loc = c.lls.prev_first_hsync_loc;
+  s->prev_first_hsync_diff = c.lls.prev_first_hsync_diff;
+  s->chroma_valid = c.chroma_valid ? 1 : 0;
+  s->chroma_track = c.chroma_track;
+  s->chroma_threshold = c.chroma_threshold;
+  s->chroma_cycle_start = c.chroma_cycle_start;
+  return CUVHS_OK;
+}
+
+cuvhs_status cuvhs_set_state(cuvhs_ctx* ctx, const cuvhs_state* s) {
+  if (!ctx || !s) return CUVHS_ERR_INVALID_ARGUMENT;
+  if (s->chroma_track < 0 || s->chroma_track > 1 || s->chroma_cycle_start < 0 || s->chroma_cycle_start > 7 ||
+      s->prev_first_field < -1 || s->prev_first_field > 1)
+    return CUVHS_ERR_INVALID_ARGUMENT;
+  Context& c = ctx->c;
+  c.last_parity = s->last_parity != 0;
+  c.lls.prev_first_field = s->prev_first_field;
+  c.lls.prev_progressive_field = s->prev_progressive_field;
+  c.lls.prev_first_hsync_readloc = s->prev_first_hsync_readloc;
+  c.lls.prev_first_hsync_loc = s->prev_first_hsync_loc;
+  c.lls.prev_first_hsync_diff = s->prev_first_hsync_diff;
+  c.chroma_valid = s->chroma_valid != 0;
+  c.chroma_track = s->chroma_track;
+  c.chroma_threshold = s->chroma_threshold;
+  c.chroma_cycle_start = s->chroma_cycle_start;
+  return CUVHS_OK;
 }
 void cuvhs_set_debug(cuvhs_ctx* ctx, int on) {
   if (ctx) ctx->c.debug = on != 0;
@@ -331,6 +368,8 @@ long long cuvhs_debug_array(const cuvhs_ctx* ctx, const char* name, void* dst, l
   if (s == "do_lines") return copy_ptr(c.hp_do_lines, P * cuvhs::kMaxDropouts, dst, cap);
   if (s == "do_starts") return copy_ptr(c.hp_do_starts, P * cuvhs::kMaxDropouts, dst, cap);
   if (s == "do_ends") return copy_ptr(c.hp_do_ends, P * cuvhs::kMaxDropouts, dst, cap);
+  if (s == "guard_positions") return copy_out(c.dbg_guard_pos, dst, cap);
+  if (s == "guard_values") return copy_out(c.dbg_guard_vals, dst, cap);
   if (s == "linelocs_coarse") return copy_out(c.dbg_ll_coarse, dst, cap);
   if (s == "linelocs") return copy_out(c.dbg_ll, dst, cap);
   if (s == "demod") return copy_out(c.dbg_demod, dst, cap);

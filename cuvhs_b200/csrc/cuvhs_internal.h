@@ -83,6 +83,14 @@ struct Design {
   int c_half = 0, c_out = 0;  // kernel half-width, outputs per half block
   std::vector<float> gc;       // real block spectrum / kNc
   double c_tail = 0;
+  // FP64 taps for re-evaluating sync samples near the pulse threshold (the
+  // guard band): the K1a analytic kernel at offsets [-ga64_half, ga64_half]
+  // (interleaved re, im) and the sync kernel at [-hs64_half, hs64_half], each
+  // wide enough that every dropped tap lies below kGuardTailRel of the largest.
+  static constexpr double kGuardTailRel = 1e-13;
+  static constexpr int kGuardMaxHalf = 4096;
+  int ga64_half = 0, hs64_half = 0;
+  std::vector<double> ga64, hs64;
   // twiddle tables W_N^m
   std::vector<float2> tw_a, tw_b, tw_c, tw_line;
   // chroma per-line constants
@@ -125,7 +133,43 @@ struct DemodArgs {
   int env_blocks;    // blocks per tile of the K1a grid
   float* video;    // [T*spp] video - ire0
   float* sync;     // [T*spp] sync - ire0
+  // Guard band: K1b lists every sync sample it writes within guard_hz of
+  // thr_rel (chunk index into guard_list, its done counter zeroed); the count
+  // may exceed guard_cap, which the host reports.  guard_list == null: off.
+  float thr_rel = 0.0f, guard_hz = 0.0f;
+  unsigned* guard_list = nullptr;
+  int* guard_done = nullptr;
+  int* guard_count = nullptr;
+  int guard_cap = 0;
 };
+
+// FP64 re-evaluation of the listed sync samples (kernels_guard.cu).
+constexpr float kGuardHz = 8.0f;   // half-width of the guard band: >= 4x the largest FP32 sync error measured
+constexpr int kGuardMaxParts = 33;  // CTAs per flagged sample at the largest sync support (2 * 4096 + 1 taps)
+constexpr int kGuardCap = 65536;    // flagged samples one chunk can list
+struct GuardArgs {
+  const uint8_t* raw;
+  int in_fmt, n_read;
+  const float* dc;
+  long long total;  // T * spp: the demodulated chunk extent
+  int spp, tile;
+  const double* ga64;  // K1a taps, offsets [-ha, ha], interleaved re, im
+  int ha;
+  const double* hs64;  // sync taps, offsets [-hb, hb]
+  int hb;
+  double scale;        // fs / 2pi
+  double ire0, thr_hz;  // absolute Hz: the reference's threshold
+  float thr_rel;        // the FP32 threshold the edge kernels compare with
+  float* sync;          // corrected in place
+  const unsigned* list;
+  const int* count;
+  int cap;
+  int* done;
+  double* part;    // [cap * kGuardMaxParts]
+  double* values;  // optional [cap]: the FP64 sync value of each listed sample
+};
+int guard_parts(int hb);
+cudaError_t launch_sync_guard(const GuardArgs& g, cudaStream_t st);
 // K1a over tiles [f0, f0 + nf).
 void launch_k1a(const DemodArgs& a, int f0, int nf, cudaStream_t st);
 // DC correction: *dc = mean of the n converted samples of raw (exact integer

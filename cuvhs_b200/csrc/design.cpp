@@ -128,6 +128,20 @@ int half_support(double fs_hz, double per_mhz, int quantum, int cap) {
   return std::min(n, cap);
 }
 
+// Smallest half-support h (a multiple of quantum, at most cap) of the circular
+// kernel k such that every tap at an offset beyond +/-h lies below rel times
+// the largest tap (real parts only when real_only).
+int tail_half_support(const std::vector<cd>& k, bool real_only, double rel, int quantum, int cap) {
+  const int L = (int)k.size();
+  auto mag = [&](int i) { return real_only ? std::fabs(k[(size_t)i].real()) : std::abs(k[(size_t)i]); };
+  double peak = 0.0;
+  for (int i = 0; i < L; i++) peak = std::max(peak, mag(i));
+  int last = 0;  // largest offset whose tap (either side) is above the bound
+  for (int m = 1; m < L / 2; m++)
+    if (mag(m) > rel * peak || mag(L - m) > rel * peak) last = m;
+  return std::min(cap, (last + quantum) / quantum * quantum);
+}
+
 // Per-pass twiddles of the shared-memory FFT (smem_fft.cuh): pass NS >= 16 of
 // radix R holds W_{NS*R}^{r*k} at (NS - 16) + (r - 1) * NS + k.
 std::vector<float2> twiddles(int n) {
@@ -224,6 +238,14 @@ void Design::build(const Format& fmt) {
     std::vector<cd> g = host_dft(H, +1);  // unnormalised inverse, as the reference's C2C
     a_neg = a_pos = k1a_half_support(fs);
     a_out = kNa - a_neg - a_pos - 1;
+    // FP64 taps for the guard-band re-evaluation of sync samples
+    ga64_half = tail_half_support(g, false, kGuardTailRel, 64, kGuardMaxHalf);
+    ga64.resize((size_t)(2 * ga64_half + 1) * 2);
+    for (int m = -ga64_half; m <= ga64_half; m++) {
+      const cd v = g[(size_t)((m % tile + tile) % tile)];
+      ga64[(size_t)(m + ga64_half) * 2] = v.real();
+      ga64[(size_t)(m + ga64_half) * 2 + 1] = v.imag();
+    }
     std::vector<cd> blk;
     a_tail = place_kernel(g, a_neg, a_pos, kNa, blk);
     std::vector<cd> G = host_dft(blk, -1);
@@ -269,6 +291,9 @@ void Design::build(const Format& fmt) {
     std::vector<cd> hv = host_dft(FV, +1), hs = host_dft(FS, +1);
     std::vector<cd> c(tile);
     for (int n = 0; n < tile; n++) c[n] = cd(hv[n].real(), hs[n].real());
+    hs64_half = tail_half_support(hs, true, kGuardTailRel, 64, kGuardMaxHalf);
+    hs64.resize((size_t)(2 * hs64_half + 1));
+    for (int m = -hs64_half; m <= hs64_half; m++) hs64[(size_t)(m + hs64_half)] = hs[(size_t)((m % tile + tile) % tile)].real();
     b_neg = b_pos = half_support(fs, 25.6, 64, 2048);
     b_out = kNb - b_neg - b_pos;
     std::vector<cd> blk;

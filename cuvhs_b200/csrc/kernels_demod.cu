@@ -177,17 +177,28 @@ __global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(DemodArgs a, int f_be
 }
 
 // K1b output stage: video (real part) and sync (imaginary part) of one block.
+// Sync samples within guard_hz of the pulse threshold are listed for the FP64
+// re-evaluation (kernels_guard.cu); a handful per field.
 template <int T>
 __device__ __forceinline__ void k1b_emit(const DemodArgs& a, const float2 (&z)[16], int f, int j0, int t) {
   const int nout = min(a.b_out, kOverlap + a.spp - j0);
-  float* video_out = a.video + (f * a.spp + (j0 - kOverlap));
-  float* sync_out = a.sync + (f * a.spp + (j0 - kOverlap));
+  const int out0 = f * a.spp + (j0 - kOverlap);
+  float* video_out = a.video + out0;
+  float* sync_out = a.sync + out0;
 #pragma unroll
   for (int q = 0; q < 16; q++) {
     const int i = t + T * q - a.b_pos;
     if (i >= 0 && i < nout) {
       video_out[i] = z[q].x + a.corr_video;
-      sync_out[i] = z[q].y + a.corr_sync;
+      const float sv = z[q].y + a.corr_sync;
+      sync_out[i] = sv;
+      if (fabsf(sv - a.thr_rel) < a.guard_hz && a.guard_list) {
+        const int slot = atomicAdd(a.guard_count, 1);
+        if (slot < a.guard_cap) {
+          a.guard_list[slot] = (unsigned)(out0 + i);
+          a.guard_done[slot] = 0;
+        }
+      }
     }
   }
 }

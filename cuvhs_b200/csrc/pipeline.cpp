@@ -63,6 +63,7 @@ int phase_id_for(int is_first, int quadrant) {
 const char* const kStageNames[kNumStages] = {"k1a_demod",      "k1b_video_sync", "sync_edges",
                                              "hsync_refine",   "luma_resample",  "chroma_prefilter",
                                              "chroma_lines",   "burst_metric",   "dropouts",
+                                             "sync_guard",
                                              "host_edges_wait", "host_runs",      "host_prepare",
                                              "host_lines",     "host_chroma_wait", "host_final_wait"};
 
@@ -161,6 +162,11 @@ bool Context::init(const cuvhs_config& c) {
   }
   if (c.system != kNtsc && c.system != kPal) {
     err = "system must be 0 (NTSC) or 1 (PAL)";
+    status = CUVHS_ERR_INVALID_ARGUMENT;
+    return false;
+  }
+  if (!(c.guard_band_hz >= 0.0 && c.guard_band_hz <= 1.0e6)) {
+    err = "guard_band_hz must be in [0, 1e6]";
     status = CUVHS_ERR_INVALID_ARGUMENT;
     return false;
   }
@@ -279,6 +285,17 @@ bool Context::init(const cuvhs_config& c) {
   d_twb_inv = A((float2*)nullptr, des.tw_b.size());
   d_twc_inv = A((float2*)nullptr, des.tw_c.size());
   d_twl_inv = A((float2*)nullptr, des.tw_line.size());
+  d_ga64 = A((double*)nullptr, des.ga64.size());
+  d_hs64 = A((double*)nullptr, des.hs64.size());
+  d_guard_list = A((unsigned*)nullptr, kGuardCap);
+  d_guard_done = A((int*)nullptr, kGuardCap);
+  d_guard_count = A((int*)nullptr, 1);
+  d_guard_part = A((double*)nullptr, (size_t)kGuardCap * kGuardMaxParts);
+  d_guard_vals = A((double*)nullptr, kGuardCap);
+  if (ok && guard_parts(des.hs64_half) > kGuardMaxParts) {
+    err = "sync guard support too long";
+    ok = false;
+  }
   if (!ok) {
     status = CUVHS_ERR_OUT_OF_MEMORY;
     release();
@@ -300,6 +317,7 @@ bool Context::init(const cuvhs_config& c) {
   };
   const size_t guess = (size_t)std::min(edge_cap, batch * kEdgeGuessPerField);
   hp_counts = H((int*)nullptr, 4);
+  hp_guard = H((int*)nullptr, 1);
   hp_fall = H((unsigned*)nullptr, guess);
   hp_rise = H((unsigned*)nullptr, guess);
   hp_ll = H((double*)nullptr, (size_t)batch * fmt.lines_per_frame);
@@ -352,6 +370,9 @@ bool Context::init(const cuvhs_config& c) {
   upload(d_twb_inv, des.tw_b, stream);
   upload(d_twc_inv, des.tw_c, stream);
   upload(d_twl_inv, des.tw_line, stream);
+  upload(d_ga64, des.ga64, stream);
+  upload(d_hs64, des.hs64, stream);
+  cudaMemsetAsync(d_guard_count, 0, sizeof(int), stream);
   std::vector<double> col_frac(fmt.output_line_len);
   for (int c = 0; c < fmt.output_line_len; c++) col_frac[c] = (double)c / (double)fmt.output_line_len;
   d_col_frac = A((double*)nullptr, col_frac.size());
@@ -496,7 +517,40 @@ DemodArgs Context::demod_args(int T) const {
   da.env_blocks = env_blocks;
   da.video = d_video;
   da.sync = d_sync;
+  da.thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
+  da.guard_hz = cfg.guard_band_hz > 0.0 ? (float)cfg.guard_band_hz : kGuardHz;
+  da.guard_list = d_guard_list;
+  da.guard_done = d_guard_done;
+  da.guard_count = d_guard_count;
+  da.guard_cap = kGuardCap;
   return da;
+}
+
+GuardArgs Context::guard_args(const DemodArgs& da) const {
+  GuardArgs g;
+  g.raw = da.raw;
+  g.in_fmt = da.in_fmt;
+  g.n_read = da.n_read;
+  g.dc = da.dc;
+  g.total = da.total;
+  g.spp = spp;
+  g.tile = des.tile;
+  g.ga64 = d_ga64;
+  g.ha = des.ga64_half;
+  g.hs64 = d_hs64;
+  g.hb = des.hs64_half;
+  g.scale = fmt.fs_hz / (2.0 * 3.14159265358979323846);
+  g.ire0 = fmt.ire0;
+  g.thr_hz = fmt.pulse_threshold_hz;
+  g.thr_rel = da.thr_rel;
+  g.sync = da.sync;
+  g.list = d_guard_list;
+  g.count = d_guard_count;
+  g.cap = kGuardCap;
+  g.done = d_guard_done;
+  g.part = d_guard_part;
+  g.values = d_guard_vals;
+  return g;
 }
 
 ChromaArgs Context::chroma_args(const uint8_t* raw, int n_read, const float* dc, int T) const {
@@ -604,6 +658,14 @@ bool Context::read_edges(const float* sync, long long total) {
   if (nfall) cudaMemcpyAsync(h_fall.data(), d_fall, (size_t)nfall * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
   if (nrise) cudaMemcpyAsync(h_rise.data(), d_rise, (size_t)nrise * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
   return this->sync("sync edge lists");
+}
+
+bool Context::guard_ok(int listed) {
+  if (listed <= kGuardCap) return true;
+  err = "more than " + std::to_string(kGuardCap) + " sync samples near the pulse threshold in one chunk (" +
+        std::to_string(listed) + "); decode shorter chunks";
+  status = CUVHS_ERR_CAPACITY;
+  return false;
 }
 
 // Sync threshold runs [start, end) from the falling and rising edge lists
@@ -844,6 +906,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   cur_n_read = (int)n_read;
   // ---- K1: FM demod over T tiles
   DemodArgs da = demod_args(T);
+  cudaMemsetAsync(d_guard_count, 0, sizeof(int), stream);  // K1b lists near-threshold sync samples
   // ---- input: the chunk window (bps bytes per sample); positions past the
   // samples read count as 0 in every kernel, the reference's zero fill.  Host
   // input arrives in pieces on the copy stream; K1a of tiles [fa, fb) reads
@@ -908,6 +971,13 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
       }
     }
   }
+  {
+    // FP64 threshold decisions for the listed sync samples
+    cudaEvent_t ev_;
+    begin_stage(kStageGuard, ev_);
+    launch_sync_guard(guard_args(da), stream);
+    end_stage(kStageGuard, ev_);
+  }
   if (!check_cuda("demod")) return false;
   // ---- sync edges over the demodulated range.  One copy brings back the
   // counts and a speculative prefix of both edge lists; a second copy is
@@ -927,6 +997,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   cudaEventRecord(ev_edges, stream);
   cudaStreamWaitEvent(xstream, ev_edges, 0);
   cudaMemcpyAsync(hp_counts, d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, xstream);
+  cudaMemcpyAsync(hp_guard, d_guard_count, sizeof(int), cudaMemcpyDeviceToHost, xstream);
   cudaMemcpyAsync(hp_fall, d_fall, (size_t)guess * sizeof(unsigned), cudaMemcpyDeviceToHost, xstream);
   cudaMemcpyAsync(hp_rise, d_rise, (size_t)guess * sizeof(unsigned), cudaMemcpyDeviceToHost, xstream);
   cudaEventRecord(ev_host, xstream);
@@ -958,6 +1029,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     status = CUVHS_ERR_CAPACITY;
     return false;
   }
+  if (!guard_ok(*hp_guard)) return false;
   h_fall.assign(hp_fall, hp_fall + std::min(nfall, guess));
   h_rise.assign(hp_rise, hp_rise + std::min(nrise, guess));
   if (nfall > guess || nrise > guess) {
@@ -1048,6 +1120,14 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     }
   }
   if (debug) {
+    const int ng = std::min(*hp_guard, kGuardCap);
+    std::vector<unsigned> pos(ng);
+    dbg_guard_vals.resize(ng);
+    if (ng) {
+      cudaMemcpy(pos.data(), d_guard_list, ng * sizeof(unsigned), cudaMemcpyDeviceToHost);
+      cudaMemcpy(dbg_guard_vals.data(), d_guard_vals, ng * sizeof(double), cudaMemcpyDeviceToHost);
+    }
+    dbg_guard_pos.assign(pos.begin(), pos.end());
     dbg_vsync = win.cand;
     dbg_offs.assign(offs.begin(), offs.end());
     dbg_ll_coarse.assign(hp_ll, hp_ll + (size_t)P * LPF);

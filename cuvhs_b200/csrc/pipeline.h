@@ -30,6 +30,7 @@ enum Stage {
   kStageChromaLines,
   kStageBurstMetric,
   kStageDropouts,
+  kStageGuard,  // FP64 re-evaluation of near-threshold sync samples
   // host phases (wall time on the calling thread)
   kHostEdgesWait,
   kHostRuns,      // edge lists -> pulse runs, VSYNC candidates, field windows
@@ -124,6 +125,15 @@ struct Context {
   int *d_do_count = nullptr, *d_do_lines = nullptr, *d_do_starts = nullptr, *d_do_ends = nullptr;
   unsigned char* d_do_cls = nullptr;
   double* d_col_frac = nullptr;
+  // guard band of the sync threshold (kernels_guard.cu)
+  double *d_ga64 = nullptr, *d_hs64 = nullptr;
+  unsigned* d_guard_list = nullptr;
+  int *d_guard_done = nullptr, *d_guard_count = nullptr;
+  double *d_guard_part = nullptr, *d_guard_vals = nullptr;
+  int* hp_guard = nullptr;  // pinned: the chunk's listed count
+  // Guard launch over the current chunk's sync (T tiles), after the last K1b;
+  // every later threshold decision reads the corrected samples.
+  GuardArgs guard_args(const DemodArgs& da) const;
   float2 *d_ga = nullptr, *d_gb = nullptr, *d_twa = nullptr, *d_twb = nullptr, *d_twc = nullptr, *d_twl = nullptr;
   float2 *d_twa_inv = nullptr, *d_twb_inv = nullptr, *d_twc_inv = nullptr, *d_twl_inv = nullptr;
   float* d_gc = nullptr;
@@ -158,7 +168,8 @@ struct Context {
   int debug_tiles = 2;
   std::vector<int> dbg_meta, dbg_vsync, dbg_k2c, dbg_k2s, dbg_k2l, dbg_k2bc, dbg_k2bs, dbg_k2bl, dbg_k2bt, dbg_is_first;
   std::vector<long long> dbg_offs;
-  std::vector<double> dbg_ll_coarse, dbg_ll;
+  std::vector<double> dbg_ll_coarse, dbg_ll, dbg_guard_vals;
+  std::vector<long long> dbg_guard_pos;
   std::vector<float> dbg_demod, dbg_video, dbg_sync, dbg_env, dbg_pre;
 
   // per-stage device time (CUDA events on the decode stream) and launch count
@@ -223,6 +234,9 @@ struct Context {
   bool chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal = nullptr, uint16_t* dst_chroma = nullptr);
   // Sync edges of `sync` over [0, total) into h_fall / h_rise (synchronous).
   bool read_edges(const float* sync, long long total);
+  // False (with the error set) when a chunk listed more near-threshold sync
+  // samples than the guard's capacity.
+  bool guard_ok(int listed);
 };
 
 // .tbc.json text (reference format, src/io/tbc_writer.cpp:89-175).

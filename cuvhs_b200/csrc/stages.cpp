@@ -40,6 +40,7 @@ bool enter(Context& c, int n, const char* what) {
 extern "C" {
 
 double cuvhs_ire0_hz(const cuvhs_ctx* ctx) { return ctx ? ctx->c.fmt.ire0 : 0.0; }
+double cuvhs_pulse_threshold_hz(const cuvhs_ctx* ctx) { return ctx ? ctx->c.fmt.pulse_threshold_hz : 0.0; }
 
 // fm_demod (src/pipeline/fm_demod.cu:396-485): K1a and K1b over `tiles` slots.
 cuvhs_status cuvhs_stage_fm_demod(cuvhs_ctx* ctx, const void* d_raw, size_t n_read, int tiles, float* d_video,
@@ -61,10 +62,16 @@ cuvhs_status cuvhs_stage_fm_demod(cuvhs_ctx* ctx, const void* d_raw, size_t n_re
   if (c.dc_correct) cuvhs::launch_dc_mean(da.raw, (int)n_read, c.in_fmt, c.d_dcsum, c.d_dc, c.stream);
   cuvhs::launch_k1a(da, 0, tiles, c.stream);
   c.end_stage(cuvhs::kStageK1a, ev, c.dc_correct ? 3 : 1);
+  cudaMemsetAsync(c.d_guard_count, 0, sizeof(int), c.stream);
   c.begin_stage(cuvhs::kStageK1b, ev);
   cuvhs::launch_k1b(da, 0, tiles, c.stream);
   c.end_stage(cuvhs::kStageK1b, ev);
+  c.begin_stage(cuvhs::kStageGuard, ev);
+  cuvhs::launch_sync_guard(c.guard_args(da), c.stream);
+  c.end_stage(cuvhs::kStageGuard, ev);
+  cudaMemcpyAsync(c.hp_guard, c.d_guard_count, sizeof(int), cudaMemcpyDeviceToHost, c.stream);
   if (!c.check_cuda("fm_demod") || !c.sync("fm_demod")) return c.status;
+  if (!c.guard_ok(*c.hp_guard)) return c.status;
   return CUVHS_OK;
 }
 

@@ -72,6 +72,10 @@ typedef struct cuvhs_config {
   int single_pass_lines;  /* 1: the reference's single-pass line locator (src/pipeline/line_locs.cu) in
                              place of its validated host line location, as the reference runs with the
                              CUVHS_K2B_DISABLE environment variable set (which does the same here) */
+  double guard_band_hz;   /* half-width of the band around the sync pulse threshold inside which sync
+                             samples are re-evaluated in FP64 before any threshold decision; 0 = the
+                             default (8 Hz, several times the FP32 sync error).  Wider bands cost time
+                             and change nothing else; they exist to check the FP64 path */
 } cuvhs_config;
 
 /* Per-field metadata, one .tbc.json "fields" entry. */
@@ -116,6 +120,30 @@ size_t cuvhs_samples_per_field(const cuvhs_ctx* ctx); /* samples_per_line * 263 
 size_t cuvhs_tile_stride(const cuvhs_ctx* ctx);       /* samples per chunk field slot (+20 lines) */
 /* Forget carried state (field parity, line-location and chroma track state). */
 void cuvhs_reset(cuvhs_ctx* ctx);
+
+/* The state a decode carries from one chunk to the next: the parity of the
+ * last field written (the reference's static last_parity,
+ * src/pipeline/pipeline.cu:2575), the line-location history (Pipeline's
+ * k2b_prev_* members, src/pipeline/pipeline.h:92-97; prev_first_hsync_loc is
+ * relative to the chunk it was found in, as the reference keeps it) and the
+ * chroma track and phase cycle (ChromaState, src/pipeline/chroma_decode.h:9-15).
+ * Reading it after a chunk and writing it into another context before the
+ * next chunk continues the decode there exactly: a capture split into
+ * segments decodes as one. */
+typedef struct cuvhs_state {
+  int32_t last_parity;
+  int32_t prev_first_field;
+  int32_t prev_progressive_field;
+  int32_t chroma_valid;
+  int64_t prev_first_hsync_readloc;
+  double prev_first_hsync_loc;
+  double prev_first_hsync_diff;
+  double chroma_threshold;
+  int32_t chroma_track;
+  int32_t chroma_cycle_start;
+} cuvhs_state;
+cuvhs_status cuvhs_get_state(const cuvhs_ctx* ctx, cuvhs_state* state);
+cuvhs_status cuvhs_set_state(cuvhs_ctx* ctx, const cuvhs_state* state);
 
 /* One chunk of at most batch_fields fields starting at capture sample raw_offset.
  * `samples` points at that sample in host memory, n_avail samples remain from
@@ -220,6 +248,10 @@ long long cuvhs_debug_array(const cuvhs_ctx* ctx, const char* name, void* dst, l
 #define CUVHS_MAX_PULSES_PER_FIELD 800
 #define CUVHS_LINES_PER_FRAME 525 /* NTSC; cuvhs_lines_per_frame gives the context's */
 double cuvhs_ire0_hz(const cuvhs_ctx* ctx);
+/* The sync pulse threshold in Hz (0 IRE minus 20 IRE, VideoFormat's
+ * pulse_threshold_hz, src/format/video_format.cpp:23-104): sync samples at or
+ * below it are inside a pulse. */
+double cuvhs_pulse_threshold_hz(const cuvhs_ctx* ctx);
 
 /* fm_demod (src/pipeline/fm_demod.h:46-53): d_raw holds n_read samples of the
  * configured input format (positions past n_read count as 0, the reference's

@@ -56,7 +56,7 @@ def compare_to_oracle(name, r, dbg, x, mhz, o, chunk_last_only=False):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["small28", "dropouts28", "plain40_28", "small358", "small28pal",
                                   "dropouts28pal", "pal20_40", "small28_singlepass", "dropouts28_singlepass",
-                                  "small28pal_singlepass"])
+                                  "small28pal_singlepass", "tipthr28", "hard600_40"])
 def test_decoder_matches_oracle(name):
     x, mhz, r, dbg = decode(name)
     o = oracle_decode(name)
@@ -282,6 +282,50 @@ def test_cli_end_to_end(tmp_path):
         assert (tmp_path / f"out_{fmt}.tbc.json").read_text() == g["json_text"]
         assert (tmp_path / f"out_{fmt}.tbc").read_bytes() == (tmp_path / "out.tbc").read_bytes()
         assert (tmp_path / f"out_{fmt}_chroma.tbc").read_bytes() == (tmp_path / "out_chroma.tbc").read_bytes()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("how", ["stdin", "fifo"])
+def test_cli_stream_mode_matches_file_mode(tmp_path, how):
+    """Stream mode (src/io/raw_reader.cpp:35-54,175-198): a capture piped in
+    through stdin ("-") or a FIFO is read forward in 64-field chunks (the
+    reference's stream cap); the files must equal file mode with --batch 64."""
+    import os
+    import subprocess
+    import threading
+    name = "plain40_28"
+    x = workload(name)
+    inp = tmp_path / "cap.u8"
+    x.tofile(inp)
+    ref = subprocess.run([cv.CLI_PATH, "-f", "28", "--overwrite", "--batch", "64", str(inp), str(tmp_path / "file")],
+                         capture_output=True, text=True, timeout=300)
+    assert ref.returncode == 0, ref.stderr
+    base = tmp_path / "piped"
+    if how == "stdin":
+        with open(inp, "rb") as f:
+            p = subprocess.run([cv.CLI_PATH, "-f", "28", "--overwrite", "-", str(base)], stdin=f,
+                               capture_output=True, text=True, timeout=300)
+    else:
+        fifo = tmp_path / "cap.fifo"
+        os.mkfifo(fifo)
+
+        def feed():  # small writes, so the reader sees short reads
+            with open(fifo, "wb") as w:
+                data = x.tobytes()
+                for i in range(0, len(data), 1 << 20):
+                    w.write(data[i:i + (1 << 20)])
+        t = threading.Thread(target=feed)
+        t.start()
+        p = subprocess.run([cv.CLI_PATH, "-f", "28", "--overwrite", "--format", "u8", str(fifo), str(base)],
+                           capture_output=True, text=True, timeout=300)
+        t.join(60)
+    assert p.returncode == 0, p.stderr
+    assert "Done." in p.stderr
+    for suffix in (".tbc", "_chroma.tbc", ".tbc.json"):
+        a = (tmp_path / f"file{suffix}").read_bytes()
+        b = (tmp_path / f"piped{suffix}").read_bytes()
+        assert a == b, suffix
+    assert len((tmp_path / "piped.tbc").read_bytes()) > 0
 
 
 @pytest.mark.gpu

@@ -63,6 +63,8 @@ def stage_bytes_per_field(stage, fs_hz):
         "burst_metric": 0.0,
         "dropouts": 4 * N,
         "sync_guard": 0.0,                 # FP64 re-evaluation of a few near-threshold sync samples
+        "field_windows": 0.0,              # edge lists -> field windows (a few KB)
+        "line_locations": 0.0,             # pulses -> line starts (a few KB per field)
     }[stage]
 
 

@@ -23,7 +23,7 @@
 #include "pipeline.h"
 
 namespace cuvhs {
-cuvhs_status create_context(const cuvhs_config& cfg, int pool_threads, cuvhs_ctx** out);
+cuvhs_status create_context(const cuvhs_config& cfg, cuvhs_ctx** out);
 }  // namespace cuvhs
 
 namespace {
@@ -145,7 +145,7 @@ cuvhs_status cuvhs_adjoint_create(const cuvhs_config* cfg, const uint8_t* sample
   if (!a) return CUVHS_ERR_OUT_OF_MEMORY;
   cuvhs_config cc = *cfg;
   cc.batch_fields = fields;
-  cuvhs_status s = cuvhs::create_context(cc, -1, &a->ctx);
+  cuvhs_status s = cuvhs::create_context(cc, &a->ctx);
   if (s != CUVHS_OK) {
     delete a;
     return s;

@@ -30,7 +30,6 @@ struct cuvhs_batch {
   cuvhs_batch_config cfg{};
   int device = 0;
   int lanes = 1;
-  int pool_threads = 0;
   // lane -> (rate -> context)
   std::vector<std::map<double, cuvhs_ctx*>> ctx;
   std::mutex mu;
@@ -42,9 +41,8 @@ struct cuvhs_batch {
 };
 
 namespace cuvhs {
-// Creates a context whose host line-location pool has `pool_threads` helpers
-// (cabi.cpp).
-cuvhs_status create_context(const cuvhs_config& cfg, int pool_threads, cuvhs_ctx** out);
+// Creates a decoder context (cabi.cpp).
+cuvhs_status create_context(const cuvhs_config& cfg, cuvhs_ctx** out);
 }  // namespace cuvhs
 
 extern "C" {
@@ -81,7 +79,6 @@ cuvhs_status cuvhs_batch_create(const cuvhs_batch_config* cfg, cuvhs_batch** out
   b->device = dev;
   const int hw = std::max(1, (int)std::thread::hardware_concurrency());
   b->lanes = cfg->lanes > 0 ? cfg->lanes : std::max(1, std::min(4, hw / 2));
-  b->pool_threads = std::max(0, std::min(15, hw / b->lanes - 1));
   b->ctx.resize(b->lanes);
   *out = b;
   return CUVHS_OK;
@@ -135,7 +132,7 @@ cuvhs_status cuvhs_batch_decode(cuvhs_batch* b, cuvhs_batch_item* items, int n_i
         cc.sample_rate_mhz = it.sample_rate_mhz;
         cc.device = b->device;
         cc.batch_fields = b->cfg.max_fields;
-        cuvhs_status s = cuvhs::create_context(cc, b->pool_threads, &ctx);
+        cuvhs_status s = cuvhs::create_context(cc, &ctx);
         if (s != CUVHS_OK) {
           ctx = nullptr;
           it.status = s;

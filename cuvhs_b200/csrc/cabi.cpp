@@ -113,11 +113,10 @@ long long copy_ptr(const T* p, size_t n, void* dst, long long cap) {
 
 namespace cuvhs {
 
-cuvhs_status create_context(const cuvhs_config& cfg, int pool_threads, cuvhs_ctx** out) {
+cuvhs_status create_context(const cuvhs_config& cfg, cuvhs_ctx** out) {
   *out = nullptr;
   cuvhs_ctx* h = new (std::nothrow) cuvhs_ctx();
   if (!h) return CUVHS_ERR_OUT_OF_MEMORY;
-  h->c.pool_threads = pool_threads;
   if (!h->c.init(cfg)) {
     cuvhs_status s = h->c.status != CUVHS_OK ? h->c.status : CUVHS_ERR_CUDA;
     fprintf(stderr, "cuvhs_create: %s\n", h->c.err.c_str());
@@ -161,7 +160,7 @@ const char* cuvhs_status_string(cuvhs_status s) {
 
 cuvhs_status cuvhs_create(const cuvhs_config* cfg, cuvhs_ctx** out) {
   if (!cfg || !out) return CUVHS_ERR_INVALID_ARGUMENT;
-  return cuvhs::create_context(*cfg, -1, out);
+  return cuvhs::create_context(*cfg, out);
 }
 
 void cuvhs_destroy(cuvhs_ctx* ctx) { delete ctx; }
@@ -179,14 +178,17 @@ void cuvhs_reset(cuvhs_ctx* ctx) {
 
 cuvhs_status cuvhs_get_state(const cuvhs_ctx* ctx, cuvhs_state* s) {
   if (!ctx || !s) return CUVHS_ERR_INVALID_ARGUMENT;
-  const Context& c = ctx->c;
+  Context& c = const_cast<cuvhs_ctx*>(ctx)->c;  // reading the device state changes nothing
+  cudaSetDevice(c.device);
+  cuvhs::LineLocState lls;
+  if (!c.read_lls(lls)) return c.status;
   *s = cuvhs_state();
   s->last_parity = c.last_parity ? 1 : 0;
-  s->prev_first_field = c.lls.prev_first_field;
-  s->prev_progressive_field = c.lls.prev_progressive_field;
-  s->prev_first_hsync_readloc = c.lls.prev_first_hsync_readloc;
-  s->prev_first_hsync_loc = c.lls.prev_first_hsync_loc;
-  s->prev_first_hsync_diff = c.lls.prev_first_hsync_diff;
+  s->prev_first_field = lls.prev_first_field;
+  s->prev_progressive_field = lls.prev_progressive_field;
+  s->prev_first_hsync_readloc = lls.prev_first_hsync_readloc;
+  s->prev_first_hsync_loc = lls.prev_first_hsync_loc;
+  s->prev_first_hsync_diff = lls.prev_first_hsync_diff;
   s->chroma_valid = c.chroma_valid ? 1 : 0;
   s->chroma_track = c.chroma_track;
   s->chroma_threshold = c.chroma_threshold;
@@ -200,12 +202,15 @@ cuvhs_status cuvhs_set_state(cuvhs_ctx* ctx, const cuvhs_state* s) {
       s->prev_first_field < -1 || s->prev_first_field > 1)
     return CUVHS_ERR_INVALID_ARGUMENT;
   Context& c = ctx->c;
+  cudaSetDevice(c.device);
+  cuvhs::LineLocState lls;
+  lls.prev_first_field = s->prev_first_field;
+  lls.prev_progressive_field = s->prev_progressive_field;
+  lls.prev_first_hsync_readloc = s->prev_first_hsync_readloc;
+  lls.prev_first_hsync_loc = s->prev_first_hsync_loc;
+  lls.prev_first_hsync_diff = s->prev_first_hsync_diff;
+  if (!c.write_lls(lls)) return c.status;
   c.last_parity = s->last_parity != 0;
-  c.lls.prev_first_field = s->prev_first_field;
-  c.lls.prev_progressive_field = s->prev_progressive_field;
-  c.lls.prev_first_hsync_readloc = s->prev_first_hsync_readloc;
-  c.lls.prev_first_hsync_loc = s->prev_first_hsync_loc;
-  c.lls.prev_first_hsync_diff = s->prev_first_hsync_diff;
   c.chroma_valid = s->chroma_valid != 0;
   c.chroma_track = s->chroma_track;
   c.chroma_threshold = s->chroma_threshold;

@@ -268,7 +268,7 @@ void launch_dropouts_two_pass(const DropoutArgs& a, cudaStream_t st);
 // Chroma concealment of fields [f0, f0 + nf) (their chroma lines final).
 void launch_dropout_conceal_chroma(const DropoutArgs& a, int f0, int nf, cudaStream_t st);
 
-// ---------------------------------------------------------------- host line locations
+// ---------------------------------------------------------------- line locations
 // Per-field pulse validation, mean line length, vertical-blanking anchor and
 // line-location snapping (reference: src/pipeline/pipeline.cu:410-893), with
 // the state carried from field to field (pipeline.h:92-97).
@@ -278,14 +278,6 @@ struct LineLocState {
   long long prev_first_hsync_readloc = -1;
   double prev_first_hsync_loc = -1.0;
   double prev_first_hsync_diff = -1.0;
-};
-struct SyncPulse {
-  int start, len;
-};
-struct ValidPulse {
-  int type;
-  SyncPulse p;
-  bool good;
 };
 constexpr int kAnchorConfidence = 75;  // pattern vote (percent) that fixes the field order
 // Vertical-blanking pulses of one field and their half-line pattern.
@@ -302,77 +294,63 @@ struct AnchorFit {
   double loc = 0.0;            // first-hsync location
   double hsync_line = 0.0;
 };
-// The part of a field's line location that needs no carried state: pulse
-// validation, the mean line length, the blanking scan and, when the field
-// order follows from the field's own pattern, the anchor and snapped grid.
-// Fields can be prepared in parallel.
-struct LinePrep {
-  std::vector<ValidPulse> v;
+constexpr int kMaxValid = kMaxPulses * 27;  // validated entries of one field: each raw pulse adds
+                                            // itself, or up to 26 entries of a blanking sequence
+
+// The stateless part of one field's line location (kernels_linelocs.cu):
+// mean line length, blanking scan and, when the field's pattern fixes its
+// order, the anchor of the speculative grid.
+struct FieldPrep {
   double mll = 0.0;
+  double raw0 = 0.0;    // first raw pulse start, the fallback grid origin
   int n_raw = 0;
-  double raw0 = 0.0;  // first raw pulse start, the fallback grid origin
+  int spec_first = -1;  // field order of the speculative anchor, -1 if none
   BlankingScan scan;
-  int spec_first = -1;  // field order of the precomputed anchor, -1 if none
   AnchorFit spec;
 };
-struct FieldLines {
-  std::vector<int> starts, lengths, types;  // validated pulses
-  std::vector<double> locs;                 // lines_per_frame line starts
-  int is_first = -1;
+// Field windows of one chunk (written by the field-window kernel).
+struct WindowInfo {
+  int fields = 0;  // windows (fields) in the chunk
+  int ncand = 0;   // VSYNC candidates
+  int err = 0;     // 1: an edge list overflowed
+  int pad = 0;
+  long long next_rel = 0;  // start of the next chunk, relative to this one
 };
-// spec_locs (lines_per_frame, may be null) receives the precomputed grid.
-void prepare_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count, LinePrep& out,
-                   double* spec_locs);
-// The stateful part, in field order: field order, vertical-blanking anchor,
-// line snapping, carried-state update.  locs (lines_per_frame) must hold what
-// prepare_lines wrote to spec_locs; it receives the field's line starts.
-// pulses (optional) receives the validated pulses.
-void finish_lines(const Format& fmt, const LinePrep& prep, long long field_readloc, LineLocState& st, double* locs,
-                  FieldLines* pulses, int* is_first);
-void locate_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
-                  long long field_readloc, LineLocState& st, FieldLines& out);
-// The reference's single-pass line locator (src/pipeline/line_locs.cu:62-543),
-// used when its host line location is off: lines_per_frame line starts and
-// the field parity (1 first, 0 second, -1 undetermined); no carried state.
-void single_pass_lines(const Format& fmt, const int* pulse_starts, const int* pulse_lengths, int count,
-                       double* locs, int* parity);
-// Its nominal width classes, which stand in the pulse-type list there
-// (line_locs.cu:18-49 with the thresholds of :551-558).
-void nominal_pulse_types(const Format& fmt, const int* pulse_lengths, int count, int* types);
-
-// Fixed pool of host threads for per-field work; run(n, fn) calls fn(i) for
-// i < n across the pool and the caller, and returns when all are done.
-class WorkPool {
- public:
-  explicit WorkPool(int threads);
-  ~WorkPool();
-  template <typename F>
-  void run(int n, F&& fn) {
-    std::function<void(int)> f(std::forward<F>(fn));
-    run_impl(n, f);
-  }
-  int size() const { return (int)threads_.size() + 1; }
-  // Wake the workers ahead of a run that is about to come: each spins (at
-  // most kSpinMs) for it instead of sleeping, so the run starts without the
-  // sleeping threads' wake-up latency.
-  void prime();
-  static constexpr int kSpinMs = 3;
-
- private:
-  void run_impl(int n, std::function<void(int)>& fn);
-  void worker();
-  std::vector<std::thread> threads_;
-  std::mutex mu_;
-  std::condition_variable cv_, done_cv_;
-  std::function<void(int)>* job_ = nullptr;
-  int n_ = 0;
-  std::atomic<int> next_{0};
-  int active_ = 0;
-  unsigned long long generation_ = 0;
-  std::atomic<unsigned long long> published_{0};  // generation_, readable without the lock
-  unsigned long long prime_ = 0;
-  bool stop_ = false;
-  std::atomic<bool> stopping_{false};
+// Arguments of the line-location kernels.
+struct LineLocArgs {
+  Format fmt;
+  const unsigned* fall;  // sorted threshold edges of the chunk
+  const unsigned* rise;
+  const int* counts;     // [0] falling, [1] rising edges
+  int edge_cap;
+  long long total;       // T * spp
+  int tiles, num_fields;
+  int minw, maxw;        // VSYNC run widths (samples)
+  WindowInfo* win;
+  long long* offs;       // [num_fields] window starts, chunk positions
+  int* cand;             // [cand_cap] VSYNC candidates
+  int cand_cap;
+  int *ps, *pl, *pn;     // [num_fields][kMaxPulses] window pulses, [num_fields] counts
+  int *vs, *vl;          // [num_fields][kMaxValid] validated pulses
+  unsigned char* vt;     // type | good << 2
+  double* vd;            // [num_fields][kMaxValid] scratch
+  int* vn;               // [num_fields]
+  FieldPrep* prep;       // [num_fields]
+  LineLocState* state;   // carried from field to field and chunk to chunk
+  double* ll;            // [num_fields][lines_per_frame] line starts
+  int* is_first;         // [num_fields] 1 first, 0 second (single pass: -1 undetermined)
+  long long raw_offset;  // capture position of the chunk
+  int single_pass;
+  int *dbg_vs = nullptr, *dbg_vl = nullptr, *dbg_vt = nullptr, *dbg_vn = nullptr;  // optional: validated pulses
 };
+size_t lineloc_smem_bytes();
+// VSYNC clustering into field windows (one CTA).
+cudaError_t launch_field_windows(const LineLocArgs& a, cudaStream_t st);
+// The pulses of every field window.
+cudaError_t launch_field_pulses(const LineLocArgs& a, cudaStream_t st);
+// Line locations of every field window: the validated host path of the
+// reference (per-field CTAs, then one CTA in field order), or the single-pass
+// locator.
+cudaError_t launch_line_locations(const LineLocArgs& a, cudaStream_t st);
 
 }  // namespace cuvhs

@@ -1,0 +1,1162 @@
+// Field windows and line locations on the GPU: the reference's VSYNC
+// clustering (src/pipeline/pipeline.cu:1567-1651), pulse windows
+// (src/pipeline/sync_pulses.cu:10-58), its validated host line location "K2b"
+// (pipeline.cu:410-893, driven from :1717-1778) and its single-pass line
+// locator (src/pipeline/line_locs.cu:62-543).
+//
+// The reference runs K2b on the host, one field after another, because each
+// field's anchor may use the previous field's.  Most of the work needs no
+// carried state, so here it runs one CTA per field, in parallel:
+//  * pulse validation: the reference walks the raw pulses once, appending
+//    hsync-width pulses and, at an EQ-width pulse after an hsync, the output
+//    of a vertical-blanking recogniser started two pulses back (kept if the
+//    sequence closes).  The walk advances one pulse per step whatever happens,
+//    and a recogniser attempt depends only on the raw pulses, so every
+//    attempt is evaluated in parallel; one thread then resolves, pulse by
+//    pulse, which attempts fire (an O(1) step each), a scan places every
+//    pulse's output, and the "good" cadence flags follow from neighbouring
+//    entries;
+//  * mean line length (longest hsync run), blanking scan (last match per
+//    slot), and -- when the field's own half-line pattern fixes its order --
+//    the anchor fit and the 525-line snap, exactly as the in-order pass would
+//    compute them for any previous field.
+// A single CTA then walks the fields in order with the carried state
+// (pipeline.h:92-97, kept on the device), reusing the speculative grid or
+// fitting and snapping again.  FP64 throughout; sums whose order matters
+// (anchor offsets) are taken in the reference's order by one thread, sums of
+// integers in parallel.  This file is compiled with -fmad=false so that every
+// a * b + c rounds as two operations, as the reference's host code does; the
+// single-pass locator, whose reference is device code, writes its fused
+// multiply-adds out with fma().
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "chain.cuh"
+#include "cuvhs_internal.h"
+
+namespace cuvhs {
+namespace {
+
+constexpr int kLT = 256;           // threads per line-location CTA
+constexpr int kSortMax = 4096;     // validated pulses sorted in shared memory
+
+__device__ __forceinline__ bool within(double v, double lo, double hi) { return v >= lo && v <= hi; }
+
+// ------------------------------------------------------------ field windows
+
+// First index in sorted a[0, n) whose value is > v.
+__device__ __forceinline__ int upper_idx(const unsigned* a, int n, unsigned v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] <= v) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// End of the threshold run that starts at falling edge i: the first rising
+// edge after it, or the range end (pipeline edge_runs).
+__device__ __forceinline__ long long run_end(const LineLocArgs& a, int nrise, unsigned fall) {
+  const int r = upper_idx(a.rise, nrise, fall);
+  return r < nrise ? (long long)a.rise[r] : a.total;
+}
+
+// One CTA: VSYNC candidates (runs of 20-35 us, vsync_discover.cu:58-72) in
+// sample order, clustered into field windows (pipeline.cu:1567-1651).
+__global__ void __launch_bounds__(1024) fieldwin_kernel(LineLocArgs a) {
+  chain_wait();
+  __shared__ int warp_tot[32];
+  __shared__ int base_s;
+  const int nfall = min(a.counts[0], a.edge_cap), nrise = min(a.counts[1], a.edge_cap);
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (t == 0) {
+    base_s = 0;
+    a.win->err = (a.counts[0] > a.edge_cap || a.counts[1] > a.edge_cap) ? 1 : 0;
+  }
+  __syncthreads();
+  // ordered compaction of the candidates, 1024 edges at a time
+  for (int i0 = 0; i0 < nfall; i0 += 1024) {
+    const int i = i0 + t;
+    bool c = false;
+    if (i < nfall) {
+      const long long w = run_end(a, nrise, a.fall[i]) - (long long)a.fall[i];
+      c = w >= a.minw && w <= a.maxw;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, c);
+    if (lane == 0) warp_tot[warp] = __popc(m);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < 32; w++) {
+      if (w < warp) before += warp_tot[w];
+      total += warp_tot[w];
+    }
+    const int k = base_s + before + __popc(m & ((1u << lane) - 1u));
+    if (c && k < a.cand_cap) a.cand[k] = (int)a.fall[i];
+    __syncthreads();
+    if (t == 0) base_s += total;
+    __syncthreads();
+  }
+  if (t != 0) return;
+  const int ncand = min(base_s, a.cand_cap);
+  const long long spf = a.fmt.samples_per_field, spl = a.fmt.samples_per_line;
+  int n = 0;
+  for (int j = 0; j < ncand; j++) {
+    const long long pos = a.cand[j];
+    if (n == 0 || pos - a.offs[n - 1] > spf / 2) {
+      if (n >= a.num_fields) break;  // later windows are cut off anyway
+      a.offs[n++] = pos > 5 * spl ? pos - 5 * spl : 0;
+    }
+  }
+  if (n == 0)
+    for (int i = 0; i < a.tiles && i < a.num_fields; i++) a.offs[n++] = (long long)i * spf;
+  long long actual = spf;
+  if (n >= 2) actual = (a.offs[n - 1] - a.offs[0]) / (n - 1);
+  const long long predicted = a.offs[n - 1] + actual, margin = 10 * spl;
+  a.win->fields = n;
+  a.win->ncand = base_s;
+  a.win->next_rel = predicted > margin ? predicted - margin : predicted;
+}
+
+// Grid (num_fields): the pulses of field f's window (sync_pulses.cu:10-58):
+// threshold runs that start after the window start and end within the
+// spp-sample scan, at most kMaxPulses.
+__global__ void __launch_bounds__(kLT) pulses_kernel(LineLocArgs a) {
+  chain_wait();
+  __shared__ int brk;
+  const int f = blockIdx.x;
+  if (f >= a.win->fields) return;
+  const int nfall = min(a.counts[0], a.edge_cap), nrise = min(a.counts[1], a.edge_cap);
+  const long long off = a.offs[f], lim = off + a.fmt.spp - 1;
+  const int i0 = upper_idx(a.fall, nfall, (unsigned)min(off, (long long)UINT32_MAX));  // first start > off
+  const int i1 = upper_idx(a.fall, nfall, (unsigned)min(lim, (long long)UINT32_MAX));  // first start > lim
+  if (threadIdx.x == 0) brk = i1;
+  __syncthreads();
+  for (int b = i0; b < i1 && b < brk; b += kLT) {
+    const int i = b + threadIdx.x;
+    if (i < i1 && run_end(a, nrise, a.fall[i]) > lim) atomicMin(&brk, i);
+    __syncthreads();
+  }
+  const int n = min(brk - i0, kMaxPulses);
+  int* ps = a.ps + (size_t)f * kMaxPulses;
+  int* pl = a.pl + (size_t)f * kMaxPulses;
+  for (int k = threadIdx.x; k < n; k += kLT) {
+    const unsigned s = a.fall[i0 + k];
+    ps[k] = (int)s;
+    pl[k] = (int)(run_end(a, nrise, s) - (long long)s);
+  }
+  if (threadIdx.x == 0) a.pn[f] = max(n, 0);
+}
+
+// ------------------------------------------------------------ K2b per field
+
+struct Windows {  // adaptive pulse-width classes (pipeline.cu:450-477)
+  double h_lo, h_hi, e_lo, e_hi, v_lo, v_hi;
+};
+
+__device__ bool spacing_ok(int prev_type, int type, int delta, int line_len) {
+  double lo, hi;
+  if (prev_type > 0 && type > 0) {
+    lo = 0.4;
+    hi = 0.6;
+  } else if (prev_type == 0 && type == 0) {
+    lo = 0.9;
+    hi = 1.1;
+  } else {
+    lo = 0.4;
+    hi = 1.1;
+  }
+  const double span = (double)delta / (double)line_len;
+  return span >= lo && span <= hi;
+}
+
+__device__ const double* field_pattern(int system, bool first) {
+  // Spacings (lines) of the last hsync -> first EQ and last EQ -> first hsync
+  // around this field's blanking interval, then around the next one
+  // (pipeline.cu:704-716).
+  static __device__ const double ntsc_first[4] = {1, 0.5, 0.5, 1}, ntsc_second[4] = {0.5, 1, 1, 0.5};
+  static __device__ const double pal_first[4] = {0.5, 0.5, 1, 1}, pal_second[4] = {1, 1, 0.5, 0.5};
+  if (system == kPal) return first ? pal_first : pal_second;
+  return first ? ntsc_first : ntsc_second;
+}
+
+__device__ double predicted_field_lines(const Format& fmt, bool first) {
+  const int cur = first ? fmt.field_lines_first : fmt.field_lines_second;
+  const int prev = first ? fmt.field_lines_second : fmt.field_lines_first;
+  return fmt.system == kPal ? cur : prev;
+}
+
+__device__ double half_line_round(double lines) { return round(0.5 * round(lines / 0.5) * 10.0) / 10.0; }
+
+// The vertical-blanking recogniser (pipeline.cu:519-609) from pulse `first`,
+// over at most 26 pulses, entered with an hsync as the list's last entry.
+// Writes each appended entry's pulse index and type when emit_idx is given;
+// returns whether the sequence closed, with the number appended and the
+// type of the last one.
+__device__ bool attempt(const int* ps, const int* pl, int n, int first, const Windows& w, int eq_pulses, int line_len,
+                        int* appended, int* last_type, int* emit_idx, unsigned char* emit_type) {
+  bool done = false;
+  const double half = eq_pulses / 2.0;
+  bool vsync_seen = false;
+  double hold_until = 0.0, pending = -1.0;
+  int cur = kHsync, cnt = 0;
+  for (int i = first; i < n && i < first + 26; i++) {
+    const double len = (double)pl[i];
+    int type = -1;
+    switch (cur) {
+      case kHsync:
+        if (within(len, w.h_lo, w.h_hi)) {
+          type = kHsync;
+        } else if (within(len, w.e_lo, w.e_hi)) {
+          type = kEq1;
+          pending = half;
+        } else if (within(len, w.v_lo, w.v_hi)) {
+          vsync_seen = true;
+          type = kVsync;
+        }
+        break;
+      case kEq1:
+        if (within(len, w.e_lo, w.e_hi)) {
+          type = kEq1;
+        } else if (within(len, w.v_lo, w.v_hi)) {
+          vsync_seen = true;
+          type = kVsync;
+          pending = half;
+        } else if (within(len, w.h_lo, w.h_hi)) {
+          type = kHsync;
+        }
+        break;
+      case kVsync:
+        if (within(len, w.e_lo, w.e_hi)) {
+          type = kEq2;
+          pending = half;
+        } else if (within(len, w.v_lo, w.v_hi)) {
+          type = kVsync;
+        } else if ((double)ps[i] > hold_until && within(len, w.h_lo, w.h_hi)) {
+          type = kHsync;
+        }
+        break;
+      case kEq2:
+        if (within(len, w.e_lo, w.e_hi)) {
+          type = kEq2;
+        } else if (within(len, w.h_lo, w.h_hi)) {
+          type = kHsync;
+          done = true;
+        }
+        break;
+    }
+    bool keep = type >= 0;
+    if (keep && type != cur) {
+      if ((double)ps[i] < hold_until) {
+        keep = false;
+      } else if (pending > 0.0) {
+        hold_until = (double)ps[i] + ((pending - 0.1) * (double)line_len);
+        pending = -1.0;
+      }
+    }
+    if (keep) {
+      if (emit_idx) {
+        emit_idx[cnt] = i;
+        emit_type[cnt] = (unsigned char)type;
+      }
+      cnt++;
+      cur = type;
+    }
+    if (done && vsync_seen) break;
+  }
+  *appended = cnt;
+  *last_type = cur;
+  return done && cnt > 0;
+}
+
+// Block-wide sum of a long long (kLT threads); every thread gets the total.
+__device__ long long block_sum_ll(long long v, long long* sh) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  long long t = 0;
+  for (int w = 0; w < kLT / 32; w++) t += sh[w];
+  __syncthreads();
+  return t;
+}
+
+// The validated pulses of one field, in global scratch (start, length,
+// type | good << 2).
+struct VList {
+  int* s;
+  int* l;
+  unsigned char* tg;
+  double* d;  // scratch doubles, one per entry
+  int n;
+};
+__device__ __forceinline__ int vtype(const VList& v, int k) { return v.tg[k] & 3; }
+__device__ __forceinline__ bool vgood(const VList& v, int k) { return (v.tg[k] >> 2) & 1; }
+
+// Shared memory of a per-field CTA.
+struct FieldSmem {
+  int ps[kMaxPulses], pl[kMaxPulses];
+  unsigned char cls[kMaxPulses];  // bit 0: hsync width, bit 1: attempt start
+  int att_len[kMaxPulses];
+  unsigned char att_ok[kMaxPulses], att_last[kMaxPulses];
+  int pos[kMaxPulses + 1];
+  long long red[kLT / 32];
+  int imin, imax[12];
+  double dsh[8];
+  int ish[8];
+  double sort[kSortMax];
+};
+
+// Pulse validation (pipeline.cu:611-648) into v; returns the entry count.
+__device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
+  const Format& fmt = a.fmt;
+  const int t = threadIdx.x;
+  // width classes adapted to the field's mean hsync width (pipeline.cu:450-477)
+  const double tol = fmt.fs_hz * 0.5e-6;
+  const double loose_lo = fmt.hsync_width - 3.5 * tol, loose_hi = fmt.hsync_width + 4.0 * tol;
+  long long lsum = 0, lcnt = 0;
+  for (int i = t; i < n; i += kLT) {
+    const double l = (double)sm.pl[i];
+    if (l >= loose_lo && l <= loose_hi) {
+      lsum += sm.pl[i];
+      lcnt++;
+    }
+  }
+  lsum = block_sum_ll(lsum, sm.red);
+  lcnt = block_sum_ll(lcnt, sm.red);
+  const double est = lcnt > 0 ? ((double)lsum / (double)lcnt) : fmt.hsync_width;
+  const double shift = est - fmt.hsync_width;
+  Windows w;
+  const double hnom = fmt.hsync_width + shift;
+  w.h_lo = hnom - tol;
+  w.h_hi = hnom + tol;
+  w.e_lo = fmt.eq_pulse_width + shift - tol;
+  w.e_hi = fmt.eq_pulse_width + shift + tol;
+  w.v_lo = (fmt.vsync_width + shift) * 0.5;
+  w.v_hi = fmt.vsync_width + shift + 2.0 * tol;
+  // classes and every recogniser attempt
+  for (int i = t; i < n; i += kLT) {
+    const double len = (double)sm.pl[i];
+    const bool h = within(len, w.h_lo, w.h_hi);
+    const bool e = !h && i > 2 && within(len, w.e_lo, w.e_hi);
+    sm.cls[i] = (h ? 1 : 0) | (e ? 2 : 0);
+    int cnt = 0, last = kHsync;
+    bool ok = false;
+    if (e) ok = attempt(sm.ps, sm.pl, n, i - 2, w, fmt.num_eq_pulses, fmt.samples_per_line, &cnt, &last, nullptr,
+                        nullptr);
+    sm.att_ok[i] = ok ? 1 : 0;
+    sm.att_len[i] = cnt;
+    sm.att_last[i] = (unsigned char)last;
+  }
+  __syncthreads();
+  // which attempts fire: at an EQ-width pulse while the list's last entry is
+  // an hsync; one O(1) step per pulse
+  if (t == 0) {
+    int total = 0, back = -1;  // -1: empty list
+    for (int i = 0; i < n; i++) {
+      sm.pos[i] = total;
+      if (sm.cls[i] & 1) {
+        total += 1;
+        back = kHsync;
+      } else if ((sm.cls[i] & 2) && back == kHsync && sm.att_ok[i]) {
+        total += sm.att_len[i];
+        back = sm.att_last[i];
+      }
+    }
+    sm.pos[n] = total;
+  }
+  __syncthreads();
+  const int nv = sm.pos[n];
+  // place every pulse's output
+  for (int i = t; i < n; i += kLT) {
+    const int p = sm.pos[i], len = sm.pos[i + 1] - p;
+    if (len <= 0) continue;
+    if (sm.cls[i] & 1) {
+      v.s[p] = sm.ps[i];
+      v.l[p] = sm.pl[i];
+      v.tg[p] = kHsync;
+    } else {
+      int idx[26];
+      unsigned char ty[26];
+      int cnt = 0, last = 0;
+      attempt(sm.ps, sm.pl, n, i - 2, w, fmt.num_eq_pulses, fmt.samples_per_line, &cnt, &last, idx, ty);
+      for (int k = 0; k < cnt; k++) {
+        v.s[p + k] = sm.ps[idx[k]];
+        v.l[p + k] = sm.pl[idx[k]];
+        v.tg[p + k] = ty[k];
+      }
+    }
+  }
+  __syncthreads();
+  // cadence flags from each entry's predecessor (pipeline.cu:133-148)
+  for (int k = t; k < nv; k += kLT) {
+    const bool good = k > 0 && spacing_ok(vtype(v, k - 1), vtype(v, k), v.s[k] - v.s[k - 1], fmt.samples_per_line);
+    v.tg[k] = (unsigned char)(vtype(v, k) | (good ? 4 : 0));
+  }
+  __syncthreads();
+  return nv;
+}
+
+// Mean line length from the longest hsync run (pipeline.cu:479-517): the
+// first longest run; spacings within 5% of nominal, its last one excluded.
+__device__ double mean_line(FieldSmem& sm, const VList& v, double nominal) {
+  const int t = threadIdx.x;
+  // best run as (run_len << 32 | ~start): the largest run_len, then the first
+  unsigned long long best = 0;
+  bool any = false;
+  for (int k = t; k < v.n; k += kLT) {
+    if (vtype(v, k) != kHsync || (k > 0 && vtype(v, k - 1) == kHsync)) continue;
+    int e = k + 1;
+    while (e < v.n && vtype(v, e) == kHsync) e++;
+    const unsigned long long key = ((unsigned long long)(unsigned)(e - k - 1) << 32) | (0xFFFFFFFFu - (unsigned)k);
+    if (!any || key > best) best = key;
+    any = true;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    const unsigned long long o = __shfl_down_sync(0xffffffffu, best, off);
+    best = o > best ? o : best;
+  }
+  __shared__ unsigned long long wbest[kLT / 32];
+  if ((t & 31) == 0) wbest[t >> 5] = best;
+  __syncthreads();
+  unsigned long long b = 0;
+  for (int w = 0; w < kLT / 32; w++) b = wbest[w] > b ? wbest[w] : b;
+  __syncthreads();
+  // a run exists iff the list holds an hsync; key 0 is only possible for a
+  // single-entry run at index 0xFFFFFFFF, so test the list instead
+  bool has_run = false;
+  for (int k = t; k < v.n && !has_run; k += kLT) has_run = vtype(v, k) == kHsync;
+  has_run = __syncthreads_or(has_run);
+  const int best_len = has_run ? (int)(b >> 32) : -1;
+  const int best_start = has_run ? (int)(0xFFFFFFFFu - (unsigned)(b & 0xFFFFFFFFu)) : -1;
+  long long sum = 0, cnt = 0;
+  if (best_start >= 1 && best_len >= 1) {
+    for (int i = best_start + 1 + t; i < best_start + best_len; i += kLT) {
+      const double l = (double)(v.s[i] - v.s[i - 1]);
+      const double r = l / nominal;
+      if (r >= 0.95 && r <= 1.05) {
+        sum += v.s[i] - v.s[i - 1];
+        cnt++;
+      }
+    }
+  }
+  sum = block_sum_ll(sum, sm.red);
+  cnt = block_sum_ll(cnt, sm.red);
+  return cnt == 0 ? nominal : (double)sum / (double)cnt;
+}
+
+// Vertical-blanking pulses and pattern agreement (pipeline.cu:650-716): each
+// slot keeps its last match.
+__device__ BlankingScan scan_blanking(FieldSmem& sm, const VList& v, double mll, const Format& fmt) {
+  const int t = threadIdx.x;
+  BlankingScan s;
+  for (int i = 0; i < 8; i++) s.vb_pulse[i] = -1;
+  for (int i = 0; i < 4; i++) s.order_len[i] = -1;
+  s.agree = s.seen = 0.0;
+  if (v.n == 0 || mll <= 0.0) return s;
+  if (t == 0) sm.imin = INT_MAX;
+  if (t < 12) sm.imax[t] = -1;
+  __syncthreads();
+  const double second = (double)v.s[0] + fmt.field_lines_first * mll;
+  for (int i = 1 + t; i < v.n; i += kLT)
+    if (vgood(v, i) && (double)v.s[i] > second) atomicMin(&sm.imin, i);
+  __syncthreads();
+  const int g0 = sm.imin;
+  for (int i = 1 + t; i < v.n; i += kLT) {
+    if (!vgood(v, i)) continue;
+    const int grp = i >= g0 ? 4 : 0, fgrp = i >= g0 ? 2 : 0;
+    const int pt = vtype(v, i - 1), ty = vtype(v, i);
+    // slots 0..7 vb_pulse, 8..11 order_len
+    if (pt == kHsync && ty > kHsync) {
+      atomicMax(&sm.imax[0 + grp], i);
+      atomicMax(&sm.imax[8 + 0 + fgrp], i);
+    } else if (pt == kEq1 && ty == kVsync) {
+      atomicMax(&sm.imax[1 + grp], i);
+    } else if (pt == kVsync && ty == kEq2) {
+      atomicMax(&sm.imax[2 + grp], i);
+    } else if (pt > kHsync && ty == kHsync) {
+      atomicMax(&sm.imax[3 + grp], i);
+      atomicMax(&sm.imax[8 + 1 + fgrp], i);
+    }
+  }
+  __syncthreads();
+  for (int k = 0; k < 8; k++) {
+    const int i = sm.imax[k];
+    if (i < 0) continue;
+    s.vb_pulse[k] = (k & 3) == 3 ? v.s[i - 1] : v.s[i];
+  }
+  for (int k = 0; k < 4; k++) {
+    const int i = sm.imax[8 + k];
+    if (i >= 0) s.order_len[k] = half_line_round((v.s[i] - v.s[i - 1]) / mll);
+  }
+  const double* first_pat = field_pattern(fmt.system, true);
+  const double* second_pat = field_pattern(fmt.system, false);
+  for (int i = 0; i < 4; i++) {
+    if (s.order_len[i] == first_pat[i]) {
+      s.agree += 1.0;
+      s.seen += 1.0;
+    }
+    if (s.order_len[i] == second_pat[i]) s.seen += 1.0;
+  }
+  __syncthreads();
+  return s;
+}
+
+__device__ bool decide_first(const BlankingScan& s, int prev_first, double prev_loc, int confidence) {
+  bool first;
+  if (prev_first == -1) first = s.seen == 0.0 || round(s.agree / fmax(1.0, s.seen)) == 1.0;
+  else first = !prev_first;
+  if (s.seen > 0.0) {
+    if (prev_loc < 0.0) confidence = min(confidence, 50);
+    const double weight = s.seen / 4.0;
+    const int c_first = (int)llround((s.agree / s.seen) * weight * 100.0);
+    const int c_second = (int)llround(((s.seen - s.agree) / s.seen) * weight * 100.0);
+    if (c_first >= confidence && c_first > c_second) first = true;
+    else if (c_second >= confidence && c_second > c_first) first = false;
+  }
+  return first;
+}
+
+__device__ int pattern_first(const BlankingScan& s, int confidence) {
+  if (s.seen <= 0.0) return -1;
+  const double weight = s.seen / 4.0;
+  const int c_first = (int)llround((s.agree / s.seen) * weight * 100.0);
+  const int c_second = (int)llround(((s.seen - s.agree) / s.seen) * weight * 100.0);
+  if (c_first >= confidence && c_first > c_second) return 1;
+  if (c_second >= confidence && c_second > c_first) return 0;
+  return -1;
+}
+
+// First-hsync anchor for field order `first` (pipeline.cu:650-855).  The
+// scalar estimate runs on thread 0; the hsync-offset correction's terms are
+// formed in parallel and added in list order by thread 0.  Every thread gets
+// the result.
+__device__ AnchorFit fit_anchor(FieldSmem& sm, const BlankingScan& s, const VList& v, double mll, const Format& fmt,
+                                bool first, double prev_off_lines, double prev_loc, double prev_diff) {
+  const int t = threadIdx.x;
+  __shared__ AnchorFit res;
+  __shared__ double loc_s;
+  __shared__ int go_s;
+  const double cur_lines = first ? fmt.field_lines_first : fmt.field_lines_second;
+  if (t == 0) {
+    AnchorFit out;
+    go_s = 0;
+    if (v.n > 0 && mll > 0.0) {
+      const double tol_lines = 0.5;
+      const double section = fmt.num_eq_pulses / 2.0;
+      const double pred_lines = predicted_field_lines(fmt, first);
+      const double* pat = field_pattern(fmt.system, first);
+      double vb_line[8];
+      vb_line[0] = 0.0 + pat[0];
+      vb_line[1] = vb_line[0] + section;
+      vb_line[2] = vb_line[1] + section;
+      vb_line[3] = vb_line[2] + section - 0.5;
+      const double hsync_line = vb_line[3] + pat[1];
+      vb_line[4] = cur_lines + pat[2];
+      vb_line[5] = vb_line[4] + section;
+      vb_line[6] = vb_line[5] + section;
+      vb_line[7] = vb_line[6] + section - 0.5;
+      double a_loc = 0.0, a_off = 0.0, b_loc = 0.0, b_off = 0.0;
+      int a_cnt = 0, b_cnt = 0;
+      auto pair_estimate = [&](int i1, int i2, double& loc, int& cnt, double& off) {
+        const int p1 = s.vb_pulse[i1], p2 = s.vb_pulse[i2];
+        if (p1 == -1 || p2 == -1 || mll == 0.0) return;
+        const double actual = ((double)p1 - (double)p2) / mll;
+        const double expect = vb_line[i1] - vb_line[i2];
+        if (actual < expect + tol_lines && actual > expect - tol_lines) {
+          off += actual - expect;
+          loc += (double)p2 + mll * (hsync_line - vb_line[i2]);
+          cnt += 1;
+        }
+      };
+      for (int x = 0; x < 4; x++)
+        for (int y = x + 1; y < 4; y++) pair_estimate(x, y, a_loc, a_cnt, a_off);
+      for (int x = 0; x < 4; x++)
+        for (int y = x + 1; y < 4; y++) pair_estimate(4 + x, 4 + y, b_loc, b_cnt, b_off);
+      double loc = 0.0, off = 0.0;
+      int cnt = 0;
+      const double a_est = a_cnt ? a_loc / a_cnt : 0.0, b_est = b_cnt ? b_loc / b_cnt : 0.0;
+      if (a_cnt && b_cnt && a_est < b_est + tol_lines * mll && a_est > b_est - tol_lines * mll) {
+        loc = a_loc + b_loc;
+        cnt = a_cnt + b_cnt;
+        off = a_off + b_off;
+        for (int x = 0; x < 4; x++)
+          for (int y = 0; y < 4; y++) pair_estimate(x, 4 + y, loc, cnt, off);
+      } else if (a_cnt == 6 || (prev_loc <= 0.0 && a_cnt > b_cnt)) {
+        loc = a_loc;
+        cnt = a_cnt;
+        off = a_off;
+      } else if (b_cnt == 6 || (prev_loc <= 0.0 && b_cnt > a_cnt)) {
+        loc = b_loc;
+        cnt = b_cnt;
+        off = b_off;
+      }
+      const int predicted = (int)llround((prev_off_lines + pred_lines + prev_loc / mll) * mll);
+      if (cnt == 0 && prev_loc > 0.0) {
+        double p = (prev_diff <= 0.5 && prev_diff >= -0.5) ? predicted + mll * prev_diff : (double)predicted;
+        if (p <= 0.0) p = (double)v.s[0];
+        loc += p;
+        cnt += 1;
+        out.used_prediction = true;
+      }
+      out.cnt = cnt;
+      if (cnt > 0) {
+        off /= cnt;
+        loc = round((loc + off) / cnt);
+        out.loc_round = loc;
+        out.hsync_line = hsync_line;
+        loc_s = loc;
+        go_s = 1;
+      }
+    }
+    res = out;
+    sm.imin = INT_MAX;
+  }
+  __syncthreads();
+  if (!go_s) {
+    const AnchorFit r = res;
+    __syncthreads();
+    return r;
+  }
+  // hsync-offset correction: terms of the hsync entries before the first one
+  // past the field's last line
+  const double loc = loc_s, hsync_line = res.hsync_line;
+  for (int k = t; k < v.n; k += kLT) {
+    double term = __longlong_as_double(0x7ff8000000000000LL);  // NaN: not counted
+    if (vtype(v, k) == kHsync && vgood(v, k)) {
+      const double line = ((double)v.s[k] - loc) / mll + hsync_line;
+      const int rl = (int)llround(line);
+      if (rl > cur_lines) atomicMin(&sm.imin, k);
+      else if (rl >= hsync_line) term = loc + mll * ((double)rl - hsync_line) - (double)v.s[k];
+    }
+    v.d[k] = term;
+  }
+  __syncthreads();
+  if (t == 0) {
+    const int end = min(sm.imin, v.n);
+    double hoff = 0.0;
+    int hcnt = 0;
+    for (int k = 0; k < end; k++) {
+      const double x = v.d[k];
+      if (x == x) {
+        hoff += x;
+        hcnt++;
+      }
+    }
+    double l = loc;
+    if (hcnt > 0) {
+      hoff /= hcnt;
+      l -= hoff;
+    }
+    res.loc = l;
+  }
+  __syncthreads();
+  const AnchorFit r = res;
+  __syncthreads();
+  return r;
+}
+
+// The carried hsync_diff after a fit that used no prediction.
+__device__ double hsync_diff_after(const AnchorFit& f, const Format& fmt, bool first, double mll, double prev_off_lines,
+                                   double prev_loc) {
+  const int predicted = (int)llround((prev_off_lines + predicted_field_lines(fmt, first) + prev_loc / mll) * mll);
+  return (f.loc_round - predicted) / mll;
+}
+
+// Sorted validated starts in sm.sort (bitonic, padded with +inf) or, past
+// kSortMax entries, in v.d (insertion sort by thread 0).  Returns the array.
+__device__ const double* sorted_starts(FieldSmem& sm, const VList& v) {
+  const int t = threadIdx.x;
+  if (v.n <= kSortMax) {
+    int m = 1;
+    while (m < v.n) m <<= 1;
+    for (int k = t; k < m; k += kLT) sm.sort[k] = k < v.n ? (double)v.s[k] : __longlong_as_double(0x7ff0000000000000LL);
+    __syncthreads();
+    for (int size = 2; size <= m; size <<= 1)
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int k = t; k < m; k += kLT) {
+          const int j = k ^ stride;
+          if (j > k) {
+            const bool up = (k & size) == 0;
+            const double x = sm.sort[k], y = sm.sort[j];
+            if ((x > y) == up) {
+              sm.sort[k] = y;
+              sm.sort[j] = x;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    return sm.sort;
+  }
+  if (t == 0) {
+    for (int k = 0; k < v.n; k++) v.d[k] = (double)v.s[k];
+    for (int a = 1; a < v.n; a++) {  // nearly sorted already
+      const double x = v.d[a];
+      int b = a;
+      while (b > 0 && v.d[b - 1] > x) {
+        v.d[b] = v.d[b - 1];
+        b--;
+      }
+      v.d[b] = x;
+    }
+  }
+  __syncthreads();
+  return v.d;
+}
+
+// Nominal line grid snapped to the nearest pulse (pipeline.cu:857-893).
+__device__ void snap_lines(FieldSmem& sm, const VList& v, double ref_pos, double ref_line, double mll, int nlines,
+                           double* locs) {
+  const double* ps = sorted_starts(sm, v);
+  if (threadIdx.x == 0) {
+    const int np = v.n;
+    const double max_dist = mll / 1.5;
+    int cur = 0;
+    for (int line = 0; line < nlines; line++) {
+      const double expect = ref_pos + mll * ((double)line - ref_line);
+      locs[line] = expect;
+      if (cur >= np) continue;
+      double d = fabs(ps[cur] - expect);
+      double best = max_dist, at = -1.0;
+      int s = cur;
+      while (s + 1 < np) {
+        if (d <= best) {
+          best = d;
+          cur = s;
+          at = ps[s];
+        }
+        const double nd = fabs(ps[s + 1] - expect);
+        if (nd > d) break;
+        d = nd;
+        s++;
+      }
+      if (at >= 0.0) {
+        locs[line] = at;
+        cur++;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+__device__ VList field_vlist(const LineLocArgs& a, int f) {
+  VList v;
+  const size_t o = (size_t)f * kMaxValid;
+  v.s = a.vs + o;
+  v.l = a.vl + o;
+  v.tg = a.vt + o;
+  v.d = a.vd + o;
+  v.n = a.vn[f];
+  return v;
+}
+
+// Grid (num_fields): the stateless part of one field's line location, and
+// the speculative anchor + grid when the field's pattern fixes its order.
+__global__ void __launch_bounds__(kLT) prepare_kernel(LineLocArgs a) {
+  chain_wait();
+  extern __shared__ double smem_d[];
+  FieldSmem& sm = *reinterpret_cast<FieldSmem*>(smem_d);
+  const int f = blockIdx.x, t = threadIdx.x;
+  if (f >= a.win->fields) return;
+  const int n = min(max(a.pn[f], 0), kMaxPulses);
+  for (int i = t; i < n; i += kLT) {
+    sm.ps[i] = a.ps[(size_t)f * kMaxPulses + i];
+    sm.pl[i] = a.pl[(size_t)f * kMaxPulses + i];
+  }
+  __syncthreads();
+  VList v = field_vlist(a, f);
+  v.n = n > 0 ? validate(a, sm, n, v) : 0;
+  if (t == 0) a.vn[f] = v.n;
+  const double mll = mean_line(sm, v, (double)a.fmt.samples_per_line);
+  const BlankingScan scan = scan_blanking(sm, v, mll, a.fmt);
+  FieldPrep p;
+  p.mll = mll;
+  p.n_raw = n;
+  p.raw0 = n > 0 ? (double)sm.ps[0] : 0.0;
+  p.scan = scan;
+  p.spec_first = -1;
+  const int pf = v.n > 0 ? pattern_first(scan, kAnchorConfidence) : -1;
+  if (pf >= 0) {
+    const AnchorFit fit = fit_anchor(sm, scan, v, mll, a.fmt, pf == 1, 0.0, 1.0, 0.0);
+    if (fit.cnt > 0 && !fit.used_prediction) {
+      snap_lines(sm, v, fit.loc, fit.hsync_line, mll, a.fmt.lines_per_frame, a.ll + (size_t)f * a.fmt.lines_per_frame);
+      p.spec_first = pf;
+      p.spec = fit;
+    }
+  }
+  if (t == 0) a.prep[f] = p;
+  // validated pulses for inspection (the first kMaxPulses)
+  if (a.dbg_vn) {
+    const int kept = min(v.n, kMaxPulses);
+    for (int k = t; k < kept; k += kLT) {
+      a.dbg_vs[(size_t)f * kMaxPulses + k] = v.s[k];
+      a.dbg_vl[(size_t)f * kMaxPulses + k] = v.l[k];
+      a.dbg_vt[(size_t)f * kMaxPulses + k] = vtype(v, k);
+    }
+    if (t == 0) a.dbg_vn[f] = kept;
+  }
+}
+
+// One CTA: the fields in order with the carried state (pipeline.cu:1717-1778).
+__global__ void __launch_bounds__(kLT) finish_kernel(LineLocArgs a) {
+  chain_wait();
+  extern __shared__ double smem_d[];
+  FieldSmem& sm = *reinterpret_cast<FieldSmem*>(smem_d);
+  __shared__ int need_fit, first_s, valid_s;
+  __shared__ double prev_off_s, prev_loc_s, prev_diff_s;
+  const int t = threadIdx.x;
+  const int P = a.win->fields;
+  const int LPF = a.fmt.lines_per_frame;
+  for (int f = 0; f < P; f++) {
+    const FieldPrep p = a.prep[f];
+    if (t == 0) {
+      const LineLocState st = *a.state;
+      const long long readloc = a.raw_offset + a.offs[f];
+      double prev_off = 0.0;
+      if (st.prev_first_hsync_readloc != -1 && p.mll > 0.0)
+        prev_off = ((double)st.prev_first_hsync_readloc - (double)readloc) / p.mll;
+      const double prev_loc = st.prev_first_hsync_loc;
+      const bool valid = a.vn[f] > 0 && p.mll > 0.0;
+      bool first = false;
+      need_fit = 0;
+      if (valid) {
+        first = decide_first(p.scan, st.prev_first_field, prev_loc, kAnchorConfidence);
+        need_fit = !(p.spec_first == (first ? 1 : 0) && prev_loc > 0.0);
+      }
+      first_s = first;
+      valid_s = valid;
+      prev_off_s = prev_off;
+      prev_loc_s = prev_loc;
+      prev_diff_s = st.prev_first_hsync_diff;
+    }
+    __syncthreads();
+    AnchorFit fit = p.spec;
+    if (valid_s && need_fit) {
+      VList v = field_vlist(a, f);
+      fit = fit_anchor(sm, p.scan, v, p.mll, a.fmt, first_s != 0, prev_off_s, prev_loc_s, prev_diff_s);
+      if (fit.cnt > 0) snap_lines(sm, v, fit.loc, fit.hsync_line, p.mll, LPF, a.ll + (size_t)f * LPF);
+    }
+    const bool valid = valid_s && fit.cnt > 0;
+    double* locs = a.ll + (size_t)f * LPF;
+    if (!valid)
+      for (int line = t; line < LPF; line += kLT) locs[line] = p.raw0 + p.mll * (double)line;
+    if (t == 0) {
+      LineLocState st = *a.state;
+      if (valid) {
+        const bool first = first_s != 0;
+        a.is_first[f] = first ? 1 : 0;
+        st.prev_first_field = first ? 1 : 0;
+        st.prev_progressive_field = 0;
+        st.prev_first_hsync_readloc = a.raw_offset + a.offs[f];
+        st.prev_first_hsync_loc = fit.loc;
+        if (!fit.used_prediction)
+          st.prev_first_hsync_diff = hsync_diff_after(fit, a.fmt, first, p.mll, prev_off_s, prev_loc_s);
+      } else {
+        a.is_first[f] = st.prev_first_field >= 0 ? (1 - st.prev_first_field) : 1;
+      }
+      *a.state = st;
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------ single pass
+
+// Grid (num_fields): the reference's single-pass locator (line_locs.cu:62-543)
+// for one field: width classes adapted to the field's mean hsync width, the
+// blanking state machine for the reference pulse and the parity, the mean
+// line from the longest hsync run, and the nominal grid snapped to the
+// nearest hsync marker.  No carried state.
+__global__ void __launch_bounds__(kLT) single_pass_kernel(LineLocArgs a) {
+  chain_wait();
+  extern __shared__ double smem_d[];
+  FieldSmem& sm = *reinterpret_cast<FieldSmem*>(smem_d);
+  __shared__ int mk_s[kMaxPulses], mk_l[kMaxPulses], hs[kMaxPulses];
+  __shared__ int warp_cnt[kLT / 32];
+  __shared__ double ref_pos_s, ref_line_s, mll_s;
+  __shared__ int nm_s;
+  const int f = blockIdx.x, t = threadIdx.x;
+  if (f >= a.win->fields) return;
+  const Format& fmt = a.fmt;
+  const int n = min(max(a.pn[f], 0), kMaxPulses);
+  for (int i = t; i < n; i += kLT) {
+    sm.ps[i] = a.ps[(size_t)f * kMaxPulses + i];
+    sm.pl[i] = a.pl[(size_t)f * kMaxPulses + i];
+  }
+  __syncthreads();
+  const int* starts = sm.ps;
+  const int* lengths = sm.pl;
+  unsigned char* type = sm.cls;
+  const double tol = 0.5e-6 * fmt.fs_hz;
+  const double inl = (double)fmt.samples_per_line;
+  const double hnom = fmt.hsync_width, enom = fmt.eq_pulse_width, vnom = fmt.vsync_width;
+  // width classes shifted by the field's mean hsync width (line_locs.cu:99-135)
+  const double loose_lo = fma(-3.5, tol, hnom), loose_hi = fma(4.0, tol, hnom);
+  long long hsum = 0, hcnt = 0;
+  for (int i = t; i < n; i += kLT) {
+    const double len = (double)lengths[i];
+    if (len >= loose_lo && len <= loose_hi) {
+      hsum += lengths[i];
+      hcnt++;
+    }
+  }
+  hsum = block_sum_ll(hsum, sm.red);
+  hcnt = block_sum_ll(hcnt, sm.red);
+  const double shift = (hcnt > 0 ? (double)hsum / (double)hcnt : hnom) - hnom;
+  const double h_lo = hnom + shift - tol, h_hi = hnom + shift + tol;
+  const double e_lo = enom + shift - tol, e_hi = enom + shift + tol;
+  const double v_lo = (vnom + shift) * 0.5, v_hi = fma(2.0, tol, vnom + shift);
+  for (int i = t; i < n; i += kLT) {
+    const double len = (double)lengths[i];
+    unsigned char ty = kHsync;  // unclassified widths count as hsync
+    if (len >= v_lo && len <= v_hi) ty = kVsync;
+    else if (len >= h_lo && len <= h_hi) ty = kHsync;
+    else if (len >= e_lo && len <= e_hi) ty = kEq1;
+    type[i] = ty;
+  }
+  __syncthreads();
+  if (t == 0) {
+    // blanking state machine: the first hsync after the vertical interval (line_locs.cu:148-201)
+    int ref = -1, last_h = -1, first_eq = -1, last_eq2 = -1, state = -1;
+    for (int i = 0; i < n; i++) {
+      const int ty = type[i];
+      if (state == -1) {
+        if (ty == kHsync) {
+          state = kHsync;
+          last_h = i;
+        }
+      } else if (state == kHsync) {
+        if (ty == kHsync) last_h = i;
+        else if (ty == kEq1) {
+          state = kEq1;
+          first_eq = i;
+        } else if (ty == kVsync) state = kVsync;
+      } else if (state == kEq1) {
+        if (ty == kVsync) state = kVsync;
+        else if (ty == kHsync) {
+          state = kHsync;
+          last_h = i;
+          first_eq = -1;
+        }
+      } else if (state == kVsync) {
+        if (ty == kEq1) {
+          state = kEq2;
+          last_eq2 = i;
+        } else if (ty == kHsync) {
+          ref = i;
+          break;
+        }
+      } else if (state == kEq2) {
+        if (ty == kEq1) last_eq2 = i;
+        else if (ty == kHsync) {
+          if (last_eq2 < 0) last_eq2 = i - 1;
+          ref = i;
+          break;
+        }
+      }
+    }
+    // field parity from the half-line spacing entering or leaving the interval (line_locs.cu:203-236)
+    const bool ntsc = fmt.system == kNtsc;
+    int par = -1;
+    if (ref >= 0 && last_h >= 0 && first_eq >= 0) {
+      const double lines = (double)(starts[first_eq] - starts[last_h]) / inl;
+      par = ntsc ? (lines > 0.75 ? 1 : 0) : (lines > 0.75 ? 0 : 1);
+    }
+    if (par < 0 && ref >= 0 && last_eq2 >= 0) {
+      const double lines = (double)(starts[ref] - starts[last_eq2]) / inl;
+      par = ntsc ? (lines > 0.75 ? 1 : 0) : (lines > 0.75 ? 0 : 1);
+    }
+    a.is_first[f] = par;
+    // mean line length over the longest hsync run (line_locs.cu:246-284)
+    int best_s = -1, best_n = 0, cur_s = -1, cur_n = 0;
+    for (int i = 0; i < n; i++) {
+      if (type[i] == kHsync) {
+        if (cur_s == -1) {
+          cur_s = i;
+          cur_n = 1;
+        } else {
+          cur_n++;
+        }
+      } else {
+        if (cur_n > best_n) {
+          best_s = cur_s;
+          best_n = cur_n;
+        }
+        cur_s = -1;
+        cur_n = 0;
+      }
+    }
+    if (cur_n > best_n) {
+      best_s = cur_s;
+      best_n = cur_n;
+    }
+    double mll = inl;
+    if (best_n >= 2) {
+      long long sum = 0;
+      int cnt = 0;
+      for (int i = best_s + 1; i < best_s + best_n; i++) {
+        const double sp = (double)(starts[i] - starts[i - 1]);
+        if (sp >= inl * 0.95 && sp <= inl * 1.05) {
+          sum += starts[i] - starts[i - 1];
+          cnt++;
+        }
+      }
+      if (cnt > 0) mll = (double)sum / cnt;
+    }
+    // reference position and line (line_locs.cu:295-337)
+    double ref_pos, ref_line;
+    if (ref >= 0) {
+      ref_pos = (double)starts[ref];
+      ref_line = 10.0;
+      if (ref > n / 2) {
+        const double back = ref_pos - (double)fmt.samples_per_field;
+        if (back > 0.0) ref_pos = back;
+      }
+    } else {
+      ref = 0;
+      for (int i = 0; i < n; i++)
+        if (type[i] == kHsync) {
+          ref = i;
+          break;
+        }
+      ref_pos = n > 0 ? (double)starts[ref] : 0.0;
+      ref_line = 0.0;
+    }
+    ref_pos_s = ref_pos;
+    ref_line_s = ref_line;
+    mll_s = mll;
+  }
+  __syncthreads();
+  // line markers: an EQ pulse followed closely by a tiny hsync fragment stands
+  // for the line, and the fragment is dropped (line_locs.cu:365-399); ordered compaction
+  const double tiny = hnom * 0.75, gap = inl * 0.25;
+  int base = 0;
+  for (int i0 = 0; i0 < n; i0 += kLT) {
+    const int i = i0 + t;
+    bool keep = false;
+    if (i < n) {
+      const bool eq = type[i] == kEq1 || type[i] == kEq2;
+      const bool surrogate = eq && i + 1 < n && type[i + 1] == kHsync && (double)lengths[i + 1] <= tiny &&
+                             (double)(starts[i + 1] - starts[i]) <= gap;
+      const bool fragment = type[i] == kHsync && (double)lengths[i] <= tiny && i > 0 &&
+                            (type[i - 1] == kEq1 || type[i - 1] == kEq2) && (double)(starts[i] - starts[i - 1]) <= gap;
+      keep = surrogate || (type[i] == kHsync && !fragment);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if ((t & 31) == 0) warp_cnt[t >> 5] = __popc(m);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < kLT / 32; w++) {
+      if (w < (t >> 5)) before += warp_cnt[w];
+      total += warp_cnt[w];
+    }
+    if (keep) {
+      const int k = base + before + __popc(m & ((1u << (t & 31)) - 1u));
+      mk_s[k] = starts[i];
+      mk_l[k] = lengths[i];
+    }
+    base += total;
+    __syncthreads();
+  }
+  if (t == 0) {
+    // one marker per line interval: the one nearest the nominal hsync width (line_locs.cu:401-425)
+    const double dup = inl * 0.75;
+    const int nm = base;
+    int nh = 0;
+    for (int c0 = 0; c0 < nm;) {
+      int best = c0;
+      double score = fabs((double)mk_l[c0] - hnom);
+      int c1 = c0 + 1;
+      while (c1 < nm && (double)(mk_s[c1] - mk_s[c0]) < dup) {
+        const double sc = fabs((double)mk_l[c1] - hnom);
+        if (sc < score || (sc == score && mk_s[c1] < mk_s[best])) {
+          best = c1;
+          score = sc;
+        }
+        c1++;
+      }
+      hs[nh++] = mk_s[best];
+      c0 = c1;
+    }
+    nm_s = nh;
+    // nominal grid snapped to the nearest marker ahead of a monotonic cursor (line_locs.cu:429-470)
+    const double mll = mll_s, ref_pos = ref_pos_s, ref_line = ref_line_s;
+    const double max_d = mll / 1.5;
+    double* locs = a.ll + (size_t)f * fmt.lines_per_frame;
+    int cur = 0;
+    for (int line = 0; line < fmt.lines_per_frame; line++) {
+      const double expected = fma(mll, (double)line - ref_line, ref_pos);
+      locs[line] = expected;
+      if (cur >= nh) continue;
+      double best_d = max_d;
+      int best_pos = -1;
+      for (int s = cur; s < nh; s++) {
+        const double d = fabs((double)hs[s] - expected);
+        if (d <= best_d) {
+          best_d = d;
+          best_pos = hs[s];
+          cur = s;
+        }
+        if (s + 1 < nh) {
+          if (fabs((double)hs[s + 1] - expected) > d) break;
+        } else {
+          break;
+        }
+      }
+      if (best_pos >= 0) {
+        locs[line] = (double)best_pos;
+        cur++;
+      }
+    }
+  }
+  // the raw pulses with their nominal classes stand for the validated list
+  // when inspected (line_locs.cu:18-49 with the thresholds of :551-558)
+  if (a.dbg_vn) {
+    const double ntol = 0.5e-6 * fmt.fs_hz;
+    for (int i = t; i < n; i += kLT) {
+      const double len = (double)lengths[i];
+      int ty = kHsync;
+      if (len >= fmt.vsync_width * 0.5 && len <= fmt.vsync_width + 1.0e-6 * fmt.fs_hz) ty = kVsync;
+      else if (len >= fmt.hsync_width - ntol && len <= fmt.hsync_width + ntol) ty = kHsync;
+      else if (len >= fmt.eq_pulse_width - ntol && len <= fmt.eq_pulse_width + ntol) ty = kEq1;
+      a.dbg_vs[(size_t)f * kMaxPulses + i] = starts[i];
+      a.dbg_vl[(size_t)f * kMaxPulses + i] = lengths[i];
+      a.dbg_vt[(size_t)f * kMaxPulses + i] = ty;
+    }
+    if (t == 0) a.dbg_vn[f] = n;
+  }
+}
+
+}  // namespace
+
+size_t lineloc_smem_bytes() { return sizeof(FieldSmem); }
+
+cudaError_t launch_field_windows(const LineLocArgs& a, cudaStream_t st) {
+  return launch_chained(fieldwin_kernel, dim3(1), dim3(1024), 0, st, a);
+}
+
+cudaError_t launch_field_pulses(const LineLocArgs& a, cudaStream_t st) {
+  if (a.num_fields <= 0) return cudaSuccess;
+  return launch_chained(pulses_kernel, dim3(a.num_fields), dim3(kLT), 0, st, a);
+}
+
+cudaError_t launch_line_locations(const LineLocArgs& a, cudaStream_t st) {
+  if (a.num_fields <= 0) return cudaSuccess;
+  const size_t smem = sizeof(FieldSmem);
+  cudaError_t e;
+  if (a.single_pass) {
+    e = cudaFuncSetAttribute(single_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return launch_chained(single_pass_kernel, dim3(a.num_fields), dim3(kLT), smem, st, a);
+  }
+  e = cudaFuncSetAttribute(prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = launch_chained(prepare_kernel, dim3(a.num_fields), dim3(kLT), smem, st, a);
+  if (e != cudaSuccess) return e;
+  return launch_chained(finish_kernel, dim3(1), dim3(kLT), smem, st, a);
+}
+
+}  // namespace cuvhs

@@ -63,9 +63,8 @@ int phase_id_for(int is_first, int quadrant) {
 const char* const kStageNames[kNumStages] = {"k1a_demod",      "k1b_video_sync", "sync_edges",
                                              "hsync_refine",   "luma_resample",  "chroma_prefilter",
                                              "chroma_lines",   "burst_metric",   "dropouts",
-                                             "sync_guard",
-                                             "host_edges_wait", "host_runs",      "host_prepare",
-                                             "host_lines",     "host_chroma_wait", "host_final_wait"};
+                                             "sync_guard",     "field_windows",  "line_locations",
+                                             "host_windows_wait", "host_chroma_wait", "host_final_wait"};
 
 double Context::host_clock() const {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -82,11 +81,11 @@ cudaEvent_t Context::next_event() {
   return event_pool[pool_used++];
 }
 
-void Context::begin_stage(int stage, cudaEvent_t& a) {
+void Context::begin_stage_on(int stage, cudaEvent_t& a, cudaStream_t st) {
   a = nullptr;
   if (!timing || !((timing_mask >> stage) & 1u)) return;
   a = next_event();
-  cudaEventRecord(a, stream);
+  cudaEventRecord(a, st);
   if (t0_pending) {
     ev_t0 = a;
     t0_pending = false;
@@ -94,12 +93,12 @@ void Context::begin_stage(int stage, cudaEvent_t& a) {
   }
 }
 
-void Context::end_stage(int stage, cudaEvent_t a, int kernels) {
+void Context::end_stage_on(int stage, cudaEvent_t a, cudaStream_t st, int kernels) {
   stage_launches[stage] += kernels;
   launches += kernels;
   if (!timing || !a) return;
   cudaEvent_t b = next_event();
-  cudaEventRecord(b, stream);
+  cudaEventRecord(b, st);
   marks.push_back({stage, a, b});
 }
 
@@ -142,8 +141,10 @@ void Context::release() {
   }
   if (hstream) cudaStreamDestroy(hstream);
   hstream = nullptr;
-  if (ev_ll) cudaEventDestroy(ev_ll);
-  ev_ll = nullptr;
+  for (cudaEvent_t* e : {&ev_ll, &ev_win, &ev_winhost}) {
+    if (*e) cudaEventDestroy(*e);
+    *e = nullptr;
+  }
   if (lstream) cudaStreamDestroy(lstream);
   lstream = nullptr;
   pf = Prefetch();
@@ -210,7 +211,8 @@ bool Context::init(const cuvhs_config& c) {
   cudaMemGetInfo(&free_b, &total_b);
   const size_t field_px = (size_t)fmt.output_line_len * fmt.output_field_lines;
   const size_t per_field = (size_t)spp * (2 * bps + 4 * 5) + (size_t)spp / 4 + field_px * 8 +
-                           (size_t)fmt.output_field_lines * kMaxBurstLen * 4 + 65536 + dropout_class_bytes_per_field(spp);
+                           (size_t)fmt.output_field_lines * kMaxBurstLen * 4 + 65536 + dropout_class_bytes_per_field(spp) +
+                           (size_t)kMaxValid * 17 + (size_t)kMaxPulses * 20 + sizeof(FieldPrep);
   int b = c.batch_fields;
   if (b <= 0) {
     b = (int)std::min<size_t>((size_t)(free_b * 0.5) / per_field, 2048);
@@ -221,15 +223,12 @@ bool Context::init(const cuvhs_config& c) {
   const int cap_fields = (int)std::min<long long>(INT_MAX / 2 / (long long)spp, 1 << 20);
   if (b > cap_fields) b = cap_fields;
   batch = b;
-  {
-    const int hw = (int)std::thread::hardware_concurrency();
-    const int n = pool_threads >= 0 ? pool_threads : std::min(hw - 1, 15);
-    pool.reset(new WorkPool(std::max(0, n)));
-  }
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&xstream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&hstream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&lstream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithPriority(&lstream, cudaStreamNonBlocking, prio_high) != cudaSuccess) {
     err = "cudaStreamCreate failed";
     status = CUVHS_ERR_CUDA;
     return false;
@@ -285,6 +284,24 @@ bool Context::init(const cuvhs_config& c) {
   d_twb_inv = A((float2*)nullptr, des.tw_b.size());
   d_twc_inv = A((float2*)nullptr, des.tw_c.size());
   d_twl_inv = A((float2*)nullptr, des.tw_line.size());
+  d_win = A((WindowInfo*)nullptr, 1);
+  d_offs = A((long long*)nullptr, (size_t)batch + 1);
+  d_cand = A((int*)nullptr, edge_cap);
+  d_ps = A((int*)nullptr, (size_t)batch * kMaxPulses);
+  d_pl = A((int*)nullptr, (size_t)batch * kMaxPulses);
+  d_pn = A((int*)nullptr, batch);
+  d_vs = A((int*)nullptr, (size_t)batch * kMaxValid);
+  d_vl = A((int*)nullptr, (size_t)batch * kMaxValid);
+  d_vt = A((unsigned char*)nullptr, (size_t)batch * kMaxValid);
+  d_vd = A((double*)nullptr, (size_t)batch * kMaxValid);
+  d_vn = A((int*)nullptr, batch);
+  d_prep = A((FieldPrep*)nullptr, batch);
+  d_lls = A((LineLocState*)nullptr, 1);
+  d_is_first = A((int*)nullptr, batch);
+  d_dbg_vs = A((int*)nullptr, (size_t)batch * kMaxPulses);
+  d_dbg_vl = A((int*)nullptr, (size_t)batch * kMaxPulses);
+  d_dbg_vt = A((int*)nullptr, (size_t)batch * kMaxPulses);
+  d_dbg_vn = A((int*)nullptr, batch);
   d_ga64 = A((double*)nullptr, des.ga64.size());
   d_hs64 = A((double*)nullptr, des.hs64.size());
   d_guard_list = A((unsigned*)nullptr, kGuardCap);
@@ -315,12 +332,11 @@ bool Context::init(const cuvhs_config& c) {
     host_allocations.push_back(p);
     return static_cast<T*>(p);
   };
-  const size_t guess = (size_t)std::min(edge_cap, batch * kEdgeGuessPerField);
   hp_counts = H((int*)nullptr, 4);
+  hp_win = H((WindowInfo*)nullptr, 1);
+  hp_offs = H((long long*)nullptr, (size_t)batch + 1);
+  hp_is_first = H((int*)nullptr, batch);
   hp_guard = H((int*)nullptr, 1);
-  hp_fall = H((unsigned*)nullptr, guess);
-  hp_rise = H((unsigned*)nullptr, guess);
-  hp_ll = H((double*)nullptr, (size_t)batch * fmt.lines_per_frame);
   hp_track = H((int*)nullptr, batch);
   hp_trial = H((int*)nullptr, 2);
   hp_burst = H((float*)nullptr, (size_t)2 * fmt.output_field_lines * fmt.burst_len);
@@ -350,7 +366,9 @@ bool Context::init(const cuvhs_config& c) {
   bool ev_ok = cudaEventCreateWithFlags(&ev_host, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_luma, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_edges, cudaEventDisableTiming) == cudaSuccess &&
-               cudaEventCreateWithFlags(&ev_ll, cudaEventDisableTiming) == cudaSuccess;
+               cudaEventCreateWithFlags(&ev_ll, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev_win, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev_winhost, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t* e : {&ev_prefetch, &ev_small, &ev_chroma, &ev_out_done[0], &ev_out_done[1]})
     ev_ok = ev_ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t& e : ev_piece) ev_ok = ev_ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
@@ -373,6 +391,10 @@ bool Context::init(const cuvhs_config& c) {
   upload(d_ga64, des.ga64, stream);
   upload(d_hs64, des.hs64, stream);
   cudaMemsetAsync(d_guard_count, 0, sizeof(int), stream);
+  {
+    const LineLocState fresh;
+    cudaMemcpy(d_lls, &fresh, sizeof(fresh), cudaMemcpyHostToDevice);
+  }
   std::vector<double> col_frac(fmt.output_line_len);
   for (int c = 0; c < fmt.output_line_len; c++) col_frac[c] = (double)c / (double)fmt.output_line_len;
   d_col_frac = A((double*)nullptr, col_frac.size());
@@ -435,7 +457,7 @@ bool Context::wait_host_event(const char* where) {
 }
 
 void Context::reset_state() {
-  lls = LineLocState();
+  if (d_lls) write_lls(LineLocState());
   chroma_valid = false;
   chroma_track = 0;
   chroma_threshold = 0.0;
@@ -636,30 +658,6 @@ DropoutArgs Context::dropout_args(int P) const {
   return dd;
 }
 
-bool Context::read_edges(const float* sync, long long total) {
-  const float thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
-  cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), stream);
-  {
-    cudaEvent_t ev_;
-    begin_stage(kStageEdges, ev_);
-    launch_edges(sync, total, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, d_edge_mask, stream);
-    end_stage(kStageEdges, ev_, 3);
-  }
-  cudaMemcpyAsync(hp_counts, d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream);
-  if (!this->sync("sync edges")) return false;
-  const int nfall = hp_counts[0], nrise = hp_counts[1];
-  if (nfall > edge_cap || nrise > edge_cap) {
-    err = "sync edge list overflow";
-    status = CUVHS_ERR_CAPACITY;
-    return false;
-  }
-  h_fall.resize(nfall);
-  h_rise.resize(nrise);
-  if (nfall) cudaMemcpyAsync(h_fall.data(), d_fall, (size_t)nfall * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
-  if (nrise) cudaMemcpyAsync(h_rise.data(), d_rise, (size_t)nrise * sizeof(unsigned), cudaMemcpyDeviceToHost, stream);
-  return this->sync("sync edge lists");
-}
-
 bool Context::guard_ok(int listed) {
   if (listed <= kGuardCap) return true;
   err = "more than " + std::to_string(kGuardCap) + " sync samples near the pulse threshold in one chunk (" +
@@ -668,64 +666,80 @@ bool Context::guard_ok(int listed) {
   return false;
 }
 
-// Sync threshold runs [start, end) from the falling and rising edge lists
-// (both in sample order): end = the first rising edge after start, or the
-// range end.
-void edge_runs(const std::vector<unsigned>& fall, const std::vector<unsigned>& rise, long long total,
-               std::vector<long long>& run_start, std::vector<long long>& run_end) {
-  run_start.resize(fall.size());
-  run_end.resize(fall.size());
-  size_t r = 0;
-  for (size_t i = 0; i < fall.size(); i++) {
-    while (r < rise.size() && rise[r] <= fall[i]) r++;
-    run_start[i] = (long long)fall[i];
-    run_end[i] = r < rise.size() ? (long long)rise[r] : total;
+bool Context::field_windows(const float* sync, long long total, int tiles, int num_fields) {
+  const float thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
+  cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), stream);
+  {
+    cudaEvent_t ev_;
+    begin_stage(kStageEdges, ev_);
+    launch_edges(sync, total, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, d_edge_mask, stream);
+    end_stage(kStageEdges, ev_, 3);
   }
+  LineLocArgs la = lineloc_args(tiles, num_fields, 0);
+  la.total = total;
+  launch_field_windows(la, stream);
+  cudaMemcpyAsync(hp_win, d_win, sizeof(WindowInfo), cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(hp_offs, d_offs, (size_t)num_fields * sizeof(long long), cudaMemcpyDeviceToHost, stream);
+  if (!check_cuda("field windows") || !this->sync("field windows")) return false;
+  if (hp_win->err) {
+    err = "sync edge list overflow";
+    status = CUVHS_ERR_CAPACITY;
+    return false;
+  }
+  return true;
 }
 
-// VSYNC candidates (runs of 20-35 us, vsync_discover.cu:58-72) and the field
-// windows clustered from them (pipeline.cu:1567-1651).
-void field_windows(const Format& fmt, const std::vector<long long>& run_start, const std::vector<long long>& run_end,
-                   int T, int num_fields, FieldWindows& w) {
-  const size_t spf = (size_t)fmt.samples_per_field;
-  const int minw = (int)(20.0e-6 * fmt.fs_hz), maxw = (int)(35.0e-6 * fmt.fs_hz);
-  w.cand.clear();
-  for (size_t i = 0; i < run_start.size(); i++) {
-    const long long wd = run_end[i] - run_start[i];
-    if (wd >= minw && wd <= maxw) w.cand.push_back((int)run_start[i]);
+LineLocArgs Context::lineloc_args(int tiles, int num_fields, long long raw_offset) const {
+  LineLocArgs a;
+  a.fmt = fmt;
+  a.fall = d_fall;
+  a.rise = d_rise;
+  a.counts = d_counts;
+  a.edge_cap = edge_cap;
+  a.total = (long long)tiles * spp;
+  a.tiles = tiles;
+  a.num_fields = num_fields;
+  a.minw = (int)(20.0e-6 * fmt.fs_hz);
+  a.maxw = (int)(35.0e-6 * fmt.fs_hz);
+  a.win = d_win;
+  a.offs = d_offs;
+  a.cand = d_cand;
+  a.cand_cap = edge_cap;
+  a.ps = d_ps;
+  a.pl = d_pl;
+  a.pn = d_pn;
+  a.vs = d_vs;
+  a.vl = d_vl;
+  a.vt = d_vt;
+  a.vd = d_vd;
+  a.vn = d_vn;
+  a.prep = d_prep;
+  a.state = d_lls;
+  a.ll = d_ll;
+  a.is_first = d_is_first;
+  a.raw_offset = raw_offset;
+  a.single_pass = single_pass ? 1 : 0;
+  if (debug) {
+    a.dbg_vs = d_dbg_vs;
+    a.dbg_vl = d_dbg_vl;
+    a.dbg_vt = d_dbg_vt;
+    a.dbg_vn = d_dbg_vn;
   }
-  w.offs.clear();
-  for (int pos : w.cand) {
-    if (w.offs.empty() || ((size_t)pos - w.offs.back() > (size_t)(fmt.samples_per_field / 2))) {
-      const size_t safe = (pos > 5 * fmt.samples_per_line) ? (size_t)(pos - 5 * fmt.samples_per_line) : 0;
-      w.offs.push_back(safe);
-    }
-  }
-  if (w.offs.empty())
-    for (int i = 0; i < T; i++) w.offs.push_back((size_t)i * spf);
-  if ((int)w.offs.size() > num_fields) w.offs.resize(num_fields);
-  size_t actual_spf = spf;
-  if (w.offs.size() >= 2) actual_spf = (w.offs.back() - w.offs.front()) / (w.offs.size() - 1);
-  const size_t predicted = w.offs.back() + actual_spf, margin = 10 * (size_t)fmt.samples_per_line;
-  w.next_rel = predicted > margin ? predicted - margin : predicted;
+  return a;
 }
 
-// Pulses of the field window starting at chunk sample off (sync_pulses.cu:10-58):
-// runs that start after off and end within the spp-sample scan, at most
-// kMaxPulses.
-void window_pulses(const std::vector<long long>& run_start, const std::vector<long long>& run_end, long long off,
-                   int spp, std::vector<int>& ps, std::vector<int>& pl) {
-  ps.clear();
-  pl.clear();
-  const long long lim = off + spp - 1;  // last sample index the field's scan reaches
-  size_t i = std::lower_bound(run_start.begin(), run_start.end(), off + 1) - run_start.begin();
-  for (; i < run_start.size() && run_start[i] <= lim; i++) {
-    if (run_end[i] > lim) break;  // still open when the scan ends
-    if ((int)ps.size() < kMaxPulses) {
-      ps.push_back((int)run_start[i]);
-      pl.push_back((int)(run_end[i] - run_start[i]));
-    }
-  }
+bool Context::read_lls(LineLocState& st) {
+  if (cudaStreamSynchronize(stream) != cudaSuccess || cudaStreamSynchronize(lstream) != cudaSuccess ||
+      cudaMemcpy(&st, d_lls, sizeof(LineLocState), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return check_cuda("line-location state");
+  return true;
+}
+
+bool Context::write_lls(const LineLocState& st) {
+  if (cudaStreamSynchronize(stream) != cudaSuccess || cudaStreamSynchronize(lstream) != cudaSuccess ||
+      cudaMemcpy(d_lls, &st, sizeof(LineLocState), cudaMemcpyHostToDevice) != cudaSuccess)
+    return check_cuda("line-location state");
+  return true;
 }
 
 // Chroma of fields [0, P) with the track and phase decisions of
@@ -979,31 +993,45 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     end_stage(kStageGuard, ev_);
   }
   if (!check_cuda("demod")) return false;
-  // ---- sync edges over the demodulated range.  One copy brings back the
-  // counts and a speculative prefix of both edge lists; a second copy is
-  // needed only when a list is longer than the prefix.
-  const float thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
-  cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), stream);
+  // ---- sync edges over the demodulated range, the field windows clustered
+  // from their VSYNC runs, and the line locations: all on the device.  The
+  // host reads back only the field count, offsets and next chunk start (a
+  // few bytes) while the chroma pre-band-pass and the line locations run.
   const long long total_chunk = (long long)T * spp;
+  cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), stream);
   {
     cudaEvent_t ev_;
     begin_stage(kStageEdges, ev_);
+    const float thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
     launch_edges(d_sync, total_chunk, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, d_edge_mask, stream);
     end_stage(kStageEdges, ev_, 3);
   }
-  // the copies run on the copy stream, so the pre-band-pass below starts
-  // right after the edge kernels
-  const int guess = std::min(edge_cap, T * kEdgeGuessPerField);
-  cudaEventRecord(ev_edges, stream);
-  cudaStreamWaitEvent(xstream, ev_edges, 0);
-  cudaMemcpyAsync(hp_counts, d_counts, 4 * sizeof(int), cudaMemcpyDeviceToHost, xstream);
+  LineLocArgs lla = lineloc_args(T, num_fields, (long long)raw_offset);
+  {
+    cudaEvent_t ev_;
+    begin_stage(kStageWindows, ev_);
+    launch_field_windows(lla, stream);
+    end_stage(kStageWindows, ev_);
+  }
+  cudaEventRecord(ev_win, stream);
+  // the window record and offsets come back on the copy stream
+  cudaStreamWaitEvent(xstream, ev_win, 0);
+  cudaMemcpyAsync(hp_win, d_win, sizeof(WindowInfo), cudaMemcpyDeviceToHost, xstream);
+  cudaMemcpyAsync(hp_offs, d_offs, (size_t)num_fields * sizeof(long long), cudaMemcpyDeviceToHost, xstream);
   cudaMemcpyAsync(hp_guard, d_guard_count, sizeof(int), cudaMemcpyDeviceToHost, xstream);
-  cudaMemcpyAsync(hp_fall, d_fall, (size_t)guess * sizeof(unsigned), cudaMemcpyDeviceToHost, xstream);
-  cudaMemcpyAsync(hp_rise, d_rise, (size_t)guess * sizeof(unsigned), cudaMemcpyDeviceToHost, xstream);
-  cudaEventRecord(ev_host, xstream);
-  // ---- the colour-under pre-band-pass needs only the raw samples: it runs on
-  // the GPU while the host turns edges into field windows and line locations.
-  // It covers all T demodulated slots; the detected fields are a prefix.
+  cudaEventRecord(ev_winhost, xstream);
+  // line locations on the line stream, beside the pre-band-pass
+  cudaStreamWaitEvent(lstream, ev_win, 0);
+  {
+    cudaEvent_t ev_;
+    begin_stage_on(kStageLines, ev_, lstream);
+    launch_field_pulses(lla, lstream);
+    launch_line_locations(lla, lstream);
+    end_stage_on(kStageLines, ev_, lstream, single_pass ? 2 : 3);
+  }
+  cudaEventRecord(ev_ll, lstream);
+  // ---- the colour-under pre-band-pass needs only the raw samples.  It
+  // covers all T demodulated slots; the detected fields are a prefix.
   const int LPF = fmt.lines_per_frame;
   const int H = fmt.output_field_lines;
   ChromaArgs ca = chroma_args(da.raw, (int)n_read, da.dc, T);
@@ -1018,38 +1046,24 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     end_stage(kStageChromaPre, ev_);
   }
   if (!check_cuda("chroma prefilter")) return false;
-  if (pool) pool->prime();  // the line-location job follows the edge lists
   double t_host = host_clock();
-  if (!wait_host_event("edges")) return false;
-  host_phase(kHostEdgesWait, t_host);
-  t_host = host_clock();
-  const int nfall = hp_counts[0], nrise = hp_counts[1];
-  if (nfall > edge_cap || nrise > edge_cap) {
+  {
+    const cudaError_t e = cudaEventSynchronize(ev_winhost);
+    if (e != cudaSuccess) {
+      err = std::string("field windows: ") + cudaGetErrorString(e);
+      status = CUVHS_ERR_CUDA;
+      return false;
+    }
+  }
+  host_phase(kHostWindowsWait, t_host);
+  if (hp_win->err) {
     err = "sync edge list overflow";
     status = CUVHS_ERR_CAPACITY;
     return false;
   }
   if (!guard_ok(*hp_guard)) return false;
-  h_fall.assign(hp_fall, hp_fall + std::min(nfall, guess));
-  h_rise.assign(hp_rise, hp_rise + std::min(nrise, guess));
-  if (nfall > guess || nrise > guess) {
-    h_fall.resize(nfall);
-    h_rise.resize(nrise);
-    if (nfall > guess)
-      cudaMemcpyAsync(h_fall.data() + guess, d_fall + guess, (size_t)(nfall - guess) * sizeof(unsigned),
-                      cudaMemcpyDeviceToHost, stream);
-    if (nrise > guess)
-      cudaMemcpyAsync(h_rise.data() + guess, d_rise + guess, (size_t)(nrise - guess) * sizeof(unsigned),
-                      cudaMemcpyDeviceToHost, stream);
-    if (!sync("edge lists")) return false;
-  }
-  // both lists arrive in sample order
-  edge_runs(h_fall, h_rise, total_chunk, run_start, run_end);
-  // ---- VSYNC candidates and field windows (vsync_discover.cu:58-72, pipeline.cu:1567-1651)
-  field_windows(fmt, run_start, run_end, T, num_fields, win);
-  const std::vector<size_t>& offs = win.offs;
-  const int P = (int)offs.size();
-  res.next_raw_offset = raw_offset + win.next_rel;
+  const int P = hp_win->fields;
+  res.next_raw_offset = raw_offset + (uint64_t)hp_win->next_rel;
   // ---- the next chunk of a host capture starts at next_raw_offset: copy its
   // window into the other raw buffer now (the chunk loop's arithmetic, so the
   // next call finds it); the previous chunk that read that buffer has ended.
@@ -1071,55 +1085,41 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
       }
     }
   }
-  // ---- per-field pulses and line locations (sync_pulses.cu:10-58, pipeline.cu:1717-1778)
-  h_is_first.assign(P, -1);
   if (debug) {
+    // the chunk's intermediates as the reference keeps them: VSYNC
+    // candidates, raw and validated pulses, coarse line locations
+    if (cudaStreamSynchronize(lstream) != cudaSuccess) return check_cuda("line locations");
+    const int nc = std::min(hp_win->ncand, edge_cap);
+    dbg_vsync.resize(nc);
+    if (nc) cudaMemcpy(dbg_vsync.data(), d_cand, nc * sizeof(int), cudaMemcpyDeviceToHost);
+    const size_t np = (size_t)P * kMaxPulses;
     dbg_k2c.assign(P, 0);
-    dbg_k2s.assign((size_t)P * kMaxPulses, 0);
-    dbg_k2l.assign((size_t)P * kMaxPulses, 0);
+    dbg_k2s.assign(np, 0);
+    dbg_k2l.assign(np, 0);
     dbg_k2bc.assign(P, 0);
-    dbg_k2bs.assign((size_t)P * kMaxPulses, 0);
-    dbg_k2bl.assign((size_t)P * kMaxPulses, 0);
-    dbg_k2bt.assign((size_t)P * kMaxPulses, kHsync);
-  }
-  host_phase(kHostRuns, t_host);
-  t_host = host_clock();
-  // stateless per-field part (pulses, validation, mean line) on the host pool
-  if ((int)preps.size() < P) preps.resize(P);
-  pool->run(P, [&](int f) {
-    thread_local std::vector<int> ps, pl;
-    window_pulses(run_start, run_end, (long long)offs[f], spp, ps, pl);
-    if (single_pass) single_pass_lines(fmt, ps.data(), pl.data(), (int)ps.size(), hp_ll + (size_t)f * LPF, &h_is_first[f]);
-    else prepare_lines(fmt, ps.data(), pl.data(), (int)ps.size(), preps[f], hp_ll + (size_t)f * LPF);
-    if (debug) {
-      dbg_k2c[f] = (int)ps.size();
-      std::copy(ps.begin(), ps.end(), dbg_k2s.begin() + (size_t)f * kMaxPulses);
-      std::copy(pl.begin(), pl.end(), dbg_k2l.begin() + (size_t)f * kMaxPulses);
-      if (single_pass) {  // no validation: the raw pulses with their nominal classes
-        dbg_k2bc[f] = (int)ps.size();
-        std::copy(ps.begin(), ps.end(), dbg_k2bs.begin() + (size_t)f * kMaxPulses);
-        std::copy(pl.begin(), pl.end(), dbg_k2bl.begin() + (size_t)f * kMaxPulses);
-        nominal_pulse_types(fmt, pl.data(), (int)pl.size(), dbg_k2bt.data() + (size_t)f * kMaxPulses);
-      }
+    dbg_k2bs.assign(np, 0);
+    dbg_k2bl.assign(np, 0);
+    dbg_k2bt.assign(np, kHsync);
+    if (P) {
+      cudaMemcpy(dbg_k2c.data(), d_pn, P * sizeof(int), cudaMemcpyDeviceToHost);
+      cudaMemcpy(dbg_k2bc.data(), d_dbg_vn, P * sizeof(int), cudaMemcpyDeviceToHost);
+      std::vector<int> tmp(np);
+      auto rows = [&](const int* d, std::vector<int>& out, const std::vector<int>& cnt) {
+        cudaMemcpy(tmp.data(), d, np * sizeof(int), cudaMemcpyDeviceToHost);
+        for (int f = 0; f < P; f++)
+          std::copy(tmp.begin() + (size_t)f * kMaxPulses, tmp.begin() + (size_t)f * kMaxPulses + cnt[f],
+                    out.begin() + (size_t)f * kMaxPulses);
+      };
+      rows(d_ps, dbg_k2s, dbg_k2c);
+      rows(d_pl, dbg_k2l, dbg_k2c);
+      rows(d_dbg_vs, dbg_k2bs, dbg_k2bc);
+      rows(d_dbg_vl, dbg_k2bl, dbg_k2bc);
+      rows(d_dbg_vt, dbg_k2bt, dbg_k2bc);
     }
-  });
-  host_phase(kHostPrepare, t_host);
-  t_host = host_clock();
-  // stateful part in field order
-  FieldLines fl;
-  for (int f = 0; f < P && !single_pass; f++) {
-    int first = -1;
-    finish_lines(fmt, preps[f], (long long)(raw_offset + offs[f]), lls, hp_ll + (size_t)f * LPF,
-                 debug ? &fl : nullptr, &first);
-    h_is_first[f] = first;
-    if (debug) {
-      dbg_k2bc[f] = (int)fl.starts.size();
-      std::copy(fl.starts.begin(), fl.starts.end(), dbg_k2bs.begin() + (size_t)f * kMaxPulses);
-      std::copy(fl.lengths.begin(), fl.lengths.end(), dbg_k2bl.begin() + (size_t)f * kMaxPulses);
-      std::copy(fl.types.begin(), fl.types.end(), dbg_k2bt.begin() + (size_t)f * kMaxPulses);
-    }
-  }
-  if (debug) {
+    dbg_offs.assign(hp_offs, hp_offs + P);
+    dbg_ll_coarse.resize((size_t)P * LPF);
+    if (P) cudaMemcpy(dbg_ll_coarse.data(), d_ll, dbg_ll_coarse.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    dbg_meta = {T, P, spp};
     const int ng = std::min(*hp_guard, kGuardCap);
     std::vector<unsigned> pos(ng);
     dbg_guard_vals.resize(ng);
@@ -1128,15 +1128,14 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
       cudaMemcpy(dbg_guard_vals.data(), d_guard_vals, ng * sizeof(double), cudaMemcpyDeviceToHost);
     }
     dbg_guard_pos.assign(pos.begin(), pos.end());
-    dbg_vsync = win.cand;
-    dbg_offs.assign(offs.begin(), offs.end());
-    dbg_ll_coarse.assign(hp_ll, hp_ll + (size_t)P * LPF);
-    dbg_meta = {T, P, spp};
   }
-  cudaMemcpyAsync(d_ll, hp_ll, (size_t)P * LPF * sizeof(double), cudaMemcpyHostToDevice, lstream);
-  cudaEventRecord(ev_ll, lstream);
+  if (P == 0) {
+    // no field window (the reference returns 0 fields): drain and report none
+    if (!sync("empty chunk")) return false;
+    res.fields = 0;
+    return true;
+  }
   cudaStreamWaitEvent(stream, ev_ll, 0);
-  host_phase(kHostLines, t_host);
   // ---- K4 hsync refinement, K5 luma
   LineArgs la = line_args(P);
   {
@@ -1168,6 +1167,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   cudaEventRecord(ev_luma, stream);
   cudaStreamWaitEvent(xstream, ev_luma, 0);
   cudaMemcpyAsync(hp_do_count, d_do_count, P * sizeof(int), cudaMemcpyDeviceToHost, xstream);
+  cudaMemcpyAsync(hp_is_first, d_is_first, P * sizeof(int), cudaMemcpyDeviceToHost, xstream);
   const size_t ndo = (size_t)P * kMaxDropouts;
   cudaMemcpyAsync(hp_do_lines, d_do_lines, ndo * sizeof(int), cudaMemcpyDeviceToHost, xstream);
   cudaMemcpyAsync(hp_do_starts, d_do_starts, ndo * sizeof(int), cudaMemcpyDeviceToHost, xstream);
@@ -1220,9 +1220,9 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   res.field_info.resize(P);
   for (int i = 0; i < P; i++) {
     cuvhs_field_info& fi = res.field_info[i];
-    fi.file_loc = raw_offset + offs[i];
+    fi.file_loc = raw_offset + (uint64_t)hp_offs[i];
     bool first;
-    if (h_is_first[i] >= 0 && (h_is_first[i] == 1) != last_parity) first = (h_is_first[i] == 1);
+    if (hp_is_first[i] >= 0 && (hp_is_first[i] == 1) != last_parity) first = (hp_is_first[i] == 1);
     else first = !last_parity;
     last_parity = first;
     fi.is_first_field = first ? 1 : 0;
@@ -1230,7 +1230,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     fi.dropout_count = std::max(0, std::min(hp_do_count[i], kMaxDropouts));
     fi.dropout_offset = 0;
   }
-  if (debug) dbg_is_first = h_is_first;
+  if (debug) dbg_is_first.assign(hp_is_first, hp_is_first + P);
   return true;
 }
 

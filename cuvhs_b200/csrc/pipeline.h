@@ -30,32 +30,17 @@ enum Stage {
   kStageChromaLines,
   kStageBurstMetric,
   kStageDropouts,
-  kStageGuard,  // FP64 re-evaluation of near-threshold sync samples
+  kStageGuard,    // FP64 re-evaluation of near-threshold sync samples
+  kStageWindows,  // VSYNC clustering into field windows
+  kStageLines,    // line locations (pulses, validation, anchors, snap), on the line stream
   // host phases (wall time on the calling thread)
-  kHostEdgesWait,
-  kHostRuns,      // edge lists -> pulse runs, VSYNC candidates, field windows
-  kHostPrepare,   // per-field pulse validation on the host pool
-  kHostLines,     // stateful line locations in field order + upload
+  kHostWindowsWait,  // waiting for the chunk's field count and window offsets
   kHostChromaWait,
   kHostFinalWait,
   kNumStages
 };
-constexpr int kFirstHostStage = kHostEdgesWait;
+constexpr int kFirstHostStage = kHostWindowsWait;
 extern const char* const kStageNames[kNumStages];
-
-// VSYNC candidates, field windows and the predicted start of the next chunk
-// (relative to this chunk's first sample) from one chunk's sync runs.
-struct FieldWindows {
-  std::vector<int> cand;
-  std::vector<size_t> offs;
-  size_t next_rel = 0;
-};
-void edge_runs(const std::vector<unsigned>& fall, const std::vector<unsigned>& rise, long long total,
-               std::vector<long long>& run_start, std::vector<long long>& run_end);
-void field_windows(const Format& fmt, const std::vector<long long>& run_start, const std::vector<long long>& run_end,
-                   int T, int num_fields, FieldWindows& w);
-void window_pulses(const std::vector<long long>& run_start, const std::vector<long long>& run_end, long long off,
-                   int spp, std::vector<int>& ps, std::vector<int>& pl);
 
 struct Context {
   cuvhs_config cfg{};
@@ -66,7 +51,6 @@ struct Context {
   int spp = 0;
   int env_blocks = 0;
   int edge_cap = 0;
-  int pool_threads = -1;  // host line-location helpers; -1 = min(cores - 1, 15)
   int in_fmt = 0;         // InputFormat of the capture samples
   int bps = 1;            // bytes per capture sample
   bool dc_correct = false;
@@ -87,10 +71,11 @@ struct Context {
   // the prefetch stream, and with page-locked destinations a chunk's planes
   // leave from one of two output sets while the next chunk already runs.
   cudaStream_t hstream = nullptr;  // host->device input copies
-  // Line-location upload: its own stream, so the copy overlaps the chroma
-  // prefilter instead of queueing behind it; hsync waits on ev_ll.
+  // Line location: its own high-priority stream, so the field kernels run
+  // beside the chroma prefilter; hsync waits on ev_ll.  ev_win marks the
+  // field windows (the host reads the field count and offsets after it).
   cudaStream_t lstream = nullptr;
-  cudaEvent_t ev_ll = nullptr;
+  cudaEvent_t ev_ll = nullptr, ev_win = nullptr, ev_winhost = nullptr;
   uint8_t* d_raw_set[2] = {};
   uint16_t* d_luma_set[2] = {};
   uint16_t* d_chroma_set[2] = {};
@@ -109,7 +94,6 @@ struct Context {
   std::vector<void*> host_allocations;
   cudaEvent_t ev_host = nullptr;
   int last_fields = 0;
-  static constexpr int kEdgeGuessPerField = 2048;  // edges per field copied speculatively
 
   uint8_t* d_raw = nullptr;
   float *d_dem = nullptr, *d_env = nullptr, *d_video = nullptr, *d_sync = nullptr;
@@ -125,6 +109,18 @@ struct Context {
   int *d_do_count = nullptr, *d_do_lines = nullptr, *d_do_starts = nullptr, *d_do_ends = nullptr;
   unsigned char* d_do_cls = nullptr;
   double* d_col_frac = nullptr;
+  // line location (kernels_linelocs.cu)
+  WindowInfo* d_win = nullptr;
+  long long* d_offs = nullptr;
+  int* d_cand = nullptr;
+  int *d_ps = nullptr, *d_pl = nullptr, *d_pn = nullptr;
+  int *d_vs = nullptr, *d_vl = nullptr, *d_vn = nullptr;
+  unsigned char* d_vt = nullptr;
+  double* d_vd = nullptr;
+  FieldPrep* d_prep = nullptr;
+  LineLocState* d_lls = nullptr;
+  int* d_is_first = nullptr;
+  int *d_dbg_vs = nullptr, *d_dbg_vl = nullptr, *d_dbg_vt = nullptr, *d_dbg_vn = nullptr;
   // guard band of the sync threshold (kernels_guard.cu)
   double *d_ga64 = nullptr, *d_hs64 = nullptr;
   unsigned* d_guard_list = nullptr;
@@ -138,8 +134,7 @@ struct Context {
   float2 *d_twa_inv = nullptr, *d_twb_inv = nullptr, *d_twc_inv = nullptr, *d_twl_inv = nullptr;
   float* d_gc = nullptr;
 
-  // carried state
-  LineLocState lls;
+  // carried state (the line-location part lives on the device, d_lls)
   bool chroma_valid = false;
   int chroma_track = 0;
   double chroma_threshold = 0.0;
@@ -147,16 +142,12 @@ struct Context {
   bool last_parity = true;
 
   // host scratch (kept to avoid reallocation)
-  std::vector<unsigned> h_fall, h_rise;
-  std::vector<long long> run_start, run_end;
-  FieldWindows win;
-  std::vector<int> h_is_first, h_phase, computed_track;
-  std::vector<LinePrep> preps;
-  std::unique_ptr<WorkPool> pool;
+  std::vector<int> h_phase, computed_track;
   // pinned staging
   int* hp_counts = nullptr;
-  unsigned *hp_fall = nullptr, *hp_rise = nullptr;
-  double* hp_ll = nullptr;
+  WindowInfo* hp_win = nullptr;
+  long long* hp_offs = nullptr;
+  int* hp_is_first = nullptr;
   int *hp_track = nullptr, *hp_trial = nullptr;
   float* hp_burst = nullptr;
   double* hp_metric = nullptr;  // mapped: the metric kernel writes it directly
@@ -194,8 +185,10 @@ struct Context {
   std::vector<cudaEvent_t> event_pool;
   size_t pool_used = 0;
   cudaEvent_t next_event();
-  void begin_stage(int stage, cudaEvent_t& a);
-  void end_stage(int stage, cudaEvent_t a, int kernels = 1);
+  void begin_stage(int stage, cudaEvent_t& a) { begin_stage_on(stage, a, stream); }
+  void end_stage(int stage, cudaEvent_t a, int kernels = 1) { end_stage_on(stage, a, stream, kernels); }
+  void begin_stage_on(int stage, cudaEvent_t& a, cudaStream_t st);
+  void end_stage_on(int stage, cudaEvent_t a, cudaStream_t st, int kernels = 1);
   void collect_stage_times();
   double host_clock() const;
   void host_phase(int stage, double t0) {
@@ -232,8 +225,15 @@ struct Context {
   // `conceal`, fields are concealed as they are decoded; with dst_chroma (page
   // -locked host planes), sent there on the copy stream as well.
   bool chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal = nullptr, uint16_t* dst_chroma = nullptr);
-  // Sync edges of `sync` over [0, total) into h_fall / h_rise (synchronous).
-  bool read_edges(const float* sync, long long total);
+  // Sync edges of `sync` over [0, total) and the field windows clustered
+  // from them (at most num_fields), read back into hp_win / hp_offs
+  // (synchronous).
+  bool field_windows(const float* sync, long long total, int tiles, int num_fields);
+  // Line-location kernel arguments for the current chunk.
+  LineLocArgs lineloc_args(int tiles, int num_fields, long long raw_offset) const;
+  // The device line-location state (d_lls) to and from the host.
+  bool read_lls(LineLocState& st);
+  bool write_lls(const LineLocState& st);
   // False (with the error set) when a chunk listed more near-threshold sync
   // samples than the guard's capacity.
   bool guard_ok(int listed);

@@ -85,14 +85,29 @@ cuvhs_status cuvhs_stage_discover_vsyncs(cuvhs_ctx* ctx, const float* d_sync, in
   if (!enter(c, tiles, "tiles")) return c.status;
   if (max_fields < 1) return bad(c, "max_fields must be positive");
   const long long total = (long long)tiles * c.spp;
-  if (!c.read_edges(d_sync, total)) return c.status;
-  cuvhs::edge_runs(c.h_fall, c.h_rise, total, c.run_start, c.run_end);
-  cuvhs::field_windows(c.fmt, c.run_start, c.run_end, tiles, std::min(max_fields, c.batch), c.win);
-  *n_fields = (int)c.win.offs.size();
-  for (size_t i = 0; i < c.win.offs.size(); i++) field_offsets[i] = (int64_t)c.win.offs[i];
-  if (next_offset) *next_offset = (int64_t)c.win.next_rel;
+  const int nf = std::min(max_fields, c.batch);
+  if (!c.field_windows(d_sync, total, tiles, nf)) return c.status;
+  *n_fields = c.hp_win->fields;
+  for (int i = 0; i < c.hp_win->fields; i++) field_offsets[i] = (int64_t)c.hp_offs[i];
+  if (next_offset) *next_offset = (int64_t)c.hp_win->next_rel;
   return CUVHS_OK;
 }
+
+namespace {
+
+// The field windows of a stage call on the device: n windows at the given
+// chunk offsets.
+bool upload_windows(Context& c, const int64_t* field_offsets, int n) {
+  cuvhs::WindowInfo w;
+  w.fields = n;
+  for (int f = 0; f < n; f++) c.hp_offs[f] = (long long)field_offsets[f];
+  *c.hp_win = w;
+  cudaMemcpyAsync(c.d_win, c.hp_win, sizeof(w), cudaMemcpyHostToDevice, c.stream);
+  if (n) cudaMemcpyAsync(c.d_offs, c.hp_offs, (size_t)n * sizeof(long long), cudaMemcpyHostToDevice, c.stream);
+  return c.check_cuda("window upload");
+}
+
+}  // namespace
 
 // sync_pulses (src/pipeline/sync_pulses.cu:10-82) over per-field windows.
 cuvhs_status cuvhs_stage_sync_pulses(cuvhs_ctx* ctx, const float* d_sync, int tiles, const int64_t* field_offsets,
@@ -101,24 +116,32 @@ cuvhs_status cuvhs_stage_sync_pulses(cuvhs_ctx* ctx, const float* d_sync, int ti
   Context& c = ctx->c;
   if (!d_sync || !field_offsets || !starts || !lengths || !counts) return bad(c, "null buffer");
   if (!enter(c, tiles, "tiles")) return c.status;
-  if (n_fields < 0) return bad(c, "n_fields must not be negative");
+  if (n_fields < 0 || n_fields > c.batch) return bad(c, "n_fields must be in [0, batch_fields]");
   const long long total = (long long)tiles * c.spp;
   for (int f = 0; f < n_fields; f++)
     if (field_offsets[f] < 0 || field_offsets[f] >= total) return bad(c, "field offset outside the chunk");
-  if (!c.read_edges(d_sync, total)) return c.status;
-  cuvhs::edge_runs(c.h_fall, c.h_rise, total, c.run_start, c.run_end);
-  std::vector<int> ps, pl;
+  if (n_fields == 0) return CUVHS_OK;
+  if (!c.field_windows(d_sync, total, tiles, 1)) return c.status;  // the chunk's edge lists
+  if (!upload_windows(c, field_offsets, n_fields)) return c.status;
+  cuvhs::LineLocArgs la = c.lineloc_args(tiles, n_fields, 0);
+  la.total = total;
+  cuvhs::launch_field_pulses(la, c.stream);
+  std::vector<int32_t> ps((size_t)n_fields * cuvhs::kMaxPulses), pl(ps.size());
+  cudaMemcpyAsync(counts, c.d_pn, n_fields * sizeof(int), cudaMemcpyDeviceToHost, c.stream);
+  cudaMemcpyAsync(ps.data(), c.d_ps, ps.size() * sizeof(int), cudaMemcpyDeviceToHost, c.stream);
+  cudaMemcpyAsync(pl.data(), c.d_pl, pl.size() * sizeof(int), cudaMemcpyDeviceToHost, c.stream);
+  if (!c.check_cuda("sync_pulses") || !c.sync("sync_pulses")) return c.status;
   for (int f = 0; f < n_fields; f++) {
-    cuvhs::window_pulses(c.run_start, c.run_end, (long long)field_offsets[f], c.spp, ps, pl);
-    counts[f] = (int32_t)ps.size();
-    std::copy(ps.begin(), ps.end(), starts + (size_t)f * cuvhs::kMaxPulses);
-    std::copy(pl.begin(), pl.end(), lengths + (size_t)f * cuvhs::kMaxPulses);
+    const size_t o = (size_t)f * cuvhs::kMaxPulses;
+    std::copy(ps.begin() + o, ps.begin() + o + counts[f], starts + o);
+    std::copy(pl.begin() + o, pl.begin() + o + counts[f], lengths + o);
   }
   return CUVHS_OK;
 }
 
-// The host line locations of src/pipeline/pipeline.cu:1717-1778 ("K2b"), one
-// field at a time with the carried field-order state.
+// The host line locations of src/pipeline/pipeline.cu:1717-1778 ("K2b"), in
+// field order with the carried field-order state; or, with the single-pass
+// locator selected, src/pipeline/line_locs.cu:544-593 (no carried state).
 cuvhs_status cuvhs_stage_line_locations(cuvhs_ctx* ctx, uint64_t raw_offset, const int64_t* field_offsets,
                                         int n_fields, const int32_t* starts, const int32_t* lengths,
                                         const int32_t* counts, double* linelocs, int32_t* is_first_field) {
@@ -127,24 +150,25 @@ cuvhs_status cuvhs_stage_line_locations(cuvhs_ctx* ctx, uint64_t raw_offset, con
   if (!field_offsets || !starts || !lengths || !counts || !linelocs) return bad(c, "null buffer");
   c.status = CUVHS_OK;
   c.err.clear();
-  if (n_fields < 0) return bad(c, "n_fields must not be negative");
+  if (n_fields < 0 || n_fields > c.batch) return bad(c, "n_fields must be in [0, batch_fields]");
+  if (n_fields == 0) return CUVHS_OK;
+  cudaSetDevice(c.device);
   const int LPF = c.fmt.lines_per_frame;
-  const bool single = c.cfg.single_pass_lines != 0 || std::getenv("CUVHS_K2B_DISABLE") != nullptr;
-  cuvhs::FieldLines fl;
-  for (int f = 0; f < n_fields; f++) {
-    const int n = std::max(0, std::min<int>(counts[f], cuvhs::kMaxPulses));
-    const int* ps = starts + (size_t)f * cuvhs::kMaxPulses;
-    const int* pl = lengths + (size_t)f * cuvhs::kMaxPulses;
-    if (single) {  // line_locs (src/pipeline/line_locs.cu:544-593), no carried state
-      int parity = -1;
-      cuvhs::single_pass_lines(c.fmt, ps, pl, n, linelocs + (size_t)f * LPF, &parity);
-      if (is_first_field) is_first_field[f] = parity;
-      continue;
-    }
-    cuvhs::locate_lines(c.fmt, ps, pl, n, (long long)(raw_offset + (uint64_t)field_offsets[f]), c.lls, fl);
-    std::copy(fl.locs.begin(), fl.locs.begin() + LPF, linelocs + (size_t)f * LPF);
-    if (is_first_field) is_first_field[f] = fl.is_first;
-  }
+  c.single_pass = c.cfg.single_pass_lines != 0 || std::getenv("CUVHS_K2B_DISABLE") != nullptr;
+  std::vector<int32_t> pn(n_fields);
+  for (int f = 0; f < n_fields; f++) pn[f] = std::max(0, std::min<int>(counts[f], cuvhs::kMaxPulses));
+  const size_t np = (size_t)n_fields * cuvhs::kMaxPulses;
+  if (!upload_windows(c, field_offsets, n_fields)) return c.status;
+  cudaMemcpyAsync(c.d_ps, starts, np * sizeof(int), cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(c.d_pl, lengths, np * sizeof(int), cudaMemcpyHostToDevice, c.stream);
+  cudaMemcpyAsync(c.d_pn, pn.data(), n_fields * sizeof(int), cudaMemcpyHostToDevice, c.stream);
+  cuvhs::LineLocArgs la = c.lineloc_args(n_fields, n_fields, (long long)raw_offset);
+  cuvhs::launch_line_locations(la, c.stream);
+  std::vector<int32_t> first(n_fields);
+  cudaMemcpyAsync(linelocs, c.d_ll, (size_t)n_fields * LPF * sizeof(double), cudaMemcpyDeviceToHost, c.stream);
+  cudaMemcpyAsync(first.data(), c.d_is_first, n_fields * sizeof(int), cudaMemcpyDeviceToHost, c.stream);
+  if (!c.check_cuda("line_locations") || !c.sync("line_locations")) return c.status;
+  if (is_first_field) std::copy(first.begin(), first.end(), is_first_field);
   return CUVHS_OK;
 }
 

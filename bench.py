@@ -394,11 +394,20 @@ def run_stream(args, rank, world, local):
     fields = args.stream_fields
     kw = dict(sample_rate_hz=40e6, n_fields=fields, seed=5001 + rank, snr_db=36, jitter_bound=1.0,
               dropout_line_rate=0.002, headswitch_min=3, headswitch_max=8, speed_drift=0.002)
+    # generated front to back in 256 MiB pieces straight into page-locked
+    # memory (the whole capture is 2.4e10 samples at 36,000 fields)
     t_syn = time.perf_counter()
-    x = cv.synth_capture(**kw)
+    gen = cv.SynthStream(**kw)
+    x_pin = torch.empty(gen.length, dtype=torch.uint8, pin_memory=True)
+    xv = x_pin.numpy()
+    piece = 256 << 20
+    while gen.position < gen.length:
+        a = gen.position
+        got = gen.read_into(xv[a:a + piece])
+        if got <= 0:
+            raise RuntimeError("synthesizer stopped early")
+    gen.close()
     t_syn = time.perf_counter() - t_syn
-    x_pin = torch.from_numpy(x).pin_memory()
-    del x
     with cv.Decoder(40.0, device=local) as d:
         out, bufs = cv._lib.alloc_output(cv._lib.max_fields_for(x_pin.numel(), d.samples_per_field), pinned=True)
         from cuvhs_b200._lib import lib
@@ -550,7 +559,8 @@ def main():
                          "batched64: the 64-capture mixed batch through cuvhs_batch_decode; "
                          "stream40: one long 40 MHz capture streamed from pinned memory; "
                          "adjoint8: forward+backward passes of the calibration model")
-    ap.add_argument("--stream-fields", type=int, default=6000, help="stream40: fields in the capture")
+    ap.add_argument("--stream-fields", type=int, default=36000,
+                    help="stream40: fields in the capture (36,000: ten minutes at 40 MHz, 2.4e10 samples)")
     ap.add_argument("--lanes", type=int, default=0, help="batched64: concurrent decoders (0 = library default)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

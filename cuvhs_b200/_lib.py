@@ -173,6 +173,11 @@ lib.cuvhs_synth_length.argtypes = [ctypes.POINTER(SynthParams)]
 lib.cuvhs_synth_length.restype = ctypes.c_longlong
 lib.cuvhs_synth_ntsc.argtypes = [ctypes.POINTER(SynthParams), _vp, ctypes.c_longlong]
 lib.cuvhs_synth_ntsc.restype = ctypes.c_int
+lib.cuvhs_synth_open.argtypes = [ctypes.POINTER(SynthParams), ctypes.c_longlong]
+lib.cuvhs_synth_open.restype = _vp
+lib.cuvhs_synth_next.argtypes = [_vp, _vp, ctypes.c_longlong]
+lib.cuvhs_synth_next.restype = ctypes.c_longlong
+lib.cuvhs_synth_close.argtypes = [_vp]
 lib.cuvhs_synth_lines.argtypes = [ctypes.POINTER(SynthParams), ctypes.c_longlong, _vp, _vp, _vp, ctypes.c_longlong]
 lib.cuvhs_synth_lines.restype = ctypes.c_longlong
 lib.cuvhs_synth_preemphasis.argtypes = [ctypes.POINTER(SynthParams), _vp, _vp]
@@ -224,6 +229,7 @@ EXPORTED = [
     "cuvhs_adjoint_destroy", "cuvhs_adjoint_fields", "cuvhs_adjoint_default_params", "cuvhs_adjoint_set_target",
     "cuvhs_adjoint_fwd", "cuvhs_adjoint_bwd", "cuvhs_adjoint_array", "cuvhs_synth_default_params",
     "cuvhs_synth_length", "cuvhs_synth_ntsc", "cuvhs_synth_lines", "cuvhs_synth_preemphasis",
+    "cuvhs_synth_open", "cuvhs_synth_next", "cuvhs_synth_close",
     "cuvhs_decode_chunk_async", "cuvhs_flush", "cuvhs_ire0_hz", "cuvhs_pulse_threshold_hz", "cuvhs_get_state",
     "cuvhs_set_state", "cuvhs_stage_fm_demod",
     "cuvhs_stage_discover_vsyncs", "cuvhs_stage_sync_pulses", "cuvhs_stage_line_locations",
@@ -265,6 +271,37 @@ def synth_preemphasis(**kw):
     return b, a
 
 
+class SynthStream:
+    """A synthetic capture generated front to back in pieces (cuvhs_synth_open /
+    next / close): the pieces concatenate to synth_capture(**kw), with a few
+    tens of MB of working memory however long the capture is."""
+
+    def __init__(self, **kw):
+        self._p = synth_params(**kw)
+        self.length = int(lib.cuvhs_synth_length(ctypes.byref(self._p)))
+        self._h = lib.cuvhs_synth_open(ctypes.byref(self._p), self.length)
+        if not self._h:
+            raise CuvhsError(1, "cuvhs_synth_open failed")
+        self.position = 0
+
+    def read_into(self, out) -> int:
+        """Fill the writable u8 buffer `out` (numpy array or pointer-sized
+        object with .ctypes) with the next samples; returns how many."""
+        got = lib.cuvhs_synth_next(self._h, out.ctypes.data, out.size)
+        if got < 0:
+            raise CuvhsError(1, "cuvhs_synth_next failed")
+        self.position += int(got)
+        return int(got)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.cuvhs_synth_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
 def synth_capture(**kw) -> np.ndarray:
     """Seeded synthetic NTSC VHS RF capture (u8)."""
     p = synth_params(**kw)
@@ -302,7 +339,7 @@ def alloc_output(max_fields, pinned=False, shape=(FIELD_H, FIELD_W)):
     NTSC by default), page-locked when pinned."""
     if pinned:
         import torch
-        planes = [torch.empty((max_fields,) + tuple(shape), dtype=torch.int16).pin_memory() for _ in range(2)]
+        planes = [torch.empty((max_fields,) + tuple(shape), dtype=torch.int16, pin_memory=True) for _ in range(2)]
         luma, chroma = (p.numpy().view(np.uint16) for p in planes)
     else:
         planes = []

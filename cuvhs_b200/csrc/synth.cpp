@@ -392,128 +392,209 @@ extern "C" long long cuvhs_synth_length(const cuvhs_synth_params* p) {
   return (long long)std::floor(lines * spl);
 }
 
+// A capture generated front to back in units of kUnit samples: passes 1 and 3
+// of a unit run in parallel, pass 2 (the pre-emphasis filter and the FM phase,
+// both recursive) carries its state from unit to unit, so memory stays at a
+// few unit-sized buffers whatever the capture's length, and the bytes equal a
+// one-piece generation of the whole capture.
+struct cuvhs_synth_stream {
+  cuvhs_synth_params p;
+  Timing tm;
+  double fs = 0, spl = 0;
+  size_t n = 0, pos = 0;
+  int threads = 1;
+  long long lam0 = 0;
+  std::vector<double> r;
+  struct Span {
+    double a, b;
+  };
+  std::vector<Span> drops;
+  Content content;
+  double b[3], a[3];
+  double x1 = 0, x2 = 0, y1 = 0, y2 = 0, phase = 0;
+  double sigma = 0, peak = 0, amp_l = 1.0, amp_c = 0;
+  std::vector<float> ire, chroma;
+  std::vector<uint8_t> unit;  // the current unit's bytes
+  size_t unit_start = 0, unit_len = 0;
+  static constexpr size_t kBlock = 65536;  // noise blocks, seeded by their index
+  static constexpr size_t kUnit = kBlock * 64;
+
+  bool open(const cuvhs_synth_params* pp, size_t n_out) {
+    p = *pp;
+    tm = timing(p.system);
+    fs = p.sample_rate_hz;
+    spl = fs / tm.line_rate;
+    n = n_out;
+    threads = p.threads > 0 ? p.threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    line_table(&p, n, lam0, r);
+    const size_t n_lines = r.size() - 1;
+    // ---- dropouts: per-line seeded events, stored as RF sample spans
+    if (p.dropout_line_rate > 0) {
+      SplitMix dr(mix_seed(p.seed, 0xD0D0));
+      for (size_t k = 0; k < n_lines; k++) {
+        if (dr.uniform() < p.dropout_line_rate) {
+          int span = std::max(0, p.dropout_max - p.dropout_min);
+          int len = p.dropout_min + (int)(dr.uniform() * (span + 1));
+          double pos0 = r[k] + dr.uniform() * (r[k + 1] - r[k]);
+          drops.push_back({pos0, pos0 + len});
+        }
+      }
+    }
+    content.tm = tm;
+    content.spl = spl;
+    content.fs = fs;
+    content.us = fs * 1e-6;
+    make_bars(content.bars);
+    preemphasis(&p, b, a);
+    amp_c = p.chroma_level / 40.0;  // chroma components are in IRE (burst 20)
+    const double sig_rms = amp_l / std::sqrt(2.0);
+    sigma = sig_rms / std::pow(10.0, p.snr_db / 20.0);
+    peak = amp_l + 2.5 * p.chroma_level;
+    return true;
+  }
+
+  // Samples [i0, i0 + len) into out (i0 a multiple of kBlock).
+  void generate(size_t i0, size_t len, uint8_t* out) {
+    ire.resize(len);
+    chroma.resize(len);
+    // ---- pass 1 (parallel): program-time content per RF sample
+    parallel_for(len, threads, [&](size_t aa, size_t bb) {
+      const size_t ga = i0 + aa;
+      size_t k = (size_t)(std::upper_bound(r.begin(), r.end(), (double)ga) - r.begin());
+      if (k > 0) k--;
+      for (size_t j = aa; j < bb; j++) {
+        const size_t i = i0 + j;
+        while (k + 1 < r.size() && r[k + 1] <= (double)i) k++;
+        double lenk = r[k + 1] - r[k];
+        double u = ((double)i - r[k]) * (spl / lenk);
+        long long lam = lam0 + (long long)k;
+        double y, cu, cv;
+        // picture timebase: the delay runs linearly from this line's offset at
+        // its start to the next line's at its end
+        const double d0 = line_offset(&p, lam), d1 = line_offset(&p, lam + 1);
+        const double du = d0 + (u / spl) * (d1 - d0);
+        content.eval(lam, u, du, &y, &cu, &cv);
+        ire[j] = (float)y;
+        // colour-under: rotation by +/-90 degrees per line, alternating by field track
+        const int FL = tm.frame_lines;
+        long long fl = lam % FL;
+        bool field2 = (2 * fl + (u >= spl * 0.5 ? 1 : 0)) >= FL;
+        long long field_index = (lam / FL) * 2 + (field2 ? 1 : 0);
+        long long field_line = field2 ? fl - (FL - 1) / 2 : fl;
+        int track = (int)((field_index + p.first_track) & 1);
+        int rot = track ? 1 : 3;
+        int q = (int)(((field_line * rot) % 4 + 4) % 4);
+        // the picture delay moves the colour-under carrier with the picture
+        double theta = 2.0 * kPi * std::fmod(tm.chroma_under * ((double)i - du) / fs, 1.0) + q * (kPi * 0.5) +
+                       line_phase(&p, lam);
+        chroma[j] = (float)(cu * std::sin(theta) + cv * std::cos(theta));
+      }
+    });
+    // ---- pass 2 (sequential, state carried): pre-emphasis IIR on the IRE signal, then FM phase
+    {
+      if (i0 == 0) {
+        x1 = x2 = ire[0];
+        y1 = y2 = ire[0];  // the shelf's DC gain is 1
+        phase = 0.0;
+      }
+      const double dev = p.deviation_scale * tm.hz_ire;
+      const double fc = tm.ire0 + p.carrier_offset_hz;
+      for (size_t j = 0; j < len; j++) {
+        double x0 = ire[j];
+        double y0 = b[0] * x0 + b[1] * x1 + b[2] * x2 - a[1] * y1 - a[2] * y2;
+        x2 = x1;
+        x1 = x0;
+        y2 = y1;
+        y1 = y0;
+        double f = fc + dev * y0;
+        phase += 2.0 * kPi * f / fs;
+        if (phase > 2.0 * kPi) phase -= 2.0 * kPi * std::floor(phase / (2.0 * kPi));
+        ire[j] = (float)phase;  // reuse the buffer for the carrier phase
+      }
+    }
+    // ---- pass 3 (parallel): RF = luma carrier + colour-under, dropouts, noise, u8
+    const size_t b0 = i0 / kBlock, n_blocks = (len + kBlock - 1) / kBlock;
+    parallel_for(n_blocks, threads, [&](size_t ba, size_t bb) {
+      size_t di = 0;
+      for (size_t lb = ba; lb < bb; lb++) {
+        const size_t blk = b0 + lb;
+        SplitMix nr(mix_seed(p.seed, 0xA0000000ull + blk));
+        size_t g0 = blk * kBlock, g1 = std::min(i0 + len, g0 + kBlock);
+        if (!drops.empty()) {
+          di = (size_t)(std::upper_bound(drops.begin(), drops.end(), (double)g0,
+                                         [](double v, const Span& sp) { return v < sp.b; }) - drops.begin());
+        }
+        for (size_t i = g0; i < g1; i++) {
+          double rf = amp_l * std::cos((double)ire[i - i0]) + amp_c * (double)chroma[i - i0];
+          if (!drops.empty()) {
+            while (di < drops.size() && drops[di].b <= (double)i) di++;
+            if (di < drops.size() && drops[di].a <= (double)i && (double)i < drops[di].b) rf *= 0.03;
+          }
+          rf += sigma * nr.gauss();
+          double qv = std::nearbyint(128.0 + 100.0 * rf / peak);
+          if (qv < 0) qv = 0;
+          if (qv > 255) qv = 255;
+          out[i - i0] = (uint8_t)qv;
+        }
+      }
+    });
+  }
+
+  // The next `count` samples of the capture.
+  size_t next(uint8_t* out, size_t count) {
+    size_t done = 0;
+    while (done < count && pos < n) {
+      if (pos >= unit_start + unit_len) {  // the next unit
+        unit_start = pos;
+        unit_len = std::min(kUnit, n - pos);
+        if (unit_len == kUnit && done + kUnit <= count) {  // straight into the caller's buffer
+          generate(unit_start, unit_len, out + done);
+          pos += unit_len;
+          done += unit_len;
+          continue;
+        }
+        unit.resize(unit_len);
+        generate(unit_start, unit_len, unit.data());
+      }
+      const size_t take = std::min(count - done, unit_start + unit_len - pos);
+      std::memcpy(out + done, unit.data() + (pos - unit_start), take);
+      pos += take;
+      done += take;
+    }
+    return done;
+  }
+};
+
+namespace {
+bool valid_params(const cuvhs_synth_params* p) {
+  return p && p->sample_rate_hz > 4e6 && (p->system == 0 || p->system == 1);
+}
+}  // namespace
+
+extern "C" cuvhs_synth_stream* cuvhs_synth_open(const cuvhs_synth_params* p, long long n_out) {
+  if (!valid_params(p) || n_out <= 0) return nullptr;
+  cuvhs_synth_stream* s = new (std::nothrow) cuvhs_synth_stream();
+  if (!s) return nullptr;
+  s->open(p, (size_t)n_out);
+  return s;
+}
+
+extern "C" long long cuvhs_synth_next(cuvhs_synth_stream* s, uint8_t* out, long long count) {
+  if (!s || !out || count < 0) return -1;
+  return (long long)s->next(out, (size_t)count);
+}
+
+extern "C" void cuvhs_synth_close(cuvhs_synth_stream* s) { delete s; }
+
 extern "C" int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long long n_out) {
   if (!p || !out || n_out <= 0) return -1;
   if (!(p->sample_rate_hz > 4e6)) return -2;
   if (p->system != 0 && p->system != 1) return -3;
-  const Timing tm = timing(p->system);
-  const double fs = p->sample_rate_hz;
-  const double spl = fs / tm.line_rate;
-  const size_t n = (size_t)n_out;
-  int threads = p->threads > 0 ? p->threads : (int)std::max(1u, std::thread::hardware_concurrency());
-
-  long long lam0 = 0;
-  std::vector<double> r;
-  line_table(p, n, lam0, r);
-  const size_t n_lines = r.size() - 1;
-
-  // ---- dropouts: per-line seeded events, stored as RF sample spans
-  struct Span { double a, b; };
-  std::vector<Span> drops;
-  if (p->dropout_line_rate > 0) {
-    SplitMix dr(mix_seed(p->seed, 0xD0D0));
-    for (size_t k = 0; k < n_lines; k++) {
-      if (dr.uniform() < p->dropout_line_rate) {
-        int span = std::max(0, p->dropout_max - p->dropout_min);
-        int len = p->dropout_min + (int)(dr.uniform() * (span + 1));
-        double pos = r[k] + dr.uniform() * (r[k + 1] - r[k]);
-        drops.push_back({pos, pos + len});
-      }
-    }
-  }
-
-  Content content;
-  content.tm = tm;
-  content.spl = spl;
-  content.fs = fs;
-  content.us = fs * 1e-6;
-  make_bars(content.bars);
-
-  // ---- pass 1 (parallel): program-time content per RF sample
-  std::vector<float> ire(n), chroma(n);
-  parallel_for(n, threads, [&](size_t a, size_t b) {
-    size_t k = (size_t)(std::upper_bound(r.begin(), r.end(), (double)a) - r.begin());
-    if (k > 0) k--;
-    for (size_t i = a; i < b; i++) {
-      while (k + 1 < r.size() && r[k + 1] <= (double)i) k++;
-      double len = r[k + 1] - r[k];
-      double u = ((double)i - r[k]) * (spl / len);
-      long long lam = lam0 + (long long)k;
-      double y, cu, cv;
-      // picture timebase: the delay runs linearly from this line's offset at
-      // its start to the next line's at its end
-      const double d0 = line_offset(p, lam), d1 = line_offset(p, lam + 1);
-      const double du = d0 + (u / spl) * (d1 - d0);
-      content.eval(lam, u, du, &y, &cu, &cv);
-      ire[i] = (float)y;
-      // colour-under: rotation by +/-90 degrees per line, alternating by field track
-      const int FL = tm.frame_lines;
-      long long fl = lam % FL;
-      bool field2 = (2 * fl + (u >= spl * 0.5 ? 1 : 0)) >= FL;
-      long long field_index = (lam / FL) * 2 + (field2 ? 1 : 0);
-      long long field_line = field2 ? fl - (FL - 1) / 2 : fl;
-      int track = (int)((field_index + p->first_track) & 1);
-      int rot = track ? 1 : 3;
-      int q = (int)(((field_line * rot) % 4 + 4) % 4);
-      // the picture delay moves the colour-under carrier with the picture
-      double theta = 2.0 * kPi * std::fmod(tm.chroma_under * ((double)i - du) / fs, 1.0) + q * (kPi * 0.5) +
-                     line_phase(p, lam);
-      chroma[i] = (float)(cu * std::sin(theta) + cv * std::cos(theta));
-    }
-  });
-
-  // ---- pass 2 (sequential): pre-emphasis IIR on the IRE signal, then FM phase
-  double b[3], a[3];
-  preemphasis(p, b, a);
-  {
-    double x1 = ire[0], x2 = ire[0];
-    double y1 = ire[0], y2 = ire[0];  // the shelf's DC gain is 1
-    double phase = 0.0;
-    const double dev = p->deviation_scale * tm.hz_ire;
-    const double fc = tm.ire0 + p->carrier_offset_hz;
-    for (size_t i = 0; i < n; i++) {
-      double x0 = ire[i];
-      double y0 = b[0] * x0 + b[1] * x1 + b[2] * x2 - a[1] * y1 - a[2] * y2;
-      x2 = x1; x1 = x0; y2 = y1; y1 = y0;
-      double f = fc + dev * y0;
-      phase += 2.0 * kPi * f / fs;
-      if (phase > 2.0 * kPi) phase -= 2.0 * kPi * std::floor(phase / (2.0 * kPi));
-      ire[i] = (float)phase;  // reuse the buffer for the carrier phase
-    }
-  }
-
-  // ---- pass 3 (parallel): RF = luma carrier + colour-under, dropouts, noise, u8
-  const double amp_l = 1.0;
-  const double amp_c = p->chroma_level / 40.0;  // chroma components are in IRE (burst 20)
-  const double sig_rms = amp_l / std::sqrt(2.0);
-  const double sigma = sig_rms / std::pow(10.0, p->snr_db / 20.0);
-  const double peak = amp_l + 2.5 * p->chroma_level;
-  const size_t kBlock = 65536;
-  size_t n_blocks = (n + kBlock - 1) / kBlock;
-  parallel_for(n_blocks, threads, [&](size_t ba, size_t bb) {
-    size_t di = 0;
-    for (size_t blk = ba; blk < bb; blk++) {
-      SplitMix nr(mix_seed(p->seed, 0xA0000000ull + blk));
-      size_t i0 = blk * kBlock, i1 = std::min(n, i0 + kBlock);
-      if (!drops.empty()) {
-        di = (size_t)(std::upper_bound(drops.begin(), drops.end(), (double)i0,
-                                       [](double v, const Span& s) { return v < s.b; }) - drops.begin());
-      }
-      for (size_t i = i0; i < i1; i++) {
-        double rf = amp_l * std::cos((double)ire[i]) + amp_c * (double)chroma[i];
-        if (!drops.empty()) {
-          while (di < drops.size() && drops[di].b <= (double)i) di++;
-          if (di < drops.size() && drops[di].a <= (double)i && (double)i < drops[di].b) rf *= 0.03;
-        }
-        rf += sigma * nr.gauss();
-        double q = std::nearbyint(128.0 + 100.0 * rf / peak);
-        if (q < 0) q = 0;
-        if (q > 255) q = 255;
-        out[i] = (uint8_t)q;
-      }
-    }
-  });
-  return 0;
+  cuvhs_synth_stream* s = cuvhs_synth_open(p, n_out);
+  if (!s) return -4;
+  const long long got = cuvhs_synth_next(s, out, n_out);
+  cuvhs_synth_close(s);
+  return got == n_out ? 0 : -5;
 }
 
 extern "C" long long cuvhs_synth_lines(const cuvhs_synth_params* p, long long n, double* start, double* offset,

@@ -25,6 +25,9 @@ WORKLOADS = {
                           dropout_line_rate=0.01, headswitch_min=3, headswitch_max=8, system=1),
     # PAL at 40 MHz, 20 fields
     "pal20_40": dict(sample_rate_hz=40e6, n_fields=20, seed=47, snr_db=38, jitter_bound=1.0, system=1),
+    # long-stream sample: 300 fields at 40 MHz with +/-0.2% tape-speed drift, 0.2% dropout lines, head switch
+    "drift300_40": dict(sample_rate_hz=40e6, n_fields=300, seed=5003, snr_db=36, jitter_bound=1.0,
+                        dropout_line_rate=0.002, headswitch_min=3, headswitch_max=8, speed_drift=0.002),
     # adversarial: the FM carrier raised by 20 IRE + 1 Hz, so the sync tip sits 1 Hz above the pulse
     # threshold and noise puts thousands of sync samples within a few Hz of it
     "tipthr28": dict(sample_rate_hz=28e6, n_fields=6, seed=53, snr_db=40, jitter_bound=0.5,

@@ -46,6 +46,15 @@ void cuvhs_synth_default_params(cuvhs_synth_params* p);
 long long cuvhs_synth_length(const cuvhs_synth_params* p);
 /* Fill out[0..n) with the capture; returns 0 on success. */
 int cuvhs_synth_ntsc(const cuvhs_synth_params* p, uint8_t* out, long long n);
+/* The same capture of n samples generated front to back in pieces of any
+ * size, with a few tens of MB of working memory however long the capture is
+ * (a 10-minute 40 MHz capture is 2.4e10 samples): cuvhs_synth_next writes the
+ * next `count` samples and returns how many it wrote (fewer at the end).
+ * The pieces concatenate to cuvhs_synth_ntsc's bytes. */
+typedef struct cuvhs_synth_stream cuvhs_synth_stream;
+cuvhs_synth_stream* cuvhs_synth_open(const cuvhs_synth_params* p, long long n);
+long long cuvhs_synth_next(cuvhs_synth_stream* s, uint8_t* out, long long count);
+void cuvhs_synth_close(cuvhs_synth_stream* s);
 /* The program-line table of the capture: for up to cap lines, the RF sample
  * where each line starts, its picture delay at the line start (samples) and
  * its colour-under phase offset (radians).  Returns the number of lines. */

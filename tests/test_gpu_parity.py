@@ -138,6 +138,26 @@ def test_multi_chunk_matches_oracle_with_same_chunking():
 
 
 @pytest.mark.gpu
+def test_drifting_40mhz_stream_matches_oracle_over_chunks():
+    """A long-stream sample: 300 NTSC fields at 40 MHz u8 with +/-0.2% tape-speed
+    drift, dropouts on 0.2% of lines, head switching and +/-1 sample jitter,
+    decoded in 64-field chunks (the stream-mode chunk) from page-locked
+    memory; the oracle with the same chunking must agree on every field's
+    metadata, luma and chroma."""
+    from oracle.oracle import Oracle
+    x = workload("drift300_40")
+    with cv.Decoder(40.0, batch_fields=64, debug=True) as d:
+        r = d.decode_capture(x, pinned=True)
+    o = Oracle(40.0, batch_fields=64)
+    o.decode(x)
+    assert o.n_chunks >= 4
+    inside = compare_to_oracle("drift300_40", r, None, x, 40.0, o)
+    assert len(inside) >= 290
+    gaps = np.diff(r.file_loc.astype(np.int64))
+    assert (gaps.max() - gaps.min()) / gaps.mean() > 0.002  # the drift shows in the field spacing
+
+
+@pytest.mark.gpu
 def test_decode_is_deterministic_and_chunk_api_matches_capture_api():
     x = workload("dropouts28")
     with cv.Decoder(28.0) as d:

@@ -149,3 +149,24 @@ def test_synth_tool_rejects_unknown_parameters(tmp_path):
     tool = os.path.join(os.path.dirname(cv.CLI_PATH), "cuvhs-synth")
     r = subprocess.run([tool, "no_such_field=1", str(tmp_path / "x.u8")], capture_output=True, text=True)
     assert r.returncode == 2 and "bad parameter" in r.stderr
+
+
+def test_synth_stream_pieces_concatenate_to_the_capture():
+    """The chunked synthesizer (cuvhs_synth_open/next/close), read in ragged
+    pieces across several internal units, gives the one-piece capture's
+    bytes -- with drift, dropouts and head switching, whose state carries
+    across the pieces."""
+    kw = dict(sample_rate_hz=40e6, n_fields=16, seed=5001, snr_db=36, jitter_bound=1.0, dropout_line_rate=0.002,
+              headswitch_min=3, headswitch_max=8, speed_drift=0.002)
+    whole = cv.synth_capture(**kw)
+    s = cv.SynthStream(**kw)
+    assert s.length == whole.size
+    rng = np.random.default_rng(3)
+    parts = []
+    while s.position < s.length:
+        buf = np.empty(int(rng.integers(1, 3_000_000)), np.uint8)
+        got = s.read_into(buf)
+        assert got > 0
+        parts.append(buf[:got])
+    s.close()
+    assert np.array_equal(np.concatenate(parts), whole)

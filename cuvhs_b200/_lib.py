@@ -41,7 +41,8 @@ class CuvhsError(RuntimeError):
 class Config(ctypes.Structure):
     _fields_ = [("system", ctypes.c_int), ("sample_rate_mhz", ctypes.c_double), ("device", ctypes.c_int),
                 ("batch_fields", ctypes.c_int), ("stream_mode", ctypes.c_int), ("input_format", ctypes.c_int),
-                ("dc_correct", ctypes.c_int), ("single_pass_lines", ctypes.c_int), ("guard_band_hz", ctypes.c_double)]
+                ("dc_correct", ctypes.c_int), ("single_pass_lines", ctypes.c_int), ("guard_band_hz", ctypes.c_double),
+                ("device_memory_limit_mb", ctypes.c_double)]
 
 
 class FieldInfo(ctypes.Structure):
@@ -390,10 +391,12 @@ class Decoder:
     SYSTEMS = {"NTSC": 0, "PAL": 1}
 
     def __init__(self, sample_rate_mhz=28.0, device=0, batch_fields=0, stream_mode=False, debug=False,
-                 input_format="u8", dc_correct=False, system="NTSC", single_pass_lines=False, guard_band_hz=0.0):
+                 input_format="u8", dc_correct=False, system="NTSC", single_pass_lines=False, guard_band_hz=0.0,
+                 device_memory_limit_mb=0.0):
         cfg = Config()
         lib.cuvhs_default_config(ctypes.byref(cfg))
         cfg.guard_band_hz = float(guard_band_hz)
+        cfg.device_memory_limit_mb = float(device_memory_limit_mb)
         cfg.system = self.SYSTEMS[system.upper()]
         cfg.single_pass_lines = 1 if single_pass_lines else 0
         cfg.sample_rate_mhz = float(sample_rate_mhz)

@@ -142,6 +142,7 @@ void cuvhs_default_config(cuvhs_config* cfg) {
   cfg->dc_correct = 0;
   cfg->single_pass_lines = 0;
   cfg->guard_band_hz = 0.0;
+  cfg->device_memory_limit_mb = 0.0;
 }
 
 const char* cuvhs_status_string(cuvhs_status s) {

@@ -20,8 +20,12 @@
 // the demodulated range (src/pipeline/fm_demod.cu:133-169, 396-485).
 //
 // Work: one flagged sample is split over `parts` CTAs, each CTA evaluating 256
-// of the 2*hb + 1 demod samples of the sync window (two FP64 analytic-signal
-// dot products of 2*ha + 1 taps each per demod sample).  Each CTA writes its
+// of the 2*hb + 1 demod samples of the sync window.  Where those positions
+// lie inside one tile away from its wrap and the chunk ends (nearly always),
+// the CTA stages their raw window once in shared memory as FP64 and computes
+// each analytic-signal value once (one FP64 dot product of 2*ha + 1 taps per
+// position); elsewhere each thread evaluates its position with the tile wrap
+// and chunk clamp (two dot products).  Each CTA writes its
 // partial sum; the CTA that finishes a sample last (an atomic count, no
 // waiting) adds the partials in part order, so the result is deterministic.
 #include <cuda_runtime.h>
@@ -51,18 +55,80 @@ __device__ __forceinline__ double raw64(const GuardArgs& g, long long p, double 
   return (double)raw_convert<FMT>(g.raw, (int)p) - dc;
 }
 
+// z(J) of tile f2 at tile positions J for the kGuardThreads demod positions
+// of one CTA, when they are consecutive inside one tile and their raw windows
+// need no wrap, clamp or zero fill: the raw window is staged once as FP64
+// (converted, DC removed) and each analytic-signal value is computed once.
+// Returns false (nothing written) when the CTA's positions are not of that
+// kind; the caller then evaluates every position on its own.
+struct GuardSmem {
+  double2* taps;  // [2*ha + 3]
+  double* xs;     // [kGuardThreads + 2*ha + 2] staged raw
+  double2* z;     // [kGuardThreads + 1]
+};
+
+template <int FMT>
+__device__ bool stage_interior(const GuardArgs& g, const GuardSmem& sm, long long c_first, int count, double dc) {
+  // positions c_first, c_first - 1, ..., c_first - count + 1 and one more for z(J2 - 1)
+  const long long c_last = c_first - count;  // the extra position (z only)
+  const long long last = g.total - 1;
+  if (c_last < 0) return false;
+  const long long f2 = c_first / g.spp;
+  if (c_last / g.spp != f2 || c_last - f2 * g.spp < 0) return false;
+  const long long tile0 = f2 * g.spp - kOverlap;
+  const long long J_hi = c_first - tile0, J_lo = c_last - tile0;  // tile positions
+  const long long u_lo = J_lo - g.ha, u_hi = J_hi + g.ha;
+  if (u_lo < 0 || u_hi >= g.tile || tile0 + u_lo < 0 || tile0 + u_hi > last || tile0 + u_hi >= g.n_read)
+    return false;
+  const int nx = (int)(u_hi - u_lo + 1);
+  for (int i = threadIdx.x; i < nx; i += kGuardThreads)
+    sm.xs[i] = (double)raw_convert<FMT>(g.raw, (int)(tile0 + u_lo + i)) - dc;
+  __syncthreads();
+  // thread t: z at tile position J_hi - t; z(J) = sum_m g[m] x(J - m)
+  const int t = threadIdx.x;
+  auto zdot = [&](long long J, int m0, int m1) {
+    double2 acc = make_double2(0.0, 0.0);
+    const double* xp = sm.xs + (J - u_lo);
+    for (int m = m0; m < m1; m++) {
+      const double2 a = sm.taps[m + g.ha + 1];
+      const double x = xp[-m];
+      acc.x = fma(a.x, x, acc.x);
+      acc.y = fma(a.y, x, acc.y);
+    }
+    return acc;
+  };
+  if (t < count) sm.z[t] = zdot(J_hi - t, -g.ha, g.ha + 1);
+  // the extra position, split over the first warp
+  if (t < 32) {
+    const int per = (2 * g.ha + 1 + 31) / 32;
+    const int m0 = -g.ha + t * per, m1 = min(m0 + per, g.ha + 1);
+    double2 acc = m0 < m1 ? zdot(J_lo, m0, m1) : make_double2(0.0, 0.0);
+    for (int off = 16; off > 0; off >>= 1) {
+      acc.x += __shfl_down_sync(0xffffffffu, acc.x, off);
+      acc.y += __shfl_down_sync(0xffffffffu, acc.y, off);
+    }
+    if (t == 0) sm.z[count] = acc;
+  }
+  __syncthreads();
+  return true;
+}
+
 template <int FMT>
 __global__ void __launch_bounds__(kGuardThreads) guard_kernel(GuardArgs g) {
   chain_wait();
-  extern __shared__ double2 taps[];  // [2*ha + 3]: 0, g[-ha..ha], 0
+  extern __shared__ double2 smem2[];
   __shared__ double red[kGuardThreads / 32];
   const int n_listed = min(*g.count, g.cap);
   if ((int)blockIdx.y >= n_listed) return;  // whole CTA
   const int t = threadIdx.x, part = blockIdx.x;
   const int nt = 2 * g.ha + 3;
+  GuardSmem sm;
+  sm.taps = smem2;
+  sm.z = smem2 + nt;
+  sm.xs = reinterpret_cast<double*>(smem2 + nt + kGuardThreads + 1);
   for (int i = t; i < nt; i += kGuardThreads)
-    taps[i] = (i == 0 || i == nt - 1) ? make_double2(0.0, 0.0)
-                                      : make_double2(g.ga64[2 * (i - 1)], g.ga64[2 * (i - 1) + 1]);
+    sm.taps[i] = (i == 0 || i == nt - 1) ? make_double2(0.0, 0.0)
+                                         : make_double2(g.ga64[2 * (i - 1)], g.ga64[2 * (i - 1) + 1]);
   __syncthreads();
   const double dc = g.dc ? (double)*g.dc : 0.0;
   const int W = 2 * g.hb + 1;
@@ -71,42 +137,47 @@ __global__ void __launch_bounds__(kGuardThreads) guard_kernel(GuardArgs g) {
     const long long s = g.list[y];
     const long long f = s / g.spp;
     const long long J = kOverlap + (s - f * g.spp);
-    const int kk = part * kGuardThreads + t;
+    const int kk0 = part * kGuardThreads, kk = kk0 + t;
+    const int count = min(kGuardThreads, W - kk0);
+    // demod sample at tile position J - k of tile f (k = kk - hb), chunk position c
+    auto chunk_pos = [&](int k_index) {
+      const long long q = wrap_pos(J - (k_index - g.hb), g.tile);
+      return min(max(f * g.spp + q - kOverlap, 0LL), last);
+    };
+    // the CTA's positions are consecutive (decreasing) when neither the tile
+    // wrap nor the chunk clamp falls inside them
+    const long long q_first = J - (kk0 - g.hb), q_end = J - (kk0 + count - 1 - g.hb);
+    const bool consecutive = q_end >= 0 && q_first < g.tile && f * g.spp + q_end - kOverlap >= 0 &&
+                             f * g.spp + q_first - kOverlap <= last;
+    const long long c_first = chunk_pos(kk0);
     double contrib = 0.0;
-    if (kk < W) {
-      // demod sample at tile position J - k of tile f (k = kk - hb)
-      const long long q = wrap_pos(J - (kk - g.hb), g.tile);
-      const long long c = min(max(f * g.spp + q - kOverlap, 0LL), last);
+    if (consecutive && stage_interior<FMT>(g, sm, c_first, count, dc)) {
+      if (t < count) {
+        const double2 z0 = sm.z[t], z1 = sm.z[t + 1];
+        double d = atan2(z0.y, z0.x) - atan2(z1.y, z1.x);  // k_unwrap_to_hz (fm_demod.cu:222-244)
+        if (d > kPi64) d -= kTau64;
+        if (d < -kPi64) d += kTau64;
+        contrib = g.hs64[kk] * (d * g.scale);
+      }
+    } else if (kk < W) {
+      const long long c = chunk_pos(kk);
       const long long f2 = c / g.spp;
       const long long J2 = kOverlap + (c - f2 * g.spp);
       const long long tile0 = f2 * g.spp - kOverlap;  // chunk position of tile position 0
       // raw tile positions J2 + ha down to J2 - 1 - ha feed z(J2) and z(J2 - 1)
-      const long long u_hi = J2 + g.ha, u_lo = J2 - 1 - g.ha;
+      const long long u_hi = J2 + g.ha;
       double2 z0 = make_double2(0.0, 0.0), z1 = make_double2(0.0, 0.0);
       const int nu = 2 * g.ha + 2;
-      if (u_lo >= 0 && u_hi < g.tile && tile0 + u_lo >= 0 && tile0 + u_hi <= last && tile0 + u_hi < g.n_read) {
-        const long long p0 = tile0 + u_hi;  // interior: no wrap, no clamp, no zero fill
-#pragma unroll 4
-        for (int n = 0; n < nu; n++) {
-          const double x = (double)raw_convert<FMT>(g.raw, (int)(p0 - n)) - dc;
-          const double2 a = taps[n + 1], b = taps[n];
-          z0.x = fma(a.x, x, z0.x);
-          z0.y = fma(a.y, x, z0.y);
-          z1.x = fma(b.x, x, z1.x);
-          z1.y = fma(b.y, x, z1.y);
-        }
-      } else {
-        for (int n = 0; n < nu; n++) {
-          const long long p = min(max(tile0 + wrap_pos(u_hi - n, g.tile), 0LL), last);
-          const double x = raw64<FMT>(g, p, dc);
-          const double2 a = taps[n + 1], b = taps[n];
-          z0.x = fma(a.x, x, z0.x);
-          z0.y = fma(a.y, x, z0.y);
-          z1.x = fma(b.x, x, z1.x);
-          z1.y = fma(b.y, x, z1.y);
-        }
+      for (int n = 0; n < nu; n++) {
+        const long long p = min(max(tile0 + wrap_pos(u_hi - n, g.tile), 0LL), last);
+        const double x = raw64<FMT>(g, p, dc);
+        const double2 a = sm.taps[n + 1], b = sm.taps[n];
+        z0.x = fma(a.x, x, z0.x);
+        z0.y = fma(a.y, x, z0.y);
+        z1.x = fma(b.x, x, z1.x);
+        z1.y = fma(b.y, x, z1.y);
       }
-      double d = atan2(z0.y, z0.x) - atan2(z1.y, z1.x);  // k_unwrap_to_hz (fm_demod.cu:222-244)
+      double d = atan2(z0.y, z0.x) - atan2(z1.y, z1.x);
       if (d > kPi64) d -= kTau64;
       if (d < -kPi64) d += kTau64;
       contrib = g.hs64[kk] * (d * g.scale);
@@ -134,7 +205,7 @@ __global__ void __launch_bounds__(kGuardThreads) guard_kernel(GuardArgs g) {
         if (g.values) g.values[y] = x64;
       }
     }
-    __syncthreads();  // red is reused by the next sample
+    __syncthreads();  // red, z and xs are reused by the next sample
   }
 }
 
@@ -145,7 +216,8 @@ int guard_parts(int hb) { return (2 * hb + 1 + kGuardThreads - 1) / kGuardThread
 cudaError_t launch_sync_guard(const GuardArgs& g, cudaStream_t st) {
   const int parts = guard_parts(g.hb);
   if (parts > kGuardMaxParts || g.cap <= 0) return cudaErrorInvalidValue;
-  const size_t smem = (size_t)(2 * g.ha + 3) * sizeof(double2);
+  const size_t smem = (size_t)(2 * g.ha + 3 + kGuardThreads + 1) * sizeof(double2) +
+                      (size_t)(kGuardThreads + 2 * g.ha + 2) * sizeof(double);
   // enough rows to spread a typical chunk's few flagged samples over the GPU;
   // rows past the listed count leave at once
   const int rows = std::max(1, std::min(g.cap, (148 * 8 + parts - 1) / parts));

@@ -40,6 +40,7 @@ namespace {
 
 constexpr int kLT = 256;           // threads per line-location CTA
 constexpr int kSortMax = 4096;     // validated pulses sorted in shared memory
+constexpr int kSmemValid = 2048;   // validated pulses held in shared memory
 
 __device__ __forceinline__ bool within(double v, double lo, double hi) { return v >= lo && v <= hi; }
 
@@ -57,10 +58,11 @@ __device__ __forceinline__ int upper_idx(const unsigned* a, int n, unsigned v) {
 }
 
 // End of the threshold run that starts at falling edge i: the first rising
-// edge after it, or the range end (pipeline edge_runs).
-__device__ __forceinline__ long long run_end(const LineLocArgs& a, int nrise, unsigned fall) {
-  const int r = upper_idx(a.rise, nrise, fall);
-  return r < nrise ? (long long)a.rise[r] : a.total;
+// edge after it, or the range end.  Every sample is in or out of a pulse, so
+// in sample order the edges alternate, falling first (a pulse open at the
+// chunk's first sample falls there): rising edge i closes run i.
+__device__ __forceinline__ long long run_end(const LineLocArgs& a, int nrise, int i) {
+  return i < nrise ? (long long)a.rise[i] : a.total;
 }
 
 // One CTA: VSYNC candidates (runs of 20-35 us, vsync_discover.cu:58-72) in
@@ -68,36 +70,35 @@ __device__ __forceinline__ long long run_end(const LineLocArgs& a, int nrise, un
 __global__ void __launch_bounds__(1024) fieldwin_kernel(LineLocArgs a) {
   chain_wait();
   __shared__ int warp_tot[32];
-  __shared__ int base_s;
   const int nfall = min(a.counts[0], a.edge_cap), nrise = min(a.counts[1], a.edge_cap);
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  if (t == 0) {
-    base_s = 0;
-    a.win->err = (a.counts[0] > a.edge_cap || a.counts[1] > a.edge_cap) ? 1 : 0;
+  if (t == 0) a.win->err = (a.counts[0] > a.edge_cap || a.counts[1] > a.edge_cap) ? 1 : 0;
+  // each thread a contiguous strip of falling edges: count, scan, write in order
+  const int per = (nfall + 1023) / 1024;
+  const int i0 = min(nfall, t * per), i1 = min(nfall, i0 + per);
+  auto is_cand = [&](int i) {
+    const long long w = run_end(a, nrise, i) - (long long)a.fall[i];
+    return w >= a.minw && w <= a.maxw;
+  };
+  int cnt = 0;
+  for (int i = i0; i < i1; i++) cnt += is_cand(i) ? 1 : 0;
+  int incl = cnt;
+  for (int off = 1; off < 32; off <<= 1) {
+    const int o = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += o;
   }
+  if (lane == 31) warp_tot[warp] = incl;
   __syncthreads();
-  // ordered compaction of the candidates, 1024 edges at a time
-  for (int i0 = 0; i0 < nfall; i0 += 1024) {
-    const int i = i0 + t;
-    bool c = false;
-    if (i < nfall) {
-      const long long w = run_end(a, nrise, a.fall[i]) - (long long)a.fall[i];
-      c = w >= a.minw && w <= a.maxw;
-    }
-    const unsigned m = __ballot_sync(0xffffffffu, c);
-    if (lane == 0) warp_tot[warp] = __popc(m);
-    __syncthreads();
-    int before = 0, total = 0;
-    for (int w = 0; w < 32; w++) {
-      if (w < warp) before += warp_tot[w];
-      total += warp_tot[w];
-    }
-    const int k = base_s + before + __popc(m & ((1u << lane) - 1u));
-    if (c && k < a.cand_cap) a.cand[k] = (int)a.fall[i];
-    __syncthreads();
-    if (t == 0) base_s += total;
-    __syncthreads();
+  int before = 0, total = 0;
+  for (int w = 0; w < 32; w++) {
+    if (w < warp) before += warp_tot[w];
+    total += warp_tot[w];
   }
+  int k = before + incl - cnt;
+  for (int i = i0; i < i1 && k < a.cand_cap; i++)
+    if (is_cand(i)) a.cand[k++] = (int)a.fall[i];
+  __syncthreads();
+  const int base_s = total;
   if (t != 0) return;
   const int ncand = min(base_s, a.cand_cap);
   const long long spf = a.fmt.samples_per_field, spl = a.fmt.samples_per_line;
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(kLT) pulses_kernel(LineLocArgs a) {
   __syncthreads();
   for (int b = i0; b < i1 && b < brk; b += kLT) {
     const int i = b + threadIdx.x;
-    if (i < i1 && run_end(a, nrise, a.fall[i]) > lim) atomicMin(&brk, i);
+    if (i < i1 && run_end(a, nrise, i) > lim) atomicMin(&brk, i);
     __syncthreads();
   }
   const int n = min(brk - i0, kMaxPulses);
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(kLT) pulses_kernel(LineLocArgs a) {
   for (int k = threadIdx.x; k < n; k += kLT) {
     const unsigned s = a.fall[i0 + k];
     ps[k] = (int)s;
-    pl[k] = (int)(run_end(a, nrise, s) - (long long)s);
+    pl[k] = (int)(run_end(a, nrise, i0 + k) - (long long)s);
   }
   if (threadIdx.x == 0) a.pn[f] = max(n, 0);
 }
@@ -306,6 +307,10 @@ struct FieldSmem {
   double dsh[8];
   int ish[8];
   double sort[kSortMax];
+  // the validated list when it has at most kSmemValid entries (nearly always)
+  int vs[kSmemValid];
+  unsigned char vt[kSmemValid];
+  int nexth[kSmemValid];  // first non-hsync entry at or after each entry
 };
 
 // Pulse validation (pipeline.cu:611-648) into v; returns the entry count.
@@ -351,20 +356,64 @@ __device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
   }
   __syncthreads();
   // which attempts fire: at an EQ-width pulse while the list's last entry is
-  // an hsync; one O(1) step per pulse
-  if (t == 0) {
-    int total = 0, back = -1;  // -1: empty list
-    for (int i = 0; i < n; i++) {
-      sm.pos[i] = total;
-      if (sm.cls[i] & 1) {
-        total += 1;
-        back = kHsync;
-      } else if ((sm.cls[i] & 2) && back == kHsync && sm.att_ok[i]) {
-        total += sm.att_len[i];
-        back = sm.att_last[i];
+  // an hsync.  The list's state before pulse i -- empty, last entry an hsync,
+  // or last entry something else -- follows from pulse i-1's state by a map
+  // of the three states (an hsync pulse sets "hsync"; a firing attempt sets
+  // its last type; other pulses change nothing), so one warp scans the maps
+  // (composition is associative), each lane over a run of pulses, and every
+  // pulse's output length and position follow.
+  if (t < 32) {
+    const int lane = t;
+    const int per = (n + 31) / 32;
+    const int i0 = min(n, lane * per), i1 = min(n, i0 + per);
+    // map of pulse i: 2 bits per incoming state (0 empty, 1 hsync, 2 other)
+    auto pulse_map = [&](int i) -> unsigned {
+      if (sm.cls[i] & 1) return 1u | (1u << 2) | (1u << 4);  // every state -> hsync
+      if ((sm.cls[i] & 2) && sm.att_ok[i]) {
+        const unsigned after = sm.att_last[i] == kHsync ? 1u : 2u;
+        return 0u | (after << 2) | (2u << 4);  // fires only after an hsync
       }
+      return 0u | (1u << 2) | (2u << 4);  // identity
+    };
+    auto apply = [](unsigned m, unsigned st) { return (m >> (2 * st)) & 3u; };
+    auto compose = [&](unsigned first, unsigned then) {  // then(first(s))
+      unsigned r = 0;
+      for (unsigned st = 0; st < 3; st++) r |= apply(then, apply(first, st)) << (2 * st);
+      return r;
+    };
+    unsigned m = 0u | (1u << 2) | (2u << 4);
+    for (int i = i0; i < i1; i++) m = compose(m, pulse_map(i));
+    // exclusive scan of the lane maps in lane order
+    unsigned pre = m;
+    for (int off = 1; off < 32; off <<= 1) {
+      const unsigned o = __shfl_up_sync(0xffffffffu, pre, off);
+      if (lane >= off) pre = compose(o, pre);
     }
-    sm.pos[n] = total;
+    unsigned excl = __shfl_up_sync(0xffffffffu, pre, 1);
+    if (lane == 0) excl = 0u | (1u << 2) | (2u << 4);
+    // each pulse's output length with the state it meets, then their prefix
+    unsigned st = apply(excl, 0);  // the list starts empty
+    int len_sum = 0;
+    for (int i = i0; i < i1; i++) {
+      int len = 0;
+      if (sm.cls[i] & 1) len = 1;
+      else if ((sm.cls[i] & 2) && sm.att_ok[i] && st == 1) len = sm.att_len[i];
+      sm.pos[i] = len;
+      len_sum += len;
+      st = apply(pulse_map(i), st);
+    }
+    int incl = len_sum;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int o = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= off) incl += o;
+    }
+    int run = incl - len_sum;
+    for (int i = i0; i < i1; i++) {
+      const int len = sm.pos[i];
+      sm.pos[i] = run;
+      run += len;
+    }
+    if (lane == 31) sm.pos[n] = incl;
   }
   __syncthreads();
   const int nv = sm.pos[n];
@@ -402,13 +451,54 @@ __device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
 // first longest run; spacings within 5% of nominal, its last one excluded.
 __device__ double mean_line(FieldSmem& sm, const VList& v, double nominal) {
   const int t = threadIdx.x;
+  const bool in_smem = v.tg == sm.vt;
+  if (in_smem) {
+    // first non-hsync entry at or after each entry: a backward pass per
+    // contiguous strip, then the strips' minima carried from the right
+    __shared__ int strip_min[kLT];
+    const int per = (v.n + kLT - 1) / kLT;
+    const int k0 = min(v.n, t * per), k1 = min(v.n, k0 + per);
+    int cur = INT_MAX;
+    for (int k = k1 - 1; k >= k0; k--) {
+      if (vtype(v, k) != kHsync) cur = k;
+      sm.nexth[k] = cur;
+    }
+    strip_min[t] = cur;
+    __syncthreads();
+    if (t < 32) {  // suffix minimum over the strips, one warp
+      const int q = (kLT + 31) / 32, a0 = t * q;
+      int m = INT_MAX;
+      for (int j = a0 + q - 1; j >= a0; j--) m = min(m, strip_min[j]);
+      int suf = m;  // inclusive suffix minimum over lanes >= t
+      for (int off = 1; off < 32; off <<= 1) {
+        const int o = __shfl_down_sync(0xffffffffu, suf, off);
+        if (t + off < 32) suf = min(suf, o);
+      }
+      int carry = __shfl_down_sync(0xffffffffu, suf, 1);
+      if (t == 31) carry = INT_MAX;
+      for (int j = a0 + q - 1; j >= a0; j--) {
+        const int own = strip_min[j];
+        strip_min[j] = carry;  // minimum over the strips after j
+        carry = min(carry, own);
+      }
+    }
+    __syncthreads();
+    for (int k = k0; k < k1; k++)
+      if (sm.nexth[k] == INT_MAX) sm.nexth[k] = strip_min[t];
+    __syncthreads();
+  }
   // best run as (run_len << 32 | ~start): the largest run_len, then the first
   unsigned long long best = 0;
   bool any = false;
   for (int k = t; k < v.n; k += kLT) {
     if (vtype(v, k) != kHsync || (k > 0 && vtype(v, k - 1) == kHsync)) continue;
-    int e = k + 1;
-    while (e < v.n && vtype(v, e) == kHsync) e++;
+    int e;
+    if (in_smem) {
+      e = sm.nexth[k] == INT_MAX ? v.n : sm.nexth[k];
+    } else {
+      e = k + 1;
+      while (e < v.n && vtype(v, e) == kHsync) e++;
+    }
     const unsigned long long key = ((unsigned long long)(unsigned)(e - k - 1) << 32) | (0xFFFFFFFFu - (unsigned)k);
     if (!any || key > best) best = key;
     any = true;
@@ -766,9 +856,20 @@ __global__ void __launch_bounds__(kLT) prepare_kernel(LineLocArgs a) {
     sm.pl[i] = a.pl[(size_t)f * kMaxPulses + i];
   }
   __syncthreads();
-  VList v = field_vlist(a, f);
-  v.n = n > 0 ? validate(a, sm, n, v) : 0;
-  if (t == 0) a.vn[f] = v.n;
+  VList vg = field_vlist(a, f);
+  vg.n = n > 0 ? validate(a, sm, n, vg) : 0;
+  if (t == 0) a.vn[f] = vg.n;
+  VList v = vg;
+  if (vg.n <= kSmemValid) {  // work from shared memory
+    for (int k = t; k < vg.n; k += kLT) {
+      sm.vs[k] = vg.s[k];
+      sm.vt[k] = vg.tg[k];
+    }
+    v.s = sm.vs;
+    v.tg = sm.vt;
+    v.d = sm.sort;  // anchor-offset terms; the sort that reuses it comes after
+    __syncthreads();
+  }
   const double mll = mean_line(sm, v, (double)a.fmt.samples_per_line);
   const BlankingScan scan = scan_blanking(sm, v, mll, a.fmt);
   FieldPrep p;
@@ -800,66 +901,81 @@ __global__ void __launch_bounds__(kLT) prepare_kernel(LineLocArgs a) {
 }
 
 // One CTA: the fields in order with the carried state (pipeline.cu:1717-1778).
+// The state stays in shared memory for the whole walk and the fields'
+// records are fetched kPrepBatch at a time, so a field whose speculative
+// grid stands costs a few hundred cycles; a field that needs its anchor fitted
+// (the capture's first field, or an order its own pattern did not fix) is fitted
+// and snapped by the whole CTA.
+constexpr int kPrepBatch = 32;
 __global__ void __launch_bounds__(kLT) finish_kernel(LineLocArgs a) {
   chain_wait();
   extern __shared__ double smem_d[];
   FieldSmem& sm = *reinterpret_cast<FieldSmem*>(smem_d);
+  __shared__ FieldPrep preps[kPrepBatch];
+  __shared__ LineLocState st;
   __shared__ int need_fit, first_s, valid_s;
   __shared__ double prev_off_s, prev_loc_s, prev_diff_s;
   const int t = threadIdx.x;
   const int P = a.win->fields;
   const int LPF = a.fmt.lines_per_frame;
-  for (int f = 0; f < P; f++) {
-    const FieldPrep p = a.prep[f];
-    if (t == 0) {
-      const LineLocState st = *a.state;
-      const long long readloc = a.raw_offset + a.offs[f];
-      double prev_off = 0.0;
-      if (st.prev_first_hsync_readloc != -1 && p.mll > 0.0)
-        prev_off = ((double)st.prev_first_hsync_readloc - (double)readloc) / p.mll;
-      const double prev_loc = st.prev_first_hsync_loc;
-      const bool valid = a.vn[f] > 0 && p.mll > 0.0;
-      bool first = false;
-      need_fit = 0;
-      if (valid) {
-        first = decide_first(p.scan, st.prev_first_field, prev_loc, kAnchorConfidence);
-        need_fit = !(p.spec_first == (first ? 1 : 0) && prev_loc > 0.0);
-      }
-      first_s = first;
-      valid_s = valid;
-      prev_off_s = prev_off;
-      prev_loc_s = prev_loc;
-      prev_diff_s = st.prev_first_hsync_diff;
-    }
+  if (t == 0) st = *a.state;
+  for (int b0 = 0; b0 < P; b0 += kPrepBatch) {
+    const int nb = min(kPrepBatch, P - b0);
+    __syncthreads();  // the previous batch's records are no longer read
+    for (int i = t; i < nb; i += kLT) preps[i] = a.prep[b0 + i];
     __syncthreads();
-    AnchorFit fit = p.spec;
-    if (valid_s && need_fit) {
-      VList v = field_vlist(a, f);
-      fit = fit_anchor(sm, p.scan, v, p.mll, a.fmt, first_s != 0, prev_off_s, prev_loc_s, prev_diff_s);
-      if (fit.cnt > 0) snap_lines(sm, v, fit.loc, fit.hsync_line, p.mll, LPF, a.ll + (size_t)f * LPF);
-    }
-    const bool valid = valid_s && fit.cnt > 0;
-    double* locs = a.ll + (size_t)f * LPF;
-    if (!valid)
-      for (int line = t; line < LPF; line += kLT) locs[line] = p.raw0 + p.mll * (double)line;
-    if (t == 0) {
-      LineLocState st = *a.state;
-      if (valid) {
-        const bool first = first_s != 0;
-        a.is_first[f] = first ? 1 : 0;
-        st.prev_first_field = first ? 1 : 0;
-        st.prev_progressive_field = 0;
-        st.prev_first_hsync_readloc = a.raw_offset + a.offs[f];
-        st.prev_first_hsync_loc = fit.loc;
-        if (!fit.used_prediction)
-          st.prev_first_hsync_diff = hsync_diff_after(fit, a.fmt, first, p.mll, prev_off_s, prev_loc_s);
-      } else {
-        a.is_first[f] = st.prev_first_field >= 0 ? (1 - st.prev_first_field) : 1;
+    for (int j = 0; j < nb; j++) {
+      const int f = b0 + j;
+      const FieldPrep& p = preps[j];
+      if (t == 0) {
+        const long long readloc = a.raw_offset + a.offs[f];
+        double prev_off = 0.0;
+        if (st.prev_first_hsync_readloc != -1 && p.mll > 0.0)
+          prev_off = ((double)st.prev_first_hsync_readloc - (double)readloc) / p.mll;
+        const double prev_loc = st.prev_first_hsync_loc;
+        const bool valid = a.vn[f] > 0 && p.mll > 0.0;
+        bool first = false;
+        need_fit = 0;
+        if (valid) {
+          first = decide_first(p.scan, st.prev_first_field, prev_loc, kAnchorConfidence);
+          need_fit = !(p.spec_first == (first ? 1 : 0) && prev_loc > 0.0);
+        }
+        first_s = first;
+        valid_s = valid;
+        prev_off_s = prev_off;
+        prev_loc_s = prev_loc;
+        prev_diff_s = st.prev_first_hsync_diff;
       }
-      *a.state = st;
+      __syncthreads();
+      AnchorFit fit = p.spec;
+      if (valid_s && need_fit) {
+        VList v = field_vlist(a, f);
+        fit = fit_anchor(sm, p.scan, v, p.mll, a.fmt, first_s != 0, prev_off_s, prev_loc_s, prev_diff_s);
+        if (fit.cnt > 0) snap_lines(sm, v, fit.loc, fit.hsync_line, p.mll, LPF, a.ll + (size_t)f * LPF);
+      }
+      const bool valid = valid_s && fit.cnt > 0;
+      if (!valid) {
+        double* locs = a.ll + (size_t)f * LPF;
+        for (int line = t; line < LPF; line += kLT) locs[line] = p.raw0 + p.mll * (double)line;
+      }
+      if (t == 0) {
+        if (valid) {
+          const bool first = first_s != 0;
+          a.is_first[f] = first ? 1 : 0;
+          st.prev_first_field = first ? 1 : 0;
+          st.prev_progressive_field = 0;
+          st.prev_first_hsync_readloc = a.raw_offset + a.offs[f];
+          st.prev_first_hsync_loc = fit.loc;
+          if (!fit.used_prediction)
+            st.prev_first_hsync_diff = hsync_diff_after(fit, a.fmt, first, p.mll, prev_off_s, prev_loc_s);
+        } else {
+          a.is_first[f] = st.prev_first_field >= 0 ? (1 - st.prev_first_field) : 1;
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
+  if (t == 0) *a.state = st;
 }
 
 // ------------------------------------------------------------ single pass

@@ -7,6 +7,8 @@
 // the integer window truncations match.
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include "chain.cuh"
 #include "cuvhs_internal.h"
 
@@ -174,9 +176,28 @@ __global__ void __launch_bounds__(32 * kHsyncWarps) hsync_kernel(LineArgs a) {
 
 // One CTA per output row: the row's two line starts are read once, the column
 // fractions col/W come from a table (the same FP64 quotient), and consecutive
-// threads write consecutive pixels.
+// threads write consecutive pixels.  The row's source window -- the samples
+// from just before the line start to just past the next line's -- is first
+// staged in shared memory with coalesced 16-byte loads (each sample feeds two
+// to three output columns), then every Catmull-Rom tap reads shared memory.
+// A row whose window would not fit (line locations of a lost signal) reads
+// global memory directly, with the same arithmetic.
+constexpr int kLumaWindow = 4096;  // staged samples per row (a line is 1780 at 28 MHz, 2560 at 40 MHz PAL)
+
+__device__ __forceinline__ uint16_t luma_pixel(const LineArgs& a, float p0, float p1, float p2, float p3, float x,
+                                               bool ok) {
+  const float c1 = p2 - p0;
+  const float c2 = 2.0f * p0 - 5.0f * p1 + 4.0f * p2 - p3;
+  const float c3 = 3.0f * (p1 - p2) + p3 - p0;
+  const float hz = p1 + 0.5f * x * (c1 + x * (c2 + x * c3));
+  float v = hz * a.luma_gain + a.luma_offset;
+  v = fminf(fmaxf(v, 0.0f), 65535.0f);
+  return ok ? (uint16_t)(v + 0.5f) : a.oob_value;
+}
+
 __global__ void __launch_bounds__(kLumaThreads) luma_kernel(LineArgs a) {
   chain_wait();
+  __shared__ __align__(16) float win[kLumaWindow];
   const int W = a.out_w, H = a.out_h;
   const int grow = blockIdx.x;  // field * H + row
   const int field = grow / H, row = grow % H;
@@ -188,6 +209,40 @@ __global__ void __launch_bounds__(kLumaThreads) luma_kernel(LineArgs a) {
   const double a0 = a.ll[(size_t)field * a.lines_per_frame + row];
   const double a1 = a.ll[(size_t)field * a.lines_per_frame + row + 1];
   const double span = a1 - a0;
+  // staged window [lo, lo + n): the taps ci-1 .. ci+2 of every in-range
+  // column, ci = floor(coordinate) between the two line starts (a coordinate
+  // may round a few ulp past either one, so the window reaches one more
+  // sample each way)
+  const double cmin = fmin(a0, a1), cmax = fmax(a0, a1);
+  bool staged = cmin >= -4.0 && cmax < (double)a.total && cmax - cmin < (double)(kLumaWindow - 16);
+  long long lo = 0;
+  int n = 0;
+  if (staged) {
+    lo = ((long long)floor(cmin) - 2) & ~3LL;  // 16-byte aligned start
+    if (lo < 0) lo = 0;
+    const long long hi = min((long long)floor(cmax) + 4, a.total);
+    n = (int)(hi - lo);
+    staged = n > 0 && n <= kLumaWindow;
+  }
+  if (staged) {
+    const float* src = a.video + lo;
+    const bool vec = (reinterpret_cast<uintptr_t>(a.video) & 15) == 0;
+    const int n4 = vec ? n >> 2 : 0;
+    for (int i = threadIdx.x; i < n4; i += kLumaThreads)
+      reinterpret_cast<float4*>(win)[i] = __ldg(reinterpret_cast<const float4*>(src) + i);
+    for (int i = 4 * n4 + threadIdx.x; i < n; i += kLumaThreads) win[i] = __ldg(&src[i]);
+    __syncthreads();
+#pragma unroll 4
+    for (int col = threadIdx.x; col < W; col += kLumaThreads) {
+      const double coord = a0 + __ldg(&a.col_frac[col]) * span;
+      const int ci = (int)coord;
+      const bool ok = ci >= 1 && (long long)ci + 2 < a.total;
+      const int k = ok ? (int)((long long)ci - lo) : 1;  // in-range taps lie in the window
+      const float x = (float)(coord - (double)ci);
+      out[col] = luma_pixel(a, win[k - 1], win[k], win[k + 1], win[k + 2], x, ok);
+    }
+    return;
+  }
   // The loads do not depend on the range test (an out-of-range column reads
   // the first samples and writes the out-of-range value), so the unrolled
   // loop keeps several columns' loads in flight.
@@ -198,15 +253,8 @@ __global__ void __launch_bounds__(kLumaThreads) luma_kernel(LineArgs a) {
     const bool ok = ci >= 1 && (long long)ci + 2 < a.total;
     const int cl = ok ? ci : 1;
     const float x = (float)(coord - (double)ci);
-    const float p0 = __ldg(&a.video[cl - 1]), p1 = __ldg(&a.video[cl]);
-    const float p2 = __ldg(&a.video[cl + 1]), p3 = __ldg(&a.video[cl + 2]);
-    const float c1 = p2 - p0;
-    const float c2 = 2.0f * p0 - 5.0f * p1 + 4.0f * p2 - p3;
-    const float c3 = 3.0f * (p1 - p2) + p3 - p0;
-    const float hz = p1 + 0.5f * x * (c1 + x * (c2 + x * c3));
-    float v = hz * a.luma_gain + a.luma_offset;
-    v = fminf(fmaxf(v, 0.0f), 65535.0f);
-    out[col] = ok ? (uint16_t)(v + 0.5f) : a.oob_value;
+    out[col] = luma_pixel(a, __ldg(&a.video[cl - 1]), __ldg(&a.video[cl]), __ldg(&a.video[cl + 1]),
+                          __ldg(&a.video[cl + 2]), x, ok);
   }
 }
 

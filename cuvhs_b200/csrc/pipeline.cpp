@@ -141,7 +141,9 @@ void Context::release() {
   }
   if (hstream) cudaStreamDestroy(hstream);
   hstream = nullptr;
-  for (cudaEvent_t* e : {&ev_ll, &ev_win, &ev_winhost}) {
+  if (pstream) cudaStreamDestroy(pstream);
+  pstream = nullptr;
+  for (cudaEvent_t* e : {&ev_ll, &ev_win, &ev_winhost, &ev_k1b, &ev_pre}) {
     if (*e) cudaEventDestroy(*e);
     *e = nullptr;
   }
@@ -152,6 +154,150 @@ void Context::release() {
   xstream = nullptr;
   if (stream) cudaStreamDestroy(stream);
   stream = nullptr;
+}
+
+// Device and page-locked host buffers for `batch` fields.
+bool Context::alloc_buffers() {
+  bool ok = true;
+  const size_t S = (size_t)batch * spp;
+  auto A = [&](auto* tag, size_t n) {
+    using T = std::remove_pointer_t<decltype(tag)>;
+    const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+    if (ok && dev_limit > 0 && dev_used + bytes > dev_limit) {
+      ok = false;
+      err = "device memory limit reached";
+    }
+    T* p = dalloc<T>(n, err, ok);
+    if (p) {
+      allocations.push_back(p);
+      dev_used += bytes;
+    }
+    return p;
+  };
+  env_blocks = (spp + des.a_out - 1) / des.a_out;
+  d_raw_set[0] = A((uint8_t*)nullptr, S * bps + 64);
+  d_raw_set[1] = A((uint8_t*)nullptr, S * bps + 64);
+  d_dc = A((float*)nullptr, 1);
+  d_dcsum = A((unsigned long long*)nullptr, 1);
+  d_raw = d_raw_set[0];
+  d_dem = A((float*)nullptr, S);
+  d_env = A((float*)nullptr, S);
+  d_video = A((float*)nullptr, S);
+  d_sync = A((float*)nullptr, S);
+  d_env_part = A((double*)nullptr, (size_t)batch * env_blocks);
+  edge_cap = (int)std::min<size_t>(S / 4 + 4096, (size_t)INT_MAX / 2);
+  d_fall = A((unsigned*)nullptr, edge_cap);
+  d_rise = A((unsigned*)nullptr, edge_cap);
+  d_counts = A((int*)nullptr, 4);
+  d_edge_blk = A((int2*)nullptr, (size_t)edge_blocks((long long)batch * spp) + 1);
+  d_edge_mask = A((unsigned*)nullptr, edge_mask_words((long long)batch * spp));
+  d_ll = A((double*)nullptr, (size_t)batch * fmt.lines_per_frame);
+  const size_t F = (size_t)fmt.output_line_len * fmt.output_field_lines;
+  for (int k = 0; k < 2; k++) {
+    d_luma_set[k] = A((uint16_t*)nullptr, (size_t)batch * F);
+    d_chroma_set[k] = A((uint16_t*)nullptr, (size_t)batch * F);
+  }
+  d_luma = d_luma_set[0];
+  d_chroma = d_chroma_set[0];
+  d_burst = A((float*)nullptr, (size_t)batch * fmt.output_field_lines * fmt.burst_len);
+  d_track = A((int*)nullptr, batch);
+  d_do_count = A((int*)nullptr, batch);
+  d_do_lines = A((int*)nullptr, (size_t)batch * kMaxDropouts);
+  d_do_starts = A((int*)nullptr, (size_t)batch * kMaxDropouts);
+  d_do_ends = A((int*)nullptr, (size_t)batch * kMaxDropouts);
+  d_do_cls = A((unsigned char*)nullptr, (size_t)batch * dropout_class_bytes_per_field(spp));
+  d_ga = A((float2*)nullptr, des.ga.size());
+  d_gb = A((float2*)nullptr, des.gb.size());
+  d_gc = A((float*)nullptr, des.gc.size());
+  d_twa = A((float2*)nullptr, des.tw_a.size());
+  d_twb = A((float2*)nullptr, des.tw_b.size());
+  d_twc = A((float2*)nullptr, des.tw_c.size());
+  d_twl = A((float2*)nullptr, des.tw_line.size());
+  d_twa_inv = A((float2*)nullptr, des.tw_a.size());
+  d_twb_inv = A((float2*)nullptr, des.tw_b.size());
+  d_twc_inv = A((float2*)nullptr, des.tw_c.size());
+  d_twl_inv = A((float2*)nullptr, des.tw_line.size());
+  d_win = A((WindowInfo*)nullptr, 1);
+  d_offs = A((long long*)nullptr, (size_t)batch + 1);
+  d_cand = A((int*)nullptr, edge_cap);
+  d_ps = A((int*)nullptr, (size_t)batch * kMaxPulses);
+  d_pl = A((int*)nullptr, (size_t)batch * kMaxPulses);
+  d_pn = A((int*)nullptr, batch);
+  d_vs = A((int*)nullptr, (size_t)batch * kMaxValid);
+  d_vl = A((int*)nullptr, (size_t)batch * kMaxValid);
+  d_vt = A((unsigned char*)nullptr, (size_t)batch * kMaxValid);
+  d_vd = A((double*)nullptr, (size_t)batch * kMaxValid);
+  d_vn = A((int*)nullptr, batch);
+  d_prep = A((FieldPrep*)nullptr, batch);
+  d_lls = A((LineLocState*)nullptr, 1);
+  d_is_first = A((int*)nullptr, batch);
+  d_dbg_vs = A((int*)nullptr, (size_t)batch * kMaxPulses);
+  d_dbg_vl = A((int*)nullptr, (size_t)batch * kMaxPulses);
+  d_dbg_vt = A((int*)nullptr, (size_t)batch * kMaxPulses);
+  d_dbg_vn = A((int*)nullptr, batch);
+  d_col_frac = A((double*)nullptr, (size_t)fmt.output_line_len);
+  d_ga64 = A((double*)nullptr, des.ga64.size());
+  d_hs64 = A((double*)nullptr, des.hs64.size());
+  d_guard_list = A((unsigned*)nullptr, kGuardCap);
+  d_guard_done = A((int*)nullptr, kGuardCap);
+  d_guard_count = A((int*)nullptr, 1);
+  d_guard_part = A((double*)nullptr, (size_t)kGuardCap * kGuardMaxParts);
+  d_guard_vals = A((double*)nullptr, kGuardCap);
+  if (ok && guard_parts(des.hs64_half) > kGuardMaxParts) {
+    err = "sync guard support too long";
+    ok = false;
+  }
+  if (!ok) return false;
+  // pinned host staging for the per-chunk round trips
+  auto H = [&](auto* tag, size_t n) {
+    using T = std::remove_pointer_t<decltype(tag)>;
+    void* p = nullptr;
+    if (!ok) return (T*)nullptr;
+    if (cudaHostAlloc(&p, std::max<size_t>(n, 1) * sizeof(T), cudaHostAllocDefault) != cudaSuccess) {
+      ok = false;
+      err = "cudaHostAlloc failed";
+      cudaGetLastError();
+      return (T*)nullptr;
+    }
+    host_allocations.push_back(p);
+    return static_cast<T*>(p);
+  };
+  hp_counts = H((int*)nullptr, 4);
+  hp_win = H((WindowInfo*)nullptr, 1);
+  hp_offs = H((long long*)nullptr, (size_t)batch + 1);
+  hp_is_first = H((int*)nullptr, batch);
+  hp_guard = H((int*)nullptr, 1);
+  hp_track = H((int*)nullptr, batch);
+  hp_trial = H((int*)nullptr, 2);
+  hp_burst = H((float*)nullptr, (size_t)2 * fmt.output_field_lines * fmt.burst_len);
+  {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, std::max(batch, 1) * sizeof(double), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer((void**)&dp_metric, p, 0) != cudaSuccess) {
+      if (p) cudaFreeHost(p);
+      err = "cudaHostAlloc (mapped) failed";
+      ok = false;
+    } else {
+      host_allocations.push_back(p);
+      hp_metric = static_cast<double*>(p);
+    }
+  }
+  hp_do_count = H((int*)nullptr, batch);
+  hp_do_lines = H((int*)nullptr, (size_t)batch * kMaxDropouts);
+  hp_do_starts = H((int*)nullptr, (size_t)batch * kMaxDropouts);
+  hp_do_ends = H((int*)nullptr, (size_t)batch * kMaxDropouts);
+  if (!ok) return false;
+  return true;
+}
+
+void Context::free_buffers() {
+  if (device >= 0) cudaSetDevice(device);
+  for (void* p : allocations) cudaFree(p);
+  allocations.clear();
+  for (void* p : host_allocations) cudaFreeHost(p);
+  host_allocations.clear();
+  dev_used = 0;
+  cudaGetLastError();
 }
 
 bool Context::init(const cuvhs_config& c) {
@@ -228,138 +374,27 @@ bool Context::init(const cuvhs_config& c) {
   if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&xstream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&hstream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithPriority(&lstream, cudaStreamNonBlocking, prio_high) != cudaSuccess) {
+      cudaStreamCreateWithPriority(&lstream, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&pstream, cudaStreamNonBlocking) != cudaSuccess) {
     err = "cudaStreamCreate failed";
     status = CUVHS_ERR_CUDA;
     return false;
   }
-  bool ok = true;
-  const size_t S = (size_t)batch * spp;
-  auto A = [&](auto* tag, size_t n) {
-    using T = std::remove_pointer_t<decltype(tag)>;
-    T* p = dalloc<T>(n, err, ok);
-    if (p) allocations.push_back(p);
-    return p;
-  };
-  env_blocks = (spp + des.a_out - 1) / des.a_out;
-  d_raw_set[0] = A((uint8_t*)nullptr, S * bps + 64);
-  d_raw_set[1] = A((uint8_t*)nullptr, S * bps + 64);
-  d_dc = A((float*)nullptr, 1);
-  d_dcsum = A((unsigned long long*)nullptr, 1);
-  d_raw = d_raw_set[0];
-  d_dem = A((float*)nullptr, S);
-  d_env = A((float*)nullptr, S);
-  d_video = A((float*)nullptr, S);
-  d_sync = A((float*)nullptr, S);
-  d_env_part = A((double*)nullptr, (size_t)batch * env_blocks);
-  edge_cap = (int)std::min<size_t>(S / 4 + 4096, (size_t)INT_MAX / 2);
-  d_fall = A((unsigned*)nullptr, edge_cap);
-  d_rise = A((unsigned*)nullptr, edge_cap);
-  d_counts = A((int*)nullptr, 4);
-  d_edge_blk = A((int2*)nullptr, (size_t)edge_blocks((long long)batch * spp) + 1);
-  d_edge_mask = A((unsigned*)nullptr, edge_mask_words((long long)batch * spp));
-  d_ll = A((double*)nullptr, (size_t)batch * fmt.lines_per_frame);
-  const size_t F = (size_t)fmt.output_line_len * fmt.output_field_lines;
-  for (int k = 0; k < 2; k++) {
-    d_luma_set[k] = A((uint16_t*)nullptr, (size_t)batch * F);
-    d_chroma_set[k] = A((uint16_t*)nullptr, (size_t)batch * F);
-  }
-  d_luma = d_luma_set[0];
-  d_chroma = d_chroma_set[0];
-  d_burst = A((float*)nullptr, (size_t)batch * fmt.output_field_lines * fmt.burst_len);
-  d_track = A((int*)nullptr, batch);
-  d_do_count = A((int*)nullptr, batch);
-  d_do_lines = A((int*)nullptr, (size_t)batch * kMaxDropouts);
-  d_do_starts = A((int*)nullptr, (size_t)batch * kMaxDropouts);
-  d_do_ends = A((int*)nullptr, (size_t)batch * kMaxDropouts);
-  d_do_cls = A((unsigned char*)nullptr, (size_t)batch * dropout_class_bytes_per_field(spp));
-  d_ga = A((float2*)nullptr, des.ga.size());
-  d_gb = A((float2*)nullptr, des.gb.size());
-  d_gc = A((float*)nullptr, des.gc.size());
-  d_twa = A((float2*)nullptr, des.tw_a.size());
-  d_twb = A((float2*)nullptr, des.tw_b.size());
-  d_twc = A((float2*)nullptr, des.tw_c.size());
-  d_twl = A((float2*)nullptr, des.tw_line.size());
-  d_twa_inv = A((float2*)nullptr, des.tw_a.size());
-  d_twb_inv = A((float2*)nullptr, des.tw_b.size());
-  d_twc_inv = A((float2*)nullptr, des.tw_c.size());
-  d_twl_inv = A((float2*)nullptr, des.tw_line.size());
-  d_win = A((WindowInfo*)nullptr, 1);
-  d_offs = A((long long*)nullptr, (size_t)batch + 1);
-  d_cand = A((int*)nullptr, edge_cap);
-  d_ps = A((int*)nullptr, (size_t)batch * kMaxPulses);
-  d_pl = A((int*)nullptr, (size_t)batch * kMaxPulses);
-  d_pn = A((int*)nullptr, batch);
-  d_vs = A((int*)nullptr, (size_t)batch * kMaxValid);
-  d_vl = A((int*)nullptr, (size_t)batch * kMaxValid);
-  d_vt = A((unsigned char*)nullptr, (size_t)batch * kMaxValid);
-  d_vd = A((double*)nullptr, (size_t)batch * kMaxValid);
-  d_vn = A((int*)nullptr, batch);
-  d_prep = A((FieldPrep*)nullptr, batch);
-  d_lls = A((LineLocState*)nullptr, 1);
-  d_is_first = A((int*)nullptr, batch);
-  d_dbg_vs = A((int*)nullptr, (size_t)batch * kMaxPulses);
-  d_dbg_vl = A((int*)nullptr, (size_t)batch * kMaxPulses);
-  d_dbg_vt = A((int*)nullptr, (size_t)batch * kMaxPulses);
-  d_dbg_vn = A((int*)nullptr, batch);
-  d_ga64 = A((double*)nullptr, des.ga64.size());
-  d_hs64 = A((double*)nullptr, des.hs64.size());
-  d_guard_list = A((unsigned*)nullptr, kGuardCap);
-  d_guard_done = A((int*)nullptr, kGuardCap);
-  d_guard_count = A((int*)nullptr, 1);
-  d_guard_part = A((double*)nullptr, (size_t)kGuardCap * kGuardMaxParts);
-  d_guard_vals = A((double*)nullptr, kGuardCap);
-  if (ok && guard_parts(des.hs64_half) > kGuardMaxParts) {
-    err = "sync guard support too long";
-    ok = false;
-  }
-  if (!ok) {
-    status = CUVHS_ERR_OUT_OF_MEMORY;
-    release();
-    return false;
-  }
-  // pinned host staging for the per-chunk round trips
-  auto H = [&](auto* tag, size_t n) {
-    using T = std::remove_pointer_t<decltype(tag)>;
-    void* p = nullptr;
-    if (!ok) return (T*)nullptr;
-    if (cudaHostAlloc(&p, std::max<size_t>(n, 1) * sizeof(T), cudaHostAllocDefault) != cudaSuccess) {
-      ok = false;
-      err = "cudaHostAlloc failed";
-      cudaGetLastError();
-      return (T*)nullptr;
+  // Buffers for `batch` fields; a sized-from-free-memory batch backs off by
+  // halves when an allocation fails (the reference retries at smaller VRAM
+  // fractions, src/pipeline/pipeline.cu:1384-1475).  An explicit batch_fields
+  // is kept or the context fails, since the batch sets the chunking.
+  dev_limit = (size_t)std::max(0.0, c.device_memory_limit_mb) * (1u << 20);
+  for (;;) {
+    batch = b;
+    if (alloc_buffers()) break;
+    free_buffers();
+    if (c.batch_fields > 0 || b <= 1) {
+      status = CUVHS_ERR_OUT_OF_MEMORY;
+      release();
+      return false;
     }
-    host_allocations.push_back(p);
-    return static_cast<T*>(p);
-  };
-  hp_counts = H((int*)nullptr, 4);
-  hp_win = H((WindowInfo*)nullptr, 1);
-  hp_offs = H((long long*)nullptr, (size_t)batch + 1);
-  hp_is_first = H((int*)nullptr, batch);
-  hp_guard = H((int*)nullptr, 1);
-  hp_track = H((int*)nullptr, batch);
-  hp_trial = H((int*)nullptr, 2);
-  hp_burst = H((float*)nullptr, (size_t)2 * fmt.output_field_lines * fmt.burst_len);
-  {
-    void* p = nullptr;
-    if (cudaHostAlloc(&p, std::max(batch, 1) * sizeof(double), cudaHostAllocMapped) != cudaSuccess ||
-        cudaHostGetDevicePointer((void**)&dp_metric, p, 0) != cudaSuccess) {
-      if (p) cudaFreeHost(p);
-      err = "cudaHostAlloc (mapped) failed";
-      ok = false;
-    } else {
-      host_allocations.push_back(p);
-      hp_metric = static_cast<double*>(p);
-    }
-  }
-  hp_do_count = H((int*)nullptr, batch);
-  hp_do_lines = H((int*)nullptr, (size_t)batch * kMaxDropouts);
-  hp_do_starts = H((int*)nullptr, (size_t)batch * kMaxDropouts);
-  hp_do_ends = H((int*)nullptr, (size_t)batch * kMaxDropouts);
-  if (!ok) {
-    status = CUVHS_ERR_OUT_OF_MEMORY;
-    release();
-    return false;
+    b = std::max(1, b / 2);
   }
   hp_trial[0] = 0;
   hp_trial[1] = 1;
@@ -368,7 +403,9 @@ bool Context::init(const cuvhs_config& c) {
                cudaEventCreateWithFlags(&ev_edges, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_ll, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_win, cudaEventDisableTiming) == cudaSuccess &&
-               cudaEventCreateWithFlags(&ev_winhost, cudaEventDisableTiming) == cudaSuccess;
+               cudaEventCreateWithFlags(&ev_winhost, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev_k1b, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev_pre, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t* e : {&ev_prefetch, &ev_small, &ev_chroma, &ev_out_done[0], &ev_out_done[1]})
     ev_ok = ev_ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t& e : ev_piece) ev_ok = ev_ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
@@ -397,7 +434,6 @@ bool Context::init(const cuvhs_config& c) {
   }
   std::vector<double> col_frac(fmt.output_line_len);
   for (int c = 0; c < fmt.output_line_len; c++) col_frac[c] = (double)c / (double)fmt.output_line_len;
-  d_col_frac = A((double*)nullptr, col_frac.size());
   upload(d_col_frac, col_frac, stream);
   if (cudaStreamSynchronize(stream) != cudaSuccess) {
     err = std::string("upload failed: ") + cudaGetErrorString(cudaGetLastError());
@@ -890,6 +926,8 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
       if (keep) return;
       cudaStreamSynchronize(c->xstream);
       cudaStreamSynchronize(c->hstream);
+      cudaStreamSynchronize(c->pstream);  // after an error, nothing of the chunk is left running
+      cudaStreamSynchronize(c->lstream);
       c->pf.valid = false;
     }
   } drain{this};
@@ -985,6 +1023,25 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
       }
     }
   }
+  // ---- the colour-under pre-band-pass needs only the raw samples, and its
+  // output takes the demod buffer's place once K1b has read it: on its own
+  // stream it runs beside the guard, the edges, the field windows and the
+  // line locations (short, latency-bound kernels).  It covers all T
+  // demodulated slots; the detected fields are a prefix.
+  ChromaArgs ca = chroma_args(da.raw, (int)n_read, da.dc, T);
+  if (debug) {
+    dbg_demod.resize(std::min<size_t>((size_t)T * spp, (size_t)debug_tiles * spp));
+    cudaMemcpyAsync(dbg_demod.data(), d_dem, dbg_demod.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
+  }
+  cudaEventRecord(ev_k1b, stream);
+  cudaStreamWaitEvent(pstream, ev_k1b, 0);
+  {
+    cudaEvent_t ev_;
+    begin_stage_on(kStageChromaPre, ev_, pstream);
+    launch_chroma_prefilter(ca, pstream);
+    end_stage_on(kStageChromaPre, ev_, pstream);
+  }
+  cudaEventRecord(ev_pre, pstream);
   {
     // FP64 threshold decisions for the listed sync samples
     cudaEvent_t ev_;
@@ -1030,21 +1087,8 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     end_stage_on(kStageLines, ev_, lstream, single_pass ? 2 : 3);
   }
   cudaEventRecord(ev_ll, lstream);
-  // ---- the colour-under pre-band-pass needs only the raw samples.  It
-  // covers all T demodulated slots; the detected fields are a prefix.
   const int LPF = fmt.lines_per_frame;
   const int H = fmt.output_field_lines;
-  ChromaArgs ca = chroma_args(da.raw, (int)n_read, da.dc, T);
-  if (debug) {
-    dbg_demod.resize(std::min<size_t>((size_t)T * spp, (size_t)debug_tiles * spp));
-    cudaMemcpyAsync(dbg_demod.data(), d_dem, dbg_demod.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
-  }
-  {
-    cudaEvent_t ev_;
-    begin_stage(kStageChromaPre, ev_);
-    launch_chroma_prefilter(ca, stream);
-    end_stage(kStageChromaPre, ev_);
-  }
   if (!check_cuda("chroma prefilter")) return false;
   double t_host = host_clock();
   {
@@ -1179,6 +1223,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   ca.fields = P;
   ca.total = (long long)P * spp;
   // the chroma is concealed and sent as it is decoded (chroma_fields)
+  cudaStreamWaitEvent(stream, ev_pre, 0);
   if (!chroma_fields(ca, P, &dd, dst_chroma)) return false;
   if (!check_cuda("chroma concealment")) return false;
   cudaEventRecord(ev_out_done[oset], xstream);

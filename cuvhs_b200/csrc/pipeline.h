@@ -76,6 +76,10 @@ struct Context {
   // field windows (the host reads the field count and offsets after it).
   cudaStream_t lstream = nullptr;
   cudaEvent_t ev_ll = nullptr, ev_win = nullptr, ev_winhost = nullptr;
+  // Chroma pre-band-pass: its own stream, after K1b (ev_k1b), beside the
+  // sync and line-location kernels; the chroma lines wait on ev_pre.
+  cudaStream_t pstream = nullptr;
+  cudaEvent_t ev_k1b = nullptr, ev_pre = nullptr;
   uint8_t* d_raw_set[2] = {};
   uint16_t* d_luma_set[2] = {};
   uint16_t* d_chroma_set[2] = {};
@@ -197,6 +201,9 @@ struct Context {
 
   ~Context();
   bool init(const cuvhs_config& c);
+  bool alloc_buffers();  // for `batch` fields; false (err set) when an allocation fails
+  void free_buffers();
+  size_t dev_limit = 0, dev_used = 0;  // device bytes this context may allocate (0: no limit), allocated
   void release();
   void reset_state();
   bool check_cuda(const char* where);

@@ -13,7 +13,11 @@ enum InputFormat { kInU8 = 0, kInS16 = 1, kInU16 = 2 };
 
 template <int FMT>
 __device__ __forceinline__ float raw_convert(const uint8_t* __restrict__ raw, int p) {
-  if constexpr (FMT == kInU8) return ((float)__ldg(raw + p) - 128.0f) * 256.0f;
+  // u8: 2^23 + x as a float by setting the exponent bits (no integer-to-float
+  // conversion, which issues at a quarter of the FP32 rate), then one exact
+  // FMA: (2^23 + x) * 256 - (2^31 + 2^15) = (x - 128) * 256.
+  if constexpr (FMT == kInU8)
+    return fmaf(__int_as_float(0x4B000000 | (int)__ldg(raw + p)), 256.0f, -2147516416.0f);
   if constexpr (FMT == kInS16) return (float)__ldg(reinterpret_cast<const int16_t*>(raw) + p);
   return (float)__ldg(reinterpret_cast<const uint16_t*>(raw) + p) - 32768.0f;
 }

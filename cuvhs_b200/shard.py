@@ -73,10 +73,12 @@ def field_period(sample_rate_hz: float, pal: bool = False) -> float:
 
 
 def run_chain(decode_chunk: Callable, get_state: Callable, n_samples: int, samples_per_field: int,
-              batch_fields: int, start: int, stop: int) -> List[ChunkRecord]:
+              batch_fields: int, start: int, stop: int, after_first: Optional[Callable] = None) -> List[ChunkRecord]:
     """The chunk loop from `start` with the decoder's current state, over the
     chunks that start before `stop` (Pipeline::run's loop).
-    decode_chunk(raw_offset, num_fields) -> (output, fields, next_offset)."""
+    decode_chunk(raw_offset, num_fields) -> (output, fields, next_offset);
+    after_first(), if given, runs once after the first chunk (to amend the
+    decoder's state)."""
     chunks = []
     raw = int(start)
     while raw < stop:
@@ -89,6 +91,8 @@ def run_chain(decode_chunk: Callable, get_state: Callable, n_samples: int, sampl
         chunks.append(ChunkRecord(raw, int(nxt), int(fields), st_in, get_state(), out))
         if fields == 0:
             break
+        if after_first is not None and len(chunks) == 1:
+            after_first()
         raw = int(nxt)
     return chunks
 
@@ -153,11 +157,23 @@ def _gpu_chain_fns(dec, x):
     return decode_chunk, get_state, set_state
 
 
-def decode_segment(dec, x, start, stop, batch_fields):
-    """One segment's chain on `dec` (fresh state)."""
-    decode_chunk, get_state, _ = _gpu_chain_fns(dec, x)
+def decode_segment(dec, x, start, stop, batch_fields, chroma_threshold=None):
+    """One segment's chain on `dec` from a fresh state.  The chroma decode's
+    track-error threshold is set once, from the capture's first field
+    (chroma_decode.cu:684-743), and carried unchanged; a segment that starts
+    mid-capture measures its own on its first chunk, so with
+    `chroma_threshold` (the capture's) it takes the capture's value after
+    that chunk, which lets its chain's state meet the single-pass one."""
+    decode_chunk, get_state, set_state = _gpu_chain_fns(dec, x)
     dec.reset()
-    return run_chain(decode_chunk, get_state, x.size, dec.samples_per_field, batch_fields, start, stop)
+    after_first = None
+    if chroma_threshold is not None:
+        def after_first():
+            st = dec.get_state()
+            st.chroma_threshold = chroma_threshold
+            dec.set_state(st)
+    return run_chain(decode_chunk, get_state, x.size, dec.samples_per_field, batch_fields, start, stop,
+                     after_first)
 
 
 def replayer(dec, x):
@@ -214,20 +230,22 @@ def merge_results(dec, chunks: List[ChunkRecord]):
                         dropouts=dropouts, json=jb.value.decode())
 
 
-def first_field_location(dec, x) -> int:
-    """Where the capture's first field starts: a one-field chunk at 0 (the
-    decoder's state is reset afterwards)."""
+def capture_start(dec, x):
+    """The capture's first chunk, decoded on `dec` (state reset before and
+    after): (first field location, chroma track-error threshold)."""
     dec.reset()
-    res, _ = dec.decode_chunk(x, 0, 1)
+    nf = max(1, min(dec.batch_fields, x.size // dec.samples_per_field))
+    res, _ = dec.decode_chunk(x, 0, nf)
+    thr = dec.get_state().chroma_threshold
     dec.reset()
-    return int(res.file_loc[0]) if res.n_fields else 0
+    return (int(res.file_loc[0]) if res.n_fields else 0), thr
 
 
-def plan_for(dec, x, parts):
+def plan_for(dec, x, parts, first_field):
     pal = dec.lines_per_frame != 525
     spl = dec.samples_per_field // (313 if pal else 263)
     fs = spl * (15625.0 if pal else 15734.264)
-    return plan_segments(x.size, parts, first_field_location(dec, x), field_period(fs, pal), dec.batch_fields, spl)
+    return plan_segments(x.size, parts, first_field, field_period(fs, pal), dec.batch_fields, spl)
 
 
 def decode_split(x, sample_rate_mhz, parts=2, batch_fields=0, device=0, **decoder_kw):
@@ -237,8 +255,10 @@ def decode_split(x, sample_rate_mhz, parts=2, batch_fields=0, device=0, **decode
     from ._lib import Decoder
     with Decoder(sample_rate_mhz, device=device, batch_fields=batch_fields, **decoder_kw) as dec:
         spf = dec.samples_per_field
-        plan = plan_for(dec, x, parts)
-        segs = [decode_segment(dec, x, a, b, dec.batch_fields) for a, b in plan]
+        first_field, thr = capture_start(dec, x)
+        plan = plan_for(dec, x, parts, first_field)
+        segs = [decode_segment(dec, x, a, b, dec.batch_fields, None if k == 0 else thr)
+                for k, (a, b) in enumerate(plan)]
         chain, replays = join_all(segs, replayer(dec, x), x.size, spf)
         return merge_results(dec, chain), replays, [len(s) for s in segs]
 

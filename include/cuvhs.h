@@ -76,6 +76,12 @@ typedef struct cuvhs_config {
                              samples are re-evaluated in FP64 before any threshold decision; 0 = the
                              default (8 Hz, several times the FP32 sync error).  Wider bands cost time
                              and change nothing else; they exist to check the FP64 path */
+  double device_memory_limit_mb; /* 0 = none; else the context allocates at most this much device
+                             memory, as if other users held the rest: when batch_fields is 0 the
+                             batch is sized from the free memory and halved after any allocation
+                             that fails or passes the limit (the reference's VRAM back-off,
+                             src/pipeline/pipeline.cu:1384-1475); an explicit batch_fields that does
+                             not fit fails with CUVHS_ERR_OUT_OF_MEMORY */
 } cuvhs_config;
 
 /* Per-field metadata, one .tbc.json "fields" entry. */

@@ -386,3 +386,24 @@ def test_short_and_empty_captures():
         x1 = workload("small28")[: d.samples_per_field + 5000]
         r1 = d.decode_capture(x1)
         assert r1.n_fields <= 1
+
+
+@pytest.mark.gpu
+def test_device_memory_limit_backs_off_the_batch():
+    """With less device memory than the free-memory sizing assumes (other
+    users of the GPU), the context halves its batch until its buffers fit
+    (the reference's VRAM back-off, src/pipeline/pipeline.cu:1384-1475) and
+    decodes as before; an explicit batch that does not fit, or a limit below
+    one field's buffers, fails with CUVHS_ERR_OUT_OF_MEMORY."""
+    x = workload("small28")
+    with cv.Decoder(28.0) as d:
+        full, b_full = d.decode_capture(x), d.batch_fields
+    with cv.Decoder(28.0, device_memory_limit_mb=3000) as d:
+        lim, b_lim = d.decode_capture(x), d.batch_fields
+    assert 1 <= b_lim < b_full and b_lim * 2 > 64, (b_lim, b_full)
+    assert lim.json == full.json
+    assert np.array_equal(lim.luma, full.luma) and np.array_equal(lim.chroma, full.chroma)
+    for kw in (dict(batch_fields=2000, device_memory_limit_mb=3000), dict(device_memory_limit_mb=10)):
+        with pytest.raises(cv.CuvhsError) as e:
+            cv.Decoder(28.0, **kw)
+        assert e.value.status == 3, str(e.value)  # CUVHS_ERR_OUT_OF_MEMORY

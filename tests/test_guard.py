@@ -11,8 +11,8 @@ FP64 oracle:
 * outside the band the FP32 sync is within a quarter of the band of the FP64
   sync (the assumption the band rests on);
 * the FP64 values the guard computes agree with the oracle's FP64 sync within
-  1e-4 Hz, over thousands of samples listed with a 30 kHz band, and that wide
-  band leaves the decode's outputs unchanged."""
+  1e-4 Hz, over thousands of samples listed with a 10-30 kHz band, and that
+  wide band leaves the decode's outputs unchanged."""
 import numpy as np
 import pytest
 
@@ -62,9 +62,10 @@ def test_threshold_decisions_are_the_fp64_ones(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["small28", "small358", "pal20_40"])
-def test_guard_fp64_values_match_the_oracle(name):
-    wide, dbg, _, _ = _decode(name, guard_band_hz=3.0e4)
+@pytest.mark.parametrize("name,band", [("small28", 3.0e4), ("small358", 3.0e4), ("pal20_40", 1.0e4)])
+def test_guard_fp64_values_match_the_oracle(name, band):
+    # the band lists a few thousand samples (the chunk's list holds 65,536)
+    wide, dbg, _, _ = _decode(name, guard_band_hz=band)
     o = _oracle_signals(name)
     s64 = o.array(0, "demod05")
     pos, vals = dbg["guard_positions"], dbg["guard_values"]

@@ -25,9 +25,10 @@ def test_split_decode_equals_single_pass(name, parts, batch):
     assert joined.json == single.json
     assert np.array_equal(joined.luma, single.luma)
     assert np.array_equal(joined.chroma, single.chroma)
-    # the predicted chunk boundaries hold on a constant-speed tape: each join
-    # replays at most the segment's first two chunks
-    assert all(r <= 2 for r in replays), replays
+    # the predicted chunk boundaries hold on a constant-speed tape and later
+    # segments take the capture's chroma threshold: each join replays at most
+    # the segment's first two chunks
+    assert all(r <= 2 for r in replays), (replays, seg_chunks)
 
 
 @pytest.mark.gpu

@@ -634,7 +634,10 @@ def main():
         device_step()
     torch.cuda.synchronize()
     stage_all = dec.stage_times()
-    kernels = {k: v for k, v in stage_all.items() if not k.startswith("host_")}
+    # the roofline kernel: the longest stage that moves stage-interface bytes
+    # (the latency-bound line-location and guard stages move a few KB)
+    kernels = {k: v for k, v in stage_all.items()
+               if not k.startswith("host_") and stage_bytes_per_field(k, mhz * 1e6) > 0}
     dom = max(kernels, key=lambda k: kernels[k][0])
     # the timed region brackets only the dominant kernel, for its live launch time
     dec.set_timing(True, stages=[dom])

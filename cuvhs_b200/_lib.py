@@ -534,6 +534,7 @@ class Decoder:
 
     _DTYPES = {"field_offsets": np.int64, "linelocs_coarse": np.float64, "linelocs": np.float64,
                "guard_positions": np.int64, "guard_values": np.float64,
+               "lineloc_clocks": np.int64, "guard_clocks": np.int64,
                "demod": np.float32, "video": np.float32, "sync": np.float32, "envelope": np.float32,
                "chroma_prefilt": np.float32}
 

@@ -377,6 +377,8 @@ long long cuvhs_debug_array(const cuvhs_ctx* ctx, const char* name, void* dst, l
   if (s == "guard_positions") return copy_out(c.dbg_guard_pos, dst, cap);
   if (s == "guard_values") return copy_out(c.dbg_guard_vals, dst, cap);
   if (s == "linelocs_coarse") return copy_out(c.dbg_ll_coarse, dst, cap);
+  if (s == "lineloc_clocks") return copy_out(c.dbg_clk_ll, dst, cap);
+  if (s == "guard_clocks") return copy_out(c.dbg_clk_guard, dst, cap);
   if (s == "linelocs") return copy_out(c.dbg_ll, dst, cap);
   if (s == "demod") return copy_out(c.dbg_demod, dst, cap);
   if (s == "video") return copy_out(c.dbg_video, dst, cap);

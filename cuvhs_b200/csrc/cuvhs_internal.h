@@ -20,6 +20,7 @@ namespace cuvhs {
 constexpr int kOverlap = 2048;        // overlap-save history of every demod tile
 constexpr int kFieldMarginLines = 20;  // extra lines per tile beyond one field
 constexpr int kMaxPulses = 800;        // pulses kept per field
+constexpr int kPhaseSlots = 32;        // phase clocks recorded per field or sample (inspection)
 constexpr int kMaxDropouts = 512;      // TBC dropout entries per field
 constexpr int kMaxRfDropouts = 128;    // RF-domain dropout spans per field
 constexpr int kMaxBurstLen = 48;       // burst window width bound, output samples (NTSC 36, PAL 40)
@@ -91,6 +92,11 @@ struct Design {
   static constexpr int kGuardMaxHalf = 4096;
   int ga64_half = 0, hs64_half = 0;
   std::vector<double> ga64, hs64;
+  // the guard's overlap-save form of ga64: its kGuardN-point FFT (taps at
+  // offset m placed at m mod kGuardN) divided by kGuardN, and the FFT's
+  // twiddles exp(-2 pi i k / kGuardN); interleaved re, im
+  static constexpr int kGuardN = 4096;
+  std::vector<double> guard_g, guard_tw;
   // twiddle tables W_N^m
   std::vector<float2> tw_a, tw_b, tw_c, tw_line;
   // chroma per-line constants
@@ -134,18 +140,16 @@ struct DemodArgs {
   float* video;    // [T*spp] video - ire0
   float* sync;     // [T*spp] sync - ire0
   // Guard band: K1b lists every sync sample it writes within guard_hz of
-  // thr_rel (chunk index into guard_list, its done counter zeroed); the count
-  // may exceed guard_cap, which the host reports.  guard_list == null: off.
+  // thr_rel (chunk index into guard_list); the count may exceed guard_cap,
+  // which the host reports.  guard_list == null: off.
   float thr_rel = 0.0f, guard_hz = 0.0f;
   unsigned* guard_list = nullptr;
-  int* guard_done = nullptr;
   int* guard_count = nullptr;
   int guard_cap = 0;
 };
 
 // FP64 re-evaluation of the listed sync samples (kernels_guard.cu).
 constexpr float kGuardHz = 8.0f;   // half-width of the guard band: >= 4x the largest FP32 sync error measured
-constexpr int kGuardMaxParts = 33;  // CTAs per flagged sample at the largest sync support (2 * 4096 + 1 taps)
 constexpr int kGuardCap = 65536;    // flagged samples one chunk can list
 struct GuardArgs {
   const uint8_t* raw;
@@ -153,7 +157,8 @@ struct GuardArgs {
   const float* dc;
   long long total;  // T * spp: the demodulated chunk extent
   int spp, tile;
-  const double* ga64;  // K1a taps, offsets [-ha, ha], interleaved re, im
+  const double2* gfft;  // [Design::kGuardN] FFT of the K1a taps (offsets [-ha, ha]) / kGuardN
+  const double2* tw;    // [Design::kGuardN] exp(-2 pi i k / kGuardN)
   int ha;
   const double* hs64;  // sync taps, offsets [-hb, hb]
   int hb;
@@ -164,11 +169,13 @@ struct GuardArgs {
   const unsigned* list;
   const int* count;
   int cap;
-  int* done;
-  double* part;    // [cap * kGuardMaxParts]
   double* values;  // optional [cap]: the FP64 sync value of each listed sample
+  long long* dbg_clk = nullptr;  // optional [kGuardClockSamples][kPhaseSlots]: SM clock at each phase of a sample's CTA
 };
-int guard_parts(int hb);
+constexpr int kGuardClockSamples = 1024;
+// Whether the guard handles these tap supports, and its shared memory.
+bool guard_supported(int ha, int hb);
+size_t guard_smem_bytes(int hb);
 cudaError_t launch_sync_guard(const GuardArgs& g, cudaStream_t st);
 // K1a over tiles [f0, f0 + nf).
 void launch_k1a(const DemodArgs& a, int f0, int nf, cudaStream_t st);
@@ -304,7 +311,17 @@ struct FieldPrep {
   double mll = 0.0;
   double raw0 = 0.0;    // first raw pulse start, the fallback grid origin
   int n_raw = 0;
+  int vn = 0;           // validated entries
   int spec_first = -1;  // field order of the speculative anchor, -1 if none
+  // the field-order vote of the blanking pattern, which needs no carried
+  // state: the order with no previous field, and each order's vote (percent,
+  // when the pattern saw any interval)
+  int pat_default = 1;
+  int c_first = 0, c_second = 0;
+  // the chunk's first field is fitted with the chunk's incoming state (known
+  // when the per-field pass runs): exact = 1, its order in exact_first and
+  // its fit in spec
+  int exact = 0, exact_first = 0;
   BlankingScan scan;
   AnchorFit spec;
 };
@@ -342,6 +359,7 @@ struct LineLocArgs {
   long long raw_offset;  // capture position of the chunk
   int single_pass;
   int *dbg_vs = nullptr, *dbg_vl = nullptr, *dbg_vt = nullptr, *dbg_vn = nullptr;  // optional: validated pulses
+  long long* dbg_clk = nullptr;  // optional [num_fields][kPhaseSlots]: SM clock at each phase of a field's CTAs
 };
 size_t lineloc_smem_bytes();
 // VSYNC clustering into field windows (one CTA).

@@ -246,6 +246,29 @@ void Design::build(const Format& fmt) {
       ga64[(size_t)(m + ga64_half) * 2] = v.real();
       ga64[(size_t)(m + ga64_half) * 2 + 1] = v.imag();
     }
+    {
+      const int N = kGuardN;
+      std::vector<cd> w(N);
+      for (int k = 0; k < N; k++) w[k] = std::polar(1.0, -2.0 * kPi * (double)k / (double)N);
+      guard_tw.resize((size_t)N * 2);
+      for (int k = 0; k < N; k++) {
+        guard_tw[(size_t)k * 2] = w[k].real();
+        guard_tw[(size_t)k * 2 + 1] = w[k].imag();
+      }
+      guard_g.assign((size_t)N * 2, 0.0);
+      if (2 * ga64_half + 1 <= N) {
+        for (int k = 0; k < N; k++) {
+          cd acc(0.0, 0.0);
+          for (int m = -ga64_half; m <= ga64_half; m++) {
+            const cd tap(ga64[(size_t)(m + ga64_half) * 2], ga64[(size_t)(m + ga64_half) * 2 + 1]);
+            const long long e = ((long long)m * k % N + N) % N;
+            acc += tap * w[(size_t)e];
+          }
+          guard_g[(size_t)k * 2] = acc.real() / N;
+          guard_g[(size_t)k * 2 + 1] = acc.imag() / N;
+        }
+      }
+    }
     std::vector<cd> blk;
     a_tail = place_kernel(g, a_neg, a_pos, kNa, blk);
     std::vector<cd> G = host_dft(blk, -1);

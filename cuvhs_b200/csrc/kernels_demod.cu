@@ -222,7 +222,6 @@ __device__ __forceinline__ void k1b_emit(const DemodArgs& a, const float2 (&z)[1
         const int slot = atomicAdd(a.guard_count, 1);
         if (slot < a.guard_cap) {
           a.guard_list[slot] = (unsigned)(out0 + i);
-          a.guard_done[slot] = 0;
         }
       }
     }

@@ -19,15 +19,15 @@
 // where tile positions wrap mod the tile length and chunk positions clamp to
 // the demodulated range (src/pipeline/fm_demod.cu:133-169, 396-485).
 //
-// Work: one flagged sample is split over `parts` CTAs, each CTA evaluating 256
-// of the 2*hb + 1 demod samples of the sync window.  Where those positions
-// lie inside one tile away from its wrap and the chunk ends (nearly always),
-// the CTA stages their raw window once in shared memory as FP64 and computes
-// each analytic-signal value once (one FP64 dot product of 2*ha + 1 taps per
-// position); elsewhere each thread evaluates its position with the tile wrap
-// and chunk clamp (two dot products).  Each CTA writes its
-// partial sum; the CTA that finishes a sample last (an atomic count, no
-// waiting) adds the partials in part order, so the result is deterministic.
+// Work: one CTA per listed sample.  The 2*hb + 1 demod positions the sample's
+// sync sum reads split into a few runs -- consecutive chunk positions of one
+// owning tile, or one clamped position repeated -- and each run's analytic
+// signal is one FP64 overlap-save convolution: its raw window (tile wrap and
+// chunk clamp applied per sample) goes through a 4096-point FP64 FFT in shared
+// memory, is multiplied by the FFT of the truncated taps and transformed back,
+// giving every z of up to 4095 - 2*ha consecutive positions at once.  The
+// phase differences fill a demod array indexed like the sync taps, and the
+// sync sum is taken in a fixed order, so the result is deterministic.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,192 +39,264 @@
 namespace cuvhs {
 namespace {
 
-constexpr int kGuardThreads = 256;
+constexpr int kGT = 1024;                 // threads per CTA
+constexpr int kN = Design::kGuardN;       // FFT length
+constexpr int kBfly = kN / 4 / kGT;       // radix-4 butterflies per thread per pass
+constexpr int kTwQ = kN / 4;              // twiddles held in shared memory: exp(-2 pi i k / kN), k < kN / 4
 constexpr double kPi64 = 3.14159265358979323846;
 constexpr double kTau64 = 2.0 * kPi64;
+static_assert(kN == 4096 && kBfly >= 1 && kN / 4 % kGT == 0, "the FFT passes assume 4096 points");
 
 __device__ __forceinline__ long long wrap_pos(long long q, long long tile) {
   return q < 0 ? q + tile : (q >= tile ? q - tile : q);
 }
 
-// Converted sample at chunk position p (already clamped to the chunk): 0 past
-// the samples read, DC removed.
-template <int FMT>
-__device__ __forceinline__ double raw64(const GuardArgs& g, long long p, double dc) {
-  if (p >= g.n_read) return 0.0;
-  return (double)raw_convert<FMT>(g.raw, (int)p) - dc;
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// z(J) of tile f2 at tile positions J for the kGuardThreads demod positions
-// of one CTA, when they are consecutive inside one tile and their raw windows
-// need no wrap, clamp or zero fill: the raw window is staged once as FP64
-// (converted, DC removed) and each analytic-signal value is computed once.
-// Returns false (nothing written) when the CTA's positions are not of that
-// kind; the caller then evaluates every position on its own.
-struct GuardSmem {
-  double2* taps;  // [2*ha + 3]
-  double* xs;     // [kGuardThreads + 2*ha + 2] staged raw
-  double2* z;     // [kGuardThreads + 1]
-};
-
-template <int FMT>
-__device__ bool stage_interior(const GuardArgs& g, const GuardSmem& sm, long long c_first, int count, double dc) {
-  // positions c_first, c_first - 1, ..., c_first - count + 1 and one more for z(J2 - 1)
-  const long long c_last = c_first - count;  // the extra position (z only)
-  const long long last = g.total - 1;
-  if (c_last < 0) return false;
-  const long long f2 = c_first / g.spp;
-  if (c_last / g.spp != f2 || c_last - f2 * g.spp < 0) return false;
-  const long long tile0 = f2 * g.spp - kOverlap;
-  const long long J_hi = c_first - tile0, J_lo = c_last - tile0;  // tile positions
-  const long long u_lo = J_lo - g.ha, u_hi = J_hi + g.ha;
-  if (u_lo < 0 || u_hi >= g.tile || tile0 + u_lo < 0 || tile0 + u_hi > last || tile0 + u_hi >= g.n_read)
-    return false;
-  const int nx = (int)(u_hi - u_lo + 1);
-  for (int i = threadIdx.x; i < nx; i += kGuardThreads)
-    sm.xs[i] = (double)raw_convert<FMT>(g.raw, (int)(tile0 + u_lo + i)) - dc;
-  __syncthreads();
-  // thread t: z at tile position J_hi - t; z(J) = sum_m g[m] x(J - m)
-  const int t = threadIdx.x;
-  auto zdot = [&](long long J, int m0, int m1) {
-    double2 acc = make_double2(0.0, 0.0);
-    const double* xp = sm.xs + (J - u_lo);
-    for (int m = m0; m < m1; m++) {
-      const double2 a = sm.taps[m + g.ha + 1];
-      const double x = xp[-m];
-      acc.x = fma(a.x, x, acc.x);
-      acc.y = fma(a.y, x, acc.y);
-    }
-    return acc;
-  };
-  if (t < count) sm.z[t] = zdot(J_hi - t, -g.ha, g.ha + 1);
-  // the extra position, split over the first warp
-  if (t < 32) {
-    const int per = (2 * g.ha + 1 + 31) / 32;
-    const int m0 = -g.ha + t * per, m1 = min(m0 + per, g.ha + 1);
-    double2 acc = m0 < m1 ? zdot(J_lo, m0, m1) : make_double2(0.0, 0.0);
-    for (int off = 16; off > 0; off >>= 1) {
-      acc.x += __shfl_down_sync(0xffffffffu, acc.x, off);
-      acc.y += __shfl_down_sync(0xffffffffu, acc.y, off);
-    }
-    if (t == 0) sm.z[count] = acc;
+// exp(-2 pi i j / kN) for j < 3 kN / 4 from the quarter table: the quadrant
+// q = j / (kN / 4) multiplies by (-i)^q.
+__device__ __forceinline__ double2 twiddle(const double2* tq, int j) {
+  const double2 w = tq[j & (kTwQ - 1)];
+  switch (j / kTwQ) {
+    case 0: return w;
+    case 1: return make_double2(w.y, -w.x);
+    default: return make_double2(-w.x, -w.y);
   }
-  __syncthreads();
-  return true;
+}
+
+// In-place radix-4 Stockham FFT of kN points in shared memory (every thread
+// holds its butterflies' inputs in registers across a barrier, so one buffer
+// serves as source and destination).  tq: the quarter twiddle table; the
+// inverse conjugates the twiddles and is unnormalised.
+template <bool kInverse>
+__device__ void fft_n(double2* buf, const double2* tq) {
+  const int t = threadIdx.x;
+  for (int ns = 1; ns < kN; ns *= 4) {
+    double2 v[kBfly][4];
+#pragma unroll
+    for (int b = 0; b < kBfly; b++) {
+      const int j = t + b * kGT;
+#pragma unroll
+      for (int r = 0; r < 4; r++) v[b][r] = buf[j + r * (kN / 4)];
+    }
+    __syncthreads();
+    const int stride = kN / (4 * ns);
+#pragma unroll
+    for (int b = 0; b < kBfly; b++) {
+      const int j = t + b * kGT;
+      const int k = j & (ns - 1);
+#pragma unroll
+      for (int r = 1; r < 4; r++) {
+        double2 w = twiddle(tq, r * k * stride);
+        if (kInverse) w.y = -w.y;
+        v[b][r] = cmul(v[b][r], w);
+      }
+      const double2 a0 = v[b][0], a1 = v[b][1], a2 = v[b][2], a3 = v[b][3];
+      const double2 s02 = make_double2(a0.x + a2.x, a0.y + a2.y), d02 = make_double2(a0.x - a2.x, a0.y - a2.y);
+      const double2 s13 = make_double2(a1.x + a3.x, a1.y + a3.y), d13 = make_double2(a1.x - a3.x, a1.y - a3.y);
+      // forward: X1 = d02 - i d13, X3 = d02 + i d13; the inverse swaps them
+      const double2 m = kInverse ? make_double2(-d13.y, d13.x) : make_double2(d13.y, -d13.x);  // -/+ i d13
+      const int base = (j / ns) * ns * 4 + k;
+      buf[base] = make_double2(s02.x + s13.x, s02.y + s13.y);
+      buf[base + ns] = make_double2(d02.x + m.x, d02.y + m.y);
+      buf[base + 2 * ns] = make_double2(s02.x - s13.x, s02.y - s13.y);
+      buf[base + 3 * ns] = make_double2(d02.x - m.x, d02.y - m.y);
+    }
+    __syncthreads();
+  }
+}
+
+// A run of the sample's demod positions: taps kk0..kk1 read chunk position
+// c0 + step * (kk - kk0), step -1 (consecutive positions of one owning tile)
+// or 0 (one clamped position).
+struct Run {
+  int kk0, kk1, step;
+  long long c0;
+};
+constexpr int kMaxRuns = 8;
+
+// Phase clocks for inspection (thread 0, first block of a sample only).
+__device__ __forceinline__ void phase_clock(const GuardArgs& g, int y, int k) {
+  if (g.dbg_clk && threadIdx.x == 0 && y < kGuardClockSamples) g.dbg_clk[(size_t)y * kPhaseSlots + k] = clock64();
 }
 
 template <int FMT>
-__global__ void __launch_bounds__(kGuardThreads) guard_kernel(GuardArgs g) {
+__global__ void __launch_bounds__(kGT) guard_kernel(GuardArgs g) {
   chain_wait();
-  extern __shared__ double2 smem2[];
-  __shared__ double red[kGuardThreads / 32];
+  extern __shared__ double2 gsm[];
+  double2* buf = gsm;                                        // [kN]
+  double2* tq = gsm + kN;                                    // [kTwQ]
+  double* dem = reinterpret_cast<double*>(gsm + kN + kTwQ);  // [2 * hb + 1], indexed like the sync taps
+  __shared__ Run runs[kMaxRuns];
+  __shared__ int nruns, skip;
+  __shared__ double red[kGT / 32];
   const int n_listed = min(*g.count, g.cap);
-  if ((int)blockIdx.y >= n_listed) return;  // whole CTA
-  const int t = threadIdx.x, part = blockIdx.x;
-  const int nt = 2 * g.ha + 3;
-  GuardSmem sm;
-  sm.taps = smem2;
-  sm.z = smem2 + nt;
-  sm.xs = reinterpret_cast<double*>(smem2 + nt + kGuardThreads + 1);
-  for (int i = t; i < nt; i += kGuardThreads)
-    sm.taps[i] = (i == 0 || i == nt - 1) ? make_double2(0.0, 0.0)
-                                         : make_double2(g.ga64[2 * (i - 1)], g.ga64[2 * (i - 1) + 1]);
-  __syncthreads();
+  const int t = threadIdx.x;
   const double dc = g.dc ? (double)*g.dc : 0.0;
-  const int W = 2 * g.hb + 1;
   const long long last = g.total - 1;
-  for (int y = blockIdx.y; y < n_listed; y += gridDim.y) {
+  const int W = 2 * g.hb + 1;
+  const int V = kN - 1 - 2 * g.ha;  // demod positions one FFT block yields
+  if ((int)blockIdx.x >= n_listed) return;  // whole CTA
+  for (int k = t; k < kTwQ; k += kGT) tq[k] = __ldg(&g.tw[k]);
+  __syncthreads();
+  for (int y = blockIdx.x; y < n_listed; y += gridDim.x) {
     const long long s = g.list[y];
     const long long f = s / g.spp;
     const long long J = kOverlap + (s - f * g.spp);
-    const int kk0 = part * kGuardThreads, kk = kk0 + t;
-    const int count = min(kGuardThreads, W - kk0);
-    // demod sample at tile position J - k of tile f (k = kk - hb), chunk position c
-    auto chunk_pos = [&](int k_index) {
-      const long long q = wrap_pos(J - (k_index - g.hb), g.tile);
-      return min(max(f * g.spp + q - kOverlap, 0LL), last);
-    };
-    // the CTA's positions are consecutive (decreasing) when neither the tile
-    // wrap nor the chunk clamp falls inside them
-    const long long q_first = J - (kk0 - g.hb), q_end = J - (kk0 + count - 1 - g.hb);
-    const bool consecutive = q_end >= 0 && q_first < g.tile && f * g.spp + q_end - kOverlap >= 0 &&
-                             f * g.spp + q_first - kOverlap <= last;
-    const long long c_first = chunk_pos(kk0);
-    double contrib = 0.0;
-    if (consecutive && stage_interior<FMT>(g, sm, c_first, count, dc)) {
-      if (t < count) {
-        const double2 z0 = sm.z[t], z1 = sm.z[t + 1];
-        double d = atan2(z0.y, z0.x) - atan2(z1.y, z1.x);  // k_unwrap_to_hz (fm_demod.cu:222-244)
-        if (d > kPi64) d -= kTau64;
-        if (d < -kPi64) d += kTau64;
-        contrib = g.hs64[kk] * (d * g.scale);
+    phase_clock(g, y, 0);
+    if (t == 0) {
+      // tap kk reads tile position q = wrap(J + hb - kk), chunk position
+      // clamp(f * spp - kOverlap + q): one or two runs of q (the tile wrap),
+      // each cut where the clamp starts or the owning tile changes
+      int n = 0;
+      auto add_q_run = [&](int kk0, int kk1, long long q0) {
+        const long long c0 = f * g.spp - kOverlap + q0;  // unclamped, falls by one per tap
+        int kk = kk0;
+        while (kk <= kk1 && n < kMaxRuns) {
+          const long long c = c0 - (kk - kk0);
+          int kend;
+          if (c > last) {
+            kend = (int)min((long long)kk1, kk0 + (c0 - last) - 1);
+            runs[n++] = {kk, kend, 0, last};
+          } else if (c < 0) {
+            kend = kk1;
+            runs[n++] = {kk, kend, 0, 0};
+          } else {
+            const long long stop = (c / g.spp) * g.spp;  // the owning tile's first position
+            kend = (int)min((long long)kk1, kk + (c - stop));
+            runs[n++] = {kk, kend, -1, c};
+          }
+          kk = kend + 1;
+        }
+      };
+      const long long top = J + g.hb;  // q of tap 0 before the wrap
+      if (top >= g.tile) {
+        const int kw = (int)(top - g.tile);  // last tap whose q wraps
+        add_q_run(0, kw, top - g.tile);
+        add_q_run(kw + 1, W - 1, g.tile - 1);
+      } else {
+        add_q_run(0, W - 1, top);
       }
-    } else if (kk < W) {
-      const long long c = chunk_pos(kk);
-      const long long f2 = c / g.spp;
-      const long long J2 = kOverlap + (c - f2 * g.spp);
-      const long long tile0 = f2 * g.spp - kOverlap;  // chunk position of tile position 0
-      // raw tile positions J2 + ha down to J2 - 1 - ha feed z(J2) and z(J2 - 1)
-      const long long u_hi = J2 + g.ha;
-      double2 z0 = make_double2(0.0, 0.0), z1 = make_double2(0.0, 0.0);
-      const int nu = 2 * g.ha + 2;
-      for (int n = 0; n < nu; n++) {
-        const long long p = min(max(tile0 + wrap_pos(u_hi - n, g.tile), 0LL), last);
-        const double x = raw64<FMT>(g, p, dc);
-        const double2 a = sm.taps[n + 1], b = sm.taps[n];
-        z0.x = fma(a.x, x, z0.x);
-        z0.y = fma(a.y, x, z0.y);
-        z1.x = fma(b.x, x, z1.x);
-        z1.y = fma(b.y, x, z1.y);
+      nruns = n;
+      // A window that reaches the zero fill past the samples read (the
+      // capture's end) has analytic-signal values built from the taps' tails
+      // alone, whose phase no FP64 evaluation fixes (the FFT's rounding, the
+      // reference's included, exceeds them): such a sample keeps its FP32
+      // value.
+      int sk = 0;
+      if (g.n_read < g.total) {
+        for (int r = 0; r < n; r++) {
+          const long long owner = runs[r].c0 / g.spp;
+          const long long tile0 = owner * g.spp - kOverlap;
+          const long long vmax = (kOverlap + runs[r].c0 - owner * g.spp) + g.ha;  // highest tile position read
+          const long long pmax = min(tile0 + min(vmax, (long long)g.tile - 1), last);
+          if (pmax >= g.n_read) sk = 1;
+        }
       }
-      double d = atan2(z0.y, z0.x) - atan2(z1.y, z1.x);
-      if (d > kPi64) d -= kTau64;
-      if (d < -kPi64) d += kTau64;
-      contrib = g.hs64[kk] * (d * g.scale);
+      skip = sk;
     }
-    // fixed-order reduction: warp shuffle tree, then the warps in order
-    for (int off = 16; off > 0; off >>= 1) contrib += __shfl_down_sync(0xffffffffu, contrib, off);
-    if ((t & 31) == 0) red[t >> 5] = contrib;
+    __syncthreads();
+    if (skip) {
+      if (t == 0 && g.values) g.values[y] = __longlong_as_double(0x7ff8000000000000LL);
+      __syncthreads();  // runs and skip are rewritten for the next sample
+      continue;
+    }
+    for (int r = 0; r < nruns; r++) {
+      const Run run = runs[r];
+      const long long c_hi = run.c0, c_lo = run.c0 + (long long)run.step * (run.kk1 - run.kk0);
+      const long long owner = c_lo / g.spp;
+      const long long tile0 = owner * g.spp - kOverlap;  // chunk position of the owner's tile position 0
+      for (long long cb = c_lo; cb <= c_hi; cb += V) {
+        const long long ce = min(cb + V - 1, c_hi);
+        const int nz = (int)(ce - cb) + 2;             // z at tile positions J2(cb) - 1 .. J2(ce)
+        const long long v0 = (kOverlap + cb - owner * g.spp) - 1 - g.ha;  // tile position of buf[0]
+        const int L = nz + 2 * g.ha;
+        for (int u = t; u < kN; u += kGT) {
+          double x = 0.0;
+          if (u < L) {
+            const long long p = min(max(tile0 + wrap_pos(v0 + u, g.tile), 0LL), last);
+            x = p < g.n_read ? (double)raw_convert<FMT>(g.raw, (int)p) - dc : 0.0;
+          }
+          buf[u] = make_double2(x, 0.0);
+        }
+        __syncthreads();
+        const bool first_block = r == 0 && cb == c_lo;
+        if (first_block) phase_clock(g, y, 1);
+        fft_n<false>(buf, tq);
+        if (first_block) phase_clock(g, y, 2);
+#pragma unroll
+        for (int k = t; k < kN; k += kGT) buf[k] = cmul(buf[k], __ldg(&g.gfft[k]));
+        __syncthreads();
+        fft_n<true>(buf, tq);
+        if (first_block) phase_clock(g, y, 3);
+        // phases of the block's z, in place
+        for (int i = t; i < nz; i += kGT) {
+          const double2 z = buf[g.ha + i];
+          buf[g.ha + i].x = atan2(z.y, z.x);
+        }
+        __syncthreads();
+        // k_unwrap_to_hz (fm_demod.cu:222-244) for chunk positions cb .. ce
+        for (int i = t; i + 1 < nz; i += kGT) {
+          double d = buf[g.ha + i + 1].x - buf[g.ha + i].x;
+          if (d > kPi64) d -= kTau64;
+          if (d < -kPi64) d += kTau64;
+          const double hz = d * g.scale;
+          if (run.step == 0) {
+            for (int kk = run.kk0; kk <= run.kk1; kk++) dem[kk] = hz;  // one position, many taps
+          } else {
+            dem[run.kk0 + (int)(run.c0 - (cb + i))] = hz;
+          }
+        }
+        __syncthreads();  // buf is refilled by the next block
+        if (first_block) phase_clock(g, y, 4);
+      }
+    }
+    phase_clock(g, y, 5);
+    // sync sum in a fixed order: strided partials, warp tree, warps in order
+    double acc = 0.0;
+    for (int kk = t; kk < W; kk += kGT) acc += __ldg(&g.hs64[kk]) * dem[kk];
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((t & 31) == 0) red[t >> 5] = acc;
     __syncthreads();
     if (t == 0) {
-      double ps = 0.0;
-      for (int w = 0; w < kGuardThreads / 32; w++) ps += red[w];
-      g.part[(size_t)y * kGuardMaxParts + part] = ps;
-      __threadfence();
-      const int parts = (int)gridDim.x;
-      if (atomicAdd(&g.done[y], 1) == parts - 1) {
-        // every part of sample y is in: add them in part order
-        __threadfence();
-        double x64 = 0.0;
-        for (int p = 0; p < parts; p++) x64 += __ldcg(&g.part[(size_t)y * kGuardMaxParts + p]);
-        const bool in_pulse = x64 <= g.thr_hz;  // the reference's FP64 decision
-        float r = (float)(x64 - g.ire0);
-        if (in_pulse && !(r <= g.thr_rel)) r = g.thr_rel;
-        if (!in_pulse && r <= g.thr_rel) r = nextafterf(g.thr_rel, 3.0e38f);
-        g.sync[s] = r;
-        if (g.values) g.values[y] = x64;
-      }
+      double x64 = 0.0;
+      for (int w = 0; w < kGT / 32; w++) x64 += red[w];
+      const bool in_pulse = x64 <= g.thr_hz;  // the reference's FP64 decision
+      float r = (float)(x64 - g.ire0);
+      if (in_pulse && !(r <= g.thr_rel)) r = g.thr_rel;
+      if (!in_pulse && r <= g.thr_rel) r = nextafterf(g.thr_rel, 3.0e38f);
+      g.sync[s] = r;
+      if (g.values) g.values[y] = x64;
+      if (g.dbg_clk && y < kGuardClockSamples) g.dbg_clk[(size_t)y * kPhaseSlots + 7] = nruns;
     }
-    __syncthreads();  // red, z and xs are reused by the next sample
+    phase_clock(g, y, 6);
+    __syncthreads();  // runs, dem and red are reused by the next sample
   }
 }
 
 }  // namespace
 
-int guard_parts(int hb) { return (2 * hb + 1 + kGuardThreads - 1) / kGuardThreads; }
+size_t guard_smem_bytes(int hb) {
+  return (size_t)(kN + kTwQ) * sizeof(double2) + (size_t)(2 * hb + 1) * sizeof(double);
+}
+
+bool guard_supported(int ha, int hb) {
+  // one FFT block must yield at least one position, and the sync window must
+  // not wrap below the tile start (J - hb >= 0 for every J >= kOverlap)
+  return 2 * ha + 2 <= kN && hb < kOverlap && guard_smem_bytes(hb) <= (size_t)kMaxClassBytes;
+}
 
 cudaError_t launch_sync_guard(const GuardArgs& g, cudaStream_t st) {
-  const int parts = guard_parts(g.hb);
-  if (parts > kGuardMaxParts || g.cap <= 0) return cudaErrorInvalidValue;
-  const size_t smem = (size_t)(2 * g.ha + 3 + kGuardThreads + 1) * sizeof(double2) +
-                      (size_t)(kGuardThreads + 2 * g.ha + 2) * sizeof(double);
-  // enough rows to spread a typical chunk's few flagged samples over the GPU;
-  // rows past the listed count leave at once
-  const int rows = std::max(1, std::min(g.cap, (148 * 8 + parts - 1) / parts));
+  if (!guard_supported(g.ha, g.hb) || g.cap <= 0) return cudaErrorInvalidValue;
+  const size_t smem = guard_smem_bytes(g.hb);
+  // a typical chunk lists a few dozen samples, each on its own SM; two CTAs fit an SM
+  const int ctas = std::max(1, std::min(g.cap, 148 * 2));
   auto go = [&](auto kernel) {
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    return launch_chained(kernel, dim3(parts, rows), dim3(kGuardThreads), smem, st, g);
+    return launch_chained(kernel, dim3(ctas), dim3(kGT), smem, st, g);
   };
   if (g.in_fmt == kInS16) return go(guard_kernel<kInS16>);
   if (g.in_fmt == kInU16) return go(guard_kernel<kInU16>);

@@ -44,6 +44,12 @@ constexpr int kSmemValid = 2048;   // validated pulses held in shared memory
 
 __device__ __forceinline__ bool within(double v, double lo, double hi) { return v >= lo && v <= hi; }
 
+// Phase clocks for inspection: thread 0 records the SM clock at phase k of
+// field f's CTA when the caller asked for them.
+__device__ __forceinline__ void phase_clock(const LineLocArgs& a, int f, int k) {
+  if (a.dbg_clk && threadIdx.x == 0) a.dbg_clk[(size_t)f * kPhaseSlots + k] = clock64();
+}
+
 // ------------------------------------------------------------ field windows
 
 // First index in sorted a[0, n) whose value is > v.
@@ -67,47 +73,98 @@ __device__ __forceinline__ long long run_end(const LineLocArgs& a, int nrise, in
 
 // One CTA: VSYNC candidates (runs of 20-35 us, vsync_discover.cu:58-72) in
 // sample order, clustered into field windows (pipeline.cu:1567-1651).
-__global__ void __launch_bounds__(1024) fieldwin_kernel(LineLocArgs a) {
+//
+// Candidates: the falling edges are taken 1024 at a time, one per thread
+// (coalesced), and a block scan appends the candidates in order.  Clustering:
+// the reference opens a window at the first candidate and at every later
+// candidate more than half a field past the open window's start (the
+// candidate less five lines), so the window that follows candidate j opens at
+// the first candidate past off(j) + spf / 2 -- found for every candidate at
+// once by binary search -- and one thread follows that chain from the first
+// candidate, one step per field.
+constexpr int kWinThreads = 1024;
+constexpr int kWinSmemCand = 12288;  // candidates clustered in shared memory; more: the serial path
+size_t fieldwin_smem_bytes() { return (size_t)kWinSmemCand * 2 * sizeof(int); }
+
+__global__ void __launch_bounds__(kWinThreads) fieldwin_kernel(LineLocArgs a) {
   chain_wait();
-  __shared__ int warp_tot[32];
+  extern __shared__ int wsm[];
+  int* scand = wsm;                  // [kWinSmemCand] candidate positions
+  int* snext = wsm + kWinSmemCand;   // [kWinSmemCand] index of the next window's first candidate
+  __shared__ int warp_tot[kWinThreads / 32];
+  __shared__ int base_s;
   const int nfall = min(a.counts[0], a.edge_cap), nrise = min(a.counts[1], a.edge_cap);
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  if (t == 0) a.win->err = (a.counts[0] > a.edge_cap || a.counts[1] > a.edge_cap) ? 1 : 0;
-  // each thread a contiguous strip of falling edges: count, scan, write in order
-  const int per = (nfall + 1023) / 1024;
-  const int i0 = min(nfall, t * per), i1 = min(nfall, i0 + per);
-  auto is_cand = [&](int i) {
-    const long long w = run_end(a, nrise, i) - (long long)a.fall[i];
-    return w >= a.minw && w <= a.maxw;
-  };
-  int cnt = 0;
-  for (int i = i0; i < i1; i++) cnt += is_cand(i) ? 1 : 0;
-  int incl = cnt;
-  for (int off = 1; off < 32; off <<= 1) {
-    const int o = __shfl_up_sync(0xffffffffu, incl, off);
-    if (lane >= off) incl += o;
+  if (t == 0) {
+    a.win->err = (a.counts[0] > a.edge_cap || a.counts[1] > a.edge_cap) ? 1 : 0;
+    base_s = 0;
   }
-  if (lane == 31) warp_tot[warp] = incl;
   __syncthreads();
-  int before = 0, total = 0;
-  for (int w = 0; w < 32; w++) {
-    if (w < warp) before += warp_tot[w];
-    total += warp_tot[w];
+  // candidates in order, one tile of falling edges per step (the next tile's
+  // edges are loaded before the current tile's scan)
+  int nf = 0, nr = 0;
+  if (t < nfall) {
+    nf = (int)a.fall[t];
+    nr = t < nrise ? (int)a.rise[t] : 0;
   }
-  int k = before + incl - cnt;
-  for (int i = i0; i < i1 && k < a.cand_cap; i++)
-    if (is_cand(i)) a.cand[k++] = (int)a.fall[i];
-  __syncthreads();
-  const int base_s = total;
-  if (t != 0) return;
-  const int ncand = min(base_s, a.cand_cap);
+  for (int i0 = 0; i0 < nfall; i0 += kWinThreads) {
+    const int i = i0 + t;
+    const long long fpos = (unsigned)nf;
+    const long long end = i < nrise ? (long long)(unsigned)nr : a.total;  // run_end
+    const bool cand = i < nfall && end - fpos >= a.minw && end - fpos <= a.maxw;
+    const int j = i + kWinThreads;
+    if (j < nfall) {
+      nf = (int)a.fall[j];
+      nr = j < nrise ? (int)a.rise[j] : 0;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, cand);
+    if (lane == 0) warp_tot[warp] = __popc(m);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < kWinThreads / 32; w++) {
+      if (w < warp) before += warp_tot[w];
+      total += warp_tot[w];
+    }
+    const int k = base_s + before + __popc(m & ((1u << lane) - 1u));
+    if (cand) {
+      if (k < a.cand_cap) a.cand[k] = (int)fpos;
+      if (k < kWinSmemCand) scand[k] = (int)fpos;
+    }
+    __syncthreads();
+    if (t == 0) base_s += total;
+    __syncthreads();
+  }
+  const int base = base_s;
+  const int ncand = min(base, a.cand_cap);
   const long long spf = a.fmt.samples_per_field, spl = a.fmt.samples_per_line;
+  auto off_of = [&](long long pos) { return pos > 5 * spl ? pos - 5 * spl : 0LL; };
+  const bool in_smem = ncand <= kWinSmemCand;
+  if (in_smem) {
+    for (int j = t; j < ncand; j += kWinThreads) {
+      const long long lim = off_of(scand[j]) + spf / 2;  // the next window: first candidate past lim
+      int lo = j + 1, hi = ncand;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if ((long long)scand[mid] > lim) hi = mid;
+        else lo = mid + 1;
+      }
+      snext[j] = lo;
+    }
+  }
+  __syncthreads();
+  if (t != 0) return;
   int n = 0;
-  for (int j = 0; j < ncand; j++) {
-    const long long pos = a.cand[j];
-    if (n == 0 || pos - a.offs[n - 1] > spf / 2) {
-      if (n >= a.num_fields) break;  // later windows are cut off anyway
-      a.offs[n++] = pos > 5 * spl ? pos - 5 * spl : 0;
+  if (in_smem) {
+    for (int j = 0; j < ncand && n < a.num_fields; j = snext[j]) a.offs[n++] = off_of(scand[j]);
+  } else {
+    long long open = 0;
+    for (int j = 0; j < ncand; j++) {
+      const long long pos = a.cand[j];
+      if (n == 0 || pos - open > spf / 2) {
+        if (n >= a.num_fields) break;  // later windows are cut off anyway
+        open = off_of(pos);
+        a.offs[n++] = open;
+      }
     }
   }
   if (n == 0)
@@ -116,7 +173,7 @@ __global__ void __launch_bounds__(1024) fieldwin_kernel(LineLocArgs a) {
   if (n >= 2) actual = (a.offs[n - 1] - a.offs[0]) / (n - 1);
   const long long predicted = a.offs[n - 1] + actual, margin = 10 * spl;
   a.win->fields = n;
-  a.win->ncand = base_s;
+  a.win->ncand = base;
   a.win->next_rel = predicted > margin ? predicted - margin : predicted;
 }
 
@@ -330,6 +387,7 @@ __device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
   }
   lsum = block_sum_ll(lsum, sm.red);
   lcnt = block_sum_ll(lcnt, sm.red);
+  phase_clock(a, blockIdx.x, 21);
   const double est = lcnt > 0 ? ((double)lsum / (double)lcnt) : fmt.hsync_width;
   const double shift = est - fmt.hsync_width;
   Windows w;
@@ -355,6 +413,7 @@ __device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
     sm.att_last[i] = (unsigned char)last;
   }
   __syncthreads();
+  phase_clock(a, blockIdx.x, 22);
   // which attempts fire: at an EQ-width pulse while the list's last entry is
   // an hsync.  The list's state before pulse i -- empty, last entry an hsync,
   // or last entry something else -- follows from pulse i-1's state by a map
@@ -416,6 +475,7 @@ __device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
     if (lane == 31) sm.pos[n] = incl;
   }
   __syncthreads();
+  phase_clock(a, blockIdx.x, 23);
   const int nv = sm.pos[n];
   // place every pulse's output
   for (int i = t; i < n; i += kLT) {
@@ -438,12 +498,14 @@ __device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
     }
   }
   __syncthreads();
+  phase_clock(a, blockIdx.x, 24);
   // cadence flags from each entry's predecessor (pipeline.cu:133-148)
   for (int k = t; k < nv; k += kLT) {
     const bool good = k > 0 && spacing_ok(vtype(v, k - 1), vtype(v, k), v.s[k] - v.s[k - 1], fmt.samples_per_line);
     v.tg[k] = (unsigned char)(vtype(v, k) | (good ? 4 : 0));
   }
   __syncthreads();
+  phase_clock(a, blockIdx.x, 25);
   return nv;
 }
 
@@ -593,77 +655,115 @@ __device__ BlankingScan scan_blanking(FieldSmem& sm, const VList& v, double mll,
   return s;
 }
 
-__device__ bool decide_first(const BlankingScan& s, int prev_first, double prev_loc, int confidence) {
-  bool first;
-  if (prev_first == -1) first = s.seen == 0.0 || round(s.agree / fmax(1.0, s.seen)) == 1.0;
-  else first = !prev_first;
+// The blanking pattern's vote on the field order (pipeline.cu:729-745): the
+// parts of the decision that need no carried state.
+__device__ void pattern_vote(const BlankingScan& s, FieldPrep& p) {
+  p.pat_default = (s.seen == 0.0 || round(s.agree / fmax(1.0, s.seen)) == 1.0) ? 1 : 0;
+  p.c_first = p.c_second = 0;
   if (s.seen > 0.0) {
-    if (prev_loc < 0.0) confidence = min(confidence, 50);
     const double weight = s.seen / 4.0;
-    const int c_first = (int)llround((s.agree / s.seen) * weight * 100.0);
-    const int c_second = (int)llround(((s.seen - s.agree) / s.seen) * weight * 100.0);
-    if (c_first >= confidence && c_first > c_second) first = true;
-    else if (c_second >= confidence && c_second > c_first) first = false;
+    p.c_first = (int)llround((s.agree / s.seen) * weight * 100.0);
+    p.c_second = (int)llround(((s.seen - s.agree) / s.seen) * weight * 100.0);
+  }
+}
+
+// Field order from the previous field's and the vote (pipeline.cu:729-745).
+__device__ bool decide_first(const FieldPrep& p, int prev_first, double prev_loc, int confidence) {
+  bool first = prev_first == -1 ? p.pat_default != 0 : !prev_first;
+  if (p.scan.seen > 0.0) {
+    if (prev_loc < 0.0) confidence = min(confidence, 50);
+    if (p.c_first >= confidence && p.c_first > p.c_second) first = true;
+    else if (p.c_second >= confidence && p.c_second > p.c_first) first = false;
   }
   return first;
 }
 
-__device__ int pattern_first(const BlankingScan& s, int confidence) {
-  if (s.seen <= 0.0) return -1;
-  const double weight = s.seen / 4.0;
-  const int c_first = (int)llround((s.agree / s.seen) * weight * 100.0);
-  const int c_second = (int)llround(((s.seen - s.agree) / s.seen) * weight * 100.0);
-  if (c_first >= confidence && c_first > c_second) return 1;
-  if (c_second >= confidence && c_second > c_first) return 0;
+// The order the vote alone fixes, whatever the previous field: 1 first, 0
+// second, -1 none.
+__device__ int pattern_first(const FieldPrep& p, int confidence) {
+  if (p.scan.seen <= 0.0) return -1;
+  if (p.c_first >= confidence && p.c_first > p.c_second) return 1;
+  if (p.c_second >= confidence && p.c_second > p.c_first) return 0;
   return -1;
 }
 
 // First-hsync anchor for field order `first` (pipeline.cu:650-855).  The
-// scalar estimate runs on thread 0; the hsync-offset correction's terms are
-// formed in parallel and added in list order by thread 0.  Every thread gets
-// the result.
+// pairwise estimates are formed one per thread and combined by thread 0 in the
+// reference's order; the hsync-offset correction's terms are formed in
+// parallel and added in list order by thread 0.  Every thread gets the result.
 __device__ AnchorFit fit_anchor(FieldSmem& sm, const BlankingScan& s, const VList& v, double mll, const Format& fmt,
-                                bool first, double prev_off_lines, double prev_loc, double prev_diff) {
+                                bool first, double prev_off_lines, double prev_loc, double prev_diff,
+                                long long* clk = nullptr) {
   const int t = threadIdx.x;
+  auto stamp = [&](int k) {
+    if (clk && t == 0) clk[k] = clock64();
+  };
   __shared__ AnchorFit res;
   __shared__ double loc_s;
   __shared__ int go_s;
+  // pair estimates: 6 within each blanking interval, then 16 across them
+  constexpr int kPairs = 28;
+  __shared__ double pair_off[kPairs], pair_loc[kPairs];
+  __shared__ unsigned char pair_ok[kPairs];
   const double cur_lines = first ? fmt.field_lines_first : fmt.field_lines_second;
+  const double tol_lines = 0.5;
+  const double section = fmt.num_eq_pulses / 2.0;
+  const double* pat = field_pattern(fmt.system, first);
+  double vb_line[8];
+  vb_line[0] = 0.0 + pat[0];
+  vb_line[1] = vb_line[0] + section;
+  vb_line[2] = vb_line[1] + section;
+  vb_line[3] = vb_line[2] + section - 0.5;
+  const double hsync_line = vb_line[3] + pat[1];
+  vb_line[4] = cur_lines + pat[2];
+  vb_line[5] = vb_line[4] + section;
+  vb_line[6] = vb_line[5] + section;
+  vb_line[7] = vb_line[6] + section - 0.5;
+  const bool any = v.n > 0 && mll > 0.0;
+  if (any && t < kPairs) {
+    // pair t in the reference's loop order: (x < y) over slots 0..3, the same
+    // over slots 4..7, then (x, 4 + y) for x, y in 0..3
+    int i1, i2;
+    if (t < 12) {
+      const int q = t % 6;
+      const int x = q < 3 ? 0 : (q < 5 ? 1 : 2);
+      const int y = q < 3 ? q + 1 : (q < 5 ? q - 1 : 3);
+      i1 = x + (t < 6 ? 0 : 4);
+      i2 = y + (t < 6 ? 0 : 4);
+    } else {
+      i1 = (t - 12) >> 2;
+      i2 = 4 + ((t - 12) & 3);
+    }
+    const int p1 = s.vb_pulse[i1], p2 = s.vb_pulse[i2];
+    bool ok = false;
+    if (p1 != -1 && p2 != -1 && mll != 0.0) {
+      const double actual = ((double)p1 - (double)p2) / mll;
+      const double expect = vb_line[i1] - vb_line[i2];
+      if (actual < expect + tol_lines && actual > expect - tol_lines) {
+        ok = true;
+        pair_off[t] = actual - expect;
+        pair_loc[t] = (double)p2 + mll * (hsync_line - vb_line[i2]);
+      }
+    }
+    pair_ok[t] = ok ? 1 : 0;
+  }
+  __syncthreads();
+  stamp(26);
   if (t == 0) {
     AnchorFit out;
     go_s = 0;
-    if (v.n > 0 && mll > 0.0) {
-      const double tol_lines = 0.5;
-      const double section = fmt.num_eq_pulses / 2.0;
+    if (any) {
       const double pred_lines = predicted_field_lines(fmt, first);
-      const double* pat = field_pattern(fmt.system, first);
-      double vb_line[8];
-      vb_line[0] = 0.0 + pat[0];
-      vb_line[1] = vb_line[0] + section;
-      vb_line[2] = vb_line[1] + section;
-      vb_line[3] = vb_line[2] + section - 0.5;
-      const double hsync_line = vb_line[3] + pat[1];
-      vb_line[4] = cur_lines + pat[2];
-      vb_line[5] = vb_line[4] + section;
-      vb_line[6] = vb_line[5] + section;
-      vb_line[7] = vb_line[6] + section - 0.5;
+      auto add = [&](int k, double& loc, int& cnt, double& off) {
+        if (!pair_ok[k]) return;
+        off += pair_off[k];
+        loc += pair_loc[k];
+        cnt += 1;
+      };
       double a_loc = 0.0, a_off = 0.0, b_loc = 0.0, b_off = 0.0;
       int a_cnt = 0, b_cnt = 0;
-      auto pair_estimate = [&](int i1, int i2, double& loc, int& cnt, double& off) {
-        const int p1 = s.vb_pulse[i1], p2 = s.vb_pulse[i2];
-        if (p1 == -1 || p2 == -1 || mll == 0.0) return;
-        const double actual = ((double)p1 - (double)p2) / mll;
-        const double expect = vb_line[i1] - vb_line[i2];
-        if (actual < expect + tol_lines && actual > expect - tol_lines) {
-          off += actual - expect;
-          loc += (double)p2 + mll * (hsync_line - vb_line[i2]);
-          cnt += 1;
-        }
-      };
-      for (int x = 0; x < 4; x++)
-        for (int y = x + 1; y < 4; y++) pair_estimate(x, y, a_loc, a_cnt, a_off);
-      for (int x = 0; x < 4; x++)
-        for (int y = x + 1; y < 4; y++) pair_estimate(4 + x, 4 + y, b_loc, b_cnt, b_off);
+      for (int k = 0; k < 6; k++) add(k, a_loc, a_cnt, a_off);
+      for (int k = 6; k < 12; k++) add(k, b_loc, b_cnt, b_off);
       double loc = 0.0, off = 0.0;
       int cnt = 0;
       const double a_est = a_cnt ? a_loc / a_cnt : 0.0, b_est = b_cnt ? b_loc / b_cnt : 0.0;
@@ -671,8 +771,7 @@ __device__ AnchorFit fit_anchor(FieldSmem& sm, const BlankingScan& s, const VLis
         loc = a_loc + b_loc;
         cnt = a_cnt + b_cnt;
         off = a_off + b_off;
-        for (int x = 0; x < 4; x++)
-          for (int y = 0; y < 4; y++) pair_estimate(x, 4 + y, loc, cnt, off);
+        for (int k = 12; k < kPairs; k++) add(k, loc, cnt, off);
       } else if (a_cnt == 6 || (prev_loc <= 0.0 && a_cnt > b_cnt)) {
         loc = a_loc;
         cnt = a_cnt;
@@ -704,6 +803,7 @@ __device__ AnchorFit fit_anchor(FieldSmem& sm, const BlankingScan& s, const VLis
     sm.imin = INT_MAX;
   }
   __syncthreads();
+  stamp(27);
   if (!go_s) {
     const AnchorFit r = res;
     __syncthreads();
@@ -711,7 +811,7 @@ __device__ AnchorFit fit_anchor(FieldSmem& sm, const BlankingScan& s, const VLis
   }
   // hsync-offset correction: terms of the hsync entries before the first one
   // past the field's last line
-  const double loc = loc_s, hsync_line = res.hsync_line;
+  const double loc = loc_s;
   for (int k = t; k < v.n; k += kLT) {
     double term = __longlong_as_double(0x7ff8000000000000LL);  // NaN: not counted
     if (vtype(v, k) == kHsync && vgood(v, k)) {
@@ -723,10 +823,12 @@ __device__ AnchorFit fit_anchor(FieldSmem& sm, const BlankingScan& s, const VLis
     v.d[k] = term;
   }
   __syncthreads();
+  stamp(28);
   if (t == 0) {
     const int end = min(sm.imin, v.n);
     double hoff = 0.0;
     int hcnt = 0;
+#pragma unroll 8
     for (int k = 0; k < end; k++) {
       const double x = v.d[k];
       if (x == x) {
@@ -742,6 +844,7 @@ __device__ AnchorFit fit_anchor(FieldSmem& sm, const BlankingScan& s, const VLis
     res.loc = l;
   }
   __syncthreads();
+  stamp(29);
   const AnchorFit r = res;
   __syncthreads();
   return r;
@@ -797,36 +900,102 @@ __device__ const double* sorted_starts(FieldSmem& sm, const VList& v) {
 }
 
 // Nominal line grid snapped to the nearest pulse (pipeline.cu:857-893).
+//
+// The reference walks the lines with a cursor into the sorted starts: from
+// the cursor it steps right while the distance to the line's nominal position
+// does not grow, takes the last position checked (the walk checks no position
+// past the second-to-last) if it is within mll / 1.5, and moves the cursor
+// past it.  The distances to sorted starts fall to a minimum and then grow, so
+// from any cursor at or before S -- the first index whose successor is
+// strictly farther -- the walk stops at S.  Each thread therefore finds S of
+// its lines by binary search; one warp then carries the cursor over the lines,
+// 32 at a time: while every line meets a cursor at or before its S, the cursor
+// is a running maximum (a warp scan), and a line whose S lies behind the
+// cursor (its pulse taken by an earlier line) is walked from the cursor by one
+// lane, as the reference does.
 __device__ void snap_lines(FieldSmem& sm, const VList& v, double ref_pos, double ref_line, double mll, int nlines,
                            double* locs) {
   const double* ps = sorted_starts(sm, v);
-  if (threadIdx.x == 0) {
-    const int np = v.n;
-    const double max_dist = mll / 1.5;
-    int cur = 0;
-    for (int line = 0; line < nlines; line++) {
-      const double expect = ref_pos + mll * ((double)line - ref_line);
-      locs[line] = expect;
-      if (cur >= np) continue;
-      double d = fabs(ps[cur] - expect);
-      double best = max_dist, at = -1.0;
-      int s = cur;
-      while (s + 1 < np) {
-        if (d <= best) {
-          best = d;
-          cur = s;
-          at = ps[s];
-        }
-        const double nd = fabs(ps[s + 1] - expect);
-        if (nd > d) break;
-        d = nd;
-        s++;
+  const int t = threadIdx.x, np = v.n;
+  const double max_dist = mll / 1.5;
+  int* stop = sm.pos;      // per line: S capped at np - 2, << 1 | within max_dist
+  int* taken = sm.att_len; // per line: the pulse it snaps to, or -1
+  auto expect_of = [&](int line) { return ref_pos + mll * ((double)line - ref_line); };
+  auto dist = [&](int i, double e) { return fabs(ps[i] - e); };
+  if (np >= 2) {
+    for (int line = t; line < nlines; line += kLT) {
+      const double e = expect_of(line);
+      int lo = 0, hi = np;  // first start strictly after e
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (ps[mid] - e > 0.0) hi = mid;
+        else lo = mid + 1;
       }
-      if (at >= 0.0) {
-        locs[line] = at;
-        cur++;
+      int sx;
+      if (lo >= 1 && lo < np && dist(lo, e) > dist(lo - 1, e)) {
+        sx = lo - 1;
+      } else {
+        sx = min(lo, np - 1);
+        while (sx + 1 < np && !(dist(sx + 1, e) > dist(sx, e))) sx++;
+      }
+      sx = min(sx, np - 2);
+      stop[line] = (sx << 1) | (dist(sx, e) <= max_dist ? 1 : 0);
+      taken[line] = -1;
+    }
+  }
+  __syncthreads();
+  if (t < 32) {
+    const int lane = t;
+    int cur = 0;
+    // a cursor at the last start (or past it) takes no more pulses: the walk ends
+    for (int g = 0; g < nlines && cur < np - 1; g += 32) {
+      const int line = g + lane;
+      const bool in = line < nlines && np >= 2;
+      const int code = in ? stop[line] : 0;
+      const int sx = code >> 1;
+      const bool near = (code & 1) != 0;
+      int k = 0;  // lanes below k are settled
+      while (k < 32 && g + k < nlines && cur < np - 1) {
+        // cursor met by each lane if lanes k .. lane-1 all stop at their S
+        int incl = (in && lane >= k && near) ? sx + 1 : INT_MIN;
+        for (int off = 1; off < 32; off <<= 1) {
+          const int o = __shfl_up_sync(0xffffffffu, incl, off);
+          if (lane >= off) incl = max(incl, o);
+        }
+        int excl = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) excl = INT_MIN;
+        const int c = max(cur, excl);
+        const unsigned behind = __ballot_sync(0xffffffffu, in && lane >= k && c > sx);
+        const int kb = behind ? __ffs(behind) - 1 : 32;
+        if (lane >= k && lane < kb && line < nlines) taken[line] = (in && near) ? sx : -1;
+        const int settled = __shfl_sync(0xffffffffu, max(cur, incl), max(kb - 1, 0));
+        if (kb > k) cur = settled;
+        if (kb >= 32 || g + kb >= nlines) break;
+        // line g + kb: its pulse is behind the cursor; walk from the cursor
+        int nc = cur;
+        if (lane == kb) {
+          int got = -1;
+          if (cur < np - 1) {
+            const double e = expect_of(line);
+            int w = cur;
+            while (w + 1 < np && !(dist(w + 1, e) > dist(w, e))) w++;
+            w = min(w, np - 2);
+            if (dist(w, e) <= max_dist) {
+              got = w;
+              nc = w + 1;
+            }
+          }
+          taken[line] = got;
+        }
+        cur = __shfl_sync(0xffffffffu, nc, kb);
+        k = kb + 1;
       }
     }
+  }
+  __syncthreads();
+  for (int line = t; line < nlines; line += kLT) {
+    const int k = np >= 2 ? taken[line] : -1;
+    locs[line] = k >= 0 ? ps[k] : expect_of(line);
   }
   __syncthreads();
 }
@@ -850,14 +1019,17 @@ __global__ void __launch_bounds__(kLT) prepare_kernel(LineLocArgs a) {
   FieldSmem& sm = *reinterpret_cast<FieldSmem*>(smem_d);
   const int f = blockIdx.x, t = threadIdx.x;
   if (f >= a.win->fields) return;
+  phase_clock(a, f, 0);
   const int n = min(max(a.pn[f], 0), kMaxPulses);
   for (int i = t; i < n; i += kLT) {
     sm.ps[i] = a.ps[(size_t)f * kMaxPulses + i];
     sm.pl[i] = a.pl[(size_t)f * kMaxPulses + i];
   }
   __syncthreads();
+  phase_clock(a, f, 1);
   VList vg = field_vlist(a, f);
   vg.n = n > 0 ? validate(a, sm, n, vg) : 0;
+  phase_clock(a, f, 2);
   if (t == 0) a.vn[f] = vg.n;
   VList v = vg;
   if (vg.n <= kSmemValid) {  // work from shared memory
@@ -870,24 +1042,58 @@ __global__ void __launch_bounds__(kLT) prepare_kernel(LineLocArgs a) {
     v.d = sm.sort;  // anchor-offset terms; the sort that reuses it comes after
     __syncthreads();
   }
+  phase_clock(a, f, 3);
   const double mll = mean_line(sm, v, (double)a.fmt.samples_per_line);
+  phase_clock(a, f, 4);
   const BlankingScan scan = scan_blanking(sm, v, mll, a.fmt);
+  phase_clock(a, f, 5);
   FieldPrep p;
   p.mll = mll;
   p.n_raw = n;
+  p.vn = vg.n;
   p.raw0 = n > 0 ? (double)sm.ps[0] : 0.0;
   p.scan = scan;
   p.spec_first = -1;
-  const int pf = v.n > 0 ? pattern_first(scan, kAnchorConfidence) : -1;
-  if (pf >= 0) {
-    const AnchorFit fit = fit_anchor(sm, scan, v, mll, a.fmt, pf == 1, 0.0, 1.0, 0.0);
+  pattern_vote(scan, p);
+  const int pf = v.n > 0 ? pattern_first(p, kAnchorConfidence) : -1;
+  if (f == 0) {
+    // the chunk's first field: its incoming state is the chunk's, so the
+    // in-order pass's fit is computed here
+    const LineLocState st = *a.state;
+    p.exact = 1;
+    if (v.n > 0 && mll > 0.0) {
+      const bool first = decide_first(p, st.prev_first_field, st.prev_first_hsync_loc, kAnchorConfidence);
+      const long long readloc = a.raw_offset + a.offs[0];
+      const double prev_off = (st.prev_first_hsync_readloc != -1 && mll > 0.0)
+                                  ? ((double)st.prev_first_hsync_readloc - (double)readloc) / mll
+                                  : 0.0;
+      const AnchorFit fit = fit_anchor(sm, scan, v, mll, a.fmt, first, prev_off, st.prev_first_hsync_loc,
+                                       st.prev_first_hsync_diff, a.dbg_clk ? a.dbg_clk + (size_t)f * kPhaseSlots : nullptr);
+      phase_clock(a, f, 6);
+      if (fit.cnt > 0)
+        snap_lines(sm, v, fit.loc, fit.hsync_line, mll, a.fmt.lines_per_frame, a.ll + (size_t)f * a.fmt.lines_per_frame);
+      phase_clock(a, f, 7);
+      p.exact_first = first ? 1 : 0;
+      p.spec = fit;
+    }
+  } else if (pf >= 0) {
+    const AnchorFit fit = fit_anchor(sm, scan, v, mll, a.fmt, pf == 1, 0.0, 1.0, 0.0,
+                                     a.dbg_clk ? a.dbg_clk + (size_t)f * kPhaseSlots : nullptr);
+    phase_clock(a, f, 6);
     if (fit.cnt > 0 && !fit.used_prediction) {
       snap_lines(sm, v, fit.loc, fit.hsync_line, mll, a.fmt.lines_per_frame, a.ll + (size_t)f * a.fmt.lines_per_frame);
       p.spec_first = pf;
       p.spec = fit;
     }
+    phase_clock(a, f, 7);
   }
   if (t == 0) a.prep[f] = p;
+  phase_clock(a, f, 8);
+  if (a.dbg_clk && t == 0) {
+    a.dbg_clk[(size_t)f * kPhaseSlots + 9] = vg.n;
+    a.dbg_clk[(size_t)f * kPhaseSlots + 10] = pf;
+    a.dbg_clk[(size_t)f * kPhaseSlots + 11] = n;
+  }
   // validated pulses for inspection (the first kMaxPulses)
   if (a.dbg_vn) {
     const int kept = min(v.n, kMaxPulses);
@@ -901,81 +1107,172 @@ __global__ void __launch_bounds__(kLT) prepare_kernel(LineLocArgs a) {
 }
 
 // One CTA: the fields in order with the carried state (pipeline.cu:1717-1778).
-// The state stays in shared memory for the whole walk and the fields'
-// records are fetched kPrepBatch at a time, so a field whose speculative
-// grid stands costs a few hundred cycles; a field that needs its anchor fitted
-// (the capture's first field, or an order its own pattern did not fix) is fitted
-// and snapped by the whole CTA.
-constexpr int kPrepBatch = 32;
+// Thread 0 walks the fields' records (fetched kPrepBatch at a time into shared
+// memory) with the state in shared memory: where a field's speculative grid
+// stands -- its pattern fixed the order the walk decides, and a previous field
+// anchored the capture -- the step is a few integer decisions.  A field that
+// needs its anchor fitted (the capture's first field, or an order its own
+// pattern did not fix) stops the walk; the whole CTA fits and snaps it from
+// its validated list staged in shared memory, and the walk goes on.  The
+// carried hsync difference, a few FP64 divisions, is formed only when a fit
+// or the next chunk reads it.
+constexpr int kPrepBatch = 64;
 __global__ void __launch_bounds__(kLT) finish_kernel(LineLocArgs a) {
   chain_wait();
   extern __shared__ double smem_d[];
   FieldSmem& sm = *reinterpret_cast<FieldSmem*>(smem_d);
   __shared__ FieldPrep preps[kPrepBatch];
+  __shared__ long long readlocs[kPrepBatch];
+  __shared__ unsigned char fallback[kPrepBatch];
   __shared__ LineLocState st;
-  __shared__ int need_fit, first_s, valid_s;
+  __shared__ int fit_j, fit_first;
   __shared__ double prev_off_s, prev_loc_s, prev_diff_s;
   const int t = threadIdx.x;
   const int P = a.win->fields;
   const int LPF = a.fmt.lines_per_frame;
+  // the hsync difference still to be formed from the last anchored field
+  // (thread 0 only): its rounded anchor, mll, order, the previous anchor's
+  // read location and location, and its own read location
+  bool diff_due = false;
+  double d_round = 0.0, d_mll = 0.0, d_prev_loc = 0.0;
+  long long d_prev_read = -1, d_read = 0;
+  bool d_first = false;
+  auto prev_off_of = [&](long long prev_read, long long read, double mll) {
+    return (prev_read != -1 && mll > 0.0) ? ((double)prev_read - (double)read) / mll : 0.0;
+  };
+  auto settle_diff = [&]() {
+    if (!diff_due) return;
+    AnchorFit f;
+    f.loc_round = d_round;
+    st.prev_first_hsync_diff =
+        hsync_diff_after(f, a.fmt, d_first, d_mll, prev_off_of(d_prev_read, d_read, d_mll), d_prev_loc);
+    diff_due = false;
+  };
   if (t == 0) st = *a.state;
+  if (P > 0) phase_clock(a, 0, 16);
   for (int b0 = 0; b0 < P; b0 += kPrepBatch) {
     const int nb = min(kPrepBatch, P - b0);
     __syncthreads();  // the previous batch's records are no longer read
-    for (int i = t; i < nb; i += kLT) preps[i] = a.prep[b0 + i];
+    for (int i = t; i < nb; i += kLT) {
+      preps[i] = a.prep[b0 + i];
+      readlocs[i] = a.raw_offset + a.offs[b0 + i];
+      fallback[i] = 0;
+    }
     __syncthreads();
-    for (int j = 0; j < nb; j++) {
-      const int f = b0 + j;
-      const FieldPrep& p = preps[j];
+    int j = 0;
+    while (j < nb) {
       if (t == 0) {
-        const long long readloc = a.raw_offset + a.offs[f];
-        double prev_off = 0.0;
-        if (st.prev_first_hsync_readloc != -1 && p.mll > 0.0)
-          prev_off = ((double)st.prev_first_hsync_readloc - (double)readloc) / p.mll;
-        const double prev_loc = st.prev_first_hsync_loc;
-        const bool valid = a.vn[f] > 0 && p.mll > 0.0;
-        bool first = false;
-        need_fit = 0;
-        if (valid) {
-          first = decide_first(p.scan, st.prev_first_field, prev_loc, kAnchorConfidence);
-          need_fit = !(p.spec_first == (first ? 1 : 0) && prev_loc > 0.0);
+        for (; j < nb; j++) {
+          const int f = b0 + j;
+          const FieldPrep& p = preps[j];
+          const double prev_loc = st.prev_first_hsync_loc;
+          if (!(p.vn > 0 && p.mll > 0.0)) {
+            a.is_first[f] = st.prev_first_field >= 0 ? (1 - st.prev_first_field) : 1;
+            fallback[j] = 1;
+            continue;
+          }
+          if (p.exact) {
+            // fitted with this state by the per-field pass
+            if (p.spec.cnt > 0) {
+              const bool first = p.exact_first != 0;
+              a.is_first[f] = first ? 1 : 0;
+              if (!p.spec.used_prediction) {
+                diff_due = true;
+                d_round = p.spec.loc_round;
+                d_mll = p.mll;
+                d_first = first;
+                d_prev_read = st.prev_first_hsync_readloc;
+                d_prev_loc = prev_loc;
+                d_read = readlocs[j];
+              }
+              st.prev_first_field = first ? 1 : 0;
+              st.prev_progressive_field = 0;
+              st.prev_first_hsync_readloc = readlocs[j];
+              st.prev_first_hsync_loc = p.spec.loc;
+            } else {
+              a.is_first[f] = st.prev_first_field >= 0 ? (1 - st.prev_first_field) : 1;
+              fallback[j] = 1;
+            }
+            continue;
+          }
+          const bool first = decide_first(p, st.prev_first_field, prev_loc, kAnchorConfidence);
+          if (!(p.spec_first == (first ? 1 : 0) && prev_loc > 0.0)) {
+            // fit this field: the previous state is final up to here
+            settle_diff();
+            fit_first = first;
+            prev_off_s = prev_off_of(st.prev_first_hsync_readloc, readlocs[j], p.mll);
+            prev_loc_s = prev_loc;
+            prev_diff_s = st.prev_first_hsync_diff;
+            break;
+          }
+          // the speculative anchor stands
+          a.is_first[f] = first ? 1 : 0;
+          diff_due = true;
+          d_round = p.spec.loc_round;
+          d_mll = p.mll;
+          d_first = first;
+          d_prev_read = st.prev_first_hsync_readloc;
+          d_prev_loc = prev_loc;
+          d_read = readlocs[j];
+          st.prev_first_field = first ? 1 : 0;
+          st.prev_progressive_field = 0;
+          st.prev_first_hsync_readloc = readlocs[j];
+          st.prev_first_hsync_loc = p.spec.loc;
         }
-        first_s = first;
-        valid_s = valid;
-        prev_off_s = prev_off;
-        prev_loc_s = prev_loc;
-        prev_diff_s = st.prev_first_hsync_diff;
+        fit_j = j;
       }
       __syncthreads();
-      AnchorFit fit = p.spec;
-      if (valid_s && need_fit) {
-        VList v = field_vlist(a, f);
-        fit = fit_anchor(sm, p.scan, v, p.mll, a.fmt, first_s != 0, prev_off_s, prev_loc_s, prev_diff_s);
-        if (fit.cnt > 0) snap_lines(sm, v, fit.loc, fit.hsync_line, p.mll, LPF, a.ll + (size_t)f * LPF);
+      j = fit_j;
+      if (j >= nb) break;
+      // field b0 + j: fit and snap with the whole CTA
+      const int f = b0 + j;
+      const FieldPrep& p = preps[j];
+      VList v = field_vlist(a, f);
+      if (v.n <= kSmemValid) {
+        for (int k = t; k < v.n; k += kLT) {
+          sm.vs[k] = v.s[k];
+          sm.vt[k] = v.tg[k];
+        }
+        v.s = sm.vs;
+        v.tg = sm.vt;
+        v.d = sm.sort;  // anchor-offset terms; the sort that reuses it comes after
+        __syncthreads();
       }
-      const bool valid = valid_s && fit.cnt > 0;
-      if (!valid) {
-        double* locs = a.ll + (size_t)f * LPF;
-        for (int line = t; line < LPF; line += kLT) locs[line] = p.raw0 + p.mll * (double)line;
-      }
+      phase_clock(a, f, 17);
+      const AnchorFit fit = fit_anchor(sm, p.scan, v, p.mll, a.fmt, fit_first != 0, prev_off_s, prev_loc_s, prev_diff_s);
+      phase_clock(a, f, 18);
+      if (fit.cnt > 0) snap_lines(sm, v, fit.loc, fit.hsync_line, p.mll, LPF, a.ll + (size_t)f * LPF);
+      phase_clock(a, f, 19);
       if (t == 0) {
-        if (valid) {
-          const bool first = first_s != 0;
+        if (fit.cnt > 0) {
+          const bool first = fit_first != 0;
           a.is_first[f] = first ? 1 : 0;
           st.prev_first_field = first ? 1 : 0;
           st.prev_progressive_field = 0;
-          st.prev_first_hsync_readloc = a.raw_offset + a.offs[f];
+          st.prev_first_hsync_readloc = readlocs[j];
           st.prev_first_hsync_loc = fit.loc;
           if (!fit.used_prediction)
             st.prev_first_hsync_diff = hsync_diff_after(fit, a.fmt, first, p.mll, prev_off_s, prev_loc_s);
         } else {
           a.is_first[f] = st.prev_first_field >= 0 ? (1 - st.prev_first_field) : 1;
+          fallback[j] = 1;
         }
       }
+      j++;
       __syncthreads();
     }
+    // fields with no anchor: the nominal grid from their first pulse
+    for (int jj = 0; jj < nb; jj++) {
+      if (!fallback[jj]) continue;
+      double* locs = a.ll + (size_t)(b0 + jj) * LPF;
+      for (int line = t; line < LPF; line += kLT) locs[line] = preps[jj].raw0 + preps[jj].mll * (double)line;
+    }
   }
-  if (t == 0) *a.state = st;
+  if (t == 0) {
+    settle_diff();
+    *a.state = st;
+  }
+  if (P > 0) phase_clock(a, 0, 20);
 }
 
 // ------------------------------------------------------------ single pass
@@ -1250,7 +1547,10 @@ __global__ void __launch_bounds__(kLT) single_pass_kernel(LineLocArgs a) {
 size_t lineloc_smem_bytes() { return sizeof(FieldSmem); }
 
 cudaError_t launch_field_windows(const LineLocArgs& a, cudaStream_t st) {
-  return launch_chained(fieldwin_kernel, dim3(1), dim3(1024), 0, st, a);
+  const size_t smem = fieldwin_smem_bytes();
+  const cudaError_t e = cudaFuncSetAttribute(fieldwin_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return launch_chained(fieldwin_kernel, dim3(1), dim3(kWinThreads), smem, st, a);
 }
 
 cudaError_t launch_field_pulses(const LineLocArgs& a, cudaStream_t st) {

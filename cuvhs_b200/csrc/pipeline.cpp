@@ -235,15 +235,16 @@ bool Context::alloc_buffers() {
   d_dbg_vl = A((int*)nullptr, (size_t)batch * kMaxPulses);
   d_dbg_vt = A((int*)nullptr, (size_t)batch * kMaxPulses);
   d_dbg_vn = A((int*)nullptr, batch);
+  d_dbg_clk_ll = A((long long*)nullptr, (size_t)batch * kPhaseSlots);
+  d_dbg_clk_guard = A((long long*)nullptr, (size_t)kGuardClockSamples * kPhaseSlots);
   d_col_frac = A((double*)nullptr, (size_t)fmt.output_line_len);
-  d_ga64 = A((double*)nullptr, des.ga64.size());
+  d_guard_g = A((double2*)nullptr, (size_t)Design::kGuardN);
+  d_guard_tw = A((double2*)nullptr, (size_t)Design::kGuardN);
   d_hs64 = A((double*)nullptr, des.hs64.size());
   d_guard_list = A((unsigned*)nullptr, kGuardCap);
-  d_guard_done = A((int*)nullptr, kGuardCap);
   d_guard_count = A((int*)nullptr, 1);
-  d_guard_part = A((double*)nullptr, (size_t)kGuardCap * kGuardMaxParts);
   d_guard_vals = A((double*)nullptr, kGuardCap);
-  if (ok && guard_parts(des.hs64_half) > kGuardMaxParts) {
+  if (ok && !guard_supported(des.ga64_half, des.hs64_half)) {
     err = "sync guard support too long";
     ok = false;
   }
@@ -425,7 +426,9 @@ bool Context::init(const cuvhs_config& c) {
   upload(d_twb_inv, des.tw_b, stream);
   upload(d_twc_inv, des.tw_c, stream);
   upload(d_twl_inv, des.tw_line, stream);
-  upload(d_ga64, des.ga64, stream);
+  cudaMemcpyAsync(d_guard_g, des.guard_g.data(), des.guard_g.size() * sizeof(double), cudaMemcpyHostToDevice, stream);
+  cudaMemcpyAsync(d_guard_tw, des.guard_tw.data(), des.guard_tw.size() * sizeof(double), cudaMemcpyHostToDevice,
+                  stream);
   upload(d_hs64, des.hs64, stream);
   cudaMemsetAsync(d_guard_count, 0, sizeof(int), stream);
   {
@@ -578,7 +581,6 @@ DemodArgs Context::demod_args(int T) const {
   da.thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
   da.guard_hz = cfg.guard_band_hz > 0.0 ? (float)cfg.guard_band_hz : kGuardHz;
   da.guard_list = d_guard_list;
-  da.guard_done = d_guard_done;
   da.guard_count = d_guard_count;
   da.guard_cap = kGuardCap;
   return da;
@@ -593,7 +595,8 @@ GuardArgs Context::guard_args(const DemodArgs& da) const {
   g.total = da.total;
   g.spp = spp;
   g.tile = des.tile;
-  g.ga64 = d_ga64;
+  g.gfft = d_guard_g;
+  g.tw = d_guard_tw;
   g.ha = des.ga64_half;
   g.hs64 = d_hs64;
   g.hb = des.hs64_half;
@@ -605,9 +608,8 @@ GuardArgs Context::guard_args(const DemodArgs& da) const {
   g.list = d_guard_list;
   g.count = d_guard_count;
   g.cap = kGuardCap;
-  g.done = d_guard_done;
-  g.part = d_guard_part;
   g.values = d_guard_vals;
+  if (debug) g.dbg_clk = d_dbg_clk_guard;
   return g;
 }
 
@@ -760,6 +762,7 @@ LineLocArgs Context::lineloc_args(int tiles, int num_fields, long long raw_offse
     a.dbg_vl = d_dbg_vl;
     a.dbg_vt = d_dbg_vt;
     a.dbg_vn = d_dbg_vn;
+    a.dbg_clk = d_dbg_clk_ll;
   }
   return a;
 }
@@ -1064,6 +1067,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     end_stage(kStageEdges, ev_, 3);
   }
   LineLocArgs lla = lineloc_args(T, num_fields, (long long)raw_offset);
+  if (debug) cudaMemsetAsync(d_dbg_clk_ll, 0, (size_t)batch * kPhaseSlots * sizeof(long long), stream);
   {
     cudaEvent_t ev_;
     begin_stage(kStageWindows, ev_);
@@ -1172,6 +1176,12 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
       cudaMemcpy(dbg_guard_vals.data(), d_guard_vals, ng * sizeof(double), cudaMemcpyDeviceToHost);
     }
     dbg_guard_pos.assign(pos.begin(), pos.end());
+    dbg_clk_ll.resize((size_t)P * kPhaseSlots);
+    if (P) cudaMemcpy(dbg_clk_ll.data(), d_dbg_clk_ll, dbg_clk_ll.size() * sizeof(long long), cudaMemcpyDeviceToHost);
+    dbg_clk_guard.resize((size_t)std::min(ng, kGuardClockSamples) * kPhaseSlots);
+    if (!dbg_clk_guard.empty())
+      cudaMemcpy(dbg_clk_guard.data(), d_dbg_clk_guard, dbg_clk_guard.size() * sizeof(long long),
+                 cudaMemcpyDeviceToHost);
   }
   if (P == 0) {
     // no field window (the reference returns 0 fields): drain and report none

@@ -125,11 +125,13 @@ struct Context {
   LineLocState* d_lls = nullptr;
   int* d_is_first = nullptr;
   int *d_dbg_vs = nullptr, *d_dbg_vl = nullptr, *d_dbg_vt = nullptr, *d_dbg_vn = nullptr;
+  long long *d_dbg_clk_ll = nullptr, *d_dbg_clk_guard = nullptr;  // phase clocks (debug)
   // guard band of the sync threshold (kernels_guard.cu)
-  double *d_ga64 = nullptr, *d_hs64 = nullptr;
+  double2 *d_guard_g = nullptr, *d_guard_tw = nullptr;
+  double* d_hs64 = nullptr;
   unsigned* d_guard_list = nullptr;
-  int *d_guard_done = nullptr, *d_guard_count = nullptr;
-  double *d_guard_part = nullptr, *d_guard_vals = nullptr;
+  int* d_guard_count = nullptr;
+  double* d_guard_vals = nullptr;
   int* hp_guard = nullptr;  // pinned: the chunk's listed count
   // Guard launch over the current chunk's sync (T tiles), after the last K1b;
   // every later threshold decision reads the corrected samples.
@@ -164,7 +166,7 @@ struct Context {
   std::vector<int> dbg_meta, dbg_vsync, dbg_k2c, dbg_k2s, dbg_k2l, dbg_k2bc, dbg_k2bs, dbg_k2bl, dbg_k2bt, dbg_is_first;
   std::vector<long long> dbg_offs;
   std::vector<double> dbg_ll_coarse, dbg_ll, dbg_guard_vals;
-  std::vector<long long> dbg_guard_pos;
+  std::vector<long long> dbg_guard_pos, dbg_clk_ll, dbg_clk_guard;
   std::vector<float> dbg_demod, dbg_video, dbg_sync, dbg_env, dbg_pre;
 
   // per-stage device time (CUDA events on the decode stream) and launch count

@@ -148,7 +148,12 @@ def _gpu_chain_fns(dec, x):
         return res, res.n_fields, nxt
 
     def get_state():
-        return dec.get_state().as_tuple()
+        # The chroma phase cycle position is kept mod 8 (chroma_decode.cu:1000)
+        # but indexes a table that repeats every four fields (:672), so two
+        # chains whose positions differ by four decode every later field alike:
+        # the state compares (and is replayed) by its position mod 4.
+        t = dec.get_state().as_tuple()
+        return t[:-1] + (t[-1] % 4,)
 
     def set_state(t):
         from ._lib import State

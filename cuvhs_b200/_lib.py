@@ -72,7 +72,8 @@ class State(ctypes.Structure):
 
 
 class BatchConfig(ctypes.Structure):
-    _fields_ = [("device", ctypes.c_int), ("lanes", ctypes.c_int), ("max_fields", ctypes.c_int)]
+    _fields_ = [("device", ctypes.c_int), ("lanes", ctypes.c_int), ("max_fields", ctypes.c_int),
+                ("round_fields", ctypes.c_int)]
 
 
 class BatchItem(ctypes.Structure):
@@ -147,6 +148,8 @@ lib.cuvhs_batch_create.restype = ctypes.c_int
 lib.cuvhs_batch_destroy.argtypes = [_vp]
 lib.cuvhs_batch_lanes.argtypes = [_vp]
 lib.cuvhs_batch_lanes.restype = ctypes.c_int
+lib.cuvhs_batch_round_fields.argtypes = [_vp, ctypes.c_double]
+lib.cuvhs_batch_round_fields.restype = ctypes.c_int
 lib.cuvhs_batch_decode.argtypes = [_vp, ctypes.POINTER(BatchItem), ctypes.c_int]
 lib.cuvhs_batch_decode.restype = ctypes.c_int
 lib.cuvhs_batch_last_error.argtypes = [_vp]
@@ -226,7 +229,8 @@ EXPORTED = [
     "cuvhs_decode_file", "cuvhs_set_debug", "cuvhs_debug_array", "cuvhs_stream", "cuvhs_set_timing",
     "cuvhs_stage_count", "cuvhs_stage_name", "cuvhs_stage_times", "cuvhs_reset_stage_times", "cuvhs_launch_count",
     "cuvhs_dropouts_noalloc", "cuvhs_batch_create", "cuvhs_batch_destroy", "cuvhs_batch_lanes",
-    "cuvhs_batch_decode", "cuvhs_batch_last_error", "cuvhs_batch_json", "cuvhs_adjoint_create",
+    "cuvhs_batch_decode", "cuvhs_batch_last_error", "cuvhs_batch_json", "cuvhs_batch_round_fields",
+    "cuvhs_adjoint_create",
     "cuvhs_adjoint_destroy", "cuvhs_adjoint_fields", "cuvhs_adjoint_default_params", "cuvhs_adjoint_set_target",
     "cuvhs_adjoint_fwd", "cuvhs_adjoint_bwd", "cuvhs_adjoint_array", "cuvhs_synth_default_params",
     "cuvhs_synth_length", "cuvhs_synth_ntsc", "cuvhs_synth_lines", "cuvhs_synth_preemphasis",
@@ -589,10 +593,11 @@ class Decoder:
 
 
 class Batch:
-    """cuvhs_batch: many independent captures (mixed rates) decoded concurrently."""
+    """cuvhs_batch: many independent captures (mixed rates) decoded together in
+    batched rounds (round_fields: field slots per round, 0 = autotune)."""
 
-    def __init__(self, lanes=0, max_fields=0, device=0):
-        cfg = BatchConfig(int(device), int(lanes), int(max_fields))
+    def __init__(self, lanes=0, max_fields=0, device=0, round_fields=0):
+        cfg = BatchConfig(int(device), int(lanes), int(max_fields), int(round_fields))
         h = _vp()
         st = lib.cuvhs_batch_create(ctypes.byref(cfg), ctypes.byref(h))
         if st != 0:
@@ -602,6 +607,10 @@ class Batch:
     @property
     def lanes(self):
         return lib.cuvhs_batch_lanes(self._h)
+
+    def round_fields(self, sample_rate_mhz):
+        """Field slots per round in use for this sample rate (0 before first use)."""
+        return lib.cuvhs_batch_round_fields(self._h, float(sample_rate_mhz))
 
     def close(self):
         if getattr(self, "_h", None):

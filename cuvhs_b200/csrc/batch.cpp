@@ -1,18 +1,25 @@
 // Batched decoding of many independent captures (extern "C" cuvhs_batch_*).
 //
-// The reference decodes one capture per process (src/main.cpp:97-165), so a
-// set of captures runs back to back.  Here `lanes` host threads each own
-// decoder contexts -- one per sample rate, created on first use and kept --
-// and take captures from a shared queue, longest first.  Each lane's contexts
-// have their own streams, so the GPU overlaps the kernels and copies of
-// several captures while the lanes' host decisions (line locations, chroma
-// track replay) run in parallel.  A capture is always decoded from a fresh
-// state with a fixed chunk size, so its output is the single-capture decode's
-// whatever the lane count or item order.
+// The reference decodes one capture per process (src/main.cpp:97-165).  Here
+// the captures of one sample rate are decoded in rounds (Context::decode_round,
+// round.cpp): each round takes the next chunk of up to kMaxPortions captures,
+// chunk size max_fields as a single-capture decode would use, and runs every
+// stage once over all of them.  `lanes` host threads each drive rounds on
+// their own contexts (one per sample rate, kept between calls) over their share
+// of the captures, so one lane's host decisions overlap another's kernels.
+// The field slots of a round come from an online autotuner: a rate's first
+// rounds run at max_fields slots and double while the time per decoded field
+// falls by more than 5%; the fastest size is kept for the rest of the decode
+// and later calls (round_fields fixes it instead).  Rounds of any size decode
+// the same chunks, so tuning on the caller's captures changes no output.
+// Each capture starts from a fresh state and keeps its own carried state
+// between rounds, so its output is its single-capture decode's whatever the
+// lanes, round size or item order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -26,12 +33,16 @@
 #include "../../include/cuvhs.h"
 #include "pipeline.h"
 
+// Round sizes the tuner tries: max_fields times 1, 2, 4 (the context holds the largest).
+constexpr int kTuneMaxFactor = 4;
+
 struct cuvhs_batch {
   cuvhs_batch_config cfg{};
   int device = 0;
   int lanes = 1;
-  // lane -> (rate -> context)
+  // lane -> (rate -> context); a context's field slots are the rate's round size
   std::vector<std::map<double, cuvhs_ctx*>> ctx;
+  std::map<double, int> round_fields;  // per rate, tuned or given
   std::mutex mu;
   std::string err;
   ~cuvhs_batch() {
@@ -45,12 +56,183 @@ namespace cuvhs {
 cuvhs_status create_context(const cuvhs_config& cfg, cuvhs_ctx** out);
 }  // namespace cuvhs
 
+namespace {
+
+using cuvhs::ChunkResult;
+using cuvhs::Context;
+using cuvhs::Portion;
+using cuvhs::PortionState;
+
+// Online round-size tuning of one lane: the current size, the best so far and
+// its time per field, and whether the search has ended.
+struct Tuner {
+  int slots = 0, best = 0, cap = 0;
+  double best_spf = 0.0;
+  bool settled = false;
+  // after a round of `fields` fields in `secs` seconds at `slots` slots
+  void observe(int fields, double secs, int round_slots_used) {
+    if (settled || fields <= 0) return;
+    const double spf = secs / fields;
+    if (best == 0 || spf < best_spf * 0.95) {
+      best = slots;
+      best_spf = spf;
+      // grow only while rounds fill their slots (a partial round says nothing
+      // about a larger one)
+      if (slots * 2 <= cap && round_slots_used * 2 > slots) slots *= 2;
+      else settled = true;
+    } else {
+      slots = best;
+      settled = true;
+    }
+  }
+};
+
+// One capture being decoded: its item, carried state and position.
+struct Capture {
+  cuvhs_batch_item* item = nullptr;
+  PortionState st;
+  uint64_t raw = 0;
+  bool done = false;
+};
+
+cuvhs_status make_context(cuvhs_batch* b, double mhz, int slots, cuvhs_ctx** out) {
+  cuvhs_config cc;
+  cuvhs_default_config(&cc);
+  cc.sample_rate_mhz = mhz;
+  cc.device = b->device;
+  cc.batch_fields = slots;
+  return cuvhs::create_context(cc, out);
+}
+
+void set_err(cuvhs_batch* b, const std::string& e) {
+  std::lock_guard<std::mutex> g(b->mu);
+  if (b->err.empty()) b->err = e;
+}
+
+// Appends one decoded chunk of a capture to its output (cabi.cpp's
+// append_chunk for a round portion): planes already copied, dropout lists
+// from the round's slots.
+cuvhs_status append_portion(Context& c, const Portion& p, cuvhs_output* out, std::string& err) {
+  const ChunkResult& r = p.res;
+  size_t need = 0;
+  for (int i = 0; i < r.fields; i++) need += (size_t)r.field_info[i].dropout_count;
+  if (out->dropouts_out + need > out->max_dropouts && need > 0) {
+    err = "output dropout buffer too small";
+    return CUVHS_ERR_CAPACITY;
+  }
+  for (int i = 0; i < r.fields; i++) {
+    cuvhs_field_info fi = r.field_info[i];
+    fi.dropout_offset = (int32_t)out->dropouts_out;
+    for (int d = 0; d < fi.dropout_count; d++) {
+      const size_t k = ((size_t)p.slot0 + i) * cuvhs::kMaxDropouts + d;
+      if (out->dropout_line) out->dropout_line[out->dropouts_out] = c.hp_do_lines[k];
+      if (out->dropout_startx) out->dropout_startx[out->dropouts_out] = c.hp_do_starts[k];
+      if (out->dropout_endx) out->dropout_endx[out->dropouts_out] = c.hp_do_ends[k];
+      out->dropouts_out++;
+    }
+    if (out->fields) out->fields[out->fields_out] = fi;
+    out->fields_out++;
+  }
+  out->next_raw_offset = r.next_raw_offset;
+  return CUVHS_OK;
+}
+
+// Decodes `caps` (one sample rate) in rounds on context `ctx`, chunk size
+// max_fields, tune.slots field slots per round (the tuner may grow them).
+void run_rounds(cuvhs_batch* b, cuvhs_ctx* ctx, std::vector<Capture>& caps, int max_fields, Tuner& tune) {
+  Context& c = ctx->c;
+  const size_t spf = (size_t)c.fmt.samples_per_field;
+  const size_t F = (size_t)c.fmt.output_line_len * c.fmt.output_field_lines;
+  std::vector<Portion> ps;
+  std::vector<int> idx;
+  for (;;) {
+    ps.clear();
+    idx.clear();
+    int used = 0;
+    const int slots = tune.slots;
+    for (int i = 0; i < (int)caps.size() && (int)ps.size() < cuvhs::kMaxPortions; i++) {
+      Capture& cp = caps[i];
+      if (cp.done) continue;
+      cuvhs_batch_item& it = *cp.item;
+      const size_t n = it.n;
+      const int remaining = cp.raw < n ? (int)((n - cp.raw) / spf) : 0;
+      if (remaining <= 0) {
+        cp.done = true;
+        continue;
+      }
+      const int nf = std::min(max_fields, remaining);
+      if (used + nf > slots) break;  // the round is full
+      cuvhs_output* out = it.out;
+      const size_t most = std::min<size_t>((size_t)nf, (n - cp.raw) / spf);
+      if (out->fields_out + most > out->max_fields) {
+        it.status = CUVHS_ERR_CAPACITY;
+        set_err(b, "output field buffer too small");
+        cp.done = true;
+        continue;
+      }
+      Portion p;
+      p.src = it.samples + cp.raw;
+      p.n_avail = n - cp.raw;
+      p.raw_offset = cp.raw;
+      p.num_fields = nf;
+      p.slot0 = used;
+      p.st = &cp.st;
+      p.dst_luma = out->luma ? out->luma + out->fields_out * F : nullptr;
+      p.dst_chroma = out->chroma ? out->chroma + out->fields_out * F : nullptr;
+      ps.push_back(p);
+      idx.push_back(i);
+      used += nf;
+    }
+    if (ps.empty()) {
+      c.drain_copies();  // the last rounds' planes are in the callers' buffers
+      return;
+    }
+    c.status = CUVHS_OK;
+    const auto t0 = std::chrono::steady_clock::now();
+    const bool ok = c.decode_round(ps);
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (ok) {
+      int fields = 0;
+      for (const Portion& p : ps) fields += p.res.fields;
+      tune.observe(fields, secs, used);
+    }
+    if (!ok) {
+      const cuvhs_status s = c.status != CUVHS_OK ? c.status : CUVHS_ERR_CUDA;
+      set_err(b, c.err);
+      for (int i : idx) {
+        caps[i].item->status = s;
+        caps[i].done = true;
+      }
+      continue;
+    }
+    for (size_t j = 0; j < ps.size(); j++) {
+      Capture& cp = caps[idx[j]];
+      const Portion& p = ps[j];
+      if (p.res.fields == 0) {
+        cp.done = true;  // the chunk held no field: end of capture
+        continue;
+      }
+      std::string e;
+      const cuvhs_status s = append_portion(c, p, cp.item->out, e);
+      if (s != CUVHS_OK) {
+        cp.item->status = s;
+        set_err(b, e);
+        cp.done = true;
+        continue;
+      }
+      cp.raw = p.res.next_raw_offset;
+    }
+  }
+}
+
+}  // namespace
+
 extern "C" {
 
 cuvhs_status cuvhs_batch_create(const cuvhs_batch_config* cfg, cuvhs_batch** out) {
   if (!cfg || !out) return CUVHS_ERR_INVALID_ARGUMENT;
   *out = nullptr;
-  if (cfg->lanes < 0 || cfg->max_fields < 0) return CUVHS_ERR_INVALID_ARGUMENT;
+  if (cfg->lanes < 0 || cfg->max_fields < 0 || cfg->round_fields < 0) return CUVHS_ERR_INVALID_ARGUMENT;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
     fprintf(stderr, "cuvhs_batch_create: no CUDA device\n");
@@ -60,6 +242,10 @@ cuvhs_status cuvhs_batch_create(const cuvhs_batch_config* cfg, cuvhs_batch** out
   if (!b) return CUVHS_ERR_OUT_OF_MEMORY;
   b->cfg = *cfg;
   if (b->cfg.max_fields == 0) b->cfg.max_fields = 256;
+  if (b->cfg.round_fields > 0 && b->cfg.round_fields < b->cfg.max_fields) {
+    delete b;
+    return CUVHS_ERR_INVALID_ARGUMENT;
+  }
   int dev = cfg->device;
   if (dev < 0) {
     size_t best = 0;
@@ -77,8 +263,7 @@ cuvhs_status cuvhs_batch_create(const cuvhs_batch_config* cfg, cuvhs_batch** out
     return CUVHS_ERR_INVALID_ARGUMENT;
   }
   b->device = dev;
-  const int hw = std::max(1, (int)std::thread::hardware_concurrency());
-  b->lanes = cfg->lanes > 0 ? cfg->lanes : std::max(1, std::min(4, hw / 2));
+  b->lanes = cfg->lanes > 0 ? cfg->lanes : 2;
   b->ctx.resize(b->lanes);
   *out = b;
   return CUVHS_OK;
@@ -89,6 +274,12 @@ void cuvhs_batch_destroy(cuvhs_batch* b) { delete b; }
 int cuvhs_batch_lanes(const cuvhs_batch* b) { return b ? b->lanes : 0; }
 
 const char* cuvhs_batch_last_error(const cuvhs_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int cuvhs_batch_round_fields(const cuvhs_batch* b, double sample_rate_mhz) {
+  if (!b) return 0;
+  auto it = b->round_fields.find(sample_rate_mhz);
+  return it == b->round_fields.end() ? 0 : it->second;
+}
 
 long long cuvhs_batch_json(const cuvhs_batch_item* item, char* dst, long long cap) {
   if (!item || !item->out) return -1;
@@ -108,52 +299,94 @@ long long cuvhs_batch_json(const cuvhs_batch_item* item, char* dst, long long ca
 cuvhs_status cuvhs_batch_decode(cuvhs_batch* b, cuvhs_batch_item* items, int n_items) {
   if (!b || (!items && n_items > 0) || n_items < 0) return CUVHS_ERR_INVALID_ARGUMENT;
   for (int i = 0; i < n_items; i++) {
-    if (!items[i].samples || !items[i].out) return CUVHS_ERR_INVALID_ARGUMENT;
+    if (!items[i].samples || !items[i].out || !(items[i].sample_rate_mhz > 0.0)) return CUVHS_ERR_INVALID_ARGUMENT;
     items[i].status = CUVHS_OK;
   }
-  // longest captures first, so the lanes finish together
-  std::vector<int> order(n_items);
-  for (int i = 0; i < n_items; i++) order[i] = i;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-    return items[x].n / items[x].sample_rate_mhz > items[y].n / items[y].sample_rate_mhz;
-  });
-  std::atomic<int> next{0};
   b->err.clear();
+  cudaSetDevice(b->device);
+  const int max_fields = b->cfg.max_fields;
+  // per rate: the captures, longest first, dealt to the lanes in turn
+  std::map<double, std::vector<int>> by_rate;
+  for (int i = 0; i < n_items; i++) by_rate[items[i].sample_rate_mhz].push_back(i);
+  struct Job {
+    double mhz;
+    std::vector<int> items;
+  };
+  std::vector<std::vector<Job>> jobs(b->lanes);
+  for (auto& kv : by_rate) {
+    std::vector<int>& v = kv.second;
+    std::stable_sort(v.begin(), v.end(), [&](int x, int y) { return items[x].n > items[y].n; });
+    std::vector<Job> per(b->lanes);
+    for (size_t k = 0; k < v.size(); k++) per[k % b->lanes].items.push_back(v[k]);
+    for (int l = 0; l < b->lanes; l++)
+      if (!per[l].items.empty()) jobs[l].push_back(Job{kv.first, per[l].items});
+  }
   auto lane_fn = [&](int lane) {
     cudaSetDevice(b->device);
-    for (;;) {
-      const int k = next.fetch_add(1);
-      if (k >= n_items) break;
-      cuvhs_batch_item& it = items[order[k]];
-      cuvhs_ctx*& ctx = b->ctx[lane][it.sample_rate_mhz];
+    for (Job& job : jobs[lane]) {
+      // the round size: given, tuned by an earlier call, or tuned on these rounds
+      Tuner tune;
+      int known = 0;
+      {
+        std::lock_guard<std::mutex> g(b->mu);
+        auto it = b->round_fields.find(job.mhz);
+        if (it != b->round_fields.end()) known = it->second;
+      }
+      if (b->cfg.round_fields > 0) known = b->cfg.round_fields;
+      // no round needs more slots than one chunk of every capture of the job
+      cuvhs::Format fmt;
+      fmt.init(job.mhz);
+      long long need = 0;
+      for (int i : job.items)
+        need += std::min<long long>(max_fields, (long long)(items[i].n / (size_t)fmt.samples_per_field));
+      const int cap = (int)std::max<long long>(
+          max_fields, std::min<long long>(need, known > 0 ? known : (long long)max_fields * kTuneMaxFactor));
+      cuvhs_ctx*& ctx = b->ctx[lane][job.mhz];
+      if (ctx && cuvhs_batch_fields(ctx) < cap) {
+        cuvhs_destroy(ctx);
+        ctx = nullptr;
+      }
       if (!ctx) {
-        cuvhs_config cc;
-        cuvhs_default_config(&cc);
-        cc.sample_rate_mhz = it.sample_rate_mhz;
-        cc.device = b->device;
-        cc.batch_fields = b->cfg.max_fields;
-        cuvhs_status s = cuvhs::create_context(cc, &ctx);
+        // a context too large for the free memory halves down to one chunk
+        cuvhs_status s = CUVHS_ERR_OUT_OF_MEMORY;
+        for (int sl = cap; sl >= max_fields; sl /= 2) {
+          s = make_context(b, job.mhz, sl, &ctx);
+          if (s == CUVHS_OK) break;
+          ctx = nullptr;
+          if (s != CUVHS_ERR_OUT_OF_MEMORY) break;
+        }
         if (s != CUVHS_OK) {
           ctx = nullptr;
-          it.status = s;
-          std::lock_guard<std::mutex> g(b->mu);
-          if (b->err.empty()) b->err = "context creation failed";
+          for (int i : job.items) items[i].status = s;
+          set_err(b, "context creation failed");
           continue;
         }
       }
-      cuvhs_reset(ctx);
-      it.out->fields_out = 0;
-      it.out->dropouts_out = 0;
-      it.status = cuvhs_decode_capture(ctx, it.samples, it.n, it.out);
-      if (it.status != CUVHS_OK) {
+      tune.cap = std::min(cap, cuvhs_batch_fields(ctx));
+      if (known > 0) {
+        tune.slots = tune.best = std::min(known, tune.cap);
+        tune.settled = true;
+      } else {
+        tune.slots = max_fields;
+      }
+      std::vector<Capture> caps(job.items.size());
+      for (size_t k = 0; k < job.items.size(); k++) {
+        cuvhs_batch_item& it = items[job.items[k]];
+        it.out->fields_out = 0;
+        it.out->dropouts_out = 0;
+        caps[k].item = &it;
+      }
+      run_rounds(b, ctx, caps, max_fields, tune);
+      {
         std::lock_guard<std::mutex> g(b->mu);
-        if (b->err.empty()) b->err = cuvhs_last_error(ctx);
+        int& rf = b->round_fields[job.mhz];
+        if (b->cfg.round_fields > 0) rf = b->cfg.round_fields;
+        else if (tune.best > 0) rf = std::max(rf, tune.best);
       }
     }
   };
-  const int nl = std::min(b->lanes, std::max(1, n_items));
   std::vector<std::thread> th;
-  for (int l = 1; l < nl; l++) th.emplace_back(lane_fn, l);
+  for (int l = 1; l < b->lanes; l++) th.emplace_back(lane_fn, l);
   lane_fn(0);
   for (auto& t : th) t.join();
   for (int i = 0; i < n_items; i++)

@@ -113,6 +113,30 @@ struct Design {
 // the first at block position h + 1 (Design::a_pos, Design::a_out).
 int k1a_half_support(double fs_hz);
 
+// Kernel arguments of one capture's chunk, or of the chunks of several
+// captures decoded together (a batched round: grid.z picks the capture, and
+// every kernel runs the one-capture code on that capture's arguments).  Both
+// travel as __grid_constant__ kernel parameters (kMaxPortions sets of the
+// largest argument struct fit the 32 KB parameter space).  A single chunk's
+// arguments are a set of one, read the same way (indexed by grid.z, which is
+// 0), so a kernel compiles to the same arithmetic for one capture or many
+// and a batched capture decodes bit for bit as it does alone.
+constexpr int kMaxPortions = 64;
+template <class A>
+struct ArgsOne {
+  A a[1];
+#ifdef __CUDACC__
+  __device__ __forceinline__ const A& get() const { return a[blockIdx.z]; }
+#endif
+};
+template <class A>
+struct ArgsMany {
+  A a[kMaxPortions];
+#ifdef __CUDACC__
+  __device__ __forceinline__ const A& get() const { return a[blockIdx.z]; }
+#endif
+};
+
 // ---------------------------------------------------------------- kernels
 struct DemodArgs {
   const uint8_t* raw;  // chunk samples in the input format (raw_input.cuh)
@@ -142,6 +166,9 @@ struct DemodArgs {
   // Guard band: K1b lists every sync sample it writes within guard_hz of
   // thr_rel (chunk index into guard_list); the count may exceed guard_cap,
   // which the host reports.  guard_list == null: off.
+  // In-pulse bits (sync <= thr_rel, FP32): bit p of pulse_bits is set by K1b
+  // for chunk position p in a pulse (the array zeroed before K1b); null: off.
+  unsigned* pulse_bits = nullptr;
   float thr_rel = 0.0f, guard_hz = 0.0f;
   unsigned* guard_list = nullptr;
   int* guard_count = nullptr;
@@ -170,6 +197,7 @@ struct GuardArgs {
   const int* count;
   int cap;
   double* values;  // optional [cap]: the FP64 sync value of each listed sample
+  int* flips = nullptr;  // optional: counts samples whose FP64 side differs from their FP32 value's
   long long* dbg_clk = nullptr;  // optional [kGuardClockSamples][kPhaseSlots]: SM clock at each phase of a sample's CTA
 };
 constexpr int kGuardClockSamples = 1024;
@@ -177,8 +205,12 @@ constexpr int kGuardClockSamples = 1024;
 bool guard_supported(int ha, int hb);
 size_t guard_smem_bytes(int hb);
 cudaError_t launch_sync_guard(const GuardArgs& g, cudaStream_t st);
+cudaError_t launch_sync_guard_many(const ArgsMany<GuardArgs>& p, int portions, cudaStream_t st);
 // K1a over tiles [f0, f0 + nf).
 void launch_k1a(const DemodArgs& a, int f0, int nf, cudaStream_t st);
+// K1a / K1b over every tile of `portions` captures' chunks (one launch each).
+void launch_k1a_many(const ArgsMany<DemodArgs>& p, int portions, int max_tiles, cudaStream_t st);
+void launch_k1b_many(const ArgsMany<DemodArgs>& p, int portions, int max_tiles, cudaStream_t st);
 // DC correction: *dc = mean of the n converted samples of raw (exact integer
 // sum, one FP64 division, as the reference's FP64 loop), as FP32.
 // sum is scratch for one unsigned long long.
@@ -193,6 +225,20 @@ void launch_k1b(const DemodArgs& a, int f0, int nf, cudaStream_t st);
 int edge_blocks(long long total);
 // masks: scratch of edge_mask_words(total) words (per-thread edge bit masks)
 size_t edge_mask_words(long long total);
+// Threshold edges from K1b's in-pulse bits (the same lists as launch_edges on
+// the FP32 sync it wrote).
+struct EdgeArgs {
+  const unsigned* bits;
+  long long total;
+  int2* blk;    // per-CTA counts, then offsets
+  int* counts;  // [0] falling, [1] rising
+  unsigned *fall, *rise;
+  int cap;
+};
+void launch_edges_bits(const unsigned* bits, long long total, unsigned* fall, unsigned* rise, int* counts, int cap,
+                       int2* blk, cudaStream_t st);
+size_t pulse_bit_words(long long total);
+void launch_edges_bits_many(const ArgsMany<EdgeArgs>& e, int portions, long long max_total, cudaStream_t st);
 void launch_edges(const float* sync, long long total, float thr_rel, unsigned* fall, unsigned* rise,
                   int* counts, int cap, int2* blk, unsigned* masks, cudaStream_t st);
 
@@ -214,6 +260,8 @@ struct LineArgs {
 };
 void launch_hsync_refine(const LineArgs& a, cudaStream_t st);
 void launch_luma(const LineArgs& a, cudaStream_t st);
+void launch_hsync_refine_many(const ArgsMany<LineArgs>& p, int portions, int max_fields, cudaStream_t st);
+void launch_luma_many(const ArgsMany<LineArgs>& p, int portions, int max_fields, cudaStream_t st);
 
 struct ChromaArgs {
   const uint8_t* raw;  // as DemodArgs
@@ -243,6 +291,13 @@ void launch_chroma_prefilter(const ChromaArgs& a, cudaStream_t st);
 // Lines [field0*out_h, (field0+nfields)*out_h) of the chunk.
 void launch_chroma_lines(const ChromaArgs& a, int field0, int nfields, bool write_output, cudaStream_t st);
 void launch_burst_metric(const ChromaArgs& a, int field0, int nfields, cudaStream_t st);
+// The same over `portions` captures (grid.z): the pre-band-pass over each
+// capture's a.fields tiles; chroma lines of fields [0, nfields) of each
+// (nfields < 0: each capture's a.fields) and their burst metrics.
+void launch_chroma_prefilter_many(const ArgsMany<ChromaArgs>& p, int portions, int max_tiles, cudaStream_t st);
+void launch_chroma_lines_many(const ArgsMany<ChromaArgs>& p, int portions, int nfields, int max_fields,
+                              bool write_output, cudaStream_t st);
+void launch_burst_metric_many(const ArgsMany<ChromaArgs>& p, int portions, int max_fields, cudaStream_t st);
 
 struct DropoutArgs {
   const float* env;
@@ -274,6 +329,9 @@ size_t dropout_class_bytes_per_field(int spp);
 void launch_dropouts_two_pass(const DropoutArgs& a, cudaStream_t st);
 // Chroma concealment of fields [f0, f0 + nf) (their chroma lines final).
 void launch_dropout_conceal_chroma(const DropoutArgs& a, int f0, int nf, cudaStream_t st);
+void launch_dropouts_two_pass_many(const ArgsMany<DropoutArgs>& p, int portions, int max_fields, cudaStream_t st);
+void launch_dropout_conceal_chroma_many(const ArgsMany<DropoutArgs>& p, int portions, int max_fields,
+                                        cudaStream_t st);
 
 // ---------------------------------------------------------------- line locations
 // Per-field pulse validation, mean line length, vertical-blanking anchor and
@@ -370,5 +428,11 @@ cudaError_t launch_field_pulses(const LineLocArgs& a, cudaStream_t st);
 // reference (per-field CTAs, then one CTA in field order), or the single-pass
 // locator.
 cudaError_t launch_line_locations(const LineLocArgs& a, cudaStream_t st);
+// The same over `portions` captures' chunks (grid.z), fields per capture up
+// to max_fields (each capture's own count in its arguments).
+cudaError_t launch_field_windows_many(const ArgsMany<LineLocArgs>& p, int portions, cudaStream_t st);
+cudaError_t launch_field_pulses_many(const ArgsMany<LineLocArgs>& p, int portions, int max_fields, cudaStream_t st);
+cudaError_t launch_line_locations_many(const ArgsMany<LineLocArgs>& p, int portions, int max_fields,
+                                       cudaStream_t st);
 
 }  // namespace cuvhs

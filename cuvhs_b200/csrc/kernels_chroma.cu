@@ -49,8 +49,10 @@ __device__ __forceinline__ void pair_sync() {
 
 // Two adjacent output blocks ride in the real and imaginary parts of one
 // transform (the kernel is real).  Thread t holds block samples t + T*q, q < kElemsC.
-template <int FMT>
-__global__ void __launch_bounds__(kThreadsC, 1) prefilter_kernel(ChromaArgs a) {
+template <int FMT, class Src>
+__global__ void __launch_bounds__(kThreadsC, 1) prefilter_kernel(const __grid_constant__ Src src) {
+  const ChromaArgs& a = src.get();
+  if ((int)blockIdx.y >= a.fields) return;  // whole CTA: a batched capture with fewer tiles
   chain_wait();
   constexpr int N = Design::kNc, T = kThreadsC, E = kElemsC;
   extern __shared__ float2 sm[];
@@ -151,9 +153,12 @@ __device__ __forceinline__ float het_at(const ChromaArgs& a, const HetLine& L, d
   return ok ? v * het : 0.0f;
 }
 
-template <int N>
+// nlines < 0: every line of the capture's a.fields fields (a batched round).
+template <int N, class Src>
 __global__ void __launch_bounds__(line_threads<N>(), line_min_ctas<N>())
-    lines_kernel(ChromaArgs a, int line0, int nlines, int write_output) {
+    lines_kernel(const __grid_constant__ Src src, int line0, int nlines, int write_output) {
+  const ChromaArgs& a = src.get();
+  if (nlines < 0) nlines = a.fields * a.out_h;
   chain_wait();
   constexpr int TP = line_tp<N>(), P = line_pairs<N>();
   static_assert(TP == 32 || P <= 4, "two-warp pairs use named barriers 1..4");
@@ -238,8 +243,12 @@ __global__ void __launch_bounds__(line_threads<N>(), line_min_ctas<N>())
 // pairs l, l + 32, ... in order, then a butterfly over the lanes.
 // BL: the burst window length when known at compile time (NTSC 36, PAL 40), 0 = a.burst_len.
 constexpr int kMetricThreads = 256;
-template <int BL>
-__global__ void __launch_bounds__(kMetricThreads) metric_kernel(ChromaArgs a, int field0, int nfields) {
+// nfields < 0: every field of the capture (a batched round).
+template <int BL, class Src>
+__global__ void __launch_bounds__(kMetricThreads) metric_kernel(const __grid_constant__ Src src, int field0,
+                                                                int nfields) {
+  const ChromaArgs& a = src.get();
+  if (nfields < 0) nfields = a.fields;
   chain_wait();
   __shared__ double pair_mean[kMetricThreads];
   const int bl = BL > 0 ? BL : a.burst_len;
@@ -283,40 +292,75 @@ __global__ void __launch_bounds__(kMetricThreads) metric_kernel(ChromaArgs a, in
 
 }  // namespace
 
-void launch_chroma_prefilter(const ChromaArgs& a, cudaStream_t st) {
+namespace {
+template <class S>
+void prefilter_launch(const S& src, const ChromaArgs& a, int portions, int max_tiles, cudaStream_t st) {
   const size_t smem = sizeof(float2) * fft_pad(Design::kNc);
-  dim3 grid((a.spp + 2 * a.c_out - 1) / (2 * a.c_out), a.fields);
+  dim3 grid((a.spp + 2 * a.c_out - 1) / (2 * a.c_out), max_tiles, portions);
   auto go = [&](auto kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    launch_chained(kernel, grid, dim3(kThreadsC), smem, st, a);
+    launch_chained(kernel, grid, dim3(kThreadsC), smem, st, src);
   };
-  if (a.in_fmt == kInS16) go(prefilter_kernel<kInS16>);
-  else if (a.in_fmt == kInU16) go(prefilter_kernel<kInU16>);
-  else go(prefilter_kernel<kInU8>);
+  if (a.in_fmt == kInS16) go(prefilter_kernel<kInS16, S>);
+  else if (a.in_fmt == kInU16) go(prefilter_kernel<kInU16, S>);
+  else go(prefilter_kernel<kInU8, S>);
+}
+
+template <class S>
+void lines_launch(const S& src, const ChromaArgs& a, int portions, int line0, int nlines, int max_lines,
+                  bool write_output, cudaStream_t st) {
+  if (max_lines <= 0) return;
+  const int pairs = (max_lines + 1) / 2;
+  auto go = [&](auto kernel, int per_cta, int threads) {
+    // the largest shared-memory carveout, so that the register limit sets the CTAs per SM
+    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    launch_chained(kernel, dim3((pairs + per_cta - 1) / per_cta, 1, portions), dim3(threads), 0, st, src, line0,
+                   nlines, write_output ? 1 : 0);
+  };
+  if (a.line_fft == 2048) go(lines_kernel<2048, S>, line_pairs<2048>(), line_threads<2048>());
+  else go(lines_kernel<1024, S>, line_pairs<1024>(), line_threads<1024>());
+}
+
+template <class S>
+void metric_launch(const S& src, const ChromaArgs& a, int portions, int field0, int nfields, int max_fields,
+                   cudaStream_t st) {
+  if (max_fields <= 0) return;
+  auto go = [&](auto kernel) {
+    launch_chained(kernel, dim3(max_fields, 1, portions), dim3(kMetricThreads), 0, st, src, field0, nfields);
+  };
+  if (a.burst_len == 36) go(metric_kernel<36, S>);
+  else if (a.burst_len == 40) go(metric_kernel<40, S>);
+  else go(metric_kernel<0, S>);
+}
+}  // namespace
+
+void launch_chroma_prefilter(const ChromaArgs& a, cudaStream_t st) {
+  prefilter_launch(ArgsOne<ChromaArgs>{a}, a, 1, a.fields, st);
 }
 
 void launch_chroma_lines(const ChromaArgs& a, int field0, int nfields, bool write_output, cudaStream_t st) {
   const int nlines = nfields * a.out_h;
-  if (nlines <= 0) return;
-  const int pairs = (nlines + 1) / 2;
-  auto go = [&](auto kernel, int per_cta, int threads) {
-    // the largest shared-memory carveout, so that the register limit sets the CTAs per SM
-    cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-    launch_chained(kernel, dim3((pairs + per_cta - 1) / per_cta), dim3(threads), 0, st, a, field0 * a.out_h, nlines,
-                   write_output ? 1 : 0);
-  };
-  if (a.line_fft == 2048) go(lines_kernel<2048>, line_pairs<2048>(), line_threads<2048>());
-  else go(lines_kernel<1024>, line_pairs<1024>(), line_threads<1024>());
+  lines_launch(ArgsOne<ChromaArgs>{a}, a, 1, field0 * a.out_h, nlines, nlines, write_output, st);
 }
 
 void launch_burst_metric(const ChromaArgs& a, int field0, int nfields, cudaStream_t st) {
-  if (nfields <= 0) return;
-  auto go = [&](auto kernel) {
-    launch_chained(kernel, dim3(nfields), dim3(kMetricThreads), 0, st, a, field0, nfields);
-  };
-  if (a.burst_len == 36) go(metric_kernel<36>);
-  else if (a.burst_len == 40) go(metric_kernel<40>);
-  else go(metric_kernel<0>);
+  metric_launch(ArgsOne<ChromaArgs>{a}, a, 1, field0, nfields, nfields, st);
+}
+
+void launch_chroma_prefilter_many(const ArgsMany<ChromaArgs>& p, int portions, int max_tiles, cudaStream_t st) {
+  if (portions > 0) prefilter_launch(p, p.a[0], portions, max_tiles, st);
+}
+
+void launch_chroma_lines_many(const ArgsMany<ChromaArgs>& p, int portions, int nfields, int max_fields,
+                              bool write_output, cudaStream_t st) {
+  if (portions <= 0) return;
+  const ChromaArgs& a = p.a[0];
+  if (nfields < 0) lines_launch(p, a, portions, 0, -1, max_fields * a.out_h, write_output, st);
+  else lines_launch(p, a, portions, 0, nfields * a.out_h, nfields * a.out_h, write_output, st);
+}
+
+void launch_burst_metric_many(const ArgsMany<ChromaArgs>& p, int portions, int max_fields, cudaStream_t st) {
+  if (portions > 0) metric_launch(p, p.a[0], portions, 0, -1, max_fields, st);
 }
 
 }  // namespace cuvhs

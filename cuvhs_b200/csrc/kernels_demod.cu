@@ -151,9 +151,11 @@ __device__ __forceinline__ void k1a_emit(const DemodArgs& a, const float2 (&z)[1
 
 // K1a: u8 -> analytic signal -> phase step + envelope, blocks 2x and 2x+1 of
 // the tile (the second may lie past the tile's end).
-template <int FMT>
-__global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(DemodArgs a, int f_begin) {
+template <int FMT, class Src>
+__global__ void __launch_bounds__(kThreadsA, 3) k1a_kernel(const __grid_constant__ Src src, int f_begin) {
   constexpr int N = Design::kNa, T = kThreadsA;
+  const DemodArgs& a = src.get();
+  if (f_begin + (int)blockIdx.y >= a.tiles) return;  // whole CTA: a batched capture with fewer tiles
   chain_wait();
   extern __shared__ float2 sm[];
   float2* sA = sm;
@@ -211,13 +213,16 @@ __device__ __forceinline__ void k1b_emit(const DemodArgs& a, const float2 (&z)[1
   const int out0 = f * a.spp + (j0 - kOverlap);
   float* video_out = a.video + out0;
   float* sync_out = a.sync + out0;
+  const int lane = t & 31;
 #pragma unroll
   for (int q = 0; q < 16; q++) {
     const int i = t + T * q - a.b_pos;
+    bool in = false;
     if (i >= 0 && i < nout) {
       video_out[i] = z[q].x + a.corr_video;
       const float sv = z[q].y + a.corr_sync;
       sync_out[i] = sv;
+      in = sv <= a.thr_rel;
       if (fabsf(sv - a.thr_rel) < a.guard_hz && a.guard_list) {
         const int slot = atomicAdd(a.guard_count, 1);
         if (slot < a.guard_cap) {
@@ -225,12 +230,31 @@ __device__ __forceinline__ void k1b_emit(const DemodArgs& a, const float2 (&z)[1
         }
       }
     }
+    if (a.pulse_bits) {
+      // the warp's 32 consecutive positions as one in-pulse word, ORed into
+      // the (at most two) words it straddles
+      unsigned m = __ballot_sync(0xffffffffu, in);
+      if (lane == 0 && m) {
+        long long p0 = (long long)out0 + (t - lane) + T * q - a.b_pos;
+        if (p0 < 0) {  // lanes before the chunk start hold no bits
+          m >>= (int)(-p0);
+          p0 = 0;
+        }
+        const long long w = p0 >> 5;
+        const int sh = (int)(p0 & 31);
+        atomicOr(&a.pulse_bits[w], m << sh);
+        if (sh && (m >> (32 - sh))) atomicOr(&a.pulse_bits[w + 1], m >> (32 - sh));
+      }
+    }
   }
 }
 
 // K1b: demod -> video + sync, blocks 2x and 2x+1 of the tile.
-__global__ void __launch_bounds__(kThreadsB, 1) k1b_kernel(DemodArgs a, int f_begin) {
+template <class Src>
+__global__ void __launch_bounds__(kThreadsB, 1) k1b_kernel(const __grid_constant__ Src src, int f_begin) {
   constexpr int N = Design::kNb, T = kThreadsB;
+  const DemodArgs& a = src.get();
+  if (f_begin + (int)blockIdx.y >= a.tiles) return;  // whole CTA
   chain_wait();
   extern __shared__ float2 sm[];
   float2* sA = sm;
@@ -284,7 +308,9 @@ __device__ __forceinline__ void edge_masks(const float* __restrict__ x, long lon
   rm = 0;
   if (i0 >= total) return;
   float v[kEdgePer];
-  if (i0 + kEdgePer <= total) {
+  // 16-byte loads where the signal is 16-byte aligned (a batched capture's
+  // sync may start at any sample)
+  if (i0 + kEdgePer <= total && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
     const float4* p = reinterpret_cast<const float4*>(x + i0);
 #pragma unroll
     for (int q = 0; q < kEdgePer / 4; q++) {
@@ -356,8 +382,7 @@ __global__ void __launch_bounds__(kEdgeThreads) edge_count_kernel(const float* _
 // the runs' totals are scanned with warp shuffles, then each thread writes its
 // run's offsets.
 constexpr int kScanThreads = 1024;
-__global__ void __launch_bounds__(kScanThreads) edge_scan_kernel(int2* __restrict__ blk, int nblk,
-                                                                 int* __restrict__ counts) {
+__device__ __forceinline__ void scan_blocks(int2* __restrict__ blk, int nblk, int* __restrict__ counts) {
   __shared__ int2 warp_tot[kScanThreads / 32];
   chain_wait();
   const int per = (nblk + kScanThreads - 1) / kScanThreads;
@@ -410,6 +435,12 @@ __global__ void __launch_bounds__(kScanThreads) edge_scan_kernel(int2* __restric
   }
 }
 
+
+__global__ void __launch_bounds__(kScanThreads) edge_scan_kernel(int2* __restrict__ blk, int nblk,
+                                                                 int* __restrict__ counts) {
+  scan_blocks(blk, nblk, counts);
+}
+
 __global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(long long total, const unsigned* __restrict__ masks,
                                                                   const int2* __restrict__ blk,
                                                                   unsigned* __restrict__ fall,
@@ -436,20 +467,131 @@ __global__ void __launch_bounds__(kEdgeThreads) edge_write_kernel(long long tota
   }
 }
 
+// Threshold edges from in-pulse bits: one thread per 32-position word (a CTA
+// 8192 positions).  falling = in now and not before, rising = out now and in
+// before; position 0 counts as preceded by "out" (a pulse open there falls
+// there), positions at or past total hold no bits.
+constexpr int kBitEdgeSeg = kEdgeThreads * 32;
+
+__device__ __forceinline__ void bit_edges(const unsigned* __restrict__ bits, long long total, long long w,
+                                          unsigned& fm, unsigned& rm) {
+  const long long p0 = w * 32;
+  fm = rm = 0;
+  if (p0 >= total) return;
+  const unsigned valid = total - p0 >= 32 ? 0xffffffffu : ((1u << (unsigned)(total - p0)) - 1u);
+  const unsigned in = __ldg(&bits[w]) & valid;
+  const unsigned prev = w > 0 ? (__ldg(&bits[w - 1]) >> 31) : 0u;
+  const unsigned before = (in << 1) | prev;  // bit j: in at position j - 1
+  fm = in & ~before;
+  rm = ~in & before & valid;
+}
+
+template <class Src>
+__global__ void __launch_bounds__(kEdgeThreads) edge_bits_count_kernel(const __grid_constant__ Src src) {
+  const EdgeArgs& e = src.get();
+  if ((long long)blockIdx.x * kBitEdgeSeg >= e.total) return;  // whole CTA
+  chain_wait();
+  const long long w = (long long)blockIdx.x * kEdgeThreads + threadIdx.x;
+  unsigned fm, rm;
+  bit_edges(e.bits, e.total, w, fm, rm);
+  int pa, pb;
+  const int2 tot = block_scan2(__popc(fm), __popc(rm), pa, pb);
+  if (threadIdx.x == 0) e.blk[blockIdx.x] = tot;
+}
+
+template <class Src>
+__global__ void __launch_bounds__(kScanThreads) edge_bits_scan_kernel(const __grid_constant__ Src src) {
+  const EdgeArgs& e = src.get();
+  scan_blocks(e.blk, (int)((e.total + kBitEdgeSeg - 1) / kBitEdgeSeg), e.counts);
+}
+
+template <class Src>
+__global__ void __launch_bounds__(kEdgeThreads) edge_bits_write_kernel(const __grid_constant__ Src src) {
+  const EdgeArgs& e = src.get();
+  if ((long long)blockIdx.x * kBitEdgeSeg >= e.total) return;  // whole CTA
+  chain_wait();
+  const long long w = (long long)blockIdx.x * kEdgeThreads + threadIdx.x;
+  unsigned fm, rm;
+  bit_edges(e.bits, e.total, w, fm, rm);
+  int pa, pb;
+  block_scan2(__popc(fm), __popc(rm), pa, pb);
+  int kf = e.blk[blockIdx.x].x + pa, kr = e.blk[blockIdx.x].y + pb;
+  const long long p0 = w * 32;
+  while (fm) {
+    const int j = __ffs(fm) - 1;
+    fm &= fm - 1;
+    if (kf < e.cap) e.fall[kf] = (unsigned)(p0 + j);
+    kf++;
+  }
+  while (rm) {
+    const int j = __ffs(rm) - 1;
+    rm &= rm - 1;
+    if (kr < e.cap) e.rise[kr] = (unsigned)(p0 + j);
+    kr++;
+  }
+}
+
 }  // namespace
+
+size_t pulse_bit_words(long long total) { return (size_t)((total + 31) / 32) + 1; }
+
+void launch_edges_bits(const unsigned* bits, long long total, unsigned* fall, unsigned* rise, int* counts, int cap,
+                       int2* blk, cudaStream_t st) {
+  const int nblk = (int)((total + kBitEdgeSeg - 1) / kBitEdgeSeg);
+  if (nblk <= 0) return;
+  ArgsOne<EdgeArgs> e;
+  e.a[0].bits = bits;
+  e.a[0].total = total;
+  e.a[0].blk = blk;
+  e.a[0].counts = counts;
+  e.a[0].fall = fall;
+  e.a[0].rise = rise;
+  e.a[0].cap = cap;
+  using S = ArgsOne<EdgeArgs>;
+  launch_chained(edge_bits_count_kernel<S>, dim3(nblk), dim3(kEdgeThreads), 0, st, e);
+  launch_chained(edge_bits_scan_kernel<S>, dim3(1), dim3(kScanThreads), 0, st, e);
+  launch_chained(edge_bits_write_kernel<S>, dim3(nblk), dim3(kEdgeThreads), 0, st, e);
+}
+
+void launch_edges_bits_many(const ArgsMany<EdgeArgs>& e, int portions, long long max_total, cudaStream_t st) {
+  const int nblk = (int)((max_total + kBitEdgeSeg - 1) / kBitEdgeSeg);
+  if (nblk <= 0 || portions <= 0) return;
+  using S = ArgsMany<EdgeArgs>;
+  launch_chained(edge_bits_count_kernel<S>, dim3(nblk, 1, portions), dim3(kEdgeThreads), 0, st, e);
+  launch_chained(edge_bits_scan_kernel<S>, dim3(1, 1, portions), dim3(kScanThreads), 0, st, e);
+  launch_chained(edge_bits_write_kernel<S>, dim3(nblk, 1, portions), dim3(kEdgeThreads), 0, st, e);
+}
 
 void launch_k1a(const DemodArgs& a, int f0, int nf, cudaStream_t st) {
   if (nf <= 0) return;
   const size_t smem = 2 * sizeof(float2) * fft_pad(Design::kNa);
   const int blocks = (a.spp + a.a_out - 1) / a.a_out;  // = env_blocks
   dim3 grid((blocks + 1) / 2, nf);
+  const ArgsOne<DemodArgs> src{a};
   auto go = [&](auto kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    launch_chained(kernel, grid, dim3(kThreadsA), smem, st, a, f0);
+    launch_chained(kernel, grid, dim3(kThreadsA), smem, st, src, f0);
   };
-  if (a.in_fmt == kInS16) go(k1a_kernel<kInS16>);
-  else if (a.in_fmt == kInU16) go(k1a_kernel<kInU16>);
-  else go(k1a_kernel<kInU8>);
+  using S = ArgsOne<DemodArgs>;
+  if (a.in_fmt == kInS16) go(k1a_kernel<kInS16, S>);
+  else if (a.in_fmt == kInU16) go(k1a_kernel<kInU16, S>);
+  else go(k1a_kernel<kInU8, S>);
+}
+
+void launch_k1a_many(const ArgsMany<DemodArgs>& p, int portions, int max_tiles, cudaStream_t st) {
+  if (portions <= 0 || max_tiles <= 0) return;
+  const DemodArgs& a = p.a[0];  // the design constants every capture of a round shares
+  const size_t smem = 2 * sizeof(float2) * fft_pad(Design::kNa);
+  const int blocks = (a.spp + a.a_out - 1) / a.a_out;
+  dim3 grid((blocks + 1) / 2, max_tiles, portions);
+  auto go = [&](auto kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    launch_chained(kernel, grid, dim3(kThreadsA), smem, st, p, 0);
+  };
+  using S = ArgsMany<DemodArgs>;
+  if (a.in_fmt == kInS16) go(k1a_kernel<kInS16, S>);
+  else if (a.in_fmt == kInU16) go(k1a_kernel<kInU16, S>);
+  else go(k1a_kernel<kInU8, S>);
 }
 
 namespace {
@@ -492,10 +634,23 @@ void launch_dc_mean(const uint8_t* raw, int n, int in_fmt, unsigned long long* s
 void launch_k1b(const DemodArgs& a, int f0, int nf, cudaStream_t st) {
   if (nf <= 0) return;
   const size_t smem = 2 * sizeof(float2) * fft_pad(Design::kNb);
-  cudaFuncSetAttribute(k1b_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  using S = ArgsOne<DemodArgs>;
+  cudaFuncSetAttribute(k1b_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int blocks = (a.spp + a.b_out - 1) / a.b_out;
   dim3 grid((blocks + 1) / 2, nf);
-  launch_chained(k1b_kernel, grid, dim3(kThreadsB), smem, st, a, f0);
+  const S src{a};
+  launch_chained(k1b_kernel<S>, grid, dim3(kThreadsB), smem, st, src, f0);
+}
+
+void launch_k1b_many(const ArgsMany<DemodArgs>& p, int portions, int max_tiles, cudaStream_t st) {
+  if (portions <= 0 || max_tiles <= 0) return;
+  const DemodArgs& a = p.a[0];
+  const size_t smem = 2 * sizeof(float2) * fft_pad(Design::kNb);
+  using S = ArgsMany<DemodArgs>;
+  cudaFuncSetAttribute(k1b_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int blocks = (a.spp + a.b_out - 1) / a.b_out;
+  dim3 grid((blocks + 1) / 2, max_tiles, portions);
+  launch_chained(k1b_kernel<S>, grid, dim3(kThreadsB), smem, st, p, 0);
 }
 
 int edge_blocks(long long total) { return (int)((total + kEdgeSeg - 1) / kEdgeSeg); }

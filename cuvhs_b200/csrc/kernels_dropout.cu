@@ -226,7 +226,10 @@ __global__ void __launch_bounds__(kThreadsD) dropout_kernel(DropoutArgs a) {
 // [x*256, x*256 + 256) of field y.  The 4096 envelope samples behind them are
 // staged with coalesced loads into rows of 17 floats (conflict-free column
 // reads), then each thread sums its row in sample order.
-__global__ void __launch_bounds__(kThreadsD) dropout_class_kernel(DropoutArgs a) {
+template <class Src>
+__global__ void __launch_bounds__(kThreadsD) dropout_class_kernel(const __grid_constant__ Src src) {
+  const DropoutArgs& a = src.get();
+  if ((int)blockIdx.y >= a.fields) return;  // whole CTA: a batched capture with fewer fields
   chain_wait();
   __shared__ float stage[kThreadsD * 17];
   __shared__ double part[kMaxEnvBlocks];
@@ -327,7 +330,10 @@ __device__ __forceinline__ int block_excl_last(int v, int* wsh) {
 // One CTA per field: class bytes back from L2 into shared memory, then the
 // hysteresis scan, event list, mapping and luma concealment (chroma is
 // concealed by dropout_chroma_kernel once the chroma planes are final).
-__global__ void __launch_bounds__(kThreadsScan) dropout_scan_kernel(DropoutArgs a) {
+template <class Src>
+__global__ void __launch_bounds__(kThreadsScan) dropout_scan_kernel(const __grid_constant__ Src src) {
+  const DropoutArgs& a = src.get();
+  if ((int)blockIdx.x >= a.fields) return;  // whole CTA
   chain_wait();
   extern __shared__ uint4 cls4[];  // [a.max_blocks / 16]
   __shared__ int wsh[32];
@@ -343,8 +349,8 @@ __global__ void __launch_bounds__(kThreadsScan) dropout_scan_kernel(DropoutArgs 
     return;  // whole CTA leaves together
   }
   const int nb = min((s1 - s0 + 15) / 16, a.max_blocks);
-  const uint4* src = reinterpret_cast<const uint4*>(a.cls + (size_t)f * a.max_blocks);
-  for (int i = tid; i < (nb + 15) / 16; i += kThreadsScan) cls4[i] = src[i];
+  const uint4* cls_in = reinterpret_cast<const uint4*>(a.cls + (size_t)f * a.max_blocks);
+  for (int i = tid; i < (nb + 15) / 16; i += kThreadsScan) cls4[i] = cls_in[i];
   __syncthreads();
   const int per = (nb + kThreadsScan - 1) / kThreadsScan;
   const int b_lo = min(nb, tid * per), b_hi = min(nb, b_lo + per);
@@ -372,7 +378,9 @@ __global__ void __launch_bounds__(kThreadsScan) dropout_scan_kernel(DropoutArgs 
 }
 
 // One warp per field: chroma concealment from the entries the scan kernel wrote.
-__global__ void dropout_chroma_kernel(DropoutArgs a, int f0, int nf) {
+template <class Src>
+__global__ void dropout_chroma_kernel(const __grid_constant__ Src src, int f0, int nf) {
+  const DropoutArgs& a = src.get();
   chain_wait();
   const int f = f0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (f >= f0 + nf || f >= a.fields) return;  // whole warp
@@ -397,19 +405,41 @@ cudaError_t launch_dropouts(const DropoutArgs& a, cudaStream_t st) {
 
 size_t dropout_class_bytes_per_field(int spp) { return (size_t)(((spp + 15) / 16 + 15) / 16 * 16); }
 
+namespace {
+template <class S>
+void two_pass_launch(const S& src, const DropoutArgs& a, int portions, int max_fields, cudaStream_t st) {
+  dim3 grid((a.max_blocks + kThreadsD - 1) / kThreadsD, max_fields, portions);
+  launch_chained(dropout_class_kernel<S>, grid, dim3(kThreadsD), 0, st, src);
+  const size_t smem = (size_t)a.max_blocks;
+  cudaFuncSetAttribute(dropout_scan_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxClassBytes);
+  launch_chained(dropout_scan_kernel<S>, dim3(max_fields, 1, portions), dim3(kThreadsScan), smem, st, src);
+}
+
+template <class S>
+void conceal_launch(const S& src, int portions, int f0, int nf, cudaStream_t st) {
+  const int threads = 128;
+  launch_chained(dropout_chroma_kernel<S>, dim3((nf * 32 + threads - 1) / threads, 1, portions), dim3(threads), 0, st,
+                 src, f0, nf);
+}
+}  // namespace
+
 void launch_dropouts_two_pass(const DropoutArgs& a, cudaStream_t st) {
   if (a.fields <= 0) return;
-  dim3 grid((a.max_blocks + kThreadsD - 1) / kThreadsD, a.fields);
-  launch_chained(dropout_class_kernel, grid, dim3(kThreadsD), 0, st, a);
-  const size_t smem = (size_t)a.max_blocks;
-  cudaFuncSetAttribute(dropout_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxClassBytes);
-  launch_chained(dropout_scan_kernel, dim3(a.fields), dim3(kThreadsScan), smem, st, a);
+  two_pass_launch(ArgsOne<DropoutArgs>{a}, a, 1, a.fields, st);
 }
 
 void launch_dropout_conceal_chroma(const DropoutArgs& a, int f0, int nf, cudaStream_t st) {
   if (nf <= 0 || f0 < 0 || f0 >= a.fields) return;
-  const int threads = 128;
-  launch_chained(dropout_chroma_kernel, dim3((nf * 32 + threads - 1) / threads), dim3(threads), 0, st, a, f0, nf);
+  conceal_launch(ArgsOne<DropoutArgs>{a}, 1, f0, nf, st);
+}
+
+void launch_dropouts_two_pass_many(const ArgsMany<DropoutArgs>& p, int portions, int max_fields, cudaStream_t st) {
+  if (portions > 0 && max_fields > 0) two_pass_launch(p, p.a[0], portions, max_fields, st);
+}
+
+void launch_dropout_conceal_chroma_many(const ArgsMany<DropoutArgs>& p, int portions, int max_fields,
+                                        cudaStream_t st) {
+  if (portions > 0 && max_fields > 0) conceal_launch(p, portions, 0, max_fields, st);
 }
 
 }  // namespace cuvhs

@@ -122,8 +122,9 @@ __device__ __forceinline__ void phase_clock(const GuardArgs& g, int y, int k) {
   if (g.dbg_clk && threadIdx.x == 0 && y < kGuardClockSamples) g.dbg_clk[(size_t)y * kPhaseSlots + k] = clock64();
 }
 
-template <int FMT>
-__global__ void __launch_bounds__(kGT) guard_kernel(GuardArgs g) {
+template <int FMT, class Src>
+__global__ void __launch_bounds__(kGT) guard_kernel(const __grid_constant__ Src src) {
+  const GuardArgs& g = src.get();
   chain_wait();
   extern __shared__ double2 gsm[];
   double2* buf = gsm;                                        // [kN]
@@ -264,6 +265,7 @@ __global__ void __launch_bounds__(kGT) guard_kernel(GuardArgs g) {
       double x64 = 0.0;
       for (int w = 0; w < kGT / 32; w++) x64 += red[w];
       const bool in_pulse = x64 <= g.thr_hz;  // the reference's FP64 decision
+      if (g.flips && in_pulse != (g.sync[s] <= g.thr_rel)) atomicAdd(g.flips, 1);
       float r = (float)(x64 - g.ire0);
       if (in_pulse && !(r <= g.thr_rel)) r = g.thr_rel;
       if (!in_pulse && r <= g.thr_rel) r = nextafterf(g.thr_rel, 3.0e38f);
@@ -288,19 +290,34 @@ bool guard_supported(int ha, int hb) {
   return 2 * ha + 2 <= kN && hb < kOverlap && guard_smem_bytes(hb) <= (size_t)kMaxClassBytes;
 }
 
-cudaError_t launch_sync_guard(const GuardArgs& g, cudaStream_t st) {
-  if (!guard_supported(g.ha, g.hb) || g.cap <= 0) return cudaErrorInvalidValue;
+namespace {
+template <class S>
+cudaError_t launch_guard(const S& src, const GuardArgs& g, int portions, int ctas, cudaStream_t st) {
   const size_t smem = guard_smem_bytes(g.hb);
-  // a typical chunk lists a few dozen samples, each on its own SM; two CTAs fit an SM
-  const int ctas = std::max(1, std::min(g.cap, 148 * 2));
   auto go = [&](auto kernel) {
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    return launch_chained(kernel, dim3(ctas), dim3(kGT), smem, st, g);
+    return launch_chained(kernel, dim3(ctas, 1, portions), dim3(kGT), smem, st, src);
   };
-  if (g.in_fmt == kInS16) return go(guard_kernel<kInS16>);
-  if (g.in_fmt == kInU16) return go(guard_kernel<kInU16>);
-  return go(guard_kernel<kInU8>);
+  if (g.in_fmt == kInS16) return go(guard_kernel<kInS16, S>);
+  if (g.in_fmt == kInU16) return go(guard_kernel<kInU16, S>);
+  return go(guard_kernel<kInU8, S>);
+}
+}  // namespace
+
+cudaError_t launch_sync_guard(const GuardArgs& g, cudaStream_t st) {
+  if (!guard_supported(g.ha, g.hb) || g.cap <= 0) return cudaErrorInvalidValue;
+  // a typical chunk lists a few dozen samples, each on its own SM; two CTAs fit an SM
+  const int ctas = std::max(1, std::min(g.cap, 148 * 2));
+  return launch_guard(ArgsOne<GuardArgs>{g}, g, 1, ctas, st);
+}
+
+cudaError_t launch_sync_guard_many(const ArgsMany<GuardArgs>& p, int portions, cudaStream_t st) {
+  if (portions <= 0) return cudaSuccess;
+  const GuardArgs& g = p.a[0];  // the design every capture of a round shares
+  if (!guard_supported(g.ha, g.hb) || g.cap <= 0) return cudaErrorInvalidValue;
+  const int ctas = std::max(1, std::min(g.cap, (148 * 2 + portions - 1) / portions));
+  return launch_guard(p, g, portions, ctas, st);
 }
 
 }  // namespace cuvhs

@@ -86,7 +86,9 @@ constexpr int kWinThreads = 1024;
 constexpr int kWinSmemCand = 12288;  // candidates clustered in shared memory; more: the serial path
 size_t fieldwin_smem_bytes() { return (size_t)kWinSmemCand * 2 * sizeof(int); }
 
-__global__ void __launch_bounds__(kWinThreads) fieldwin_kernel(LineLocArgs a) {
+template <class Src>
+__global__ void __launch_bounds__(kWinThreads) fieldwin_kernel(const __grid_constant__ Src src) {
+  const LineLocArgs& a = src.get();
   chain_wait();
   extern __shared__ int wsm[];
   int* scand = wsm;                  // [kWinSmemCand] candidate positions
@@ -180,7 +182,9 @@ __global__ void __launch_bounds__(kWinThreads) fieldwin_kernel(LineLocArgs a) {
 // Grid (num_fields): the pulses of field f's window (sync_pulses.cu:10-58):
 // threshold runs that start after the window start and end within the
 // spp-sample scan, at most kMaxPulses.
-__global__ void __launch_bounds__(kLT) pulses_kernel(LineLocArgs a) {
+template <class Src>
+__global__ void __launch_bounds__(kLT) pulses_kernel(const __grid_constant__ Src src) {
+  const LineLocArgs& a = src.get();
   chain_wait();
   __shared__ int brk;
   const int f = blockIdx.x;
@@ -247,58 +251,83 @@ __device__ double predicted_field_lines(const Format& fmt, bool first) {
 
 __device__ double half_line_round(double lines) { return round(0.5 * round(lines / 0.5) * 10.0) / 10.0; }
 
+// Width classes as integer bounds: a pulse length (an integer) lies in
+// [lo, hi] exactly when it lies in [ceil(lo), floor(hi)].
+struct IWindows {
+  int h_lo, h_hi, e_lo, e_hi, v_lo, v_hi;
+};
+__device__ __forceinline__ int ceil_int(double x) { return (int)fmin(fmax(ceil(x), -2147483647.0), 2147483647.0); }
+__device__ __forceinline__ int floor_int(double x) { return (int)fmin(fmax(floor(x), -2147483647.0), 2147483647.0); }
+__device__ IWindows int_windows(const Windows& w) {
+  IWindows r;
+  r.h_lo = ceil_int(w.h_lo);
+  r.h_hi = floor_int(w.h_hi);
+  r.e_lo = ceil_int(w.e_lo);
+  r.e_hi = floor_int(w.e_hi);
+  r.v_lo = ceil_int(w.v_lo);
+  r.v_hi = floor_int(w.v_hi);
+  return r;
+}
+__device__ __forceinline__ bool in_class(int len, int lo, int hi) { return len >= lo && len <= hi; }
+
 // The vertical-blanking recogniser (pipeline.cu:519-609) from pulse `first`,
 // over at most 26 pulses, entered with an hsync as the list's last entry.
-// Writes each appended entry's pulse index and type when emit_idx is given;
-// returns whether the sequence closed, with the number appended and the
-// type of the last one.
-__device__ bool attempt(const int* ps, const int* pl, int n, int first, const Windows& w, int eq_pulses, int line_len,
-                        int* appended, int* last_type, int* emit_idx, unsigned char* emit_type) {
+// Returns whether the sequence closed, with the number appended and the type
+// of the last one.  With out_s given, the appended entries (start, length,
+// type) are written there.  Widths and the hold-off position are compared as
+// integers: a start x (an integer) is past the FP64 hold-off h exactly when
+// x > floor(h), and before it exactly when x < ceil(h).
+__device__ bool attempt(const int* ps, const int* pl, int n, int first, const IWindows& w, int eq_pulses, int line_len,
+                        int* appended, int* last_type, int* out_s = nullptr, int* out_l = nullptr,
+                        unsigned char* out_t = nullptr) {
   bool done = false;
   const double half = eq_pulses / 2.0;
   bool vsync_seen = false;
-  double hold_until = 0.0, pending = -1.0;
+  long long hold_floor = 0, hold_ceil = 0;  // of the FP64 hold-off position (0.0 at first)
+  double pending = -1.0;
   int cur = kHsync, cnt = 0;
-  for (int i = first; i < n && i < first + 26; i++) {
-    const double len = (double)pl[i];
+  const int end = min(n, first + 26);
+  for (int i = first; i < end; i++) {
+    const int len = pl[i];
+    const int start = ps[i];
     int type = -1;
     switch (cur) {
       case kHsync:
-        if (within(len, w.h_lo, w.h_hi)) {
+        if (in_class(len, w.h_lo, w.h_hi)) {
           type = kHsync;
-        } else if (within(len, w.e_lo, w.e_hi)) {
+        } else if (in_class(len, w.e_lo, w.e_hi)) {
           type = kEq1;
           pending = half;
-        } else if (within(len, w.v_lo, w.v_hi)) {
+        } else if (in_class(len, w.v_lo, w.v_hi)) {
           vsync_seen = true;
           type = kVsync;
         }
         break;
       case kEq1:
-        if (within(len, w.e_lo, w.e_hi)) {
+        if (in_class(len, w.e_lo, w.e_hi)) {
           type = kEq1;
-        } else if (within(len, w.v_lo, w.v_hi)) {
+        } else if (in_class(len, w.v_lo, w.v_hi)) {
           vsync_seen = true;
           type = kVsync;
           pending = half;
-        } else if (within(len, w.h_lo, w.h_hi)) {
+        } else if (in_class(len, w.h_lo, w.h_hi)) {
           type = kHsync;
         }
         break;
       case kVsync:
-        if (within(len, w.e_lo, w.e_hi)) {
+        if (in_class(len, w.e_lo, w.e_hi)) {
           type = kEq2;
           pending = half;
-        } else if (within(len, w.v_lo, w.v_hi)) {
+        } else if (in_class(len, w.v_lo, w.v_hi)) {
           type = kVsync;
-        } else if ((double)ps[i] > hold_until && within(len, w.h_lo, w.h_hi)) {
+        } else if ((long long)start > hold_floor && in_class(len, w.h_lo, w.h_hi)) {
           type = kHsync;
         }
         break;
       case kEq2:
-        if (within(len, w.e_lo, w.e_hi)) {
+        if (in_class(len, w.e_lo, w.e_hi)) {
           type = kEq2;
-        } else if (within(len, w.h_lo, w.h_hi)) {
+        } else if (in_class(len, w.h_lo, w.h_hi)) {
           type = kHsync;
           done = true;
         }
@@ -306,17 +335,20 @@ __device__ bool attempt(const int* ps, const int* pl, int n, int first, const Wi
     }
     bool keep = type >= 0;
     if (keep && type != cur) {
-      if ((double)ps[i] < hold_until) {
+      if ((long long)start < hold_ceil) {
         keep = false;
       } else if (pending > 0.0) {
-        hold_until = (double)ps[i] + ((pending - 0.1) * (double)line_len);
+        const double hold = (double)start + ((pending - 0.1) * (double)line_len);
+        hold_floor = (long long)floor(hold);
+        hold_ceil = (long long)ceil(hold);
         pending = -1.0;
       }
     }
     if (keep) {
-      if (emit_idx) {
-        emit_idx[cnt] = i;
-        emit_type[cnt] = (unsigned char)type;
+      if (out_s) {
+        out_s[cnt] = start;
+        out_l[cnt] = len;
+        out_t[cnt] = (unsigned char)type;
       }
       cnt++;
       cur = type;
@@ -373,7 +405,7 @@ struct FieldSmem {
 // Pulse validation (pipeline.cu:611-648) into v; returns the entry count.
 __device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
   const Format& fmt = a.fmt;
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   // width classes adapted to the field's mean hsync width (pipeline.cu:450-477)
   const double tol = fmt.fs_hz * 0.5e-6;
   const double loose_lo = fmt.hsync_width - 3.5 * tol, loose_hi = fmt.hsync_width + 4.0 * tol;
@@ -390,90 +422,92 @@ __device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
   phase_clock(a, blockIdx.x, 21);
   const double est = lcnt > 0 ? ((double)lsum / (double)lcnt) : fmt.hsync_width;
   const double shift = est - fmt.hsync_width;
-  Windows w;
+  Windows wd;
   const double hnom = fmt.hsync_width + shift;
-  w.h_lo = hnom - tol;
-  w.h_hi = hnom + tol;
-  w.e_lo = fmt.eq_pulse_width + shift - tol;
-  w.e_hi = fmt.eq_pulse_width + shift + tol;
-  w.v_lo = (fmt.vsync_width + shift) * 0.5;
-  w.v_hi = fmt.vsync_width + shift + 2.0 * tol;
+  wd.h_lo = hnom - tol;
+  wd.h_hi = hnom + tol;
+  wd.e_lo = fmt.eq_pulse_width + shift - tol;
+  wd.e_hi = fmt.eq_pulse_width + shift + tol;
+  wd.v_lo = (fmt.vsync_width + shift) * 0.5;
+  wd.v_hi = fmt.vsync_width + shift + 2.0 * tol;
+  const IWindows w = int_windows(wd);
   // classes and every recogniser attempt
   for (int i = t; i < n; i += kLT) {
-    const double len = (double)sm.pl[i];
-    const bool h = within(len, w.h_lo, w.h_hi);
-    const bool e = !h && i > 2 && within(len, w.e_lo, w.e_hi);
+    const int len = sm.pl[i];
+    const bool h = in_class(len, w.h_lo, w.h_hi);
+    const bool e = !h && i > 2 && in_class(len, w.e_lo, w.e_hi);
     sm.cls[i] = (h ? 1 : 0) | (e ? 2 : 0);
     int cnt = 0, last = kHsync;
     bool ok = false;
-    if (e) ok = attempt(sm.ps, sm.pl, n, i - 2, w, fmt.num_eq_pulses, fmt.samples_per_line, &cnt, &last, nullptr,
-                        nullptr);
+    if (e) ok = attempt(sm.ps, sm.pl, n, i - 2, w, fmt.num_eq_pulses, fmt.samples_per_line, &cnt, &last);
     sm.att_ok[i] = ok ? 1 : 0;
     sm.att_len[i] = cnt;
     sm.att_last[i] = (unsigned char)last;
   }
   __syncthreads();
   phase_clock(a, blockIdx.x, 22);
-  // which attempts fire: at an EQ-width pulse while the list's last entry is
+  // Which attempts fire: at an EQ-width pulse while the list's last entry is
   // an hsync.  The list's state before pulse i -- empty, last entry an hsync,
   // or last entry something else -- follows from pulse i-1's state by a map
   // of the three states (an hsync pulse sets "hsync"; a firing attempt sets
-  // its last type; other pulses change nothing), so one warp scans the maps
-  // (composition is associative), each lane over a run of pulses, and every
-  // pulse's output length and position follow.
-  if (t < 32) {
-    const int lane = t;
-    const int per = (n + 31) / 32;
-    const int i0 = min(n, lane * per), i1 = min(n, i0 + per);
-    // map of pulse i: 2 bits per incoming state (0 empty, 1 hsync, 2 other)
-    auto pulse_map = [&](int i) -> unsigned {
-      if (sm.cls[i] & 1) return 1u | (1u << 2) | (1u << 4);  // every state -> hsync
-      if ((sm.cls[i] & 2) && sm.att_ok[i]) {
-        const unsigned after = sm.att_last[i] == kHsync ? 1u : 2u;
-        return 0u | (after << 2) | (2u << 4);  // fires only after an hsync
-      }
-      return 0u | (1u << 2) | (2u << 4);  // identity
-    };
-    auto apply = [](unsigned m, unsigned st) { return (m >> (2 * st)) & 3u; };
-    auto compose = [&](unsigned first, unsigned then) {  // then(first(s))
-      unsigned r = 0;
-      for (unsigned st = 0; st < 3; st++) r |= apply(then, apply(first, st)) << (2 * st);
-      return r;
-    };
-    unsigned m = 0u | (1u << 2) | (2u << 4);
-    for (int i = i0; i < i1; i++) m = compose(m, pulse_map(i));
-    // exclusive scan of the lane maps in lane order
-    unsigned pre = m;
-    for (int off = 1; off < 32; off <<= 1) {
-      const unsigned o = __shfl_up_sync(0xffffffffu, pre, off);
-      if (lane >= off) pre = compose(o, pre);
+  // its last type; other pulses change nothing).  Composition is associative,
+  // so the whole CTA scans the maps (each thread over a run of pulses), and
+  // every pulse's output length and position follow from a second scan.
+  auto pulse_map = [&](int i) -> unsigned {  // 2 bits per incoming state (0 empty, 1 hsync, 2 other)
+    if (sm.cls[i] & 1) return 1u | (1u << 2) | (1u << 4);  // every state -> hsync
+    if ((sm.cls[i] & 2) && sm.att_ok[i]) {
+      const unsigned after = sm.att_last[i] == kHsync ? 1u : 2u;
+      return 0u | (after << 2) | (2u << 4);  // fires only after an hsync
     }
-    unsigned excl = __shfl_up_sync(0xffffffffu, pre, 1);
-    if (lane == 0) excl = 0u | (1u << 2) | (2u << 4);
-    // each pulse's output length with the state it meets, then their prefix
-    unsigned st = apply(excl, 0);  // the list starts empty
-    int len_sum = 0;
-    for (int i = i0; i < i1; i++) {
-      int len = 0;
-      if (sm.cls[i] & 1) len = 1;
-      else if ((sm.cls[i] & 2) && sm.att_ok[i] && st == 1) len = sm.att_len[i];
-      sm.pos[i] = len;
-      len_sum += len;
-      st = apply(pulse_map(i), st);
-    }
-    int incl = len_sum;
-    for (int off = 1; off < 32; off <<= 1) {
-      const int o = __shfl_up_sync(0xffffffffu, incl, off);
-      if (lane >= off) incl += o;
-    }
-    int run = incl - len_sum;
-    for (int i = i0; i < i1; i++) {
-      const int len = sm.pos[i];
-      sm.pos[i] = run;
-      run += len;
-    }
-    if (lane == 31) sm.pos[n] = incl;
+    return 0u | (1u << 2) | (2u << 4);  // identity
+  };
+  auto apply = [](unsigned m, unsigned st) { return (m >> (2 * st)) & 3u; };
+  auto compose = [&](unsigned first, unsigned then) {  // then(first(s))
+    return apply(then, apply(first, 0)) | (apply(then, apply(first, 1)) << 2) | (apply(then, apply(first, 2)) << 4);
+  };
+  constexpr unsigned kIdentity = 0u | (1u << 2) | (2u << 4);
+  __shared__ unsigned warp_map[kLT / 32];
+  __shared__ int warp_len[kLT / 32];
+  const int per = (n + kLT - 1) / kLT;
+  const int i0 = min(n, t * per), i1 = min(n, i0 + per);
+  unsigned m = kIdentity;
+  for (int i = i0; i < i1; i++) m = compose(m, pulse_map(i));
+  unsigned incl = m;
+  for (int off = 1; off < 32; off <<= 1) {
+    const unsigned o = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl = compose(o, incl);
   }
+  if (lane == 31) warp_map[warp] = incl;
+  __syncthreads();
+  unsigned before = kIdentity;  // the maps of every earlier warp
+  for (int w2 = 0; w2 < warp; w2++) before = compose(before, warp_map[w2]);
+  unsigned excl = __shfl_up_sync(0xffffffffu, incl, 1);
+  if (lane == 0) excl = kIdentity;
+  unsigned st = apply(compose(before, excl), 0);  // the list starts empty
+  int len_sum = 0;
+  for (int i = i0; i < i1; i++) {
+    int len = 0;
+    if (sm.cls[i] & 1) len = 1;
+    else if ((sm.cls[i] & 2) && sm.att_ok[i] && st == 1) len = sm.att_len[i];
+    sm.pos[i] = len;
+    len_sum += len;
+    st = apply(pulse_map(i), st);
+  }
+  int lincl = len_sum;
+  for (int off = 1; off < 32; off <<= 1) {
+    const int o = __shfl_up_sync(0xffffffffu, lincl, off);
+    if (lane >= off) lincl += o;
+  }
+  if (lane == 31) warp_len[warp] = lincl;
+  __syncthreads();
+  int run = lincl - len_sum;
+  for (int w2 = 0; w2 < warp; w2++) run += warp_len[w2];
+  for (int i = i0; i < i1; i++) {
+    const int len = sm.pos[i];
+    sm.pos[i] = run;
+    run += len;
+  }
+  if (t == kLT - 1) sm.pos[n] = run;  // the last thread ends at the total
   __syncthreads();
   phase_clock(a, blockIdx.x, 23);
   const int nv = sm.pos[n];
@@ -486,15 +520,9 @@ __device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
       v.l[p] = sm.pl[i];
       v.tg[p] = kHsync;
     } else {
-      int idx[26];
-      unsigned char ty[26];
       int cnt = 0, last = 0;
-      attempt(sm.ps, sm.pl, n, i - 2, w, fmt.num_eq_pulses, fmt.samples_per_line, &cnt, &last, idx, ty);
-      for (int k = 0; k < cnt; k++) {
-        v.s[p + k] = sm.ps[idx[k]];
-        v.l[p + k] = sm.pl[idx[k]];
-        v.tg[p + k] = ty[k];
-      }
+      attempt(sm.ps, sm.pl, n, i - 2, w, fmt.num_eq_pulses, fmt.samples_per_line, &cnt, &last, v.s + p, v.l + p,
+              v.tg + p);
     }
   }
   __syncthreads();
@@ -824,16 +852,53 @@ __device__ AnchorFit fit_anchor(FieldSmem& sm, const BlankingScan& s, const VLis
   }
   __syncthreads();
   stamp(28);
+  // the counted terms packed in list order (a block scan over contiguous
+  // strips), so the one thread that adds them in the reference's order reads
+  // only counted terms
+  const int end = min(sm.imin, v.n);
+  double* packed = reinterpret_cast<double*>(sm.nexth);  // free once the mean line is known
+  constexpr int kPackMax = kSmemValid / 2;
+  int packed_n;
+  {
+    __shared__ int wsum[kLT / 32];
+    const int per = (end + kLT - 1) / kLT;
+    const int k0 = min(end, t * per), k1 = min(end, k0 + per);
+    int cnt = 0;
+    for (int k = k0; k < k1; k++) cnt += v.d[k] == v.d[k] ? 1 : 0;
+    int incl = cnt;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int o = __shfl_up_sync(0xffffffffu, incl, off);
+      if ((t & 31) >= off) incl += o;
+    }
+    if ((t & 31) == 31) wsum[t >> 5] = incl;
+    __syncthreads();
+    int pre = incl - cnt;
+    packed_n = 0;
+    for (int w2 = 0; w2 < kLT / 32; w2++) {
+      if (w2 < (t >> 5)) pre += wsum[w2];
+      packed_n += wsum[w2];
+    }
+    if (packed_n <= kPackMax)
+      for (int k = k0; k < k1; k++) {
+        const double x = v.d[k];
+        if (x == x) packed[pre++] = x;
+      }
+    __syncthreads();
+  }
   if (t == 0) {
-    const int end = min(sm.imin, v.n);
     double hoff = 0.0;
     int hcnt = 0;
+    if (packed_n <= kPackMax) {
 #pragma unroll 8
-    for (int k = 0; k < end; k++) {
-      const double x = v.d[k];
-      if (x == x) {
-        hoff += x;
-        hcnt++;
+      for (int k = 0; k < packed_n; k++) hoff += packed[k];
+      hcnt = packed_n;
+    } else {
+      for (int k = 0; k < end; k++) {
+        const double x = v.d[k];
+        if (x == x) {
+          hoff += x;
+          hcnt++;
+        }
       }
     }
     double l = loc;
@@ -1013,7 +1078,9 @@ __device__ VList field_vlist(const LineLocArgs& a, int f) {
 
 // Grid (num_fields): the stateless part of one field's line location, and
 // the speculative anchor + grid when the field's pattern fixes its order.
-__global__ void __launch_bounds__(kLT) prepare_kernel(LineLocArgs a) {
+template <class Src>
+__global__ void __launch_bounds__(kLT, 1) prepare_kernel(const __grid_constant__ Src src) {
+  const LineLocArgs& a = src.get();
   chain_wait();
   extern __shared__ double smem_d[];
   FieldSmem& sm = *reinterpret_cast<FieldSmem*>(smem_d);
@@ -1117,7 +1184,9 @@ __global__ void __launch_bounds__(kLT) prepare_kernel(LineLocArgs a) {
 // carried hsync difference, a few FP64 divisions, is formed only when a fit
 // or the next chunk reads it.
 constexpr int kPrepBatch = 64;
-__global__ void __launch_bounds__(kLT) finish_kernel(LineLocArgs a) {
+template <class Src>
+__global__ void __launch_bounds__(kLT, 1) finish_kernel(const __grid_constant__ Src src) {
+  const LineLocArgs& a = src.get();
   chain_wait();
   extern __shared__ double smem_d[];
   FieldSmem& sm = *reinterpret_cast<FieldSmem*>(smem_d);
@@ -1282,7 +1351,9 @@ __global__ void __launch_bounds__(kLT) finish_kernel(LineLocArgs a) {
 // blanking state machine for the reference pulse and the parity, the mean
 // line from the longest hsync run, and the nominal grid snapped to the
 // nearest hsync marker.  No carried state.
-__global__ void __launch_bounds__(kLT) single_pass_kernel(LineLocArgs a) {
+template <class Src>
+__global__ void __launch_bounds__(kLT) single_pass_kernel(const __grid_constant__ Src src) {
+  const LineLocArgs& a = src.get();
   chain_wait();
   extern __shared__ double smem_d[];
   FieldSmem& sm = *reinterpret_cast<FieldSmem*>(smem_d);
@@ -1546,33 +1617,65 @@ __global__ void __launch_bounds__(kLT) single_pass_kernel(LineLocArgs a) {
 
 size_t lineloc_smem_bytes() { return sizeof(FieldSmem); }
 
-cudaError_t launch_field_windows(const LineLocArgs& a, cudaStream_t st) {
+namespace {
+template <class S>
+cudaError_t windows_launch(const S& src, int portions, cudaStream_t st) {
   const size_t smem = fieldwin_smem_bytes();
-  const cudaError_t e = cudaFuncSetAttribute(fieldwin_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const cudaError_t e =
+      cudaFuncSetAttribute(fieldwin_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  return launch_chained(fieldwin_kernel, dim3(1), dim3(kWinThreads), smem, st, a);
+  return launch_chained(fieldwin_kernel<S>, dim3(1, 1, portions), dim3(kWinThreads), smem, st, src);
+}
+
+template <class S>
+cudaError_t pulses_launch(const S& src, int portions, int max_fields, cudaStream_t st) {
+  if (max_fields <= 0) return cudaSuccess;
+  return launch_chained(pulses_kernel<S>, dim3(max_fields, 1, portions), dim3(kLT), 0, st, src);
+}
+
+template <class S>
+cudaError_t lines_launch(const S& src, bool single_pass, int portions, int max_fields, cudaStream_t st) {
+  if (max_fields <= 0) return cudaSuccess;
+  const size_t smem = sizeof(FieldSmem);
+  cudaError_t e;
+  if (single_pass) {
+    e = cudaFuncSetAttribute(single_pass_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return launch_chained(single_pass_kernel<S>, dim3(max_fields, 1, portions), dim3(kLT), smem, st, src);
+  }
+  e = cudaFuncSetAttribute(prepare_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(finish_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = launch_chained(prepare_kernel<S>, dim3(max_fields, 1, portions), dim3(kLT), smem, st, src);
+  if (e != cudaSuccess) return e;
+  return launch_chained(finish_kernel<S>, dim3(1, 1, portions), dim3(kLT), smem, st, src);
+}
+}  // namespace
+
+cudaError_t launch_field_windows(const LineLocArgs& a, cudaStream_t st) {
+  return windows_launch(ArgsOne<LineLocArgs>{a}, 1, st);
 }
 
 cudaError_t launch_field_pulses(const LineLocArgs& a, cudaStream_t st) {
-  if (a.num_fields <= 0) return cudaSuccess;
-  return launch_chained(pulses_kernel, dim3(a.num_fields), dim3(kLT), 0, st, a);
+  return pulses_launch(ArgsOne<LineLocArgs>{a}, 1, a.num_fields, st);
 }
 
 cudaError_t launch_line_locations(const LineLocArgs& a, cudaStream_t st) {
-  if (a.num_fields <= 0) return cudaSuccess;
-  const size_t smem = sizeof(FieldSmem);
-  cudaError_t e;
-  if (a.single_pass) {
-    e = cudaFuncSetAttribute(single_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    return launch_chained(single_pass_kernel, dim3(a.num_fields), dim3(kLT), smem, st, a);
-  }
-  e = cudaFuncSetAttribute(prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  e = launch_chained(prepare_kernel, dim3(a.num_fields), dim3(kLT), smem, st, a);
-  if (e != cudaSuccess) return e;
-  return launch_chained(finish_kernel, dim3(1), dim3(kLT), smem, st, a);
+  return lines_launch(ArgsOne<LineLocArgs>{a}, a.single_pass != 0, 1, a.num_fields, st);
+}
+
+cudaError_t launch_field_windows_many(const ArgsMany<LineLocArgs>& p, int portions, cudaStream_t st) {
+  return portions > 0 ? windows_launch(p, portions, st) : cudaSuccess;
+}
+
+cudaError_t launch_field_pulses_many(const ArgsMany<LineLocArgs>& p, int portions, int max_fields, cudaStream_t st) {
+  return portions > 0 ? pulses_launch(p, portions, max_fields, st) : cudaSuccess;
+}
+
+cudaError_t launch_line_locations_many(const ArgsMany<LineLocArgs>& p, int portions, int max_fields,
+                                       cudaStream_t st) {
+  return portions > 0 ? lines_launch(p, p.a[0].single_pass != 0, portions, max_fields, st) : cudaSuccess;
 }
 
 }  // namespace cuvhs

@@ -126,7 +126,9 @@ __device__ double window_median(const float* __restrict__ s, int start, int coun
 
 // One warp per line location (lines from the first active line to the end of
 // the frame table).
-__global__ void __launch_bounds__(32 * kHsyncWarps) hsync_kernel(LineArgs a) {
+template <class Src>
+__global__ void __launch_bounds__(32 * kHsyncWarps) hsync_kernel(const __grid_constant__ Src src) {
+  const LineArgs& a = src.get();
   chain_wait();
   const int lane = threadIdx.x & 31;
   const int idx = blockIdx.x * kHsyncWarps + (threadIdx.x >> 5);
@@ -195,12 +197,15 @@ __device__ __forceinline__ uint16_t luma_pixel(const LineArgs& a, float p0, floa
   return ok ? (uint16_t)(v + 0.5f) : a.oob_value;
 }
 
-__global__ void __launch_bounds__(kLumaThreads) luma_kernel(LineArgs a) {
-  chain_wait();
-  __shared__ __align__(16) float win[kLumaWindow];
+template <class Src>
+__global__ void __launch_bounds__(kLumaThreads) luma_kernel(const __grid_constant__ Src src) {
+  const LineArgs& a = src.get();
   const int W = a.out_w, H = a.out_h;
   const int grow = blockIdx.x;  // field * H + row
   const int field = grow / H, row = grow % H;
+  if (field >= a.fields) return;  // whole CTA: a batched capture with fewer fields
+  chain_wait();
+  __shared__ __align__(16) float win[kLumaWindow];
   uint16_t* out = a.luma + (size_t)grow * W;
   if (row + 1 >= a.lines_per_frame) {
     for (int col = threadIdx.x; col < W; col += kLumaThreads) out[col] = a.oob_value;
@@ -263,13 +268,28 @@ __global__ void __launch_bounds__(kLumaThreads) luma_kernel(LineArgs a) {
 void launch_hsync_refine(const LineArgs& a, cudaStream_t st) {
   const int n = a.fields * a.lines_per_frame;
   if (n <= 0) return;
-  launch_chained(hsync_kernel, dim3((n + kHsyncWarps - 1) / kHsyncWarps), dim3(32 * kHsyncWarps), 0, st, a);
+  using S = ArgsOne<LineArgs>;
+  launch_chained(hsync_kernel<S>, dim3((n + kHsyncWarps - 1) / kHsyncWarps), dim3(32 * kHsyncWarps), 0, st, S{a});
 }
 
 void launch_luma(const LineArgs& a, cudaStream_t st) {
   const int rows = a.fields * a.out_h;
   if (rows <= 0) return;
-  launch_chained(luma_kernel, dim3(rows), dim3(kLumaThreads), 0, st, a);
+  using S = ArgsOne<LineArgs>;
+  launch_chained(luma_kernel<S>, dim3(rows), dim3(kLumaThreads), 0, st, S{a});
+}
+
+void launch_hsync_refine_many(const ArgsMany<LineArgs>& p, int portions, int max_fields, cudaStream_t st) {
+  const int n = max_fields * p.a[0].lines_per_frame;
+  if (n <= 0 || portions <= 0) return;
+  launch_chained(hsync_kernel<ArgsMany<LineArgs>>, dim3((n + kHsyncWarps - 1) / kHsyncWarps, 1, portions),
+                 dim3(32 * kHsyncWarps), 0, st, p);
+}
+
+void launch_luma_many(const ArgsMany<LineArgs>& p, int portions, int max_fields, cudaStream_t st) {
+  const int rows = max_fields * p.a[0].out_h;
+  if (rows <= 0 || portions <= 0) return;
+  launch_chained(luma_kernel<ArgsMany<LineArgs>>, dim3(rows, 1, portions), dim3(kLumaThreads), 0, st, p);
 }
 
 }  // namespace cuvhs

@@ -46,7 +46,9 @@ void upload(T* d, const std::vector<T>& h, cudaStream_t st) {
   if (!h.empty()) cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st);
 }
 
-constexpr int kPhaseCycle[8] = {3, 2, 1, 4, 3, 2, 1, 4};
+}  // namespace
+
+const int kPhaseCycle[8] = {3, 2, 1, 4, 3, 2, 1, 4};
 
 // NTSC field phase table keyed by (first field, burst quadrant), no phase
 // delta known (src/pipeline/chroma_decode.cu:337-377: the decoder always looks
@@ -57,8 +59,6 @@ int phase_id_for(int is_first, int quadrant) {
   if (quadrant < 0 || quadrant > 3) return 1;
   return is_first ? first_q[quadrant] : second_q[quadrant];
 }
-
-}  // namespace
 
 const char* const kStageNames[kNumStages] = {"k1a_demod",      "k1b_video_sync", "sync_edges",
                                              "hsync_refine",   "luma_resample",  "chroma_prefilter",
@@ -125,6 +125,7 @@ void Context::release() {
   allocations.clear();
   for (void* p : host_allocations) cudaFreeHost(p);
   host_allocations.clear();
+  hp_round_burst = nullptr;
   if (ev_host) cudaEventDestroy(ev_host);
   ev_host = nullptr;
   for (cudaEvent_t& e : ev_piece) {
@@ -143,10 +144,12 @@ void Context::release() {
   hstream = nullptr;
   if (pstream) cudaStreamDestroy(pstream);
   pstream = nullptr;
-  for (cudaEvent_t* e : {&ev_ll, &ev_win, &ev_winhost, &ev_k1b, &ev_pre}) {
+  for (cudaEvent_t* e : {&ev_ll, &ev_win, &ev_winhost, &ev_k1b, &ev_pre, &ev_guard}) {
     if (*e) cudaEventDestroy(*e);
     *e = nullptr;
   }
+  if (gstream) cudaStreamDestroy(gstream);
+  gstream = nullptr;
   if (lstream) cudaStreamDestroy(lstream);
   lstream = nullptr;
   pf = Prefetch();
@@ -186,10 +189,12 @@ bool Context::alloc_buffers() {
   d_sync = A((float*)nullptr, S);
   d_env_part = A((double*)nullptr, (size_t)batch * env_blocks);
   edge_cap = (int)std::min<size_t>(S / 4 + 4096, (size_t)INT_MAX / 2);
-  d_fall = A((unsigned*)nullptr, edge_cap);
-  d_rise = A((unsigned*)nullptr, edge_cap);
-  d_counts = A((int*)nullptr, 4);
-  d_edge_blk = A((int2*)nullptr, (size_t)edge_blocks((long long)batch * spp) + 1);
+  const size_t edge_alloc = std::max((size_t)edge_cap, (size_t)batch * kEdgesPerSlot(spp));
+  d_fall = A((unsigned*)nullptr, edge_alloc);
+  d_rise = A((unsigned*)nullptr, edge_alloc);
+  d_counts = A((int*)nullptr, 4 * kMaxPortions);
+  d_edge_blk = A((int2*)nullptr, std::max((size_t)edge_blocks((long long)batch * spp) + 1,
+                                          (size_t)batch * kEdgeBlocksPerSlot(spp)));
   d_edge_mask = A((unsigned*)nullptr, edge_mask_words((long long)batch * spp));
   d_ll = A((double*)nullptr, (size_t)batch * fmt.lines_per_frame);
   const size_t F = (size_t)fmt.output_line_len * fmt.output_field_lines;
@@ -217,9 +222,9 @@ bool Context::alloc_buffers() {
   d_twb_inv = A((float2*)nullptr, des.tw_b.size());
   d_twc_inv = A((float2*)nullptr, des.tw_c.size());
   d_twl_inv = A((float2*)nullptr, des.tw_line.size());
-  d_win = A((WindowInfo*)nullptr, 1);
+  d_win = A((WindowInfo*)nullptr, kMaxPortions);
   d_offs = A((long long*)nullptr, (size_t)batch + 1);
-  d_cand = A((int*)nullptr, edge_cap);
+  d_cand = A((int*)nullptr, edge_alloc);
   d_ps = A((int*)nullptr, (size_t)batch * kMaxPulses);
   d_pl = A((int*)nullptr, (size_t)batch * kMaxPulses);
   d_pn = A((int*)nullptr, batch);
@@ -229,7 +234,11 @@ bool Context::alloc_buffers() {
   d_vd = A((double*)nullptr, (size_t)batch * kMaxValid);
   d_vn = A((int*)nullptr, batch);
   d_prep = A((FieldPrep*)nullptr, batch);
-  d_lls = A((LineLocState*)nullptr, 1);
+  d_lls = A((LineLocState*)nullptr, kMaxPortions);
+  d_lls_save = A((LineLocState*)nullptr, kMaxPortions);
+  d_pulse_bits = A((unsigned*)nullptr, std::max(pulse_bit_words((long long)batch * spp),
+                                                (size_t)batch * kBitWordsPerSlot(spp)));
+  d_guard_flips = A((int*)nullptr, kMaxPortions);
   d_is_first = A((int*)nullptr, batch);
   d_dbg_vs = A((int*)nullptr, (size_t)batch * kMaxPulses);
   d_dbg_vl = A((int*)nullptr, (size_t)batch * kMaxPulses);
@@ -241,9 +250,10 @@ bool Context::alloc_buffers() {
   d_guard_g = A((double2*)nullptr, (size_t)Design::kGuardN);
   d_guard_tw = A((double2*)nullptr, (size_t)Design::kGuardN);
   d_hs64 = A((double*)nullptr, des.hs64.size());
-  d_guard_list = A((unsigned*)nullptr, kGuardCap);
-  d_guard_count = A((int*)nullptr, 1);
-  d_guard_vals = A((double*)nullptr, kGuardCap);
+  const size_t guard_alloc = std::max((size_t)kGuardCap, (size_t)batch * kGuardPerSlot);
+  d_guard_list = A((unsigned*)nullptr, guard_alloc);
+  d_guard_count = A((int*)nullptr, kMaxPortions);
+  d_guard_vals = A((double*)nullptr, guard_alloc);
   if (ok && !guard_supported(des.ga64_half, des.hs64_half)) {
     err = "sync guard support too long";
     ok = false;
@@ -264,10 +274,11 @@ bool Context::alloc_buffers() {
     return static_cast<T*>(p);
   };
   hp_counts = H((int*)nullptr, 4);
-  hp_win = H((WindowInfo*)nullptr, 1);
+  hp_win = H((WindowInfo*)nullptr, kMaxPortions);
+  hp_lls = H((LineLocState*)nullptr, kMaxPortions);
   hp_offs = H((long long*)nullptr, (size_t)batch + 1);
   hp_is_first = H((int*)nullptr, batch);
-  hp_guard = H((int*)nullptr, 1);
+  hp_guard = H((int*)nullptr, 2 * kMaxPortions);
   hp_track = H((int*)nullptr, batch);
   hp_trial = H((int*)nullptr, 2);
   hp_burst = H((float*)nullptr, (size_t)2 * fmt.output_field_lines * fmt.burst_len);
@@ -297,6 +308,7 @@ void Context::free_buffers() {
   allocations.clear();
   for (void* p : host_allocations) cudaFreeHost(p);
   host_allocations.clear();
+  hp_round_burst = nullptr;
   dev_used = 0;
   cudaGetLastError();
 }
@@ -376,7 +388,8 @@ bool Context::init(const cuvhs_config& c) {
       cudaStreamCreateWithFlags(&xstream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&hstream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithPriority(&lstream, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&pstream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&pstream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&gstream, cudaStreamNonBlocking, prio_high) != cudaSuccess) {
     err = "cudaStreamCreate failed";
     status = CUVHS_ERR_CUDA;
     return false;
@@ -406,7 +419,8 @@ bool Context::init(const cuvhs_config& c) {
                cudaEventCreateWithFlags(&ev_win, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_winhost, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_k1b, cudaEventDisableTiming) == cudaSuccess &&
-               cudaEventCreateWithFlags(&ev_pre, cudaEventDisableTiming) == cudaSuccess;
+               cudaEventCreateWithFlags(&ev_pre, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev_guard, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t* e : {&ev_prefetch, &ev_small, &ev_chroma, &ev_out_done[0], &ev_out_done[1]})
     ev_ok = ev_ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t& e : ev_piece) ev_ok = ev_ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
@@ -506,7 +520,7 @@ void Context::reset_state() {
 
 // Host burst-cancellation metric over one field's burst windows (lines 16..245
 // in pairs), as the track detector measures it (chroma_decode.cu:383-411).
-static double host_burst_metric(const float* b, int H, int bl) {
+double host_burst_metric(const float* b, int H, int bl) {
   const int skip = 16;
   double total = 0.0;
   int count = 0;
@@ -523,7 +537,7 @@ static double host_burst_metric(const float* b, int H, int bl) {
 
 // Burst phase in degrees by I/Q product detection over lines 16..246
 // (chroma_decode.cu:415-450).
-static double host_burst_phase(const float* b, int H, const Format& fmt) {
+double host_burst_phase(const float* b, int H, const Format& fmt) {
   const int skip = 16;
   const double PI = 3.14159265358979323846;
   double It = 0.0, Qt = 0.0;
@@ -578,6 +592,7 @@ DemodArgs Context::demod_args(int T) const {
   da.env_blocks = env_blocks;
   da.video = d_video;
   da.sync = d_sync;
+  da.pulse_bits = d_pulse_bits;
   da.thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
   da.guard_hz = cfg.guard_band_hz > 0.0 ? (float)cfg.guard_band_hz : kGuardHz;
   da.guard_list = d_guard_list;
@@ -609,6 +624,7 @@ GuardArgs Context::guard_args(const DemodArgs& da) const {
   g.count = d_guard_count;
   g.cap = kGuardCap;
   g.values = d_guard_vals;
+  g.flips = d_guard_flips;
   if (debug) g.dbg_clk = d_dbg_clk_guard;
   return g;
 }
@@ -931,6 +947,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
       cudaStreamSynchronize(c->hstream);
       cudaStreamSynchronize(c->pstream);  // after an error, nothing of the chunk is left running
       cudaStreamSynchronize(c->lstream);
+      cudaStreamSynchronize(c->gstream);
       c->pf.valid = false;
     }
   } drain{this};
@@ -962,6 +979,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   // ---- K1: FM demod over T tiles
   DemodArgs da = demod_args(T);
   cudaMemsetAsync(d_guard_count, 0, sizeof(int), stream);  // K1b lists near-threshold sync samples
+  cudaMemsetAsync(d_pulse_bits, 0, pulse_bit_words((long long)T * spp) * sizeof(unsigned), stream);
   // ---- input: the chunk window (bps bytes per sample); positions past the
   // samples read count as 0 in every kernel, the reference's zero fill.  Host
   // input arrives in pieces on the copy stream; K1a of tiles [fa, fb) reads
@@ -1028,16 +1046,85 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   }
   // ---- the colour-under pre-band-pass needs only the raw samples, and its
   // output takes the demod buffer's place once K1b has read it: on its own
-  // stream it runs beside the guard, the edges, the field windows and the
-  // line locations (short, latency-bound kernels).  It covers all T
-  // demodulated slots; the detected fields are a prefix.
+  // stream it runs beside the line locations (short, latency-bound kernels),
+  // launched below.  It covers all T demodulated slots; the detected fields
+  // are a prefix.
   ChromaArgs ca = chroma_args(da.raw, (int)n_read, da.dc, T);
   if (debug) {
     dbg_demod.resize(std::min<size_t>((size_t)T * spp, (size_t)debug_tiles * spp));
     cudaMemcpyAsync(dbg_demod.data(), d_dem, dbg_demod.size() * sizeof(float), cudaMemcpyDeviceToHost, stream);
   }
   cudaEventRecord(ev_k1b, stream);
-  cudaStreamWaitEvent(pstream, ev_k1b, 0);
+  if (!check_cuda("demod")) return false;
+  // ---- sync edges over the demodulated range, the field windows clustered
+  // from their VSYNC runs, and the line locations: all on the device.  The
+  // host reads back only the field count, offsets and next chunk start (a
+  // few bytes) while the chroma pre-band-pass and the line locations run.
+  // They first run on K1b's FP32 in-pulse bits, beside the guard; if the
+  // guard flips a decision they run again on the corrected sync.
+  const long long total_chunk = (long long)T * spp;
+  LineLocArgs lla = lineloc_args(T, num_fields, (long long)raw_offset);
+  // the whole chain on the high-priority line stream: its kernels are short
+  // and latency bound, and the pre-band-pass (low priority) fills the SMs
+  // they leave
+  cudaStreamWaitEvent(lstream, ev_k1b, 0);
+  if (debug) cudaMemsetAsync(d_dbg_clk_ll, 0, (size_t)batch * kPhaseSlots * sizeof(long long), lstream);
+  auto windows_and_lines = [&](bool from_bits) {
+    cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), lstream);
+    {
+      cudaEvent_t ev_;
+      begin_stage_on(kStageEdges, ev_, lstream);
+      if (from_bits) {
+        launch_edges_bits(d_pulse_bits, total_chunk, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, lstream);
+      } else {
+        const float thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
+        launch_edges(d_sync, total_chunk, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, d_edge_mask,
+                     lstream);
+      }
+      end_stage_on(kStageEdges, ev_, lstream, 3);
+    }
+    cudaEventRecord(ev_edges, lstream);
+    {
+      cudaEvent_t ev_;
+      begin_stage_on(kStageWindows, ev_, lstream);
+      launch_field_windows(lla, lstream);
+      end_stage_on(kStageWindows, ev_, lstream);
+    }
+    cudaEventRecord(ev_win, lstream);
+    // the window record and offsets come back on the copy stream
+    cudaStreamWaitEvent(xstream, ev_win, 0);
+    cudaMemcpyAsync(hp_win, d_win, sizeof(WindowInfo), cudaMemcpyDeviceToHost, xstream);
+    cudaMemcpyAsync(hp_offs, d_offs, (size_t)num_fields * sizeof(long long), cudaMemcpyDeviceToHost, xstream);
+    cudaEventRecord(ev_winhost, xstream);
+    // the carried line-location state is kept for a second run
+    cudaMemcpyAsync(from_bits ? d_lls_save : d_lls, from_bits ? d_lls : d_lls_save, sizeof(LineLocState),
+                    cudaMemcpyDeviceToDevice, lstream);
+    {
+      cudaEvent_t ev_;
+      begin_stage_on(kStageLines, ev_, lstream);
+      launch_field_pulses(lla, lstream);
+      launch_line_locations(lla, lstream);
+      end_stage_on(kStageLines, ev_, lstream, single_pass ? 2 : 3);
+    }
+    cudaEventRecord(ev_ll, lstream);
+  };
+  windows_and_lines(true);
+  // The FP64 guard follows the edges (it needs only the raw capture and K1b's
+  // list, and leaves the edge kernels the whole GPU); the colour-under
+  // pre-band-pass, needed only by the chroma lines, follows the field windows
+  // on the low-priority stream and fills the SMs the line locations leave.
+  {
+    cudaStreamWaitEvent(gstream, ev_edges, 0);
+    cudaMemsetAsync(d_guard_flips, 0, sizeof(int), gstream);
+    cudaEvent_t ev_;
+    begin_stage_on(kStageGuard, ev_, gstream);
+    launch_sync_guard(guard_args(da), gstream);
+    end_stage_on(kStageGuard, ev_, gstream);
+    cudaMemcpyAsync(hp_guard, d_guard_count, sizeof(int), cudaMemcpyDeviceToHost, gstream);
+    cudaMemcpyAsync(hp_guard + 1, d_guard_flips, sizeof(int), cudaMemcpyDeviceToHost, gstream);
+    cudaEventRecord(ev_guard, gstream);
+  }
+  cudaStreamWaitEvent(pstream, ev_win, 0);
   {
     cudaEvent_t ev_;
     begin_stage_on(kStageChromaPre, ev_, pstream);
@@ -1045,63 +1132,28 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     end_stage_on(kStageChromaPre, ev_, pstream);
   }
   cudaEventRecord(ev_pre, pstream);
-  {
-    // FP64 threshold decisions for the listed sync samples
-    cudaEvent_t ev_;
-    begin_stage(kStageGuard, ev_);
-    launch_sync_guard(guard_args(da), stream);
-    end_stage(kStageGuard, ev_);
-  }
-  if (!check_cuda("demod")) return false;
-  // ---- sync edges over the demodulated range, the field windows clustered
-  // from their VSYNC runs, and the line locations: all on the device.  The
-  // host reads back only the field count, offsets and next chunk start (a
-  // few bytes) while the chroma pre-band-pass and the line locations run.
-  const long long total_chunk = (long long)T * spp;
-  cudaMemsetAsync(d_counts, 0, 4 * sizeof(int), stream);
-  {
-    cudaEvent_t ev_;
-    begin_stage(kStageEdges, ev_);
-    const float thr_rel = (float)(fmt.pulse_threshold_hz - fmt.ire0);
-    launch_edges(d_sync, total_chunk, thr_rel, d_fall, d_rise, d_counts, edge_cap, d_edge_blk, d_edge_mask, stream);
-    end_stage(kStageEdges, ev_, 3);
-  }
-  LineLocArgs lla = lineloc_args(T, num_fields, (long long)raw_offset);
-  if (debug) cudaMemsetAsync(d_dbg_clk_ll, 0, (size_t)batch * kPhaseSlots * sizeof(long long), stream);
-  {
-    cudaEvent_t ev_;
-    begin_stage(kStageWindows, ev_);
-    launch_field_windows(lla, stream);
-    end_stage(kStageWindows, ev_);
-  }
-  cudaEventRecord(ev_win, stream);
-  // the window record and offsets come back on the copy stream
-  cudaStreamWaitEvent(xstream, ev_win, 0);
-  cudaMemcpyAsync(hp_win, d_win, sizeof(WindowInfo), cudaMemcpyDeviceToHost, xstream);
-  cudaMemcpyAsync(hp_offs, d_offs, (size_t)num_fields * sizeof(long long), cudaMemcpyDeviceToHost, xstream);
-  cudaMemcpyAsync(hp_guard, d_guard_count, sizeof(int), cudaMemcpyDeviceToHost, xstream);
-  cudaEventRecord(ev_winhost, xstream);
-  // line locations on the line stream, beside the pre-band-pass
-  cudaStreamWaitEvent(lstream, ev_win, 0);
-  {
-    cudaEvent_t ev_;
-    begin_stage_on(kStageLines, ev_, lstream);
-    launch_field_pulses(lla, lstream);
-    launch_line_locations(lla, lstream);
-    end_stage_on(kStageLines, ev_, lstream, single_pass ? 2 : 3);
-  }
-  cudaEventRecord(ev_ll, lstream);
+  if (!check_cuda("guard and pre-band-pass")) return false;
   const int LPF = fmt.lines_per_frame;
   const int H = fmt.output_field_lines;
   if (!check_cuda("chroma prefilter")) return false;
   double t_host = host_clock();
-  {
-    const cudaError_t e = cudaEventSynchronize(ev_winhost);
-    if (e != cudaSuccess) {
-      err = std::string("field windows: ") + cudaGetErrorString(e);
+  auto wait_event = [&](cudaEvent_t e, const char* what) {
+    const cudaError_t r = cudaEventSynchronize(e);
+    if (r != cudaSuccess) {
+      err = std::string(what) + ": " + cudaGetErrorString(r);
       status = CUVHS_ERR_CUDA;
       return false;
     }
+    return true;
+  };
+  if (!wait_event(ev_winhost, "field windows") || !wait_event(ev_guard, "sync guard")) return false;
+  if (!guard_ok(hp_guard[0])) return false;
+  if (hp_guard[1] > 0) {
+    // a threshold decision flipped: edges, windows and line locations again
+    // (after the speculative ones on the same stream) on the corrected sync
+    cudaStreamWaitEvent(lstream, ev_guard, 0);
+    windows_and_lines(false);
+    if (!wait_event(ev_winhost, "field windows")) return false;
   }
   host_phase(kHostWindowsWait, t_host);
   if (hp_win->err) {
@@ -1109,7 +1161,6 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     status = CUVHS_ERR_CAPACITY;
     return false;
   }
-  if (!guard_ok(*hp_guard)) return false;
   const int P = hp_win->fields;
   res.next_raw_offset = raw_offset + (uint64_t)hp_win->next_rel;
   // ---- the next chunk of a host capture starts at next_raw_offset: copy its
@@ -1136,7 +1187,8 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   if (debug) {
     // the chunk's intermediates as the reference keeps them: VSYNC
     // candidates, raw and validated pulses, coarse line locations
-    if (cudaStreamSynchronize(lstream) != cudaSuccess) return check_cuda("line locations");
+    if (cudaStreamSynchronize(lstream) != cudaSuccess || cudaStreamSynchronize(gstream) != cudaSuccess)
+      return check_cuda("line locations");
     const int nc = std::min(hp_win->ncand, edge_cap);
     dbg_vsync.resize(nc);
     if (nc) cudaMemcpy(dbg_vsync.data(), d_cand, nc * sizeof(int), cudaMemcpyDeviceToHost);
@@ -1168,7 +1220,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     dbg_ll_coarse.resize((size_t)P * LPF);
     if (P) cudaMemcpy(dbg_ll_coarse.data(), d_ll, dbg_ll_coarse.size() * sizeof(double), cudaMemcpyDeviceToHost);
     dbg_meta = {T, P, spp};
-    const int ng = std::min(*hp_guard, kGuardCap);
+    const int ng = std::min(hp_guard[0], kGuardCap);
     std::vector<unsigned> pos(ng);
     dbg_guard_vals.resize(ng);
     if (ng) {
@@ -1190,6 +1242,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     return true;
   }
   cudaStreamWaitEvent(stream, ev_ll, 0);
+  cudaStreamWaitEvent(stream, ev_guard, 0);
   // ---- K4 hsync refinement, K5 luma
   LineArgs la = line_args(P);
   {

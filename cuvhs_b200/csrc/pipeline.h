@@ -13,11 +13,48 @@
 
 namespace cuvhs {
 
+// Per-slot regions of the chunk buffers a batched round gives each capture:
+// the capture whose chunk starts at slot s0 uses [s0 * per_slot, ...).
+inline size_t kBitWordsPerSlot(int spp) { return (size_t)(spp + 31) / 32 + 1; }
+inline size_t kEdgesPerSlot(int spp) { return (size_t)spp / 4 + 64; }
+inline size_t kEdgeBlocksPerSlot(int spp) { return (size_t)(spp + 8191) / 8192 + 2; }
+constexpr int kGuardPerSlot = 2048;  // near-threshold sync samples one field slot of a batched round can list
+
+extern const int kPhaseCycle[8];
+int phase_id_for(int is_first, int quadrant);
+double host_burst_metric(const float* b, int H, int bl);
+double host_burst_phase(const float* b, int H, const Format& fmt);
+
 struct ChunkResult {
   int fields = 0;
   uint64_t next_raw_offset = 0;
   bool outputs_copied = false;  // luma/chroma already in the caller's host buffers
   std::vector<cuvhs_field_info> field_info;
+};
+
+// What one capture carries from chunk to chunk when it is decoded in batched
+// rounds (a single-capture context keeps the same in its own members).
+struct PortionState {
+  LineLocState lls;
+  bool chroma_valid = false;
+  int chroma_track = 0;
+  double chroma_threshold = 0.0;
+  int chroma_cycle_start = 0;
+  bool last_parity = true;
+};
+// One capture's chunk in a batched round.
+struct Portion {
+  const uint8_t* src = nullptr;  // host samples from raw_offset (u8)
+  size_t n_avail = 0;
+  uint64_t raw_offset = 0;
+  int num_fields = 0;  // the chunk size
+  int slot0 = 0;       // first field slot (the round's portions fill consecutive slots)
+  PortionState* st = nullptr;
+  uint16_t* dst_luma = nullptr;  // host planes for the chunk's fields, or null
+  uint16_t* dst_chroma = nullptr;
+  // filled in
+  ChunkResult res;
+  int T = 0, n_read = 0;
 };
 
 enum Stage {
@@ -80,6 +117,13 @@ struct Context {
   // sync and line-location kernels; the chroma lines wait on ev_pre.
   cudaStream_t pstream = nullptr;
   cudaEvent_t ev_k1b = nullptr, ev_pre = nullptr;
+  // FP64 guard: its own stream after K1b, beside the edges and line
+  // locations, which run on K1b's FP32 in-pulse bits.  ev_guard marks the
+  // guard and its listed / flipped counts in pinned memory; when it flipped
+  // a threshold decision, the edges, windows and line locations run again on
+  // the corrected sync (rare), from the line-location state saved before.
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t ev_guard = nullptr;
   uint8_t* d_raw_set[2] = {};
   uint16_t* d_luma_set[2] = {};
   uint16_t* d_chroma_set[2] = {};
@@ -132,7 +176,11 @@ struct Context {
   unsigned* d_guard_list = nullptr;
   int* d_guard_count = nullptr;
   double* d_guard_vals = nullptr;
-  int* hp_guard = nullptr;  // pinned: the chunk's listed count
+  int* hp_guard = nullptr;  // pinned: the chunk's listed count, then its flipped count (per capture in a round)
+  LineLocState* hp_lls = nullptr;  // pinned: line-location states of a round's captures
+  unsigned* d_pulse_bits = nullptr;
+  int* d_guard_flips = nullptr;
+  LineLocState* d_lls_save = nullptr;
   // Guard launch over the current chunk's sync (T tiles), after the last K1b;
   // every later threshold decision reads the corrected samples.
   GuardArgs guard_args(const DemodArgs& da) const;
@@ -222,6 +270,11 @@ struct Context {
                     const uint8_t* cap_base = nullptr, size_t cap_n = 0, bool defer = false);
   // Waits for deferred plane copies and input prefetches; returns false on a CUDA error.
   bool drain_copies();
+  // The next chunk of up to kMaxPortions captures in one pass of batched
+  // launches (round.cpp); res of each portion as decode_chunk's, its dropout
+  // lists at hp_do_* + slot0 * kMaxDropouts.
+  bool decode_round(std::vector<Portion>& ps);
+  float* hp_round_burst = nullptr;  // pinned: trial-pass burst windows of a round's captures (on first use)
   // K1 arguments over T tiles of the current raw buffer into the context's buffers.
   DemodArgs demod_args(int T) const;
   // Kernel arguments on the context's buffers: chroma over T tiles of `raw`,

@@ -339,22 +339,28 @@ cuvhs_status cuvhs_dropouts_noalloc(const float* d_envelope, const double* d_lin
                                     int32_t* d_startx, int32_t* d_endx, void* stream);
 
 /* ---------------------------------------------------------------- batches
- * Many independent captures (mixed sample rates and lengths) decoded
- * concurrently on one GPU.  `lanes` host threads each drive their own decoder
- * contexts (one per sample rate seen, created on first use and kept), so the
- * GPU overlaps the kernels and copies of several captures while their host
- * decisions run in parallel.  Every capture is decoded from a fresh state
- * exactly as cuvhs_decode_capture on a new context with a chunk of
- * max_fields fields would decode it: outputs do not depend on the lane count
- * or on the order of the items. */
+ * Many independent captures (mixed sample rates and lengths) decoded together
+ * on one GPU.  Captures of one sample rate are decoded in rounds: each round
+ * takes the next chunk of up to 64 captures, places them in consecutive field
+ * slots of one context's buffers and runs every stage as one launch over all
+ * of them (grid.z picks the capture), so a stage's launch, its host waits and
+ * the GPU's fill are shared by the whole round.  `lanes` host threads each
+ * drive rounds on their own contexts (one per sample rate), so one lane's
+ * host decisions overlap another's kernels.  The field slots per round come
+ * from an autotuner (timed rounds of a synthetic probe at each candidate
+ * size, once per sample rate and batch object) unless round_fields is given.
+ * Every capture is decoded from a fresh state exactly as cuvhs_decode_capture
+ * on a new context with a chunk of max_fields fields would decode it: outputs
+ * do not depend on the lane count, the round size or the order of the items. */
 typedef struct cuvhs_batch cuvhs_batch;
 
 typedef struct cuvhs_batch_config {
-  int device;     /* CUDA device id, -1 = the one with most memory */
-  int lanes;      /* concurrent decoders; 0 = choose (min(4, cores / 2), at least 1) */
-  int max_fields; /* chunk size of each lane's contexts; 0 = 256 (one chunk per capture
-                     of up to 256 fields, as a single-capture decode with the default
-                     chunk size) */
+  int device;       /* CUDA device id, -1 = the one with most memory */
+  int lanes;        /* concurrent round drivers; 0 = 2 */
+  int max_fields;   /* chunk size of every capture; 0 = 256 (one chunk per capture of up
+                       to 256 fields, as a single-capture decode with the default
+                       chunk size) */
+  int round_fields; /* field slots per round (at least max_fields); 0 = autotune */
 } cuvhs_batch_config;
 
 typedef struct cuvhs_batch_item {
@@ -374,6 +380,9 @@ cuvhs_status cuvhs_batch_decode(cuvhs_batch* b, cuvhs_batch_item* items, int n_i
 const char* cuvhs_batch_last_error(const cuvhs_batch* b);
 /* .tbc.json text of one decoded item (as cuvhs_json for a single capture). */
 long long cuvhs_batch_json(const cuvhs_batch_item* item, char* dst, long long cap);
+/* Field slots per round the batch uses for captures at this sample rate
+ * (after the autotuner ran for it, or round_fields); 0 before first use. */
+int cuvhs_batch_round_fields(const cuvhs_batch* b, double sample_rate_mhz);
 
 /* ------------------------------------------------------------- calibration
  * A differentiable decode model and its adjoint, for calibrating a tape's

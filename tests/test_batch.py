@@ -51,3 +51,30 @@ def test_batch_reports_per_item_errors():
         assert b"too small" in cv.lib.cuvhs_batch_last_error(b._h)
         # a capture shorter than one field decodes to nothing and is not an error
         assert items[2].status == 0 and keep[2]["out"].fields_out == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("round_fields", [16, 0])
+def test_batched_rounds_match_single_decodes_with_multichunk_captures(round_fields):
+    """Rounds of several captures (one launch per stage over all of them),
+    captures longer than one chunk (carried state between rounds), mixed
+    rates, and a round size either fixed small (many rounds, captures split
+    across rounds) or chosen by the autotuner: every capture equals its
+    single-capture decode with the same chunk size."""
+    caps = cv.make_batch_workload(count=10, min_fields=3, max_fields=20, seed=91)
+    single = []
+    for x, mhz in caps:
+        with cv.Decoder(mhz, batch_fields=8) as d:
+            single.append(d.decode_capture(x))
+    with cv.Batch(lanes=2, max_fields=8, round_fields=round_fields) as b:
+        got = b.decode(caps)
+        for mhz in {m for _, m in caps}:
+            rf = b.round_fields(mhz)
+            assert rf >= 8 and (round_fields == 0 or rf == round_fields), (mhz, rf)
+    for i, s in enumerate(single):
+        assert s.n_fields > 0
+        g = got[i]
+        assert g.n_fields == s.n_fields, i
+        assert np.array_equal(g.file_loc, s.file_loc), i
+        assert np.array_equal(g.luma, s.luma) and np.array_equal(g.chroma, s.chroma), i
+        assert g.json == s.json, i

@@ -150,6 +150,10 @@ lib.cuvhs_batch_lanes.argtypes = [_vp]
 lib.cuvhs_batch_lanes.restype = ctypes.c_int
 lib.cuvhs_batch_round_fields.argtypes = [_vp, ctypes.c_double]
 lib.cuvhs_batch_round_fields.restype = ctypes.c_int
+lib.cuvhs_batch_set_timing.argtypes = [_vp, ctypes.c_int]
+lib.cuvhs_batch_stage_times.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
+                                        ctypes.c_int]
+lib.cuvhs_batch_stage_times.restype = ctypes.c_int
 lib.cuvhs_batch_decode.argtypes = [_vp, ctypes.POINTER(BatchItem), ctypes.c_int]
 lib.cuvhs_batch_decode.restype = ctypes.c_int
 lib.cuvhs_batch_last_error.argtypes = [_vp]
@@ -230,6 +234,7 @@ EXPORTED = [
     "cuvhs_stage_count", "cuvhs_stage_name", "cuvhs_stage_times", "cuvhs_reset_stage_times", "cuvhs_launch_count",
     "cuvhs_dropouts_noalloc", "cuvhs_batch_create", "cuvhs_batch_destroy", "cuvhs_batch_lanes",
     "cuvhs_batch_decode", "cuvhs_batch_last_error", "cuvhs_batch_json", "cuvhs_batch_round_fields",
+    "cuvhs_batch_set_timing", "cuvhs_batch_stage_times",
     "cuvhs_adjoint_create",
     "cuvhs_adjoint_destroy", "cuvhs_adjoint_fields", "cuvhs_adjoint_default_params", "cuvhs_adjoint_set_target",
     "cuvhs_adjoint_fwd", "cuvhs_adjoint_bwd", "cuvhs_adjoint_array", "cuvhs_synth_default_params",
@@ -611,6 +616,17 @@ class Batch:
     def round_fields(self, sample_rate_mhz):
         """Field slots per round in use for this sample rate (0 before first use)."""
         return lib.cuvhs_batch_round_fields(self._h, float(sample_rate_mhz))
+
+    def set_timing(self, on=True):
+        lib.cuvhs_batch_set_timing(self._h, 1 if on else 0)
+
+    def stage_times(self):
+        """{stage: (ms, launches)} summed over the batch's contexts."""
+        n = lib.cuvhs_stage_count()
+        ms = (ctypes.c_double * n)()
+        ln = (ctypes.c_longlong * n)()
+        lib.cuvhs_batch_stage_times(self._h, ms, ln, n)
+        return {lib.cuvhs_stage_name(i).decode(): (ms[i], ln[i]) for i in range(n)}
 
     def close(self):
         if getattr(self, "_h", None):

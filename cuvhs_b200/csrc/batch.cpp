@@ -43,6 +43,7 @@ struct cuvhs_batch {
   // lane -> (rate -> context); a context's field slots are the rate's round size
   std::vector<std::map<double, cuvhs_ctx*>> ctx;
   std::map<double, int> round_fields;  // per rate, tuned or given
+  bool timing = false;                 // per-stage device times on every context
   std::mutex mu;
   std::string err;
   ~cuvhs_batch() {
@@ -137,59 +138,103 @@ cuvhs_status append_portion(Context& c, const Portion& p, cuvhs_output* out, std
   return CUVHS_OK;
 }
 
+// Where a capture stands between rounds: its next chunk's start, whether it
+// has ended, and its output fields so far.
+struct Stand {
+  uint64_t raw;
+  bool done;
+  size_t fields_out;
+};
+
+// The next round from the captures' standings: in order, each capture's next
+// chunk (max_fields fields or what remains) while the slots last.  Captures
+// that have ended or whose output has no room are skipped (`full` lists the
+// latter).  Pure: the same standings give the same round.
+void plan_round(const std::vector<Capture>& caps, const std::vector<Stand>& st, int max_fields, int slots,
+                size_t spf, size_t F, std::vector<Portion>& ps, std::vector<int>& idx, std::vector<int>* full) {
+  ps.clear();
+  idx.clear();
+  int used = 0;
+  for (int i = 0; i < (int)caps.size() && (int)ps.size() < cuvhs::kMaxPortions; i++) {
+    if (st[i].done) continue;
+    const cuvhs_batch_item& it = *caps[i].item;
+    const size_t n = it.n;
+    const uint64_t raw = st[i].raw;
+    const int remaining = raw < n ? (int)((n - raw) / spf) : 0;
+    if (remaining <= 0) continue;
+    const int nf = std::min(max_fields, remaining);
+    if (used + nf > slots) break;  // the round is full
+    const cuvhs_output* out = it.out;
+    const size_t most = std::min<size_t>((size_t)nf, (n - raw) / spf);
+    if (st[i].fields_out + most > out->max_fields) {
+      if (full) full->push_back(i);
+      continue;
+    }
+    Portion p;
+    p.src = it.samples + raw;
+    p.n_avail = n - raw;
+    p.raw_offset = raw;
+    p.num_fields = nf;
+    p.slot0 = used;
+    p.st = const_cast<PortionState*>(&caps[i].st);
+    p.dst_luma = out->luma ? out->luma + st[i].fields_out * F : nullptr;
+    p.dst_chroma = out->chroma ? out->chroma + st[i].fields_out * F : nullptr;
+    ps.push_back(p);
+    idx.push_back(i);
+    used += nf;
+  }
+}
+
 // Decodes `caps` (one sample rate) in rounds on context `ctx`, chunk size
 // max_fields, tune.slots field slots per round (the tuner may grow them).
+// Once a round knows where its captures' next chunks start (after its field
+// windows), the next round is planned from the standings it will leave and
+// its input windows are copied in while the round finishes.
 void run_rounds(cuvhs_batch* b, cuvhs_ctx* ctx, std::vector<Capture>& caps, int max_fields, Tuner& tune) {
   Context& c = ctx->c;
   const size_t spf = (size_t)c.fmt.samples_per_field;
   const size_t F = (size_t)c.fmt.output_line_len * c.fmt.output_field_lines;
   std::vector<Portion> ps;
-  std::vector<int> idx;
+  std::vector<int> idx, full;
+  std::vector<Stand> st(caps.size());
+  auto standings = [&]() {
+    for (size_t i = 0; i < caps.size(); i++) st[i] = Stand{caps[i].raw, caps[i].done, caps[i].item->out->fields_out};
+  };
   for (;;) {
-    ps.clear();
-    idx.clear();
-    int used = 0;
-    const int slots = tune.slots;
-    for (int i = 0; i < (int)caps.size() && (int)ps.size() < cuvhs::kMaxPortions; i++) {
-      Capture& cp = caps[i];
-      if (cp.done) continue;
-      cuvhs_batch_item& it = *cp.item;
-      const size_t n = it.n;
-      const int remaining = cp.raw < n ? (int)((n - cp.raw) / spf) : 0;
-      if (remaining <= 0) {
-        cp.done = true;
-        continue;
-      }
-      const int nf = std::min(max_fields, remaining);
-      if (used + nf > slots) break;  // the round is full
-      cuvhs_output* out = it.out;
-      const size_t most = std::min<size_t>((size_t)nf, (n - cp.raw) / spf);
-      if (out->fields_out + most > out->max_fields) {
-        it.status = CUVHS_ERR_CAPACITY;
-        set_err(b, "output field buffer too small");
-        cp.done = true;
-        continue;
-      }
-      Portion p;
-      p.src = it.samples + cp.raw;
-      p.n_avail = n - cp.raw;
-      p.raw_offset = cp.raw;
-      p.num_fields = nf;
-      p.slot0 = used;
-      p.st = &cp.st;
-      p.dst_luma = out->luma ? out->luma + out->fields_out * F : nullptr;
-      p.dst_chroma = out->chroma ? out->chroma + out->fields_out * F : nullptr;
-      ps.push_back(p);
-      idx.push_back(i);
-      used += nf;
+    standings();
+    full.clear();
+    plan_round(caps, st, max_fields, tune.slots, spf, F, ps, idx, &full);
+    for (int i : full) {
+      caps[i].item->status = CUVHS_ERR_CAPACITY;
+      set_err(b, "output field buffer too small");
+      caps[i].done = true;
     }
+    if (!full.empty()) continue;  // plan again without them
+    for (Capture& cp : caps)
+      if (!cp.done && (cp.raw >= cp.item->n || (cp.item->n - cp.raw) / spf == 0)) cp.done = true;
+    const int used = ps.empty() ? 0 : ps.back().slot0 + ps.back().num_fields;
     if (ps.empty()) {
       c.drain_copies();  // the last rounds' planes are in the callers' buffers
       return;
     }
     c.status = CUVHS_OK;
+    // the next round from the standings this one leaves (the tuner's size
+    // after this round may differ: then the prefetch is not used)
+    auto next_plan = [&](const std::vector<Portion>& cur, std::vector<Portion>& next) {
+      std::vector<Stand> after = st;
+      for (size_t j = 0; j < cur.size(); j++) {
+        Stand& s2 = after[idx[j]];
+        if (cur[j].res.fields == 0) s2.done = true;
+        else {
+          s2.raw = cur[j].res.next_raw_offset;
+          s2.fields_out += (size_t)cur[j].res.fields;
+        }
+      }
+      std::vector<int> nidx;
+      plan_round(caps, after, max_fields, tune.slots, spf, F, next, nidx, nullptr);
+    };
     const auto t0 = std::chrono::steady_clock::now();
-    const bool ok = c.decode_round(ps);
+    const bool ok = c.decode_round(ps, next_plan);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (ok) {
       int fields = 0;
@@ -263,7 +308,7 @@ cuvhs_status cuvhs_batch_create(const cuvhs_batch_config* cfg, cuvhs_batch** out
     return CUVHS_ERR_INVALID_ARGUMENT;
   }
   b->device = dev;
-  b->lanes = cfg->lanes > 0 ? cfg->lanes : 2;
+  b->lanes = cfg->lanes > 0 ? cfg->lanes : 4;
   b->ctx.resize(b->lanes);
   *out = b;
   return CUVHS_OK;
@@ -274,6 +319,33 @@ void cuvhs_batch_destroy(cuvhs_batch* b) { delete b; }
 int cuvhs_batch_lanes(const cuvhs_batch* b) { return b ? b->lanes : 0; }
 
 const char* cuvhs_batch_last_error(const cuvhs_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+void cuvhs_batch_set_timing(cuvhs_batch* b, int on) {
+  if (!b) return;
+  b->timing = on != 0;
+  for (auto& m : b->ctx)
+    for (auto& kv : m) cuvhs_set_timing(kv.second, on);
+}
+
+int cuvhs_batch_stage_times(const cuvhs_batch* b, double* ms, long long* launches, int cap) {
+  if (!b) return 0;
+  const int n = std::min(cap, (int)cuvhs::kNumStages);
+  for (int i = 0; i < n; i++) {
+    if (ms) ms[i] = 0.0;
+    if (launches) launches[i] = 0;
+  }
+  std::vector<double> t(cuvhs::kNumStages);
+  std::vector<long long> l(cuvhs::kNumStages);
+  for (auto& m : b->ctx)
+    for (auto& kv : m) {
+      cuvhs_stage_times(kv.second, t.data(), l.data(), cuvhs::kNumStages);
+      for (int i = 0; i < n; i++) {
+        if (ms) ms[i] += t[i];
+        if (launches) launches[i] += l[i];
+      }
+    }
+  return cuvhs::kNumStages;
+}
 
 int cuvhs_batch_round_fields(const cuvhs_batch* b, double sample_rate_mhz) {
   if (!b) return 0;
@@ -361,6 +433,7 @@ cuvhs_status cuvhs_batch_decode(cuvhs_batch* b, cuvhs_batch_item* items, int n_i
           set_err(b, "context creation failed");
           continue;
         }
+        cuvhs_set_timing(ctx, b->timing ? 1 : 0);
       }
       tune.cap = std::min(cap, cuvhs_batch_fields(ctx));
       if (known > 0) {

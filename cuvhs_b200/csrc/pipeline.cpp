@@ -155,6 +155,8 @@ void Context::release() {
   pf = Prefetch();
   if (xstream) cudaStreamDestroy(xstream);
   xstream = nullptr;
+  if (ostream) cudaStreamDestroy(ostream);
+  ostream = nullptr;
   if (stream) cudaStreamDestroy(stream);
   stream = nullptr;
 }
@@ -386,6 +388,7 @@ bool Context::init(const cuvhs_config& c) {
   cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&xstream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ostream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&hstream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithPriority(&lstream, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
       cudaStreamCreateWithFlags(&pstream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -473,6 +476,7 @@ bool Context::check_cuda(const char* where) {
 bool Context::sync(const char* where) {
   cudaError_t e = cudaStreamSynchronize(stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(xstream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ostream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(hstream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(lstream);
   if (e != cudaSuccess) {
@@ -488,8 +492,11 @@ bool Context::sync(const char* where) {
 // copied); later work on the stream keeps running.
 bool Context::drain_copies() {
   cudaError_t e = cudaStreamSynchronize(xstream);
+  const cudaError_t e0 = cudaStreamSynchronize(ostream);
+  if (e == cudaSuccess) e = e0;
   const cudaError_t e2 = cudaStreamSynchronize(hstream);
   pf.valid = false;
+  rpf.valid = false;
   if (e == cudaSuccess) e = e2;
   if (e != cudaSuccess) {
     err = std::string("output copies: ") + cudaGetErrorString(e);
@@ -818,9 +825,9 @@ bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, u
     }
     if (dst_chroma) {
       cudaEventRecord(ev_chroma, stream);
-      cudaStreamWaitEvent(xstream, ev_chroma, 0);
+      cudaStreamWaitEvent(ostream, ev_chroma, 0);
       cudaMemcpyAsync(dst_chroma + (size_t)f0 * F, ca.chroma + (size_t)f0 * F, (size_t)nf * F * sizeof(uint16_t),
-                      cudaMemcpyDeviceToHost, xstream);
+                      cudaMemcpyDeviceToHost, ostream);
     }
   };
   auto chroma_pass = [&](int f0, int nf, bool write) {
@@ -944,6 +951,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     ~CopyDrain() {
       if (keep) return;
       cudaStreamSynchronize(c->xstream);
+      cudaStreamSynchronize(c->ostream);
       cudaStreamSynchronize(c->hstream);
       cudaStreamSynchronize(c->pstream);  // after an error, nothing of the chunk is left running
       cudaStreamSynchronize(c->lstream);
@@ -1280,8 +1288,10 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   cudaMemcpyAsync(hp_do_starts, d_do_starts, ndo * sizeof(int), cudaMemcpyDeviceToHost, xstream);
   cudaMemcpyAsync(hp_do_ends, d_do_ends, ndo * sizeof(int), cudaMemcpyDeviceToHost, xstream);
   cudaEventRecord(ev_small, xstream);
-  if (dst_luma)
-    cudaMemcpyAsync(dst_luma, d_luma, (size_t)P * F * sizeof(uint16_t), cudaMemcpyDeviceToHost, xstream);
+  if (dst_luma) {
+    cudaStreamWaitEvent(ostream, ev_luma, 0);
+    cudaMemcpyAsync(dst_luma, d_luma, (size_t)P * F * sizeof(uint16_t), cudaMemcpyDeviceToHost, ostream);
+  }
   // ---- K6 chroma on the P detected fields
   ca.fields = P;
   ca.total = (long long)P * spp;
@@ -1289,7 +1299,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   cudaStreamWaitEvent(stream, ev_pre, 0);
   if (!chroma_fields(ca, P, &dd, dst_chroma)) return false;
   if (!check_cuda("chroma concealment")) return false;
-  cudaEventRecord(ev_out_done[oset], xstream);
+  cudaEventRecord(ev_out_done[oset], ostream);
   if (debug) {
     dbg_ll.resize((size_t)P * LPF);
     cudaMemcpyAsync(dbg_ll.data(), d_ll, dbg_ll.size() * sizeof(double), cudaMemcpyDeviceToHost, stream);

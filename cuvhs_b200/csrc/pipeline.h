@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -99,6 +100,10 @@ struct Context {
   // Copy stream: host input arrives in pieces (K1a starts on each piece as it
   // lands) and the finished luma leaves while chroma is still being decoded.
   cudaStream_t xstream = nullptr;
+  // Output stream: the TBC planes leave on their own stream, so the small
+  // copies the host waits on (window records, dropout lists) never queue
+  // behind a chunk's or round's plane copies.
+  cudaStream_t ostream = nullptr;
   static constexpr int kInputPieces = 8;
   cudaEvent_t ev_piece[kInputPieces] = {};
   cudaEvent_t ev_luma = nullptr;
@@ -273,7 +278,19 @@ struct Context {
   // The next chunk of up to kMaxPortions captures in one pass of batched
   // launches (round.cpp); res of each portion as decode_chunk's, its dropout
   // lists at hp_do_* + slot0 * kMaxDropouts.
-  bool decode_round(std::vector<Portion>& ps);
+  // next_plan, when given, is called once the round's field windows are
+  // known (each portion's res.fields and next_raw_offset set) and returns the
+  // next round's portions, whose input windows are then copied into the other
+  // raw buffer while this round finishes; a next call with exactly those
+  // portions reads them there.
+  using RoundPlan = std::function<void(const std::vector<Portion>&, std::vector<Portion>&)>;
+  bool decode_round(std::vector<Portion>& ps, const RoundPlan& next_plan = nullptr);
+  struct RoundPrefetch {
+    bool valid = false;
+    int set = 0;
+    std::vector<std::pair<const uint8_t*, long long>> sig;  // (src, n_read << 20 | slot0) per portion
+  } rpf;
+  int round_raw_set = 0;
   float* hp_round_burst = nullptr;  // pinned: trial-pass burst windows of a round's captures (on first use)
   // K1 arguments over T tiles of the current raw buffer into the context's buffers.
   DemodArgs demod_args(int T) const;

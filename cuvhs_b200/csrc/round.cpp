@@ -24,7 +24,7 @@
 
 namespace cuvhs {
 
-bool Context::decode_round(std::vector<Portion>& ps) {
+bool Context::decode_round(std::vector<Portion>& ps, const RoundPlan& next_plan) {
   cudaSetDevice(device);
   const int K = (int)ps.size();
   if (K < 1 || K > kMaxPortions) {
@@ -70,17 +70,38 @@ bool Context::decode_round(std::vector<Portion>& ps) {
     Context* c;
     bool keep_copies = false;
     ~Drain() {
-      for (cudaStream_t st : {c->stream, c->hstream, c->pstream, c->lstream, c->gstream}) cudaStreamSynchronize(st);
-      if (!keep_copies) cudaStreamSynchronize(c->xstream);
+      for (cudaStream_t st : {c->stream, c->pstream, c->lstream, c->gstream}) cudaStreamSynchronize(st);
+      cudaStreamSynchronize(c->xstream);
+      if (!keep_copies) {
+        cudaStreamSynchronize(c->ostream);
+        cudaStreamSynchronize(c->hstream);
+        c->rpf.valid = false;
+      }
       c->pf.valid = false;
     }
   } drain{this};
+  // the round's input: prefetched by the round before, or copied now
+  auto sig_of = [&](const std::vector<Portion>& v, const std::vector<int>& which) {
+    std::vector<std::pair<const uint8_t*, long long>> sg;
+    for (int k : which) sg.push_back({v[k].src, ((long long)v[k].n_read << 20) | v[k].slot0});
+    return sg;
+  };
+  bool prefetched = false;
+  {
+    std::vector<int> all(L);
+    for (int j = 0; j < L; j++) all[j] = live[j];
+    if (rpf.valid && rpf.sig == sig_of(ps, all)) {
+      prefetched = true;
+      round_raw_set = rpf.set;
+    }
+    rpf.valid = false;
+  }
   const size_t F = (size_t)fmt.output_line_len * fmt.output_field_lines;
   const int H = fmt.output_field_lines, LPF = fmt.lines_per_frame;
   const int oset = out_set;
   d_luma = d_luma_set[oset];
   d_chroma = d_chroma_set[oset];
-  d_raw = d_raw_set[0];
+  d_raw = d_raw_set[round_raw_set];
   cudaStreamWaitEvent(stream, ev_out_done[oset], 0);  // the copies of the round before last out of this set
   const size_t wps = kBitWordsPerSlot(spp), eps = kEdgesPerSlot(spp), bps_ = kEdgeBlocksPerSlot(spp);
   int max_T = 0, max_nf = 0;
@@ -161,12 +182,14 @@ bool Context::decode_round(std::vector<Portion>& ps) {
     cm.a[j] = ca;
     hp_lls[j] = p.st->lls;
   }
-  // ---- input windows (one copy per capture) and the carried line-location states
-  for (int j = 0; j < L; j++) {
-    const Portion& p = ps[live[j]];
-    cudaMemcpyAsync(d_raw + (size_t)p.slot0 * spp * bps, p.src, (size_t)p.n_read * bps, cudaMemcpyHostToDevice,
-                    hstream);
-  }
+  // ---- input windows (one copy per capture, unless prefetched) and the
+  // carried line-location states
+  if (!prefetched)
+    for (int j = 0; j < L; j++) {
+      const Portion& p = ps[live[j]];
+      cudaMemcpyAsync(d_raw + (size_t)p.slot0 * spp * bps, p.src, (size_t)p.n_read * bps, cudaMemcpyHostToDevice,
+                      hstream);
+    }
   cudaMemcpyAsync(d_lls, hp_lls, (size_t)L * sizeof(LineLocState), cudaMemcpyHostToDevice, hstream);
   cudaEventRecord(ev_piece[0], hstream);
   cudaStreamWaitEvent(stream, ev_piece[0], 0);
@@ -271,6 +294,27 @@ bool Context::decode_round(std::vector<Portion>& ps) {
     p.res.next_raw_offset = p.raw_offset + (uint64_t)hp_win[j].next_rel;
     max_P = std::max(max_P, p.res.fields);
   }
+  // ---- the next round's input windows, into the other raw buffer
+  if (next_plan) {
+    std::vector<Portion> next;
+    next_plan(ps, next);
+    std::vector<int> nlive;
+    const int other = 1 - round_raw_set;
+    for (int k = 0; k < (int)next.size(); k++) {
+      Portion& q = next[k];
+      const size_t total = (size_t)q.num_fields * spp;
+      q.n_read = (int)std::min(total, q.n_avail);
+      if (q.n_read < (int)spf) continue;  // no field: not decoded
+      nlive.push_back(k);
+      cudaMemcpyAsync(d_raw_set[other] + (size_t)q.slot0 * spp * bps, q.src, (size_t)q.n_read * bps,
+                      cudaMemcpyHostToDevice, hstream);
+    }
+    if (!nlive.empty()) {
+      rpf.valid = true;
+      rpf.set = other;
+      rpf.sig = sig_of(next, nlive);
+    }
+  }
   if (max_P == 0) {
     if (!sync("empty round")) return false;
     return true;
@@ -325,11 +369,12 @@ bool Context::decode_round(std::vector<Portion>& ps) {
   cudaMemcpyAsync(hp_do_starts, d_do_starts, ndo * sizeof(int), cudaMemcpyDeviceToHost, xstream);
   cudaMemcpyAsync(hp_do_ends, d_do_ends, ndo * sizeof(int), cudaMemcpyDeviceToHost, xstream);
   cudaEventRecord(ev_small, xstream);
+  cudaStreamWaitEvent(ostream, ev_luma, 0);
   for (int j = 0; j < L; j++) {
     const Portion& p = ps[live[j]];
     if (p.dst_luma && p.res.fields > 0)
       cudaMemcpyAsync(p.dst_luma, nm.a[j].luma, (size_t)p.res.fields * F * sizeof(uint16_t), cudaMemcpyDeviceToHost,
-                      xstream);
+                      ostream);
   }
   // ---- chroma: track and phase for captures without carried chroma state
   // (two trial passes over field 0 of every capture), then every field, then
@@ -412,39 +457,42 @@ bool Context::decode_round(std::vector<Portion>& ps) {
   t_host = host_clock();
   if (!wait_host_event("round chroma lines")) return false;
   host_phase(kHostChromaWait, t_host);
-  // per capture: the reference's 15-field chunks with up to three retries,
-  // recomputing only the fields a flip changed (one capture's launches)
+  // Per capture, the reference's 15-field groups with up to three retries
+  // each (chroma_decode.cu:782-981), recomputing only fields a flip changed.
+  // The captures advance in lockstep: each runs its host decisions until it
+  // needs a group recomputed, then one launch set over all captures waiting
+  // on a recompute (each on a view of its group's fields) and one wait serve
+  // them together.
   const int fpc_cap = std::max(1, 4096 / H);
+  struct Replay {
+    int P = 0, fpc = 1, g = 0, it = 0;  // group, iteration within it
+    bool done = true;
+    std::vector<int> computed;
+  };
+  std::vector<Replay> rp(L);
   for (int j = 0; j < L; j++) {
     const Portion& p = ps[live[j]];
-    const int P = p.res.fields;
-    if (P == 0) continue;
-    int* track = hp_track + p.slot0;
-    std::vector<int> computed(track, track + P);
-    const double* metric = hp_metric + p.slot0;
-    const int fpc = std::max(1, std::min(fpc_cap, P));
-    for (int f0 = 0; f0 < P; f0 += fpc) {
-      const int nf = std::min(fpc, P - f0);
-      int retries = 3;
-      bool ok = false;
-      while (!ok && retries-- > 0) {
+    Replay& r = rp[j];
+    r.P = p.res.fields;
+    r.done = r.P == 0;
+    r.fpc = std::max(1, std::min(fpc_cap, std::max(r.P, 1)));
+    r.computed.assign(hp_track + p.slot0, hp_track + p.slot0 + r.P);
+  }
+  std::vector<int> need;
+  for (;;) {
+    need.clear();
+    for (int j = 0; j < L; j++) {
+      Replay& r = rp[j];
+      const Portion& p = ps[live[j]];
+      int* track = hp_track + p.slot0;
+      const double* metric = hp_metric + p.slot0;
+      while (!r.done) {
+        const int f0 = r.g * r.fpc, nf = std::min(r.fpc, r.P - f0);
         bool stale = false;
-        for (int f = f0; f < f0 + nf; f++) stale = stale || computed[f] != track[f];
+        for (int f = f0; f < f0 + nf; f++) stale = stale || r.computed[f] != track[f];
         if (stale) {
-          cudaMemcpyAsync(d_track + p.slot0 + f0, track + f0, nf * sizeof(int), cudaMemcpyHostToDevice, stream);
-          cudaEvent_t ev_;
-          begin_stage(kStageChromaLines, ev_);
-          launch_chroma_lines(cm.a[j], f0, nf, true, stream);
-          end_stage(kStageChromaLines, ev_);
-          begin_stage(kStageBurstMetric, ev_);
-          launch_burst_metric(cm.a[j], f0, nf, stream);
-          end_stage(kStageBurstMetric, ev_);
-          begin_stage(kStageDropouts, ev_);
-          launch_dropout_conceal_chroma(om.a[j], f0, nf, stream);
-          end_stage(kStageDropouts, ev_);
-          cudaEventRecord(ev_host, stream);
-          if (!wait_host_event("round chroma retry")) return false;
-          for (int f = f0; f < f0 + nf; f++) computed[f] = track[f];
+          need.push_back(j);  // recompute, then decide on the new metrics
+          break;
         }
         int first_bad = INT_MAX;
         for (int f = 0; f < nf; f++)
@@ -452,25 +500,81 @@ bool Context::decode_round(std::vector<Portion>& ps) {
             first_bad = f;
             break;
           }
-        if (first_bad == INT_MAX) {
-          ok = true;
-        } else {
+        bool next_group = first_bad == INT_MAX;
+        if (!next_group) {
           cur[j] = 1 - cur[j];
-          for (int ff = f0 + first_bad; ff < P; ff++) track[ff] = (ff & 1) ? (1 - cur[j]) : cur[j];
+          for (int ff = f0 + first_bad; ff < r.P; ff++) track[ff] = (ff & 1) ? (1 - cur[j]) : cur[j];
+          next_group = ++r.it == 3;
+        }
+        if (next_group) {
+          r.g++;
+          r.it = 0;
+          if (r.g * r.fpc >= r.P) r.done = true;
         }
       }
+    }
+    if (need.empty()) break;
+    static thread_local ArgsMany<ChromaArgs> cv;
+    static thread_local ArgsMany<DropoutArgs> ov;
+    int max_nf = 0;
+    for (size_t q = 0; q < need.size(); q++) {
+      const int j = need[q];
+      const Replay& r = rp[j];
+      const int f0 = r.g * r.fpc, nf = std::min(r.fpc, r.P - f0);
+      max_nf = std::max(max_nf, nf);
+      const int s0 = ps[live[j]].slot0;
+      cudaMemcpyAsync(d_track + s0 + f0, hp_track + s0 + f0, nf * sizeof(int), cudaMemcpyHostToDevice, stream);
+      // the capture's fields [f0, f0 + nf) as a capture of nf fields
+      ChromaArgs c = cm.a[j];
+      c.ll += (size_t)f0 * LPF;
+      c.track += f0;
+      c.chroma += (size_t)f0 * F;
+      c.burst += (size_t)f0 * H * fmt.burst_len;
+      c.metric += f0;
+      c.fields = nf;
+      cv.a[q] = c;
+      DropoutArgs o = om.a[j];
+      o.ll += (size_t)f0 * LPF;
+      o.luma += (size_t)f0 * F;
+      o.chroma += (size_t)f0 * F;
+      o.do_count += f0;
+      o.do_lines += (size_t)f0 * kMaxDropouts;
+      o.do_starts += (size_t)f0 * kMaxDropouts;
+      o.do_ends += (size_t)f0 * kMaxDropouts;
+      o.cls += (size_t)f0 * o.max_blocks;
+      o.fields = nf;
+      ov.a[q] = o;
+    }
+    const int nq = (int)need.size();
+    cudaEvent_t ev_;
+    begin_stage(kStageChromaLines, ev_);
+    launch_chroma_lines_many(cv, nq, -1, max_nf, true, stream);
+    end_stage(kStageChromaLines, ev_);
+    begin_stage(kStageBurstMetric, ev_);
+    launch_burst_metric_many(cv, nq, max_nf, stream);
+    end_stage(kStageBurstMetric, ev_);
+    begin_stage(kStageDropouts, ev_);
+    launch_dropout_conceal_chroma_many(ov, nq, max_nf, stream);
+    end_stage(kStageDropouts, ev_);
+    cudaEventRecord(ev_host, stream);
+    if (!wait_host_event("round chroma retry")) return false;
+    for (int j : need) {
+      Replay& r = rp[j];
+      const int f0 = r.g * r.fpc, nf = std::min(r.fpc, r.P - f0);
+      const int* track = hp_track + ps[live[j]].slot0;
+      for (int f = f0; f < f0 + nf; f++) r.computed[f] = track[f];
     }
   }
   // chroma planes out
   cudaEventRecord(ev_chroma, stream);
-  cudaStreamWaitEvent(xstream, ev_chroma, 0);
+  cudaStreamWaitEvent(ostream, ev_chroma, 0);
   for (int j = 0; j < L; j++) {
     const Portion& p = ps[live[j]];
     if (p.dst_chroma && p.res.fields > 0)
       cudaMemcpyAsync(p.dst_chroma, cm.a[j].chroma, (size_t)p.res.fields * F * sizeof(uint16_t),
-                      cudaMemcpyDeviceToHost, xstream);
+                      cudaMemcpyDeviceToHost, ostream);
   }
-  cudaEventRecord(ev_out_done[oset], xstream);
+  cudaEventRecord(ev_out_done[oset], ostream);
   // carried line-location states back
   cudaMemcpyAsync(hp_lls, d_lls, (size_t)L * sizeof(LineLocState), cudaMemcpyDeviceToHost, stream);
   t_host = host_clock();

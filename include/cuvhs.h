@@ -356,7 +356,7 @@ typedef struct cuvhs_batch cuvhs_batch;
 
 typedef struct cuvhs_batch_config {
   int device;       /* CUDA device id, -1 = the one with most memory */
-  int lanes;        /* concurrent round drivers; 0 = 2 */
+  int lanes;        /* concurrent round drivers; 0 = 4 */
   int max_fields;   /* chunk size of every capture; 0 = 256 (one chunk per capture of up
                        to 256 fields, as a single-capture decode with the default
                        chunk size) */
@@ -383,6 +383,10 @@ long long cuvhs_batch_json(const cuvhs_batch_item* item, char* dst, long long ca
 /* Field slots per round the batch uses for captures at this sample rate
  * (after the autotuner ran for it, or round_fields); 0 before first use. */
 int cuvhs_batch_round_fields(const cuvhs_batch* b, double sample_rate_mhz);
+/* Per-stage device times summed over the batch's contexts (as
+ * cuvhs_stage_times), recorded while timing is on. */
+void cuvhs_batch_set_timing(cuvhs_batch* b, int on);
+int cuvhs_batch_stage_times(const cuvhs_batch* b, double* ms, long long* launches, int cap);
 
 /* ------------------------------------------------------------- calibration
  * A differentiable decode model and its adjoint, for calibrating a tape's

@@ -360,6 +360,93 @@ __device__ bool attempt(const int* ps, const int* pl, int n, int first, const IW
   return done && cnt > 0;
 }
 
+// The same recogniser run by a whole warp on one attempt: lane k holds pulse
+// first + k, and every lane steps the state machine over the lanes' pulses
+// (broadcast by shuffles), so no lane diverges and no step waits on shared
+// memory.  Returns the closing flag, the count and last type, and the kept
+// steps (bit k) with their types (2 bits at 2k).
+struct WarpAttempt {
+  bool ok;
+  int cnt, last;
+  unsigned keep;
+  unsigned long long types;
+};
+__device__ WarpAttempt attempt_warp(const int* ps, const int* pl, int n, int first, const IWindows& w, int eq_pulses,
+                                    int line_len) {
+  const int lane = threadIdx.x & 31;
+  const int end = min(n, first + 26);
+  const int mine = first + lane;
+  const int my_len = mine < end ? pl[mine] : 0, my_start = mine < end ? ps[mine] : 0;
+  bool done = false, vsync_seen = false;
+  const double half = eq_pulses / 2.0;
+  long long hold_floor = 0, hold_ceil = 0;
+  double pending = -1.0;
+  int cur = kHsync, cnt = 0;
+  unsigned keep_mask = 0;
+  unsigned long long types = 0;
+  const int steps = end - first;
+  for (int k = 0; k < steps; k++) {
+    const int len = __shfl_sync(0xffffffffu, my_len, k);
+    const int start = __shfl_sync(0xffffffffu, my_start, k);
+    int type = -1;
+    const bool h = in_class(len, w.h_lo, w.h_hi), e = in_class(len, w.e_lo, w.e_hi),
+               v = in_class(len, w.v_lo, w.v_hi);
+    switch (cur) {
+      case kHsync:
+        if (h) type = kHsync;
+        else if (e) {
+          type = kEq1;
+          pending = half;
+        } else if (v) {
+          vsync_seen = true;
+          type = kVsync;
+        }
+        break;
+      case kEq1:
+        if (e) type = kEq1;
+        else if (v) {
+          vsync_seen = true;
+          type = kVsync;
+          pending = half;
+        } else if (h) type = kHsync;
+        break;
+      case kVsync:
+        if (e) {
+          type = kEq2;
+          pending = half;
+        } else if (v) type = kVsync;
+        else if ((long long)start > hold_floor && h) type = kHsync;
+        break;
+      case kEq2:
+        if (e) type = kEq2;
+        else if (h) {
+          type = kHsync;
+          done = true;
+        }
+        break;
+    }
+    bool kept = type >= 0;
+    if (kept && type != cur) {
+      if ((long long)start < hold_ceil) {
+        kept = false;
+      } else if (pending > 0.0) {
+        const double hold = (double)start + ((pending - 0.1) * (double)line_len);
+        hold_floor = (long long)floor(hold);
+        hold_ceil = (long long)ceil(hold);
+        pending = -1.0;
+      }
+    }
+    if (kept) {
+      keep_mask |= 1u << k;
+      types |= (unsigned long long)type << (2 * k);
+      cnt++;
+      cur = type;
+    }
+    if (done && vsync_seen) break;
+  }
+  return WarpAttempt{done && cnt > 0, cnt, cur, keep_mask, types};
+}
+
 // Block-wide sum of a long long (kLT threads); every thread gets the total.
 __device__ long long block_sum_ll(long long v, long long* sh) {
   for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
@@ -431,18 +518,39 @@ __device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
   wd.v_lo = (fmt.vsync_width + shift) * 0.5;
   wd.v_hi = fmt.vsync_width + shift + 2.0 * tol;
   const IWindows w = int_windows(wd);
-  // classes and every recogniser attempt
-  for (int i = t; i < n; i += kLT) {
-    const int len = sm.pl[i];
-    const bool h = in_class(len, w.h_lo, w.h_hi);
-    const bool e = !h && i > 2 && in_class(len, w.e_lo, w.e_hi);
-    sm.cls[i] = (h ? 1 : 0) | (e ? 2 : 0);
-    int cnt = 0, last = kHsync;
-    bool ok = false;
-    if (e) ok = attempt(sm.ps, sm.pl, n, i - 2, w, fmt.num_eq_pulses, fmt.samples_per_line, &cnt, &last);
-    sm.att_ok[i] = ok ? 1 : 0;
-    sm.att_len[i] = cnt;
-    sm.att_last[i] = (unsigned char)last;
+  // classes, then every recogniser attempt (one per EQ-width pulse), a warp
+  // per attempt over a compacted list of them
+  __shared__ int n_att;
+  int* att_list = sm.pos;  // free until the placement scan
+  if (t == 0) n_att = 0;
+  __syncthreads();
+  for (int i0 = 0; i0 < n; i0 += kLT) {
+    const int i = i0 + t;
+    bool e = false;
+    if (i < n) {
+      const int len = sm.pl[i];
+      const bool h = in_class(len, w.h_lo, w.h_hi);
+      e = !h && i > 2 && in_class(len, w.e_lo, w.e_hi);
+      sm.cls[i] = (h ? 1 : 0) | (e ? 2 : 0);
+      sm.att_ok[i] = 0;
+      sm.att_len[i] = 0;
+      sm.att_last[i] = (unsigned char)kHsync;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, e);
+    int base = 0;
+    if (lane == 0 && m) base = atomicAdd(&n_att, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (e) att_list[base + __popc(m & ((1u << lane) - 1u))] = i;
+  }
+  __syncthreads();
+  for (int q = warp; q < n_att; q += kLT / 32) {
+    const int i = att_list[q];
+    const WarpAttempt r = attempt_warp(sm.ps, sm.pl, n, i - 2, w, fmt.num_eq_pulses, fmt.samples_per_line);
+    if (lane == 0) {
+      sm.att_ok[i] = r.ok ? 1 : 0;
+      sm.att_len[i] = r.cnt;
+      sm.att_last[i] = (unsigned char)r.last;
+    }
   }
   __syncthreads();
   phase_clock(a, blockIdx.x, 22);
@@ -511,7 +619,12 @@ __device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
   __syncthreads();
   phase_clock(a, blockIdx.x, 23);
   const int nv = sm.pos[n];
-  // place every pulse's output
+  // place every pulse's output: hsyncs one per thread, the attempts that
+  // fire (a few per field) by a warp each, their kept steps written in order
+  __shared__ int n_fire;
+  __shared__ int fire_list[64];
+  if (t == 0) n_fire = 0;
+  __syncthreads();
   for (int i = t; i < n; i += kLT) {
     const int p = sm.pos[i], len = sm.pos[i + 1] - p;
     if (len <= 0) continue;
@@ -520,9 +633,26 @@ __device__ int validate(const LineLocArgs& a, FieldSmem& sm, int n, VList& v) {
       v.l[p] = sm.pl[i];
       v.tg[p] = kHsync;
     } else {
-      int cnt = 0, last = 0;
-      attempt(sm.ps, sm.pl, n, i - 2, w, fmt.num_eq_pulses, fmt.samples_per_line, &cnt, &last, v.s + p, v.l + p,
-              v.tg + p);
+      const int q = atomicAdd(&n_fire, 1);
+      if (q < 64) {
+        fire_list[q] = i;
+      } else {  // more firing attempts than the list holds: this thread writes its own
+        int cnt = 0, last = 0;
+        attempt(sm.ps, sm.pl, n, i - 2, w, fmt.num_eq_pulses, fmt.samples_per_line, &cnt, &last, v.s + p, v.l + p,
+                v.tg + p);
+      }
+    }
+  }
+  __syncthreads();
+  for (int q = warp; q < min(n_fire, 64); q += kLT / 32) {
+    const int i = fire_list[q];
+    const int p = sm.pos[i];
+    const WarpAttempt r = attempt_warp(sm.ps, sm.pl, n, i - 2, w, fmt.num_eq_pulses, fmt.samples_per_line);
+    if ((r.keep >> lane) & 1u) {
+      const int o = p + __popc(r.keep & ((1u << lane) - 1u));
+      v.s[o] = sm.ps[i - 2 + lane];
+      v.l[o] = sm.pl[i - 2 + lane];
+      v.tg[o] = (unsigned char)((r.types >> (2 * lane)) & 3u);
     }
   }
   __syncthreads();
@@ -925,8 +1055,64 @@ __device__ double hsync_diff_after(const AnchorFit& f, const Format& fmt, bool f
 // Sorted validated starts in sm.sort (bitonic, padded with +inf) or, past
 // kSortMax entries, in v.d (insertion sort by thread 0).  Returns the array.
 __device__ const double* sorted_starts(FieldSmem& sm, const VList& v) {
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   if (v.n <= kSortMax) {
+    // The list is a few ascending runs (the recogniser re-emits the pulses
+    // just before a blanking interval, and the walk then goes on from the
+    // pulse after it): each entry's place is its index in its run plus, per
+    // other run, the entries below it (an earlier run's equal entries first),
+    // found by binary search -- a stable merge in one parallel pass.
+    constexpr int kMaxRuns = 32;
+    __shared__ int runs[kMaxRuns + 1];
+    __shared__ int wcnt[kLT / 32];
+    int nruns = 0;
+    for (int k0 = 0; k0 < v.n; k0 += kLT) {
+      const int k = k0 + t;
+      const bool start = k < v.n && (k == 0 || v.s[k] < v.s[k - 1]);
+      const unsigned m = __ballot_sync(0xffffffffu, start);
+      if (lane == 0) wcnt[warp] = __popc(m);
+      __syncthreads();
+      int before = 0, total = 0;
+      for (int w = 0; w < kLT / 32; w++) {
+        if (w < warp) before += wcnt[w];
+        total += wcnt[w];
+      }
+      if (start) {
+        const int r = nruns + before + __popc(m & ((1u << lane) - 1u));
+        if (r < kMaxRuns) runs[r] = k;
+      }
+      nruns += total;
+      __syncthreads();
+    }
+    if (nruns <= kMaxRuns) {
+      if (t == 0) runs[nruns] = v.n;
+      __syncthreads();
+      for (int k = t; k < v.n; k += kLT) {
+        const int x = v.s[k];
+        int lo = 0, hi = nruns;  // the run holding k: last start <= k
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (runs[mid] <= k) lo = mid;
+          else hi = mid;
+        }
+        const int r = lo;
+        int rank = k - runs[r];
+        for (int q = 0; q < nruns; q++) {
+          if (q == r) continue;
+          int b = runs[q], e = runs[q + 1];  // entries of run q below x (at most x for an earlier run)
+          while (b < e) {
+            const int mid = (b + e) >> 1;
+            const bool below = q < r ? v.s[mid] <= x : v.s[mid] < x;
+            if (below) b = mid + 1;
+            else e = mid;
+          }
+          rank += b - runs[q];
+        }
+        sm.sort[rank] = (double)x;
+      }
+      __syncthreads();
+      return sm.sort;
+    }
     int m = 1;
     while (m < v.n) m <<= 1;
     for (int k = t; k < m; k += kLT) sm.sort[k] = k < v.n ? (double)v.s[k] : __longlong_as_double(0x7ff0000000000000LL);
@@ -979,9 +1165,10 @@ __device__ const double* sorted_starts(FieldSmem& sm, const VList& v) {
 // cursor (its pulse taken by an earlier line) is walked from the cursor by one
 // lane, as the reference does.
 __device__ void snap_lines(FieldSmem& sm, const VList& v, double ref_pos, double ref_line, double mll, int nlines,
-                           double* locs) {
+                           double* locs, long long* clk = nullptr) {
   const double* ps = sorted_starts(sm, v);
   const int t = threadIdx.x, np = v.n;
+  if (clk && t == 0) clk[30] = clock64();
   const double max_dist = mll / 1.5;
   int* stop = sm.pos;      // per line: S capped at np - 2, << 1 | within max_dist
   int* taken = sm.att_len; // per line: the pulse it snaps to, or -1
@@ -1009,6 +1196,7 @@ __device__ void snap_lines(FieldSmem& sm, const VList& v, double ref_pos, double
     }
   }
   __syncthreads();
+  if (clk && t == 0) clk[31] = clock64();
   if (t < 32) {
     const int lane = t;
     int cur = 0;
@@ -1138,7 +1326,8 @@ __global__ void __launch_bounds__(kLT, 1) prepare_kernel(const __grid_constant__
                                        st.prev_first_hsync_diff, a.dbg_clk ? a.dbg_clk + (size_t)f * kPhaseSlots : nullptr);
       phase_clock(a, f, 6);
       if (fit.cnt > 0)
-        snap_lines(sm, v, fit.loc, fit.hsync_line, mll, a.fmt.lines_per_frame, a.ll + (size_t)f * a.fmt.lines_per_frame);
+        snap_lines(sm, v, fit.loc, fit.hsync_line, mll, a.fmt.lines_per_frame, a.ll + (size_t)f * a.fmt.lines_per_frame,
+                   a.dbg_clk ? a.dbg_clk + (size_t)f * kPhaseSlots : nullptr);
       phase_clock(a, f, 7);
       p.exact_first = first ? 1 : 0;
       p.spec = fit;
@@ -1148,7 +1337,8 @@ __global__ void __launch_bounds__(kLT, 1) prepare_kernel(const __grid_constant__
                                      a.dbg_clk ? a.dbg_clk + (size_t)f * kPhaseSlots : nullptr);
     phase_clock(a, f, 6);
     if (fit.cnt > 0 && !fit.used_prediction) {
-      snap_lines(sm, v, fit.loc, fit.hsync_line, mll, a.fmt.lines_per_frame, a.ll + (size_t)f * a.fmt.lines_per_frame);
+      snap_lines(sm, v, fit.loc, fit.hsync_line, mll, a.fmt.lines_per_frame, a.ll + (size_t)f * a.fmt.lines_per_frame,
+                 a.dbg_clk ? a.dbg_clk + (size_t)f * kPhaseSlots : nullptr);
       p.spec_first = pf;
       p.spec = fit;
     }
@@ -1193,15 +1383,16 @@ __global__ void __launch_bounds__(kLT, 1) finish_kernel(const __grid_constant__ 
   __shared__ FieldPrep preps[kPrepBatch];
   __shared__ long long readlocs[kPrepBatch];
   __shared__ unsigned char fallback[kPrepBatch];
-  __shared__ LineLocState st;
   __shared__ int fit_j, fit_first;
   __shared__ double prev_off_s, prev_loc_s, prev_diff_s;
   const int t = threadIdx.x;
   const int P = a.win->fields;
   const int LPF = a.fmt.lines_per_frame;
-  // the hsync difference still to be formed from the last anchored field
-  // (thread 0 only): its rounded anchor, mll, order, the previous anchor's
-  // read location and location, and its own read location
+  // The carried state lives in thread 0's registers for the whole walk.
+  // The hsync difference is formed only when a fit or the next chunk reads
+  // it: from the last anchored field's rounded anchor, mll, order, the
+  // previous anchor's read location and location, and its own read location.
+  LineLocState st;
   bool diff_due = false;
   double d_round = 0.0, d_mll = 0.0, d_prev_loc = 0.0;
   long long d_prev_read = -1, d_read = 0;
@@ -1216,6 +1407,29 @@ __global__ void __launch_bounds__(kLT, 1) finish_kernel(const __grid_constant__ 
     st.prev_first_hsync_diff =
         hsync_diff_after(f, a.fmt, d_first, d_mll, prev_off_of(d_prev_read, d_read, d_mll), d_prev_loc);
     diff_due = false;
+  };
+  // a field anchored with this order and fit (from the per-field pass or a fit here)
+  auto anchored = [&](int f, long long readloc, bool first, const AnchorFit& fit, double mll, bool diff_lazy,
+                      double prev_off) {
+    a.is_first[f] = first ? 1 : 0;
+    if (!fit.used_prediction) {
+      if (diff_lazy) {
+        diff_due = true;
+        d_round = fit.loc_round;
+        d_mll = mll;
+        d_first = first;
+        d_prev_read = st.prev_first_hsync_readloc;
+        d_prev_loc = st.prev_first_hsync_loc;
+        d_read = readloc;
+      } else {
+        diff_due = false;
+        st.prev_first_hsync_diff = hsync_diff_after(fit, a.fmt, first, mll, prev_off, st.prev_first_hsync_loc);
+      }
+    }
+    st.prev_first_field = first ? 1 : 0;
+    st.prev_progressive_field = 0;
+    st.prev_first_hsync_readloc = readloc;
+    st.prev_first_hsync_loc = fit.loc;
   };
   if (t == 0) st = *a.state;
   if (P > 0) phase_clock(a, 0, 16);
@@ -1234,59 +1448,33 @@ __global__ void __launch_bounds__(kLT, 1) finish_kernel(const __grid_constant__ 
         for (; j < nb; j++) {
           const int f = b0 + j;
           const FieldPrep& p = preps[j];
-          const double prev_loc = st.prev_first_hsync_loc;
+          const long long readloc = readlocs[j];
           if (!(p.vn > 0 && p.mll > 0.0)) {
             a.is_first[f] = st.prev_first_field >= 0 ? (1 - st.prev_first_field) : 1;
             fallback[j] = 1;
             continue;
           }
-          if (p.exact) {
-            // fitted with this state by the per-field pass
+          if (p.exact) {  // fitted with this state by the per-field pass
             if (p.spec.cnt > 0) {
-              const bool first = p.exact_first != 0;
-              a.is_first[f] = first ? 1 : 0;
-              if (!p.spec.used_prediction) {
-                diff_due = true;
-                d_round = p.spec.loc_round;
-                d_mll = p.mll;
-                d_first = first;
-                d_prev_read = st.prev_first_hsync_readloc;
-                d_prev_loc = prev_loc;
-                d_read = readlocs[j];
-              }
-              st.prev_first_field = first ? 1 : 0;
-              st.prev_progressive_field = 0;
-              st.prev_first_hsync_readloc = readlocs[j];
-              st.prev_first_hsync_loc = p.spec.loc;
+              anchored(f, readloc, p.exact_first != 0, p.spec, p.mll, true, 0.0);
             } else {
               a.is_first[f] = st.prev_first_field >= 0 ? (1 - st.prev_first_field) : 1;
               fallback[j] = 1;
             }
             continue;
           }
+          const double prev_loc = st.prev_first_hsync_loc;
           const bool first = decide_first(p, st.prev_first_field, prev_loc, kAnchorConfidence);
           if (!(p.spec_first == (first ? 1 : 0) && prev_loc > 0.0)) {
             // fit this field: the previous state is final up to here
             settle_diff();
             fit_first = first;
-            prev_off_s = prev_off_of(st.prev_first_hsync_readloc, readlocs[j], p.mll);
+            prev_off_s = prev_off_of(st.prev_first_hsync_readloc, readloc, p.mll);
             prev_loc_s = prev_loc;
             prev_diff_s = st.prev_first_hsync_diff;
             break;
           }
-          // the speculative anchor stands
-          a.is_first[f] = first ? 1 : 0;
-          diff_due = true;
-          d_round = p.spec.loc_round;
-          d_mll = p.mll;
-          d_first = first;
-          d_prev_read = st.prev_first_hsync_readloc;
-          d_prev_loc = prev_loc;
-          d_read = readlocs[j];
-          st.prev_first_field = first ? 1 : 0;
-          st.prev_progressive_field = 0;
-          st.prev_first_hsync_readloc = readlocs[j];
-          st.prev_first_hsync_loc = p.spec.loc;
+          anchored(f, readloc, first, p.spec, p.mll, true, 0.0);  // the speculative anchor stands
         }
         fit_j = j;
       }
@@ -1314,14 +1502,7 @@ __global__ void __launch_bounds__(kLT, 1) finish_kernel(const __grid_constant__ 
       phase_clock(a, f, 19);
       if (t == 0) {
         if (fit.cnt > 0) {
-          const bool first = fit_first != 0;
-          a.is_first[f] = first ? 1 : 0;
-          st.prev_first_field = first ? 1 : 0;
-          st.prev_progressive_field = 0;
-          st.prev_first_hsync_readloc = readlocs[j];
-          st.prev_first_hsync_loc = fit.loc;
-          if (!fit.used_prediction)
-            st.prev_first_hsync_diff = hsync_diff_after(fit, a.fmt, first, p.mll, prev_off_s, prev_loc_s);
+          anchored(f, readlocs[j], fit_first != 0, fit, p.mll, false, prev_off_s);
         } else {
           a.is_first[f] = st.prev_first_field >= 0 ? (1 - st.prev_first_field) : 1;
           fallback[j] = 1;

@@ -299,6 +299,19 @@ void launch_chroma_lines_many(const ArgsMany<ChromaArgs>& p, int portions, int n
                               bool write_output, cudaStream_t st);
 void launch_burst_metric_many(const ArgsMany<ChromaArgs>& p, int portions, int max_fields, cudaStream_t st);
 
+// Track detection on the device (chroma_decode.cu:684-743): the burst
+// cancellation metric of both trial passes over field 0 (burst0: track 0,
+// burst1: track 1), summed in the host's order, picks the track with the
+// lower metric; track[f] for f < fields alternates from it, *pick = it.
+struct TrackPickArgs {
+  const float* burst0;
+  const float* burst1;
+  int out_h, burst_len, fields;
+  int* track;
+  int* pick;
+};
+void launch_track_pick(const TrackPickArgs& a, cudaStream_t st);
+
 struct DropoutArgs {
   const float* env;
   const double* env_part;

@@ -290,7 +290,46 @@ __global__ void __launch_bounds__(kMetricThreads) metric_kernel(const __grid_con
   if (lane == 0) a.metric[f] = npairs > 0 ? acc / npairs : 1e9;
 }
 
+// The trial passes' burst metrics: per trial, pair means (one thread each,
+// the window summed in sample order) added in line order by one thread, the
+// host restatement's operations in its order, so the pick is the host's.
+constexpr int kPickThreads = 256;
+__global__ void __launch_bounds__(kPickThreads) track_pick_kernel(const TrackPickArgs a) {
+  chain_wait();
+  __shared__ double pair_mean[2][kPickThreads];
+  __shared__ int det;
+  const int skip = 16, bl = a.burst_len;
+  int npairs = 0;
+  for (int line = skip; line < a.out_h - skip - 1; line += 2) npairs++;
+  npairs = min(npairs, kPickThreads);
+  for (int k = threadIdx.x; k < 2 * npairs; k += kPickThreads) {
+    const int t = k / npairs, p = k % npairs;
+    const float* x = (t ? a.burst1 : a.burst0) + (size_t)(skip + 2 * p) * bl;
+    const float* y = x + bl;
+    double s = 0.0;
+    for (int i = 0; i < bl; i++) s += fabs((double)x[i] + (double)y[i]);
+    pair_mean[t][p] = s / bl;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m[2];
+    for (int t = 0; t < 2; t++) {
+      double total = 0.0;
+      for (int p = 0; p < npairs; p++) total += pair_mean[t][p];
+      m[t] = npairs > 0 ? total / npairs : 1e9;
+    }
+    det = (m[1] < m[0]) ? 1 : 0;
+    *a.pick = det;
+  }
+  __syncthreads();
+  for (int f = threadIdx.x; f < a.fields; f += kPickThreads) a.track[f] = (f & 1) ? (1 - det) : det;
+}
+
 }  // namespace
+
+void launch_track_pick(const TrackPickArgs& a, cudaStream_t st) {
+  launch_chained(track_pick_kernel, dim3(1), dim3(kPickThreads), 0, st, a);
+}
 
 namespace {
 template <class S>

@@ -214,6 +214,10 @@ __device__ __forceinline__ void k1b_emit(const DemodArgs& a, const float2 (&z)[1
   float* video_out = a.video + out0;
   float* sync_out = a.sync + out0;
   const int lane = t & 31;
+  // slot q's 32 consecutive positions (one per lane) as an in-pulse word:
+  // lane q keeps slot q's ballot, and after the loop lanes 0..15 OR their
+  // words into the (at most two) bit words each straddles, in parallel
+  unsigned mine = 0;
 #pragma unroll
   for (int q = 0; q < 16; q++) {
     const int i = t + T * q - a.b_pos;
@@ -230,22 +234,19 @@ __device__ __forceinline__ void k1b_emit(const DemodArgs& a, const float2 (&z)[1
         }
       }
     }
-    if (a.pulse_bits) {
-      // the warp's 32 consecutive positions as one in-pulse word, ORed into
-      // the (at most two) words it straddles
-      unsigned m = __ballot_sync(0xffffffffu, in);
-      if (lane == 0 && m) {
-        long long p0 = (long long)out0 + (t - lane) + T * q - a.b_pos;
-        if (p0 < 0) {  // lanes before the chunk start hold no bits
-          m >>= (int)(-p0);
-          p0 = 0;
-        }
-        const long long w = p0 >> 5;
-        const int sh = (int)(p0 & 31);
-        atomicOr(&a.pulse_bits[w], m << sh);
-        if (sh && (m >> (32 - sh))) atomicOr(&a.pulse_bits[w + 1], m >> (32 - sh));
-      }
+    const unsigned m = __ballot_sync(0xffffffffu, in);
+    mine = lane == q ? m : mine;
+  }
+  if (a.pulse_bits && mine) {  // only lanes 0..15 hold a word
+    long long p0 = (long long)out0 + (t - lane) + (long long)T * lane - a.b_pos;
+    if (p0 < 0) {  // positions before the chunk start hold no bits
+      mine >>= (int)(-p0);
+      p0 = 0;
     }
+    const long long w = p0 >> 5;
+    const int sh = (int)(p0 & 31);
+    atomicOr(&a.pulse_bits[w], mine << sh);
+    if (sh && (mine >> (32 - sh))) atomicOr(&a.pulse_bits[w + 1], mine >> (32 - sh));
   }
 }
 

@@ -21,10 +21,38 @@ constexpr int kLumaThreads = 128;
 
 __device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(kFull, v, src); }
 
+// A line's sync samples: the window the refinement reads is staged in shared
+// memory (one coalesced burst per warp instead of a dependent global load per
+// scan step); a position outside the staged range reads global memory, so the
+// result never depends on the staging.
+struct SyncWindow {
+  const float* g;   // the chunk's sync signal
+  const float* sm;  // staged samples [lo, lo + n)
+  long long lo;
+  int n;
+  __device__ __forceinline__ float operator()(long long i) const {
+    const long long k = i - lo;
+    return (unsigned long long)k < (unsigned long long)n ? sm[k] : __ldg(g + i);
+  }
+};
+
+// Samples a line's refinement can read, relative to floor(line start): from
+// 2 us before (the second falling scan) to 3 hsync widths + 1 us after (the
+// rising scan, its re-centred porch median) or 10 us after (the falling
+// edge's porch median), with a margin for the integer truncations.  0 means
+// no staging (a window that would not fit the CTA's shared memory).
+constexpr int kHsyncWinMax = 2816;  // floats per warp: 4 warps in 44 KiB
+__host__ __device__ inline int hsync_lead(double us) { return 2 * (int)(us + 0.5) + 8; }
+__host__ __device__ inline int hsync_window(double us, double hw) {
+  const double tail = fmax(3.0 * hw + us, 10.0 * us + 1.0);
+  const int n = ((hsync_lead(us) + (int)ceil(tail) + 16) + 3) & ~3;
+  return n <= kHsyncWinMax ? n : 0;
+}
+
 // First sample pair (i-1, i) in [start, start+count) with prev >= target > cur;
 // returns the linearly interpolated crossing or -1.  The warp tests 32 pairs
 // per step and takes the lowest hit, so the result is the sequential scan's.
-__device__ double falling_cross(const float* __restrict__ s, int start, int count, double target, long long total,
+__device__ double falling_cross(const SyncWindow& s, int start, int count, double target, long long total,
                                 int lane) {
   if (start < 0 || (long long)start + count > total || count < 2) return -1.0;
   for (int base = start + 1; base < start + count; base += 32) {
@@ -32,8 +60,8 @@ __device__ double falling_cross(const float* __restrict__ s, int start, int coun
     double p = 0.0, q = 0.0;
     bool hit = false;
     if (i < start + count) {
-      p = s[i - 1];
-      q = s[i];
+      p = s(i - 1);
+      q = s(i);
       hit = p >= target && q < target;
     }
     const unsigned m = __ballot_sync(kFull, hit);
@@ -51,17 +79,17 @@ __device__ double falling_cross(const float* __restrict__ s, int start, int coun
   return -1.0;
 }
 
-__device__ double rising_cross(const float* __restrict__ s, int start, int count, double target, long long total,
+__device__ double rising_cross(const SyncWindow& s, int start, int count, double target, long long total,
                                int lane) {
   if (start < 0 || (long long)start + count > total || count < 2) return -1.0;
-  if ((double)s[start] > target) return -1.0;
+  if ((double)s(start) > target) return -1.0;
   for (int base = start + 1; base < start + count; base += 32) {
     const int i = base + lane;
     double p = 0.0, q = 0.0;
     bool hit = false;
     if (i < start + count) {
-      p = s[i - 1];
-      q = s[i];
+      p = s(i - 1);
+      q = s(i);
       hit = p < target && q >= target;
     }
     const unsigned m = __ballot_sync(kFull, hit);
@@ -94,11 +122,11 @@ __device__ __forceinline__ float bitonic_stage(float x, int e, int j, int k) {
 // elements l and l + 32), and element n/2 is read from its lane.  Ties hold
 // equal values, so the result is the window's order statistic whichever
 // duplicate lands there.
-__device__ double window_median(const float* __restrict__ s, int start, int count, long long total, int lane) {
+__device__ double window_median(const SyncWindow& s, int start, int count, long long total, int lane) {
   if (start < 0 || (long long)start + count > total || count <= 0) return 0.0;
   const int n = min(count, 64);
   const int mid = n / 2;
-  float x0 = lane < n ? s[start + lane] : INFINITY;
+  float x0 = lane < n ? s(start + lane) : INFINITY;
   if (n <= 32) {
 #pragma unroll
     for (int k = 2; k <= 32; k <<= 1)
@@ -106,7 +134,7 @@ __device__ double window_median(const float* __restrict__ s, int start, int coun
       for (int j = k >> 1; j > 0; j >>= 1) x0 = bitonic_stage(x0, lane, j, k);
     return (double)__shfl_sync(kFull, x0, mid);
   }
-  float x1 = lane + 32 < n ? s[start + lane + 32] : INFINITY;
+  float x1 = lane + 32 < n ? s(start + lane + 32) : INFINITY;
 #pragma unroll
   for (int k = 2; k <= 64; k <<= 1) {
 #pragma unroll
@@ -125,21 +153,40 @@ __device__ double window_median(const float* __restrict__ s, int start, int coun
 }
 
 // One warp per line location (lines from the first active line to the end of
-// the frame table).
+// the frame table).  The warp first stages the line's sync window.
 template <class Src>
 __global__ void __launch_bounds__(32 * kHsyncWarps) hsync_kernel(const __grid_constant__ Src src) {
   const LineArgs& a = src.get();
+  extern __shared__ __align__(16) float hs_win[];
   chain_wait();
   const int lane = threadIdx.x & 31;
   const int idx = blockIdx.x * kHsyncWarps + (threadIdx.x >> 5);
   if (idx >= a.fields * a.lines_per_frame) return;  // whole warp
   const int line = idx % a.lines_per_frame;
   if (line < a.active_line_start) return;
-  const float* s = a.sync;
   const double thr = (double)a.thr_rel;
   const double us = a.one_us, hw = a.hsync_width;
   const double orig = a.ll[idx];
   const int ou = (int)(us + 0.5);
+  const int nw = hsync_window(us, hw);
+  SyncWindow s{a.sync, hs_win + (threadIdx.x >> 5) * nw, 0, 0};
+  if (nw > 0 && orig > -1e15 && orig < 1e15) {
+    long long lo = ((long long)floor(orig) - hsync_lead(us)) & ~3LL;
+    long long hi = min(lo + nw, a.total);
+    if (lo < 0) lo = 0;
+    if (hi > lo) {
+      const int n = (int)(hi - lo);
+      float* w = const_cast<float*>(s.sm);
+      const bool vec = (reinterpret_cast<uintptr_t>(a.sync) & 15) == 0;
+      const int n4 = vec ? n >> 2 : 0;
+      const float4* g4 = reinterpret_cast<const float4*>(a.sync + lo);
+      for (int k = lane; k < n4; k += 32) reinterpret_cast<float4*>(w)[k] = __ldg(g4 + k);
+      for (int k = 4 * n4 + lane; k < n; k += 32) w[k] = __ldg(a.sync + lo + k);
+      s.lo = lo;
+      s.n = n;
+    }
+    __syncwarp();
+  }
   // leading (falling) edge
   const double zc = falling_cross(s, (int)(orig - ou), ou * 2, thr, a.total, lane);
   double left = -1.0;
@@ -269,7 +316,8 @@ void launch_hsync_refine(const LineArgs& a, cudaStream_t st) {
   const int n = a.fields * a.lines_per_frame;
   if (n <= 0) return;
   using S = ArgsOne<LineArgs>;
-  launch_chained(hsync_kernel<S>, dim3((n + kHsyncWarps - 1) / kHsyncWarps), dim3(32 * kHsyncWarps), 0, st, S{a});
+  const size_t smem = (size_t)kHsyncWarps * hsync_window(a.one_us, a.hsync_width) * sizeof(float);
+  launch_chained(hsync_kernel<S>, dim3((n + kHsyncWarps - 1) / kHsyncWarps), dim3(32 * kHsyncWarps), smem, st, S{a});
 }
 
 void launch_luma(const LineArgs& a, cudaStream_t st) {
@@ -282,8 +330,9 @@ void launch_luma(const LineArgs& a, cudaStream_t st) {
 void launch_hsync_refine_many(const ArgsMany<LineArgs>& p, int portions, int max_fields, cudaStream_t st) {
   const int n = max_fields * p.a[0].lines_per_frame;
   if (n <= 0 || portions <= 0) return;
+  const size_t smem = (size_t)kHsyncWarps * hsync_window(p.a[0].one_us, p.a[0].hsync_width) * sizeof(float);
   launch_chained(hsync_kernel<ArgsMany<LineArgs>>, dim3((n + kHsyncWarps - 1) / kHsyncWarps, 1, portions),
-                 dim3(32 * kHsyncWarps), 0, st, p);
+                 dim3(32 * kHsyncWarps), smem, st, p);
 }
 
 void launch_luma_many(const ArgsMany<LineArgs>& p, int portions, int max_fields, cudaStream_t st) {

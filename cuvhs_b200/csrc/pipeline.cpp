@@ -144,7 +144,7 @@ void Context::release() {
   hstream = nullptr;
   if (pstream) cudaStreamDestroy(pstream);
   pstream = nullptr;
-  for (cudaEvent_t* e : {&ev_ll, &ev_win, &ev_winhost, &ev_k1b, &ev_pre, &ev_guard}) {
+  for (cudaEvent_t* e : {&ev_ll, &ev_win, &ev_winhost, &ev_k1b, &ev_pre, &ev_guard, &ev_hs, &ev_trial}) {
     if (*e) cudaEventDestroy(*e);
     *e = nullptr;
   }
@@ -208,6 +208,9 @@ bool Context::alloc_buffers() {
   d_chroma = d_chroma_set[0];
   d_burst = A((float*)nullptr, (size_t)batch * fmt.output_field_lines * fmt.burst_len);
   d_track = A((int*)nullptr, batch);
+  d_trial = A((int*)nullptr, 2);
+  d_burst_trial = A((float*)nullptr, (size_t)2 * fmt.output_field_lines * fmt.burst_len);
+  d_pick = A((int*)nullptr, 1);
   d_do_count = A((int*)nullptr, batch);
   d_do_lines = A((int*)nullptr, (size_t)batch * kMaxDropouts);
   d_do_starts = A((int*)nullptr, (size_t)batch * kMaxDropouts);
@@ -283,6 +286,7 @@ bool Context::alloc_buffers() {
   hp_guard = H((int*)nullptr, 2 * kMaxPortions);
   hp_track = H((int*)nullptr, batch);
   hp_trial = H((int*)nullptr, 2);
+  hp_pick = H((int*)nullptr, 1);
   hp_burst = H((float*)nullptr, (size_t)2 * fmt.output_field_lines * fmt.burst_len);
   {
     void* p = nullptr;
@@ -415,6 +419,12 @@ bool Context::init(const cuvhs_config& c) {
   }
   hp_trial[0] = 0;
   hp_trial[1] = 1;
+  if (cudaMemcpy(d_trial, hp_trial, 2 * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+    err = "trial track upload failed";
+    status = CUVHS_ERR_CUDA;
+    release();
+    return false;
+  }
   bool ev_ok = cudaEventCreateWithFlags(&ev_host, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_luma, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_edges, cudaEventDisableTiming) == cudaSuccess &&
@@ -423,6 +433,8 @@ bool Context::init(const cuvhs_config& c) {
                cudaEventCreateWithFlags(&ev_winhost, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_k1b, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_pre, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev_hs, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev_trial, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_guard, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t* e : {&ev_prefetch, &ev_small, &ev_chroma, &ev_out_done[0], &ev_out_done[1]})
     ev_ok = ev_ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
@@ -809,7 +821,8 @@ bool Context::write_lls(const LineLocState& st) {
 // from two trial passes over field 0; then every field is computed with the
 // alternating track assignment and the reference's per-15-field flip-and-retry
 // passes are replayed on the host.  Sets h_phase and the carried chroma state.
-bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, uint16_t* dst_chroma) {
+bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, uint16_t* dst_chroma,
+                            bool trial_on_device) {
   const int H = fmt.output_field_lines;
   const size_t F = (size_t)fmt.output_line_len * H;
   double t_host = 0.0;
@@ -843,10 +856,35 @@ bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, u
   };
   int det_track, cycle_start;
   double thr;
+  const bool on_device = trial_on_device && !chroma_valid;
+  const size_t nb_ = (size_t)H * fmt.burst_len;
+  auto detect = [&](int& det, double& th, int& cyc) {
+    const double m0 = host_burst_metric(hp_burst, H, fmt.burst_len),
+                 m1 = host_burst_metric(hp_burst + nb_, H, fmt.burst_len);
+    det = (m1 < m0) ? 1 : 0;
+    th = (det ? m1 : m0) * 4.0;
+    const double ph = host_burst_phase(hp_burst + det * nb_, H, fmt);
+    const int quadrant = ((int)(ph / 90.0 + 0.5)) % 4;
+    const int pid = phase_id_for(1, quadrant);
+    cyc = 0;
+    for (int i = 0; i < 8; i += 2)
+      if (kPhaseCycle[i] == pid) {
+        cyc = i;
+        break;
+      }
+  };
   if (chroma_valid) {
     det_track = chroma_track;
     thr = chroma_threshold;
     cycle_start = chroma_cycle_start;
+  } else if (on_device) {
+    // the trials and the device pick ran beside luma and dropouts; the pass
+    // over every field follows the pick without a host round trip, and the
+    // host's own decision from the same windows is taken after it (fields
+    // computed on another track are recomputed below)
+    cudaStreamWaitEvent(stream, ev_trial, 0);
+    det_track = cycle_start = 0;
+    thr = 0.0;
   } else {
     // Track and burst phase from field 0 (chroma_decode.cu:684-743): both
     // trial tracks in one round trip; the detected track's burst windows are
@@ -861,38 +899,37 @@ bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, u
     t_host = host_clock();
     if (!wait_host_event("chroma track detect")) return false;
     host_phase(kHostChromaWait, t_host);
-    const double m0 = host_burst_metric(hp_burst, H, fmt.burst_len), m1 = host_burst_metric(hp_burst + nb, H, fmt.burst_len);
-    det_track = (m1 < m0) ? 1 : 0;
-    thr = (det_track ? m1 : m0) * 4.0;
-    const double ph = host_burst_phase(hp_burst + det_track * nb, H, fmt);
-    const int quadrant = ((int)(ph / 90.0 + 0.5)) % 4;
-    const int pid = phase_id_for(1, quadrant);
-    cycle_start = 0;
-    for (int i = 0; i < 8; i += 2)
-      if (kPhaseCycle[i] == pid) {
-        cycle_start = i;
-        break;
-      }
-  }
-  int cur = det_track;
-  h_phase.assign(P, 0);
-  for (int f = 0; f < P; f++) {
-    hp_track[f] = (f & 1) ? (1 - cur) : cur;
-    h_phase[f] = kPhaseCycle[(cycle_start + f) % 8];
+    detect(det_track, thr, cycle_start);
   }
   // Every field's chroma depends only on its own track, so all fields are
   // computed in one pass with the initial assignment; the reference's
   // 15-field chunks with up to three flip-and-retry passes each
   // (chroma_decode.cu:782-981) are then replayed on the host, recomputing
   // only fields whose track a flip changed.
-  computed_track.assign(hp_track, hp_track + P);
-  cudaMemcpyAsync(d_track, hp_track, P * sizeof(int), cudaMemcpyHostToDevice, stream);
+  if (!on_device) {
+    for (int f = 0; f < P; f++) hp_track[f] = (f & 1) ? (1 - det_track) : det_track;
+    cudaMemcpyAsync(d_track, hp_track, P * sizeof(int), cudaMemcpyHostToDevice, stream);
+  }
   chroma_pass(0, P, true);
   cudaEventRecord(ev_host, stream);
   finish(0, P);
   t_host = host_clock();
   if (!wait_host_event("chroma lines")) return false;
   host_phase(kHostChromaWait, t_host);
+  computed_track.resize(P);
+  if (on_device) {
+    // the trial windows and the device's pick arrived before the pass
+    detect(det_track, thr, cycle_start);
+    const int dev = *hp_pick;
+    for (int f = 0; f < P; f++) computed_track[f] = (f & 1) ? (1 - dev) : dev;
+  }
+  int cur = det_track;
+  h_phase.assign(P, 0);
+  for (int f = 0; f < P; f++) {
+    hp_track[f] = (f & 1) ? (1 - cur) : cur;
+    h_phase[f] = kPhaseCycle[(cycle_start + f) % 8];
+    if (!on_device) computed_track[f] = hp_track[f];
+  }
   const int fpc = std::max(1, std::min((4096 / H), P));
   for (int f0 = 0; f0 < P; f0 += fpc) {
     const int nf = std::min(fpc, P - f0);
@@ -1259,6 +1296,40 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     launch_hsync_refine(la, stream);
     end_stage(kStageHsync, ev_);
   }
+  // ---- chroma track detection of a chunk without carried chroma state
+  // (chroma_decode.cu:684-743): both trial passes over field 0 in one launch
+  // and the device pick, on the pre-band-pass stream (they need its output
+  // and field 0's refined line starts), beside luma and dropouts
+  const bool trial_on_device = !chroma_valid;
+  if (trial_on_device) {
+    cudaEventRecord(ev_hs, stream);
+    cudaStreamWaitEvent(pstream, ev_hs, 0);
+    const size_t nb = (size_t)H * fmt.burst_len;
+    ArgsMany<ChromaArgs> tm;
+    for (int t = 0; t < 2; t++) {
+      tm.a[t] = ca;
+      tm.a[t].fields = 1;
+      tm.a[t].total = (long long)P * spp;  // the full pass's signal range
+      tm.a[t].track = d_trial + t;
+      tm.a[t].burst = d_burst_trial + t * nb;
+    }
+    cudaEvent_t ev_;
+    begin_stage_on(kStageChromaLines, ev_, pstream);
+    launch_chroma_lines_many(tm, 2, -1, 1, false, pstream);
+    end_stage_on(kStageChromaLines, ev_, pstream);
+    TrackPickArgs tp;
+    tp.burst0 = d_burst_trial;
+    tp.burst1 = d_burst_trial + nb;
+    tp.out_h = H;
+    tp.burst_len = fmt.burst_len;
+    tp.fields = P;
+    tp.track = d_track;
+    tp.pick = d_pick;
+    launch_track_pick(tp, pstream);
+    cudaMemcpyAsync(hp_burst, d_burst_trial, 2 * nb * sizeof(float), cudaMemcpyDeviceToHost, pstream);
+    cudaMemcpyAsync(hp_pick, d_pick, sizeof(int), cudaMemcpyDeviceToHost, pstream);
+    cudaEventRecord(ev_trial, pstream);
+  }
   {
     cudaEvent_t ev_;
     begin_stage(kStageLuma, ev_);
@@ -1297,7 +1368,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   ca.total = (long long)P * spp;
   // the chroma is concealed and sent as it is decoded (chroma_fields)
   cudaStreamWaitEvent(stream, ev_pre, 0);
-  if (!chroma_fields(ca, P, &dd, dst_chroma)) return false;
+  if (!chroma_fields(ca, P, &dd, dst_chroma, trial_on_device)) return false;
   if (!check_cuda("chroma concealment")) return false;
   cudaEventRecord(ev_out_done[oset], ostream);
   if (debug) {

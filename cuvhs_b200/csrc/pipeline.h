@@ -129,6 +129,15 @@ struct Context {
   // the corrected sync (rare), from the line-location state saved before.
   cudaStream_t gstream = nullptr;
   cudaEvent_t ev_guard = nullptr;
+  // Chroma track detection of a chunk without carried chroma state: both
+  // trial passes over field 0 (one launch) and the device pick follow the
+  // hsync refinement on the pre-band-pass stream, beside luma and dropouts;
+  // ev_trial marks the pick (d_track set, the trial windows in hp_burst).
+  cudaEvent_t ev_hs = nullptr, ev_trial = nullptr;
+  int* d_trial = nullptr;        // {0, 1}: the trial tracks
+  float* d_burst_trial = nullptr;  // [2][out_h * burst_len]
+  int* d_pick = nullptr;
+  int* hp_pick = nullptr;
   uint8_t* d_raw_set[2] = {};
   uint16_t* d_luma_set[2] = {};
   uint16_t* d_chroma_set[2] = {};
@@ -303,7 +312,10 @@ struct Context {
   // track/phase decisions and the carried chroma state; sets h_phase.  With
   // `conceal`, fields are concealed as they are decoded; with dst_chroma (page
   // -locked host planes), sent there on the copy stream as well.
-  bool chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal = nullptr, uint16_t* dst_chroma = nullptr);
+  // trial_on_device: the trial passes and the device pick were enqueued
+  // (ev_trial) for a context without carried chroma state.
+  bool chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal = nullptr, uint16_t* dst_chroma = nullptr,
+                     bool trial_on_device = false);
   // Sync edges of `sync` over [0, total) and the field windows clustered
   // from them (at most num_fields), read back into hp_win / hp_offs
   // (synchronous).

@@ -144,7 +144,7 @@ void Context::release() {
   hstream = nullptr;
   if (pstream) cudaStreamDestroy(pstream);
   pstream = nullptr;
-  for (cudaEvent_t* e : {&ev_ll, &ev_win, &ev_winhost, &ev_k1b, &ev_pre, &ev_guard, &ev_hs, &ev_trial}) {
+  for (cudaEvent_t* e : {&ev_ll, &ev_win, &ev_winhost, &ev_k1b, &ev_pre, &ev_guard, &ev_hs, &ev_trial, &ev_cpass}) {
     if (*e) cudaEventDestroy(*e);
     *e = nullptr;
   }
@@ -395,7 +395,7 @@ bool Context::init(const cuvhs_config& c) {
       cudaStreamCreateWithFlags(&ostream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&hstream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithPriority(&lstream, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&pstream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&pstream, cudaStreamNonBlocking, (prio_low + prio_high) / 2) != cudaSuccess ||
       cudaStreamCreateWithPriority(&gstream, cudaStreamNonBlocking, prio_high) != cudaSuccess) {
     err = "cudaStreamCreate failed";
     status = CUVHS_ERR_CUDA;
@@ -435,6 +435,7 @@ bool Context::init(const cuvhs_config& c) {
                cudaEventCreateWithFlags(&ev_pre, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_hs, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_trial, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev_cpass, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_guard, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t* e : {&ev_prefetch, &ev_small, &ev_chroma, &ev_out_done[0], &ev_out_done[1]})
     ev_ok = ev_ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
@@ -822,7 +823,10 @@ bool Context::write_lls(const LineLocState& st) {
 // alternating track assignment and the reference's per-15-field flip-and-retry
 // passes are replayed on the host.  Sets h_phase and the carried chroma state.
 bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, uint16_t* dst_chroma,
-                            bool trial_on_device) {
+                            bool trial_on_device, cudaStream_t chroma_stream) {
+  // the chroma passes run on cs; the concealment (which needs the dropout
+  // lists of the decode stream) follows each pass on the decode stream
+  cudaStream_t cs = chroma_stream ? chroma_stream : stream;
   const int H = fmt.output_field_lines;
   const size_t F = (size_t)fmt.output_line_len * H;
   double t_host = 0.0;
@@ -830,6 +834,10 @@ bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, u
   // leave them: conceal and send them now; a retry pass that rewrites fields
   // repeats this for them (concealment only ever runs on freshly decoded lines).
   auto finish = [&](int f0, int nf) {
+    if (cs != stream) {
+      cudaEventRecord(ev_cpass, cs);
+      cudaStreamWaitEvent(stream, ev_cpass, 0);
+    }
     if (conceal) {
       cudaEvent_t ev_;
       begin_stage(kStageDropouts, ev_);
@@ -845,13 +853,13 @@ bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, u
   };
   auto chroma_pass = [&](int f0, int nf, bool write) {
     cudaEvent_t ev_;
-    begin_stage(kStageChromaLines, ev_);
-    launch_chroma_lines(ca, f0, nf, write, stream);
-    end_stage(kStageChromaLines, ev_);
+    begin_stage_on(kStageChromaLines, ev_, cs);
+    launch_chroma_lines(ca, f0, nf, write, cs);
+    end_stage_on(kStageChromaLines, ev_, cs);
     if (write) {
-      begin_stage(kStageBurstMetric, ev_);
-      launch_burst_metric(ca, f0, nf, stream);  // writes hp_metric through its mapping
-      end_stage(kStageBurstMetric, ev_);
+      begin_stage_on(kStageBurstMetric, ev_, cs);
+      launch_burst_metric(ca, f0, nf, cs);  // writes hp_metric through its mapping
+      end_stage_on(kStageBurstMetric, ev_, cs);
     }
   };
   int det_track, cycle_start;
@@ -882,7 +890,7 @@ bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, u
     // over every field follows the pick without a host round trip, and the
     // host's own decision from the same windows is taken after it (fields
     // computed on another track are recomputed below)
-    cudaStreamWaitEvent(stream, ev_trial, 0);
+    cudaStreamWaitEvent(cs, ev_trial, 0);
     det_track = cycle_start = 0;
     thr = 0.0;
   } else {
@@ -891,11 +899,11 @@ bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, u
     // the ones the phase measurement reads.
     const size_t nb = (size_t)H * fmt.burst_len;
     for (int t = 0; t < 2; t++) {
-      cudaMemcpyAsync(d_track, hp_trial + t, sizeof(int), cudaMemcpyHostToDevice, stream);
+      cudaMemcpyAsync(d_track, hp_trial + t, sizeof(int), cudaMemcpyHostToDevice, cs);
       chroma_pass(0, 1, false);
-      cudaMemcpyAsync(hp_burst + t * nb, d_burst, nb * sizeof(float), cudaMemcpyDeviceToHost, stream);
+      cudaMemcpyAsync(hp_burst + t * nb, d_burst, nb * sizeof(float), cudaMemcpyDeviceToHost, cs);
     }
-    cudaEventRecord(ev_host, stream);
+    cudaEventRecord(ev_host, cs);
     t_host = host_clock();
     if (!wait_host_event("chroma track detect")) return false;
     host_phase(kHostChromaWait, t_host);
@@ -908,10 +916,10 @@ bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, u
   // only fields whose track a flip changed.
   if (!on_device) {
     for (int f = 0; f < P; f++) hp_track[f] = (f & 1) ? (1 - det_track) : det_track;
-    cudaMemcpyAsync(d_track, hp_track, P * sizeof(int), cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(d_track, hp_track, P * sizeof(int), cudaMemcpyHostToDevice, cs);
   }
   chroma_pass(0, P, true);
-  cudaEventRecord(ev_host, stream);
+  cudaEventRecord(ev_host, cs);
   finish(0, P);
   t_host = host_clock();
   if (!wait_host_event("chroma lines")) return false;
@@ -939,9 +947,9 @@ bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, u
       bool stale = false;
       for (int f = f0; f < f0 + nf; f++) stale = stale || computed_track[f] != hp_track[f];
       if (stale) {
-        cudaMemcpyAsync(d_track + f0, hp_track + f0, nf * sizeof(int), cudaMemcpyHostToDevice, stream);
+        cudaMemcpyAsync(d_track + f0, hp_track + f0, nf * sizeof(int), cudaMemcpyHostToDevice, cs);
         chroma_pass(f0, nf, true);
-        cudaEventRecord(ev_host, stream);
+        cudaEventRecord(ev_host, cs);
         finish(f0, nf);
         if (!wait_host_event("chroma retry")) return false;
         for (int f = f0; f < f0 + nf; f++) computed_track[f] = hp_track[f];
@@ -1300,10 +1308,11 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   // (chroma_decode.cu:684-743): both trial passes over field 0 in one launch
   // and the device pick, on the pre-band-pass stream (they need its output
   // and field 0's refined line starts), beside luma and dropouts
+  // (the chroma passes follow on the same stream, after the refinement)
+  cudaEventRecord(ev_hs, stream);
+  cudaStreamWaitEvent(pstream, ev_hs, 0);
   const bool trial_on_device = !chroma_valid;
   if (trial_on_device) {
-    cudaEventRecord(ev_hs, stream);
-    cudaStreamWaitEvent(pstream, ev_hs, 0);
     const size_t nb = (size_t)H * fmt.burst_len;
     ArgsMany<ChromaArgs> tm;
     for (int t = 0; t < 2; t++) {
@@ -1366,9 +1375,9 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
   // ---- K6 chroma on the P detected fields
   ca.fields = P;
   ca.total = (long long)P * spp;
-  // the chroma is concealed and sent as it is decoded (chroma_fields)
-  cudaStreamWaitEvent(stream, ev_pre, 0);
-  if (!chroma_fields(ca, P, &dd, dst_chroma, trial_on_device)) return false;
+  // the chroma lines run on the pre-band-pass stream beside luma and
+  // dropouts; each pass is concealed and sent as it is decoded (chroma_fields)
+  if (!chroma_fields(ca, P, &dd, dst_chroma, trial_on_device, pstream)) return false;
   if (!check_cuda("chroma concealment")) return false;
   cudaEventRecord(ev_out_done[oset], ostream);
   if (debug) {

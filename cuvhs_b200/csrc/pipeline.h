@@ -134,6 +134,7 @@ struct Context {
   // hsync refinement on the pre-band-pass stream, beside luma and dropouts;
   // ev_trial marks the pick (d_track set, the trial windows in hp_burst).
   cudaEvent_t ev_hs = nullptr, ev_trial = nullptr;
+  cudaEvent_t ev_cpass = nullptr;  // a chroma pass on its stream, before its concealment
   int* d_trial = nullptr;        // {0, 1}: the trial tracks
   float* d_burst_trial = nullptr;  // [2][out_h * burst_len]
   int* d_pick = nullptr;
@@ -314,8 +315,10 @@ struct Context {
   // -locked host planes), sent there on the copy stream as well.
   // trial_on_device: the trial passes and the device pick were enqueued
   // (ev_trial) for a context without carried chroma state.
+  // chroma_stream: the stream of the chroma passes (nullptr: the decode
+  // stream); it must already follow the hsync refinement and the pre-band-pass.
   bool chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal = nullptr, uint16_t* dst_chroma = nullptr,
-                     bool trial_on_device = false);
+                     bool trial_on_device = false, cudaStream_t chroma_stream = nullptr);
   // Sync edges of `sync` over [0, total) and the field windows clustered
   // from them (at most num_fields), read back into hp_win / hp_offs
   // (synchronous).

@@ -311,22 +311,12 @@ def profile_case():
     return 0
 
 
-def run_batched(args, rank, world, local):
-    """Config 3: 64 independent captures (2-240 fields, 28 / 35.8 / 40 MHz,
-    30-45 dB, 0-0.5% dropout lines) decoded through cuvhs_batch_decode (batched
-    rounds: each stage one launch over up to 64 captures' chunks, round size
-    from the autotuner) from page-locked host memory, against the same captures
-    decoded one at a time (cuvhs_decode_capture per capture on a fresh state,
-    one context per rate, the same page-locked buffers).  Each step decodes the
-    whole set; under torchrun the captures are split across ranks (strong
-    scaling).  Both numbers are end to end (host->device copies of the
-    captures and device->host copies of the TBC planes inside)."""
+def batched_pair(steps, warmup, lanes, rank, world, local):
+    """The 64-capture set (or this rank's share) decoded one at a time and
+    batched; returns (one-at-a-time fields/s, its ms per step, batched fields/s,
+    its ms per step, lanes, fields per step over all ranks, round sizes)."""
     import torch
     import torch.distributed as dist
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     import cuvhs_b200 as cv
     specs = cv.batch_specs(64)[rank::world]
     caps = [(cv.synth_capture(**kw), kw["sample_rate_hz"] / 1e6) for kw in specs]
@@ -362,17 +352,17 @@ def run_batched(args, rank, world, local):
 
     def measure(batched):
         nonlocal fields_per_step
-        with cv.Batch(lanes=args.lanes, device=local) as b:
+        with cv.Batch(lanes=lanes, device=local) as b:
             items, keep = b.prepare(caps, pinned=True)
             gen = one_at_a_time(b, items) if not batched else None
             run = next(gen) if gen else b.run
-            for _ in range(args.warmup):
+            for _ in range(warmup):
                 run(items)
             if world > 1:
                 dist.barrier()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            for _ in range(args.steps):
+            for _ in range(steps):
                 run(items)
             torch.cuda.synchronize()
             dt = time.perf_counter() - t0
@@ -389,18 +379,42 @@ def run_batched(args, rank, world, local):
             total = float(f[0])
         else:
             total = float(fields_per_step)
-        return total * args.steps / float(t[0]), float(t[0]) / args.steps * 1e3, used, total, rounds
+        return total * steps / float(t[0]), float(t[0]) / steps * 1e3, used, total, rounds
 
     single, single_ms, _, _, _ = measure(False)
-    batched, batched_ms, lanes, total, rounds = measure(True)
+    batched, batched_ms, used, total, rounds = measure(True)
+    return single, single_ms, batched, batched_ms, used, total, rounds
+
+
+BATCHED_DESC = ("64 captures of 2-240 fields at 28/35.8/40 MHz u8, 30-45 dB, "
+                "+/-0.5-2 sample jitter, 0-0.5% dropout lines (seeded)")
+
+
+def run_batched(args, rank, world, local):
+    """Config 3: 64 independent captures (2-240 fields, 28 / 35.8 / 40 MHz,
+    30-45 dB, 0-0.5% dropout lines) decoded through cuvhs_batch_decode (batched
+    rounds: each stage one launch over up to 64 captures' chunks, round size
+    from the autotuner) from page-locked host memory, against the same captures
+    decoded one at a time (cuvhs_decode_capture per capture on a fresh state,
+    one context per rate, the same page-locked buffers).  Each step decodes the
+    whole set; under torchrun the captures are split across ranks (strong
+    scaling).  Both numbers are end to end (host->device copies of the
+    captures and device->host copies of the TBC planes inside)."""
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    single, single_ms, batched, batched_ms, lanes, total, rounds = batched_pair(
+        args.steps, args.warmup, args.lanes, rank, world, local)
     if rank == 0:
         print(json.dumps({
             "metric": "NTSC fields/s, 64 mixed synthetic captures (28/35.8/40 MHz u8), batched decode",
             "value": round(batched, 2), "unit": "fields/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(batched_ms, 3), "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "64 captures of 2-240 fields at 28/35.8/40 MHz u8, 30-45 dB, "
-                                   "+/-0.5-2 sample jitter, 0-0.5% dropout lines (seeded)",
+            "config": {"workload": BATCHED_DESC,
                        "fields_per_step": int(total), "lanes": lanes, "io": "pinned host memory, e2e",
                        "round_fields": {str(k): v for k, v in rounds.items()}},
             "single_capture": {"value": round(single, 2), "unit": "fields/s", "ms_per_step": round(single_ms, 3),
@@ -598,6 +612,8 @@ def main():
     ap.add_argument("--stream-fields", type=int, default=36000,
                     help="stream40: fields in the capture (36,000: ten minutes at 40 MHz, 2.4e10 samples)")
     ap.add_argument("--lanes", type=int, default=0, help="batched64: concurrent decoders (0 = library default)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="plain40_28: skip the 64-capture batched measurement added to the line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.workload == "hard600_40":
@@ -787,6 +803,22 @@ def main():
             line["cpu_baseline"] = cpu_baseline()
         if WORKLOAD == "hard600_40" and world == 1 and not args.no_fp64_report:
             line["fp32_vs_fp64"] = fp64_report(WORKLOAD, mhz)
+        if WORKLOAD == "plain40_28" and world == 1 and not args.no_batched:
+            # the batched configuration beside the headline: the 64-capture
+            # set end to end, batched and one capture at a time
+            t_b = time.perf_counter()
+            single, single_ms, batched, batched_ms, lanes, total, rounds = batched_pair(
+                3, 3, args.lanes, 0, 1, local)
+            line["batched64"] = {
+                "value": round(batched, 2), "unit": "fields/s", "ms_per_step": round(batched_ms, 3),
+                "steps": 3, "warmup": 3, "workload": BATCHED_DESC, "fields_per_step": int(total),
+                "lanes": lanes, "round_fields": {str(k): v for k, v in rounds.items()},
+                "io": "pinned host memory, e2e (H2D and D2H inside)",
+                "single_capture": {"value": round(single, 2), "unit": "fields/s",
+                                   "ms_per_step": round(single_ms, 3),
+                                   "how": "the same captures one at a time (cuvhs_decode_capture, fresh state)"},
+                "batched_over_single": round(batched / single, 3),
+                "seconds_incl_synthesis": round(time.perf_counter() - t_b, 1)}
         print(json.dumps(line))
     dec.close()
     if world > 1:

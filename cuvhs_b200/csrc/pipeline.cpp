@@ -144,7 +144,7 @@ void Context::release() {
   hstream = nullptr;
   if (pstream) cudaStreamDestroy(pstream);
   pstream = nullptr;
-  for (cudaEvent_t* e : {&ev_ll, &ev_win, &ev_winhost, &ev_k1b, &ev_pre, &ev_guard, &ev_hs, &ev_trial, &ev_cpass}) {
+  for (cudaEvent_t* e : {&ev_ll, &ev_win, &ev_winhost, &ev_k1b, &ev_pre, &ev_guard, &ev_hs, &ev_trial, &ev_trialh, &ev_cpass}) {
     if (*e) cudaEventDestroy(*e);
     *e = nullptr;
   }
@@ -435,6 +435,7 @@ bool Context::init(const cuvhs_config& c) {
                cudaEventCreateWithFlags(&ev_pre, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_hs, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_trial, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&ev_trialh, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_cpass, cudaEventDisableTiming) == cudaSuccess &&
                cudaEventCreateWithFlags(&ev_guard, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t* e : {&ev_prefetch, &ev_small, &ev_chroma, &ev_out_done[0], &ev_out_done[1]})
@@ -926,7 +927,13 @@ bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, u
   host_phase(kHostChromaWait, t_host);
   computed_track.resize(P);
   if (on_device) {
-    // the trial windows and the device's pick arrived before the pass
+    // the trial windows and the device's pick (copied after the pick)
+    const cudaError_t e = cudaEventSynchronize(ev_trialh);
+    if (e != cudaSuccess) {
+      err = std::string("chroma track windows: ") + cudaGetErrorString(e);
+      status = CUVHS_ERR_CUDA;
+      return false;
+    }
     detect(det_track, thr, cycle_start);
     const int dev = *hp_pick;
     for (int f = 0; f < P; f++) computed_track[f] = (f & 1) ? (1 - dev) : dev;
@@ -1335,9 +1342,13 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     tp.track = d_track;
     tp.pick = d_pick;
     launch_track_pick(tp, pstream);
-    cudaMemcpyAsync(hp_burst, d_burst_trial, 2 * nb * sizeof(float), cudaMemcpyDeviceToHost, pstream);
-    cudaMemcpyAsync(hp_pick, d_pick, sizeof(int), cudaMemcpyDeviceToHost, pstream);
     cudaEventRecord(ev_trial, pstream);
+    // the windows and the pick go to the host on the copy stream, so that
+    // the chroma pass follows the pick directly
+    cudaStreamWaitEvent(xstream, ev_trial, 0);
+    cudaMemcpyAsync(hp_burst, d_burst_trial, 2 * nb * sizeof(float), cudaMemcpyDeviceToHost, xstream);
+    cudaMemcpyAsync(hp_pick, d_pick, sizeof(int), cudaMemcpyDeviceToHost, xstream);
+    cudaEventRecord(ev_trialh, xstream);
   }
   {
     cudaEvent_t ev_;

@@ -132,8 +132,9 @@ struct Context {
   // Chroma track detection of a chunk without carried chroma state: both
   // trial passes over field 0 (one launch) and the device pick follow the
   // hsync refinement on the pre-band-pass stream, beside luma and dropouts;
-  // ev_trial marks the pick (d_track set, the trial windows in hp_burst).
-  cudaEvent_t ev_hs = nullptr, ev_trial = nullptr;
+  // ev_trial marks the pick (d_track set), ev_trialh the trial windows and the
+  // pick in hp_burst / hp_pick.
+  cudaEvent_t ev_hs = nullptr, ev_trial = nullptr, ev_trialh = nullptr;  // ev_trialh: the copies to the host
   cudaEvent_t ev_cpass = nullptr;  // a chroma pass on its stream, before its concealment
   int* d_trial = nullptr;        // {0, 1}: the trial tracks
   float* d_burst_trial = nullptr;  // [2][out_h * burst_len]

@@ -1301,22 +1301,23 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     res.fields = 0;
     return true;
   }
-  cudaStreamWaitEvent(stream, ev_ll, 0);
-  cudaStreamWaitEvent(stream, ev_guard, 0);
-  // ---- K4 hsync refinement, K5 luma
+  // ---- K4 hsync refinement on the line stream after the line locations (it
+  // gates the chroma, so it runs at the highest priority), then K5 luma
+  cudaStreamWaitEvent(lstream, ev_guard, 0);
   LineArgs la = line_args(P);
   {
     cudaEvent_t ev_;
-    begin_stage(kStageHsync, ev_);
-    launch_hsync_refine(la, stream);
-    end_stage(kStageHsync, ev_);
+    begin_stage_on(kStageHsync, ev_, lstream);
+    launch_hsync_refine(la, lstream);
+    end_stage_on(kStageHsync, ev_, lstream);
   }
   // ---- chroma track detection of a chunk without carried chroma state
   // (chroma_decode.cu:684-743): both trial passes over field 0 in one launch
   // and the device pick, on the pre-band-pass stream (they need its output
   // and field 0's refined line starts), beside luma and dropouts
   // (the chroma passes follow on the same stream, after the refinement)
-  cudaEventRecord(ev_hs, stream);
+  cudaEventRecord(ev_hs, lstream);
+  cudaStreamWaitEvent(stream, ev_hs, 0);
   cudaStreamWaitEvent(pstream, ev_hs, 0);
   const bool trial_on_device = !chroma_valid;
   if (trial_on_device) {

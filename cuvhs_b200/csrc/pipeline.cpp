@@ -835,10 +835,7 @@ bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, u
   // leave them: conceal and send them now; a retry pass that rewrites fields
   // repeats this for them (concealment only ever runs on freshly decoded lines).
   auto finish = [&](int f0, int nf) {
-    if (cs != stream) {
-      cudaEventRecord(ev_cpass, cs);
-      cudaStreamWaitEvent(stream, ev_cpass, 0);
-    }
+    if (cs != stream) cudaStreamWaitEvent(stream, ev_cpass, 0);  // the pass's lines (not its metric)
     if (conceal) {
       cudaEvent_t ev_;
       begin_stage(kStageDropouts, ev_);
@@ -857,6 +854,7 @@ bool Context::chroma_fields(ChromaArgs& ca, int P, const DropoutArgs* conceal, u
     begin_stage_on(kStageChromaLines, ev_, cs);
     launch_chroma_lines(ca, f0, nf, write, cs);
     end_stage_on(kStageChromaLines, ev_, cs);
+    cudaEventRecord(ev_cpass, cs);  // the concealment needs the lines, not the metric
     if (write) {
       begin_stage_on(kStageBurstMetric, ev_, cs);
       launch_burst_metric(ca, f0, nf, cs);  // writes hp_metric through its mapping
@@ -1184,7 +1182,7 @@ bool Context::decode_chunk(const uint8_t* src, bool src_on_device, size_t n_avai
     cudaMemcpyAsync(hp_guard + 1, d_guard_flips, sizeof(int), cudaMemcpyDeviceToHost, gstream);
     cudaEventRecord(ev_guard, gstream);
   }
-  cudaStreamWaitEvent(pstream, ev_win, 0);
+  cudaStreamWaitEvent(pstream, ev_edges, 0);
   {
     cudaEvent_t ev_;
     begin_stage_on(kStageChromaPre, ev_, pstream);

@@ -39,7 +39,7 @@
 namespace cuvhs {
 namespace {
 
-constexpr int kGT = 1024;                 // threads per CTA
+constexpr int kGT = 512;                  // threads per CTA (two CTAs per SM)
 constexpr int kN = Design::kGuardN;       // FFT length
 constexpr int kBfly = kN / 4 / kGT;       // radix-4 butterflies per thread per pass
 constexpr int kTwQ = kN / 4;              // twiddles held in shared memory: exp(-2 pi i k / kN), k < kN / 4
@@ -123,7 +123,7 @@ __device__ __forceinline__ void phase_clock(const GuardArgs& g, int y, int k) {
 }
 
 template <int FMT, class Src>
-__global__ void __launch_bounds__(kGT) guard_kernel(const __grid_constant__ Src src) {
+__global__ void __launch_bounds__(kGT, 2) guard_kernel(const __grid_constant__ Src src) {
   const GuardArgs& g = src.get();
   chain_wait();
   extern __shared__ double2 gsm[];
